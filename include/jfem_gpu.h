@@ -1,0 +1,152 @@
+/*
+ * jfem_gpu.h -- C ABI of the B200 element hot path for OpenJFEM (SOL 101/105).
+ *
+ * The library replaces the two assembly calls of the reference solver:
+ *
+ *   Solver.assemble_stiffness(model; ...)             src/solver/assembly.jl:1953-4375
+ *   Solver.assemble_geometric_stiffness(model, ...)   src/solver/assembly.jl:4382-6634
+ *
+ * called from _solve_sol105 / solve_model at src/JFEMSolver.jl:807-810 and
+ * :1452-1457.  The caller keeps its own model build, SPC/MPC reduction,
+ * factorization and eigensolve; this library only produces the same sparse
+ * matrices (Julia SparseMatrixCSC{Float64,Int64} arrays: 1-based colptr,
+ * rowval, nzval) that those two functions return.
+ *
+ * Every entry point takes plain pointers and sizes.  Host arrays are owned by
+ * the caller; the library copies what it needs and keeps no pointer into
+ * caller memory after a call returns.  Device state (mesh, property records,
+ * CSR pattern, element-to-nonzero scatter map, staging) is owned by the
+ * jfg_model handle until jfg_model_destroy.  Calls on one handle must not
+ * overlap; different handles are independent.
+ *
+ * Errors: every entry returns a jfg_status.  On failure the handle keeps a
+ * message (jfg_last_error), mirroring the reference's error(...) calls.
+ */
+#ifndef JFEM_GPU_H
+#define JFEM_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t jfg_status;
+enum {
+    JFG_OK = 0,
+    JFG_ERR_INVALID = 1,      /* malformed input (bad index, size, null pointer) */
+    JFG_ERR_UNSUPPORTED = 2,  /* deck leaves the reference's default branch */
+    JFG_ERR_CUDA = 3,         /* CUDA runtime error */
+    JFG_ERR_TIMEOUT = 4,      /* a bounded device wait expired */
+    JFG_ERR_STATE = 5,        /* call order violated (e.g. no pattern yet) */
+    JFG_ERR_NOMEM = 6,        /* device or host allocation failed */
+    JFG_ERR_REFERENCE_RAISES = 7 /* the reference raises on this input (see message) */
+};
+
+/* Per-shell property record, 7 doubles per element, in this order:
+ *   h      PSHELL T
+ *   E, nu  MAT1 of MID (membrane/bending), G completed as extract_mats does
+ *   G      MAT1 G of MID
+ *   br     PSHELL 12I/T^3 (BEND_RATIO; 0 when MID2 is blank)
+ *   tst    PSHELL TS/T (default 5/6)
+ *   Gs     shear modulus of the MID3 material (MID when MID3 is blank)
+ * Constitutive build: assembly.jl:2460-2469, shell_transverse_shear_matrix
+ * assembly.jl:1808-1856. */
+#define JFG_SHELL_PROP 7
+
+/* Per-bar record (CBAR and CBEAM, identical in the reference), 18 doubles:
+ *   A, I1, I2, I12, J, K1, K2   PBARL/PBAR section (extract_pbarl)
+ *   E, G                        MAT1
+ *   vx, vy, vz                  orientation vector in basic (G0 resolved by caller)
+ *   wax, way, waz, wbx, wby, wbz  CBAR offsets WA, WB
+ * Element: assembly.jl:3961-4092 (K), :6277-6424 (KG). */
+#define JFG_BAR_PROP 18
+
+typedef struct jfg_model_desc {
+    int64_t n_nodes;            /* nodes in id_map order (sorted GRID IDs)           */
+    const double *coords;       /* n_nodes*3, basic system                           */
+    const double *node_R;       /* n_nodes*9 row-major CD frames, or NULL (all basic)*/
+    int64_t n_quad4;
+    const int32_t *quad4_nodes; /* n_quad4*4, 0-based node indices                   */
+    const double *quad4_prop;   /* n_quad4*JFG_SHELL_PROP                           */
+    int64_t n_tria3;
+    const int32_t *tria3_nodes; /* n_tria3*3                                         */
+    const double *tria3_prop;   /* n_tria3*JFG_SHELL_PROP                           */
+    int64_t n_bar;
+    const int32_t *bar_nodes;   /* n_bar*2 (GA, GB)                                  */
+    const double *bar_prop;     /* n_bar*JFG_BAR_PROP                               */
+    const int32_t *bar_pin;     /* n_bar*2 (PA, PB) or NULL                          */
+    int64_t n_rbe2;
+    const int32_t *rbe2_master; /* n_rbe2, GN node index                             */
+    const int32_t *rbe2_cm;     /* n_rbe2, CM components as bit mask (bit0 = comp 1) */
+    const int64_t *rbe2_slave_ptr; /* n_rbe2+1                                       */
+    const int32_t *rbe2_slaves; /* GM node indices                                   */
+    double k6rot;               /* PARAM K6ROT (reference default 100)               */
+    double param_snorm;         /* PARAM SNORM; must be <= 0 (default branch)        */
+} jfg_model_desc;
+
+typedef struct jfg_model jfg_model;
+
+/* Build a handle: validates the default-branch predicates, uploads the mesh,
+ * builds the CSR pattern and the element-to-nonzero scatter map on the GPU.
+ * Replaces the per-call node indexing, pre-extraction and sparse() pattern
+ * work of assemble_stiffness (assembly.jl:1957-2536, :4371). */
+jfg_status jfg_model_create(const jfg_model_desc *desc, jfg_model **out);
+
+/* Size of the assembled matrices: ndof = 6*n_nodes and the structural
+ * nonzero count of K (identical for KG on the supported element set). */
+jfg_status jfg_pattern(jfg_model *m, int64_t *ndof, int64_t *nnz);
+
+/* Fill caller-allocated CSC arrays (colptr: ndof+1, rowval: nnz), 1-based,
+ * rows sorted within each column -- SparseArrays.sparse semantics with
+ * explicit zeros kept (assembly.jl:4371, :6624). */
+jfg_status jfg_pattern_fill(jfg_model *m, int64_t *colptr, int64_t *rowval);
+
+/* Stiffness assembly (assemble_stiffness, assembly.jl:1953-4375).
+ * nzval: nnz doubles in CSC order; max_elem_stiff: max |V| over element
+ * triplets before constraints (:4353-4356); orig_diag: ndof doubles, sum of
+ * element diagonal triplets before constraints (:4359-4364).  Any output
+ * pointer may be NULL to skip it.  All pointers are host memory. */
+jfg_status jfg_assemble_k(jfg_model *m, double *nzval, double *max_elem_stiff, double *orig_diag);
+
+/* Geometric stiffness assembly (assemble_geometric_stiffness,
+ * assembly.jl:4382-6634) from the static displacement u_global (ndof
+ * doubles, node displacement systems).  Host pointers. */
+jfg_status jfg_assemble_kg(jfg_model *m, const double *u_global, double *nzval);
+
+/* Device-resident variants: the same work with all pointers in device
+ * memory on the handle's stream (no host copies).  nzval_dev is nnz doubles;
+ * orig_diag_dev (ndof) and max_elem_stiff_dev (1) may be NULL. */
+jfg_status jfg_assemble_k_device(jfg_model *m, double *nzval_dev, double *max_elem_stiff_dev,
+                                 double *orig_diag_dev);
+jfg_status jfg_assemble_kg_device(jfg_model *m, const double *u_global_dev, double *nzval_dev);
+
+/* Replace the per-element shell thicknesses (PSHELL T) in place; the mesh,
+ * pattern and scatter map stay resident.  Semantics of the thickness update
+ * of optimize_thickness.jl:209-240 / :307-313.  Host pointers, n_quad4 and
+ * n_tria3 doubles (either may be NULL to keep the current values). */
+jfg_status jfg_update_properties(jfg_model *m, const double *quad4_h, const double *tria3_h);
+
+/* Multipoint-constraint map returned by assemble_stiffness as rbe3_map
+ * (constraints.jl:319, merged at :319-322): dependent dof -> list of
+ * (independent dof, coefficient), 1-based dofs.  Query the sizes with NULL
+ * arrays first: n_dep entries, n_terms pairs in total. */
+jfg_status jfg_constraint_map(jfg_model *m, int64_t *n_dep, int64_t *n_terms,
+                              int64_t *dep_dof, int64_t *term_ptr, int64_t *ind_dof, double *coeff);
+
+/* Set the CUDA stream (a cudaStream_t passed as void*) used by the handle;
+ * NULL selects the handle's own stream. */
+jfg_status jfg_set_stream(jfg_model *m, void *stream);
+
+/* Timing of the last assembly on the device (CUDA events around the element
+ * kernels and the segmented reduction), milliseconds. */
+jfg_status jfg_last_timing(jfg_model *m, double *element_ms, double *reduce_ms, double *total_ms);
+
+void jfg_model_destroy(jfg_model *m);
+const char *jfg_last_error(jfg_model *m);
+const char *jfg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* JFEM_GPU_H */

@@ -1,0 +1,1008 @@
+// jfg_api.cu -- C ABI of the B200 element hot path (include/jfem_gpu.h).
+//
+// Handle life cycle:
+//   jfg_model_create  validate the default-branch predicates, upload the mesh,
+//                     build the CSR pattern and the element-entry -> sorted
+//                     contribution slot map on the GPU (radix sort of
+//                     (row, col) keys), RBE2 expansion for the few elements
+//                     that touch dependent dofs (constraints.jl:37-74,
+//                     :329-361).
+//   jfg_assemble_k    element kernels write every packed element-matrix
+//                     value to its slot, a segmented reduction sums each
+//                     nonzero's contiguous segment in a fixed order and writes
+//                     it to both symmetric CSC positions.  No floating-point
+//                     atomics: K and KG are bitwise repeatable.
+//   jfg_assemble_kg   same pipeline with the KG element kernels.
+//
+// Pattern semantics are those of SparseArrays.sparse over the reference's
+// triplets (assembly.jl:4371, :6624): every element entry is a structural
+// nonzero (explicit zeros kept), dependent dofs of RBE2 sets are replaced by
+// their weighted independent images with |coeff| > 1e-15
+// (constraints.jl:25-34), and zero-length bars contribute nothing.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+
+#include "../../include/jfem_gpu.h"
+#include "elem_bar.cuh"
+#include "elem_q4.cuh"
+#include "elem_t3.cuh"
+
+using namespace jfg;
+
+namespace {
+
+constexpr uint64_t kSentinel = ~0ull;
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct jfg_model {
+    std::string err;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own = nullptr;
+    bool own_stream = false;
+    int device = 0;
+    int64_t n_nodes = 0, ndof = 0, nq = 0, nt = 0, nb = 0;
+    double k6rot = 100.0;
+    bool has_nodeR = false;
+    bool bar_offsets = false;
+    // device mesh
+    double *d_coords = nullptr, *d_nodeR = nullptr;
+    int32_t *d_q4n = nullptr, *d_t3n = nullptr, *d_barn = nullptr;
+    double *d_q4p = nullptr, *d_t3p = nullptr, *d_barp = nullptr;
+    // scatter map
+    int32_t *d_slot = nullptr;          // packed slots, all types concatenated
+    int64_t slot_q4 = 0, slot_t3 = 0, slot_bar = 0, n_slots = 0;
+    int64_t n_contrib = 0, n_upper = 0, nnz = 0;
+    double *d_staging = nullptr;
+    double *d_exc_raw = nullptr;
+    int64_t n_exc_raw = 0, n_exc = 0;
+    int32_t *d_exc_q = nullptr, *d_exc_src = nullptr;
+    double *d_exc_w = nullptr;
+    int32_t *d_seg = nullptr;           // n_upper + 1 contribution segment bounds
+    int64_t *d_posA = nullptr, *d_posB = nullptr;
+    int64_t *d_rowptr = nullptr, *d_colind = nullptr;   // 0-based symmetric CSR == CSC
+    // orig_diag map
+    int32_t *d_dslot = nullptr;
+    int64_t dslot_q4 = 0, dslot_t3 = 0, dslot_bar = 0;
+    int32_t *d_dseg = nullptr;           // ndof + 1
+    double *d_dstaging = nullptr;
+    int64_t n_dcontrib = 0;
+    // work buffers
+    double *d_nz = nullptr, *d_u = nullptr, *d_diag = nullptr, *d_max = nullptr, *d_h = nullptr;
+    // constraint map (host, 0-based dofs)
+    std::vector<int64_t> dep_dof, dep_ptr, dep_ind;
+    std::vector<double> dep_coef;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    float last_elem_ms = 0.f, last_reduce_ms = 0.f, last_total_ms = 0.f;
+    std::vector<void *> allocs;
+};
+
+namespace {
+
+jfg_status fail(jfg_model *m, jfg_status st, const std::string &msg) {
+    if (m) m->err = msg;
+    return st;
+}
+
+#define CK(call)                                                                                     \
+    do {                                                                                             \
+        cudaError_t _e = (call);                                                                     \
+        if (_e != cudaSuccess)                                                                       \
+            return fail(m, _e == cudaErrorMemoryAllocation ? JFG_ERR_NOMEM : JFG_ERR_CUDA,           \
+                        std::string(#call) + ": " + cudaGetErrorString(_e));                         \
+    } while (0)
+
+template <typename T>
+cudaError_t dalloc(jfg_model *m, T **p, size_t n) {
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    if (e == cudaSuccess) m->allocs.push_back(*p);
+    return e;
+}
+
+inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// ---------------------------------------------------------------------------
+// host-side geometry checks (same tests as the K/KG loops)
+// ---------------------------------------------------------------------------
+
+bool host_q4_flat(const double *p1, const double *p2, const double *p3, const double *p4) {
+    double d13[3], d24[3], n[3], c[3];
+    sub3(p3, p1, d13);
+    sub3(p4, p2, d24);
+    cross3(d13, d24, n);
+    double len = std::sqrt(dot3(n, n));
+    for (int i = 0; i < 3; ++i) c[i] = (p1[i] + p2[i] + p3[i] + p4[i]) / 4.0;
+    double maxdev = 0.0;
+    if (len > 1e-12) {
+        double g[3] = {n[0] / len, n[1] / len, n[2] / len};
+        const double *ps[4] = {p1, p2, p3, p4};
+        for (int k = 0; k < 4; ++k) {
+            double d[3];
+            sub3(ps[k], c, d);
+            maxdev = std::max(maxdev, std::fabs(dot3(d, g)));
+        }
+    }
+    double L = std::max(std::sqrt(dot3(d13, d13)), std::sqrt(dot3(d24, d24)));
+    return maxdev < 1e-6 * std::max(L, 1e-12);
+}
+
+// RBE2 dependent -> independent map (constraints.jl:7-74), 0-based dofs.
+void build_rbe2(const jfg_model_desc *d, std::map<int64_t, std::vector<std::pair<int64_t, double>>> &mp) {
+    auto R_of = [&](int64_t n, double *tmp) -> const double * {
+        if (d->node_R) return d->node_R + 9 * n;
+        for (int i = 0; i < 9; ++i) tmp[i] = (i % 4 == 0) ? 1.0 : 0.0;
+        return tmp;
+    };
+    for (int64_t r = 0; r < d->n_rbe2; ++r) {
+        int64_t gm = d->rbe2_master[r];
+        const double *pm = d->coords + 3 * gm;
+        double tm[9];
+        const double *Rm = R_of(gm, tm);
+        for (int64_t s = d->rbe2_slave_ptr[r]; s < d->rbe2_slave_ptr[r + 1]; ++s) {
+            int64_t gs = d->rbe2_slaves[s];
+            const double *ps = d->coords + 3 * gs;
+            double dx = ps[0] - pm[0], dy = ps[1] - pm[1], dz = ps[2] - pm[2];
+            double ts[9];
+            const double *Rs = R_of(gs, ts);
+            double comp[3][3], O[3][3] = {{0.0, dz, -dy}, {-dz, 0.0, dx}, {dy, -dx, 0.0}}, RsO[3][3], off[3][3];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) comp[i][j] = Rs[i] * Rm[j] + Rs[3 + i] * Rm[3 + j] + Rs[6 + i] * Rm[6 + j];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) RsO[i][j] = Rs[i] * O[0][j] + Rs[3 + i] * O[1][j] + Rs[6 + i] * O[2][j];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) off[i][j] = RsO[i][0] * Rm[j] + RsO[i][1] * Rm[3 + j] + RsO[i][2] * Rm[6 + j];
+            for (int c = 1; c <= 6; ++c) {
+                if (!(d->rbe2_cm[r] & (1 << (c - 1)))) continue;
+                double row[6];
+                if (c <= 3) {
+                    for (int j = 0; j < 3; ++j) { row[j] = comp[c - 1][j]; row[3 + j] = off[c - 1][j]; }
+                } else {
+                    for (int j = 0; j < 3; ++j) { row[j] = 0.0; row[3 + j] = comp[c - 4][j]; }
+                }
+                std::vector<std::pair<int64_t, double>> pairs;
+                for (int j = 0; j < 6; ++j)
+                    if (std::fabs(row[j]) > 1e-15) pairs.push_back({6 * gm + j, row[j]});
+                if (!pairs.empty()) mp[6 * gs + (c - 1)] = pairs;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// pattern kernels
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void unpack_index(int p, int N, int &i, int &j) {
+    int row = 0, start = 0;
+    while (p >= start + (N - row)) { start += N - row; ++row; }
+    i = row;
+    j = row + (p - start);
+}
+
+__global__ void gen_keys_kernel(int64_t ne, int NN, const int32_t *__restrict__ nodes, const uint8_t *__restrict__ regular,
+                                int64_t base, int64_t ndof, uint64_t *keys, int32_t *vals) {
+    const int N = 6 * NN, P = N * (N + 1) / 2;
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ne * P) return;
+    int64_t e = t / P;
+    int p = (int)(t - e * P);
+    uint64_t key = kSentinel;
+    if (regular[e]) {
+        int i, j;
+        unpack_index(p, N, i, j);
+        int64_t r = 6 * (int64_t)nodes[NN * e + i / 6] + i % 6;
+        int64_t c = 6 * (int64_t)nodes[NN * e + j / 6] + j % 6;
+        int64_t lo = r < c ? r : c, hi = r < c ? c : r;
+        key = (uint64_t)lo * (uint64_t)ndof + (uint64_t)hi;
+    }
+    keys[base + t] = key;
+    vals[base + t] = (int32_t)(base + t);
+}
+
+__global__ void gen_diag_keys_kernel(int64_t ne, int NN, const int32_t *__restrict__ nodes, const uint8_t *__restrict__ active,
+                                     int64_t base, uint32_t *keys, int32_t *vals) {
+    const int N = 6 * NN;
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ne * N) return;
+    int64_t e = t / N;
+    int i = (int)(t - e * N);
+    keys[base + t] = active[e] ? (uint32_t)(6 * (int64_t)nodes[NN * e + i / 6] + i % 6) : 0xffffffffu;
+    vals[base + t] = (int32_t)(base + t);
+}
+
+__global__ void head_flags_kernel(int64_t n, const uint64_t *__restrict__ keys, int32_t *flags) {
+    int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    flags[q] = (q == 0 || keys[q] != keys[q - 1]) ? 1 : 0;
+}
+
+__global__ void seg_kernel(int64_t n, const int32_t *__restrict__ flags, const int32_t *__restrict__ upos,
+                           const uint64_t *__restrict__ keys, int64_t ndof, int32_t *seg, uint64_t *ukeys,
+                           int32_t *up_row_cnt, int32_t *low_cnt) {
+    int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n || !flags[q]) return;
+    int32_t u = upos[q];
+    seg[u] = (int32_t)q;
+    uint64_t k = keys[q];
+    ukeys[u] = k;
+    int64_t r = (int64_t)(k / (uint64_t)ndof), c = (int64_t)(k % (uint64_t)ndof);
+    atomicAdd(up_row_cnt + r, 1);
+    if (r < c) atomicAdd(low_cnt + c, 1);
+}
+
+__global__ void inv_kernel(int64_t n, const int32_t *__restrict__ vals, int32_t *inv) {
+    int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    inv[vals[q]] = (int32_t)q;
+}
+
+__global__ void regular_slot_kernel(int64_t n_slots, const int32_t *__restrict__ inv, int32_t *slot) {
+    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_slots) return;
+    slot[s] = inv[s];
+}
+
+__global__ void scatter_i32_kernel(int64_t n, const int64_t *__restrict__ idx, const int32_t *__restrict__ val, int32_t *dst) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    dst[idx[t]] = val[t];
+}
+
+__global__ void rowcnt_kernel(int64_t ndof, const int32_t *__restrict__ up, const int32_t *__restrict__ low, int64_t *cnt) {
+    int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= ndof) return;
+    cnt[r] = (int64_t)up[r] + (int64_t)low[r];
+}
+
+__global__ void posA_kernel(int64_t n_upper, const uint64_t *__restrict__ ukeys, int64_t ndof,
+                            const int64_t *__restrict__ rowptr, const int32_t *__restrict__ low_cnt,
+                            const int64_t *__restrict__ up_row_start, int64_t *posA, int64_t *colind,
+                            uint32_t *lowkeys, int32_t *lowvals, int32_t *lowflag) {
+    int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= n_upper) return;
+    uint64_t k = ukeys[u];
+    int64_t r = (int64_t)(k / (uint64_t)ndof), c = (int64_t)(k % (uint64_t)ndof);
+    int64_t pa = rowptr[r] + low_cnt[r] + (u - up_row_start[r]);
+    posA[u] = pa;
+    colind[pa] = c;
+    lowkeys[u] = r < c ? (uint32_t)c : 0xffffffffu;
+    lowvals[u] = (int32_t)u;
+    lowflag[u] = r < c ? 1 : 0;
+}
+
+__global__ void posB_kernel(int64_t n_low, const uint32_t *__restrict__ skeys, const int32_t *__restrict__ svals,
+                            const int64_t *__restrict__ low_start, const int64_t *__restrict__ rowptr,
+                            const uint64_t *__restrict__ ukeys, int64_t ndof, int64_t *posB, int64_t *colind) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_low) return;
+    int64_t c = skeys[t];
+    int32_t u = svals[t];
+    int64_t rank = t - low_start[c];
+    int64_t pb = rowptr[c] + rank;
+    posB[u] = pb;
+    colind[pb] = (int64_t)(ukeys[u] / (uint64_t)ndof);
+}
+
+__global__ void fill_i64_kernel(int64_t n, int64_t v, int64_t *dst) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) dst[t] = v;
+}
+
+__global__ void diag_seg_kernel(int64_t n, const uint32_t *__restrict__ keys, int32_t *cnt) {
+    int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    uint32_t k = keys[q];
+    if (k != 0xffffffffu) atomicAdd(cnt + k, 1);
+}
+
+// ---------------------------------------------------------------------------
+// assembly kernels
+// ---------------------------------------------------------------------------
+
+__global__ void expand_kernel(int64_t n, const int32_t *__restrict__ q, const int32_t *__restrict__ src,
+                              const double *__restrict__ w, const double *__restrict__ raw, double *staging) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    staging[q[t]] = w[t] * raw[src[t]];
+}
+
+// Deterministic segmented reduction: nonzero u sums staging[seg[u], seg[u+1])
+// left to right and writes both symmetric CSC positions.
+__global__ void __launch_bounds__(256) reduce_kernel(int64_t n_upper, const int32_t *__restrict__ seg,
+                                                     const double *__restrict__ staging, const int64_t *__restrict__ posA,
+                                                     const int64_t *__restrict__ posB, double *nz) {
+    int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= n_upper) return;
+    int32_t a = __ldg(seg + u), b = __ldg(seg + u + 1);
+    double s = 0.0;
+    for (int32_t q = a; q < b; ++q) s += __ldg(staging + q);
+    nz[__ldg(posA + u)] = s;
+    int64_t pb = __ldg(posB + u);
+    if (pb >= 0) nz[pb] = s;
+}
+
+__global__ void diag_reduce_kernel(int64_t ndof, const int32_t *__restrict__ seg, const double *__restrict__ st, double *out) {
+    int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= ndof) return;
+    double s = 0.0;
+    for (int32_t q = seg[d]; q < seg[d + 1]; ++q) s += st[q];
+    out[d] = s;
+}
+
+__global__ void set_h_kernel(int64_t n, const double *__restrict__ h, double *prop) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n) prop[7 * e] = h[e];
+}
+
+template <typename K, typename V>
+cudaError_t radix_sort(jfg_model *m, K *kin, K *kout, V *vin, V *vout, int64_t n, int end_bit) {
+    size_t tmp = 0;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, tmp, kin, kout, vin, vout, n, 0, end_bit, m->stream);
+    if (e != cudaSuccess) return e;
+    void *d_tmp = nullptr;
+    e = cudaMallocAsync(&d_tmp, tmp, m->stream);
+    if (e != cudaSuccess) return e;
+    e = cub::DeviceRadixSort::SortPairs(d_tmp, tmp, kin, kout, vin, vout, n, 0, end_bit, m->stream);
+    cudaFreeAsync(d_tmp, m->stream);
+    return e;
+}
+
+template <typename T, typename U>
+cudaError_t exclusive_sum(jfg_model *m, T *in, U *out, int64_t n) {
+    size_t tmp = 0;
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, tmp, in, out, n, m->stream);
+    if (e != cudaSuccess) return e;
+    void *d_tmp = nullptr;
+    e = cudaMallocAsync(&d_tmp, tmp, m->stream);
+    if (e != cudaSuccess) return e;
+    e = cub::DeviceScan::ExclusiveSum(d_tmp, tmp, in, out, n, m->stream);
+    cudaFreeAsync(d_tmp, m->stream);
+    return e;
+}
+
+jfg_status validate(jfg_model *m, const jfg_model_desc *d) {
+    if (!d) return fail(m, JFG_ERR_INVALID, "null descriptor");
+    if (d->n_nodes <= 0 || !d->coords) return fail(m, JFG_ERR_INVALID, "model has no nodes (is this a standalone deck?)");
+    if (d->param_snorm > 0.0) return fail(m, JFG_ERR_UNSUPPORTED, "PARAM,SNORM > 0 leaves the default branch (snorm.jl:72-83)");
+    if ((d->n_quad4 && (!d->quad4_nodes || !d->quad4_prop)) || (d->n_tria3 && (!d->tria3_nodes || !d->tria3_prop)) ||
+        (d->n_bar && (!d->bar_nodes || !d->bar_prop)) ||
+        (d->n_rbe2 && (!d->rbe2_master || !d->rbe2_cm || !d->rbe2_slave_ptr || !d->rbe2_slaves)))
+        return fail(m, JFG_ERR_INVALID, "null array for a non-empty element set");
+    if (6 * d->n_nodes >= (int64_t)1 << 31) return fail(m, JFG_ERR_UNSUPPORTED, "more than 2^31 dofs");
+    for (int64_t e = 0; e < d->n_quad4; ++e) {
+        const int32_t *n = d->quad4_nodes + 4 * e;
+        for (int k = 0; k < 4; ++k)
+            if (n[k] < 0 || n[k] >= d->n_nodes) return fail(m, JFG_ERR_INVALID, "CQUAD4 node index out of range");
+        const double *pr = d->quad4_prop + JFG_SHELL_PROP * e;
+        if (!(pr[0] > 0.0) || !(pr[1] > 0.0)) return fail(m, JFG_ERR_INVALID, "shell thickness and E must be positive");
+        if (!host_q4_flat(d->coords + 3 * n[0], d->coords + 3 * n[1], d->coords + 3 * n[2], d->coords + 3 * n[3]))
+            return fail(m, JFG_ERR_UNSUPPORTED,
+                        "non-flat CQUAD4 (warp >= 1e-6 of the diagonal) leaves the flat default branch (assembly.jl:2824-2840)");
+    }
+    for (int64_t e = 0; e < d->n_tria3; ++e) {
+        for (int k = 0; k < 3; ++k) {
+            int32_t n = d->tria3_nodes[3 * e + k];
+            if (n < 0 || n >= d->n_nodes) return fail(m, JFG_ERR_INVALID, "CTRIA3 node index out of range");
+        }
+        const double *pr = d->tria3_prop + JFG_SHELL_PROP * e;
+        if (!(pr[0] > 0.0) || !(pr[1] > 0.0)) return fail(m, JFG_ERR_INVALID, "shell thickness and E must be positive");
+    }
+    for (int64_t e = 0; e < d->n_bar; ++e) {
+        for (int k = 0; k < 2; ++k) {
+            int32_t n = d->bar_nodes[2 * e + k];
+            if (n < 0 || n >= d->n_nodes) return fail(m, JFG_ERR_INVALID, "CBAR node index out of range");
+        }
+        if (d->bar_pin && (d->bar_pin[2 * e] != 0 || d->bar_pin[2 * e + 1] != 0))
+            return fail(m, JFG_ERR_UNSUPPORTED, "CBAR pin flags PA/PB are outside the supported branch (helpers.jl:1630-1660)");
+    }
+    for (int64_t r = 0; r < d->n_rbe2; ++r) {
+        if (d->rbe2_master[r] < 0 || d->rbe2_master[r] >= d->n_nodes) return fail(m, JFG_ERR_INVALID, "RBE2 GN out of range");
+        for (int64_t s = d->rbe2_slave_ptr[r]; s < d->rbe2_slave_ptr[r + 1]; ++s)
+            if (d->rbe2_slaves[s] < 0 || d->rbe2_slaves[s] >= d->n_nodes) return fail(m, JFG_ERR_INVALID, "RBE2 GM out of range");
+    }
+    return JFG_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+const char *jfg_version(void) { return "jfem-b200 0.1 (sm_100a, fp64)"; }
+
+const char *jfg_last_error(jfg_model *m) { return m ? m->err.c_str() : "null handle"; }
+
+void jfg_model_destroy(jfg_model *m) {
+    if (!m) return;
+    if (m->stream) cudaStreamSynchronize(m->stream);
+    for (void *p : m->allocs) cudaFree(p);
+    for (auto &e : m->ev)
+        if (e) cudaEventDestroy(e);
+    if (m->own_stream && m->own) {
+        cudaStreamSynchronize(m->own);
+        cudaStreamDestroy(m->own);
+    }
+    delete m;
+}
+
+jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
+    if (!out) return JFG_ERR_INVALID;
+    *out = nullptr;
+    jfg_model *m = new jfg_model();
+    *out = m;
+    jfg_status st = validate(m, d);
+    if (st) return st;
+    CK(cudaGetDevice(&m->device));
+    CK(cudaStreamCreateWithFlags(&m->own, cudaStreamNonBlocking));
+    m->stream = m->own;
+    m->own_stream = true;
+    for (auto &e : m->ev) CK(cudaEventCreate(&e));
+    m->n_nodes = d->n_nodes;
+    m->ndof = 6 * d->n_nodes;
+    m->nq = d->n_quad4;
+    m->nt = d->n_tria3;
+    m->nb = d->n_bar;
+    m->k6rot = d->k6rot;
+    m->has_nodeR = d->node_R != nullptr;
+    const int64_t ndof = m->ndof;
+
+    // --- mesh upload ---
+    CK(dalloc(m, &m->d_coords, 3 * m->n_nodes));
+    CK(cudaMemcpyAsync(m->d_coords, d->coords, sizeof(double) * 3 * m->n_nodes, cudaMemcpyHostToDevice, m->stream));
+    if (m->has_nodeR) {
+        CK(dalloc(m, &m->d_nodeR, 9 * m->n_nodes));
+        CK(cudaMemcpyAsync(m->d_nodeR, d->node_R, sizeof(double) * 9 * m->n_nodes, cudaMemcpyHostToDevice, m->stream));
+    }
+    CK(dalloc(m, &m->d_q4n, 4 * m->nq));
+    CK(dalloc(m, &m->d_q4p, JFG_SHELL_PROP * m->nq));
+    CK(dalloc(m, &m->d_t3n, 3 * m->nt));
+    CK(dalloc(m, &m->d_t3p, JFG_SHELL_PROP * m->nt));
+    CK(dalloc(m, &m->d_barn, 2 * m->nb));
+    CK(dalloc(m, &m->d_barp, JFG_BAR_PROP * m->nb));
+    if (m->nq) {
+        CK(cudaMemcpyAsync(m->d_q4n, d->quad4_nodes, sizeof(int32_t) * 4 * m->nq, cudaMemcpyHostToDevice, m->stream));
+        CK(cudaMemcpyAsync(m->d_q4p, d->quad4_prop, sizeof(double) * JFG_SHELL_PROP * m->nq, cudaMemcpyHostToDevice, m->stream));
+    }
+    if (m->nt) {
+        CK(cudaMemcpyAsync(m->d_t3n, d->tria3_nodes, sizeof(int32_t) * 3 * m->nt, cudaMemcpyHostToDevice, m->stream));
+        CK(cudaMemcpyAsync(m->d_t3p, d->tria3_prop, sizeof(double) * JFG_SHELL_PROP * m->nt, cudaMemcpyHostToDevice, m->stream));
+    }
+    if (m->nb) {
+        CK(cudaMemcpyAsync(m->d_barn, d->bar_nodes, sizeof(int32_t) * 2 * m->nb, cudaMemcpyHostToDevice, m->stream));
+        CK(cudaMemcpyAsync(m->d_barp, d->bar_prop, sizeof(double) * JFG_BAR_PROP * m->nb, cudaMemcpyHostToDevice, m->stream));
+    }
+
+    // --- constraint map and exception elements ---
+    std::map<int64_t, std::vector<std::pair<int64_t, double>>> mp;
+    build_rbe2(d, mp);
+    std::vector<const std::vector<std::pair<int64_t, double>> *> dep(ndof, nullptr);
+    std::vector<uint8_t> node_dep(m->n_nodes, 0);
+    for (auto &kv : mp) {
+        dep[kv.first] = &kv.second;
+        node_dep[kv.first / 6] = 1;
+        m->dep_dof.push_back(kv.first);
+    }
+    m->dep_ptr.push_back(0);
+    for (auto &kv : mp) {
+        for (auto &p : kv.second) { m->dep_ind.push_back(p.first); m->dep_coef.push_back(p.second); }
+        m->dep_ptr.push_back((int64_t)m->dep_ind.size());
+    }
+    // element flags: 1 = regular, 0 = exception (touches a dependent dof) or inactive
+    std::vector<uint8_t> reg_q4(m->nq, 1), reg_t3(m->nt, 1), reg_bar(m->nb, 1), act_bar(m->nb, 1);
+    for (int64_t e = 0; e < m->nq; ++e)
+        for (int k = 0; k < 4; ++k)
+            if (node_dep[d->quad4_nodes[4 * e + k]]) reg_q4[e] = 0;
+    for (int64_t e = 0; e < m->nt; ++e)
+        for (int k = 0; k < 3; ++k)
+            if (node_dep[d->tria3_nodes[3 * e + k]]) reg_t3[e] = 0;
+    for (int64_t e = 0; e < m->nb; ++e) {
+        const double *pr = d->bar_prop + JFG_BAR_PROP * e;
+        const double *p1 = d->coords + 3 * (int64_t)d->bar_nodes[2 * e], *p2 = d->coords + 3 * (int64_t)d->bar_nodes[2 * e + 1];
+        double wa[3] = {pr[12], pr[13], pr[14]}, wb[3] = {pr[15], pr[16], pr[17]};
+        bool off = dot3(wa, wa) > 1e-20 || dot3(wb, wb) > 1e-20;
+        double dd[3];
+        for (int i = 0; i < 3; ++i) dd[i] = (off ? p2[i] + wb[i] : p2[i]) - (off ? p1[i] + wa[i] : p1[i]);
+        if (std::sqrt(dot3(dd, dd)) < 1e-9) { act_bar[e] = 0; reg_bar[e] = 0; continue; }
+        if (off) m->bar_offsets = true;
+        for (int k = 0; k < 2; ++k)
+            if (node_dep[d->bar_nodes[2 * e + k]]) reg_bar[e] = 0;
+    }
+    m->slot_q4 = 0;
+    m->slot_t3 = m->nq * 300;
+    m->slot_bar = m->slot_t3 + m->nt * 171;
+    m->n_slots = m->slot_bar + m->nb * 78;
+    if (m->n_slots >= ((int64_t)1 << 31) - 1) return fail(m, JFG_ERR_UNSUPPORTED, "more than 2^31 element entries in one handle");
+
+    // host expansion of exception elements: ordered local pairs -> (key, raw src, weight)
+    struct ExcC { uint64_t key; int32_t src; double w; };
+    std::vector<ExcC> exc;
+    std::vector<int64_t> exc_slot_idx;    // packed slot s that becomes a raw-buffer reference
+    std::vector<int32_t> exc_slot_code;
+    int64_t raw_count = 0;
+    auto expand_elem = [&](const int32_t *nodes, int NN, int64_t slot_base) {
+        const int N = 6 * NN, P = N * (N + 1) / 2;
+        int64_t raw_base = raw_count;
+        raw_count += P;
+        for (int p = 0; p < P; ++p) {
+            exc_slot_idx.push_back(slot_base + p);
+            exc_slot_code.push_back((int32_t)(-(raw_base + p) - 1));
+        }
+        std::map<std::pair<uint64_t, int32_t>, double> acc;
+        for (int i = 0; i < N; ++i)
+            for (int j = 0; j < N; ++j) {
+                int64_t r = 6 * (int64_t)nodes[i / 6] + i % 6, c = 6 * (int64_t)nodes[j / 6] + j % 6;
+                std::vector<std::pair<int64_t, double>> ri, cj;
+                if (dep[r]) ri = *dep[r]; else ri.push_back({r, 1.0});
+                if (dep[c]) cj = *dep[c]; else cj.push_back({c, 1.0});
+                int pi = std::min(i, j), pj = std::max(i, j);
+                int32_t src = (int32_t)(raw_base + packed_index(pi, pj, N));
+                for (auto &a : ri)
+                    for (auto &b : cj) {
+                        if (a.first > b.first) continue;
+                        uint64_t key = (uint64_t)a.first * (uint64_t)ndof + (uint64_t)b.first;
+                        acc[{key, src}] += a.second * b.second;
+                    }
+            }
+        for (auto &kv : acc) exc.push_back({kv.first.first, kv.first.second, kv.second});
+    };
+    for (int64_t e = 0; e < m->nq; ++e)
+        if (!reg_q4[e]) expand_elem(d->quad4_nodes + 4 * e, 4, m->slot_q4 + e * 300);
+    for (int64_t e = 0; e < m->nt; ++e)
+        if (!reg_t3[e]) expand_elem(d->tria3_nodes + 3 * e, 3, m->slot_t3 + e * 171);
+    for (int64_t e = 0; e < m->nb; ++e)
+        if (!reg_bar[e] && act_bar[e]) expand_elem(d->bar_nodes + 2 * e, 2, m->slot_bar + e * 78);
+    int64_t n_inactive_slots = 0, n_exc_only = (int64_t)exc_slot_idx.size();
+    for (int64_t e = 0; e < m->nb; ++e)
+        if (!act_bar[e]) n_inactive_slots += 78;
+    m->n_exc = (int64_t)exc.size();
+    m->n_exc_raw = raw_count;
+    const int64_t S = m->n_slots;
+    const int64_t n_total = S + m->n_exc;
+    m->n_contrib = S - n_exc_only - n_inactive_slots + m->n_exc;
+    // zero-length bars never write; their slots still point at a dummy cell
+    for (int64_t e = 0; e < m->nb; ++e)
+        if (!act_bar[e])
+            for (int p = 0; p < 78; ++p) {
+                exc_slot_idx.push_back(m->slot_bar + e * 78 + p);
+                exc_slot_code.push_back((int32_t)m->n_contrib);
+            }
+    const int64_t n_exc_elem_slots = (int64_t)exc_slot_idx.size();
+    if (n_total >= ((int64_t)1 << 31) - 1) return fail(m, JFG_ERR_UNSUPPORTED, "more than 2^31 contributions in one handle");
+
+    // --- GPU key generation and sort ---
+    uint8_t *d_reg = nullptr;
+    int64_t ne_max = std::max(std::max(m->nq, m->nt), m->nb);
+    CK(cudaMallocAsync(&d_reg, std::max<int64_t>(ne_max, 1), m->stream));
+    uint64_t *d_keys = nullptr, *d_keys2 = nullptr;
+    int32_t *d_vals = nullptr, *d_vals2 = nullptr;
+    CK(cudaMallocAsync(&d_keys, sizeof(uint64_t) * std::max<int64_t>(n_total, 1), m->stream));
+    CK(cudaMallocAsync(&d_keys2, sizeof(uint64_t) * std::max<int64_t>(n_total, 1), m->stream));
+    CK(cudaMallocAsync(&d_vals, sizeof(int32_t) * std::max<int64_t>(n_total, 1), m->stream));
+    CK(cudaMallocAsync(&d_vals2, sizeof(int32_t) * std::max<int64_t>(n_total, 1), m->stream));
+    auto gen = [&](int64_t ne, int NN, const int32_t *dnodes, const std::vector<uint8_t> &reg, int64_t base) -> cudaError_t {
+        if (ne == 0) return cudaSuccess;
+        cudaError_t e = cudaMemcpyAsync(d_reg, reg.data(), ne, cudaMemcpyHostToDevice, m->stream);
+        if (e != cudaSuccess) return e;
+        int64_t P = (6 * NN) * (6 * NN + 1) / 2;
+        gen_keys_kernel<<<(unsigned)cdiv(ne * P, 256), 256, 0, m->stream>>>(ne, NN, dnodes, d_reg, base, ndof, d_keys, d_vals);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        return cudaStreamSynchronize(m->stream);  // reg buffer reused
+    };
+    CK(gen(m->nq, 4, m->d_q4n, reg_q4, m->slot_q4));
+    CK(gen(m->nt, 3, m->d_t3n, reg_t3, m->slot_t3));
+    CK(gen(m->nb, 2, m->d_barn, reg_bar, m->slot_bar));
+    if (m->n_exc) {
+        std::vector<uint64_t> hk(m->n_exc);
+        std::vector<int32_t> hv(m->n_exc);
+        for (int64_t k = 0; k < m->n_exc; ++k) { hk[k] = exc[k].key; hv[k] = (int32_t)(S + k); }
+        CK(cudaMemcpyAsync(d_keys + S, hk.data(), sizeof(uint64_t) * m->n_exc, cudaMemcpyHostToDevice, m->stream));
+        CK(cudaMemcpyAsync(d_vals + S, hv.data(), sizeof(int32_t) * m->n_exc, cudaMemcpyHostToDevice, m->stream));
+        CK(cudaStreamSynchronize(m->stream));
+    }
+    int end_bit = 64;  // sentinel uses all bits
+    CK(radix_sort(m, d_keys, d_keys2, d_vals, d_vals2, n_total, end_bit));
+    const int64_t nv = m->n_contrib;  // valid (non-sentinel) prefix
+
+    // --- unique upper nonzeros and segments ---
+    int32_t *d_flags = nullptr, *d_upos = nullptr;
+    CK(cudaMallocAsync(&d_flags, sizeof(int32_t) * std::max<int64_t>(nv, 1), m->stream));
+    CK(cudaMallocAsync(&d_upos, sizeof(int32_t) * std::max<int64_t>(nv, 1), m->stream));
+    if (nv) head_flags_kernel<<<(unsigned)cdiv(nv, 256), 256, 0, m->stream>>>(nv, d_keys2, d_flags);
+    CK(cudaGetLastError());
+    CK(exclusive_sum(m, d_flags, d_upos, nv));
+    int32_t last_flag = 0, last_pos = 0;
+    if (nv) {
+        CK(cudaMemcpyAsync(&last_flag, d_flags + nv - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, m->stream));
+        CK(cudaMemcpyAsync(&last_pos, d_upos + nv - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, m->stream));
+    }
+    CK(cudaStreamSynchronize(m->stream));
+    m->n_upper = nv ? (int64_t)last_pos + last_flag : 0;
+    const int64_t nu = m->n_upper;
+    CK(dalloc(m, &m->d_seg, nu + 1));
+    uint64_t *d_ukeys = nullptr;
+    int32_t *d_upcnt = nullptr, *d_lowcnt = nullptr;
+    CK(cudaMallocAsync(&d_ukeys, sizeof(uint64_t) * std::max<int64_t>(nu, 1), m->stream));
+    CK(cudaMallocAsync(&d_upcnt, sizeof(int32_t) * ndof, m->stream));
+    CK(cudaMallocAsync(&d_lowcnt, sizeof(int32_t) * ndof, m->stream));
+    CK(cudaMemsetAsync(d_upcnt, 0, sizeof(int32_t) * ndof, m->stream));
+    CK(cudaMemsetAsync(d_lowcnt, 0, sizeof(int32_t) * ndof, m->stream));
+    if (nv) seg_kernel<<<(unsigned)cdiv(nv, 256), 256, 0, m->stream>>>(nv, d_flags, d_upos, d_keys2, ndof, m->d_seg, d_ukeys, d_upcnt, d_lowcnt);
+    CK(cudaGetLastError());
+    {
+        int32_t nv32 = (int32_t)nv;
+        CK(cudaMemcpyAsync(m->d_seg + nu, &nv32, sizeof(int32_t), cudaMemcpyHostToDevice, m->stream));
+        CK(cudaStreamSynchronize(m->stream));
+    }
+
+    // --- slot map: inverse permutation ---
+    int32_t *d_inv = nullptr;
+    CK(cudaMallocAsync(&d_inv, sizeof(int32_t) * std::max<int64_t>(n_total, 1), m->stream));
+    if (n_total) inv_kernel<<<(unsigned)cdiv(n_total, 256), 256, 0, m->stream>>>(n_total, d_vals2, d_inv);
+    CK(cudaGetLastError());
+    CK(dalloc(m, &m->d_slot, S));
+    if (S) regular_slot_kernel<<<(unsigned)cdiv(S, 256), 256, 0, m->stream>>>(S, d_inv, m->d_slot);
+    CK(cudaGetLastError());
+    if (n_exc_elem_slots) {
+        int64_t *d_si = nullptr;
+        int32_t *d_sc = nullptr;
+        CK(cudaMallocAsync(&d_si, sizeof(int64_t) * n_exc_elem_slots, m->stream));
+        CK(cudaMallocAsync(&d_sc, sizeof(int32_t) * n_exc_elem_slots, m->stream));
+        CK(cudaMemcpyAsync(d_si, exc_slot_idx.data(), sizeof(int64_t) * n_exc_elem_slots, cudaMemcpyHostToDevice, m->stream));
+        CK(cudaMemcpyAsync(d_sc, exc_slot_code.data(), sizeof(int32_t) * n_exc_elem_slots, cudaMemcpyHostToDevice, m->stream));
+        scatter_i32_kernel<<<(unsigned)cdiv(n_exc_elem_slots, 256), 256, 0, m->stream>>>(n_exc_elem_slots, d_si, d_sc, m->d_slot);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(m->stream));
+        cudaFreeAsync(d_si, m->stream);
+        cudaFreeAsync(d_sc, m->stream);
+    }
+    if (m->n_exc) {
+        std::vector<int32_t> hq(m->n_exc), hs(m->n_exc);
+        std::vector<double> hw(m->n_exc);
+        CK(cudaMemcpyAsync(hq.data(), d_inv + S, sizeof(int32_t) * m->n_exc, cudaMemcpyDeviceToHost, m->stream));
+        CK(cudaStreamSynchronize(m->stream));
+        for (int64_t k = 0; k < m->n_exc; ++k) { hs[k] = exc[k].src; hw[k] = exc[k].w; }
+        CK(dalloc(m, &m->d_exc_q, m->n_exc));
+        CK(dalloc(m, &m->d_exc_src, m->n_exc));
+        CK(dalloc(m, &m->d_exc_w, m->n_exc));
+        CK(cudaMemcpyAsync(m->d_exc_q, hq.data(), sizeof(int32_t) * m->n_exc, cudaMemcpyHostToDevice, m->stream));
+        CK(cudaMemcpyAsync(m->d_exc_src, hs.data(), sizeof(int32_t) * m->n_exc, cudaMemcpyHostToDevice, m->stream));
+        CK(cudaMemcpyAsync(m->d_exc_w, hw.data(), sizeof(double) * m->n_exc, cudaMemcpyHostToDevice, m->stream));
+        CK(cudaStreamSynchronize(m->stream));
+    }
+    CK(dalloc(m, &m->d_exc_raw, m->n_exc_raw));
+    CK(dalloc(m, &m->d_staging, nv + 1));
+
+    // --- symmetric CSR (== CSC) positions ---
+    int64_t *d_rowcnt = nullptr, *d_uprs = nullptr;
+    CK(dalloc(m, &m->d_rowptr, ndof + 1));
+    CK(cudaMallocAsync(&d_rowcnt, sizeof(int64_t) * (ndof + 1), m->stream));
+    CK(cudaMallocAsync(&d_uprs, sizeof(int64_t) * (ndof + 1), m->stream));
+    rowcnt_kernel<<<(unsigned)cdiv(ndof, 256), 256, 0, m->stream>>>(ndof, d_upcnt, d_lowcnt, d_rowcnt);
+    CK(cudaGetLastError());
+    CK(cudaMemsetAsync(d_rowcnt + ndof, 0, sizeof(int64_t), m->stream));
+    CK(exclusive_sum(m, d_rowcnt, m->d_rowptr, ndof + 1));
+    CK(exclusive_sum(m, d_upcnt, d_uprs, ndof));
+    CK(cudaMemcpyAsync(&m->nnz, m->d_rowptr + ndof, sizeof(int64_t), cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    CK(dalloc(m, &m->d_colind, m->nnz));
+    CK(dalloc(m, &m->d_posA, nu));
+    CK(dalloc(m, &m->d_posB, nu));
+    uint32_t *d_lk = nullptr, *d_lk2 = nullptr;
+    int32_t *d_lv = nullptr, *d_lv2 = nullptr, *d_lf = nullptr;
+    int64_t *d_lowstart = nullptr;
+    CK(cudaMallocAsync(&d_lk, sizeof(uint32_t) * std::max<int64_t>(nu, 1), m->stream));
+    CK(cudaMallocAsync(&d_lk2, sizeof(uint32_t) * std::max<int64_t>(nu, 1), m->stream));
+    CK(cudaMallocAsync(&d_lv, sizeof(int32_t) * std::max<int64_t>(nu, 1), m->stream));
+    CK(cudaMallocAsync(&d_lv2, sizeof(int32_t) * std::max<int64_t>(nu, 1), m->stream));
+    CK(cudaMallocAsync(&d_lf, sizeof(int32_t) * std::max<int64_t>(nu, 1), m->stream));
+    CK(cudaMallocAsync(&d_lowstart, sizeof(int64_t) * ndof, m->stream));
+    if (nu) {
+        posA_kernel<<<(unsigned)cdiv(nu, 256), 256, 0, m->stream>>>(nu, d_ukeys, ndof, m->d_rowptr, d_lowcnt, d_uprs,
+                                                                      m->d_posA, m->d_colind, d_lk, d_lv, d_lf);
+        CK(cudaGetLastError());
+        fill_i64_kernel<<<(unsigned)cdiv(nu, 256), 256, 0, m->stream>>>(nu, -1, m->d_posB);
+        CK(cudaGetLastError());
+        CK(radix_sort(m, d_lk, d_lk2, d_lv, d_lv2, nu, 32));
+        CK(exclusive_sum(m, d_lowcnt, d_lowstart, ndof));
+        // lower entries are the sorted prefix whose key is not the sentinel
+        const int64_t n_low = m->nnz - nu;  // every off-diagonal upper entry has one mirror
+        if (n_low)
+            posB_kernel<<<(unsigned)cdiv(n_low, 256), 256, 0, m->stream>>>(n_low, d_lk2, d_lv2, d_lowstart, m->d_rowptr,
+                                                                             d_ukeys, ndof, m->d_posB, m->d_colind);
+        CK(cudaGetLastError());
+    }
+
+    // --- orig_diag map (raw element diagonal, no constraint expansion) ---
+    m->dslot_q4 = 0;
+    m->dslot_t3 = m->nq * 24;
+    m->dslot_bar = m->dslot_t3 + m->nt * 18;
+    int64_t nd_total = m->dslot_bar + m->nb * 12;
+    CK(dalloc(m, &m->d_dslot, nd_total));
+    CK(dalloc(m, &m->d_dseg, ndof + 1));
+    {
+        uint32_t *d_dk = nullptr, *d_dk2 = nullptr;
+        int32_t *d_dv = nullptr, *d_dv2 = nullptr, *d_dcnt = nullptr;
+        CK(cudaMallocAsync(&d_dk, sizeof(uint32_t) * std::max<int64_t>(nd_total, 1), m->stream));
+        CK(cudaMallocAsync(&d_dk2, sizeof(uint32_t) * std::max<int64_t>(nd_total, 1), m->stream));
+        CK(cudaMallocAsync(&d_dv, sizeof(int32_t) * std::max<int64_t>(nd_total, 1), m->stream));
+        CK(cudaMallocAsync(&d_dv2, sizeof(int32_t) * std::max<int64_t>(nd_total, 1), m->stream));
+        CK(cudaMallocAsync(&d_dcnt, sizeof(int32_t) * (ndof + 1), m->stream));
+        std::vector<uint8_t> all_q4(m->nq, 1), all_t3(m->nt, 1);
+        auto dgen = [&](int64_t ne, int NN, const int32_t *dn, const std::vector<uint8_t> &act, int64_t base) -> cudaError_t {
+            if (!ne) return cudaSuccess;
+            cudaError_t e = cudaMemcpyAsync(d_reg, act.data(), ne, cudaMemcpyHostToDevice, m->stream);
+            if (e != cudaSuccess) return e;
+            gen_diag_keys_kernel<<<(unsigned)cdiv(ne * 6 * NN, 256), 256, 0, m->stream>>>(ne, NN, dn, d_reg, base, d_dk, d_dv);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+            return cudaStreamSynchronize(m->stream);
+        };
+        CK(dgen(m->nq, 4, m->d_q4n, all_q4, m->dslot_q4));
+        CK(dgen(m->nt, 3, m->d_t3n, all_t3, m->dslot_t3));
+        CK(dgen(m->nb, 2, m->d_barn, act_bar, m->dslot_bar));
+        if (nd_total) CK(radix_sort(m, d_dk, d_dk2, d_dv, d_dv2, nd_total, 32));
+        if (nd_total) inv_kernel<<<(unsigned)cdiv(nd_total, 256), 256, 0, m->stream>>>(nd_total, d_dv2, m->d_dslot);
+        CK(cudaGetLastError());
+        CK(cudaMemsetAsync(d_dcnt, 0, sizeof(int32_t) * (ndof + 1), m->stream));
+        if (nd_total) diag_seg_kernel<<<(unsigned)cdiv(nd_total, 256), 256, 0, m->stream>>>(nd_total, d_dk2, d_dcnt);
+        CK(cudaGetLastError());
+        CK(exclusive_sum(m, d_dcnt, m->d_dseg, ndof + 1));
+        m->n_dcontrib = nd_total;
+        CK(dalloc(m, &m->d_dstaging, nd_total));
+        CK(cudaStreamSynchronize(m->stream));
+        cudaFreeAsync(d_dk, m->stream); cudaFreeAsync(d_dk2, m->stream);
+        cudaFreeAsync(d_dv, m->stream); cudaFreeAsync(d_dv2, m->stream); cudaFreeAsync(d_dcnt, m->stream);
+    }
+
+    // --- release build temporaries ---
+    for (void *p : {(void *)d_reg, (void *)d_keys, (void *)d_keys2, (void *)d_vals, (void *)d_vals2, (void *)d_flags,
+                    (void *)d_upos, (void *)d_ukeys, (void *)d_upcnt, (void *)d_lowcnt, (void *)d_inv, (void *)d_rowcnt,
+                    (void *)d_uprs, (void *)d_lk, (void *)d_lk2, (void *)d_lv, (void *)d_lv2, (void *)d_lf,
+                    (void *)d_lowstart})
+        if (p) cudaFreeAsync(p, m->stream);
+    // --- persistent work buffers ---
+    CK(dalloc(m, &m->d_nz, m->nnz));
+    CK(dalloc(m, &m->d_u, ndof));
+    CK(dalloc(m, &m->d_diag, ndof));
+    CK(dalloc(m, &m->d_max, 1));
+    CK(cudaStreamSynchronize(m->stream));
+    CK(cudaGetLastError());
+    return JFG_OK;
+}
+
+jfg_status jfg_set_stream(jfg_model *m, void *stream) {
+    if (!m) return JFG_ERR_INVALID;
+    m->stream = stream ? (cudaStream_t)stream : m->own;
+    return JFG_OK;
+}
+
+jfg_status jfg_pattern(jfg_model *m, int64_t *ndof, int64_t *nnz) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "no pattern");
+    if (ndof) *ndof = m->ndof;
+    if (nnz) *nnz = m->nnz;
+    return JFG_OK;
+}
+
+jfg_status jfg_pattern_fill(jfg_model *m, int64_t *colptr, int64_t *rowval) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "no pattern");
+    if (colptr) {
+        CK(cudaMemcpyAsync(colptr, m->d_rowptr, sizeof(int64_t) * (m->ndof + 1), cudaMemcpyDeviceToHost, m->stream));
+    }
+    if (rowval) {
+        CK(cudaMemcpyAsync(rowval, m->d_colind, sizeof(int64_t) * m->nnz, cudaMemcpyDeviceToHost, m->stream));
+    }
+    CK(cudaStreamSynchronize(m->stream));
+    if (colptr)
+        for (int64_t i = 0; i <= m->ndof; ++i) colptr[i] += 1;
+    if (rowval)
+        for (int64_t i = 0; i < m->nnz; ++i) rowval[i] += 1;
+    return JFG_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+jfg_status launch_k(jfg_model *m, double *nz, double *dmax, double *ddiag) {
+    CK(cudaEventRecord(m->ev[0], m->stream));
+    ElemOut o;
+    o.staging = m->d_staging;
+    o.exc_raw = m->d_exc_raw;
+    o.diag_staging = ddiag ? m->d_dstaging : nullptr;
+    o.maxabs = dmax;
+    if (dmax) CK(cudaMemsetAsync(dmax, 0, sizeof(double), m->stream));
+    if (m->nq) {
+        o.slot = m->d_slot + m->slot_q4;
+        o.diag_slot = m->d_dslot + m->dslot_q4;
+        q4_k_kernel<<<(unsigned)cdiv(m->nq, Q4_ELEMS_PER_BLOCK), Q4_THREADS, 0, m->stream>>>(
+            m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, m->k6rot, o);
+        CK(cudaGetLastError());
+    }
+    if (m->nt) {
+        o.slot = m->d_slot + m->slot_t3;
+        o.diag_slot = m->d_dslot + m->dslot_t3;
+        t3_k_kernel<<<(unsigned)cdiv(m->nt, T3_WARPS), T3_THREADS, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords,
+                                                                                   m->d_nodeR, m->k6rot, o);
+        CK(cudaGetLastError());
+    }
+    if (m->nb) {
+        o.slot = m->d_slot + m->slot_bar;
+        o.diag_slot = m->d_dslot + m->dslot_bar;
+        bar_k_kernel<<<(unsigned)cdiv(m->nb, 128), 128, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, o);
+        CK(cudaGetLastError());
+    }
+    if (m->n_exc) {
+        expand_kernel<<<(unsigned)cdiv(m->n_exc, 256), 256, 0, m->stream>>>(m->n_exc, m->d_exc_q, m->d_exc_src, m->d_exc_w,
+                                                                           m->d_exc_raw, m->d_staging);
+        CK(cudaGetLastError());
+    }
+    CK(cudaEventRecord(m->ev[1], m->stream));
+    if (m->n_upper)
+        reduce_kernel<<<(unsigned)cdiv(m->n_upper, 256), 256, 0, m->stream>>>(m->n_upper, m->d_seg, m->d_staging, m->d_posA,
+                                                                             m->d_posB, nz);
+    CK(cudaGetLastError());
+    if (ddiag)
+        diag_reduce_kernel<<<(unsigned)cdiv(m->ndof, 256), 256, 0, m->stream>>>(m->ndof, m->d_dseg, m->d_dstaging, ddiag);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(m->ev[2], m->stream));
+    return JFG_OK;
+}
+
+jfg_status launch_kg(jfg_model *m, const double *du, double *nz) {
+    if (m->bar_offsets)
+        return fail(m, JFG_ERR_REFERENCE_RAISES,
+                    "assemble_geometric_stiffness raises BoundsError for CBAR/CBEAM with offsets (assembly.jl:6326)");
+    CK(cudaEventRecord(m->ev[0], m->stream));
+    ElemOut o;
+    o.staging = m->d_staging;
+    o.exc_raw = m->d_exc_raw;
+    o.diag_staging = nullptr;
+    o.diag_slot = nullptr;
+    o.maxabs = nullptr;
+    if (m->nq) {
+        o.slot = m->d_slot + m->slot_q4;
+        q4_kg_kernel<<<(unsigned)cdiv(m->nq, Q4_ELEMS_PER_BLOCK), Q4_THREADS, 0, m->stream>>>(
+            m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, du, o);
+        CK(cudaGetLastError());
+    }
+    if (m->nt) {
+        o.slot = m->d_slot + m->slot_t3;
+        t3_kg_kernel<<<(unsigned)cdiv(m->nt, 128), 128, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords, m->d_nodeR, du, o);
+        CK(cudaGetLastError());
+    }
+    if (m->nb) {
+        o.slot = m->d_slot + m->slot_bar;
+        bar_kg_kernel<<<(unsigned)cdiv(m->nb, 128), 128, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, du, o);
+        CK(cudaGetLastError());
+    }
+    if (m->n_exc) {
+        expand_kernel<<<(unsigned)cdiv(m->n_exc, 256), 256, 0, m->stream>>>(m->n_exc, m->d_exc_q, m->d_exc_src, m->d_exc_w,
+                                                                           m->d_exc_raw, m->d_staging);
+        CK(cudaGetLastError());
+    }
+    CK(cudaEventRecord(m->ev[1], m->stream));
+    if (m->n_upper)
+        reduce_kernel<<<(unsigned)cdiv(m->n_upper, 256), 256, 0, m->stream>>>(m->n_upper, m->d_seg, m->d_staging, m->d_posA,
+                                                                             m->d_posB, nz);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(m->ev[2], m->stream));
+    return JFG_OK;
+}
+
+jfg_status finish_timing(jfg_model *m) {
+    CK(cudaEventSynchronize(m->ev[2]));
+    CK(cudaEventElapsedTime(&m->last_elem_ms, m->ev[0], m->ev[1]));
+    CK(cudaEventElapsedTime(&m->last_reduce_ms, m->ev[1], m->ev[2]));
+    m->last_total_ms = m->last_elem_ms + m->last_reduce_ms;
+    return JFG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+jfg_status jfg_assemble_k_device(jfg_model *m, double *nzval_dev, double *max_dev, double *diag_dev) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    if (!nzval_dev) return fail(m, JFG_ERR_INVALID, "null nzval");
+    return launch_k(m, nzval_dev, max_dev, diag_dev);
+}
+
+jfg_status jfg_assemble_kg_device(jfg_model *m, const double *u_dev, double *nzval_dev) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    if (!u_dev || !nzval_dev) return fail(m, JFG_ERR_INVALID, "null pointer");
+    return launch_kg(m, u_dev, nzval_dev);
+}
+
+jfg_status jfg_assemble_k(jfg_model *m, double *nzval, double *max_elem_stiff, double *orig_diag) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    jfg_status st = launch_k(m, m->d_nz, m->d_max, orig_diag ? m->d_diag : nullptr);
+    if (st) return st;
+    if (nzval) CK(cudaMemcpyAsync(nzval, m->d_nz, sizeof(double) * m->nnz, cudaMemcpyDeviceToHost, m->stream));
+    if (max_elem_stiff) CK(cudaMemcpyAsync(max_elem_stiff, m->d_max, sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+    if (orig_diag) CK(cudaMemcpyAsync(orig_diag, m->d_diag, sizeof(double) * m->ndof, cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    return finish_timing(m);
+}
+
+jfg_status jfg_assemble_kg(jfg_model *m, const double *u_global, double *nzval) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    if (!u_global) return fail(m, JFG_ERR_INVALID, "null u_global");
+    if (m->bar_offsets)
+        return fail(m, JFG_ERR_REFERENCE_RAISES,
+                    "assemble_geometric_stiffness raises BoundsError for CBAR/CBEAM with offsets (assembly.jl:6326)");
+    CK(cudaMemcpyAsync(m->d_u, u_global, sizeof(double) * m->ndof, cudaMemcpyHostToDevice, m->stream));
+    jfg_status st = launch_kg(m, m->d_u, m->d_nz);
+    if (st) return st;
+    if (nzval) CK(cudaMemcpyAsync(nzval, m->d_nz, sizeof(double) * m->nnz, cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    return finish_timing(m);
+}
+
+jfg_status jfg_update_properties(jfg_model *m, const double *quad4_h, const double *tria3_h) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    int64_t n = std::max(m->nq, m->nt);
+    if (!m->d_h) CK(dalloc(m, &m->d_h, n));
+    if (quad4_h && m->nq) {
+        for (int64_t e = 0; e < m->nq; ++e)
+            if (!(quad4_h[e] > 0.0)) return fail(m, JFG_ERR_INVALID, "shell thickness must be positive");
+        CK(cudaMemcpyAsync(m->d_h, quad4_h, sizeof(double) * m->nq, cudaMemcpyHostToDevice, m->stream));
+        set_h_kernel<<<(unsigned)cdiv(m->nq, 256), 256, 0, m->stream>>>(m->nq, m->d_h, m->d_q4p);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(m->stream));
+    }
+    if (tria3_h && m->nt) {
+        for (int64_t e = 0; e < m->nt; ++e)
+            if (!(tria3_h[e] > 0.0)) return fail(m, JFG_ERR_INVALID, "shell thickness must be positive");
+        CK(cudaMemcpyAsync(m->d_h, tria3_h, sizeof(double) * m->nt, cudaMemcpyHostToDevice, m->stream));
+        set_h_kernel<<<(unsigned)cdiv(m->nt, 256), 256, 0, m->stream>>>(m->nt, m->d_h, m->d_t3p);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(m->stream));
+    }
+    return JFG_OK;
+}
+
+jfg_status jfg_constraint_map(jfg_model *m, int64_t *n_dep, int64_t *n_terms, int64_t *dep_dof, int64_t *term_ptr,
+                              int64_t *ind_dof, double *coeff) {
+    if (!m) return JFG_ERR_INVALID;
+    if (n_dep) *n_dep = (int64_t)m->dep_dof.size();
+    if (n_terms) *n_terms = (int64_t)m->dep_ind.size();
+    for (size_t i = 0; i < m->dep_dof.size(); ++i)
+        if (dep_dof) dep_dof[i] = m->dep_dof[i] + 1;
+    if (term_ptr)
+        for (size_t i = 0; i < m->dep_ptr.size(); ++i) term_ptr[i] = m->dep_ptr[i];
+    for (size_t i = 0; i < m->dep_ind.size(); ++i) {
+        if (ind_dof) ind_dof[i] = m->dep_ind[i] + 1;
+        if (coeff) coeff[i] = m->dep_coef[i];
+    }
+    return JFG_OK;
+}
+
+jfg_status jfg_last_timing(jfg_model *m, double *element_ms, double *reduce_ms, double *total_ms) {
+    if (!m) return JFG_ERR_INVALID;
+    jfg_status st = finish_timing(m);
+    if (st) return st;
+    if (element_ms) *element_ms = m->last_elem_ms;
+    if (reduce_ms) *reduce_ms = m->last_reduce_ms;
+    if (total_ms) *total_ms = m->last_total_ms;
+    return JFG_OK;
+}
+
+}  // extern "C"

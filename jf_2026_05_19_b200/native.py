@@ -1,0 +1,182 @@
+"""ctypes binding of ``libjfemgpu.so`` and a handle class over it.
+
+The product path is the CUDA library only: if the shared object is missing
+or no CUDA device is visible, the calls raise -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from . import abi
+from .abi import JfgModelDesc, make_desc
+from .decks import ModelArrays
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libjfemgpu.so")
+
+# every entry point declared in include/jfem_gpu.h
+EXPORTS = ("jfg_model_create", "jfg_pattern", "jfg_pattern_fill", "jfg_assemble_k", "jfg_assemble_kg",
+           "jfg_assemble_k_device", "jfg_assemble_kg_device", "jfg_update_properties", "jfg_constraint_map",
+           "jfg_set_stream", "jfg_last_timing", "jfg_model_destroy", "jfg_last_error", "jfg_version")
+
+_lib = None
+
+_pd = C.POINTER(C.c_double)
+_pi64 = C.POINTER(C.c_int64)
+
+
+class JfgError(RuntimeError):
+    """Nonzero jfg_status, with the handle's message (the reference's error(...))."""
+
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"jfg status {status} ({abi.STATUS_NAMES.get(status, '?')}): {msg}")
+        self.status = status
+        self.msg = msg
+
+
+def load(path: str = LIB_PATH):
+    """Load the library (building it first when the sources are newer)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        try:
+            from .build import build
+            build()
+        except Exception as exc:  # pragma: no cover - reported loudly below
+            raise RuntimeError(f"CUDA library {path} missing and could not be built: {exc}") from exc
+    L = C.CDLL(path)
+    L.jfg_model_create.argtypes = [C.POINTER(JfgModelDesc), C.POINTER(C.c_void_p)]
+    L.jfg_model_create.restype = C.c_int32
+    L.jfg_pattern.argtypes = [C.c_void_p, _pi64, _pi64]
+    L.jfg_pattern_fill.argtypes = [C.c_void_p, _pi64, _pi64]
+    L.jfg_assemble_k.argtypes = [C.c_void_p, _pd, _pd, _pd]
+    L.jfg_assemble_kg.argtypes = [C.c_void_p, _pd, _pd]
+    L.jfg_assemble_k_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.jfg_assemble_kg_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.jfg_update_properties.argtypes = [C.c_void_p, _pd, _pd]
+    L.jfg_constraint_map.argtypes = [C.c_void_p, _pi64, _pi64, _pi64, _pi64, _pi64, _pd]
+    L.jfg_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+    L.jfg_last_timing.argtypes = [C.c_void_p, _pd, _pd, _pd]
+    L.jfg_model_destroy.argtypes = [C.c_void_p]
+    L.jfg_model_destroy.restype = None
+    L.jfg_last_error.argtypes = [C.c_void_p]
+    L.jfg_last_error.restype = C.c_char_p
+    L.jfg_version.restype = C.c_char_p
+    for name in ("jfg_pattern", "jfg_pattern_fill", "jfg_assemble_k", "jfg_assemble_kg", "jfg_assemble_k_device",
+                 "jfg_assemble_kg_device", "jfg_update_properties", "jfg_constraint_map", "jfg_set_stream",
+                 "jfg_last_timing"):
+        getattr(L, name).restype = C.c_int32
+    _lib = L
+    return L
+
+
+def _ptr(a: Optional[np.ndarray], ctype):
+    return C.cast(None, ctype) if a is None else a.ctypes.data_as(ctype)
+
+
+class GpuModel:
+    """One jfg_model handle: mesh, pattern and scatter map resident on the GPU."""
+
+    def __init__(self, m: ModelArrays):
+        self.L = load()
+        self.model = m
+        self.h = C.c_void_p()
+        d, keep = make_desc(m)
+        st = self.L.jfg_model_create(C.byref(d), C.byref(self.h))
+        if st != 0:
+            msg = self.L.jfg_last_error(self.h).decode()
+            self.L.jfg_model_destroy(self.h)
+            self.h = C.c_void_p()
+            raise JfgError(st, msg)
+        del keep
+        nd = C.c_int64(); nnz = C.c_int64()
+        self._check(self.L.jfg_pattern(self.h, C.byref(nd), C.byref(nnz)))
+        self.ndof = int(nd.value)
+        self.nnz = int(nnz.value)
+        self._pattern = None
+
+    def _check(self, st: int):
+        if st != 0:
+            raise JfgError(st, self.L.jfg_last_error(self.h).decode())
+
+    def close(self):
+        if self.h:
+            self.L.jfg_model_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- pattern -----------------------------------------------------------
+    def pattern(self):
+        """(colptr, rowval), 1-based int64, SparseMatrixCSC layout."""
+        if self._pattern is None:
+            colptr = np.empty(self.ndof + 1, np.int64)
+            rowval = np.empty(self.nnz, np.int64)
+            self._check(self.L.jfg_pattern_fill(self.h, _ptr(colptr, _pi64), _ptr(rowval, _pi64)))
+            self._pattern = (colptr, rowval)
+        return self._pattern
+
+    # -- host-buffer assembly (the reference-facing calls) -----------------
+    def assemble_k(self, nzval: Optional[np.ndarray] = None, want_diag: bool = True):
+        nz = np.empty(self.nnz) if nzval is None else nzval
+        mx = np.zeros(1)
+        diag = np.empty(self.ndof) if want_diag else None
+        self._check(self.L.jfg_assemble_k(self.h, _ptr(nz, _pd), _ptr(mx, _pd), _ptr(diag, _pd)))
+        return nz, float(mx[0]), diag
+
+    def assemble_kg(self, u: np.ndarray, nzval: Optional[np.ndarray] = None):
+        u = np.ascontiguousarray(u, np.float64)
+        if u.shape != (self.ndof,):
+            raise ValueError(f"u_global must have {self.ndof} entries")
+        nz = np.empty(self.nnz) if nzval is None else nzval
+        self._check(self.L.jfg_assemble_kg(self.h, _ptr(u, _pd), _ptr(nz, _pd)))
+        return nz
+
+    # -- device-resident assembly (torch CUDA tensors or raw pointers) ------
+    def assemble_k_device(self, nz_ptr: int, max_ptr: int = 0, diag_ptr: int = 0):
+        self._check(self.L.jfg_assemble_k_device(self.h, C.c_void_p(nz_ptr), C.c_void_p(max_ptr or None),
+                                                 C.c_void_p(diag_ptr or None)))
+
+    def assemble_kg_device(self, u_ptr: int, nz_ptr: int):
+        self._check(self.L.jfg_assemble_kg_device(self.h, C.c_void_p(u_ptr), C.c_void_p(nz_ptr)))
+
+    def set_stream(self, stream_ptr: int):
+        self._check(self.L.jfg_set_stream(self.h, C.c_void_p(stream_ptr or None)))
+
+    def update_thickness(self, q4_h: Optional[np.ndarray], t3_h: Optional[np.ndarray]):
+        q = None if q4_h is None else np.ascontiguousarray(q4_h, np.float64)
+        t = None if t3_h is None else np.ascontiguousarray(t3_h, np.float64)
+        self._check(self.L.jfg_update_properties(self.h, _ptr(q, _pd), _ptr(t, _pd)))
+
+    def timing(self):
+        a = C.c_double(); b = C.c_double(); c = C.c_double()
+        self._check(self.L.jfg_last_timing(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def constraint_map(self):
+        nd = C.c_int64(); nt = C.c_int64()
+        self._check(self.L.jfg_constraint_map(self.h, C.byref(nd), C.byref(nt), None, None, None, None))
+        dep = np.empty(nd.value, np.int64); ptr = np.empty(nd.value + 1, np.int64)
+        ind = np.empty(nt.value, np.int64); coef = np.empty(nt.value)
+        self._check(self.L.jfg_constraint_map(self.h, None, None, _ptr(dep, _pi64), _ptr(ptr, _pi64),
+                                              _ptr(ind, _pi64), _ptr(coef, _pd)))
+        return dep, ptr, ind, coef
+
+
+def version() -> str:
+    return load().jfg_version().decode()

@@ -1,0 +1,1296 @@
+// jfem_oracle.cpp -- CPU restatement of the OpenJFEM element hot path.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is the parity oracle and the timed CPU
+// baseline; nothing in the product library links or calls it.  It restates,
+// in plain C++ with OpenMP over elements, the default branch of
+//   assemble_stiffness            src/solver/assembly.jl:1953-4375
+//   assemble_geometric_stiffness  src/solver/assembly.jl:4382-6634
+// and the element kernels they call in src/FEMKernels.jl, restricted to the
+// predicates the library accepts (flat isotropic PSHELL/MAT1 CQUAD4/CTRIA3,
+// CBAR/CBEAM without pin flags, RBE2, PARAM SNORM <= 0, no JFEM_* overrides).
+//
+// PARITY UNPINNED: the reference is Julia 1.12 and cannot run in this build
+// environment (no julia, no network), and it ships no golden vectors or
+// known-answer tests for this path.  The restatement follows the cited lines;
+// agreement with it is checked by tests, and physics known-answers (symmetry,
+// rigid-body null space, plate buckling coefficient) add sanity checks that
+// are not reference-pinned.
+//
+// Third-party arithmetic restated here (not vendored in the reference):
+//   StaticArrays 1.9.17 inv(SMatrix{4,4})     -> Gauss-Jordan with pivoting
+//   LinearAlgebra (OpenBLAS 0.3.29) small '\' -> LU with partial pivoting
+//   SparseArrays 1.12.0 sparse(I,J,V,m,n)     -> CSC, duplicates summed,
+//                                                 explicit zeros kept
+// They differ from the reference only by rounding.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../include/jfem_gpu.h"
+
+namespace {
+
+typedef double V3[3];
+
+inline void sub3(const double *a, const double *b, double *o) { o[0] = a[0] - b[0]; o[1] = a[1] - b[1]; o[2] = a[2] - b[2]; }
+inline double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+inline void cross3(const double *a, const double *b, double *o) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+inline double norm3(const double *a) { return std::sqrt(dot3(a, a)); }
+inline void normalize3(const double *a, double *o) { double n = norm3(a); o[0] = a[0] / n; o[1] = a[1] / n; o[2] = a[2] / n; }
+
+// Dense LU with partial pivoting: solve A X = B in place (A n x n, B n x m),
+// row-major.  Returns false on an exactly singular pivot.
+bool lu_solve(int n, int m, double *A, double *B) {
+    std::vector<int> piv(n);
+    for (int k = 0; k < n; ++k) {
+        int p = k;
+        double best = std::fabs(A[k * n + k]);
+        for (int i = k + 1; i < n; ++i) {
+            double v = std::fabs(A[i * n + k]);
+            if (v > best) { best = v; p = i; }
+        }
+        if (best == 0.0) return false;
+        if (p != k) {
+            for (int j = 0; j < n; ++j) std::swap(A[k * n + j], A[p * n + j]);
+            for (int j = 0; j < m; ++j) std::swap(B[k * m + j], B[p * m + j]);
+        }
+        for (int i = k + 1; i < n; ++i) {
+            double f = A[i * n + k] / A[k * n + k];
+            A[i * n + k] = f;
+            for (int j = k + 1; j < n; ++j) A[i * n + j] -= f * A[k * n + j];
+            for (int j = 0; j < m; ++j) B[i * m + j] -= f * B[k * m + j];
+        }
+    }
+    for (int k = n - 1; k >= 0; --k) {
+        for (int j = 0; j < m; ++j) {
+            double s = B[k * m + j];
+            for (int i = k + 1; i < n; ++i) s -= A[k * n + i] * B[i * m + j];
+            B[k * m + j] = s / A[k * n + k];
+        }
+    }
+    return true;
+}
+
+// inv(SMatrix{4,4}) restated as Gauss-Jordan (identity right-hand side).
+void inv4(const double A[4][4], double Ai[4][4]) {
+    double a[16], b[16];
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) { a[i * 4 + j] = A[i][j]; b[i * 4 + j] = (i == j) ? 1.0 : 0.0; }
+    lu_solve(4, 4, a, b);
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) Ai[i][j] = b[i * 4 + j];
+}
+
+// shape_derivs_quad (FEMKernels.jl:237-241)
+inline void shape_derivs_quad(double xi, double eta, double dNr[4], double dNs[4]) {
+    dNr[0] = -0.25 * (1 - eta); dNr[1] = 0.25 * (1 - eta); dNr[2] = 0.25 * (1 + eta); dNr[3] = -0.25 * (1 + eta);
+    dNs[0] = -0.25 * (1 - xi); dNs[1] = -0.25 * (1 + xi); dNs[2] = 0.25 * (1 + xi); dNs[3] = 0.25 * (1 - xi);
+}
+
+struct Jac {
+    double J11, J12, J21, J22, det, iJ11, iJ12, iJ21, iJ22;
+};
+inline Jac jacobian(const double lc[4][2], const double dNr[4], const double dNs[4]) {
+    Jac j;
+    j.J11 = dNr[0] * lc[0][0] + dNr[1] * lc[1][0] + dNr[2] * lc[2][0] + dNr[3] * lc[3][0];
+    j.J12 = dNr[0] * lc[0][1] + dNr[1] * lc[1][1] + dNr[2] * lc[2][1] + dNr[3] * lc[3][1];
+    j.J21 = dNs[0] * lc[0][0] + dNs[1] * lc[1][0] + dNs[2] * lc[2][0] + dNs[3] * lc[3][0];
+    j.J22 = dNs[0] * lc[0][1] + dNs[1] * lc[1][1] + dNs[2] * lc[2][1] + dNs[3] * lc[3][1];
+    j.det = j.J11 * j.J22 - j.J12 * j.J21;
+    double inv = 1.0 / j.det;
+    j.iJ11 = j.J22 * inv; j.iJ12 = -j.J12 * inv; j.iJ21 = -j.J21 * inv; j.iJ22 = j.J11 * inv;
+    return j;
+}
+
+// C += alpha * A' * B  with A (k x m), B (k x n), C (m x n), all row-major.
+void mul_At_add(double *C, const double *A, const double *B, int k, int m, int n, double alpha) {
+    for (int j = 0; j < n; ++j)
+        for (int l = 0; l < k; ++l) {
+            double v = alpha * B[l * n + j];
+            for (int i = 0; i < m; ++i) C[i * n + j] += A[l * m + i] * v;
+        }
+}
+// C = A * B  (A m x k, B k x n)
+void mul(double *C, const double *A, const double *B, int m, int k, int n) {
+    for (int i = 0; i < m * n; ++i) C[i] = 0.0;
+    for (int j = 0; j < n; ++j)
+        for (int l = 0; l < k; ++l) {
+            double v = B[l * n + j];
+            for (int i = 0; i < m; ++i) C[i * n + j] += A[i * k + l] * v;
+        }
+}
+
+// add_quad4_macneal_shear_rbf! default branch (FEMKernels.jl:4715-4978):
+// epsilon 0.04, "diag" flexibility, paper length mode, zb_scale 0.65,
+// zb_u = zb_d, no per-GP delta, rigid_shear = false.
+void macneal_shear(double Ke[24][24], const double lc[4][2], const double Cb[3][3], const double Cs[2][2], double h) {
+    double csmax = std::max(std::max(std::fabs(Cs[0][0]), std::fabs(Cs[0][1])), std::max(std::fabs(Cs[1][0]), std::fabs(Cs[1][1])));
+    if (h < 1e-30 || csmax < 1e-30) return;
+    const double pt = 1.0 / std::sqrt(3.0);
+    const double sp[4][3] = {{0.0, -pt, 1}, {0.0, pt, 1}, {-pt, 0.0, 2}, {pt, 0.0, 2}};
+    double D[4][12] = {};
+    double Jp[4];
+    for (int s = 0; s < 4; ++s) {
+        double xi = sp[s][0], eta = sp[s][1];
+        int comp = (int)sp[s][2];
+        double dNr[4], dNs[4];
+        shape_derivs_quad(xi, eta, dNr, dNs);
+        double J11 = dNr[0] * lc[0][0] + dNr[1] * lc[1][0] + dNr[2] * lc[2][0] + dNr[3] * lc[3][0];
+        double J12 = dNr[0] * lc[0][1] + dNr[1] * lc[1][1] + dNr[2] * lc[2][1] + dNr[3] * lc[3][1];
+        double J21 = dNs[0] * lc[0][0] + dNs[1] * lc[1][0] + dNs[2] * lc[2][0] + dNs[3] * lc[3][0];
+        double J22 = dNs[0] * lc[0][1] + dNs[1] * lc[1][1] + dNs[2] * lc[2][1] + dNs[3] * lc[3][1];
+        double det = J11 * J22 - J12 * J21;
+        if (std::fabs(det) < 1e-14) det = det < 0.0 ? -1e-14 : 1e-14;
+        Jp[s] = std::fabs(det);
+        double inv = 1.0 / det;
+        double iJ11 = J22 * inv, iJ12 = -J12 * inv, iJ21 = -J21 * inv, iJ22 = J11 * inv;
+        double N[4] = {0.25 * (1 - xi) * (1 - eta), 0.25 * (1 + xi) * (1 - eta), 0.25 * (1 + xi) * (1 + eta), 0.25 * (1 - xi) * (1 + eta)};
+        for (int k = 0; k < 4; ++k) {
+            double dx = iJ11 * dNr[k] + iJ12 * dNs[k];
+            double dy = iJ21 * dNr[k] + iJ22 * dNs[k];
+            int col = 3 * k;
+            if (comp == 1) { D[s][col + 0] = dx; D[s][col + 2] = N[k]; }
+            else { D[s][col + 0] = dy; D[s][col + 1] = -N[k]; }
+        }
+    }
+    double Dx = 0.5 * (lc[1][0] + lc[2][0] - lc[0][0] - lc[3][0]);
+    double Dy = 0.5 * (lc[2][1] + lc[3][1] - lc[0][1] - lc[1][1]);
+    double Dx2 = Dx * Dx, Dy2 = Dy * Dy;
+    const double dNr_c[4] = {-0.25, 0.25, 0.25, -0.25}, dNs_c[4] = {-0.25, -0.25, 0.25, 0.25};
+    double J11c = dNr_c[0] * lc[0][0] + dNr_c[1] * lc[1][0] + dNr_c[2] * lc[2][0] + dNr_c[3] * lc[3][0];
+    double J12c = dNr_c[0] * lc[0][1] + dNr_c[1] * lc[1][1] + dNr_c[2] * lc[2][1] + dNr_c[3] * lc[3][1];
+    double J21c = dNs_c[0] * lc[0][0] + dNs_c[1] * lc[1][0] + dNs_c[2] * lc[2][0] + dNs_c[3] * lc[3][0];
+    double J22c = dNs_c[0] * lc[0][1] + dNs_c[1] * lc[1][1] + dNs_c[2] * lc[2][1] + dNs_c[3] * lc[3][1];
+    double A_elem = 4.0 * std::fabs(J11c * J22c - J12c * J21c);
+    double eps = std::min(std::max(0.04, 1e-12), 1.0);
+    double a_param = eps / (eps + (1.0 - eps) * Dx2 / std::max(Dy2, 1e-30));
+    double b_param = eps / (eps + (1.0 - eps) * Dy2 / std::max(Dx2, 1e-30));
+    double flex_x = 1.0 / std::max(std::fabs(Cb[0][0]), 1e-30);
+    double flex_y = 1.0 / std::max(std::fabs(Cb[1][1]), 1e-30);
+    double inv12A = 1.0 / (12.0 * A_elem);
+    const double zb = 0.65;
+    double zbx_u = zb * inv12A * Dx2 * flex_x;
+    double zbx_d = zb * inv12A * a_param * Dx2 * flex_x;
+    double zby_u = zb * inv12A * Dy2 * flex_y;
+    double zby_d = zb * inv12A * b_param * Dy2 * flex_y;
+    double Zb[4][4] = {};
+    Zb[0][0] = zbx_u + zbx_d; Zb[0][1] = zbx_u - zbx_d; Zb[1][0] = Zb[0][1]; Zb[1][1] = Zb[0][0];
+    Zb[2][2] = zby_u + zby_d; Zb[2][3] = zby_u - zby_d; Zb[3][2] = Zb[2][3]; Zb[3][3] = Zb[2][2];
+    // physical shear compliance (eq 23-25)
+    const int comps[4] = {1, 1, 2, 2};
+    double VGV[4][4];
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) {
+            double Jfac = std::sqrt(2.0 * Jp[i]) * std::sqrt(2.0 * Jp[j]);
+            if (comps[i] == comps[j]) VGV[i][j] = (i == j) ? Jfac * (comps[i] == 1 ? Cs[0][0] : Cs[1][1]) : 0.0;
+            else VGV[i][j] = 0.5 * Jfac * Cs[0][1];
+        }
+    for (int i = 0; i < 4; ++i)
+        if (VGV[i][i] < 1e-30) VGV[i][i] = 1e-30;
+    double VS[4][4], Zs[4][4], Zi[4][4];
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) VS[i][j] = 0.5 * (VGV[i][j] + VGV[j][i]);
+    inv4(VS, Zi);
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) Zs[i][j] = 0.5 * (Zi[i][j] + Zi[j][i]);
+    double Zt[4][4], Z[16];
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) Zt[i][j] = Zs[i][j] + Zb[i][j];
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) Z[i * 4 + j] = 0.5 * (Zt[i][j] + Zt[j][i]);
+    double X[4 * 12];
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 12; ++j) X[i * 12 + j] = D[i][j];
+    lu_solve(4, 12, Z, X);
+    double Kp[12][12];
+    for (int i = 0; i < 12; ++i)
+        for (int j = 0; j < 12; ++j) {
+            double s = 0.0;
+            for (int l = 0; l < 4; ++l) s += D[l][i] * X[l * 12 + j];
+            Kp[i][j] = s;
+        }
+    const int pd[12] = {2, 3, 4, 8, 9, 10, 14, 15, 16, 20, 21, 22};
+    for (int j = 0; j < 12; ++j)
+        for (int i = 0; i < 12; ++i) Ke[pd[i]][pd[j]] += 0.5 * (Kp[i][j] + Kp[j][i]);
+}
+
+// stiffness_quad4_matrices, default branch (FEMKernels.jl:3185-4034) for a
+// planar element: JFEM_Q4_KERNEL=macneal with the twist correction
+// (:3466-3492), MITC4 shear skipped (:3762), Hughes-Brezzi drill
+// (:3556-3559), Wilson incompatible modes and 4x4 condensations
+// (:3790-3801, :3964-4011).  No Bmb, no curvature terms.
+void q4_stiffness(const double lc[4][2], const double Cm[3][3], const double Cb[3][3], const double Cs[2][2],
+                  double h, double E_ref, double k6rot, double drill_scale, bool bending_incomp,
+                  bool membrane_incomp, double Ke[24][24]) {
+    std::memset(Ke, 0, sizeof(double) * 576);
+    double K_ab[24][4] = {}, K_bb[4][4] = {}, K_abb[24][4] = {}, K_bbb[4][4] = {};
+    const double dNr_c[4] = {-0.25, 0.25, 0.25, -0.25}, dNs_c[4] = {-0.25, -0.25, 0.25, 0.25};
+    Jac jc = jacobian(lc, dNr_c, dNs_c);
+    double dNdx_c[4], dNdy_c[4];
+    for (int k = 0; k < 4; ++k) {
+        dNdx_c[k] = jc.iJ11 * dNr_c[k] + jc.iJ12 * dNs_c[k];
+        dNdy_c[k] = jc.iJ21 * dNr_c[k] + jc.iJ22 * dNs_c[k];
+    }
+    const double pt = 1.0 / std::sqrt(3.0);
+    const double gp[4][2] = {{-pt, -pt}, {pt, -pt}, {pt, pt}, {-pt, pt}};
+    double G_drill = Cm[2][2] / h;
+    if (G_drill < 1e-6) G_drill = E_ref / (2 * 3.0);
+    double alpha_drill = drill_scale * (k6rot / 1e5) * G_drill * h;
+
+    for (int g = 0; g < 4; ++g) {
+        double r = gp[g][0], s = gp[g][1];
+        double dNr[4], dNs[4];
+        shape_derivs_quad(r, s, dNr, dNs);
+        Jac j = jacobian(lc, dNr, dNs);
+        double absdet = std::fabs(j.det);
+        if (absdet < 1e-12) absdet = 1e-12;
+        double Bm[3][24] = {}, Bb[3][24] = {}, Bd[1][24] = {};
+        for (int k = 0; k < 4; ++k) {
+            double dx = j.iJ11 * dNr[k] + j.iJ12 * dNs[k];
+            double dy = j.iJ21 * dNr[k] + j.iJ22 * dNs[k];
+            int idx = 6 * k;
+            double Nk = 0.25 * (1 + ((k == 1 || k == 2) ? r : -r)) * (1 + (k >= 2 ? s : -s));
+            Bm[0][idx + 0] = dx; Bm[1][idx + 1] = dy;
+            Bm[2][idx + 0] = dy; Bm[2][idx + 1] = dx;
+            Bb[0][idx + 4] = dx; Bb[1][idx + 3] = -dy;
+            // MacNeal twist compatibility: 2 chi_xy(gp) - chi_xy(0)
+            Bb[2][idx + 4] = 2.0 * dy - dNdy_c[k];
+            Bb[2][idx + 3] = 2.0 * (-dx) - (-dNdx_c[k]);
+            Bd[0][idx + 0] = 0.5 * dy; Bd[0][idx + 1] = -0.5 * dx; Bd[0][idx + 5] = Nk;
+        }
+        double dphi1_dx = j.iJ11 * (-2.0 * r), dphi1_dy = j.iJ21 * (-2.0 * r);
+        double dphi2_dx = j.iJ12 * (-2.0 * s), dphi2_dy = j.iJ22 * (-2.0 * s);
+        double Bi[3][4] = {}, Bib[3][4] = {};
+        Bi[0][0] = dphi1_dx; Bi[2][0] = dphi1_dy; Bi[1][1] = dphi1_dy; Bi[2][1] = dphi1_dx;
+        Bi[0][2] = dphi2_dx; Bi[2][2] = dphi2_dy; Bi[1][3] = dphi2_dy; Bi[2][3] = dphi2_dx;
+        Bib[1][0] = -dphi1_dy; Bib[1][1] = -dphi2_dy;
+        Bib[0][2] = dphi1_dx; Bib[0][3] = dphi2_dx;
+        Bib[2][0] = -dphi1_dx; Bib[2][1] = -dphi2_dx;
+        Bib[2][2] = dphi1_dy; Bib[2][3] = dphi2_dy;
+        double t3x24[3 * 24], t3x4[3 * 4];
+        mul(t3x24, &Cm[0][0], &Bm[0][0], 3, 3, 24);
+        mul_At_add(&Ke[0][0], &Bm[0][0], t3x24, 3, 24, 24, absdet);
+        mul(t3x24, &Cb[0][0], &Bb[0][0], 3, 3, 24);
+        mul_At_add(&Ke[0][0], &Bb[0][0], t3x24, 3, 24, 24, absdet);
+        mul_At_add(&Ke[0][0], &Bd[0][0], &Bd[0][0], 1, 24, 24, absdet * alpha_drill);
+        if (membrane_incomp) {
+            mul(t3x4, &Cm[0][0], &Bi[0][0], 3, 3, 4);
+            mul_At_add(&K_ab[0][0], &Bm[0][0], t3x4, 3, 24, 4, absdet);
+            mul_At_add(&K_bb[0][0], &Bi[0][0], t3x4, 3, 4, 4, absdet);
+        }
+        mul(t3x4, &Cb[0][0], &Bib[0][0], 3, 3, 4);
+        mul_At_add(&K_abb[0][0], &Bb[0][0], t3x4, 3, 24, 4, absdet);
+        mul_At_add(&K_bbb[0][0], &Bib[0][0], t3x4, 3, 4, 4, absdet);
+    }
+    macneal_shear(Ke, lc, Cb, Cs, h);
+
+    double kbbmax = 0.0;
+    for (int i = 0; i < 4; ++i)
+        for (int jj = 0; jj < 4; ++jj) kbbmax = std::max(kbbmax, std::fabs(K_bbb[i][jj]));
+    auto condense = [&](double Kab[24][4], double Kbb[4][4]) {
+        double Ii[4][4];
+        inv4(Kbb, Ii);
+        for (int jj = 0; jj < 24; ++jj)
+            for (int i = 0; i < 24; ++i) {
+                double sm = 0.0;
+                for (int l = 0; l < 4; ++l) {
+                    double t = 0.0;
+                    for (int q = 0; q < 4; ++q) t += Ii[l][q] * Kab[jj][q];
+                    sm += Kab[i][l] * t;
+                }
+                Ke[i][jj] -= sm;
+            }
+    };
+    if (bending_incomp && kbbmax > 0.0) {
+        condense(K_abb, K_bbb);
+        if (membrane_incomp) condense(K_ab, K_bb);
+    } else if (membrane_incomp) {
+        condense(K_ab, K_bb);
+    }
+}
+
+// stiffness_tria3_matrices_generic (FEMKernels.jl:7315-7385) with
+// tria3_plate_macro_data (:7157-7209): CST membrane, plate block from three
+// default-kwarg virtual quads condensed to the corners, Hughes-Brezzi drill.
+void t3_stiffness(const double lc[3][2], const double Dm[3][3], const double Db[3][3], const double Ds[2][2],
+                  double h, double G_ref, double br, double k6rot, double Ke[18][18]) {
+    std::memset(Ke, 0, sizeof(double) * 324);
+    double x[3] = {lc[0][0], lc[1][0], lc[2][0]}, y[3] = {lc[0][1], lc[1][1], lc[2][1]};
+    double A2 = x[0] * (y[1] - y[2]) + x[1] * (y[2] - y[0]) + x[2] * (y[0] - y[1]);
+    double A = 0.5 * std::fabs(A2);
+    if (A < 1e-12) return;
+    double bv[3] = {(y[1] - y[2]) / (2 * A), (y[2] - y[0]) / (2 * A), (y[0] - y[1]) / (2 * A)};
+    double cv[3] = {(x[2] - x[1]) / (2 * A), (x[0] - x[2]) / (2 * A), (x[1] - x[0]) / (2 * A)};
+    double Bm[3][6] = {};
+    for (int i = 0; i < 3; ++i) {
+        Bm[0][2 * i] = bv[i]; Bm[1][2 * i + 1] = cv[i]; Bm[2][2 * i] = cv[i]; Bm[2][2 * i + 1] = bv[i];
+    }
+    double DB[3 * 6], Km[6 * 6] = {};
+    mul(DB, &Dm[0][0], &Bm[0][0], 3, 3, 6);
+    mul_At_add(Km, &Bm[0][0], DB, 3, 6, 6, A);
+    const int m_idx[6] = {0, 1, 6, 7, 12, 13};
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) Ke[m_idx[i]][m_idx[j]] = Km[i * 6 + j];
+    // plate macro data
+    if (br > 1e-12) {
+        double pts[7][2];
+        for (int i = 0; i < 3; ++i) { pts[i][0] = x[i]; pts[i][1] = y[i]; }
+        pts[3][0] = (x[0] + x[1]) / 2; pts[3][1] = (y[0] + y[1]) / 2;
+        pts[4][0] = (x[1] + x[2]) / 2; pts[4][1] = (y[1] + y[2]) / 2;
+        pts[5][0] = (x[2] + x[0]) / 2; pts[5][1] = (y[2] + y[0]) / 2;
+        pts[6][0] = (x[0] + x[1] + x[2]) / 3; pts[6][1] = (y[0] + y[1] + y[2]) / 3;
+        const int quads[3][4] = {{0, 3, 6, 5}, {1, 4, 6, 3}, {2, 5, 6, 4}};
+        const int pd[12] = {2, 3, 4, 8, 9, 10, 14, 15, 16, 20, 21, 22};
+        static thread_local double K21[21][21];
+        std::memset(K21, 0, sizeof(K21));
+        for (int q = 0; q < 3; ++q) {
+            double qc[4][2];
+            for (int k = 0; k < 4; ++k) { qc[k][0] = pts[quads[q][k]][0]; qc[k][1] = pts[quads[q][k]][1]; }
+            double Kq[24][24];
+            q4_stiffness(qc, Dm, Db, Ds, h, G_ref, k6rot, 1.0, /*bending_incomp=*/false, /*membrane_incomp=*/true, Kq);
+            int ed[12];
+            for (int k = 0; k < 4; ++k)
+                for (int d = 0; d < 3; ++d) ed[3 * k + d] = 3 * quads[q][k] + d;
+            for (int i = 0; i < 12; ++i)
+                for (int j = 0; j < 12; ++j) K21[ed[i]][ed[j]] += Kq[pd[i]][pd[j]];
+        }
+        double Kii[12 * 12], Aint[12 * 9];
+        for (int i = 0; i < 12; ++i) {
+            for (int j = 0; j < 12; ++j) Kii[i * 12 + j] = K21[9 + i][9 + j];
+            for (int j = 0; j < 9; ++j) Aint[i * 9 + j] = K21[9 + i][j];
+        }
+        lu_solve(12, 9, Kii, Aint);
+        for (int i = 0; i < 12 * 9; ++i) Aint[i] = -Aint[i];
+        const int b_idx[9] = {2, 3, 4, 8, 9, 10, 14, 15, 16};
+        for (int i = 0; i < 9; ++i)
+            for (int j = 0; j < 9; ++j) {
+                double s = K21[i][j];
+                for (int l = 0; l < 12; ++l) s += K21[i][9 + l] * Aint[l * 9 + j];
+                Ke[b_idx[i]][b_idx[j]] += s;
+            }
+    }
+    double alpha_drill = (k6rot / 1e5) * G_ref * h;
+    double Bd[18] = {};
+    for (int i = 0; i < 3; ++i) {
+        Bd[6 * i + 0] = 0.5 * cv[i]; Bd[6 * i + 1] = -0.5 * bv[i]; Bd[6 * i + 5] = 1.0 / 3.0;
+    }
+    for (int i = 0; i < 18; ++i)
+        for (int j = 0; j < 18; ++j) Ke[i][j] += alpha_drill * (Bd[i] * Bd[j]) * A;
+}
+
+// stiffness_frame3d_generic (FEMKernels.jl:140-209)
+void frame3d_stiffness(double L, double A, double Iy, double Iz, double J, double E, double G, double As_y,
+                       double As_z, double I12, double k[12][12]) {
+    std::memset(k, 0, sizeof(double) * 144);
+    if (L < 1e-9) return;
+    double X = E * A / L;
+    k[0][0] = X; k[0][6] = -X; k[6][0] = -X; k[6][6] = X;
+    double T = G * J / L;
+    k[3][3] = T; k[3][9] = -T; k[9][3] = -T; k[9][9] = T;
+    double Phi_y = std::isinf(As_z) ? 0.0 : 12 * E * Iy / (G * As_z * L * L);
+    double Phi_z = std::isinf(As_y) ? 0.0 : 12 * E * Iz / (G * As_y * L * L);
+    double a_y = 12 * E * Iy / (L * L * L * (1 + Phi_y)), b_y = 6 * E * Iy / (L * L * (1 + Phi_y));
+    double c_y = (4 + Phi_y) * E * Iy / (L * (1 + Phi_y)), d_y = (2 - Phi_y) * E * Iy / (L * (1 + Phi_y));
+    k[2][2] = a_y; k[2][8] = -a_y; k[8][2] = -a_y; k[8][8] = a_y;
+    k[2][4] = -b_y; k[2][10] = -b_y; k[4][2] = -b_y; k[10][2] = -b_y;
+    k[8][4] = b_y; k[8][10] = b_y; k[4][8] = b_y; k[10][8] = b_y;
+    k[4][4] = c_y; k[4][10] = d_y; k[10][4] = d_y; k[10][10] = c_y;
+    double a_z = 12 * E * Iz / (L * L * L * (1 + Phi_z)), b_z = 6 * E * Iz / (L * L * (1 + Phi_z));
+    double c_z = (4 + Phi_z) * E * Iz / (L * (1 + Phi_z)), d_z = (2 - Phi_z) * E * Iz / (L * (1 + Phi_z));
+    k[1][1] = a_z; k[1][7] = -a_z; k[7][1] = -a_z; k[7][7] = a_z;
+    k[1][5] = b_z; k[1][11] = b_z; k[5][1] = b_z; k[11][1] = b_z;
+    k[7][5] = -b_z; k[7][11] = -b_z; k[5][7] = -b_z; k[11][7] = -b_z;
+    k[5][5] = c_z; k[5][11] = d_z; k[11][5] = d_z; k[11][11] = c_z;
+    if (std::fabs(I12) > 0.0) {
+        double a = 12 * E * I12 / (L * L * L), b = 6 * E * I12 / (L * L), c = 4 * E * I12 / L, d = 2 * E * I12 / L;
+        k[1][2] += a; k[2][1] += a; k[1][8] += -a; k[8][1] += -a;
+        k[7][2] += -a; k[2][7] += -a; k[7][8] += a; k[8][7] += a;
+        k[1][4] += -b; k[4][1] += -b; k[1][10] += -b; k[10][1] += -b;
+        k[7][4] += b; k[4][7] += b; k[7][10] += b; k[10][7] += b;
+        k[2][5] += b; k[5][2] += b; k[2][11] += b; k[11][2] += b;
+        k[8][5] += -b; k[5][8] += -b; k[8][11] += -b; k[11][8] += -b;
+        k[4][5] += -c; k[5][4] += -c; k[4][11] += -d; k[11][4] += -d;
+        k[10][5] += -d; k[5][10] += -d; k[10][11] += -c; k[11][10] += -c;
+    }
+}
+
+// quad4_membrane_force_field with incompatible modes (FEMKernels.jl:6341-6539)
+void q4_membrane_force_field(const double lc[4][2], const double u[24], const double Cm[3][3], double Ngp[4][3]) {
+    const double pt = 1.0 / std::sqrt(3.0);
+    const double gp[4][2] = {{-pt, -pt}, {pt, -pt}, {pt, pt}, {-pt, pt}};
+    double K_ab[24][4] = {}, K_bb[4][4] = {};
+    double Bm_g[4][3][24], Bi_g[4][3][4];
+    for (int g = 0; g < 4; ++g) {
+        double r = gp[g][0], s = gp[g][1];
+        double dNr[4], dNs[4];
+        shape_derivs_quad(r, s, dNr, dNs);
+        Jac j = jacobian(lc, dNr, dNs);
+        double detg = std::fabs(j.det);
+        if (detg < 1e-12) detg = 1e-12;
+        std::memset(Bm_g[g], 0, sizeof(Bm_g[g]));
+        std::memset(Bi_g[g], 0, sizeof(Bi_g[g]));
+        for (int k = 0; k < 4; ++k) {
+            double dx = j.iJ11 * dNr[k] + j.iJ12 * dNs[k];
+            double dy = j.iJ21 * dNr[k] + j.iJ22 * dNs[k];
+            Bm_g[g][0][6 * k] = dx; Bm_g[g][1][6 * k + 1] = dy; Bm_g[g][2][6 * k] = dy; Bm_g[g][2][6 * k + 1] = dx;
+        }
+        double d1x = j.iJ11 * (-2.0 * r), d1y = j.iJ21 * (-2.0 * r), d2x = j.iJ12 * (-2.0 * s), d2y = j.iJ22 * (-2.0 * s);
+        Bi_g[g][0][0] = d1x; Bi_g[g][2][0] = d1y; Bi_g[g][1][1] = d1y; Bi_g[g][2][1] = d1x;
+        Bi_g[g][0][2] = d2x; Bi_g[g][2][2] = d2y; Bi_g[g][1][3] = d2y; Bi_g[g][2][3] = d2x;
+        double CBi[3 * 4];
+        mul(CBi, &Cm[0][0], &Bi_g[g][0][0], 3, 3, 4);
+        mul_At_add(&K_ab[0][0], &Bm_g[g][0][0], CBi, 3, 24, 4, detg);
+        mul_At_add(&K_bb[0][0], &Bi_g[g][0][0], CBi, 3, 4, 4, detg);
+    }
+    double rhs[4], A[16];
+    for (int l = 0; l < 4; ++l) {
+        double s = 0.0;
+        for (int i = 0; i < 24; ++i) s += K_ab[i][l] * u[i];
+        rhs[l] = s;
+    }
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) A[i * 4 + j] = K_bb[i][j];
+    lu_solve(4, 1, A, rhs);
+    double alpha[4] = {-rhs[0], -rhs[1], -rhs[2], -rhs[3]};
+    for (int g = 0; g < 4; ++g) {
+        double eps[3];
+        for (int c = 0; c < 3; ++c) {
+            double s = 0.0;
+            for (int i = 0; i < 24; ++i) s += Bm_g[g][c][i] * u[i];
+            for (int l = 0; l < 4; ++l) s += Bi_g[g][c][l] * alpha[l];
+            eps[c] = s;
+        }
+        for (int c = 0; c < 3; ++c) Ngp[g][c] = Cm[c][0] * eps[0] + Cm[c][1] * eps[1] + Cm[c][2] * eps[2];
+    }
+}
+
+// quad4_membrane_incompatible_condensation_map (FEMKernels.jl:6708-6785):
+// returns A = -(K_bb \ K_ab') (4 x 24).
+void q4_incomp_map(const double lc[4][2], const double Cm[3][3], double Amap[4][24]) {
+    const double pt = 1.0 / std::sqrt(3.0);
+    const double gp[4][2] = {{-pt, -pt}, {pt, -pt}, {pt, pt}, {-pt, pt}};
+    double K_ab[24][4] = {}, K_bb[4][4] = {};
+    for (int g = 0; g < 4; ++g) {
+        double r = gp[g][0], s = gp[g][1];
+        double dNr[4], dNs[4];
+        shape_derivs_quad(r, s, dNr, dNs);
+        Jac j = jacobian(lc, dNr, dNs);
+        double detg = std::fabs(j.det);
+        if (detg < 1e-12) detg = 1e-12;
+        double Bm[3][24] = {}, Bi[3][4] = {};
+        for (int k = 0; k < 4; ++k) {
+            double dx = j.iJ11 * dNr[k] + j.iJ12 * dNs[k];
+            double dy = j.iJ21 * dNr[k] + j.iJ22 * dNs[k];
+            Bm[0][6 * k] = dx; Bm[1][6 * k + 1] = dy; Bm[2][6 * k] = dy; Bm[2][6 * k + 1] = dx;
+        }
+        double d1x = j.iJ11 * (-2.0 * r), d1y = j.iJ21 * (-2.0 * r), d2x = j.iJ12 * (-2.0 * s), d2y = j.iJ22 * (-2.0 * s);
+        Bi[0][0] = d1x; Bi[2][0] = d1y; Bi[1][1] = d1y; Bi[2][1] = d1x;
+        Bi[0][2] = d2x; Bi[2][2] = d2y; Bi[1][3] = d2y; Bi[2][3] = d2x;
+        double CBi[12];
+        mul(CBi, &Cm[0][0], &Bi[0][0], 3, 3, 4);
+        mul_At_add(&K_ab[0][0], &Bm[0][0], CBi, 3, 24, 4, detg);
+        mul_At_add(&K_bb[0][0], &Bi[0][0], CBi, 3, 4, 4, detg);
+    }
+    double A[16], B[4 * 24];
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) A[i * 4 + j] = K_bb[i][j];
+    for (int l = 0; l < 4; ++l)
+        for (int i = 0; i < 24; ++i) B[l * 24 + i] = K_ab[i][l];
+    lu_solve(4, 24, A, B);
+    for (int l = 0; l < 4; ++l)
+        for (int i = 0; i < 24; ++i) Amap[l][i] = -B[l * 24 + i];
+}
+
+// principal_stress_2d_components (FEMKernels.jl:6891-6902)
+void principal2d(double sxx, double syy, double sxy, double out[6]) {
+    double mean = 0.5 * (sxx + syy), hd = 0.5 * (sxx - syy);
+    double rad = std::sqrt(hd * hd + sxy * sxy);
+    if (rad <= 1e-30) { out[0] = mean; out[1] = 1.0; out[2] = 0.0; out[3] = mean; out[4] = 0.0; out[5] = 1.0; return; }
+    double th = 0.5 * std::atan2(2.0 * sxy, sxx - syy);
+    double c = std::cos(th), s = std::sin(th);
+    out[0] = mean + rad; out[1] = c; out[2] = s; out[3] = mean - rad; out[4] = -s; out[5] = c;
+}
+
+// geometric_stiffness_quad4 (matrix-sigma method, FEMKernels.jl:7554-7985)
+// with trans_mode = :principal_transverse, membrane_incomp = true,
+// rot_grad_scale = 0 (flat), shear factors 1.
+void q4_geometric_stiffness(const double lc[4][2], const double sig[4][3], double h, const double Cm[3][3],
+                            double Kg[24][24]) {
+    std::memset(Kg, 0, sizeof(double) * 576);
+    if (h < 1e-30) return;
+    double Amap[4][24];
+    q4_incomp_map(lc, Cm, Amap);
+    const double pt = 1.0 / std::sqrt(3.0);
+    const double gp[4][2] = {{-pt, -pt}, {pt, -pt}, {pt, pt}, {-pt, pt}};
+    for (int g = 0; g < 4; ++g) {
+        double sxx = sig[g][0], syy = sig[g][1], sxy = sig[g][2];
+        double r = gp[g][0], s = gp[g][1];
+        double dNr[4], dNs[4];
+        shape_derivs_quad(r, s, dNr, dNs);
+        Jac j = jacobian(lc, dNr, dNs);
+        double absdet = std::fabs(j.det);
+        if (absdet < 1e-12) absdet = 1e-12;
+        double uxx[24] = {}, uxy[24] = {}, uyx[24] = {}, uyy[24] = {}, uzx[24] = {}, uzy[24] = {};
+        for (int i = 0; i < 4; ++i) {
+            double dx = j.iJ11 * dNr[i] + j.iJ12 * dNs[i];
+            double dy = j.iJ21 * dNr[i] + j.iJ22 * dNs[i];
+            int r0 = 6 * i;
+            uxx[r0] = dx; uxy[r0] = dy; uyx[r0 + 1] = dx; uyy[r0 + 1] = dy; uzx[r0 + 2] = dx; uzy[r0 + 2] = dy;
+        }
+        double d1x = j.iJ11 * (-2.0 * r), d1y = j.iJ21 * (-2.0 * r), d2x = j.iJ12 * (-2.0 * s), d2y = j.iJ22 * (-2.0 * s);
+        for (int a = 0; a < 24; ++a) {
+            double a1 = Amap[0][a], a2 = Amap[1][a], a3 = Amap[2][a], a4 = Amap[3][a];
+            uxx[a] += d1x * a1 + d2x * a3;
+            uxy[a] += d1y * a1 + d2y * a3;
+            uyx[a] += d1x * a2 + d2x * a4;
+            uyy[a] += d1y * a2 + d2y * a4;
+        }
+        double scale = h * absdet;
+        double pr[6];
+        principal2d(sxx, syy, sxy, pr);
+        for (int dir = 0; dir < 2; ++dir) {
+            double lam = pr[3 * dir], c = pr[3 * dir + 1], sn = pr[3 * dir + 2];
+            if (std::fabs(lam) <= 1e-30) continue;
+            double p11 = sn * sn, p22 = c * c, p12 = -c * sn;
+            double f = scale * lam;
+            for (int jj = 0; jj < 24; ++jj) {
+                double gxj = c * uxx[jj] + sn * uxy[jj], gyj = c * uyx[jj] + sn * uyy[jj], gzj = c * uzx[jj] + sn * uzy[jj];
+                for (int ii = 0; ii < 24; ++ii) {
+                    double gxi = c * uxx[ii] + sn * uxy[ii], gyi = c * uyx[ii] + sn * uyy[ii], gzi = c * uzx[ii] + sn * uzy[ii];
+                    Kg[ii][jj] += f * (p11 * gxi * gxj + p22 * gyi * gyj + p12 * (gxi * gyj + gyi * gxj) + gzi * gzj);
+                }
+            }
+        }
+    }
+}
+
+// geometric_stiffness_frame3d (FEMKernels.jl:7441-7471)
+void frame3d_geometric(double L, double P, double kg[12][12]) {
+    std::memset(kg, 0, sizeof(double) * 144);
+    if (L < 1e-9 || std::fabs(P) < 1e-30) return;
+    double c1 = 6.0 * P / (5.0 * L), c2 = P / 10.0, c3 = 2.0 * P * L / 15.0, c4 = -P * L / 30.0;
+    kg[1][1] = c1; kg[7][7] = c1; kg[1][7] = -c1; kg[7][1] = -c1;
+    kg[1][5] = c2; kg[5][1] = c2; kg[1][11] = c2; kg[11][1] = c2;
+    kg[5][5] = c3; kg[11][11] = c3; kg[5][11] = c4; kg[11][5] = c4;
+    kg[7][5] = -c2; kg[5][7] = -c2; kg[7][11] = -c2; kg[11][7] = -c2;
+    kg[2][2] = c1; kg[8][8] = c1; kg[2][8] = -c1; kg[8][2] = -c1;
+    kg[2][4] = -c2; kg[4][2] = -c2; kg[2][10] = -c2; kg[10][2] = -c2;
+    kg[4][4] = c3; kg[10][10] = c3; kg[4][10] = c4; kg[10][4] = c4;
+    kg[8][4] = c2; kg[4][8] = c2; kg[8][10] = c2; kg[10][8] = c2;
+}
+
+// ---------------------------------------------------------------------------
+// model-level assembly
+// ---------------------------------------------------------------------------
+
+struct Triplets {
+    std::vector<int64_t> I, J;  // 0-based
+    std::vector<double> V;
+};
+
+const double *node_R_of(const jfg_model_desc *d, int64_t n, double tmp[9]) {
+    if (d->node_R) return d->node_R + 9 * n;
+    for (int i = 0; i < 9; ++i) tmp[i] = (i % 4 == 0) ? 1.0 : 0.0;
+    return tmp;
+}
+
+// Q4 frame (shell_element_frame_quad4 :diag mode, helpers.jl:1134-1193)
+void q4_frame(const double *p1, const double *p2, const double *p3, const double *p4, double v1[3], double v2[3], double v3[3]) {
+    double gxi[3], geta[3], v3r[3];
+    for (int i = 0; i < 3; ++i) {
+        gxi[i] = 0.25 * (-p1[i] + p2[i] + p3[i] - p4[i]);
+        geta[i] = 0.25 * (-p1[i] - p2[i] + p3[i] + p4[i]);
+    }
+    cross3(gxi, geta, v3r);
+    if (dot3(v3r, v3r) <= 1e-24) {
+        double d13[3], d24[3];
+        sub3(p3, p1, d13); sub3(p4, p2, d24);
+        cross3(d13, d24, v3r);
+    }
+    normalize3(v3r, v3);
+    double d13[3], d24[3], d13n[3], d24n[3], xr[3];
+    sub3(p3, p1, d13); sub3(p4, p2, d24);
+    normalize3(d13, d13n); normalize3(d24, d24n);
+    for (int i = 0; i < 3; ++i) xr[i] = d13n[i] - d24n[i];
+    if (dot3(xr, xr) < 1e-20)
+        for (int i = 0; i < 3; ++i) xr[i] = d13n[i] + d24n[i];
+    double xp[3], dv = dot3(xr, v3);
+    for (int i = 0; i < 3; ++i) xp[i] = xr[i] - dv * v3[i];
+    if (dot3(xp, xp) <= 1e-24) {
+        double ga = dot3(geta, v3);
+        for (int i = 0; i < 3; ++i) xp[i] = geta[i] - ga * v3[i];
+        if (dot3(xp, xp) <= 1e-24) {
+            double e[3];
+            sub3(p2, p1, e);
+            double ev = dot3(e, v3);
+            for (int i = 0; i < 3; ++i) xp[i] = e[i] - ev * v3[i];
+        }
+    }
+    normalize3(xp, v1);
+    cross3(v3, v1, v2);
+}
+
+// flatness test of the K/KG loops (assembly.jl:2824-2840, :4817-4832)
+bool q4_is_flat(const double *p1, const double *p2, const double *p3, const double *p4) {
+    double d13[3], d24[3], n[3], c[3];
+    sub3(p3, p1, d13); sub3(p4, p2, d24);
+    cross3(d13, d24, n);
+    double len = norm3(n);
+    for (int i = 0; i < 3; ++i) c[i] = (p1[i] + p2[i] + p3[i] + p4[i]) / 4.0;
+    double maxdev = 0.0;
+    if (len > 1e-12) {
+        double g[3] = {n[0] / len, n[1] / len, n[2] / len};
+        const double *ps[4] = {p1, p2, p3, p4};
+        for (int k = 0; k < 4; ++k) {
+            double d[3];
+            sub3(ps[k], c, d);
+            maxdev = std::max(maxdev, std::fabs(dot3(d, g)));
+        }
+    }
+    double L = std::max(norm3(d13), norm3(d24));
+    return maxdev < 1e-6 * std::max(L, 1e-12);
+}
+
+void shell_constitutive(const double *pr, double Cm[3][3], double Cb[3][3], double Cs[2][2]) {
+    double h = pr[0], E = pr[1], nu = pr[2], br = pr[4], tst = pr[5], Gs = pr[6];
+    double cm = E * h / (1 - nu * nu);
+    double cb = br * (E * h * h * h) / (12 * (1 - nu * nu));
+    double base[3][3] = {{1.0, nu, 0.0}, {nu, 1.0, 0.0}, {0.0, 0.0, (1 - nu) / 2}};
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) { Cm[i][j] = cm * base[i][j]; Cb[i][j] = cb * base[i][j]; }
+    double G = Gs;
+    Cs[0][0] = tst * h * G; Cs[0][1] = 0.0; Cs[1][0] = 0.0; Cs[1][1] = tst * h * G;
+    if (br <= 1e-12) { Cs[0][0] = Cs[0][1] = Cs[1][0] = Cs[1][1] = 0.0; }
+}
+
+// T' K T for a block-diagonal T built from 3x3 node blocks Q_k = Rel * node_R
+void transform_sym(int nn, const double *Q /* nn*9 */, const double *K, double *out) {
+    int n = 6 * nn;
+    std::vector<double> T(n * n, 0.0), tmp(n * n, 0.0);
+    for (int k = 0; k < nn; ++k)
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) {
+                T[(6 * k + r) * n + 6 * k + c] = Q[9 * k + 3 * r + c];
+                T[(6 * k + 3 + r) * n + 6 * k + 3 + c] = Q[9 * k + 3 * r + c];
+            }
+    mul(tmp.data(), K, T.data(), n, n, n);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            double s = 0.0;
+            for (int l = 0; l < n; ++l) s += T[l * n + i] * tmp[l * n + j];
+            out[i * n + j] = s;
+        }
+}
+
+struct Err { int code = 0; std::string msg; };
+
+int check_predicates(const jfg_model_desc *d, std::string &msg) {
+    if (d->param_snorm > 0.0) { msg = "PARAM,SNORM > 0 leaves the default branch (snorm.jl:72-83)"; return JFG_ERR_UNSUPPORTED; }
+    for (int64_t e = 0; e < d->n_quad4; ++e) {
+        const int32_t *n = d->quad4_nodes + 4 * e;
+        if (!(d->quad4_prop[JFG_SHELL_PROP * e] > 0.0) || !(d->quad4_prop[JFG_SHELL_PROP * e + 1] > 0.0)) { msg = "shell thickness and E must be positive"; return JFG_ERR_INVALID; }
+        for (int k = 0; k < 4; ++k)
+            if (n[k] < 0 || n[k] >= d->n_nodes) { msg = "quad4 node index out of range"; return JFG_ERR_INVALID; }
+        if (!q4_is_flat(d->coords + 3 * n[0], d->coords + 3 * n[1], d->coords + 3 * n[2], d->coords + 3 * n[3])) {
+            msg = "non-flat CQUAD4 (warp >= 1e-6 of the diagonal) leaves the flat default branch (assembly.jl:2824-2840)";
+            return JFG_ERR_UNSUPPORTED;
+        }
+    }
+    for (int64_t e = 0; e < d->n_tria3; ++e) {
+        if (!(d->tria3_prop[JFG_SHELL_PROP * e] > 0.0) || !(d->tria3_prop[JFG_SHELL_PROP * e + 1] > 0.0)) { msg = "shell thickness and E must be positive"; return JFG_ERR_INVALID; }
+        for (int k = 0; k < 3; ++k)
+            if (d->tria3_nodes[3 * e + k] < 0 || d->tria3_nodes[3 * e + k] >= d->n_nodes) { msg = "tria3 node index out of range"; return JFG_ERR_INVALID; }
+    }
+    for (int64_t e = 0; e < d->n_bar; ++e) {
+        for (int k = 0; k < 2; ++k)
+            if (d->bar_nodes[2 * e + k] < 0 || d->bar_nodes[2 * e + k] >= d->n_nodes) { msg = "bar node index out of range"; return JFG_ERR_INVALID; }
+        if (d->bar_pin && (d->bar_pin[2 * e] != 0 || d->bar_pin[2 * e + 1] != 0)) {
+            msg = "CBAR pin flags PA/PB are outside the supported branch (helpers.jl:1630-1660)"; return JFG_ERR_UNSUPPORTED;
+        }
+    }
+    return 0;
+}
+
+// Q4 and T3 geometry helpers shared by K and KG
+void t3_frame(const double *p1, const double *p2, const double *p3, double v1[3], double v2[3], double v3[3]) {
+    double e[3], f[3], c[3];
+    sub3(p2, p1, e);
+    normalize3(e, v1);
+    sub3(p3, p1, f);
+    cross3(v1, f, c);
+    normalize3(c, v3);
+    cross3(v3, v1, v2);
+}
+
+void node_blocks(const jfg_model_desc *d, const int32_t *nodes, int nn, const double v1[3], const double v2[3], const double v3[3], double *Q) {
+    double Rel[9] = {v1[0], v1[1], v1[2], v2[0], v2[1], v2[2], v3[0], v3[1], v3[2]};
+    for (int k = 0; k < nn; ++k) {
+        double tmp[9];
+        const double *R = node_R_of(d, nodes[k], tmp);
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) Q[9 * k + 3 * r + c] = Rel[3 * r] * R[c] + Rel[3 * r + 1] * R[3 + c] + Rel[3 * r + 2] * R[6 + c];
+    }
+}
+
+// bar frame + T12 (assembly.jl:3961-4025)
+bool bar_setup(const jfg_model_desc *d, int64_t e, double &L, double T12[12][12], bool &has_offset) {
+    const int32_t *nd = d->bar_nodes + 2 * e;
+    const double *pr = d->bar_prop + JFG_BAR_PROP * e;
+    const double *p1 = d->coords + 3 * nd[0], *p2 = d->coords + 3 * nd[1];
+    double wa[3] = {pr[12], pr[13], pr[14]}, wb[3] = {pr[15], pr[16], pr[17]};
+    has_offset = dot3(wa, wa) > 1e-20 || dot3(wb, wb) > 1e-20;
+    double a[3], b[3];
+    for (int i = 0; i < 3; ++i) { a[i] = has_offset ? p1[i] + wa[i] : p1[i]; b[i] = has_offset ? p2[i] + wb[i] : p2[i]; }
+    double dd[3];
+    sub3(b, a, dd);
+    L = norm3(dd);
+    if (L < 1e-9) return false;
+    double vx[3], vref[3] = {pr[9], pr[10], pr[11]}, vz[3], vy[3], t[3];
+    normalize3(dd, vx);
+    if (norm3(vref) < 1e-6) {
+        vref[0] = 0.0; vref[1] = 0.0; vref[2] = 1.0;
+        if (std::fabs(dot3(vx, vref)) > 0.9) { vref[0] = 0.0; vref[1] = 1.0; vref[2] = 0.0; }
+    }
+    cross3(vx, vref, t);
+    normalize3(t, vz);
+    cross3(vz, vx, vy);
+    double Rel[3][3] = {{vx[0], vx[1], vx[2]}, {vy[0], vy[1], vy[2]}, {vz[0], vz[1], vz[2]}};
+    std::memset(T12, 0, sizeof(double) * 144);
+    for (int k = 0; k < 2; ++k) {
+        double tmp[9];
+        const double *R = node_R_of(d, nd[k], tmp);
+        double TR[3][3];
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) TR[r][c] = Rel[r][0] * R[c] + Rel[r][1] * R[3 + c] + Rel[r][2] * R[6 + c];
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) { T12[6 * k + r][6 * k + c] = TR[r][c]; T12[6 * k + 3 + r][6 * k + 3 + c] = TR[r][c]; }
+        if (has_offset) {
+            const double *w = k == 0 ? wa : wb;
+            double S[3][3] = {{0.0, -w[2], w[1]}, {w[2], 0.0, -w[0]}, {-w[1], w[0], 0.0}};
+            double RS[3][3];
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) RS[r][c] = Rel[r][0] * S[0][c] + Rel[r][1] * S[1][c] + Rel[r][2] * S[2][c];
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) T12[6 * k + r][6 * k + 3 + c] = -(RS[r][0] * R[c] + RS[r][1] * R[3 + c] + RS[r][2] * R[6 + c]);
+        }
+    }
+    return true;
+}
+
+void bar_section(const double *pr, double &A, double &Iy, double &Iz, double &I12, double &J, double &E, double &G, double &Asy, double &Asz) {
+    A = pr[0];
+    Iy = pr[2]; Iz = pr[1];
+    if (Iy == 0.0) Iy = Iz;
+    if (Iz == 0.0) Iz = Iy;
+    I12 = pr[3]; J = pr[4];
+    double K1 = pr[5], K2 = pr[6];
+    E = pr[7]; G = pr[8];
+    Asy = K1 > 0.0 ? K1 * A : INFINITY;
+    Asz = K2 > 0.0 ? K2 * A : INFINITY;
+}
+
+// RBE2 dependent map (constraints.jl:7-74)
+std::map<int64_t, std::vector<std::pair<int64_t, double>>> rbe2_map(const jfg_model_desc *d) {
+    std::map<int64_t, std::vector<std::pair<int64_t, double>>> mp;
+    for (int64_t r = 0; r < d->n_rbe2; ++r) {
+        int64_t gm = d->rbe2_master[r];
+        const double *pm = d->coords + 3 * gm;
+        double tm[9];
+        const double *Rm = node_R_of(d, gm, tm);
+        for (int64_t s = d->rbe2_slave_ptr[r]; s < d->rbe2_slave_ptr[r + 1]; ++s) {
+            int64_t gs = d->rbe2_slaves[s];
+            const double *ps = d->coords + 3 * gs;
+            double dx = ps[0] - pm[0], dy = ps[1] - pm[1], dz = ps[2] - pm[2];
+            double ts[9];
+            const double *Rs = node_R_of(d, gs, ts);
+            double comp[3][3], O[3][3] = {{0.0, dz, -dy}, {-dz, 0.0, dx}, {dy, -dx, 0.0}}, RsO[3][3], off[3][3];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) comp[i][j] = Rs[i] * Rm[j] + Rs[3 + i] * Rm[3 + j] + Rs[6 + i] * Rm[6 + j];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) RsO[i][j] = Rs[i] * O[0][j] + Rs[3 + i] * O[1][j] + Rs[6 + i] * O[2][j];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) off[i][j] = RsO[i][0] * Rm[j] + RsO[i][1] * Rm[3 + j] + RsO[i][2] * Rm[6 + j];
+            for (int c = 1; c <= 6; ++c) {
+                if (!(d->rbe2_cm[r] & (1 << (c - 1)))) continue;
+                double row[6];
+                if (c <= 3) {
+                    for (int j = 0; j < 3; ++j) { row[j] = comp[c - 1][j]; row[3 + j] = off[c - 1][j]; }
+                } else {
+                    for (int j = 0; j < 3; ++j) { row[j] = 0.0; row[3 + j] = comp[c - 4][j]; }
+                }
+                std::vector<std::pair<int64_t, double>> pairs;
+                for (int j = 0; j < 6; ++j)
+                    if (std::fabs(row[j]) > 1e-15) pairs.push_back({6 * gm + j, row[j]});
+                if (!pairs.empty()) mp[6 * gs + (c - 1)] = pairs;
+            }
+        }
+    }
+    return mp;
+}
+
+// triplet redistribution (constraints.jl:329-361) + sparse() to 1-based CSC
+void constrain_and_csc(const jfg_model_desc *d, Triplets &t, std::vector<int64_t> &colptr, std::vector<int64_t> &rowval,
+                       std::vector<double> &nzval) {
+    auto mp = rbe2_map(d);
+    int64_t ndof = 6 * d->n_nodes;
+    std::vector<const std::vector<std::pair<int64_t, double>> *> dep(ndof, nullptr);
+    for (auto &kv : mp) dep[kv.first] = &kv.second;
+    std::vector<std::pair<uint64_t, double>> kv;
+    kv.reserve(t.V.size() + t.V.size() / 10);
+    auto key = [&](int64_t i, int64_t j) { return (uint64_t)j * (uint64_t)ndof + (uint64_t)i; };
+    for (size_t k = 0; k < t.V.size(); ++k) {
+        int64_t i = t.I[k], j = t.J[k];
+        double v = t.V[k];
+        const auto *di = dep[i], *dj = dep[j];
+        if (!di && !dj) kv.push_back({key(i, j), v});
+        else if (di && !dj) { for (auto &p : *di) kv.push_back({key(p.first, j), v * p.second}); }
+        else if (!di && dj) { for (auto &p : *dj) kv.push_back({key(i, p.first), v * p.second}); }
+        else {
+            for (auto &a : *di)
+                for (auto &b : *dj) kv.push_back({key(a.first, b.first), v * a.second * b.second});
+        }
+    }
+    std::stable_sort(kv.begin(), kv.end(), [](const std::pair<uint64_t, double> &a, const std::pair<uint64_t, double> &b) { return a.first < b.first; });
+    colptr.assign(ndof + 1, 0);
+    rowval.clear(); nzval.clear();
+    size_t k = 0;
+    while (k < kv.size()) {
+        uint64_t kk = kv[k].first;
+        double s = 0.0;
+        while (k < kv.size() && kv[k].first == kk) { s += kv[k].second; ++k; }
+        int64_t col = (int64_t)(kk / ndof), row = (int64_t)(kk % ndof);
+        rowval.push_back(row + 1);
+        nzval.push_back(s);
+        colptr[col + 1] += 1;
+    }
+    colptr[0] = 1;
+    for (int64_t c = 0; c < ndof; ++c) colptr[c + 1] += colptr[c];
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// exported oracle API (test infrastructure)
+// ---------------------------------------------------------------------------
+
+struct OracleCSC {
+    std::vector<int64_t> colptr, rowval;
+    std::vector<double> nzval, orig_diag;
+    double max_elem_stiff = 0.0;
+    std::string err;
+};
+
+extern "C" {
+
+// Element-level entry points (local frame), used by tests on single elements.
+void oracle_q4_stiffness_local(const double *lc8, const double *prop7, double k6rot, double *Ke576) {
+    double lc[4][2], Cm[3][3], Cb[3][3], Cs[2][2];
+    for (int k = 0; k < 4; ++k) { lc[k][0] = lc8[2 * k]; lc[k][1] = lc8[2 * k + 1]; }
+    shell_constitutive(prop7, Cm, Cb, Cs);
+    double br = prop7[4];
+    double ek6 = br <= 1e-12 ? 0.0 : k6rot, eds = br <= 1e-12 ? 0.0 : 1.0;
+    q4_stiffness(lc, Cm, Cb, Cs, prop7[0], prop7[1], ek6, eds, true, true, (double(*)[24])Ke576);
+}
+
+void oracle_t3_stiffness_local(const double *lc6, const double *prop7, double k6rot, double *Ke324) {
+    double lc[3][2], Cm[3][3], Cb[3][3], Cs[2][2];
+    for (int k = 0; k < 3; ++k) { lc[k][0] = lc6[2 * k]; lc[k][1] = lc6[2 * k + 1]; }
+    shell_constitutive(prop7, Cm, Cb, Cs);
+    double br = prop7[4];
+    t3_stiffness(lc, Cm, Cb, Cs, prop7[0], prop7[6], br, br <= 1e-12 ? 0.0 : k6rot, (double(*)[18])Ke324);
+}
+
+int oracle_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+void oracle_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
+// Element triplets of K (before constraints), element order: quads, trias, bars.
+// Returns 0 or a jfg status; *handle receives an OracleCSC.
+int oracle_assemble_k(const jfg_model_desc *d, void **handle) {
+    auto *out = new OracleCSC();
+    *handle = out;
+    int st = check_predicates(d, out->err);
+    if (st) return st;
+    int64_t nq = d->n_quad4, nt = d->n_tria3, nb = d->n_bar;
+    Triplets t;
+    size_t total = (size_t)nq * 576 + (size_t)nt * 324 + (size_t)nb * 144;
+    t.I.resize(total); t.J.resize(total); t.V.resize(total);
+    // CQUAD4 loop (assembly.jl:2657-3852)
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < nq; ++e) {
+        const int32_t *nd = d->quad4_nodes + 4 * e;
+        const double *p[4];
+        for (int k = 0; k < 4; ++k) p[k] = d->coords + 3 * nd[k];
+        double v1[3], v2[3], v3[3];
+        q4_frame(p[0], p[1], p[2], p[3], v1, v2, v3);
+        double c[3];
+        for (int i = 0; i < 3; ++i) c[i] = (p[0][i] + p[1][i] + p[2][i] + p[3][i]) / 4.0;
+        double lc[4][2];
+        for (int k = 0; k < 4; ++k) {
+            double dd[3];
+            sub3(p[k], c, dd);
+            lc[k][0] = dot3(dd, v1); lc[k][1] = dot3(dd, v2);
+        }
+        const double *pr = d->quad4_prop + JFG_SHELL_PROP * e;
+        double Cm[3][3], Cb[3][3], Cs[2][2];
+        shell_constitutive(pr, Cm, Cb, Cs);
+        double br = pr[4];
+        double k6 = br <= 1e-12 ? 0.0 : d->k6rot, ds = br <= 1e-12 ? 0.0 : 1.0;
+        double Ke[24][24];
+        // elem_membrane_incomp is true for flat isotropic shells (assembly.jl:3393)
+        q4_stiffness(lc, Cm, Cb, Cs, pr[0], pr[1], k6, ds, true, true, Ke);
+        double Q[36], G[576];
+        node_blocks(d, nd, 4, v1, v2, v3, Q);
+        transform_sym(4, Q, &Ke[0][0], G);
+        size_t base = (size_t)e * 576;
+        int cnt = 0;
+        for (int cc = 0; cc < 24; ++cc)
+            for (int rr = 0; rr < 24; ++rr) {
+                t.I[base + cnt] = 6 * (int64_t)nd[rr / 6] + rr % 6;
+                t.J[base + cnt] = 6 * (int64_t)nd[cc / 6] + cc % 6;
+                t.V[base + cnt] = G[rr * 24 + cc];
+                ++cnt;
+            }
+    }
+    // CTRIA3 loop (assembly.jl:3866-3955)
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < nt; ++e) {
+        const int32_t *nd = d->tria3_nodes + 3 * e;
+        const double *p1 = d->coords + 3 * nd[0], *p2 = d->coords + 3 * nd[1], *p3 = d->coords + 3 * nd[2];
+        double v1[3], v2[3], v3[3];
+        t3_frame(p1, p2, p3, v1, v2, v3);
+        double c[3];
+        for (int i = 0; i < 3; ++i) c[i] = (p1[i] + p2[i] + p3[i]) / 3.0;
+        const double *ps[3] = {p1, p2, p3};
+        double lc[3][2];
+        for (int k = 0; k < 3; ++k) {
+            double dd[3];
+            sub3(ps[k], c, dd);
+            lc[k][0] = dot3(dd, v1); lc[k][1] = dot3(dd, v2);
+        }
+        const double *pr = d->tria3_prop + JFG_SHELL_PROP * e;
+        double Cm[3][3], Cb[3][3], Cs[2][2];
+        shell_constitutive(pr, Cm, Cb, Cs);
+        double br = pr[4];
+        double Ke[18][18];
+        t3_stiffness(lc, Cm, Cb, Cs, pr[0], pr[6], br, br <= 1e-12 ? 0.0 : d->k6rot, Ke);
+        double Q[27], G[324];
+        node_blocks(d, nd, 3, v1, v2, v3, Q);
+        transform_sym(3, Q, &Ke[0][0], G);
+        size_t base = (size_t)nq * 576 + (size_t)e * 324;
+        int cnt = 0;
+        for (int cc = 0; cc < 18; ++cc)
+            for (int rr = 0; rr < 18; ++rr) {
+                t.I[base + cnt] = 6 * (int64_t)nd[rr / 6] + rr % 6;
+                t.J[base + cnt] = 6 * (int64_t)nd[cc / 6] + cc % 6;
+                t.V[base + cnt] = G[rr * 18 + cc];
+                ++cnt;
+            }
+    }
+    // CBAR / CBEAM (assembly.jl:3961-4092)
+    std::vector<char> bar_ok(nb, 1);
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < nb; ++e) {
+        double L, T12[12][12];
+        bool off;
+        size_t base = (size_t)nq * 576 + (size_t)nt * 324 + (size_t)e * 144;
+        if (!bar_setup(d, e, L, T12, off)) { bar_ok[e] = 0; continue; }
+        double A, Iy, Iz, I12, J, E, G, Asy, Asz;
+        bar_section(d->bar_prop + JFG_BAR_PROP * e, A, Iy, Iz, I12, J, E, G, Asy, Asz);
+        double k[12][12], tmp[144], Kg[144];
+        frame3d_stiffness(L, A, Iy, Iz, J, E, G, Asy, Asz, I12, k);
+        mul(tmp, &k[0][0], &T12[0][0], 12, 12, 12);
+        for (int i = 0; i < 12; ++i)
+            for (int j = 0; j < 12; ++j) {
+                double s = 0.0;
+                for (int l = 0; l < 12; ++l) s += T12[l][i] * tmp[l * 12 + j];
+                Kg[i * 12 + j] = s;
+            }
+        const int32_t *nd = d->bar_nodes + 2 * e;
+        int cnt = 0;
+        for (int cc = 0; cc < 12; ++cc)
+            for (int rr = 0; rr < 12; ++rr) {
+                t.I[base + cnt] = 6 * (int64_t)nd[rr / 6] + rr % 6;
+                t.J[base + cnt] = 6 * (int64_t)nd[cc / 6] + cc % 6;
+                t.V[base + cnt] = Kg[rr * 12 + cc];
+                ++cnt;
+            }
+    }
+    // zero-length bars are skipped (no triplets): compact
+    {
+        Triplets u;
+        size_t nbase = (size_t)nq * 576 + (size_t)nt * 324;
+        bool any = false;
+        for (int64_t e = 0; e < nb; ++e) any |= !bar_ok[e];
+        if (any) {
+            u.I.assign(t.I.begin(), t.I.begin() + nbase); u.J.assign(t.J.begin(), t.J.begin() + nbase); u.V.assign(t.V.begin(), t.V.begin() + nbase);
+            for (int64_t e = 0; e < nb; ++e)
+                if (bar_ok[e])
+                    for (int q = 0; q < 144; ++q) { size_t s = nbase + e * 144 + q; u.I.push_back(t.I[s]); u.J.push_back(t.J[s]); u.V.push_back(t.V[s]); }
+            t = std::move(u);
+        }
+    }
+    // max_elem_stiff and orig_diag before constraints (assembly.jl:4353-4364)
+    double mx = 0.0;
+    for (double v : t.V) mx = std::max(mx, std::fabs(v));
+    out->max_elem_stiff = mx;
+    out->orig_diag.assign(6 * d->n_nodes, 0.0);
+    for (size_t k = 0; k < t.V.size(); ++k)
+        if (t.I[k] == t.J[k]) out->orig_diag[t.I[k]] += t.V[k];
+    constrain_and_csc(d, t, out->colptr, out->rowval, out->nzval);
+    return 0;
+}
+
+// KG assembly (assembly.jl:4382-6634), element order quads, trias, bars.
+int oracle_assemble_kg(const jfg_model_desc *d, const double *u, void **handle) {
+    auto *out = new OracleCSC();
+    *handle = out;
+    int st = check_predicates(d, out->err);
+    if (st) return st;
+    int64_t nq = d->n_quad4, nt = d->n_tria3, nb = d->n_bar;
+    // CBAR/CBEAM with offsets: the reference's u_bar extraction indexes
+    // T12[6+dd, 9+d] for d = 4..6, which is out of bounds for the 12x12 T12
+    // and raises a BoundsError (assembly.jl:6322-6327, :6398-6403).
+    for (int64_t e = 0; e < nb; ++e) {
+        double L, T12[12][12];
+        bool off;
+        if (bar_setup(d, e, L, T12, off) && off) {
+            out->err = "assemble_geometric_stiffness raises BoundsError for CBAR/CBEAM with offsets (assembly.jl:6326)";
+            return JFG_ERR_REFERENCE_RAISES;
+        }
+    }
+    Triplets t;
+    size_t total = (size_t)nq * 576 + (size_t)nt * 324 + (size_t)nb * 144;
+    t.I.resize(total); t.J.resize(total); t.V.resize(total);
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < nq; ++e) {
+        const int32_t *nd = d->quad4_nodes + 4 * e;
+        const double *p[4];
+        for (int k = 0; k < 4; ++k) p[k] = d->coords + 3 * nd[k];
+        double v1[3], v2[3], v3[3];
+        q4_frame(p[0], p[1], p[2], p[3], v1, v2, v3);
+        double c[3];
+        for (int i = 0; i < 3; ++i) c[i] = (p[0][i] + p[1][i] + p[2][i] + p[3][i]) / 4.0;
+        double lc[4][2];
+        for (int k = 0; k < 4; ++k) {
+            double dd[3];
+            sub3(p[k], c, dd);
+            lc[k][0] = dot3(dd, v1); lc[k][1] = dot3(dd, v2);
+        }
+        double Q[36];
+        node_blocks(d, nd, 4, v1, v2, v3, Q);
+        // u_elem = T u_global (assembly.jl:5176-5185)
+        double ue[24];
+        for (int k = 0; k < 4; ++k) {
+            const double *ug = u + 6 * (int64_t)nd[k];
+            for (int dd = 0; dd < 3; ++dd) {
+                ue[6 * k + dd] = Q[9 * k + 3 * dd] * ug[0] + Q[9 * k + 3 * dd + 1] * ug[1] + Q[9 * k + 3 * dd + 2] * ug[2];
+                ue[6 * k + 3 + dd] = Q[9 * k + 3 * dd] * ug[3] + Q[9 * k + 3 * dd + 1] * ug[4] + Q[9 * k + 3 * dd + 2] * ug[5];
+            }
+        }
+        const double *pr = d->quad4_prop + JFG_SHELL_PROP * e;
+        double h = pr[0], E = pr[1], nu = pr[2];
+        double cm = E / (1 - nu * nu);
+        double Cm[3][3] = {{cm * 1.0 * h, cm * nu * h, 0.0}, {cm * nu * h, cm * 1.0 * h, 0.0}, {0.0, 0.0, cm * ((1 - nu) / 2) * h}};
+        double Ngp[4][3], sig[4][3];
+        q4_membrane_force_field(lc, ue, Cm, Ngp);
+        for (int g = 0; g < 4; ++g)
+            for (int cc = 0; cc < 3; ++cc) sig[g][cc] = Ngp[g][cc] / h;
+        double Kl[24][24], G[576];
+        q4_geometric_stiffness(lc, sig, h, Cm, Kl);
+        transform_sym(4, Q, &Kl[0][0], G);
+        for (int k = 0; k < 4; ++k) {
+            int dd = 6 * k + 5;
+            for (int r = 0; r < 24; ++r) { G[r * 24 + dd] = 0.0; G[dd * 24 + r] = 0.0; }
+        }
+        size_t base = (size_t)e * 576;
+        int cnt = 0;
+        for (int cc = 0; cc < 24; ++cc)
+            for (int rr = 0; rr < 24; ++rr) {
+                t.I[base + cnt] = 6 * (int64_t)nd[rr / 6] + rr % 6;
+                t.J[base + cnt] = 6 * (int64_t)nd[cc / 6] + cc % 6;
+                t.V[base + cnt] = G[rr * 24 + cc];
+                ++cnt;
+            }
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < nt; ++e) {
+        const int32_t *nd = d->tria3_nodes + 3 * e;
+        const double *p1 = d->coords + 3 * nd[0], *p2 = d->coords + 3 * nd[1], *p3 = d->coords + 3 * nd[2];
+        double v1[3], v2[3], v3[3];
+        t3_frame(p1, p2, p3, v1, v2, v3);
+        double c[3];
+        for (int i = 0; i < 3; ++i) c[i] = (p1[i] + p2[i] + p3[i]) / 3.0;
+        const double *ps[3] = {p1, p2, p3};
+        double lc[3][2];
+        for (int k = 0; k < 3; ++k) {
+            double dd[3];
+            sub3(ps[k], c, dd);
+            lc[k][0] = dot3(dd, v1); lc[k][1] = dot3(dd, v2);
+        }
+        double Q[27];
+        node_blocks(d, nd, 3, v1, v2, v3, Q);
+        double ue[18];
+        for (int k = 0; k < 3; ++k) {
+            const double *ug = u + 6 * (int64_t)nd[k];
+            for (int dd = 0; dd < 3; ++dd) {
+                ue[6 * k + dd] = Q[9 * k + 3 * dd] * ug[0] + Q[9 * k + 3 * dd + 1] * ug[1] + Q[9 * k + 3 * dd + 2] * ug[2];
+                ue[6 * k + 3 + dd] = Q[9 * k + 3 * dd] * ug[3] + Q[9 * k + 3 * dd + 1] * ug[4] + Q[9 * k + 3 * dd + 2] * ug[5];
+            }
+        }
+        const double *pr = d->tria3_prop + JFG_SHELL_PROP * e;
+        double h = pr[0], E = pr[1], nu = pr[2];
+        double Kl[18][18] = {};
+        double x[3] = {lc[0][0], lc[1][0], lc[2][0]}, y[3] = {lc[0][1], lc[1][1], lc[2][1]};
+        double A = 0.5 * std::fabs(x[0] * (y[1] - y[2]) + x[1] * (y[2] - y[0]) + x[2] * (y[0] - y[1]));
+        if (A >= 1e-12 && h >= 1e-30) {
+            // stress_strain_tria3 membrane part (FEMKernels.jl:7391-7404)
+            double b[3] = {(y[1] - y[2]) / (2 * A), (y[2] - y[0]) / (2 * A), (y[0] - y[1]) / (2 * A)};
+            double cv[3] = {(x[2] - x[1]) / (2 * A), (x[0] - x[2]) / (2 * A), (x[1] - x[0]) / (2 * A)};
+            double um[6] = {ue[0], ue[1], ue[6], ue[7], ue[12], ue[13]};
+            double eps[3] = {0, 0, 0};
+            for (int i = 0; i < 3; ++i) {
+                eps[0] += b[i] * um[2 * i];
+                eps[1] += cv[i] * um[2 * i + 1];
+                eps[2] += cv[i] * um[2 * i] + b[i] * um[2 * i + 1];
+            }
+            double cm = E / (1 - nu * nu);
+            double D[3][3] = {{cm, cm * nu, 0.0}, {cm * nu, cm, 0.0}, {0.0, 0.0, cm * (1 - nu) / 2}};
+            double N[3];
+            for (int i = 0; i < 3; ++i) N[i] = (D[i][0] * eps[0] + D[i][1] * eps[1] + D[i][2] * eps[2]) * h;
+            double sxx = N[0] / h, syy = N[1] / h, sxy = N[2] / h;
+            // geometric_stiffness_tria3, non-curvature branch (FEMKernels.jl:8083-8097)
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    double val = h * A * (sxx * b[i] * b[j] + syy * cv[i] * cv[j] + sxy * (b[i] * cv[j] + cv[i] * b[j]));
+                    for (int dd = 0; dd < 3; ++dd) Kl[6 * i + dd][6 * j + dd] += val;
+                }
+        }
+        double G[324];
+        transform_sym(3, Q, &Kl[0][0], G);
+        for (int k = 0; k < 3; ++k) {
+            int dd = 6 * k + 5;
+            for (int r = 0; r < 18; ++r) { G[r * 18 + dd] = 0.0; G[dd * 18 + r] = 0.0; }
+        }
+        size_t base = (size_t)nq * 576 + (size_t)e * 324;
+        int cnt = 0;
+        for (int cc = 0; cc < 18; ++cc)
+            for (int rr = 0; rr < 18; ++rr) {
+                t.I[base + cnt] = 6 * (int64_t)nd[rr / 6] + rr % 6;
+                t.J[base + cnt] = 6 * (int64_t)nd[cc / 6] + cc % 6;
+                t.V[base + cnt] = G[rr * 18 + cc];
+                ++cnt;
+            }
+    }
+    std::vector<char> bar_ok(nb, 1);
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < nb; ++e) {
+        double L, T12[12][12];
+        bool off;
+        if (!bar_setup(d, e, L, T12, off)) { bar_ok[e] = 0; continue; }
+        const int32_t *nd = d->bar_nodes + 2 * e;
+        double ub[12] = {};
+        for (int k = 0; k < 2; ++k) {
+            const double *ug = u + 6 * (int64_t)nd[k];
+            for (int dd = 0; dd < 6; ++dd)
+                for (int q = 0; q < 6; ++q) ub[6 * k + dd] += T12[6 * k + dd][6 * k + q] * ug[q];
+        }
+        double A, Iy, Iz, I12, J, E, G, Asy, Asz;
+        bar_section(d->bar_prop + JFG_BAR_PROP * e, A, Iy, Iz, I12, J, E, G, Asy, Asz);
+        double k[12][12];
+        frame3d_stiffness(L, A, Iy, Iz, J, E, G, Asy, Asz, I12, k);
+        double P = 0.0;
+        for (int q = 0; q < 12; ++q) P += k[6][q] * ub[q];
+        double kg[12][12], tmp[144], Kb[144];
+        frame3d_geometric(L, P, kg);
+        mul(tmp, &kg[0][0], &T12[0][0], 12, 12, 12);
+        for (int i = 0; i < 12; ++i)
+            for (int j = 0; j < 12; ++j) {
+                double s = 0.0;
+                for (int l = 0; l < 12; ++l) s += T12[l][i] * tmp[l * 12 + j];
+                Kb[i * 12 + j] = s;
+            }
+        size_t base = (size_t)nq * 576 + (size_t)nt * 324 + (size_t)e * 144;
+        int cnt = 0;
+        for (int cc = 0; cc < 12; ++cc)
+            for (int rr = 0; rr < 12; ++rr) {
+                t.I[base + cnt] = 6 * (int64_t)nd[rr / 6] + rr % 6;
+                t.J[base + cnt] = 6 * (int64_t)nd[cc / 6] + cc % 6;
+                t.V[base + cnt] = Kb[rr * 12 + cc];
+                ++cnt;
+            }
+    }
+    {
+        size_t nbase = (size_t)nq * 576 + (size_t)nt * 324;
+        bool any = false;
+        for (int64_t e = 0; e < nb; ++e) any |= !bar_ok[e];
+        if (any) {
+            Triplets u2;
+            u2.I.assign(t.I.begin(), t.I.begin() + nbase); u2.J.assign(t.J.begin(), t.J.begin() + nbase); u2.V.assign(t.V.begin(), t.V.begin() + nbase);
+            for (int64_t e = 0; e < nb; ++e)
+                if (bar_ok[e])
+                    for (int q = 0; q < 144; ++q) { size_t s = nbase + e * 144 + q; u2.I.push_back(t.I[s]); u2.J.push_back(t.J[s]); u2.V.push_back(t.V[s]); }
+            t = std::move(u2);
+        }
+    }
+    constrain_and_csc(d, t, out->colptr, out->rowval, out->nzval);
+    return 0;
+}
+
+int64_t oracle_nnz(void *h) { return (int64_t)((OracleCSC *)h)->nzval.size(); }
+int64_t oracle_ndof(void *h) { return (int64_t)((OracleCSC *)h)->colptr.size() - 1; }
+const char *oracle_error(void *h) { return ((OracleCSC *)h)->err.c_str(); }
+double oracle_max_elem_stiff(void *h) { return ((OracleCSC *)h)->max_elem_stiff; }
+void oracle_fetch(void *h, int64_t *colptr, int64_t *rowval, double *nzval, double *orig_diag) {
+    auto *o = (OracleCSC *)h;
+    if (colptr) std::memcpy(colptr, o->colptr.data(), sizeof(int64_t) * o->colptr.size());
+    if (rowval) std::memcpy(rowval, o->rowval.data(), sizeof(int64_t) * o->rowval.size());
+    if (nzval) std::memcpy(nzval, o->nzval.data(), sizeof(double) * o->nzval.size());
+    if (orig_diag && !o->orig_diag.empty()) std::memcpy(orig_diag, o->orig_diag.data(), sizeof(double) * o->orig_diag.size());
+}
+void oracle_free(void *h) { delete (OracleCSC *)h; }
+
+// rbe3_map as returned by assemble_stiffness (constraints.jl:319-322), 1-based
+int64_t oracle_constraint_map(const jfg_model_desc *d, int64_t *dep, int64_t *ptr, int64_t *ind, double *coef) {
+    auto mp = rbe2_map(d);
+    int64_t n = 0, t = 0;
+    if (ptr) ptr[0] = 0;
+    for (auto &kv : mp) {
+        if (dep) dep[n] = kv.first + 1;
+        for (auto &p : kv.second) {
+            if (ind) ind[t] = p.first + 1;
+            if (coef) coef[t] = p.second;
+            ++t;
+        }
+        ++n;
+        if (ptr) ptr[n] = t;
+    }
+    return n;
+}
+
+}  // extern "C"

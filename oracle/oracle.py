@@ -1,0 +1,148 @@
+"""ctypes wrapper of the CPU oracle (``liboracle.so``).
+
+TEST INFRASTRUCTURE ONLY: imported by ``tests/``, ``__graft_entry__.smoke()``
+and the CPU-baseline leg of ``bench.py`` as the checker / reference arm.  The
+product library never imports it.  Parity unpinned (see jfem_oracle.cpp).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import scipy.sparse as sp
+
+from jf_2026_05_19_b200.abi import JfgModelDesc, make_desc
+from jf_2026_05_19_b200.decks import ModelArrays
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    if force or not os.path.exists(LIB_PATH) or \
+            os.path.getmtime(LIB_PATH) < os.path.getmtime(os.path.join(HERE, "jfem_oracle.cpp")):
+        subprocess.run(["make", "-C", HERE, "-B" if force else "liboracle.so"], check=True,
+                       stdout=subprocess.DEVNULL)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(LIB_PATH)
+        pd = C.POINTER(C.c_double)
+        pi64 = C.POINTER(C.c_int64)
+        L.oracle_assemble_k.argtypes = [C.POINTER(JfgModelDesc), C.POINTER(C.c_void_p)]
+        L.oracle_assemble_kg.argtypes = [C.POINTER(JfgModelDesc), pd, C.POINTER(C.c_void_p)]
+        L.oracle_nnz.argtypes = [C.c_void_p]; L.oracle_nnz.restype = C.c_int64
+        L.oracle_ndof.argtypes = [C.c_void_p]; L.oracle_ndof.restype = C.c_int64
+        L.oracle_error.argtypes = [C.c_void_p]; L.oracle_error.restype = C.c_char_p
+        L.oracle_max_elem_stiff.argtypes = [C.c_void_p]; L.oracle_max_elem_stiff.restype = C.c_double
+        L.oracle_fetch.argtypes = [C.c_void_p, pi64, pi64, pd, pd]
+        L.oracle_free.argtypes = [C.c_void_p]
+        L.oracle_q4_stiffness_local.argtypes = [pd, pd, C.c_double, pd]
+        L.oracle_t3_stiffness_local.argtypes = [pd, pd, C.c_double, pd]
+        L.oracle_constraint_map.argtypes = [C.POINTER(JfgModelDesc), pi64, pi64, pi64, pd]
+        L.oracle_constraint_map.restype = C.c_int64
+        L.oracle_num_threads.restype = C.c_int
+        L.oracle_set_threads.argtypes = [C.c_int]
+        _lib = L
+    return _lib
+
+
+class OracleError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"oracle status {status}: {msg}")
+        self.status = status
+
+
+def _fetch(h, with_diag):
+    L = lib()
+    nnz = L.oracle_nnz(h); ndof = L.oracle_ndof(h)
+    colptr = np.empty(ndof + 1, np.int64); rowval = np.empty(nnz, np.int64); nzval = np.empty(nnz)
+    diag = np.empty(ndof) if with_diag else None
+    pd = C.POINTER(C.c_double); pi64 = C.POINTER(C.c_int64)
+    L.oracle_fetch(h, colptr.ctypes.data_as(pi64), rowval.ctypes.data_as(pi64), nzval.ctypes.data_as(pd),
+                   diag.ctypes.data_as(pd) if diag is not None else C.cast(None, pd))
+    return colptr, rowval, nzval, diag
+
+
+def assemble_k(m: ModelArrays):
+    """Returns (colptr, rowval, nzval, max_elem_stiff, orig_diag), 1-based CSC."""
+    L = lib()
+    d, keep = make_desc(m)
+    h = C.c_void_p()
+    st = L.oracle_assemble_k(C.byref(d), C.byref(h))
+    try:
+        if st != 0:
+            raise OracleError(st, L.oracle_error(h).decode())
+        colptr, rowval, nzval, diag = _fetch(h, True)
+        return colptr, rowval, nzval, L.oracle_max_elem_stiff(h), diag
+    finally:
+        L.oracle_free(h)
+        del keep
+
+
+def assemble_kg(m: ModelArrays, u: np.ndarray):
+    L = lib()
+    d, keep = make_desc(m)
+    u = np.ascontiguousarray(u, np.float64)
+    h = C.c_void_p()
+    st = L.oracle_assemble_kg(C.byref(d), u.ctypes.data_as(C.POINTER(C.c_double)), C.byref(h))
+    try:
+        if st != 0:
+            raise OracleError(st, L.oracle_error(h).decode())
+        colptr, rowval, nzval, _ = _fetch(h, False)
+        return colptr, rowval, nzval
+    finally:
+        L.oracle_free(h)
+        del keep
+
+
+def constraint_map(m: ModelArrays):
+    L = lib()
+    d, keep = make_desc(m)
+    n = L.oracle_constraint_map(C.byref(d), None, None, None, None)
+    dep = np.empty(n, np.int64); ptr = np.empty(n + 1, np.int64)
+    L.oracle_constraint_map(C.byref(d), dep.ctypes.data_as(C.POINTER(C.c_int64)), ptr.ctypes.data_as(C.POINTER(C.c_int64)), None, None)
+    ind = np.empty(ptr[-1], np.int64); coef = np.empty(ptr[-1])
+    L.oracle_constraint_map(C.byref(d), dep.ctypes.data_as(C.POINTER(C.c_int64)), ptr.ctypes.data_as(C.POINTER(C.c_int64)),
+                            ind.ctypes.data_as(C.POINTER(C.c_int64)), coef.ctypes.data_as(C.POINTER(C.c_double)))
+    del keep
+    return dep, ptr, ind, coef
+
+
+def q4_local(lc: np.ndarray, prop: np.ndarray, k6rot: float = 100.0) -> np.ndarray:
+    L = lib()
+    lc = np.ascontiguousarray(lc, np.float64).reshape(8)
+    prop = np.ascontiguousarray(prop, np.float64).reshape(7)
+    out = np.empty((24, 24))
+    pd = C.POINTER(C.c_double)
+    L.oracle_q4_stiffness_local(lc.ctypes.data_as(pd), prop.ctypes.data_as(pd), k6rot, out.ctypes.data_as(pd))
+    return out
+
+
+def t3_local(lc: np.ndarray, prop: np.ndarray, k6rot: float = 100.0) -> np.ndarray:
+    L = lib()
+    lc = np.ascontiguousarray(lc, np.float64).reshape(6)
+    prop = np.ascontiguousarray(prop, np.float64).reshape(7)
+    out = np.empty((18, 18))
+    pd = C.POINTER(C.c_double)
+    L.oracle_t3_stiffness_local(lc.ctypes.data_as(pd), prop.ctypes.data_as(pd), k6rot, out.ctypes.data_as(pd))
+    return out
+
+
+def to_scipy(colptr, rowval, nzval, ndof):
+    return sp.csc_matrix((nzval, rowval - 1, colptr - 1), shape=(ndof, ndof))
+
+
+def set_threads(n: int):
+    lib().oracle_set_threads(int(n))
+
+
+def num_threads() -> int:
+    return int(lib().oracle_num_threads())
