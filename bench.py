@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""K+KG assembly throughput of the OpenJFEM element hot path on B200.
+
+One step = one stiffness assembly (K, with max_elem_stiff and orig_diag) and
+one geometric-stiffness assembly (KG from a static displacement field) of the
+whole model, i.e. the two calls SOL 105 makes per preload.  The workload is
+the cylindrical barrel: R 2000 mm, L 6000 mm, 1440 x 696 cells with 10% of
+them split into CTRIA3 pairs, I-section CBEAM rings every 500 mm, CBAR
+longerons every 5 degrees and an RBE2 tying the loaded end to a centre node
+(about 1.17M elements, 6.0M dof).  Synthetic, seeded inputs.
+
+value: elements/s with all inputs resident in HBM (device-pointer C ABI).
+e2e:   the same metric through the host-buffer C ABI calls (pinned host
+       u in, K and KG values out, copies inside the timed region).
+
+--impl reference times the CPU restatement of the reference algorithm (the
+reference itself is Julia and cannot run on this image) on a bounded sample.
+
+Multi-GPU (torchrun): every rank assembles its own barrel replica (design
+variants are independent units, no data-path collective); value is the sum
+over ranks divided by the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "K+KG assembly elements/s"
+UNIT = "elements/s"
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=["barrel", "barrel_medium", "barrel_small", "panel", "plate"], default="barrel")
+    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    return p.parse_args()
+
+
+def make_model(workload: str, seed: int):
+    from jf_2026_05_19_b200 import decks
+    if workload == "barrel":
+        return decks.barrel_c4(seed=seed)
+    if workload == "barrel_medium":
+        return decks.barrel_c4(seed=seed, n_circ=720, n_axial=348, ring_every=29, longeron_every=10, name="barrel_720x348")
+    if workload == "barrel_small":
+        return decks.barrel_c4(seed=seed, n_circ=240, n_axial=96, ring_every=8, longeron_every=10, name="barrel_240x96")
+    if workload == "panel":
+        return decks.stiffened_panel_c2(seed=seed, stringer_offset=0.0, name="stiffened_panel_no_offset")
+    return decks.plate_c1()
+
+
+def workload_config(m, workload: str, world: int):
+    c = m.counts()
+    return {"workload": m.name if workload != "barrel" else
+            "barrel R2000 L6000 1440x696 cells, 10% CTRIA3, CBEAM rings, CBAR longerons, RBE2 end",
+            "elements_per_gpu": int(m.n_elements), "quad4": c["quad4"], "tria3": c["tria3"], "bar": c["bar"],
+            "nodes": c["nodes"], "ndof": int(m.ndof), "rbe2_slaves": c["rbe2_slaves"],
+            "replicas": world, "l2": "inputs and outputs larger than L2 (staging and CSR values are GBs)"}
+
+
+def cpu_sample_model(seed: int = 0):
+    """Bounded sample with the barrel's element mix (~50k elements)."""
+    from jf_2026_05_19_b200 import decks
+    return decks.barrel_c4(seed=seed, n_circ=480, n_axial=96, ring_every=8, longeron_every=7, name="barrel_480x96")
+
+
+def time_cpu_oracle(seconds: float, reps_max: int = 50):
+    """Oracle K+KG on the bounded sample; returns (elements/s, threads, sample text)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # CPU restatement: reported baseline only
+    from jf_2026_05_19_b200 import decks
+    m = cpu_sample_model()
+    u = decks.smooth_displacement(m, seed=1)
+    threads = O.num_threads()
+    O.assemble_k(m)  # warm caches / page in
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        O.assemble_k(m)
+        O.assemble_kg(m, u)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or reps >= reps_max:
+            break
+    return m.n_elements * reps / el, threads, f"{m.name}: {m.n_elements} elements, {reps} K+KG passes, {el:.1f} s"
+
+
+class ClockSampler:
+    def __init__(self):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self, device_index: int):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                if int(parts[0]) != device_index:
+                    continue
+                sm.append(float(parts[1])); mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measure_fp64_peak(torch, dev):
+    """Dense FP64 GEMM throughput on this GPU (cuBLAS DGEMM via torch), TFLOP/s."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(3):
+        s = torch.cuda.Event(enable_timing=True); e = torch.cuda.Event(enable_timing=True)
+        s.record(); torch.matmul(a, b); e.record(); e.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2 * n ** 3 / best / 1e12
+
+
+def load_traffic():
+    """Per-launch DRAM traffic of the dominant kernels from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if os.path.exists(path):
+        try:
+            return json.load(open(path))
+        except Exception:
+            return {}
+    return {}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from jf_2026_05_19_b200 import decks
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    m = cpu_sample_model()
+    u = decks.smooth_displacement(m, seed=1)
+    threads = O.num_threads()
+    for _ in range(max(args.warmup, 1)):
+        O.assemble_k(m); O.assemble_kg(m, u)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.assemble_k(m); O.assemble_kg(m, u)
+    el = time.perf_counter() - t0
+    v = m.n_elements * args.steps / el
+    sample = f"{m.name}: {m.n_elements} elements per step, barrel element mix"
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded barrel deck)",
+            "config": workload_config(m, "barrel_sample", 1),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                             "note": "reference is Julia 1.12 (absent here); C++ restatement of its algorithm"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device (the CPU oracle is only the reference arm)")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    from jf_2026_05_19_b200 import decks, native, roofline
+
+    fp64_peak = measure_fp64_peak(torch, dev)
+    m = make_model(args.workload, seed=rank)
+    g = native.GpuModel(m)
+    stream = torch.cuda.current_stream(dev)
+    g.set_stream(stream.cuda_stream)
+    u_host = decks.smooth_displacement(m, seed=1 + rank)
+    u_dev = torch.from_numpy(u_host).to(dev)
+    nz_k = torch.empty(g.nnz, dtype=torch.float64, device=dev)
+    nz_kg = torch.empty(g.nnz, dtype=torch.float64, device=dev)
+    diag = torch.empty(g.ndof, dtype=torch.float64, device=dev)
+    mx = torch.zeros(1, dtype=torch.float64, device=dev)
+
+    def step():
+        g.assemble_k_device(nz_k.data_ptr(), mx.data_ptr(), diag.data_ptr())
+        g.assemble_kg_device(u_dev.data_ptr(), nz_kg.data_ptr())
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    g.timing_accumulated("k", reset=True)
+    g.timing_accumulated("kg", reset=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler()
+    clocks.start()
+    start = torch.cuda.Event(enable_timing=True); end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(args.steps):
+        step()
+    end.record(stream)
+    end.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop(local)
+    elapsed = start.elapsed_time(end) / 1e3
+    if dist:
+        t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    kt, kn = g.timing_accumulated("k", reset=True)
+    gt, gn = g.timing_accumulated("kg", reset=True)
+
+    # end-to-end through the host-buffer C ABI (pinned host memory)
+    e2e_steps = max(1, min(args.e2e_steps, args.steps))
+    u_pin = torch.from_numpy(u_host).pin_memory()
+    nzk_pin = torch.empty(g.nnz, dtype=torch.float64).pin_memory()
+    nzg_pin = torch.empty(g.nnz, dtype=torch.float64).pin_memory()
+    dg_pin = torch.empty(g.ndof, dtype=torch.float64).pin_memory()
+    un, nkn, ngn, dgn = u_pin.numpy(), nzk_pin.numpy(), nzg_pin.numpy(), dg_pin.numpy()
+    g.assemble_k(nkn, want_diag=True); g.assemble_kg(un, ngn)  # warm
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    s2 = torch.cuda.Event(enable_timing=True); e2 = torch.cuda.Event(enable_timing=True)
+    s2.record(stream)
+    for _ in range(e2e_steps):
+        nz, mxv, dgv = g.assemble_k(nkn, want_diag=True)
+        g.assemble_kg(un, ngn)
+    e2.record(stream)
+    e2.synchronize()
+    e2e_el = s2.elapsed_time(e2) / 1e3
+    if dist:
+        t = torch.tensor([e2e_el], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_el = float(t.item())
+
+    n_el = m.n_elements
+    value = world * n_el * args.steps / elapsed
+    e2e_value = world * n_el * e2e_steps / e2e_el
+    counts = m.counts()
+    # dominant kernel over the timed region
+    per_kernel = {
+        "quad4_k": kt["quad4"] / max(kn, 1), "tria3_k": kt["tria3"] / max(kn, 1), "bar_k": kt["bar"] / max(kn, 1),
+        "reduce_k": kt["reduce"] / max(kn, 1), "diag_k": kt["diag"] / max(kn, 1), "expand_k": kt["expand"] / max(kn, 1),
+        "quad4_kg": gt["quad4"] / max(gn, 1), "tria3_kg": gt["tria3"] / max(gn, 1), "bar_kg": gt["bar"] / max(gn, 1),
+        "reduce_kg": gt["reduce"] / max(gn, 1), "expand_kg": gt["expand"] / max(gn, 1),
+    }
+    dominant = max(per_kernel, key=per_kernel.get)
+    traffic = load_traffic()
+    st = g.stats()
+    if dominant.startswith("reduce"):
+        # staging read, segment bounds and both CSC positions per upper nonzero, value writes
+        alg_bytes = 8 * st["n_contrib"] + 20 * st["n_upper"] + 8 * st["nnz"]
+        mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+        peak = json.load(open(mp))["hbm_gbs"] if os.path.exists(mp) else 6650.0
+        roof = {"bound": "hbm", "unit": "GB/s",
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs" if os.path.exists(mp) else "fallback 6.65 TB/s"}
+        achieved = alg_bytes / (per_kernel[dominant] / 1e3) / 1e9
+    else:
+        etype = dominant.split("_")[0]
+        alg = roofline.kernel_flops(dominant, counts[etype])
+        achieved = alg / (per_kernel[dominant] / 1e3) / 1e12
+        peak = fp64_peak
+        roof = {"bound": "tensor", "unit": "TFLOP/s",
+                "peak_source": "FP64 DGEMM (torch.matmul float64 8192^3, best of 3) measured in this run"}
+    roof.update({"kernel": dominant, "achieved": achieved, "peak": peak, "frac": achieved / peak,
+                 "traffic": traffic.get(dominant), "launch_ms": per_kernel[dominant]})
+    ms_step = elapsed / args.steps * 1e3
+    h2d = 8 * m.ndof
+    d2h = 8 * g.nnz * 2 + 8 * m.ndof + 8
+    launches_per_step = (sum(1 for t in ("quad4", "tria3", "bar") if counts[t] > 0) * 2
+                         + 2 * (1 if st["n_exc"] else 0) + 2 + 1)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded deck generator; smooth seeded displacement for KG)",
+            "config": dict(workload_config(m, args.workload, world), parallelism=f"replicas x{world}", nnz=g.nnz),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": e2e_steps},
+            "roofline": roof, "gpu_launches": launches_per_step * args.steps, "clocks": clk,
+            "kernel_ms": per_kernel, "fp64_dgemm_tflops": fp64_peak, "model_stats": st,
+            "whole_step_roofline": {"flops": roofline.flops_per_step(counts), "bytes": roofline.bytes_per_step(counts, g.nnz)}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, thr, sample = time_cpu_oracle(args.cpu_seconds)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    g.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

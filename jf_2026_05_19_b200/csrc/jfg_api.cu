@@ -85,8 +85,17 @@ struct jfg_model {
     // constraint map (host, 0-based dofs)
     std::vector<int64_t> dep_dof, dep_ptr, dep_ind;
     std::vector<double> dep_coef;
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // ring of event sets, one per assembly call, so that per-kernel device
+    // times can be accumulated over many back-to-back calls without a sync
+    struct EvSet { cudaEvent_t e[7]; int kind; bool pending; };
+    static constexpr int kRing = 64;
+    EvSet ring[kRing];
+    int ring_head = 0, last_set = -1;
+    cudaEvent_t *ev = nullptr;
     float last_elem_ms = 0.f, last_reduce_ms = 0.f, last_total_ms = 0.f;
+    float last_kernel_ms[6] = {0, 0, 0, 0, 0, 0};  // quad4, tria3, bar, expand, reduce, diag
+    double acc_ms[2][6] = {{0, 0, 0, 0, 0, 0}, {0, 0, 0, 0, 0, 0}};
+    int64_t acc_calls[2] = {0, 0};
     std::vector<void *> allocs;
 };
 
@@ -433,8 +442,9 @@ void jfg_model_destroy(jfg_model *m) {
     if (!m) return;
     if (m->stream) cudaStreamSynchronize(m->stream);
     for (void *p : m->allocs) cudaFree(p);
-    for (auto &e : m->ev)
-        if (e) cudaEventDestroy(e);
+    for (auto &set : m->ring)
+        for (auto &e : set.e)
+            if (e) cudaEventDestroy(e);
     if (m->own_stream && m->own) {
         cudaStreamSynchronize(m->own);
         cudaStreamDestroy(m->own);
@@ -453,7 +463,11 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
     CK(cudaStreamCreateWithFlags(&m->own, cudaStreamNonBlocking));
     m->stream = m->own;
     m->own_stream = true;
-    for (auto &e : m->ev) CK(cudaEventCreate(&e));
+    for (auto &set : m->ring) {
+        for (auto &e : set.e) CK(cudaEventCreate(&e));
+        set.pending = false;
+        set.kind = 0;
+    }
     m->n_nodes = d->n_nodes;
     m->ndof = 6 * d->n_nodes;
     m->nq = d->n_quad4;
@@ -821,14 +835,18 @@ jfg_status jfg_pattern_fill(jfg_model *m, int64_t *colptr, int64_t *rowval) {
 
 namespace {
 
+jfg_status begin_set(jfg_model *m, int kind);
+
 jfg_status launch_k(jfg_model *m, double *nz, double *dmax, double *ddiag) {
-    CK(cudaEventRecord(m->ev[0], m->stream));
+    jfg_status bst = begin_set(m, 0);
+    if (bst) return bst;
     ElemOut o;
     o.staging = m->d_staging;
     o.exc_raw = m->d_exc_raw;
     o.diag_staging = ddiag ? m->d_dstaging : nullptr;
     o.maxabs = dmax;
     if (dmax) CK(cudaMemsetAsync(dmax, 0, sizeof(double), m->stream));
+    CK(cudaEventRecord(m->ev[0], m->stream));
     if (m->nq) {
         o.slot = m->d_slot + m->slot_q4;
         o.diag_slot = m->d_dslot + m->dslot_q4;
@@ -836,6 +854,7 @@ jfg_status launch_k(jfg_model *m, double *nz, double *dmax, double *ddiag) {
             m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, m->k6rot, o);
         CK(cudaGetLastError());
     }
+    CK(cudaEventRecord(m->ev[1], m->stream));
     if (m->nt) {
         o.slot = m->d_slot + m->slot_t3;
         o.diag_slot = m->d_dslot + m->dslot_t3;
@@ -843,26 +862,29 @@ jfg_status launch_k(jfg_model *m, double *nz, double *dmax, double *ddiag) {
                                                                                    m->d_nodeR, m->k6rot, o);
         CK(cudaGetLastError());
     }
+    CK(cudaEventRecord(m->ev[2], m->stream));
     if (m->nb) {
         o.slot = m->d_slot + m->slot_bar;
         o.diag_slot = m->d_dslot + m->dslot_bar;
         bar_k_kernel<<<(unsigned)cdiv(m->nb, 128), 128, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, o);
         CK(cudaGetLastError());
     }
+    CK(cudaEventRecord(m->ev[3], m->stream));
     if (m->n_exc) {
         expand_kernel<<<(unsigned)cdiv(m->n_exc, 256), 256, 0, m->stream>>>(m->n_exc, m->d_exc_q, m->d_exc_src, m->d_exc_w,
                                                                            m->d_exc_raw, m->d_staging);
         CK(cudaGetLastError());
     }
-    CK(cudaEventRecord(m->ev[1], m->stream));
+    CK(cudaEventRecord(m->ev[4], m->stream));
     if (m->n_upper)
         reduce_kernel<<<(unsigned)cdiv(m->n_upper, 256), 256, 0, m->stream>>>(m->n_upper, m->d_seg, m->d_staging, m->d_posA,
                                                                              m->d_posB, nz);
     CK(cudaGetLastError());
+    CK(cudaEventRecord(m->ev[5], m->stream));
     if (ddiag)
         diag_reduce_kernel<<<(unsigned)cdiv(m->ndof, 256), 256, 0, m->stream>>>(m->ndof, m->d_dseg, m->d_dstaging, ddiag);
     CK(cudaGetLastError());
-    CK(cudaEventRecord(m->ev[2], m->stream));
+    CK(cudaEventRecord(m->ev[6], m->stream));
     return JFG_OK;
 }
 
@@ -870,48 +892,88 @@ jfg_status launch_kg(jfg_model *m, const double *du, double *nz) {
     if (m->bar_offsets)
         return fail(m, JFG_ERR_REFERENCE_RAISES,
                     "assemble_geometric_stiffness raises BoundsError for CBAR/CBEAM with offsets (assembly.jl:6326)");
-    CK(cudaEventRecord(m->ev[0], m->stream));
+    jfg_status bst = begin_set(m, 1);
+    if (bst) return bst;
     ElemOut o;
     o.staging = m->d_staging;
     o.exc_raw = m->d_exc_raw;
     o.diag_staging = nullptr;
     o.diag_slot = nullptr;
     o.maxabs = nullptr;
+    CK(cudaEventRecord(m->ev[0], m->stream));
     if (m->nq) {
         o.slot = m->d_slot + m->slot_q4;
         q4_kg_kernel<<<(unsigned)cdiv(m->nq, Q4_ELEMS_PER_BLOCK), Q4_THREADS, 0, m->stream>>>(
             m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, du, o);
         CK(cudaGetLastError());
     }
+    CK(cudaEventRecord(m->ev[1], m->stream));
     if (m->nt) {
         o.slot = m->d_slot + m->slot_t3;
         t3_kg_kernel<<<(unsigned)cdiv(m->nt, 128), 128, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords, m->d_nodeR, du, o);
         CK(cudaGetLastError());
     }
+    CK(cudaEventRecord(m->ev[2], m->stream));
     if (m->nb) {
         o.slot = m->d_slot + m->slot_bar;
         bar_kg_kernel<<<(unsigned)cdiv(m->nb, 128), 128, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, du, o);
         CK(cudaGetLastError());
     }
+    CK(cudaEventRecord(m->ev[3], m->stream));
     if (m->n_exc) {
         expand_kernel<<<(unsigned)cdiv(m->n_exc, 256), 256, 0, m->stream>>>(m->n_exc, m->d_exc_q, m->d_exc_src, m->d_exc_w,
                                                                            m->d_exc_raw, m->d_staging);
         CK(cudaGetLastError());
     }
-    CK(cudaEventRecord(m->ev[1], m->stream));
+    CK(cudaEventRecord(m->ev[4], m->stream));
     if (m->n_upper)
         reduce_kernel<<<(unsigned)cdiv(m->n_upper, 256), 256, 0, m->stream>>>(m->n_upper, m->d_seg, m->d_staging, m->d_posA,
                                                                              m->d_posB, nz);
     CK(cudaGetLastError());
-    CK(cudaEventRecord(m->ev[2], m->stream));
+    CK(cudaEventRecord(m->ev[5], m->stream));
+    CK(cudaEventRecord(m->ev[6], m->stream));
+    return JFG_OK;
+}
+
+// Complete one event set: per-kernel times into the accumulators and "last".
+jfg_status finish_set(jfg_model *m, int idx) {
+    auto &set = m->ring[idx];
+    if (!set.pending) return JFG_OK;
+    CK(cudaEventSynchronize(set.e[6]));
+    float k[6];
+    for (int i = 0; i < 6; ++i) {
+        CK(cudaEventElapsedTime(&k[i], set.e[i], set.e[i + 1]));
+        m->acc_ms[set.kind][i] += k[i];
+    }
+    m->acc_calls[set.kind] += 1;
+    if (idx == m->last_set) {
+        for (int i = 0; i < 6; ++i) m->last_kernel_ms[i] = k[i];
+        CK(cudaEventElapsedTime(&m->last_elem_ms, set.e[0], set.e[4]));
+        CK(cudaEventElapsedTime(&m->last_reduce_ms, set.e[4], set.e[6]));
+        CK(cudaEventElapsedTime(&m->last_total_ms, set.e[0], set.e[6]));
+    }
+    set.pending = false;
     return JFG_OK;
 }
 
 jfg_status finish_timing(jfg_model *m) {
-    CK(cudaEventSynchronize(m->ev[2]));
-    CK(cudaEventElapsedTime(&m->last_elem_ms, m->ev[0], m->ev[1]));
-    CK(cudaEventElapsedTime(&m->last_reduce_ms, m->ev[1], m->ev[2]));
-    m->last_total_ms = m->last_elem_ms + m->last_reduce_ms;
+    for (int i = 0; i < jfg_model::kRing; ++i) {
+        jfg_status st = finish_set(m, i);
+        if (st) return st;
+    }
+    return JFG_OK;
+}
+
+// Select the next event set for an assembly call of the given kind.
+jfg_status begin_set(jfg_model *m, int kind) {
+    int idx = m->ring_head;
+    jfg_status st = finish_set(m, idx);  // waits only if 64 calls are still in flight
+    if (st) return st;
+    m->ring_head = (idx + 1) % jfg_model::kRing;
+    m->ring[idx].kind = kind;
+    m->ring[idx].pending = true;
+    m->last_set = idx;
+    m->ev = m->ring[idx].e;
     return JFG_OK;
 }
 
@@ -992,6 +1054,43 @@ jfg_status jfg_constraint_map(jfg_model *m, int64_t *n_dep, int64_t *n_terms, in
         if (ind_dof) ind_dof[i] = m->dep_ind[i] + 1;
         if (coeff) coeff[i] = m->dep_coef[i];
     }
+    return JFG_OK;
+}
+
+jfg_status jfg_timing_accumulated(jfg_model *m, int kind, double *ms6_sum, int64_t *n_calls, int reset) {
+    if (!m || kind < 0 || kind > 1) return JFG_ERR_INVALID;
+    jfg_status st = finish_timing(m);
+    if (st) return st;
+    if (ms6_sum)
+        for (int k = 0; k < 6; ++k) ms6_sum[k] = m->acc_ms[kind][k];
+    if (n_calls) *n_calls = m->acc_calls[kind];
+    if (reset) {
+        for (int k = 0; k < 6; ++k) m->acc_ms[kind][k] = 0.0;
+        m->acc_calls[kind] = 0;
+    }
+    return JFG_OK;
+}
+
+jfg_status jfg_kernel_timing(jfg_model *m, double *ms6) {
+    if (!m) return JFG_ERR_INVALID;
+    jfg_status st = finish_timing(m);
+    if (st) return st;
+    for (int k = 0; k < 6; ++k) ms6[k] = m->last_kernel_ms[k];
+    return JFG_OK;
+}
+
+jfg_status jfg_model_stats(jfg_model *m, int64_t *out8) {
+    if (!m || !out8) return JFG_ERR_INVALID;
+    out8[0] = m->n_contrib;               // staging values per assembly
+    out8[1] = m->n_upper;                 // unique upper-triangle nonzeros
+    out8[2] = m->nnz;                     // CSC nonzeros
+    out8[3] = m->n_exc;                   // constraint-expanded contributions
+    out8[4] = m->n_exc_raw;               // raw values of constraint-touching elements
+    out8[5] = m->n_slots;                 // packed element entries (scatter-map length)
+    out8[6] = m->n_dcontrib;              // element diagonal entries (orig_diag map)
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    out8[7] = (int64_t)(total_b - free_b);  // device bytes in use on this GPU
     return JFG_OK;
 }
 

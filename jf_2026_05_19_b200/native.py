@@ -21,7 +21,7 @@ LIB_PATH = os.path.join(PKG, "libjfemgpu.so")
 # every entry point declared in include/jfem_gpu.h
 EXPORTS = ("jfg_model_create", "jfg_pattern", "jfg_pattern_fill", "jfg_assemble_k", "jfg_assemble_kg",
            "jfg_assemble_k_device", "jfg_assemble_kg_device", "jfg_update_properties", "jfg_constraint_map",
-           "jfg_set_stream", "jfg_last_timing", "jfg_model_destroy", "jfg_last_error", "jfg_version")
+           "jfg_set_stream", "jfg_last_timing", "jfg_kernel_timing", "jfg_timing_accumulated", "jfg_model_stats", "jfg_model_destroy", "jfg_last_error", "jfg_version")
 
 _lib = None
 
@@ -62,6 +62,9 @@ def load(path: str = LIB_PATH):
     L.jfg_constraint_map.argtypes = [C.c_void_p, _pi64, _pi64, _pi64, _pi64, _pi64, _pd]
     L.jfg_set_stream.argtypes = [C.c_void_p, C.c_void_p]
     L.jfg_last_timing.argtypes = [C.c_void_p, _pd, _pd, _pd]
+    L.jfg_kernel_timing.argtypes = [C.c_void_p, _pd]
+    L.jfg_model_stats.argtypes = [C.c_void_p, _pi64]
+    L.jfg_timing_accumulated.argtypes = [C.c_void_p, C.c_int, _pd, _pi64, C.c_int]
     L.jfg_model_destroy.argtypes = [C.c_void_p]
     L.jfg_model_destroy.restype = None
     L.jfg_last_error.argtypes = [C.c_void_p]
@@ -69,7 +72,7 @@ def load(path: str = LIB_PATH):
     L.jfg_version.restype = C.c_char_p
     for name in ("jfg_pattern", "jfg_pattern_fill", "jfg_assemble_k", "jfg_assemble_kg", "jfg_assemble_k_device",
                  "jfg_assemble_kg_device", "jfg_update_properties", "jfg_constraint_map", "jfg_set_stream",
-                 "jfg_last_timing"):
+                 "jfg_last_timing", "jfg_kernel_timing", "jfg_timing_accumulated", "jfg_model_stats"):
         getattr(L, name).restype = C.c_int32
     _lib = L
     return L
@@ -167,6 +170,23 @@ class GpuModel:
         a = C.c_double(); b = C.c_double(); c = C.c_double()
         self._check(self.L.jfg_last_timing(self.h, C.byref(a), C.byref(b), C.byref(c)))
         return a.value, b.value, c.value
+
+    def kernel_timing(self) -> dict:
+        ms = np.zeros(6)
+        self._check(self.L.jfg_kernel_timing(self.h, _ptr(ms, _pd)))
+        return dict(zip(("quad4", "tria3", "bar", "expand", "reduce", "diag"), ms.tolist()))
+
+    def timing_accumulated(self, kind: str, reset: bool = True):
+        """Summed per-kernel ms and call count of 'k' or 'kg' assemblies."""
+        ms = np.zeros(6); n = C.c_int64()
+        self._check(self.L.jfg_timing_accumulated(self.h, 0 if kind == "k" else 1, _ptr(ms, _pd), C.byref(n), int(reset)))
+        return dict(zip(("quad4", "tria3", "bar", "expand", "reduce", "diag"), ms.tolist())), int(n.value)
+
+    def stats(self) -> dict:
+        out = np.zeros(8, np.int64)
+        self._check(self.L.jfg_model_stats(self.h, _ptr(out, _pi64)))
+        keys = ("n_contrib", "n_upper", "nnz", "n_exc", "n_exc_raw", "n_slots", "n_diag", "device_bytes_in_use")
+        return dict(zip(keys, (int(x) for x in out)))
 
     def constraint_map(self):
         nd = C.c_int64(); nt = C.c_int64()
