@@ -142,9 +142,9 @@ jfg_status jfg_set_stream(jfg_model *m, void *stream);
  * kernels and the segmented reduction), milliseconds. */
 jfg_status jfg_last_timing(jfg_model *m, double *element_ms, double *reduce_ms, double *total_ms);
 
-/* Per-kernel device times of the last assembly, milliseconds, in the order
- * quad4 elements, tria3 elements, bar elements, constraint expansion,
- * segmented reduction, orig_diag reduction (6 doubles). */
+/* Per-kernel device times of the last assembly, milliseconds, 6 doubles in
+ * the order: quad4 elements, tria3 elements, bar elements, dof-level
+ * (RBE2-expanded) reduction, node-pair block reduction, orig_diag reduction. */
 jfg_status jfg_kernel_timing(jfg_model *m, double *ms6);
 
 /* Per-kernel device times summed over all K (kind 0) or KG (kind 1)
@@ -152,9 +152,10 @@ jfg_status jfg_kernel_timing(jfg_model *m, double *ms6);
  * clears the sums after reading.  Waits for the recorded calls. */
 jfg_status jfg_timing_accumulated(jfg_model *m, int kind, double *ms6_sum, int64_t *n_calls, int reset);
 
-/* Sizes of the resident data: out8 = {staging values, upper nonzeros, CSC
- * nonzeros, constraint-expanded contributions, raw constraint-element values,
- * scatter-map entries, orig_diag entries, device bytes in use}. */
+/* Sizes of the resident data: out8 = {staging values, global node-pair
+ * blocks, CSC nonzeros, constraint-expanded contributions, raw values of
+ * constraint-touching pairs, element node pairs (scatter-map length),
+ * orig_diag entries, device bytes in use}. */
 jfg_status jfg_model_stats(jfg_model *m, int64_t *out8);
 
 void jfg_model_destroy(jfg_model *m);

@@ -12,7 +12,6 @@
 
 namespace jfg {
 
-constexpr int BAR_PACKED = 78;
 
 struct BarFrame {
     double L;
@@ -133,17 +132,22 @@ __device__ __forceinline__ void bar_write(const ElemOut &o, int64_t e, const Bar
             for (int l = 0; l < 12; ++l) s += k[i][l] * bar_T(F, l, j);
             KT[i][j] = s;
         }
-    const int32_t *sl = o.slot + e * BAR_PACKED;
+    double G[12][12];
     for (int i = 0; i < 12; ++i)
-        for (int j = i; j < 12; ++j) {
+        for (int j = 0; j < 12; ++j) {
             double s = 0.0;
             for (int l = 0; l < 12; ++l) s += bar_T(F, l, i) * KT[l][j];
+            G[i][j] = s;
             lmax = fmax(lmax, fabs(s));
-            int32_t sidx = __ldg(sl + packed_index(i, j, 12));
-            if (sidx >= 0) o.staging[sidx] = s;
-            else o.exc_raw[-(int64_t)sidx - 1] = s;
-            if (o.diag_staging && i == j) o.diag_staging[__ldg(o.diag_slot + e * 12 + i)] = s;
         }
+    const int pa[3] = {0, 0, 1}, pb[3] = {0, 1, 1};
+    for (int p = 0; p < 3; ++p) {
+        const int32_t s = __ldg(o.blk_slot + e * 3 + p);
+        for (int i = 0; i < 6; ++i)
+            for (int j = 0; j < 6; ++j) *blk_entry(o, s, i, j) = G[6 * pa[p] + i][6 * pb[p] + j];
+    }
+    if (o.diag_staging)
+        for (int i = 0; i < 12; ++i) o.diag_staging[__ldg(o.diag_slot + e * 12 + i)] = G[i][i];
 }
 
 __global__ void __launch_bounds__(128) bar_k_kernel(int64_t nb, const int32_t *__restrict__ nodes,

@@ -40,14 +40,32 @@ constexpr int Q4_PACKED = 300;
 __constant__ int c_pair_a[10] = {0, 0, 0, 0, 1, 1, 1, 2, 2, 3};
 __constant__ int c_pair_b[10] = {0, 1, 2, 3, 1, 2, 3, 2, 3, 3};
 
+// Output of an element kernel.  Every element node pair (a <= b) owns one
+// 36-double block: rows = dofs of local node a, columns = dofs of node b.
+//   blk_slot >= 0: block index in `staging` (bits 0..29) with bit 30 set when
+//                  the global node order is reversed (the block is stored
+//                  transposed so that it reads as rows of the lower-numbered
+//                  node);
+//   blk_slot <  0: the pair touches an RBE2 node; the raw block goes to
+//                  exc_raw[36 * (-slot - 1)] for the dof-level expansion.
 struct ElemOut {
-    double *staging;          // values at sorted contribution slots
-    double *exc_raw;          // raw packed values of elements touching constrained dofs
-    const int32_t *slot;      // per element packed entry: >=0 staging slot, <0 -> exc_raw[-s-1]
-    double *diag_staging;     // K only: raw element diagonal at sorted dof slots (or null)
-    const int32_t *diag_slot; // per element local dof (or null)
-    double *maxabs;           // K only: max |value| (bit-pattern atomic), or null
+    double *staging;           // 36 doubles per sorted block slot
+    double *exc_raw;           // 36 doubles per constraint-touching pair
+    const int32_t *blk_slot;   // per element node pair
+    double *diag_staging;      // K only: raw element diagonal at sorted dof slots (or null)
+    const int32_t *diag_slot;  // per element local dof (or null)
+    double *maxabs;            // K only: max |value| (bit-pattern atomic), or null
 };
+
+constexpr int32_t kBlkTranspose = 1 << 30;
+constexpr int32_t kBlkIndexMask = kBlkTranspose - 1;
+
+// Address of entry (i, j) of a pair block given its slot.
+__device__ __forceinline__ double *blk_entry(const ElemOut &o, int32_t s, int i, int j) {
+    if (s < 0) return o.exc_raw + 36 * (int64_t)(-(s + 1)) + 6 * i + j;
+    double *base = o.staging + 36 * (int64_t)(s & kBlkIndexMask);
+    return (s & kBlkTranspose) ? base + 6 * j + i : base + 6 * i + j;
+}
 
 struct Q4Geo {
     double p[4][3];
@@ -199,27 +217,24 @@ __device__ __forceinline__ void rot_block(const double *Qa, const double L[3][3]
         for (int j = 0; j < 3; ++j) out[i][j] = Qa[i] * W[0][j] + Qa[3 + i] * W[1][j] + Qa[6 + i] * W[2][j];
 }
 
-// Write one global 6x6 node-pair block (a <= b) of an element with n local
-// nodes: all 36 entries for a < b, the upper triangle for a == b.
-template <int NN>
-__device__ __forceinline__ void write_pair_block(const ElemOut &o, int64_t e, int a, int b, const double Gb[6][6],
+// Write one global 6x6 node-pair block (a <= b, pair index p) of element e
+// with NP node pairs; diagonal entries of diagonal pairs also go to the
+// orig_diag staging (K only).
+template <int NN, int NP>
+__device__ __forceinline__ void write_pair_block(const ElemOut &o, int64_t e, int p, int a, int b, const double Gb[6][6],
                                                  double &lmax) {
-    constexpr int N = 6 * NN;
-    constexpr int P = N * (N + 1) / 2;
-    const int32_t *sl = o.slot + e * P;
+    const int32_t s = __ldg(o.blk_slot + e * NP + p);
 #pragma unroll
-    for (int i = 0; i < 6; ++i) {
+    for (int i = 0; i < 6; ++i)
 #pragma unroll
         for (int j = 0; j < 6; ++j) {
-            if (a == b && j < i) continue;
-            int p = packed_index(6 * a + i, 6 * b + j, N);
-            int32_t s = __ldg(sl + p);
             double v = Gb[i][j];
             lmax = fmax(lmax, fabs(v));
-            if (s >= 0) o.staging[s] = v;
-            else o.exc_raw[-(int64_t)s - 1] = v;
-            if (o.diag_staging && a == b && i == j) o.diag_staging[__ldg(o.diag_slot + e * N + 6 * a + i)] = v;
+            *blk_entry(o, s, i, j) = v;
         }
+    if (o.diag_staging && a == b) {
+#pragma unroll
+        for (int i = 0; i < 6; ++i) o.diag_staging[__ldg(o.diag_slot + e * 6 * NN + 6 * a + i)] = Gb[i][i];
     }
 }
 
@@ -487,7 +502,7 @@ __global__ void __launch_bounds__(Q4_THREADS) q4_k_kernel(int64_t nq, const int3
 #pragma unroll
                     for (int j = 0; j < 3; ++j) Gb[3 * bi + i][3 * bj + j] = O[i][j];
             }
-        write_pair_block<4>(o, e, a, b, Gb, lmax);
+        write_pair_block<4, 10>(o, e, tl, a, b, Gb, lmax);
     }
     if (o.maxabs) {
         for (int off = 16; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
@@ -643,7 +658,7 @@ __global__ void __launch_bounds__(Q4_THREADS) q4_kg_kernel(int64_t nq, const int
 #pragma unroll
             for (int j = 0; j < 6; ++j) Gb[i][j] = (i < 3 && j < 3) ? O[i][j] : 0.0;
         double lmax = 0.0;
-        write_pair_block<4>(o, e, a, b, Gb, lmax);
+        write_pair_block<4, 10>(o, e, tl, a, b, Gb, lmax);
     }
 }
 

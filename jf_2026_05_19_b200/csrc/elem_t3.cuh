@@ -19,7 +19,6 @@ namespace jfg {
 
 constexpr int T3_WARPS = 4;
 constexpr int T3_THREADS = 32 * T3_WARPS;
-constexpr int T3_PACKED = 171;
 
 __constant__ int c_t3_quads[3][4] = {{0, 3, 6, 5}, {1, 4, 6, 3}, {2, 5, 6, 4}};
 
@@ -300,42 +299,36 @@ __global__ void __launch_bounds__(T3_THREADS) t3_k_kernel(int64_t nt, const int3
         const int pr_a[6] = {0, 0, 0, 1, 1, 2}, pr_b[6] = {0, 1, 2, 1, 2, 2};
         const int pair = lane >> 2, sub = lane & 3;
         const int a = pr_a[pair], b = pr_b[pair];
-        const bool skip = (a == b && sub == 2);  // lower block of a diagonal pair
-        if (!skip) {
-            const int bi = sub >> 1, bj = sub & 1;
-            double L[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-            if (!degenerate) {
-                const double A = S.A;
-                // membrane CST (u, v) and drill (u, v, theta_z) terms
-                double Bd_a[6] = {0.5 * S.cv[a], -0.5 * S.bv[a], 0, 0, 0, 1.0 / 3.0};
-                double Bd_b[6] = {0.5 * S.cv[b], -0.5 * S.bv[b], 0, 0, 0, 1.0 / 3.0};
-                double ma[2][3] = {{S.bv[a], 0.0, S.cv[a]}, {0.0, S.cv[a], S.bv[a]}};
-                double mb[2][3] = {{S.bv[b], 0.0, S.cv[b]}, {0.0, S.cv[b], S.bv[b]}};
-                for (int i = 0; i < 3; ++i)
-                    for (int j = 0; j < 3; ++j) {
-                        int gi = 3 * bi + i, gj = 3 * bj + j;  // local dof index 0..5
-                        double v = S.alpha_d * (Bd_a[gi] * Bd_b[gj]) * A;
-                        if (gi < 2 && gj < 2) v += quad_form(ma[gi], S.Cm, mb[gj]) * A;
-                        // plate (w, theta_x, theta_y) = local 2, 3, 4
-                        if (S.plate && gi >= 2 && gi <= 4 && gj >= 2 && gj <= 4) v += S.K[3 * a + gi - 2][3 * b + gj - 2];
-                        L[i][j] = v;
-                    }
-            }
-            double O[3][3];
-            rot_block(S.Q[a], L, S.Q[b], O);
-            const int32_t *sl = o.slot + e * T3_PACKED;
+        const int bi = sub >> 1, bj = sub & 1;
+        double L[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        if (!degenerate) {
+            const double A = S.A;
+            // membrane CST (u, v) and drill (u, v, theta_z) terms
+            double Bd_a[6] = {0.5 * S.cv[a], -0.5 * S.bv[a], 0, 0, 0, 1.0 / 3.0};
+            double Bd_b[6] = {0.5 * S.cv[b], -0.5 * S.bv[b], 0, 0, 0, 1.0 / 3.0};
+            double ma[2][3] = {{S.bv[a], 0.0, S.cv[a]}, {0.0, S.cv[a], S.bv[a]}};
+            double mb[2][3] = {{S.bv[b], 0.0, S.cv[b]}, {0.0, S.cv[b], S.bv[b]}};
             for (int i = 0; i < 3; ++i)
                 for (int j = 0; j < 3; ++j) {
-                    int gi = 6 * a + 3 * bi + i, gj = 6 * b + 3 * bj + j;
-                    if (gi > gj) continue;
-                    int32_t s = __ldg(sl + packed_index(gi, gj, 18));
-                    double v = O[i][j];
-                    lmax = fmax(lmax, fabs(v));
-                    if (s >= 0) o.staging[s] = v;
-                    else o.exc_raw[-(int64_t)s - 1] = v;
-                    if (o.diag_staging && gi == gj) o.diag_staging[__ldg(o.diag_slot + e * 18 + gi)] = v;
+                    int gi = 3 * bi + i, gj = 3 * bj + j;  // local dof index 0..5
+                    double v = S.alpha_d * (Bd_a[gi] * Bd_b[gj]) * A;
+                    if (gi < 2 && gj < 2) v += quad_form(ma[gi], S.Cm, mb[gj]) * A;
+                    // plate (w, theta_x, theta_y) = local 2, 3, 4
+                    if (S.plate && gi >= 2 && gi <= 4 && gj >= 2 && gj <= 4) v += S.K[3 * a + gi - 2][3 * b + gj - 2];
+                    L[i][j] = v;
                 }
         }
+        double O[3][3];
+        rot_block(S.Q[a], L, S.Q[b], O);
+        const int32_t s = __ldg(o.blk_slot + e * 6 + pair);
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double v = O[i][j];
+                lmax = fmax(lmax, fabs(v));
+                *blk_entry(o, s, 3 * bi + i, 3 * bj + j) = v;
+                if (o.diag_staging && a == b && bi == bj && i == j)
+                    o.diag_staging[__ldg(o.diag_slot + e * 18 + 6 * a + 3 * bi + i)] = v;
+            }
     }
     if (o.maxabs) {
         for (int off = 16; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
@@ -400,20 +393,15 @@ __global__ void __launch_bounds__(128) t3_kg_kernel(int64_t nt, const int32_t *_
             for (int j = 0; j < 3; ++j)
                 val[i][j] = h * A * (sxx * b[i] * b[j] + syy * cv[i] * cv[j] + sxy * (b[i] * cv[j] + cv[i] * b[j]));
     }
-    const int32_t *sl = o.slot + e * T3_PACKED;
+    int pair = 0;
     for (int a = 0; a < 3; ++a)
-        for (int bb = a; bb < 3; ++bb) {
+        for (int bb = a; bb < 3; ++bb, ++pair) {
             double L[3][3] = {{val[a][bb], 0, 0}, {0, val[a][bb], 0}, {0, 0, val[a][bb]}};
             double O[3][3];
             rot_block(Q[a], L, Q[bb], O);
+            const int32_t s = __ldg(o.blk_slot + e * 6 + pair);
             for (int i = 0; i < 6; ++i)
-                for (int j = 0; j < 6; ++j) {
-                    if (a == bb && j < i) continue;
-                    double v = (i < 3 && j < 3) ? O[i][j] : 0.0;
-                    int32_t s = __ldg(sl + packed_index(6 * a + i, 6 * bb + j, 18));
-                    if (s >= 0) o.staging[s] = v;
-                    else o.exc_raw[-(int64_t)s - 1] = v;
-                }
+                for (int j = 0; j < 6; ++j) *blk_entry(o, s, i, j) = (i < 3 && j < 3) ? O[i][j] : 0.0;
         }
 }
 

@@ -62,18 +62,20 @@ struct jfg_model {
     double *d_coords = nullptr, *d_nodeR = nullptr;
     int32_t *d_q4n = nullptr, *d_t3n = nullptr, *d_barn = nullptr;
     double *d_q4p = nullptr, *d_t3p = nullptr, *d_barp = nullptr;
-    // scatter map
-    int32_t *d_slot = nullptr;          // packed slots, all types concatenated
-    int64_t slot_q4 = 0, slot_t3 = 0, slot_bar = 0, n_slots = 0;
-    int64_t n_contrib = 0, n_upper = 0, nnz = 0;
-    double *d_staging = nullptr;
-    double *d_exc_raw = nullptr;
-    int64_t n_exc_raw = 0, n_exc = 0;
-    int32_t *d_exc_q = nullptr, *d_exc_src = nullptr;
-    double *d_exc_w = nullptr;
-    int32_t *d_seg = nullptr;           // n_upper + 1 contribution segment bounds
-    int64_t *d_posA = nullptr, *d_posB = nullptr;
+    // node-pair block scatter map
+    int64_t pair_q4 = 0, pair_t3 = 0, pair_bar = 0, n_pairs = 0;  // element pair index bases
+    int32_t *d_blk_slot = nullptr;      // per element pair: block slot | transpose, or -(exception + 1)
+    int64_t n_blk = 0, n_blk_contrib = 0, n_upper = 0, nnz = 0;
+    int32_t *d_blk_seg = nullptr;       // n_blk + 1 segment bounds (in blocks)
+    int32_t *d_blk_A = nullptr, *d_blk_B = nullptr, *d_blk_offAB = nullptr, *d_blk_offBA = nullptr;
+    double *d_staging = nullptr;        // 36 doubles per regular element pair
     int64_t *d_rowptr = nullptr, *d_colind = nullptr;   // 0-based symmetric CSR == CSC
+    // dof-level path for pairs that touch RBE2 nodes
+    int64_t n_xpair = 0, n_xkey = 0, n_xcontrib = 0;
+    double *d_exc_raw = nullptr;        // 36 doubles per exception pair
+    int64_t *d_x_pos = nullptr;         // CSC position per unique (row, col)
+    int32_t *d_x_seg = nullptr, *d_x_src = nullptr;
+    double *d_x_w = nullptr;
     // orig_diag map
     int32_t *d_dslot = nullptr;
     int64_t dslot_q4 = 0, dslot_t3 = 0, dslot_bar = 0;
@@ -259,11 +261,6 @@ __global__ void inv_kernel(int64_t n, const int32_t *__restrict__ vals, int32_t 
     inv[vals[q]] = (int32_t)q;
 }
 
-__global__ void regular_slot_kernel(int64_t n_slots, const int32_t *__restrict__ inv, int32_t *slot) {
-    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n_slots) return;
-    slot[s] = inv[s];
-}
 
 __global__ void scatter_i32_kernel(int64_t n, const int64_t *__restrict__ idx, const int32_t *__restrict__ val, int32_t *dst) {
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -306,10 +303,6 @@ __global__ void posB_kernel(int64_t n_low, const uint32_t *__restrict__ skeys, c
     colind[pb] = (int64_t)(ukeys[u] / (uint64_t)ndof);
 }
 
-__global__ void fill_i64_kernel(int64_t n, int64_t v, int64_t *dst) {
-    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n) dst[t] = v;
-}
 
 __global__ void diag_seg_kernel(int64_t n, const uint32_t *__restrict__ keys, int32_t *cnt) {
     int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -318,30 +311,140 @@ __global__ void diag_seg_kernel(int64_t n, const uint32_t *__restrict__ keys, in
     if (k != 0xffffffffu) atomicAdd(cnt + k, 1);
 }
 
+__constant__ int c_pa4[10] = {0, 0, 0, 0, 1, 1, 1, 2, 2, 3};
+__constant__ int c_pb4[10] = {0, 1, 2, 3, 1, 2, 3, 2, 3, 3};
+__constant__ int c_pa3[6] = {0, 0, 0, 1, 1, 2};
+__constant__ int c_pb3[6] = {0, 1, 2, 1, 2, 2};
+__constant__ int c_pa2[3] = {0, 0, 1};
+__constant__ int c_pb2[3] = {0, 1, 1};
+
+__device__ __forceinline__ void pair_nodes(int NN, int p, int &a, int &b) {
+    if (NN == 4) { a = c_pa4[p]; b = c_pb4[p]; }
+    else if (NN == 3) { a = c_pa3[p]; b = c_pb3[p]; }
+    else { a = c_pa2[p]; b = c_pb2[p]; }
+}
+
+// Keys (min node, max node) of every regular element node pair; pairs that
+// touch a special (RBE2) node or belong to an inactive element sort last.
+__global__ void gen_pair_keys_kernel(int64_t ne, int NN, const int32_t *__restrict__ nodes, const uint8_t *__restrict__ active,
+                                     const uint8_t *__restrict__ special, int64_t base, int64_t n_nodes, uint64_t *keys,
+                                     int32_t *vals) {
+    const int NP = NN * (NN + 1) / 2;
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ne * NP) return;
+    int64_t e = t / NP;
+    int p = (int)(t - e * NP), a, b;
+    pair_nodes(NN, p, a, b);
+    int64_t A = nodes[NN * e + a], B = nodes[NN * e + b];
+    uint64_t key = kSentinel;
+    if (active[e] && !special[A] && !special[B]) {
+        int64_t lo = A < B ? A : B, hi = A < B ? B : A;
+        key = (uint64_t)lo * (uint64_t)n_nodes + (uint64_t)hi;
+    }
+    keys[base + t] = key;
+    vals[base + t] = (int32_t)(base + t);
+}
+
+__global__ void blk_seg_kernel(int64_t n, const int32_t *__restrict__ flags, const int32_t *__restrict__ pos,
+                               const uint64_t *__restrict__ keys, int64_t n_nodes, int32_t *seg, int32_t *A, int32_t *B) {
+    int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n || !flags[q]) return;
+    int32_t k = pos[q];
+    seg[k] = (int32_t)q;
+    A[k] = (int32_t)(keys[q] / (uint64_t)n_nodes);
+    B[k] = (int32_t)(keys[q] % (uint64_t)n_nodes);
+}
+
+__device__ __forceinline__ int64_t find_col(const int64_t *__restrict__ rowptr, const int64_t *__restrict__ colind,
+                                            int64_t r, int64_t c) {
+    int64_t lo = rowptr[r], hi = rowptr[r + 1];
+    while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if (colind[mid] < c) lo = mid + 1; else hi = mid;
+    }
+    return (lo < rowptr[r + 1] && colind[lo] == c) ? lo : -1;
+}
+
+// Column offsets of block (A, B) inside the rows of node A and of node B.
+__global__ void blk_offsets_kernel(int64_t n_blk, const int32_t *__restrict__ A, const int32_t *__restrict__ B,
+                                   const int64_t *__restrict__ rowptr, const int64_t *__restrict__ colind, int32_t *offAB,
+                                   int32_t *offBA, int32_t *err) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n_blk) return;
+    int64_t a = A[k], b = B[k];
+    int64_t pa = find_col(rowptr, colind, 6 * a, 6 * b);
+    int64_t pb = find_col(rowptr, colind, 6 * b, 6 * a);
+    if (pa < 0 || pb < 0) { atomicExch(err, 1); offAB[k] = 0; offBA[k] = 0; return; }
+    offAB[k] = (int32_t)(pa - rowptr[6 * a]);
+    offBA[k] = (int32_t)(pb - rowptr[6 * b]);
+}
+
+// Element pair -> sorted block slot, with the transpose bit when the pair's
+// local orientation (a <= b) maps to global node order A > B.
+__global__ void blk_slot_kernel(int64_t nbc, const int32_t *__restrict__ vals, int64_t pair_t3, int64_t pair_bar,
+                                const int32_t *__restrict__ q4n, const int32_t *__restrict__ t3n,
+                                const int32_t *__restrict__ barn, int32_t *slot) {
+    int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nbc) return;
+    int64_t pid = vals[q];
+    int NN;
+    int64_t local;
+    const int32_t *nodes;
+    if (pid < pair_t3) { NN = 4; local = pid; nodes = q4n; }
+    else if (pid < pair_bar) { NN = 3; local = pid - pair_t3; nodes = t3n; }
+    else { NN = 2; local = pid - pair_bar; nodes = barn; }
+    const int NP = NN * (NN + 1) / 2;
+    int64_t e = local / NP;
+    int p = (int)(local - e * NP), a, b;
+    pair_nodes(NN, p, a, b);
+    int32_t A = nodes[NN * e + a], B = nodes[NN * e + b];
+    slot[pid] = (int32_t)q | (A > B ? jfg::kBlkTranspose : 0);
+}
+
+__global__ void key_pos_kernel(int64_t n, const uint64_t *__restrict__ keys, int64_t ndof, const int64_t *__restrict__ rowptr,
+                               const int64_t *__restrict__ colind, int64_t *pos, int32_t *err) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    int64_t r = (int64_t)(keys[t] / (uint64_t)ndof), c = (int64_t)(keys[t] % (uint64_t)ndof);
+    int64_t p = find_col(rowptr, colind, r, c);
+    if (p < 0) { atomicExch(err, 1); p = 0; }
+    pos[t] = p;
+}
+
 // ---------------------------------------------------------------------------
 // assembly kernels
 // ---------------------------------------------------------------------------
 
-__global__ void expand_kernel(int64_t n, const int32_t *__restrict__ q, const int32_t *__restrict__ src,
-                              const double *__restrict__ w, const double *__restrict__ raw, double *staging) {
+// Deterministic block reduction: thread (k, e) sums entry e of every element
+// block in global block k's segment, in slot order, and writes it to row
+// 6A+i (columns of B) and, for A != B, to the mirrored row 6B+j.
+__global__ void __launch_bounds__(288) block_reduce_kernel(int64_t n_blk, const int32_t *__restrict__ seg,
+                                                           const double *__restrict__ staging, const int32_t *__restrict__ A,
+                                                           const int32_t *__restrict__ B, const int32_t *__restrict__ offAB,
+                                                           const int32_t *__restrict__ offBA, const int64_t *__restrict__ rowptr,
+                                                           double *nz) {
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    staging[q[t]] = w[t] * raw[src[t]];
+    if (t >= n_blk * 36) return;
+    int64_t k = t / 36;
+    int e = (int)(t - 36 * k), i = e / 6, j = e - 6 * (e / 6);
+    int32_t a = __ldg(seg + k), b = __ldg(seg + k + 1);
+    double s = 0.0;
+    for (int32_t q = a; q < b; ++q) s += __ldg(staging + 36 * (int64_t)q + e);
+    int64_t nA = __ldg(A + k), nB = __ldg(B + k);
+    nz[__ldg(rowptr + 6 * nA + i) + __ldg(offAB + k) + j] = s;
+    if (nA != nB) nz[__ldg(rowptr + 6 * nB + j) + __ldg(offBA + k) + i] = s;
 }
 
-// Deterministic segmented reduction: nonzero u sums staging[seg[u], seg[u+1])
-// left to right and writes both symmetric CSC positions.
-__global__ void __launch_bounds__(256) reduce_kernel(int64_t n_upper, const int32_t *__restrict__ seg,
-                                                     const double *__restrict__ staging, const int64_t *__restrict__ posA,
-                                                     const int64_t *__restrict__ posB, double *nz) {
-    int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (u >= n_upper) return;
-    int32_t a = __ldg(seg + u), b = __ldg(seg + u + 1);
+// Dof-level path: each CSC position touched by an RBE2-expanded entry sums
+// its weighted raw element values in a fixed order.
+__global__ void exc_reduce_kernel(int64_t n, const int32_t *__restrict__ seg, const int32_t *__restrict__ src,
+                                  const double *__restrict__ w, const double *__restrict__ raw,
+                                  const int64_t *__restrict__ pos, double *nz) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
     double s = 0.0;
-    for (int32_t q = a; q < b; ++q) s += __ldg(staging + q);
-    nz[__ldg(posA + u)] = s;
-    int64_t pb = __ldg(posB + u);
-    if (pb >= 0) nz[pb] = s;
+    for (int32_t q = seg[t]; q < seg[t + 1]; ++q) s += w[q] * raw[src[q]];
+    nz[pos[t]] = s;
 }
 
 __global__ void diag_reduce_kernel(int64_t ndof, const int32_t *__restrict__ seg, const double *__restrict__ st, double *out) {
@@ -398,6 +501,9 @@ jfg_status validate(jfg_model *m, const jfg_model_desc *d) {
             if (n[k] < 0 || n[k] >= d->n_nodes) return fail(m, JFG_ERR_INVALID, "CQUAD4 node index out of range");
         const double *pr = d->quad4_prop + JFG_SHELL_PROP * e;
         if (!(pr[0] > 0.0) || !(pr[1] > 0.0)) return fail(m, JFG_ERR_INVALID, "shell thickness and E must be positive");
+        for (int a = 0; a < 4; ++a)
+            for (int b = a + 1; b < 4; ++b)
+                if (n[a] == n[b]) return fail(m, JFG_ERR_INVALID, "CQUAD4 with a repeated node");
         if (!host_q4_flat(d->coords + 3 * n[0], d->coords + 3 * n[1], d->coords + 3 * n[2], d->coords + 3 * n[3]))
             return fail(m, JFG_ERR_UNSUPPORTED,
                         "non-flat CQUAD4 (warp >= 1e-6 of the diagonal) leaves the flat default branch (assembly.jl:2824-2840)");
@@ -409,6 +515,8 @@ jfg_status validate(jfg_model *m, const jfg_model_desc *d) {
         }
         const double *pr = d->tria3_prop + JFG_SHELL_PROP * e;
         if (!(pr[0] > 0.0) || !(pr[1] > 0.0)) return fail(m, JFG_ERR_INVALID, "shell thickness and E must be positive");
+        const int32_t *tn = d->tria3_nodes + 3 * e;
+        if (tn[0] == tn[1] || tn[0] == tn[2] || tn[1] == tn[2]) return fail(m, JFG_ERR_INVALID, "CTRIA3 with a repeated node");
     }
     for (int64_t e = 0; e < d->n_bar; ++e) {
         for (int k = 0; k < 2; ++k) {
@@ -538,72 +646,43 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
         for (int k = 0; k < 2; ++k)
             if (node_dep[d->bar_nodes[2 * e + k]]) reg_bar[e] = 0;
     }
-    m->slot_q4 = 0;
-    m->slot_t3 = m->nq * 300;
-    m->slot_bar = m->slot_t3 + m->nt * 171;
-    m->n_slots = m->slot_bar + m->nb * 78;
-    if (m->n_slots >= ((int64_t)1 << 31) - 1) return fail(m, JFG_ERR_UNSUPPORTED, "more than 2^31 element entries in one handle");
-
-    // host expansion of exception elements: ordered local pairs -> (key, raw src, weight)
-    struct ExcC { uint64_t key; int32_t src; double w; };
-    std::vector<ExcC> exc;
-    std::vector<int64_t> exc_slot_idx;    // packed slot s that becomes a raw-buffer reference
-    std::vector<int32_t> exc_slot_code;
-    int64_t raw_count = 0;
-    auto expand_elem = [&](const int32_t *nodes, int NN, int64_t slot_base) {
-        const int N = 6 * NN, P = N * (N + 1) / 2;
-        int64_t raw_base = raw_count;
-        raw_count += P;
-        for (int p = 0; p < P; ++p) {
-            exc_slot_idx.push_back(slot_base + p);
-            exc_slot_code.push_back((int32_t)(-(raw_base + p) - 1));
-        }
-        std::map<std::pair<uint64_t, int32_t>, double> acc;
+    // ===================== 1. CSC pattern (entry level) =====================
+    // Keys of every upper-triangle element entry after constraint expansion;
+    // elements touching a dependent dof are expanded on the host.
+    const int64_t slot_q4 = 0, slot_t3 = m->nq * 300, slot_bar = slot_t3 + m->nt * 171;
+    const int64_t S = slot_bar + m->nb * 78;
+    if (S >= ((int64_t)1 << 31) - 1) return fail(m, JFG_ERR_UNSUPPORTED, "more than 2^31 element entries in one handle");
+    std::vector<uint64_t> pexc;   // upper keys of constraint-expanded entries
+    auto expand_pattern = [&](const int32_t *nodes, int NN) {
+        const int N = 6 * NN;
         for (int i = 0; i < N; ++i)
             for (int j = 0; j < N; ++j) {
                 int64_t r = 6 * (int64_t)nodes[i / 6] + i % 6, c = 6 * (int64_t)nodes[j / 6] + j % 6;
                 std::vector<std::pair<int64_t, double>> ri, cj;
                 if (dep[r]) ri = *dep[r]; else ri.push_back({r, 1.0});
                 if (dep[c]) cj = *dep[c]; else cj.push_back({c, 1.0});
-                int pi = std::min(i, j), pj = std::max(i, j);
-                int32_t src = (int32_t)(raw_base + packed_index(pi, pj, N));
                 for (auto &a : ri)
-                    for (auto &b : cj) {
-                        if (a.first > b.first) continue;
-                        uint64_t key = (uint64_t)a.first * (uint64_t)ndof + (uint64_t)b.first;
-                        acc[{key, src}] += a.second * b.second;
-                    }
+                    for (auto &b : cj)
+                        if (a.first <= b.first) pexc.push_back((uint64_t)a.first * (uint64_t)ndof + (uint64_t)b.first);
             }
-        for (auto &kv : acc) exc.push_back({kv.first.first, kv.first.second, kv.second});
     };
+    int64_t n_sent = 0;
     for (int64_t e = 0; e < m->nq; ++e)
-        if (!reg_q4[e]) expand_elem(d->quad4_nodes + 4 * e, 4, m->slot_q4 + e * 300);
+        if (!reg_q4[e]) { expand_pattern(d->quad4_nodes + 4 * e, 4); n_sent += 300; }
     for (int64_t e = 0; e < m->nt; ++e)
-        if (!reg_t3[e]) expand_elem(d->tria3_nodes + 3 * e, 3, m->slot_t3 + e * 171);
+        if (!reg_t3[e]) { expand_pattern(d->tria3_nodes + 3 * e, 3); n_sent += 171; }
     for (int64_t e = 0; e < m->nb; ++e)
-        if (!reg_bar[e] && act_bar[e]) expand_elem(d->bar_nodes + 2 * e, 2, m->slot_bar + e * 78);
-    int64_t n_inactive_slots = 0, n_exc_only = (int64_t)exc_slot_idx.size();
-    for (int64_t e = 0; e < m->nb; ++e)
-        if (!act_bar[e]) n_inactive_slots += 78;
-    m->n_exc = (int64_t)exc.size();
-    m->n_exc_raw = raw_count;
-    const int64_t S = m->n_slots;
-    const int64_t n_total = S + m->n_exc;
-    m->n_contrib = S - n_exc_only - n_inactive_slots + m->n_exc;
-    // zero-length bars never write; their slots still point at a dummy cell
-    for (int64_t e = 0; e < m->nb; ++e)
-        if (!act_bar[e])
-            for (int p = 0; p < 78; ++p) {
-                exc_slot_idx.push_back(m->slot_bar + e * 78 + p);
-                exc_slot_code.push_back((int32_t)m->n_contrib);
-            }
-    const int64_t n_exc_elem_slots = (int64_t)exc_slot_idx.size();
-    if (n_total >= ((int64_t)1 << 31) - 1) return fail(m, JFG_ERR_UNSUPPORTED, "more than 2^31 contributions in one handle");
+        if (!reg_bar[e]) { if (act_bar[e]) expand_pattern(d->bar_nodes + 2 * e, 2); n_sent += 78; }
+    std::sort(pexc.begin(), pexc.end());
+    pexc.erase(std::unique(pexc.begin(), pexc.end()), pexc.end());
+    const int64_t n_pexc = (int64_t)pexc.size();
+    const int64_t n_total = S + n_pexc;
+    const int64_t nv = S - n_sent + n_pexc;   // non-sentinel keys
+    if (n_total >= ((int64_t)1 << 31) - 1) return fail(m, JFG_ERR_UNSUPPORTED, "more than 2^31 pattern keys in one handle");
 
-    // --- GPU key generation and sort ---
     uint8_t *d_reg = nullptr;
     int64_t ne_max = std::max(std::max(m->nq, m->nt), m->nb);
-    CK(cudaMallocAsync(&d_reg, std::max<int64_t>(ne_max, 1), m->stream));
+    CK(cudaMallocAsync(&d_reg, std::max<int64_t>(std::max(ne_max, m->n_nodes), 1), m->stream));
     uint64_t *d_keys = nullptr, *d_keys2 = nullptr;
     int32_t *d_vals = nullptr, *d_vals2 = nullptr;
     CK(cudaMallocAsync(&d_keys, sizeof(uint64_t) * std::max<int64_t>(n_total, 1), m->stream));
@@ -620,23 +699,19 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
         if (e != cudaSuccess) return e;
         return cudaStreamSynchronize(m->stream);  // reg buffer reused
     };
-    CK(gen(m->nq, 4, m->d_q4n, reg_q4, m->slot_q4));
-    CK(gen(m->nt, 3, m->d_t3n, reg_t3, m->slot_t3));
-    CK(gen(m->nb, 2, m->d_barn, reg_bar, m->slot_bar));
-    if (m->n_exc) {
-        std::vector<uint64_t> hk(m->n_exc);
-        std::vector<int32_t> hv(m->n_exc);
-        for (int64_t k = 0; k < m->n_exc; ++k) { hk[k] = exc[k].key; hv[k] = (int32_t)(S + k); }
-        CK(cudaMemcpyAsync(d_keys + S, hk.data(), sizeof(uint64_t) * m->n_exc, cudaMemcpyHostToDevice, m->stream));
-        CK(cudaMemcpyAsync(d_vals + S, hv.data(), sizeof(int32_t) * m->n_exc, cudaMemcpyHostToDevice, m->stream));
+    CK(gen(m->nq, 4, m->d_q4n, reg_q4, slot_q4));
+    CK(gen(m->nt, 3, m->d_t3n, reg_t3, slot_t3));
+    CK(gen(m->nb, 2, m->d_barn, reg_bar, slot_bar));
+    if (n_pexc) {
+        std::vector<int32_t> hv(n_pexc);
+        for (int64_t k = 0; k < n_pexc; ++k) hv[k] = (int32_t)(S + k);
+        CK(cudaMemcpyAsync(d_keys + S, pexc.data(), sizeof(uint64_t) * n_pexc, cudaMemcpyHostToDevice, m->stream));
+        CK(cudaMemcpyAsync(d_vals + S, hv.data(), sizeof(int32_t) * n_pexc, cudaMemcpyHostToDevice, m->stream));
         CK(cudaStreamSynchronize(m->stream));
     }
-    int end_bit = 64;  // sentinel uses all bits
-    CK(radix_sort(m, d_keys, d_keys2, d_vals, d_vals2, n_total, end_bit));
-    const int64_t nv = m->n_contrib;  // valid (non-sentinel) prefix
+    CK(radix_sort(m, d_keys, d_keys2, d_vals, d_vals2, n_total, 64));
 
-    // --- unique upper nonzeros and segments ---
-    int32_t *d_flags = nullptr, *d_upos = nullptr;
+    int32_t *d_flags = nullptr, *d_upos = nullptr, *d_seg = nullptr;
     CK(cudaMallocAsync(&d_flags, sizeof(int32_t) * std::max<int64_t>(nv, 1), m->stream));
     CK(cudaMallocAsync(&d_upos, sizeof(int32_t) * std::max<int64_t>(nv, 1), m->stream));
     if (nv) head_flags_kernel<<<(unsigned)cdiv(nv, 256), 256, 0, m->stream>>>(nv, d_keys2, d_flags);
@@ -650,62 +725,26 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
     CK(cudaStreamSynchronize(m->stream));
     m->n_upper = nv ? (int64_t)last_pos + last_flag : 0;
     const int64_t nu = m->n_upper;
-    CK(dalloc(m, &m->d_seg, nu + 1));
     uint64_t *d_ukeys = nullptr;
     int32_t *d_upcnt = nullptr, *d_lowcnt = nullptr;
+    CK(cudaMallocAsync(&d_seg, sizeof(int32_t) * (nu + 1), m->stream));
     CK(cudaMallocAsync(&d_ukeys, sizeof(uint64_t) * std::max<int64_t>(nu, 1), m->stream));
     CK(cudaMallocAsync(&d_upcnt, sizeof(int32_t) * ndof, m->stream));
     CK(cudaMallocAsync(&d_lowcnt, sizeof(int32_t) * ndof, m->stream));
     CK(cudaMemsetAsync(d_upcnt, 0, sizeof(int32_t) * ndof, m->stream));
     CK(cudaMemsetAsync(d_lowcnt, 0, sizeof(int32_t) * ndof, m->stream));
-    if (nv) seg_kernel<<<(unsigned)cdiv(nv, 256), 256, 0, m->stream>>>(nv, d_flags, d_upos, d_keys2, ndof, m->d_seg, d_ukeys, d_upcnt, d_lowcnt);
+    if (nv) seg_kernel<<<(unsigned)cdiv(nv, 256), 256, 0, m->stream>>>(nv, d_flags, d_upos, d_keys2, ndof, d_seg, d_ukeys, d_upcnt, d_lowcnt);
     CK(cudaGetLastError());
-    {
-        int32_t nv32 = (int32_t)nv;
-        CK(cudaMemcpyAsync(m->d_seg + nu, &nv32, sizeof(int32_t), cudaMemcpyHostToDevice, m->stream));
-        CK(cudaStreamSynchronize(m->stream));
-    }
+    cudaFreeAsync(d_keys, m->stream); d_keys = nullptr;
+    cudaFreeAsync(d_keys2, m->stream); d_keys2 = nullptr;
+    cudaFreeAsync(d_vals, m->stream); d_vals = nullptr;
+    cudaFreeAsync(d_vals2, m->stream); d_vals2 = nullptr;
+    cudaFreeAsync(d_flags, m->stream); d_flags = nullptr;
+    cudaFreeAsync(d_upos, m->stream); d_upos = nullptr;
+    cudaFreeAsync(d_seg, m->stream); d_seg = nullptr;
 
-    // --- slot map: inverse permutation ---
-    int32_t *d_inv = nullptr;
-    CK(cudaMallocAsync(&d_inv, sizeof(int32_t) * std::max<int64_t>(n_total, 1), m->stream));
-    if (n_total) inv_kernel<<<(unsigned)cdiv(n_total, 256), 256, 0, m->stream>>>(n_total, d_vals2, d_inv);
-    CK(cudaGetLastError());
-    CK(dalloc(m, &m->d_slot, S));
-    if (S) regular_slot_kernel<<<(unsigned)cdiv(S, 256), 256, 0, m->stream>>>(S, d_inv, m->d_slot);
-    CK(cudaGetLastError());
-    if (n_exc_elem_slots) {
-        int64_t *d_si = nullptr;
-        int32_t *d_sc = nullptr;
-        CK(cudaMallocAsync(&d_si, sizeof(int64_t) * n_exc_elem_slots, m->stream));
-        CK(cudaMallocAsync(&d_sc, sizeof(int32_t) * n_exc_elem_slots, m->stream));
-        CK(cudaMemcpyAsync(d_si, exc_slot_idx.data(), sizeof(int64_t) * n_exc_elem_slots, cudaMemcpyHostToDevice, m->stream));
-        CK(cudaMemcpyAsync(d_sc, exc_slot_code.data(), sizeof(int32_t) * n_exc_elem_slots, cudaMemcpyHostToDevice, m->stream));
-        scatter_i32_kernel<<<(unsigned)cdiv(n_exc_elem_slots, 256), 256, 0, m->stream>>>(n_exc_elem_slots, d_si, d_sc, m->d_slot);
-        CK(cudaGetLastError());
-        CK(cudaStreamSynchronize(m->stream));
-        cudaFreeAsync(d_si, m->stream);
-        cudaFreeAsync(d_sc, m->stream);
-    }
-    if (m->n_exc) {
-        std::vector<int32_t> hq(m->n_exc), hs(m->n_exc);
-        std::vector<double> hw(m->n_exc);
-        CK(cudaMemcpyAsync(hq.data(), d_inv + S, sizeof(int32_t) * m->n_exc, cudaMemcpyDeviceToHost, m->stream));
-        CK(cudaStreamSynchronize(m->stream));
-        for (int64_t k = 0; k < m->n_exc; ++k) { hs[k] = exc[k].src; hw[k] = exc[k].w; }
-        CK(dalloc(m, &m->d_exc_q, m->n_exc));
-        CK(dalloc(m, &m->d_exc_src, m->n_exc));
-        CK(dalloc(m, &m->d_exc_w, m->n_exc));
-        CK(cudaMemcpyAsync(m->d_exc_q, hq.data(), sizeof(int32_t) * m->n_exc, cudaMemcpyHostToDevice, m->stream));
-        CK(cudaMemcpyAsync(m->d_exc_src, hs.data(), sizeof(int32_t) * m->n_exc, cudaMemcpyHostToDevice, m->stream));
-        CK(cudaMemcpyAsync(m->d_exc_w, hw.data(), sizeof(double) * m->n_exc, cudaMemcpyHostToDevice, m->stream));
-        CK(cudaStreamSynchronize(m->stream));
-    }
-    CK(dalloc(m, &m->d_exc_raw, m->n_exc_raw));
-    CK(dalloc(m, &m->d_staging, nv + 1));
-
-    // --- symmetric CSR (== CSC) positions ---
-    int64_t *d_rowcnt = nullptr, *d_uprs = nullptr;
+    // symmetric CSR (== CSC) row pointers and column indices
+    int64_t *d_rowcnt = nullptr, *d_uprs = nullptr, *d_posA = nullptr, *d_posB = nullptr;
     CK(dalloc(m, &m->d_rowptr, ndof + 1));
     CK(cudaMallocAsync(&d_rowcnt, sizeof(int64_t) * (ndof + 1), m->stream));
     CK(cudaMallocAsync(&d_uprs, sizeof(int64_t) * (ndof + 1), m->stream));
@@ -717,8 +756,8 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
     CK(cudaMemcpyAsync(&m->nnz, m->d_rowptr + ndof, sizeof(int64_t), cudaMemcpyDeviceToHost, m->stream));
     CK(cudaStreamSynchronize(m->stream));
     CK(dalloc(m, &m->d_colind, m->nnz));
-    CK(dalloc(m, &m->d_posA, nu));
-    CK(dalloc(m, &m->d_posB, nu));
+    CK(cudaMallocAsync(&d_posA, sizeof(int64_t) * std::max<int64_t>(nu, 1), m->stream));
+    CK(cudaMallocAsync(&d_posB, sizeof(int64_t) * std::max<int64_t>(nu, 1), m->stream));
     uint32_t *d_lk = nullptr, *d_lk2 = nullptr;
     int32_t *d_lv = nullptr, *d_lv2 = nullptr, *d_lf = nullptr;
     int64_t *d_lowstart = nullptr;
@@ -730,19 +769,198 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
     CK(cudaMallocAsync(&d_lowstart, sizeof(int64_t) * ndof, m->stream));
     if (nu) {
         posA_kernel<<<(unsigned)cdiv(nu, 256), 256, 0, m->stream>>>(nu, d_ukeys, ndof, m->d_rowptr, d_lowcnt, d_uprs,
-                                                                      m->d_posA, m->d_colind, d_lk, d_lv, d_lf);
-        CK(cudaGetLastError());
-        fill_i64_kernel<<<(unsigned)cdiv(nu, 256), 256, 0, m->stream>>>(nu, -1, m->d_posB);
+                                                                      d_posA, m->d_colind, d_lk, d_lv, d_lf);
         CK(cudaGetLastError());
         CK(radix_sort(m, d_lk, d_lk2, d_lv, d_lv2, nu, 32));
         CK(exclusive_sum(m, d_lowcnt, d_lowstart, ndof));
-        // lower entries are the sorted prefix whose key is not the sentinel
         const int64_t n_low = m->nnz - nu;  // every off-diagonal upper entry has one mirror
         if (n_low)
             posB_kernel<<<(unsigned)cdiv(n_low, 256), 256, 0, m->stream>>>(n_low, d_lk2, d_lv2, d_lowstart, m->d_rowptr,
-                                                                             d_ukeys, ndof, m->d_posB, m->d_colind);
+                                                                             d_ukeys, ndof, d_posB, m->d_colind);
         CK(cudaGetLastError());
     }
+    CK(cudaStreamSynchronize(m->stream));
+    for (void *p : {(void *)d_ukeys, (void *)d_upcnt, (void *)d_lowcnt, (void *)d_rowcnt, (void *)d_uprs, (void *)d_posA,
+                    (void *)d_posB, (void *)d_lk, (void *)d_lk2, (void *)d_lv, (void *)d_lv2, (void *)d_lf, (void *)d_lowstart})
+        cudaFreeAsync(p, m->stream);
+
+    // ===================== 2. node-pair block scatter map =====================
+    // Regular pairs (neither node is an RBE2 slave or master): one 6x6 block
+    // per element pair, sorted by global node pair (min, max).
+    std::vector<uint8_t> special(m->n_nodes, 0);
+    for (auto &kv : mp) {
+        special[kv.first / 6] = 1;
+        for (auto &p : kv.second) special[p.first / 6] = 1;
+    }
+    m->pair_q4 = 0;
+    m->pair_t3 = m->nq * 10;
+    m->pair_bar = m->pair_t3 + m->nt * 6;
+    m->n_pairs = m->pair_bar + m->nb * 3;
+    const int64_t NP = m->n_pairs;
+    uint8_t *d_special = nullptr;
+    CK(cudaMallocAsync(&d_special, std::max<int64_t>(m->n_nodes, 1), m->stream));
+    CK(cudaMemcpyAsync(d_special, special.data(), m->n_nodes, cudaMemcpyHostToDevice, m->stream));
+    uint64_t *d_bk = nullptr, *d_bk2 = nullptr;
+    int32_t *d_bv = nullptr, *d_bv2 = nullptr;
+    CK(cudaMallocAsync(&d_bk, sizeof(uint64_t) * std::max<int64_t>(NP, 1), m->stream));
+    CK(cudaMallocAsync(&d_bk2, sizeof(uint64_t) * std::max<int64_t>(NP, 1), m->stream));
+    CK(cudaMallocAsync(&d_bv, sizeof(int32_t) * std::max<int64_t>(NP, 1), m->stream));
+    CK(cudaMallocAsync(&d_bv2, sizeof(int32_t) * std::max<int64_t>(NP, 1), m->stream));
+    std::vector<uint8_t> all_q4(m->nq, 1), all_t3(m->nt, 1);
+    auto pgen = [&](int64_t ne, int NN, const int32_t *dn, const std::vector<uint8_t> &act, int64_t base) -> cudaError_t {
+        if (!ne) return cudaSuccess;
+        cudaError_t e = cudaMemcpyAsync(d_reg, act.data(), ne, cudaMemcpyHostToDevice, m->stream);
+        if (e != cudaSuccess) return e;
+        int NPe = NN * (NN + 1) / 2;
+        gen_pair_keys_kernel<<<(unsigned)cdiv(ne * NPe, 256), 256, 0, m->stream>>>(ne, NN, dn, d_reg, d_special, base,
+                                                                                     m->n_nodes, d_bk, d_bv);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        return cudaStreamSynchronize(m->stream);
+    };
+    CK(pgen(m->nq, 4, m->d_q4n, all_q4, m->pair_q4));
+    CK(pgen(m->nt, 3, m->d_t3n, all_t3, m->pair_t3));
+    CK(pgen(m->nb, 2, m->d_barn, act_bar, m->pair_bar));
+    if (NP) CK(radix_sort(m, d_bk, d_bk2, d_bv, d_bv2, NP, 64));
+    // host view of the pair classes: exception pairs (touch a special node) and
+    // inactive pairs (zero-length bars) sort as sentinels
+    struct XPair { int64_t pair; int64_t e; int type; int a, b; };
+    std::vector<XPair> xpairs;
+    int64_t n_inactive_pairs = 0;
+    auto scan_pairs = [&](int64_t ne, int NN, const int32_t *nodes, const std::vector<uint8_t> &act, int64_t base, int type) {
+        int pa[10], pb[10], np = 0;  // up to 10 node pairs (CQUAD4)
+        for (int a = 0; a < NN; ++a)
+            for (int b = a; b < NN; ++b) { pa[np] = a; pb[np] = b; ++np; }
+        for (int64_t e = 0; e < ne; ++e) {
+            if (!act[e]) { n_inactive_pairs += np; continue; }
+            for (int p = 0; p < np; ++p) {
+                int32_t A = nodes[NN * e + pa[p]], B = nodes[NN * e + pb[p]];
+                if (special[A] || special[B]) xpairs.push_back({base + e * np + p, e, type, pa[p], pb[p]});
+            }
+        }
+    };
+    scan_pairs(m->nq, 4, d->quad4_nodes, all_q4, m->pair_q4, 0);
+    scan_pairs(m->nt, 3, d->tria3_nodes, all_t3, m->pair_t3, 1);
+    scan_pairs(m->nb, 2, d->bar_nodes, act_bar, m->pair_bar, 2);
+    m->n_blk_contrib = NP - (int64_t)xpairs.size() - n_inactive_pairs;
+    const int64_t nbc = m->n_blk_contrib;
+    if (36 * nbc >= ((int64_t)1 << 40)) return fail(m, JFG_ERR_UNSUPPORTED, "block staging too large");
+    // unique global blocks and their segments
+    int32_t *d_bflags = nullptr, *d_bpos = nullptr;
+    CK(cudaMallocAsync(&d_bflags, sizeof(int32_t) * std::max<int64_t>(nbc, 1), m->stream));
+    CK(cudaMallocAsync(&d_bpos, sizeof(int32_t) * std::max<int64_t>(nbc, 1), m->stream));
+    if (nbc) head_flags_kernel<<<(unsigned)cdiv(nbc, 256), 256, 0, m->stream>>>(nbc, d_bk2, d_bflags);
+    CK(cudaGetLastError());
+    CK(exclusive_sum(m, d_bflags, d_bpos, nbc));
+    int32_t bl_flag = 0, bl_pos = 0;
+    if (nbc) {
+        CK(cudaMemcpyAsync(&bl_flag, d_bflags + nbc - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, m->stream));
+        CK(cudaMemcpyAsync(&bl_pos, d_bpos + nbc - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, m->stream));
+    }
+    CK(cudaStreamSynchronize(m->stream));
+    m->n_blk = nbc ? (int64_t)bl_pos + bl_flag : 0;
+    CK(dalloc(m, &m->d_blk_seg, m->n_blk + 1));
+    CK(dalloc(m, &m->d_blk_A, m->n_blk));
+    CK(dalloc(m, &m->d_blk_B, m->n_blk));
+    CK(dalloc(m, &m->d_blk_offAB, m->n_blk));
+    CK(dalloc(m, &m->d_blk_offBA, m->n_blk));
+    CK(dalloc(m, &m->d_blk_slot, NP));
+    CK(cudaMemsetAsync(m->d_blk_slot, 0, sizeof(int32_t) * std::max<int64_t>(NP, 1), m->stream));
+    int32_t *d_err = nullptr;
+    CK(cudaMallocAsync(&d_err, sizeof(int32_t), m->stream));
+    CK(cudaMemsetAsync(d_err, 0, sizeof(int32_t), m->stream));
+    if (nbc) {
+        blk_seg_kernel<<<(unsigned)cdiv(nbc, 256), 256, 0, m->stream>>>(nbc, d_bflags, d_bpos, d_bk2, m->n_nodes, m->d_blk_seg,
+                                                                        m->d_blk_A, m->d_blk_B);
+        CK(cudaGetLastError());
+        int32_t nbc32 = (int32_t)nbc;
+        CK(cudaMemcpyAsync(m->d_blk_seg + m->n_blk, &nbc32, sizeof(int32_t), cudaMemcpyHostToDevice, m->stream));
+        blk_offsets_kernel<<<(unsigned)cdiv(m->n_blk, 256), 256, 0, m->stream>>>(m->n_blk, m->d_blk_A, m->d_blk_B, m->d_rowptr,
+                                                                                 m->d_colind, m->d_blk_offAB, m->d_blk_offBA, d_err);
+        CK(cudaGetLastError());
+        blk_slot_kernel<<<(unsigned)cdiv(nbc, 256), 256, 0, m->stream>>>(nbc, d_bv2, m->pair_t3, m->pair_bar, m->d_q4n, m->d_t3n,
+                                                                         m->d_barn, m->d_blk_slot);
+        CK(cudaGetLastError());
+    }
+    // exception pairs: raw blocks, then dof-level weighted contributions
+    m->n_xpair = (int64_t)xpairs.size();
+    if (m->n_xpair) {
+        std::vector<int64_t> xi(m->n_xpair);
+        std::vector<int32_t> xc(m->n_xpair);
+        for (int64_t k = 0; k < m->n_xpair; ++k) { xi[k] = xpairs[k].pair; xc[k] = (int32_t)(-(k + 1)); }
+        int64_t *d_xi = nullptr;
+        int32_t *d_xc = nullptr;
+        CK(cudaMallocAsync(&d_xi, sizeof(int64_t) * m->n_xpair, m->stream));
+        CK(cudaMallocAsync(&d_xc, sizeof(int32_t) * m->n_xpair, m->stream));
+        CK(cudaMemcpyAsync(d_xi, xi.data(), sizeof(int64_t) * m->n_xpair, cudaMemcpyHostToDevice, m->stream));
+        CK(cudaMemcpyAsync(d_xc, xc.data(), sizeof(int32_t) * m->n_xpair, cudaMemcpyHostToDevice, m->stream));
+        scatter_i32_kernel<<<(unsigned)cdiv(m->n_xpair, 256), 256, 0, m->stream>>>(m->n_xpair, d_xi, d_xc, m->d_blk_slot);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(m->stream));
+        cudaFreeAsync(d_xi, m->stream);
+        cudaFreeAsync(d_xc, m->stream);
+        // (row, col, src, weight) over ordered entries of every exception pair
+        struct XC { uint64_t key; int32_t src; double w; };
+        std::vector<XC> xcs;
+        for (int64_t k = 0; k < m->n_xpair; ++k) {
+            const XPair &x = xpairs[k];
+            const int32_t *nodes = x.type == 0 ? d->quad4_nodes + 4 * x.e : x.type == 1 ? d->tria3_nodes + 3 * x.e : d->bar_nodes + 2 * x.e;
+            int64_t A = nodes[x.a], B = nodes[x.b];
+            std::map<std::pair<uint64_t, int32_t>, double> acc;
+            for (int i = 0; i < 6; ++i)
+                for (int j = 0; j < 6; ++j) {
+                    int32_t src = (int32_t)(36 * k + 6 * i + j);
+                    for (int t = 0; t < (x.a == x.b ? 1 : 2); ++t) {
+                        int64_t r = t == 0 ? 6 * A + i : 6 * B + j;
+                        int64_t c = t == 0 ? 6 * B + j : 6 * A + i;
+                        std::vector<std::pair<int64_t, double>> ri, cj;
+                        if (dep[r]) ri = *dep[r]; else ri.push_back({r, 1.0});
+                        if (dep[c]) cj = *dep[c]; else cj.push_back({c, 1.0});
+                        for (auto &pr : ri)
+                            for (auto &pc : cj) acc[{(uint64_t)pr.first * (uint64_t)ndof + (uint64_t)pc.first, src}] += pr.second * pc.second;
+                    }
+                }
+            for (auto &kv : acc) xcs.push_back({kv.first.first, kv.first.second, kv.second});
+        }
+        std::stable_sort(xcs.begin(), xcs.end(), [](const XC &p, const XC &q) { return p.key < q.key; });
+        std::vector<uint64_t> ukey;
+        std::vector<int32_t> seg, src;
+        std::vector<double> w;
+        for (size_t q = 0; q < xcs.size(); ++q) {
+            if (q == 0 || xcs[q].key != xcs[q - 1].key) { ukey.push_back(xcs[q].key); seg.push_back((int32_t)q); }
+            src.push_back(xcs[q].src);
+            w.push_back(xcs[q].w);
+        }
+        seg.push_back((int32_t)xcs.size());
+        m->n_xkey = (int64_t)ukey.size();
+        m->n_xcontrib = (int64_t)xcs.size();
+        uint64_t *d_uk = nullptr;
+        CK(cudaMallocAsync(&d_uk, sizeof(uint64_t) * m->n_xkey, m->stream));
+        CK(cudaMemcpyAsync(d_uk, ukey.data(), sizeof(uint64_t) * m->n_xkey, cudaMemcpyHostToDevice, m->stream));
+        CK(dalloc(m, &m->d_x_pos, m->n_xkey));
+        CK(dalloc(m, &m->d_x_seg, m->n_xkey + 1));
+        CK(dalloc(m, &m->d_x_src, m->n_xcontrib));
+        CK(dalloc(m, &m->d_x_w, m->n_xcontrib));
+        CK(cudaMemcpyAsync(m->d_x_seg, seg.data(), sizeof(int32_t) * seg.size(), cudaMemcpyHostToDevice, m->stream));
+        CK(cudaMemcpyAsync(m->d_x_src, src.data(), sizeof(int32_t) * src.size(), cudaMemcpyHostToDevice, m->stream));
+        CK(cudaMemcpyAsync(m->d_x_w, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice, m->stream));
+        key_pos_kernel<<<(unsigned)cdiv(m->n_xkey, 256), 256, 0, m->stream>>>(m->n_xkey, d_uk, ndof, m->d_rowptr, m->d_colind,
+                                                                             m->d_x_pos, d_err);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(m->stream));
+        cudaFreeAsync(d_uk, m->stream);
+    }
+    CK(dalloc(m, &m->d_exc_raw, 36 * m->n_xpair));
+    CK(dalloc(m, &m->d_staging, 36 * nbc));
+    {
+        int32_t herr = 0;
+        CK(cudaMemcpyAsync(&herr, d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, m->stream));
+        CK(cudaStreamSynchronize(m->stream));
+        if (herr) return fail(m, JFG_ERR_STATE, "internal: a block or constrained entry is missing from the pattern");
+    }
+    for (void *p : {(void *)d_special, (void *)d_bk, (void *)d_bk2, (void *)d_bv, (void *)d_bv2, (void *)d_bflags,
+                    (void *)d_bpos, (void *)d_err})
+        cudaFreeAsync(p, m->stream);
 
     // --- orig_diag map (raw element diagonal, no constraint expansion) ---
     m->dslot_q4 = 0;
@@ -786,12 +1004,7 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
         cudaFreeAsync(d_dv, m->stream); cudaFreeAsync(d_dv2, m->stream); cudaFreeAsync(d_dcnt, m->stream);
     }
 
-    // --- release build temporaries ---
-    for (void *p : {(void *)d_reg, (void *)d_keys, (void *)d_keys2, (void *)d_vals, (void *)d_vals2, (void *)d_flags,
-                    (void *)d_upos, (void *)d_ukeys, (void *)d_upcnt, (void *)d_lowcnt, (void *)d_inv, (void *)d_rowcnt,
-                    (void *)d_uprs, (void *)d_lk, (void *)d_lk2, (void *)d_lv, (void *)d_lv2, (void *)d_lf,
-                    (void *)d_lowstart})
-        if (p) cudaFreeAsync(p, m->stream);
+    if (d_reg) cudaFreeAsync(d_reg, m->stream);
     // --- persistent work buffers ---
     CK(dalloc(m, &m->d_nz, m->nnz));
     CK(dalloc(m, &m->d_u, ndof));
@@ -837,48 +1050,61 @@ namespace {
 
 jfg_status begin_set(jfg_model *m, int kind);
 
-jfg_status launch_k(jfg_model *m, double *nz, double *dmax, double *ddiag) {
-    jfg_status bst = begin_set(m, 0);
-    if (bst) return bst;
+jfg_status launch_elements(jfg_model *m, bool kg, const double *du, double *dmax, double *ddiag) {
     ElemOut o;
     o.staging = m->d_staging;
     o.exc_raw = m->d_exc_raw;
     o.diag_staging = ddiag ? m->d_dstaging : nullptr;
+    o.diag_slot = nullptr;
     o.maxabs = dmax;
-    if (dmax) CK(cudaMemsetAsync(dmax, 0, sizeof(double), m->stream));
     CK(cudaEventRecord(m->ev[0], m->stream));
     if (m->nq) {
-        o.slot = m->d_slot + m->slot_q4;
+        o.blk_slot = m->d_blk_slot + m->pair_q4;
         o.diag_slot = m->d_dslot + m->dslot_q4;
-        q4_k_kernel<<<(unsigned)cdiv(m->nq, Q4_ELEMS_PER_BLOCK), Q4_THREADS, 0, m->stream>>>(
-            m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, m->k6rot, o);
+        if (kg)
+            q4_kg_kernel<<<(unsigned)cdiv(m->nq, Q4_ELEMS_PER_BLOCK), Q4_THREADS, 0, m->stream>>>(
+                m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, du, o);
+        else
+            q4_k_kernel<<<(unsigned)cdiv(m->nq, Q4_ELEMS_PER_BLOCK), Q4_THREADS, 0, m->stream>>>(
+                m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, m->k6rot, o);
         CK(cudaGetLastError());
     }
     CK(cudaEventRecord(m->ev[1], m->stream));
     if (m->nt) {
-        o.slot = m->d_slot + m->slot_t3;
+        o.blk_slot = m->d_blk_slot + m->pair_t3;
         o.diag_slot = m->d_dslot + m->dslot_t3;
-        t3_k_kernel<<<(unsigned)cdiv(m->nt, T3_WARPS), T3_THREADS, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords,
-                                                                                   m->d_nodeR, m->k6rot, o);
+        if (kg)
+            t3_kg_kernel<<<(unsigned)cdiv(m->nt, 128), 128, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords, m->d_nodeR,
+                                                                            du, o);
+        else
+            t3_k_kernel<<<(unsigned)cdiv(m->nt, T3_WARPS), T3_THREADS, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords,
+                                                                                       m->d_nodeR, m->k6rot, o);
         CK(cudaGetLastError());
     }
     CK(cudaEventRecord(m->ev[2], m->stream));
     if (m->nb) {
-        o.slot = m->d_slot + m->slot_bar;
+        o.blk_slot = m->d_blk_slot + m->pair_bar;
         o.diag_slot = m->d_dslot + m->dslot_bar;
-        bar_k_kernel<<<(unsigned)cdiv(m->nb, 128), 128, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, o);
+        if (kg)
+            bar_kg_kernel<<<(unsigned)cdiv(m->nb, 128), 128, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR,
+                                                                             du, o);
+        else
+            bar_k_kernel<<<(unsigned)cdiv(m->nb, 128), 128, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, o);
         CK(cudaGetLastError());
     }
     CK(cudaEventRecord(m->ev[3], m->stream));
-    if (m->n_exc) {
-        expand_kernel<<<(unsigned)cdiv(m->n_exc, 256), 256, 0, m->stream>>>(m->n_exc, m->d_exc_q, m->d_exc_src, m->d_exc_w,
-                                                                           m->d_exc_raw, m->d_staging);
-        CK(cudaGetLastError());
-    }
+    return JFG_OK;
+}
+
+jfg_status launch_reduce(jfg_model *m, double *nz, double *ddiag) {
+    if (m->n_xkey)
+        exc_reduce_kernel<<<(unsigned)cdiv(m->n_xkey, 256), 256, 0, m->stream>>>(m->n_xkey, m->d_x_seg, m->d_x_src, m->d_x_w,
+                                                                                 m->d_exc_raw, m->d_x_pos, nz);
+    CK(cudaGetLastError());
     CK(cudaEventRecord(m->ev[4], m->stream));
-    if (m->n_upper)
-        reduce_kernel<<<(unsigned)cdiv(m->n_upper, 256), 256, 0, m->stream>>>(m->n_upper, m->d_seg, m->d_staging, m->d_posA,
-                                                                             m->d_posB, nz);
+    if (m->n_blk)
+        block_reduce_kernel<<<(unsigned)cdiv(m->n_blk * 36, 288), 288, 0, m->stream>>>(
+            m->n_blk, m->d_blk_seg, m->d_staging, m->d_blk_A, m->d_blk_B, m->d_blk_offAB, m->d_blk_offBA, m->d_rowptr, nz);
     CK(cudaGetLastError());
     CK(cudaEventRecord(m->ev[5], m->stream));
     if (ddiag)
@@ -888,51 +1114,26 @@ jfg_status launch_k(jfg_model *m, double *nz, double *dmax, double *ddiag) {
     return JFG_OK;
 }
 
+jfg_status begin_set(jfg_model *m, int kind);
+
+jfg_status launch_k(jfg_model *m, double *nz, double *dmax, double *ddiag) {
+    jfg_status st = begin_set(m, 0);
+    if (st) return st;
+    if (dmax) CK(cudaMemsetAsync(dmax, 0, sizeof(double), m->stream));
+    st = launch_elements(m, false, nullptr, dmax, ddiag);
+    if (st) return st;
+    return launch_reduce(m, nz, ddiag);
+}
+
 jfg_status launch_kg(jfg_model *m, const double *du, double *nz) {
     if (m->bar_offsets)
         return fail(m, JFG_ERR_REFERENCE_RAISES,
                     "assemble_geometric_stiffness raises BoundsError for CBAR/CBEAM with offsets (assembly.jl:6326)");
-    jfg_status bst = begin_set(m, 1);
-    if (bst) return bst;
-    ElemOut o;
-    o.staging = m->d_staging;
-    o.exc_raw = m->d_exc_raw;
-    o.diag_staging = nullptr;
-    o.diag_slot = nullptr;
-    o.maxabs = nullptr;
-    CK(cudaEventRecord(m->ev[0], m->stream));
-    if (m->nq) {
-        o.slot = m->d_slot + m->slot_q4;
-        q4_kg_kernel<<<(unsigned)cdiv(m->nq, Q4_ELEMS_PER_BLOCK), Q4_THREADS, 0, m->stream>>>(
-            m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, du, o);
-        CK(cudaGetLastError());
-    }
-    CK(cudaEventRecord(m->ev[1], m->stream));
-    if (m->nt) {
-        o.slot = m->d_slot + m->slot_t3;
-        t3_kg_kernel<<<(unsigned)cdiv(m->nt, 128), 128, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords, m->d_nodeR, du, o);
-        CK(cudaGetLastError());
-    }
-    CK(cudaEventRecord(m->ev[2], m->stream));
-    if (m->nb) {
-        o.slot = m->d_slot + m->slot_bar;
-        bar_kg_kernel<<<(unsigned)cdiv(m->nb, 128), 128, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, du, o);
-        CK(cudaGetLastError());
-    }
-    CK(cudaEventRecord(m->ev[3], m->stream));
-    if (m->n_exc) {
-        expand_kernel<<<(unsigned)cdiv(m->n_exc, 256), 256, 0, m->stream>>>(m->n_exc, m->d_exc_q, m->d_exc_src, m->d_exc_w,
-                                                                           m->d_exc_raw, m->d_staging);
-        CK(cudaGetLastError());
-    }
-    CK(cudaEventRecord(m->ev[4], m->stream));
-    if (m->n_upper)
-        reduce_kernel<<<(unsigned)cdiv(m->n_upper, 256), 256, 0, m->stream>>>(m->n_upper, m->d_seg, m->d_staging, m->d_posA,
-                                                                             m->d_posB, nz);
-    CK(cudaGetLastError());
-    CK(cudaEventRecord(m->ev[5], m->stream));
-    CK(cudaEventRecord(m->ev[6], m->stream));
-    return JFG_OK;
+    jfg_status st = begin_set(m, 1);
+    if (st) return st;
+    st = launch_elements(m, true, du, nullptr, nullptr);
+    if (st) return st;
+    return launch_reduce(m, nz, nullptr);
 }
 
 // Complete one event set: per-kernel times into the accumulators and "last".
@@ -1081,12 +1282,12 @@ jfg_status jfg_kernel_timing(jfg_model *m, double *ms6) {
 
 jfg_status jfg_model_stats(jfg_model *m, int64_t *out8) {
     if (!m || !out8) return JFG_ERR_INVALID;
-    out8[0] = m->n_contrib;               // staging values per assembly
-    out8[1] = m->n_upper;                 // unique upper-triangle nonzeros
+    out8[0] = 36 * m->n_blk_contrib;      // staging values per assembly
+    out8[1] = m->n_blk;                   // unique global node-pair blocks
     out8[2] = m->nnz;                     // CSC nonzeros
-    out8[3] = m->n_exc;                   // constraint-expanded contributions
-    out8[4] = m->n_exc_raw;               // raw values of constraint-touching elements
-    out8[5] = m->n_slots;                 // packed element entries (scatter-map length)
+    out8[3] = m->n_xcontrib;              // constraint-expanded contributions
+    out8[4] = 36 * m->n_xpair;            // raw values of constraint-touching pairs
+    out8[5] = m->n_pairs;                 // element node pairs (scatter-map length)
     out8[6] = m->n_dcontrib;              // element diagonal entries (orig_diag map)
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);

@@ -174,18 +174,19 @@ class GpuModel:
     def kernel_timing(self) -> dict:
         ms = np.zeros(6)
         self._check(self.L.jfg_kernel_timing(self.h, _ptr(ms, _pd)))
-        return dict(zip(("quad4", "tria3", "bar", "expand", "reduce", "diag"), ms.tolist()))
+        return dict(zip(("quad4", "tria3", "bar", "dof_reduce", "block_reduce", "diag"), ms.tolist()))
 
     def timing_accumulated(self, kind: str, reset: bool = True):
         """Summed per-kernel ms and call count of 'k' or 'kg' assemblies."""
         ms = np.zeros(6); n = C.c_int64()
         self._check(self.L.jfg_timing_accumulated(self.h, 0 if kind == "k" else 1, _ptr(ms, _pd), C.byref(n), int(reset)))
-        return dict(zip(("quad4", "tria3", "bar", "expand", "reduce", "diag"), ms.tolist())), int(n.value)
+        return dict(zip(("quad4", "tria3", "bar", "dof_reduce", "block_reduce", "diag"), ms.tolist())), int(n.value)
 
     def stats(self) -> dict:
         out = np.zeros(8, np.int64)
         self._check(self.L.jfg_model_stats(self.h, _ptr(out, _pi64)))
-        keys = ("n_contrib", "n_upper", "nnz", "n_exc", "n_exc_raw", "n_slots", "n_diag", "device_bytes_in_use")
+        keys = ("staging_values", "n_blocks", "nnz", "dof_contribs", "dof_raw_values", "element_pairs", "n_diag",
+                "device_bytes_in_use")
         return dict(zip(keys, (int(x) for x in out)))
 
     def constraint_map(self):

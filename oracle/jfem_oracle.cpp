@@ -704,6 +704,9 @@ int check_predicates(const jfg_model_desc *d, std::string &msg) {
         if (!(d->quad4_prop[JFG_SHELL_PROP * e] > 0.0) || !(d->quad4_prop[JFG_SHELL_PROP * e + 1] > 0.0)) { msg = "shell thickness and E must be positive"; return JFG_ERR_INVALID; }
         for (int k = 0; k < 4; ++k)
             if (n[k] < 0 || n[k] >= d->n_nodes) { msg = "quad4 node index out of range"; return JFG_ERR_INVALID; }
+        for (int a = 0; a < 4; ++a)
+            for (int b = a + 1; b < 4; ++b)
+                if (n[a] == n[b]) { msg = "CQUAD4 with a repeated node"; return JFG_ERR_INVALID; }
         if (!q4_is_flat(d->coords + 3 * n[0], d->coords + 3 * n[1], d->coords + 3 * n[2], d->coords + 3 * n[3])) {
             msg = "non-flat CQUAD4 (warp >= 1e-6 of the diagonal) leaves the flat default branch (assembly.jl:2824-2840)";
             return JFG_ERR_UNSUPPORTED;
@@ -713,6 +716,8 @@ int check_predicates(const jfg_model_desc *d, std::string &msg) {
         if (!(d->tria3_prop[JFG_SHELL_PROP * e] > 0.0) || !(d->tria3_prop[JFG_SHELL_PROP * e + 1] > 0.0)) { msg = "shell thickness and E must be positive"; return JFG_ERR_INVALID; }
         for (int k = 0; k < 3; ++k)
             if (d->tria3_nodes[3 * e + k] < 0 || d->tria3_nodes[3 * e + k] >= d->n_nodes) { msg = "tria3 node index out of range"; return JFG_ERR_INVALID; }
+        const int32_t *tn = d->tria3_nodes + 3 * e;
+        if (tn[0] == tn[1] || tn[0] == tn[2] || tn[1] == tn[2]) { msg = "CTRIA3 with a repeated node"; return JFG_ERR_INVALID; }
     }
     for (int64_t e = 0; e < d->n_bar; ++e) {
         for (int k = 0; k < 2; ++k)

@@ -110,10 +110,12 @@ def test_device_api_matches_host_api(cuda_device):
         ddg = torch.empty(g.ndof, dtype=torch.float64, device="cuda")
         dmx = torch.zeros(1, dtype=torch.float64, device="cuda")
         du = torch.from_numpy(u).cuda()
-        g.set_stream(torch.cuda.current_stream().cuda_stream)
+        s = torch.cuda.Stream()
+        torch.cuda.synchronize()
+        g.set_stream(s.cuda_stream)
         g.assemble_k_device(dnz.data_ptr(), dmx.data_ptr(), ddg.data_ptr())
         g.assemble_kg_device(du.data_ptr(), dkg.data_ptr())
-        torch.cuda.synchronize()
+        s.synchronize()
         assert np.array_equal(dnz.cpu().numpy(), nz)
         assert np.array_equal(dkg.cpu().numpy(), kg)
         assert np.array_equal(ddg.cpu().numpy(), dg) and float(dmx.item()) == mx
