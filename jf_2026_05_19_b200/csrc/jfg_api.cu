@@ -436,15 +436,21 @@ __global__ void __launch_bounds__(288) block_reduce_kernel(int64_t n_blk, const 
 }
 
 // Dof-level path: each CSC position touched by an RBE2-expanded entry sums
-// its weighted raw element values in a fixed order.
-__global__ void exc_reduce_kernel(int64_t n, const int32_t *__restrict__ seg, const int32_t *__restrict__ src,
-                                  const double *__restrict__ w, const double *__restrict__ raw,
-                                  const int64_t *__restrict__ pos, double *nz) {
-    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
+// its weighted raw element values.  One warp per position: lane l sums the
+// contributions l, l+32, ... and a fixed xor-butterfly combines the lanes, so
+// the order (and the result) is the same on every run even for the master
+// node's entries, which collect tens of thousands of contributions.
+__global__ void __launch_bounds__(256) exc_reduce_kernel(int64_t n, const int32_t *__restrict__ seg,
+                                                         const int32_t *__restrict__ src, const double *__restrict__ w,
+                                                         const double *__restrict__ raw, const int64_t *__restrict__ pos,
+                                                         double *nz) {
+    int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (t >= n) return;  // warp-uniform
     double s = 0.0;
-    for (int32_t q = seg[t]; q < seg[t + 1]; ++q) s += w[q] * raw[src[q]];
-    nz[pos[t]] = s;
+    for (int32_t q = seg[t] + lane; q < seg[t + 1]; q += 32) s += w[q] * raw[src[q]];
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) nz[pos[t]] = s;
 }
 
 __global__ void diag_reduce_kernel(int64_t ndof, const int32_t *__restrict__ seg, const double *__restrict__ st, double *out) {
@@ -1098,7 +1104,7 @@ jfg_status launch_elements(jfg_model *m, bool kg, const double *du, double *dmax
 
 jfg_status launch_reduce(jfg_model *m, double *nz, double *ddiag) {
     if (m->n_xkey)
-        exc_reduce_kernel<<<(unsigned)cdiv(m->n_xkey, 256), 256, 0, m->stream>>>(m->n_xkey, m->d_x_seg, m->d_x_src, m->d_x_w,
+        exc_reduce_kernel<<<(unsigned)cdiv(m->n_xkey * 32, 256), 256, 0, m->stream>>>(m->n_xkey, m->d_x_seg, m->d_x_src, m->d_x_w,
                                                                                  m->d_exc_raw, m->d_x_pos, nz);
     CK(cudaGetLastError());
     CK(cudaEventRecord(m->ev[4], m->stream));
@@ -1306,3 +1312,4 @@ jfg_status jfg_last_timing(jfg_model *m, double *element_ms, double *reduce_ms, 
 }
 
 }  // extern "C"
+

@@ -193,3 +193,30 @@ def test_barrel_load_factors_match(cuda_device):
         Kg_ = to_csc(cp, rv, g.assemble_k()[0], m.ndof)
         lam_g = load_factors(Kg_, to_csc(cp, rv, g.assemble_kg(u), m.ndof), free, k=6, sigma=0.0)
     assert np.all(np.abs(lam_g - lam_o) <= LAMBDA_TOL * np.abs(lam_o))
+
+
+def test_reference_interface_mirror(cuda_device):
+    """assemble_stiffness / assemble_geometric_stiffness on a reference-style model dictionary."""
+    from jf_2026_05_19_b200 import solver
+    m = DECKS["barrel_small"]
+    model = solver.model_dict_from_arrays(m)
+    K, id_map, X, ndof, node_R, mx, rbe3_map, snorm, diag = solver.assemble_stiffness(model, membrane_incomp=False)
+    ocp, orv, onz, omx, odg = O.assemble_k(m)
+    Kc = K.tocsc()
+    assert np.array_equal(Kc.indptr + 1, ocp) and np.array_equal(Kc.indices + 1, orv)
+    assert rowmax_rel_err(ocp, onz, Kc.data) <= ROW_TOL and abs(mx - omx) <= 1e-12 * omx
+    assert ndof == m.ndof and snorm == {} and len(rbe3_map) == 72 * 6
+    u = decks.smooth_displacement(m, seed=5)
+    Kg = solver.assemble_geometric_stiffness(model, id_map, X, node_R, ndof, u, snorm, rbe3_map).tocsc()
+    _, _, ognz = O.assemble_kg(m, u)
+    assert rowmax_rel_err(ocp, ognz, Kg.data) <= ROW_TOL
+    # a thickness update in the dictionary is picked up (handle reused, properties updated)
+    for p in model["PSHELLs"].values():
+        p["T"] *= 1.5
+    K2 = solver.assemble_stiffness(model)[0].tocsc()
+    m2 = m.with_thickness(m.q4_prop[:, 0] * 1.5, m.t3_prop[:, 0] * 1.5)
+    _, _, onz2, _, _ = O.assemble_k(m2)
+    assert rowmax_rel_err(ocp, onz2, K2.data) <= ROW_TOL
+    with pytest.raises(NotImplementedError):
+        solver.assemble_stiffness(model, shear_center_only=True)
+    solver.release()
