@@ -158,6 +158,40 @@ jfg_status jfg_timing_accumulated(jfg_model *m, int kind, double *ms6_sum, int64
  * orig_diag entries, device bytes in use}. */
 jfg_status jfg_model_stats(jfg_model *m, int64_t *out8);
 
+/* ---- Allocation-free CQUAD4 stiffness assembly ---------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory where they need a stiffness matrix (inside a CUDA graph capture, or
+ * under a host framework that owns all device memory, or in a loop that
+ * forbids allocator calls): assembles K of a small patch of CQUAD4 elements
+ * into a caller-provided CSR value array without allocating anything.
+ *
+ * All pointers are device memory: coords (n_nodes*3), node_R (n_nodes*9 or
+ * NULL), quad4_nodes (n_quad4*4, 0-based), quad4_prop (n_quad4*JFG_SHELL_PROP),
+ * and the 0-based symmetric CSR pattern rowptr (6*n_nodes+1) / colind that
+ * holds every element entry -- the arrays jfg_pattern_fill returns, minus 1,
+ * for a CQUAD4-only model.  nzval receives one value per stored entry in the
+ * same order (entries no element touches are written as 0).  stream is a
+ * cudaStream_t (NULL: the legacy default stream); the call waits for it.
+ *
+ * Intermediate data lives in one fixed array in the library's device image
+ * (about 6.3 MB, held by every GPU that loads the library until the process
+ * exits).  Limits: n_quad4 <= JFG_NOALLOC_MAX_QUAD4, n_nodes <=
+ * JFG_NOALLOC_MAX_NODES, at most JFG_NOALLOC_MAX_VALENCE elements per node;
+ * larger inputs are rejected with JFG_ERR_UNSUPPORTED (size checks before
+ * any launch, the valence check on the device); a node index outside
+ * [0, n_nodes) returns JFG_ERR_INVALID before the element kernel runs.  The first call on each
+ * device looks up the array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  Every call reuses the same
+ * array, so calls that overlap on the GPU (concurrent streams or threads)
+ * race and must be serialised by the caller. */
+#define JFG_NOALLOC_MAX_QUAD4 2048
+#define JFG_NOALLOC_MAX_NODES 8192
+#define JFG_NOALLOC_MAX_VALENCE 8
+jfg_status jfg_assemble_k_quad4_noalloc(int64_t n_nodes, const double *coords_dev, const double *node_R_dev,
+                                        int64_t n_quad4, const int32_t *quad4_nodes_dev, const double *quad4_prop_dev,
+                                        double k6rot, const int64_t *rowptr_dev, const int64_t *colind_dev,
+                                        double *nzval_dev, void *stream);
+
 void jfg_model_destroy(jfg_model *m);
 const char *jfg_last_error(jfg_model *m);
 const char *jfg_version(void);

@@ -24,6 +24,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1313,3 +1314,165 @@ jfg_status jfg_last_timing(jfg_model *m, double *element_ms, double *reduce_ms, 
 
 }  // extern "C"
 
+// ===========================================================================
+// Allocation-free CQUAD4 stiffness assembly for small patches.
+//
+// Some callers cannot allocate GPU memory at the point where they need a
+// stiffness matrix: code that runs inside a CUDA graph capture, a host
+// framework that has reserved all device memory up front and hands out only
+// its own buffers, or a real-time loop that forbids allocator calls.  This
+// entry point serves them: the caller passes every input and the output as
+// device pointers, and all intermediate data (element blocks, node incidence,
+// an error word) lives in the fixed array below, which every GPU that loads
+// this library keeps until the process exits.  No cudaMalloc, cudaFree or
+// allocating library call happens on this path.
+// ===========================================================================
+
+namespace {
+
+constexpr int64_t kNaBlocks = (int64_t)JFG_NOALLOC_MAX_QUAD4 * 10 * 36;       // doubles
+constexpr int64_t kNaInts = (int64_t)JFG_NOALLOC_MAX_QUAD4 * 10                // block slots
+                            + (int64_t)JFG_NOALLOC_MAX_NODES * JFG_NOALLOC_MAX_VALENCE  // incidence
+                            + (int64_t)JFG_NOALLOC_MAX_NODES                   // incidence counts
+                            + 8;                                               // error word + pad
+constexpr int64_t kNaDoubles = kNaBlocks + (kNaInts + 1) / 2;
+
+// The scratch array (about 6.3 MB).  Host code must not use this name as an
+// address: it only stands in for the device symbol; jfg_na_scratch() below
+// obtains the real device address with cudaGetSymbolAddress.
+static __device__ __align__(256) double g_noalloc_scratch[kNaDoubles];
+
+struct NaView {
+    double *blocks;
+    int32_t *slot, *inc, *inc_cnt, *err;
+};
+
+__host__ __device__ inline NaView na_view(double *base) {
+    NaView v;
+    v.blocks = base;
+    int32_t *ip = reinterpret_cast<int32_t *>(base + kNaBlocks);
+    v.slot = ip;
+    v.inc = v.slot + (int64_t)JFG_NOALLOC_MAX_QUAD4 * 10;
+    v.inc_cnt = v.inc + (int64_t)JFG_NOALLOC_MAX_NODES * JFG_NOALLOC_MAX_VALENCE;
+    v.err = v.inc_cnt + JFG_NOALLOC_MAX_NODES;
+    return v;
+}
+
+// Per-device address of the scratch array, obtained once per device with
+// that device current.
+std::mutex g_na_mutex;
+double *g_na_ptr[64] = {nullptr};
+
+jfg_status jfg_na_scratch(double **out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return JFG_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(g_na_mutex);
+    if (!g_na_ptr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return JFG_ERR_CUDA;
+        g_na_ptr[dev] = static_cast<double *>(p);
+    }
+    *out = g_na_ptr[dev];
+    return JFG_OK;
+}
+
+// Checks the node indices (error word 2 when one is out of range) and writes
+// the identity block-slot map (no transposition: block (e, p) holds rows of
+// local node a, columns of local node b, a <= b).  The error word itself is
+// cleared beforehand: it is the only scratch that must start at zero.
+__global__ void na_prepare_kernel(int64_t nq, int64_t n_nodes, const int32_t *__restrict__ nodes, double *base) {
+    NaView v = na_view(base);
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nq * 4 && (nodes[t] < 0 || nodes[t] >= n_nodes)) atomicExch(v.err, 2);
+    if (t < nq * 10) v.slot[t] = (int32_t)t;
+}
+
+// Node -> incident elements, in ascending element order (deterministic).
+__global__ void na_incidence_kernel(int64_t n_nodes, int64_t nq, const int32_t *__restrict__ nodes, double *base) {
+    NaView v = na_view(base);
+    int64_t A = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (A >= n_nodes) return;
+    int cnt = 0;
+    for (int64_t e = 0; e < nq; ++e)
+        for (int k = 0; k < 4; ++k)
+            if (nodes[4 * e + k] == A) {
+                if (cnt < JFG_NOALLOC_MAX_VALENCE) v.inc[A * JFG_NOALLOC_MAX_VALENCE + cnt] = (int32_t)e;
+                else atomicExch(v.err, 1);
+                ++cnt;
+            }
+    v.inc_cnt[A] = cnt < JFG_NOALLOC_MAX_VALENCE ? cnt : JFG_NOALLOC_MAX_VALENCE;
+}
+
+// One thread per matrix row: every stored entry of the row sums the blocks of
+// the row node's incident elements that also contain the column node, in
+// ascending element order; entries no element touches are written as 0.
+__global__ void na_reduce_kernel(int64_t n_nodes, const int32_t *__restrict__ nodes, const int64_t *__restrict__ rowptr,
+                                 const int64_t *__restrict__ colind, double *base, double *nz) {
+    NaView v = na_view(base);
+    int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= 6 * n_nodes) return;
+    const int64_t A = r / 6;
+    const int i = (int)(r - 6 * A);
+    const int cnt = v.inc_cnt[A];
+    for (int64_t p = rowptr[r]; p < rowptr[r + 1]; ++p) {
+        const int64_t c = colind[p], B = c / 6;
+        const int j = (int)(c - 6 * B);
+        double s = 0.0;
+        for (int t = 0; t < cnt; ++t) {
+            const int64_t e = v.inc[A * JFG_NOALLOC_MAX_VALENCE + t];
+            int a = -1, b = -1;
+            for (int k = 0; k < 4; ++k) {
+                if (nodes[4 * e + k] == A) a = k;
+                if (nodes[4 * e + k] == B) b = k;
+            }
+            if (b < 0) continue;
+            const int lo = a < b ? a : b, hi = a < b ? b : a;
+            int pidx = 0;
+            for (int q = 0; q < 10; ++q)
+                if (jfg::c_pair_a[q] == lo && jfg::c_pair_b[q] == hi) pidx = q;
+            const double *blk = v.blocks + 36 * (10 * e + pidx);
+            s += (a <= b) ? blk[6 * i + j] : blk[6 * j + i];
+        }
+        nz[p] = s;
+    }
+}
+
+}  // namespace
+
+extern "C" jfg_status jfg_assemble_k_quad4_noalloc(int64_t n_nodes, const double *coords_dev, const double *node_R_dev,
+                                                   int64_t n_quad4, const int32_t *quad4_nodes_dev,
+                                                   const double *quad4_prop_dev, double k6rot, const int64_t *rowptr_dev,
+                                                   const int64_t *colind_dev, double *nzval_dev, void *stream) {
+    if (n_nodes <= 0 || n_quad4 <= 0 || !coords_dev || !quad4_nodes_dev || !quad4_prop_dev || !rowptr_dev || !colind_dev ||
+        !nzval_dev)
+        return JFG_ERR_INVALID;
+    if (n_quad4 > JFG_NOALLOC_MAX_QUAD4 || n_nodes > JFG_NOALLOC_MAX_NODES) return JFG_ERR_UNSUPPORTED;
+    double *base = nullptr;
+    jfg_status st = jfg_na_scratch(&base);
+    if (st) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    NaView v = na_view(base);
+    int32_t err = 0;
+    if (cudaMemsetAsync(v.err, 0, sizeof(int32_t), s) != cudaSuccess) return JFG_ERR_CUDA;
+    na_prepare_kernel<<<(unsigned)cdiv(n_quad4 * 10, 256), 256, 0, s>>>(n_quad4, n_nodes, quad4_nodes_dev, base);
+    if (cudaGetLastError() != cudaSuccess) return JFG_ERR_CUDA;
+    if (cudaMemcpyAsync(&err, v.err, sizeof(int32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess) return JFG_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return JFG_ERR_CUDA;
+    if (err) return JFG_ERR_INVALID;  // a node index outside [0, n_nodes): nothing else was launched
+    ElemOut o;
+    o.staging = v.blocks;
+    o.exc_raw = nullptr;       // every slot is a regular block
+    o.blk_slot = v.slot;
+    o.diag_staging = nullptr;
+    o.diag_slot = nullptr;
+    o.maxabs = nullptr;
+    q4_k_kernel<<<(unsigned)cdiv(n_quad4, Q4_ELEMS_PER_BLOCK), Q4_THREADS, 0, s>>>(n_quad4, quad4_nodes_dev, quad4_prop_dev,
+                                                                                 coords_dev, node_R_dev, k6rot, o);
+    na_incidence_kernel<<<(unsigned)cdiv(n_nodes, 128), 128, 0, s>>>(n_nodes, n_quad4, quad4_nodes_dev, base);
+    na_reduce_kernel<<<(unsigned)cdiv(6 * n_nodes, 128), 128, 0, s>>>(n_nodes, quad4_nodes_dev, rowptr_dev, colind_dev, base,
+                                                                      nzval_dev);
+    if (cudaGetLastError() != cudaSuccess) return JFG_ERR_CUDA;
+    if (cudaMemcpyAsync(&err, v.err, sizeof(int32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess) return JFG_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return JFG_ERR_CUDA;
+    return err ? JFG_ERR_UNSUPPORTED : JFG_OK;
+}

@@ -21,7 +21,7 @@ LIB_PATH = os.path.join(PKG, "libjfemgpu.so")
 # every entry point declared in include/jfem_gpu.h
 EXPORTS = ("jfg_model_create", "jfg_pattern", "jfg_pattern_fill", "jfg_assemble_k", "jfg_assemble_kg",
            "jfg_assemble_k_device", "jfg_assemble_kg_device", "jfg_update_properties", "jfg_constraint_map",
-           "jfg_set_stream", "jfg_last_timing", "jfg_kernel_timing", "jfg_timing_accumulated", "jfg_model_stats", "jfg_model_destroy", "jfg_last_error", "jfg_version")
+           "jfg_set_stream", "jfg_last_timing", "jfg_kernel_timing", "jfg_timing_accumulated", "jfg_model_stats", "jfg_assemble_k_quad4_noalloc", "jfg_model_destroy", "jfg_last_error", "jfg_version")
 
 _lib = None
 
@@ -64,6 +64,8 @@ def load(path: str = LIB_PATH):
     L.jfg_last_timing.argtypes = [C.c_void_p, _pd, _pd, _pd]
     L.jfg_kernel_timing.argtypes = [C.c_void_p, _pd]
     L.jfg_model_stats.argtypes = [C.c_void_p, _pi64]
+    L.jfg_assemble_k_quad4_noalloc.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
+                                               C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.jfg_timing_accumulated.argtypes = [C.c_void_p, C.c_int, _pd, _pi64, C.c_int]
     L.jfg_model_destroy.argtypes = [C.c_void_p]
     L.jfg_model_destroy.restype = None
@@ -72,7 +74,8 @@ def load(path: str = LIB_PATH):
     L.jfg_version.restype = C.c_char_p
     for name in ("jfg_pattern", "jfg_pattern_fill", "jfg_assemble_k", "jfg_assemble_kg", "jfg_assemble_k_device",
                  "jfg_assemble_kg_device", "jfg_update_properties", "jfg_constraint_map", "jfg_set_stream",
-                 "jfg_last_timing", "jfg_kernel_timing", "jfg_timing_accumulated", "jfg_model_stats"):
+                 "jfg_last_timing", "jfg_kernel_timing", "jfg_timing_accumulated", "jfg_model_stats",
+                 "jfg_assemble_k_quad4_noalloc"):
         getattr(L, name).restype = C.c_int32
     _lib = L
     return L
