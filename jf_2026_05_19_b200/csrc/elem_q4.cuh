@@ -84,7 +84,8 @@ struct Q4KShared {
     int skip_macneal, bend_cond;
     double Kabm[8][4], Kbbm[16], Kabb[8][4], Kbbb[16];
     double Xm[4][8], Xb[4][8];
-    double D[4][12], Jp[4], Zinv[16], Y[4][12];
+    double D[4][12], Jp[4], Y[4][12];
+    MacNealZ mz;
 };
 
 struct Q4GShared {
@@ -238,7 +239,25 @@ __device__ __forceinline__ void write_pair_block(const ElemOut &o, int64_t e, in
     }
 }
 
-__global__ void __launch_bounds__(Q4_THREADS) q4_k_kernel(int64_t nq, const int32_t *__restrict__ nodes,
+// Write one 3x3 sub-block (bi, bj) of the node-pair block (a, b) of element
+// e; diagonal entries of diagonal pairs also go to the orig_diag staging.
+__device__ __forceinline__ void write_sub_block(const ElemOut &o, int64_t e, int32_t sl, int a, int b, int bi, int bj,
+                                                const double O[3][3], double &lmax, int ndof_e) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            double v = O[i][j];
+            lmax = fmax(lmax, fabs(v));
+            *blk_entry(o, sl, 3 * bi + i, 3 * bj + j) = v;
+        }
+    if (o.diag_staging && a == b && bi == bj) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) o.diag_staging[__ldg(o.diag_slot + e * ndof_e + 6 * a + 3 * bi + i)] = O[i][i];
+    }
+}
+
+__global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const int32_t *__restrict__ nodes,
                                                          const double *__restrict__ prop,
                                                          const double *__restrict__ coords,
                                                          const double *__restrict__ nodeR, double k6rot, ElemOut o) {
@@ -345,62 +364,26 @@ __global__ void __launch_bounds__(Q4_THREADS) q4_k_kernel(int64_t nq, const int3
     }
     __syncwarp();
 
-    // Phase 2: 4x4 inverses and MacNeal compliance.
-    if (valid && tl == 0) {
-        inv4_inplace(S.Kbbm);
-    } else if (valid && tl == 1) {
-        double mx = 0.0;
-        for (int i = 0; i < 16; ++i) mx = fmax(mx, fabs(S.Kbbb[i]));
-        S.bend_cond = mx > 0.0 ? 1 : 0;
-        if (S.bend_cond) inv4_inplace(S.Kbbb);
+    // Phase 2: the two 4x4 inverses (lanes 0 and 1 in one code path) and the
+    // MacNeal compliance factors (lane 2).
+    if (valid && tl < 2) {
+        double *M = tl == 0 ? S.Kbbm : S.Kbbb;
+        bool inv = true;
+        if (tl == 1) {
+            double mx = 0.0;
+            for (int i = 0; i < 16; ++i) mx = fmax(mx, fabs(M[i]));
+            S.bend_cond = mx > 0.0 ? 1 : 0;
+            inv = mx > 0.0;
+        }
+        if (inv) inv4_inplace(M);
     } else if (valid && tl == 2 && !S.skip_macneal) {
-        const Q4Geo &G = S.g;
-        double Dx = 0.5 * (G.lc[1][0] + G.lc[2][0] - G.lc[0][0] - G.lc[3][0]);
-        double Dy = 0.5 * (G.lc[2][1] + G.lc[3][1] - G.lc[0][1] - G.lc[1][1]);
-        double Dx2 = Dx * Dx, Dy2 = Dy * Dy;
-        double J11c = 0.25 * (-G.lc[0][0] + G.lc[1][0] + G.lc[2][0] - G.lc[3][0]);
-        double J12c = 0.25 * (-G.lc[0][1] + G.lc[1][1] + G.lc[2][1] - G.lc[3][1]);
-        double J21c = 0.25 * (-G.lc[0][0] - G.lc[1][0] + G.lc[2][0] + G.lc[3][0]);
-        double J22c = 0.25 * (-G.lc[0][1] - G.lc[1][1] + G.lc[2][1] + G.lc[3][1]);
-        double A_elem = 4.0 * fabs(J11c * J22c - J12c * J21c);
-        const double eps = 0.04;
-        double ap = eps / (eps + (1.0 - eps) * Dx2 / fmax(Dy2, 1e-30));
-        double bp = eps / (eps + (1.0 - eps) * Dy2 / fmax(Dx2, 1e-30));
-        double flex_x = 1.0 / fmax(fabs(S.Cb[0]), 1e-30), flex_y = 1.0 / fmax(fabs(S.Cb[4]), 1e-30);
-        double inv12A = 1.0 / (12.0 * A_elem);
-        const double zb = 0.65;
-        double zxu = zb * inv12A * Dx2 * flex_x, zxd = zb * inv12A * ap * Dx2 * flex_x;
-        double zyu = zb * inv12A * Dy2 * flex_y, zyd = zb * inv12A * bp * Dy2 * flex_y;
-        double Zb[16] = {zxu + zxd, zxu - zxd, 0, 0, zxu - zxd, zxu + zxd, 0, 0,
-                         0, 0, zyu + zyd, zyu - zyd, 0, 0, zyu - zyd, zyu + zyd};
-        double VGV[16];
-        const int comps[4] = {1, 1, 2, 2};
-        for (int i = 0; i < 4; ++i)
-            for (int j = 0; j < 4; ++j) {
-                double Jf = sqrt(2.0 * S.Jp[i]) * sqrt(2.0 * S.Jp[j]);
-                double v;
-                if (comps[i] == comps[j]) v = (i == j) ? Jf * (comps[i] == 1 ? S.Cs[0] : S.Cs[3]) : 0.0;
-                else v = 0.5 * Jf * S.Cs[1];
-                VGV[4 * i + j] = v;
-            }
-        for (int i = 0; i < 4; ++i)
-            if (VGV[5 * i] < 1e-30) VGV[5 * i] = 1e-30;
-        double Zs[16];
-        for (int i = 0; i < 4; ++i)
-            for (int j = 0; j < 4; ++j) Zs[4 * i + j] = 0.5 * (VGV[4 * i + j] + VGV[4 * j + i]);
-        inv4_inplace(Zs);
-        double Zt[16];
-        for (int i = 0; i < 4; ++i)
-            for (int j = 0; j < 4; ++j) Zt[4 * i + j] = 0.5 * (Zs[4 * i + j] + Zs[4 * j + i]) + Zb[4 * i + j];
-        for (int i = 0; i < 4; ++i)
-            for (int j = 0; j < 4; ++j) S.Zinv[4 * i + j] = 0.5 * (Zt[4 * i + j] + Zt[4 * j + i]);
-        inv4_inplace(S.Zinv);
+        S.mz = macneal_z(S.g.lc, S.Jp, S.Cs[0], S.Cb[0], S.Cb[4]);
     }
     __syncwarp();
 
-    // Phase 3: X = Kbb^-1 Kab' for both condensations, Y = Z^-1 D.
+    // Phase 3: X = Kbb^-1 Kab' for both condensations, Y = Z \ D by columns.
     if (valid) {
-        for (int w = tl; w < 112; w += Q4_TEAM) {
+        for (int w = tl; w < 76; w += Q4_TEAM) {
             if (w < 32) {
                 int l = w >> 3, r = w & 7;
                 double s = 0.0;
@@ -412,12 +395,11 @@ __global__ void __launch_bounds__(Q4_THREADS) q4_k_kernel(int64_t nq, const int3
                 if (S.bend_cond)
                     for (int q = 0; q < 4; ++q) s += S.Kbbb[4 * l + q] * S.Kabb[r][q];
                 S.Xb[l][r] = s;
-            } else {
-                int l = (w - 64) / 12, j = (w - 64) % 12;
-                double s = 0.0;
-                if (!S.skip_macneal)
-                    for (int q = 0; q < 4; ++q) s += S.Zinv[4 * l + q] * S.D[q][j];
-                S.Y[l][j] = s;
+            } else if (!S.skip_macneal) {
+                int j = w - 64;
+                double d[4] = {S.D[0][j], S.D[1][j], S.D[2][j], S.D[3][j]}, y[4];
+                macneal_y(S.mz, d, y);
+                for (int l = 0; l < 4; ++l) S.Y[l][j] = y[l];
             }
         }
     }
@@ -444,12 +426,19 @@ __global__ void __launch_bounds__(Q4_THREADS) q4_k_kernel(int64_t nq, const int3
             q4_bend_col(S.g, g, a, 0, ba[0]); q4_bend_col(S.g, g, a, 1, ba[1]);
             q4_bend_col(S.g, g, b, 0, bb[0]); q4_bend_col(S.g, g, b, 1, bb[1]);
 #pragma unroll
-            for (int al = 0; al < 2; ++al)
+            for (int be = 0; be < 2; ++be) {
+                double cm[3], cb[3];
 #pragma unroll
-                for (int be = 0; be < 2; ++be) {
-                    L[al][be] += wd * quad_form(ma[al], S.Cm, mb[be]);
-                    L[3 + al][3 + be] += wd * quad_form(ba[al], S.Cb, bb[be]);
+                for (int r = 0; r < 3; ++r) {
+                    cm[r] = wd * (S.Cm[3 * r] * mb[be][0] + S.Cm[3 * r + 1] * mb[be][1] + S.Cm[3 * r + 2] * mb[be][2]);
+                    cb[r] = wd * (S.Cb[3 * r] * bb[be][0] + S.Cb[3 * r + 1] * bb[be][1] + S.Cb[3 * r + 2] * bb[be][2]);
                 }
+#pragma unroll
+                for (int al = 0; al < 2; ++al) {
+                    L[al][be] += ma[al][0] * cm[0] + ma[al][1] * cm[1] + ma[al][2] * cm[2];
+                    L[3 + al][3 + be] += ba[al][0] * cb[0] + ba[al][1] * cb[1] + ba[al][2] * cb[2];
+                }
+            }
             // drilling: Bd = [0.5 dN/dy, -0.5 dN/dx, N] on (u, v, theta_z)
             double da[3] = {0.5 * S.g.dNy[g][a], -0.5 * S.g.dNx[g][a], q4_N(a, r, s)};
             double db[3] = {0.5 * S.g.dNy[g][b], -0.5 * S.g.dNx[g][b], q4_N(b, r, s)};
@@ -485,8 +474,9 @@ __global__ void __launch_bounds__(Q4_THREADS) q4_k_kernel(int64_t nq, const int3
                 L[al][be] -= sm;
                 if (S.bend_cond) L[3 + al][3 + be] -= sb;
             }
-        // T'KT on the node pair
-        double Gb[6][6];
+        // T'KT on the node pair, one 3x3 sub-block at a time (keeps the
+        // register footprint to the local 6x6 block)
+        const int32_t sl = __ldg(o.blk_slot + e * 10 + tl);
 #pragma unroll
         for (int bi = 0; bi < 2; ++bi)
 #pragma unroll
@@ -497,12 +487,8 @@ __global__ void __launch_bounds__(Q4_THREADS) q4_k_kernel(int64_t nq, const int3
 #pragma unroll
                     for (int j = 0; j < 3; ++j) Ls[i][j] = L[3 * bi + i][3 * bj + j];
                 rot_block(S.g.Q[a], Ls, S.g.Q[b], O);
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) Gb[3 * bi + i][3 * bj + j] = O[i][j];
+                write_sub_block(o, e, sl, a, b, bi, bj, O, lmax, 24);
             }
-        write_pair_block<4, 10>(o, e, tl, a, b, Gb, lmax);
     }
     if (o.maxabs) {
         for (int off = 16; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
@@ -652,13 +638,13 @@ __global__ void __launch_bounds__(Q4_THREADS) q4_kg_kernel(int64_t nq, const int
         }
         double O[3][3];
         rot_block(S.g.Q[a], M, S.g.Q[b], O);
-        double Gb[6][6];
-#pragma unroll
-        for (int i = 0; i < 6; ++i)
-#pragma unroll
-            for (int j = 0; j < 6; ++j) Gb[i][j] = (i < 3 && j < 3) ? O[i][j] : 0.0;
+        const int32_t sl = __ldg(o.blk_slot + e * 10 + tl);
+        const double Z[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
         double lmax = 0.0;
-        write_pair_block<4, 10>(o, e, tl, a, b, Gb, lmax);
+        write_sub_block(o, e, sl, a, b, 0, 0, O, lmax, 24);
+        write_sub_block(o, e, sl, a, b, 0, 1, Z, lmax, 24);
+        write_sub_block(o, e, sl, a, b, 1, 0, Z, lmax, 24);
+        write_sub_block(o, e, sl, a, b, 1, 1, Z, lmax, 24);
     }
 }
 

@@ -1,12 +1,22 @@
 // elem_t3.cuh -- CTRIA3 stiffness (K) and differential stiffness (KG) kernels.
 //
-// K: one warp per element.  stiffness_tria3_matrices_generic
+// K: a team of 16 lanes per element, two teams per warp; each team
+// synchronises only its own lanes.  stiffness_tria3_matrices_generic
 // (src/FEMKernels.jl:7315-7385): CST membrane, plate block from the three
 // virtual quads of tria3_plate_macro_data (:7157-7209) -- each the plate
 // part (bending with twist correction + MacNeal shear, no bending
 // incompatible modes) of a default-kwarg stiffness_quad4_matrices -- summed
-// into a 21x21 system whose 12 internal dofs are condensed by an LU solve,
-// plus the centroidal Hughes-Brezzi drill; then T'KT (assembly.jl:3866-3955).
+// into a 21x21 system whose 12 internal dofs are condensed, plus the
+// centroidal Hughes-Brezzi drill; then T'KT (assembly.jl:3866-3955).
+//
+// Macro nodes: corners 0-2, edge midpoints 3 (0-1), 4 (1-2), 5 (2-0),
+// centroid 6.  No virtual quad holds two corners, so Kee is block diagonal
+// and every Kei entry comes from the one quad that holds the corner.  The
+// internal solve lu(Kii) \ Kie runs as Gauss-Jordan elimination with one row
+// of [Kii | Kie] per lane in registers: pivot choice, row positions and the
+// forward elimination are those of LU with partial pivoting (max |a_ik|,
+// first position on ties); eliminating above the pivot as well replaces the
+// back substitution.
 //
 // KG: one thread per element.  CST membrane resultant of stress_strain_tria3
 // (FEMKernels.jl:7391-7404) and geometric_stiffness_tria3's non-curvature
@@ -17,55 +27,75 @@
 
 namespace jfg {
 
+constexpr int T3_TEAM = 16;
+constexpr int T3_TEAMS_PER_WARP = 2;
 constexpr int T3_WARPS = 4;
 constexpr int T3_THREADS = 32 * T3_WARPS;
+constexpr int T3_ELEMS_PER_BLOCK = T3_TEAMS_PER_WARP * T3_WARPS;
 
+// virtual quads of tria3_plate_macro_data (TRIA3_MACRO_QUADS), macro node ids
+__host__ __device__ constexpr int t3_quad_node(int q, int k) {
+    return q == 0 ? (k == 0 ? 0 : k == 1 ? 3 : k == 2 ? 6 : 5)
+         : q == 1 ? (k == 0 ? 1 : k == 1 ? 4 : k == 2 ? 6 : 3)
+                  : (k == 0 ? 2 : k == 1 ? 5 : k == 2 ? 6 : 4);
+}
 __constant__ int c_t3_quads[3][4] = {{0, 3, 6, 5}, {1, 4, 6, 3}, {2, 5, 6, 4}};
 
 struct T3KShared {
     double p[3][3];
     double v[3][3];
-    double lc[3][2];
     double Q[3][9];
     double pts[7][2];
     double bv[3], cv[3], A;
-    double Cm[9], Cb[9], Cs[4], h, alpha_d;
-    int plate, skip_macneal;
-    double dNx[3][5][4], dNy[3][5][4], wdet[3][4];
-    double D[3][4][12], Jp[3][4], Zinv[3][16], Y[3][4][12];
-    double K[21][22];     // padded row stride
-    double X[12][9];      // condensation right-hand side / solution
-    int piv;
+    double Cm[9], Cb[9], cs, alpha_d;
+    int nd[3], plate, skip_macneal;
+    union {
+        struct {  // virtual-quad data (phases 2-4)
+            double dNx[3][5][4], dNy[3][5][4], wdet[3][4];
+            double D[3][4][12], Jp[3][4];
+            MacNealZ mz[3];
+        } q;
+        struct {  // condensation (phases 5-7)
+            double X[12][9];
+            double Kc[9][9];
+        } c;
+    } u;
+    double Pb[3][10][9];  // quad q, local node pair (a <= b): 3x3 over (w, theta_x, theta_y)
 };
 
 __global__ void __launch_bounds__(T3_THREADS) t3_k_kernel(int64_t nt, const int32_t *__restrict__ nodes,
                                                          const double *__restrict__ prop,
                                                          const double *__restrict__ coords,
                                                          const double *__restrict__ nodeR, double k6rot, ElemOut o) {
-    __shared__ T3KShared sh[T3_WARPS];
+    __shared__ T3KShared sh[T3_ELEMS_PER_BLOCK];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t e = (int64_t)blockIdx.x * T3_WARPS + warp;
-    if (e >= nt) return;  // whole warp exits together
-    T3KShared &S = sh[warp];
-    int32_t nd[3];
-    for (int k = 0; k < 3; ++k) nd[k] = __ldg(nodes + 3 * e + k);
-    if (lane < 3) {
-        for (int i = 0; i < 3; ++i) S.p[lane][i] = __ldg(coords + 3 * (int64_t)nd[lane] + i);
+    const int team = lane >> 4, tl = lane & 15;
+    const unsigned tm = 0xFFFFu << (16 * team);
+    const int64_t e = (int64_t)blockIdx.x * T3_ELEMS_PER_BLOCK + warp * T3_TEAMS_PER_WARP + team;
+    if (e >= nt) return;  // the whole team leaves; syncs below are team-local
+    T3KShared &S = sh[warp * T3_TEAMS_PER_WARP + team];
+
+    // Phase 0: connectivity and coordinates.
+    if (tl < 3) {
+        const int32_t n = __ldg(nodes + 3 * e + tl);
+        S.nd[tl] = n;
+        for (int i = 0; i < 3; ++i) S.p[tl][i] = __ldg(coords + 3 * (int64_t)n + i);
     }
-    __syncwarp();
-    if (lane == 0) {
+    __syncwarp(tm);
+    // Phase 1: frame, macro points, constitutive data (one lane).
+    if (tl == 0) {
         double v1[3], v2[3], v3[3];
         t3_frame(S.p[0], S.p[1], S.p[2], v1, v2, v3);
-        double c[3];
+        double c[3], lc[3][2];
         for (int i = 0; i < 3; ++i) c[i] = (S.p[0][i] + S.p[1][i] + S.p[2][i]) / 3.0;
         for (int k = 0; k < 3; ++k) {
             double d[3];
             sub3(S.p[k], c, d);
-            S.lc[k][0] = dot3(d, v1);
-            S.lc[k][1] = dot3(d, v2);
+            lc[k][0] = dot3(d, v1);
+            lc[k][1] = dot3(d, v2);
         }
         for (int i = 0; i < 3; ++i) { S.v[0][i] = v1[i]; S.v[1][i] = v2[i]; S.v[2][i] = v3[i]; }
-        double x[3] = {S.lc[0][0], S.lc[1][0], S.lc[2][0]}, y[3] = {S.lc[0][1], S.lc[1][1], S.lc[2][1]};
+        double x[3] = {lc[0][0], lc[1][0], lc[2][0]}, y[3] = {lc[0][1], lc[1][1], lc[2][1]};
         double A2 = x[0] * (y[1] - y[2]) + x[1] * (y[2] - y[0]) + x[2] * (y[0] - y[1]);
         double A = 0.5 * fabs(A2);
         S.A = A;
@@ -84,26 +114,27 @@ __global__ void __launch_bounds__(T3_THREADS) t3_k_kernel(int64_t nt, const int3
         for (int i = 0; i < 9; ++i) { S.Cm[i] = cm * base[i]; S.Cb[i] = cb * base[i]; }
         bool membrane_only = br <= 1e-12;
         double cs = membrane_only ? 0.0 : tst * h * Gs;
-        S.Cs[0] = cs; S.Cs[1] = 0.0; S.Cs[2] = 0.0; S.Cs[3] = cs;
-        S.h = h;
+        S.cs = cs;
         S.plate = (!membrane_only && A >= 1e-12) ? 1 : 0;
         S.skip_macneal = (h < 1e-30 || fabs(cs) < 1e-30) ? 1 : 0;
         double k6 = membrane_only ? 0.0 : k6rot;
         S.alpha_d = (k6 / 1e5) * Gs * h;  // G_ref = shear-material G (assembly.jl:2468)
     }
-    __syncwarp();
-    const bool degenerate = S.A < 1e-12;
-    if (lane < 3) {
-        const double *R = nodeR ? nodeR + 9 * (int64_t)nd[lane] : nullptr;
-        double Rl[9];
-        if (R)
-            for (int i = 0; i < 9; ++i) Rl[i] = __ldg(R + i);
-        node_block(S.v[0], S.v[1], S.v[2], R ? Rl : nullptr, S.Q[lane]);
-    }
-    if (S.plate) {
-        // virtual-quad Jacobians: lanes 3..17 -> (quad q, point g)
-        if (lane >= 3 && lane < 18) {
-            int q = (lane - 3) / 5, g = (lane - 3) % 5;
+    __syncwarp(tm);
+    const bool plate = S.plate != 0, macneal = plate && !S.skip_macneal;
+
+    // Phase 2: node blocks (items 0-2), virtual-quad Jacobians (3-17) and
+    // MacNeal strain-sampling rows (18-29), two items per lane.
+    for (int it = tl; it < 30; it += T3_TEAM) {
+        if (it < 3) {
+            const double *R = nodeR ? nodeR + 9 * (int64_t)S.nd[it] : nullptr;
+            double Rl[9];
+            if (R)
+                for (int i = 0; i < 9; ++i) Rl[i] = __ldg(R + i);
+            node_block(S.v[0], S.v[1], S.v[2], R ? Rl : nullptr, S.Q[it]);
+        } else if (!plate) {
+        } else if (it < 18) {
+            int q = (it - 3) / 5, g = (it - 3) % 5;
             double lq[4][2];
             for (int k = 0; k < 4; ++k) { lq[k][0] = S.pts[c_t3_quads[q][k]][0]; lq[k][1] = S.pts[c_t3_quads[q][k]][1]; }
             double r = 0.0, s = 0.0;
@@ -119,18 +150,16 @@ __global__ void __launch_bounds__(T3_THREADS) t3_k_kernel(int64_t nt, const int3
             double inv = 1.0 / det;
             double iJ11 = J22 * inv, iJ12 = -J12 * inv, iJ21 = -J21 * inv, iJ22 = J11 * inv;
             for (int k = 0; k < 4; ++k) {
-                S.dNx[q][g][k] = iJ11 * dNr[k] + iJ12 * dNs[k];
-                S.dNy[q][g][k] = iJ21 * dNr[k] + iJ22 * dNs[k];
+                S.u.q.dNx[q][g][k] = iJ11 * dNr[k] + iJ12 * dNs[k];
+                S.u.q.dNy[q][g][k] = iJ21 * dNr[k] + iJ22 * dNs[k];
             }
-            if (g < 4) { double a = fabs(det); S.wdet[q][g] = a < 1e-12 ? 1e-12 : a; }
-        } else if (lane >= 18 && lane < 30) {
-            // MacNeal strain-sampling rows: (quad q, sample point sp)
-            int q = (lane - 18) >> 2, sp = (lane - 18) & 3;
+            if (g < 4) { double a = fabs(det); S.u.q.wdet[q][g] = a < 1e-12 ? 1e-12 : a; }
+        } else {
+            int q = (it - 18) >> 2, sp = (it - 18) & 3;
             double lq[4][2];
             for (int k = 0; k < 4; ++k) { lq[k][0] = S.pts[c_t3_quads[q][k]][0]; lq[k][1] = S.pts[c_t3_quads[q][k]][1]; }
             const double pt = 0.57735026918962576451;
-            const double xs[4] = {0.0, 0.0, -pt, pt}, es[4] = {-pt, pt, 0.0, 0.0};
-            double xi = xs[sp], eta = es[sp];
+            double xi = sp < 2 ? 0.0 : (sp == 2 ? -pt : pt), eta = sp >= 2 ? 0.0 : (sp == 0 ? -pt : pt);
             double dNr[4] = {-0.25 * (1 - eta), 0.25 * (1 - eta), 0.25 * (1 + eta), -0.25 * (1 + eta)};
             double dNs[4] = {-0.25 * (1 - xi), -0.25 * (1 + xi), 0.25 * (1 + xi), 0.25 * (1 - xi)};
             double J11 = 0, J12 = 0, J21 = 0, J22 = 0;
@@ -140,164 +169,172 @@ __global__ void __launch_bounds__(T3_THREADS) t3_k_kernel(int64_t nt, const int3
             }
             double det = J11 * J22 - J12 * J21;
             if (fabs(det) < 1e-14) det = det < 0.0 ? -1e-14 : 1e-14;
-            S.Jp[q][sp] = fabs(det);
+            S.u.q.Jp[q][sp] = fabs(det);
             double inv = 1.0 / det;
             double iJ11 = J22 * inv, iJ12 = -J12 * inv, iJ21 = -J21 * inv, iJ22 = J11 * inv;
             for (int k = 0; k < 4; ++k) {
                 double dx = iJ11 * dNr[k] + iJ12 * dNs[k], dy = iJ21 * dNr[k] + iJ22 * dNs[k];
                 double Nk = 0.25 * (1 + ((k == 1 || k == 2) ? xi : -xi)) * (1 + (k >= 2 ? eta : -eta));
-                if (sp < 2) { S.D[q][sp][3 * k] = dx; S.D[q][sp][3 * k + 1] = 0.0; S.D[q][sp][3 * k + 2] = Nk; }
-                else { S.D[q][sp][3 * k] = dy; S.D[q][sp][3 * k + 1] = -Nk; S.D[q][sp][3 * k + 2] = 0.0; }
+                double *Dr = S.u.q.D[q][sp] + 3 * k;
+                if (sp < 2) { Dr[0] = dx; Dr[1] = 0.0; Dr[2] = Nk; }
+                else { Dr[0] = dy; Dr[1] = -Nk; Dr[2] = 0.0; }
             }
         }
-        for (int i = lane; i < 21 * 22; i += 32) (&S.K[0][0])[i] = 0.0;
     }
-    __syncwarp();
-    if (S.plate && !S.skip_macneal && lane < 3) {
-        const int q = lane;
+    __syncwarp(tm);
+    // Phase 3: MacNeal compliance factors per virtual quad.
+    if (macneal && tl < 3) {
         double lq[4][2];
-        for (int k = 0; k < 4; ++k) { lq[k][0] = S.pts[c_t3_quads[q][k]][0]; lq[k][1] = S.pts[c_t3_quads[q][k]][1]; }
-        double Dx = 0.5 * (lq[1][0] + lq[2][0] - lq[0][0] - lq[3][0]);
-        double Dy = 0.5 * (lq[2][1] + lq[3][1] - lq[0][1] - lq[1][1]);
-        double Dx2 = Dx * Dx, Dy2 = Dy * Dy;
-        double J11c = 0.25 * (-lq[0][0] + lq[1][0] + lq[2][0] - lq[3][0]);
-        double J12c = 0.25 * (-lq[0][1] + lq[1][1] + lq[2][1] - lq[3][1]);
-        double J21c = 0.25 * (-lq[0][0] - lq[1][0] + lq[2][0] + lq[3][0]);
-        double J22c = 0.25 * (-lq[0][1] - lq[1][1] + lq[2][1] + lq[3][1]);
-        double A_elem = 4.0 * fabs(J11c * J22c - J12c * J21c);
-        const double eps = 0.04;
-        double ap = eps / (eps + (1.0 - eps) * Dx2 / fmax(Dy2, 1e-30));
-        double bp = eps / (eps + (1.0 - eps) * Dy2 / fmax(Dx2, 1e-30));
-        double flex_x = 1.0 / fmax(fabs(S.Cb[0]), 1e-30), flex_y = 1.0 / fmax(fabs(S.Cb[4]), 1e-30);
-        double inv12A = 1.0 / (12.0 * A_elem);
-        const double zb = 0.65;
-        double zxu = zb * inv12A * Dx2 * flex_x, zxd = zb * inv12A * ap * Dx2 * flex_x;
-        double zyu = zb * inv12A * Dy2 * flex_y, zyd = zb * inv12A * bp * Dy2 * flex_y;
-        double Zb[16] = {zxu + zxd, zxu - zxd, 0, 0, zxu - zxd, zxu + zxd, 0, 0,
-                         0, 0, zyu + zyd, zyu - zyd, 0, 0, zyu - zyd, zyu + zyd};
-        double VGV[16];
-        const int comps[4] = {1, 1, 2, 2};
-        for (int i = 0; i < 4; ++i)
-            for (int j = 0; j < 4; ++j) {
-                double Jf = sqrt(2.0 * S.Jp[q][i]) * sqrt(2.0 * S.Jp[q][j]);
-                double v;
-                if (comps[i] == comps[j]) v = (i == j) ? Jf * (comps[i] == 1 ? S.Cs[0] : S.Cs[3]) : 0.0;
-                else v = 0.5 * Jf * S.Cs[1];
-                VGV[4 * i + j] = v;
+        for (int k = 0; k < 4; ++k) { lq[k][0] = S.pts[c_t3_quads[tl][k]][0]; lq[k][1] = S.pts[c_t3_quads[tl][k]][1]; }
+        S.u.q.mz[tl] = macneal_z(lq, S.u.q.Jp[tl], S.cs, S.Cb[0], S.Cb[4]);
+    }
+    __syncwarp(tm);
+
+    if (plate) {
+        // Phase 4: plate 3x3 block of every (virtual quad, node pair).
+        for (int it = tl; it < 30; it += T3_TEAM) {
+            const int q = it / 10, pp = it - 10 * q;
+            const int ka = c_pair_a[pp], kb = c_pair_b[pp];
+            double v[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            const double xca = S.u.q.dNx[q][4][ka], yca = S.u.q.dNy[q][4][ka];
+            const double xcb = S.u.q.dNx[q][4][kb], ycb = S.u.q.dNy[q][4][kb];
+#pragma unroll
+            for (int g = 0; g < 4; ++g) {
+                const double xa = S.u.q.dNx[q][g][ka], ya = S.u.q.dNy[q][g][ka];
+                const double xb = S.u.q.dNx[q][g][kb], yb = S.u.q.dNy[q][g][kb];
+                const double wd = S.u.q.wdet[q][g];
+                // bending columns (theta_x, theta_y) with the twist correction
+                const double ac[2][3] = {{0.0, -ya, 2.0 * (-xa) - (-xca)}, {xa, 0.0, 2.0 * ya - yca}};
+                const double bc[2][3] = {{0.0, -yb, 2.0 * (-xb) - (-xcb)}, {xb, 0.0, 2.0 * yb - ycb}};
+#pragma unroll
+                for (int cj = 0; cj < 2; ++cj) {
+                    double cbb[3];
+#pragma unroll
+                    for (int r = 0; r < 3; ++r)
+                        cbb[r] = S.Cb[3 * r] * bc[cj][0] + S.Cb[3 * r + 1] * bc[cj][1] + S.Cb[3 * r + 2] * bc[cj][2];
+#pragma unroll
+                    for (int ci = 0; ci < 2; ++ci)
+                        v[1 + ci][1 + cj] += wd * (ac[ci][0] * cbb[0] + ac[ci][1] * cbb[1] + ac[ci][2] * cbb[2]);
+                }
             }
-        for (int i = 0; i < 4; ++i)
-            if (VGV[5 * i] < 1e-30) VGV[5 * i] = 1e-30;
-        double Zs[16];
-        for (int i = 0; i < 4; ++i)
-            for (int j = 0; j < 4; ++j) Zs[4 * i + j] = 0.5 * (VGV[4 * i + j] + VGV[4 * j + i]);
-        inv4_inplace(Zs);
-        double Zt[16];
-        for (int i = 0; i < 4; ++i)
-            for (int j = 0; j < 4; ++j) Zt[4 * i + j] = 0.5 * (Zs[4 * i + j] + Zs[4 * j + i]) + Zb[4 * i + j];
-        for (int i = 0; i < 4; ++i)
-            for (int j = 0; j < 4; ++j) S.Zinv[q][4 * i + j] = 0.5 * (Zt[4 * i + j] + Zt[4 * j + i]);
-        inv4_inplace(S.Zinv[q]);
-    }
-    __syncwarp();
-    if (S.plate && !S.skip_macneal) {
-        for (int w = lane; w < 144; w += 32) {
-            int q = w / 48, l = (w % 48) / 12, j = w % 12;
-            double s = 0.0;
-            for (int m = 0; m < 4; ++m) s += S.Zinv[q][4 * l + m] * S.D[q][m][j];
-            S.Y[q][l][j] = s;
+            if (macneal) {
+                double Da[4][3], Db[4][3], Ya[4][3], Yb[4][3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    double d[4], y[4];
+#pragma unroll
+                    for (int l = 0; l < 4; ++l) d[l] = Da[l][c] = S.u.q.D[q][l][3 * ka + c];
+                    macneal_y(S.u.q.mz[q], d, y);
+#pragma unroll
+                    for (int l = 0; l < 4; ++l) Ya[l][c] = y[l];
+#pragma unroll
+                    for (int l = 0; l < 4; ++l) d[l] = Db[l][c] = S.u.q.D[q][l][3 * kb + c];
+                    macneal_y(S.u.q.mz[q], d, y);
+#pragma unroll
+                    for (int l = 0; l < 4; ++l) Yb[l][c] = y[l];
+                }
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+                        for (int l = 0; l < 4; ++l) {
+                            s1 += Da[l][i] * Yb[l][j];
+                            s2 += Db[l][j] * Ya[l][i];
+                        }
+                        v[i][j] += 0.5 * (s1 + s2);
+                    }
+            }
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) S.Pb[q][pp][3 * i + j] = v[i][j];
         }
-    }
-    __syncwarp();
-    // plate blocks of the three virtual quads into the 21x21 system
-    if (S.plate) {
-        for (int q = 0; q < 3; ++q) {
-            for (int w = lane; w < 144; w += 32) {
-                int i = w / 12, j = w % 12;       // plate index: node i/3, comp i%3 (w, theta_x, theta_y)
-                int ka = i / 3, ca = i % 3, kb = j / 3, cb = j % 3;
-                double v = 0.0;
-                if (ca > 0 && cb > 0) {
-                    for (int g = 0; g < 4; ++g) {
-                        double a[3], b[3];
-                        double xa = S.dNx[q][g][ka], ya = S.dNy[q][g][ka], xb = S.dNx[q][g][kb], yb = S.dNy[q][g][kb];
-                        if (ca == 1) { a[0] = 0.0; a[1] = -ya; a[2] = 2.0 * (-xa) - (-S.dNx[q][4][ka]); }
-                        else { a[0] = xa; a[1] = 0.0; a[2] = 2.0 * ya - S.dNy[q][4][ka]; }
-                        if (cb == 1) { b[0] = 0.0; b[1] = -yb; b[2] = 2.0 * (-xb) - (-S.dNx[q][4][kb]); }
-                        else { b[0] = xb; b[1] = 0.0; b[2] = 2.0 * yb - S.dNy[q][4][kb]; }
-                        v += S.wdet[q][g] * quad_form(a, S.Cb, b);
+        __syncwarp(tm);
+
+        // Phase 5: lane r < 12 holds row r of [Kii | Kie] (internal dof r =
+        // macro node 3 + r/3, component r%3), summed over quads in order.
+        const bool act = tl < 12;
+        const int nA = 3 + tl / 3, ci = tl - 3 * (tl / 3);
+        double row[21];
+#pragma unroll
+        for (int c = 0; c < 21; ++c) row[c] = 0.0;
+        if (act) {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                int la = -1;
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (t3_quad_node(q, k) == nA) la = k;
+                if (la >= 0) {
+#pragma unroll
+                    for (int kb = 0; kb < 4; ++kb) {
+                        const int nB = t3_quad_node(q, kb);
+                        const int cb0 = nB >= 3 ? 3 * (nB - 3) : 12 + 3 * nB;
+                        const bool tr = la > kb;
+                        const int pid = tr ? packed_index(kb, la, 4) : packed_index(la, kb, 4);
+#pragma unroll
+                        for (int cj = 0; cj < 3; ++cj) row[cb0 + cj] += S.Pb[q][pid][tr ? 3 * cj + ci : 3 * ci + cj];
                     }
                 }
-                if (!S.skip_macneal) {
-                    double s1 = 0.0, s2 = 0.0;
-                    for (int l = 0; l < 4; ++l) {
-                        s1 += S.D[q][l][i] * S.Y[q][l][j];
-                        s2 += S.D[q][l][j] * S.Y[q][l][i];
-                    }
-                    v += 0.5 * (s1 + s2);
-                }
-                int ri = 3 * c_t3_quads[q][ka] + ca, rj = 3 * c_t3_quads[q][kb] + cb;
-                S.K[ri][rj] += v;
             }
-            __syncwarp();
         }
-        // condensation: solve Kii X = Kie (12 x 12, 9 rhs), partial pivoting
-        for (int w = lane; w < 108; w += 32) S.X[w / 9][w % 9] = S.K[9 + w / 9][w % 9];
-        __syncwarp();
+        int pos = act ? tl : 64;
+        double diag = 1.0;
+#pragma unroll
         for (int k = 0; k < 12; ++k) {
-            if (lane == 0) {
-                int p = k;
-                double best = fabs(S.K[9 + k][9 + k]);
-                for (int i = k + 1; i < 12; ++i) {
-                    double v = fabs(S.K[9 + i][9 + k]);
-                    if (v > best) { best = v; p = i; }
-                }
-                S.piv = p;
+            const bool cand_ok = act && pos >= k;
+            double cv = cand_ok ? fabs(row[k]) : -1.0;
+            int cp = cand_ok ? pos : 64;
+#pragma unroll
+            for (int off = 8; off > 0; off >>= 1) {
+                const double ov = __shfl_xor_sync(tm, cv, off, 16);
+                const int op = __shfl_xor_sync(tm, cp, off, 16);
+                if (ov > cv || (ov == cv && op < cp)) { cv = ov; cp = op; }
             }
-            __syncwarp();
-            int p = S.piv;
-            if (p != k) {
-                if (lane < 12) { double t = S.K[9 + k][9 + lane]; S.K[9 + k][9 + lane] = S.K[9 + p][9 + lane]; S.K[9 + p][9 + lane] = t; }
-                else if (lane < 21) { int j = lane - 12; double t = S.X[k][j]; S.X[k][j] = S.X[p][j]; S.X[p][j] = t; }
-            }
-            __syncwarp();
-            const double pivv = S.K[9 + k][9 + k];
-            // rows i > k: factor and update (lanes over (i, column) items)
-            const int nr = 11 - k;
-            for (int w = lane; w < nr * 22; w += 32) {
-                int i = k + 1 + w / 22, j = w % 22;
-                double f = S.K[9 + i][9 + k] / pivv;
-                if (j < 12) { if (j > k) S.K[9 + i][9 + j] -= f * S.K[9 + k][9 + j]; }
-                else if (j < 21) S.X[i][j - 12] -= f * S.X[k][j - 12];
-            }
-            __syncwarp();
-        }
-        // back substitution, one lane per right-hand side column
-        if (lane < 9) {
-            for (int k = 11; k >= 0; --k) {
-                double s = S.X[k][lane];
-                for (int i = k + 1; i < 12; ++i) s -= S.K[9 + k][9 + i] * S.X[i][lane];
-                S.X[k][lane] = s / S.K[9 + k][9 + k];
+            const bool is_piv = act && pos == cp;
+            const unsigned bal = __ballot_sync(tm, is_piv) & tm;
+            const int src = (__ffs(bal) - 1) & 15;
+            if (act && pos == k) pos = cp;  // LU row swap of positions k and cp
+            if (is_piv) pos = k;
+            const double akk = __shfl_sync(tm, row[k], src, 16);
+            if (is_piv) diag = akk;
+            const double f = (act && !is_piv) ? row[k] / akk : 0.0;
+#pragma unroll
+            for (int j = k + 1; j < 21; ++j) {
+                const double pj = __shfl_sync(tm, row[j], src, 16);
+                row[j] -= f * pj;
             }
         }
-        __syncwarp();
-        // Kcond = Kee + Kei * Aint,  Aint = -X   (stored back into K[0:9][0:9])
-        double kc[3];
-        int cnt = 0;
-        for (int w = lane; w < 81; w += 32) {
-            int i = w / 9, j = w % 9;
-            double s = S.K[i][j];
-            for (int l = 0; l < 12; ++l) s -= S.K[i][9 + l] * S.X[l][j];
-            kc[cnt++] = s;
+        __syncwarp(tm);  // every lane is past its last read of the quad data
+        if (act && pos < 12)
+#pragma unroll
+            for (int c = 0; c < 9; ++c) S.u.c.X[pos][c] = row[12 + c] / diag;
+        __syncwarp(tm);
+
+        // Phase 6: Kcond = Kee - Kei X (Kee, Kei from the corner's own quad).
+        for (int it = tl; it < 81; it += T3_TEAM) {
+            const int r = it / 9, col = it - 9 * r;
+            const int c = r / 3, i = r - 3 * c, c2 = col / 3, j = col - 3 * c2;
+            double kee = (c == c2) ? S.Pb[c][0][3 * i + j] : 0.0;
+            double s = 0.0;
+            for (int kl = 1; kl < 4; ++kl) {
+                const int l0 = 3 * (c_t3_quads[c][kl] - 3);
+#pragma unroll
+                for (int lj = 0; lj < 3; ++lj) s += S.Pb[c][kl][3 * i + lj] * S.u.c.X[l0 + lj][col];
+            }
+            S.u.c.Kc[r][col] = kee - s;
         }
-        __syncwarp();
-        cnt = 0;
-        for (int w = lane; w < 81; w += 32) S.K[w / 9][w % 9] = kc[cnt++];
-        __syncwarp();
+        __syncwarp(tm);
     }
-    // node-pair sub-blocks: lane -> (pair 0..5, sub-block tt, tr, rt, rr)
+
+    // Phase 7: node-pair sub-blocks: item -> (pair 0..5, sub-block tt, tr, rt, rr)
     double lmax = 0.0;
-    if (lane < 24) {
+    const bool degenerate = S.A < 1e-12;
+    for (int it = tl; it < 24; it += T3_TEAM) {
         const int pr_a[6] = {0, 0, 0, 1, 1, 2}, pr_b[6] = {0, 1, 2, 1, 2, 2};
-        const int pair = lane >> 2, sub = lane & 3;
+        const int pair = it >> 2, sub = it & 3;
         const int a = pr_a[pair], b = pr_b[pair];
         const int bi = sub >> 1, bj = sub & 1;
         double L[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
@@ -314,25 +351,18 @@ __global__ void __launch_bounds__(T3_THREADS) t3_k_kernel(int64_t nt, const int3
                     double v = S.alpha_d * (Bd_a[gi] * Bd_b[gj]) * A;
                     if (gi < 2 && gj < 2) v += quad_form(ma[gi], S.Cm, mb[gj]) * A;
                     // plate (w, theta_x, theta_y) = local 2, 3, 4
-                    if (S.plate && gi >= 2 && gi <= 4 && gj >= 2 && gj <= 4) v += S.K[3 * a + gi - 2][3 * b + gj - 2];
+                    if (plate && gi >= 2 && gi <= 4 && gj >= 2 && gj <= 4) v += S.u.c.Kc[3 * a + gi - 2][3 * b + gj - 2];
                     L[i][j] = v;
                 }
         }
         double O[3][3];
         rot_block(S.Q[a], L, S.Q[b], O);
-        const int32_t s = __ldg(o.blk_slot + e * 6 + pair);
-        for (int i = 0; i < 3; ++i)
-            for (int j = 0; j < 3; ++j) {
-                double v = O[i][j];
-                lmax = fmax(lmax, fabs(v));
-                *blk_entry(o, s, 3 * bi + i, 3 * bj + j) = v;
-                if (o.diag_staging && a == b && bi == bj && i == j)
-                    o.diag_staging[__ldg(o.diag_slot + e * 18 + 6 * a + 3 * bi + i)] = v;
-            }
+        const int32_t sl = __ldg(o.blk_slot + e * 6 + pair);
+        write_sub_block(o, e, sl, a, b, bi, bj, O, lmax, 18);
     }
     if (o.maxabs) {
-        for (int off = 16; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
-        if (lane == 0 && lmax > 0.0) atomic_max_nonneg(o.maxabs, lmax);
+        for (int off = 8; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_xor_sync(tm, lmax, off, 16));
+        if (tl == 0 && lmax > 0.0) atomic_max_nonneg(o.maxabs, lmax);
     }
 }
 

@@ -1084,7 +1084,7 @@ jfg_status launch_elements(jfg_model *m, bool kg, const double *du, double *dmax
             t3_kg_kernel<<<(unsigned)cdiv(m->nt, 128), 128, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords, m->d_nodeR,
                                                                             du, o);
         else
-            t3_k_kernel<<<(unsigned)cdiv(m->nt, T3_WARPS), T3_THREADS, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords,
+            t3_k_kernel<<<(unsigned)cdiv(m->nt, T3_ELEMS_PER_BLOCK), T3_THREADS, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords,
                                                                                        m->d_nodeR, m->k6rot, o);
         CK(cudaGetLastError());
     }

@@ -86,31 +86,104 @@ JFG_HD void node_block(const double v1[3], const double v2[3], const double v3[3
 }
 
 // In-place Gauss-Jordan inverse of a 4x4 (row-major) with partial pivoting.
+// Fully unrolled with predicated row swaps, so both working matrices stay in
+// registers.
 JFG_HD void inv4_inplace(double A[16]) {
-    double B[16];
-    for (int i = 0; i < 16; ++i) B[i] = (i % 5 == 0) ? 1.0 : 0.0;
+    double a[16], b[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) { a[i] = A[i]; b[i] = (i % 5 == 0) ? 1.0 : 0.0; }
+#pragma unroll
     for (int k = 0; k < 4; ++k) {
         int p = k;
-        double best = fabs(A[4 * k + k]);
+        double best = fabs(a[5 * k]);
+#pragma unroll
         for (int i = k + 1; i < 4; ++i) {
-            double v = fabs(A[4 * i + k]);
+            double v = fabs(a[4 * i + k]);
             if (v > best) { best = v; p = i; }
         }
-        if (p != k)
+#pragma unroll
+        for (int i = k + 1; i < 4; ++i)
+#pragma unroll
             for (int j = 0; j < 4; ++j) {
-                double t = A[4 * k + j]; A[4 * k + j] = A[4 * p + j]; A[4 * p + j] = t;
-                t = B[4 * k + j]; B[4 * k + j] = B[4 * p + j]; B[4 * p + j] = t;
+                const bool sw = (p == i);
+                double ta = a[4 * k + j], tb = b[4 * k + j];
+                a[4 * k + j] = sw ? a[4 * i + j] : ta; a[4 * i + j] = sw ? ta : a[4 * i + j];
+                b[4 * k + j] = sw ? b[4 * i + j] : tb; b[4 * i + j] = sw ? tb : b[4 * i + j];
             }
-        double inv = 1.0 / A[4 * k + k];
-        for (int j = 0; j < 4; ++j) { A[4 * k + j] *= inv; B[4 * k + j] *= inv; }
+        const double inv = 1.0 / a[5 * k];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) { a[4 * k + j] *= inv; b[4 * k + j] *= inv; }
+#pragma unroll
         for (int i = 0; i < 4; ++i) {
             if (i == k) continue;
-            double f = A[4 * i + k];
-            if (f != 0.0)
-                for (int j = 0; j < 4; ++j) { A[4 * i + j] -= f * A[4 * k + j]; B[4 * i + j] -= f * B[4 * k + j]; }
+            const double f = a[4 * i + k];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) { a[4 * i + j] -= f * a[4 * k + j]; b[4 * i + j] -= f * b[4 * k + j]; }
         }
     }
-    for (int i = 0; i < 16; ++i) A[i] = B[i];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) A[i] = b[i];
+}
+
+// MacNeal residual-bending-flexibility compliance of one (virtual) quad for
+// an isotropic shear matrix Cs = cs I (add_quad4_macneal_shear_rbf!,
+// FEMKernels.jl:4715-4978).  With Cs off-diagonal zero, VGV is diagonal, so
+// Z = sym(inv(sym(VGV)) + Zb) is block diagonal with 2x2 blocks on the
+// xi-sampling rows (0, 1) and the eta-sampling rows (2, 3); neither block
+// pivots (|z01| < z00 since 1/VGV > 0), so the reference's LU solve Z \ D
+// reduces to two 2x2 eliminations whose factors are kept here.
+struct MacNealZ {
+    double z01, r00, f01, r11;  // rows 0-1: off-diagonal, 1/z00, z01/z00, 1/(z11 - f01 z01)
+    double z23, r22, f23, r33;  // rows 2-3
+};
+
+// lq: corner local coordinates (4 x 2); Jp: |det J| at the four strain
+// sampling points; cs: transverse shear stiffness; cb00, cb11: bending
+// stiffness diagonal.
+JFG_HD MacNealZ macneal_z(const double lq[4][2], const double Jp[4], double cs, double cb00, double cb11) {
+    double Dx = 0.5 * (lq[1][0] + lq[2][0] - lq[0][0] - lq[3][0]);
+    double Dy = 0.5 * (lq[2][1] + lq[3][1] - lq[0][1] - lq[1][1]);
+    double Dx2 = Dx * Dx, Dy2 = Dy * Dy;
+    double J11c = 0.25 * (-lq[0][0] + lq[1][0] + lq[2][0] - lq[3][0]);
+    double J12c = 0.25 * (-lq[0][1] + lq[1][1] + lq[2][1] - lq[3][1]);
+    double J21c = 0.25 * (-lq[0][0] - lq[1][0] + lq[2][0] + lq[3][0]);
+    double J22c = 0.25 * (-lq[0][1] - lq[1][1] + lq[2][1] + lq[3][1]);
+    double A_elem = 4.0 * fabs(J11c * J22c - J12c * J21c);
+    const double eps = 0.04;
+    double ap = eps / (eps + (1.0 - eps) * Dx2 / fmax(Dy2, 1e-30));
+    double bp = eps / (eps + (1.0 - eps) * Dy2 / fmax(Dx2, 1e-30));
+    double flex_x = 1.0 / fmax(fabs(cb00), 1e-30), flex_y = 1.0 / fmax(fabs(cb11), 1e-30);
+    double inv12A = 1.0 / (12.0 * A_elem);
+    const double zb = 0.65;
+    double zxu = zb * inv12A * Dx2 * flex_x, zxd = zb * inv12A * ap * Dx2 * flex_x;
+    double zyu = zb * inv12A * Dy2 * flex_y, zyd = zb * inv12A * bp * Dy2 * flex_y;
+    double vd[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        double s = sqrt(2.0 * Jp[i]);
+        double v = s * s * cs;
+        vd[i] = v < 1e-30 ? 1e-30 : v;
+    }
+    MacNealZ z;
+    double z00 = 1.0 / vd[0] + (zxu + zxd), z11 = 1.0 / vd[1] + (zxu + zxd);
+    double z22 = 1.0 / vd[2] + (zyu + zyd), z33 = 1.0 / vd[3] + (zyu + zyd);
+    z.z01 = zxu - zxd;
+    z.r00 = 1.0 / z00;
+    z.f01 = z.z01 / z00;
+    z.r11 = 1.0 / (z11 - z.f01 * z.z01);
+    z.z23 = zyu - zyd;
+    z.r22 = 1.0 / z22;
+    z.f23 = z.z23 / z22;
+    z.r33 = 1.0 / (z33 - z.f23 * z.z23);
+    return z;
+}
+
+// One column of Y = Z \ D from the matching column d of the sampling rows.
+JFG_HD void macneal_y(const MacNealZ &z, const double d[4], double y[4]) {
+    y[1] = (d[1] - z.f01 * d[0]) * z.r11;
+    y[0] = (d[0] - z.z01 * y[1]) * z.r00;
+    y[3] = (d[3] - z.f23 * d[2]) * z.r33;
+    y[2] = (d[2] - z.z23 * y[3]) * z.r22;
 }
 
 // Order-independent max of non-negative doubles through their bit patterns.
