@@ -104,24 +104,78 @@ def time_cpu_oracle(seconds: float, reps_max: int = 50):
 
 
 class ClockSampler:
-    def __init__(self):
-        self.path = tempfile.mktemp(suffix=".csv")
-        self.proc = None
+    """SM clock and clock-event reasons sampled during the timed region.
+
+    NVML is read every 5 ms from a background thread (read-only queries), so
+    even a short timed region gets many samples; nvidia-smi at 200 ms is the
+    fallback when the NVML bindings are missing.
+    """
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
+
+    def __init__(self, uuid=None, index=0, period_s=0.005):
+        self.uuid, self.index, self.period = uuid, index, period_s
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self.thread, self.proc, self.source = None, None, None
+
+    def _nvml_loop(self, nv, h):
+        bits = [(n, getattr(nv, attr)) for n, attr in self.REASONS]
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self.stop_flag.is_set():
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                r = get_reasons(h)
+                for n, b in bits:
+                    if r & b:
+                        self.reasons.add(n)
+            except Exception:
+                pass
+            self.stop_flag.wait(self.period)
 
     def start(self):
+        import threading
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = None
+            if self.uuid:
+                try:
+                    h = nv.nvmlDeviceGetHandleByUUID(self.uuid)
+                except Exception:
+                    h = None
+            if h is None:
+                h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.stop_flag = threading.Event()
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self.thread.start()
+            self.source = "nvml 5 ms"
+            return
+        except Exception:
+            self.thread = None
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
+            self.path = tempfile.mktemp(suffix=".csv")
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
+            self.source = "nvidia-smi 200 ms"
         except Exception:
             self.proc = None
 
-    def stop(self, device_index: int):
+    def stop(self):
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            sm = self.samples
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                    "reasons": sorted(self.reasons), "samples": len(sm), "source": self.source}
         if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -129,23 +183,31 @@ class ClockSampler:
             self.proc.kill()
         self.f.close()
         sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in open(self.path):
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
             try:
-                if int(parts[0]) != device_index:
+                if int(parts[0]) != self.index:
                     continue
                 sm.append(float(parts[1])); mx.append(float(parts[2]))
             except ValueError:
                 continue
-            for n, v in zip(names, parts[5:9]):
+            for (n, _), v in zip(self.REASONS, parts[5:9]):
                 if v.lower() == "active":
                     reasons.add(n)
         os.unlink(self.path)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": self.source}
+
+
+def device_uuid(torch, dev):
+    """NVML UUID string of a torch CUDA device, or None."""
+    try:
+        u = str(torch.cuda.get_device_properties(dev).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        return None
 
 
 def measure_fp64_peak(torch, dev):
@@ -250,7 +312,7 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler()
+    clocks = ClockSampler(uuid=device_uuid(torch, dev), index=local)
     clocks.start()
     start = torch.cuda.Event(enable_timing=True); end = torch.cuda.Event(enable_timing=True)
     start.record(stream)
@@ -261,7 +323,7 @@ def main():
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    clk = clocks.stop(local)
+    clk = clocks.stop()
     elapsed = start.elapsed_time(end) / 1e3
     if dist:
         t = torch.tensor([elapsed], dtype=torch.float64, device=dev)

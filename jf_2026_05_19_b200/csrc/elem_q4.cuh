@@ -83,15 +83,22 @@ struct Q4KShared {
     double h, alpha_d;
     int skip_macneal, bend_cond;
     double Kabm[8][4], Kbbm[16], Kabb[8][4], Kbbb[16];
-    double Xm[4][8], Xb[4][8];
-    double D[4][12], Jp[4], Y[4][12];
+    double D[4][12], Jp[4];
     MacNealZ mz;
+    union {
+        double P[2][4][4][3];  // phase 1: C b_l(g) for membrane (0) / bending (1) incompatible modes
+        struct {
+            double Xm[4][8], Xb[4][8];
+            double Y[4][12];
+        } x;                   // phases 3-4
+    } u;
 };
 
 struct Q4GShared {
     Q4Geo g;
     double Cm[9], h;
     double uuv[8];
+    double P[4][4][3];  // Cm b_l(g) of the membrane incompatible modes
     double Kabm[8][4], Kbbm[16];
     double Am[4][8];
     double alpha[4];
@@ -319,46 +326,46 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
             else { S.D[tl][3 * k] = dy; S.D[tl][3 * k + 1] = -Nk; S.D[tl][3 * k + 2] = 0.0; }
         }
     }
+    // C b_l(g) of every incompatible-mode column (membrane, bending).
     if (valid) {
-        // 32 + 16 membrane items, 32 + 16 bending items
-        for (int w = tl; w < 96; w += Q4_TEAM) {
-            double acc = 0.0;
-            if (w < 32) {  // K_ab membrane: row r = 2k + comp, column l
-                int r = w >> 2, l = w & 3;
-                for (int g = 0; g < 4; ++g) {
-                    double a[3], b[3];
-                    q4_mem_col(S.g, g, r >> 1, r & 1, a);
-                    q4_bi_col(S.g, g, l, b);
-                    acc += S.g.wdet[g] * quad_form(a, S.Cm, b);
+        for (int w = tl; w < 32; w += Q4_TEAM) {
+            const int kind = w >> 4, g = (w >> 2) & 3, l = w & 3;
+            double b[3];
+            if (kind == 0) q4_bi_col(S.g, g, l, b);
+            else q4_bib_col(S.g, g, l, b);
+            const double *C = kind == 0 ? S.Cm : S.Cb;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) S.u.P[kind][g][l][r] = C[3 * r] * b[0] + C[3 * r + 1] * b[1] + C[3 * r + 2] * b[2];
+        }
+    }
+    __syncwarp();
+    // K_ab / K_bb rows (membrane then bending): 8 + 4 + 8 + 4 row items,
+    // four independent accumulators each.
+    if (valid) {
+        for (int w = tl; w < 24; w += Q4_TEAM) {
+            const int kind = w >= 12 ? 1 : 0, r = w - 12 * kind;
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+            for (int g = 0; g < 4; ++g) {
+                double a[3];
+                if (r < 8) {
+                    if (kind == 0) q4_mem_col(S.g, g, r >> 1, r & 1, a);
+                    else q4_bend_col(S.g, g, r >> 1, r & 1, a);
+                } else {
+                    if (kind == 0) q4_bi_col(S.g, g, r - 8, a);
+                    else q4_bib_col(S.g, g, r - 8, a);
                 }
-                S.Kabm[r][l] = acc;
-            } else if (w < 48) {
-                int l = (w - 32) >> 2, m = (w - 32) & 3;
-                for (int g = 0; g < 4; ++g) {
-                    double a[3], b[3];
-                    q4_bi_col(S.g, g, l, a);
-                    q4_bi_col(S.g, g, m, b);
-                    acc += S.g.wdet[g] * quad_form(a, S.Cm, b);
+                const double wd = S.g.wdet[g];
+#pragma unroll
+                for (int l = 0; l < 4; ++l) {
+                    const double *P = S.u.P[kind][g][l];
+                    acc[l] += wd * (a[0] * P[0] + a[1] * P[1] + a[2] * P[2]);
                 }
-                S.Kbbm[4 * l + m] = acc;
-            } else if (w < 80) {  // K_ab bending: row r = 2k + (theta_x, theta_y)
-                int r = (w - 48) >> 2, l = (w - 48) & 3;
-                for (int g = 0; g < 4; ++g) {
-                    double a[3], b[3];
-                    q4_bend_col(S.g, g, r >> 1, r & 1, a);
-                    q4_bib_col(S.g, g, l, b);
-                    acc += S.g.wdet[g] * quad_form(a, S.Cb, b);
-                }
-                S.Kabb[r][l] = acc;
-            } else {
-                int l = (w - 80) >> 2, m = (w - 80) & 3;
-                for (int g = 0; g < 4; ++g) {
-                    double a[3], b[3];
-                    q4_bib_col(S.g, g, l, a);
-                    q4_bib_col(S.g, g, m, b);
-                    acc += S.g.wdet[g] * quad_form(a, S.Cb, b);
-                }
-                S.Kbbb[4 * l + m] = acc;
+            }
+#pragma unroll
+            for (int l = 0; l < 4; ++l) {
+                if (r < 8) (kind == 0 ? S.Kabm : S.Kabb)[r][l] = acc[l];
+                else (kind == 0 ? S.Kbbm : S.Kbbb)[4 * (r - 8) + l] = acc[l];
             }
         }
     }
@@ -388,18 +395,18 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
                 int l = w >> 3, r = w & 7;
                 double s = 0.0;
                 for (int q = 0; q < 4; ++q) s += S.Kbbm[4 * l + q] * S.Kabm[r][q];
-                S.Xm[l][r] = s;
+                S.u.x.Xm[l][r] = s;
             } else if (w < 64) {
                 int l = (w - 32) >> 3, r = (w - 32) & 7;
                 double s = 0.0;
                 if (S.bend_cond)
                     for (int q = 0; q < 4; ++q) s += S.Kbbb[4 * l + q] * S.Kabb[r][q];
-                S.Xb[l][r] = s;
+                S.u.x.Xb[l][r] = s;
             } else if (!S.skip_macneal) {
                 int j = w - 64;
                 double d[4] = {S.D[0][j], S.D[1][j], S.D[2][j], S.D[3][j]}, y[4];
                 macneal_y(S.mz, d, y);
-                for (int l = 0; l < 4; ++l) S.Y[l][j] = y[l];
+                for (int l = 0; l < 4; ++l) S.u.x.Y[l][j] = y[l];
             }
         }
     }
@@ -456,8 +463,8 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
                 for (int j = 0; j < 3; ++j) {
                     double s1 = 0.0, s2 = 0.0;
                     for (int l = 0; l < 4; ++l) {
-                        s1 += S.D[l][3 * a + i] * S.Y[l][3 * b + j];
-                        s2 += S.D[l][3 * b + j] * S.Y[l][3 * a + i];
+                        s1 += S.D[l][3 * a + i] * S.u.x.Y[l][3 * b + j];
+                        s2 += S.D[l][3 * b + j] * S.u.x.Y[l][3 * a + i];
                     }
                     L[2 + i][2 + j] += 0.5 * (s1 + s2);
                 }
@@ -468,8 +475,8 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
             for (int be = 0; be < 2; ++be) {
                 double sm = 0.0, sb = 0.0;
                 for (int l = 0; l < 4; ++l) {
-                    sm += S.Kabm[2 * a + al][l] * S.Xm[l][2 * b + be];
-                    sb += S.Kabb[2 * a + al][l] * S.Xb[l][2 * b + be];
+                    sm += S.Kabm[2 * a + al][l] * S.u.x.Xm[l][2 * b + be];
+                    sb += S.Kabb[2 * a + al][l] * S.u.x.Xb[l][2 * b + be];
                 }
                 L[al][be] -= sm;
                 if (S.bend_cond) L[3 + al][3 + be] -= sb;
@@ -531,27 +538,37 @@ __global__ void __launch_bounds__(Q4_THREADS) q4_kg_kernel(int64_t nq, const int
         S.uuv[2 * tl] = Q[0] * u0 + Q[1] * u1 + Q[2] * u2;
         S.uuv[2 * tl + 1] = Q[3] * u0 + Q[4] * u1 + Q[5] * u2;
     }
+    // C b_l(g) of the membrane incompatible-mode columns, then K_ab / K_bb
+    // rows with four independent accumulators.
     if (valid) {
-        for (int w = tl; w < 48; w += Q4_TEAM) {
-            double acc = 0.0;
-            if (w < 32) {
-                int r = w >> 2, l = w & 3;
-                for (int g = 0; g < 4; ++g) {
-                    double a[3], b[3];
-                    q4_mem_col(S.g, g, r >> 1, r & 1, a);
-                    q4_bi_col(S.g, g, l, b);
-                    acc += S.g.wdet[g] * quad_form(a, S.Cm, b);
+        for (int w = tl; w < 16; w += Q4_TEAM) {
+            const int g = w >> 2, l = w & 3;
+            double b[3];
+            q4_bi_col(S.g, g, l, b);
+#pragma unroll
+            for (int r = 0; r < 3; ++r) S.P[g][l][r] = S.Cm[3 * r] * b[0] + S.Cm[3 * r + 1] * b[1] + S.Cm[3 * r + 2] * b[2];
+        }
+    }
+    __syncwarp();
+    if (valid) {
+        for (int r = tl; r < 12; r += Q4_TEAM) {
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+            for (int g = 0; g < 4; ++g) {
+                double a[3];
+                if (r < 8) q4_mem_col(S.g, g, r >> 1, r & 1, a);
+                else q4_bi_col(S.g, g, r - 8, a);
+                const double wd = S.g.wdet[g];
+#pragma unroll
+                for (int l = 0; l < 4; ++l) {
+                    const double *P = S.P[g][l];
+                    acc[l] += wd * (a[0] * P[0] + a[1] * P[1] + a[2] * P[2]);
                 }
-                S.Kabm[r][l] = acc;
-            } else {
-                int l = (w - 32) >> 2, m = (w - 32) & 3;
-                for (int g = 0; g < 4; ++g) {
-                    double a[3], b[3];
-                    q4_bi_col(S.g, g, l, a);
-                    q4_bi_col(S.g, g, m, b);
-                    acc += S.g.wdet[g] * quad_form(a, S.Cm, b);
-                }
-                S.Kbbm[4 * l + m] = acc;
+            }
+#pragma unroll
+            for (int l = 0; l < 4; ++l) {
+                if (r < 8) S.Kabm[r][l] = acc[l];
+                else S.Kbbm[4 * (r - 8) + l] = acc[l];
             }
         }
     }
@@ -603,9 +620,18 @@ __global__ void __launch_bounds__(Q4_THREADS) q4_kg_kernel(int64_t nq, const int
             c = dir == 0 ? 1.0 : 0.0;
             sn = dir == 0 ? 0.0 : 1.0;
         } else {
-            double th = 0.5 * atan2(2.0 * sxy, sxx - syy);
+            // theta = atan2(2 sxy, sxx - syy) / 2 lies in [-pi/2, pi/2], so
+            // (cos theta, sin theta) follow from cos 2theta = hd / rad and
+            // sin 2theta = sxy / rad by the half-angle identities, taking the
+            // square root on the side without cancellation.
             double c1, s1;
-            sincos(th, &s1, &c1);
+            if (hd >= 0.0) {
+                c1 = sqrt((rad + hd) / (2.0 * rad));
+                s1 = sxy / (2.0 * c1 * rad);
+            } else {
+                s1 = copysign(sqrt((rad - hd) / (2.0 * rad)), sxy);
+                c1 = sxy / (2.0 * s1 * rad);
+            }
             if (dir == 0) { lam = mean + rad; c = c1; sn = s1; }
             else { lam = mean - rad; c = -s1; sn = c1; }
         }

@@ -75,8 +75,12 @@ struct jfg_model {
     int64_t n_xpair = 0, n_xkey = 0, n_xcontrib = 0;
     double *d_exc_raw = nullptr;        // 36 doubles per exception pair
     int64_t *d_x_pos = nullptr;         // CSC position per unique (row, col)
-    int32_t *d_x_seg = nullptr, *d_x_src = nullptr;
+    int32_t *d_x_src = nullptr;
     double *d_x_w = nullptr;
+    int64_t n_xchunk = 0;
+    int32_t *d_x_cseg = nullptr;        // n_xchunk + 1 chunk bounds over the contributions
+    int32_t *d_x_kchunk = nullptr;      // n_xkey + 1 first chunk of each position
+    double *d_x_part = nullptr;         // per chunk partial sum
     // orig_diag map
     int32_t *d_dslot = nullptr;
     int64_t dslot_q4 = 0, dslot_t3 = 0, dslot_bar = 0;
@@ -416,42 +420,85 @@ __global__ void key_pos_kernel(int64_t n, const uint64_t *__restrict__ keys, int
 // assembly kernels
 // ---------------------------------------------------------------------------
 
-// Deterministic block reduction: thread (k, e) sums entry e of every element
-// block in global block k's segment, in slot order, and writes it to row
-// 6A+i (columns of B) and, for A != B, to the mirrored row 6B+j.
-__global__ void __launch_bounds__(288) block_reduce_kernel(int64_t n_blk, const int32_t *__restrict__ seg,
+// Deterministic block reduction: thread (k, i) sums row i (six values) of
+// every element block in global block k's segment, in slot order, and writes
+// it to row 6A+i (columns of B) and, for A != B, into column i of the
+// mirrored rows 6B+j.  Staging rows are 48-byte aligned, so they are read as
+// three double2 loads, two contributions per loop trip.
+__global__ void __launch_bounds__(256) block_reduce_kernel(int64_t n_blk, const int32_t *__restrict__ seg,
                                                            const double *__restrict__ staging, const int32_t *__restrict__ A,
                                                            const int32_t *__restrict__ B, const int32_t *__restrict__ offAB,
                                                            const int32_t *__restrict__ offBA, const int64_t *__restrict__ rowptr,
                                                            double *nz) {
-    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n_blk * 36) return;
-    int64_t k = t / 36;
-    int e = (int)(t - 36 * k), i = e / 6, j = e - 6 * (e / 6);
-    int32_t a = __ldg(seg + k), b = __ldg(seg + k + 1);
-    double s = 0.0;
-    for (int32_t q = a; q < b; ++q) s += __ldg(staging + 36 * (int64_t)q + e);
-    int64_t nA = __ldg(A + k), nB = __ldg(B + k);
-    nz[__ldg(rowptr + 6 * nA + i) + __ldg(offAB + k) + j] = s;
-    if (nA != nB) nz[__ldg(rowptr + 6 * nB + j) + __ldg(offBA + k) + i] = s;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_blk * 6) return;
+    const int64_t k = t / 6;
+    const int i = (int)(t - 6 * k);
+    const int32_t a = __ldg(seg + k), b = __ldg(seg + k + 1);
+    double s[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    int32_t q = a;
+    for (; q + 1 < b; q += 2) {
+        const double2 *p0 = reinterpret_cast<const double2 *>(staging + 36 * (int64_t)q + 6 * i);
+        const double2 *p1 = reinterpret_cast<const double2 *>(staging + 36 * (int64_t)(q + 1) + 6 * i);
+        const double2 x0 = __ldg(p0), x1 = __ldg(p0 + 1), x2 = __ldg(p0 + 2);
+        const double2 y0 = __ldg(p1), y1 = __ldg(p1 + 1), y2 = __ldg(p1 + 2);
+        s[0] += x0.x; s[1] += x0.y; s[2] += x1.x; s[3] += x1.y; s[4] += x2.x; s[5] += x2.y;
+        s[0] += y0.x; s[1] += y0.y; s[2] += y1.x; s[3] += y1.y; s[4] += y2.x; s[5] += y2.y;
+    }
+    if (q < b) {
+        const double2 *p0 = reinterpret_cast<const double2 *>(staging + 36 * (int64_t)q + 6 * i);
+        const double2 x0 = __ldg(p0), x1 = __ldg(p0 + 1), x2 = __ldg(p0 + 2);
+        s[0] += x0.x; s[1] += x0.y; s[2] += x1.x; s[3] += x1.y; s[4] += x2.x; s[5] += x2.y;
+    }
+    const int64_t nA = __ldg(A + k), nB = __ldg(B + k);
+    double *row = nz + __ldg(rowptr + 6 * nA + i) + __ldg(offAB + k);
+#pragma unroll
+    for (int j = 0; j < 6; ++j) row[j] = s[j];
+    if (nA != nB) {
+        const int64_t cb = __ldg(offBA + k) + i;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) nz[__ldg(rowptr + 6 * nB + j) + cb] = s[j];
+    }
 }
 
 // Dof-level path: each CSC position touched by an RBE2-expanded entry sums
-// its weighted raw element values.  One warp per position: lane l sums the
-// contributions l, l+32, ... and a fixed xor-butterfly combines the lanes, so
-// the order (and the result) is the same on every run even for the master
-// node's entries, which collect tens of thousands of contributions.
-__global__ void __launch_bounds__(256) exc_reduce_kernel(int64_t n, const int32_t *__restrict__ seg,
-                                                         const int32_t *__restrict__ src, const double *__restrict__ w,
-                                                         const double *__restrict__ raw, const int64_t *__restrict__ pos,
-                                                         double *nz) {
-    int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
-    if (t >= n) return;  // warp-uniform
+// its weighted raw element values.  The contributions of a position are cut
+// into fixed chunks of kXChunk when the model is built; one warp sums a chunk
+// (lane l takes contributions l, l+32, ..., then a fixed xor-butterfly), and
+// one warp per position sums its chunk partials the same way.  The order, and
+// so the result, is the same on every run, and the master node's positions,
+// which collect tens of thousands of contributions, are spread over many
+// warps.
+constexpr int kXChunk = 256;
+
+__global__ void __launch_bounds__(256) exc_chunk_kernel(int64_t n_chunk, const int32_t *__restrict__ cseg,
+                                                        const int32_t *__restrict__ src, const double *__restrict__ w,
+                                                        const double *__restrict__ raw, double *__restrict__ part) {
+    const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (t >= n_chunk) return;  // warp-uniform
+    const int32_t q0 = __ldg(cseg + t), q1 = __ldg(cseg + t + 1);
     double s = 0.0;
-    for (int32_t q = seg[t] + lane; q < seg[t + 1]; q += 32) s += w[q] * raw[src[q]];
+#pragma unroll
+    for (int r = 0; r < kXChunk / 32; ++r) {
+        const int32_t q = q0 + lane + 32 * r;
+        if (q < q1) s += __ldg(w + q) * __ldg(raw + __ldg(src + q));
+    }
     for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-    if (lane == 0) nz[pos[t]] = s;
+    if (lane == 0) part[t] = s;
+}
+
+__global__ void __launch_bounds__(256) exc_key_kernel(int64_t n, const int32_t *__restrict__ kchunk,
+                                                      const double *__restrict__ part, const int64_t *__restrict__ pos,
+                                                      double *nz) {
+    const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (t >= n) return;  // warp-uniform
+    const int32_t c0 = __ldg(kchunk + t), c1 = __ldg(kchunk + t + 1);
+    double s = 0.0;
+    for (int32_t c = c0 + lane; c < c1; c += 32) s += __ldg(part + c);
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) nz[__ldg(pos + t)] = s;
 }
 
 __global__ void diag_reduce_kernel(int64_t ndof, const int32_t *__restrict__ seg, const double *__restrict__ st, double *out) {
@@ -941,14 +988,25 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
         seg.push_back((int32_t)xcs.size());
         m->n_xkey = (int64_t)ukey.size();
         m->n_xcontrib = (int64_t)xcs.size();
+        std::vector<int32_t> cseg, kchunk;
+        for (int64_t t = 0; t < m->n_xkey; ++t) {
+            kchunk.push_back((int32_t)cseg.size());
+            for (int32_t q = seg[t]; q < seg[t + 1]; q += kXChunk) cseg.push_back(q);
+        }
+        kchunk.push_back((int32_t)cseg.size());
+        cseg.push_back((int32_t)xcs.size());
+        m->n_xchunk = (int64_t)cseg.size() - 1;
+        CK(dalloc(m, &m->d_x_cseg, cseg.size()));
+        CK(dalloc(m, &m->d_x_kchunk, kchunk.size()));
+        CK(dalloc(m, &m->d_x_part, m->n_xchunk));
+        CK(cudaMemcpyAsync(m->d_x_cseg, cseg.data(), sizeof(int32_t) * cseg.size(), cudaMemcpyHostToDevice, m->stream));
+        CK(cudaMemcpyAsync(m->d_x_kchunk, kchunk.data(), sizeof(int32_t) * kchunk.size(), cudaMemcpyHostToDevice, m->stream));
         uint64_t *d_uk = nullptr;
         CK(cudaMallocAsync(&d_uk, sizeof(uint64_t) * m->n_xkey, m->stream));
         CK(cudaMemcpyAsync(d_uk, ukey.data(), sizeof(uint64_t) * m->n_xkey, cudaMemcpyHostToDevice, m->stream));
         CK(dalloc(m, &m->d_x_pos, m->n_xkey));
-        CK(dalloc(m, &m->d_x_seg, m->n_xkey + 1));
         CK(dalloc(m, &m->d_x_src, m->n_xcontrib));
         CK(dalloc(m, &m->d_x_w, m->n_xcontrib));
-        CK(cudaMemcpyAsync(m->d_x_seg, seg.data(), sizeof(int32_t) * seg.size(), cudaMemcpyHostToDevice, m->stream));
         CK(cudaMemcpyAsync(m->d_x_src, src.data(), sizeof(int32_t) * src.size(), cudaMemcpyHostToDevice, m->stream));
         CK(cudaMemcpyAsync(m->d_x_w, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice, m->stream));
         key_pos_kernel<<<(unsigned)cdiv(m->n_xkey, 256), 256, 0, m->stream>>>(m->n_xkey, d_uk, ndof, m->d_rowptr, m->d_colind,
@@ -1104,13 +1162,17 @@ jfg_status launch_elements(jfg_model *m, bool kg, const double *du, double *dmax
 }
 
 jfg_status launch_reduce(jfg_model *m, double *nz, double *ddiag) {
-    if (m->n_xkey)
-        exc_reduce_kernel<<<(unsigned)cdiv(m->n_xkey * 32, 256), 256, 0, m->stream>>>(m->n_xkey, m->d_x_seg, m->d_x_src, m->d_x_w,
-                                                                                 m->d_exc_raw, m->d_x_pos, nz);
+    if (m->n_xkey) {
+        exc_chunk_kernel<<<(unsigned)cdiv(m->n_xchunk * 32, 256), 256, 0, m->stream>>>(m->n_xchunk, m->d_x_cseg, m->d_x_src,
+                                                                                  m->d_x_w, m->d_exc_raw, m->d_x_part);
+        CK(cudaGetLastError());
+        exc_key_kernel<<<(unsigned)cdiv(m->n_xkey * 32, 256), 256, 0, m->stream>>>(m->n_xkey, m->d_x_kchunk, m->d_x_part,
+                                                                              m->d_x_pos, nz);
+    }
     CK(cudaGetLastError());
     CK(cudaEventRecord(m->ev[4], m->stream));
     if (m->n_blk)
-        block_reduce_kernel<<<(unsigned)cdiv(m->n_blk * 36, 288), 288, 0, m->stream>>>(
+        block_reduce_kernel<<<(unsigned)cdiv(m->n_blk * 6, 256), 256, 0, m->stream>>>(
             m->n_blk, m->d_blk_seg, m->d_staging, m->d_blk_A, m->d_blk_B, m->d_blk_offAB, m->d_blk_offBA, m->d_rowptr, nz);
     CK(cudaGetLastError());
     CK(cudaEventRecord(m->ev[5], m->stream));
