@@ -1,6 +1,6 @@
 // elem_bar.cuh -- CBAR/CBEAM stiffness and differential stiffness kernels.
 //
-// One thread per element.  K: stiffness_frame3d_generic (Timoshenko frame
+// One thread per (element, node pair).  K: stiffness_frame3d_generic (Timoshenko frame
 // with Cowper shear areas and I12 coupling, src/FEMKernels.jl:140-209) in the
 // bar frame of assembly.jl:3961-4025 (offset-aware T with -R*skew(w)*R_node
 // blocks), T'kT.  KG: axial force P = (k u_bar)[7] (forces_frame3d,
@@ -15,6 +15,7 @@ namespace jfg {
 
 struct BarFrame {
     double L;
+    bool off;            // any offset vector nonzero
     double Rel[3][3];
     double TR[2][9];     // Rel * node_R for GA, GB
     double Toff[2][9];   // -Rel * skew(w) * node_R, zero without offsets
@@ -34,6 +35,7 @@ __device__ __forceinline__ bool bar_frame(int64_t e, const int32_t *__restrict__
         wb[i] = __ldg(pr + 15 + i);
     }
     bool off = dot3(wa, wa) > 1e-20 || dot3(wb, wb) > 1e-20;
+    F.off = off;
     double a[3], b[3], d[3];
     for (int i = 0; i < 3; ++i) { a[i] = off ? p1[i] + wa[i] : p1[i]; b[i] = off ? p2[i] + wb[i] : p2[i]; }
     sub3(b, a, d);
@@ -71,97 +73,191 @@ __device__ __forceinline__ bool bar_frame(int64_t e, const int32_t *__restrict__
     return true;
 }
 
-// T12 entry (row i, col j) from the block structure.
-__device__ __forceinline__ double bar_T(const BarFrame &F, int i, int j) {
-    int ki = i / 6, kj = j / 6;
-    if (ki != kj) return 0.0;
-    int ri = i % 6, cj = j % 6;
-    if (ri < 3 && cj < 3) return F.TR[ki][3 * ri + cj];
-    if (ri >= 3 && cj >= 3) return F.TR[ki][3 * (ri - 3) + cj - 3];
-    if (ri < 3 && cj >= 3) return F.Toff[ki][3 * ri + cj - 3];
+// Local 12x12 frame matrix of stiffness_frame3d_generic
+// (FEMKernels.jl:140-209) or geometric_stiffness_frame3d (:7441-7471) as
+// closed-form coefficients.  Dofs per node: u, v, w, theta_x, theta_y,
+// theta_z; entry (i, j) is evaluated by frame_k with compile-time indices,
+// so the zero pattern folds away and no 12x12 array is formed.
+struct FrameK {
+    double X, T;               // axial EA/L, torsion GJ/L
+    double ay, by, cy, dy;     // bending in the x-z plane (w, theta_y)
+    double az, bz, cz, dz;     // bending in the x-y plane (v, theta_z)
+    double a12, b12, c12, d12; // I12 coupling (zero when I12 == 0)
+};
+
+__device__ __forceinline__ double frame_k(const FrameK &c, int i, int j) {
+    const int ni = i / 6, nj = j / 6, li = i % 6, lj = j % 6;
+    const bool same = ni == nj;
+    if (li == 0 && lj == 0) return same ? c.X : -c.X;
+    if (li == 3 && lj == 3) return same ? c.T : -c.T;
+    if (li == 2 && lj == 2) return same ? c.ay : -c.ay;
+    if (li == 2 && lj == 4) return ni == 0 ? -c.by : c.by;
+    if (li == 4 && lj == 2) return nj == 0 ? -c.by : c.by;
+    if (li == 4 && lj == 4) return same ? c.cy : c.dy;
+    if (li == 1 && lj == 1) return same ? c.az : -c.az;
+    if (li == 1 && lj == 5) return ni == 0 ? c.bz : -c.bz;
+    if (li == 5 && lj == 1) return nj == 0 ? c.bz : -c.bz;
+    if (li == 5 && lj == 5) return same ? c.cz : c.dz;
+    if ((li == 1 && lj == 2) || (li == 2 && lj == 1)) return same ? c.a12 : -c.a12;
+    if (li == 1 && lj == 4) return ni == 0 ? -c.b12 : c.b12;
+    if (li == 4 && lj == 1) return nj == 0 ? -c.b12 : c.b12;
+    if (li == 2 && lj == 5) return ni == 0 ? c.b12 : -c.b12;
+    if (li == 5 && lj == 2) return nj == 0 ? c.b12 : -c.b12;
+    if ((li == 4 && lj == 5) || (li == 5 && lj == 4)) return same ? -c.c12 : -c.d12;
     return 0.0;
 }
 
-__device__ void frame3d_k(const double *__restrict__ pr, double L, double k[12][12]) {
+// Structural nonzeros of the local frame matrix (same pattern as frame_k).
+__host__ __device__ constexpr bool frame_nz(int i, int j) {
+    return ((i % 6 == 0) && (j % 6 == 0)) || ((i % 6 == 3) && (j % 6 == 3)) ||
+           ((i % 6 == 1 || i % 6 == 2 || i % 6 == 4 || i % 6 == 5) && (j % 6 == 1 || j % 6 == 2 || j % 6 == 4 || j % 6 == 5));
+}
+
+__device__ __forceinline__ FrameK frame3d_k(const double *__restrict__ pr, double L) {
     double A = __ldg(pr), Iz = __ldg(pr + 1), Iy = __ldg(pr + 2), I12 = __ldg(pr + 3), J = __ldg(pr + 4);
     double K1 = __ldg(pr + 5), K2 = __ldg(pr + 6), E = __ldg(pr + 7), G = __ldg(pr + 8);
     if (Iy == 0.0) Iy = Iz;
     if (Iz == 0.0) Iz = Iy;
-    for (int i = 0; i < 12; ++i)
-        for (int j = 0; j < 12; ++j) k[i][j] = 0.0;
-    double X = E * A / L;
-    k[0][0] = X; k[0][6] = -X; k[6][0] = -X; k[6][6] = X;
-    double T = G * J / L;
-    k[3][3] = T; k[3][9] = -T; k[9][3] = -T; k[9][9] = T;
+    FrameK c;
+    c.X = E * A / L;
+    c.T = G * J / L;
     bool inf_y = !(K1 > 0.0), inf_z = !(K2 > 0.0);
     double Asy = K1 * A, Asz = K2 * A;
     double Phi_y = inf_z ? 0.0 : 12 * E * Iy / (G * Asz * L * L);
     double Phi_z = inf_y ? 0.0 : 12 * E * Iz / (G * Asy * L * L);
-    double a_y = 12 * E * Iy / (L * L * L * (1 + Phi_y)), b_y = 6 * E * Iy / (L * L * (1 + Phi_y));
-    double c_y = (4 + Phi_y) * E * Iy / (L * (1 + Phi_y)), d_y = (2 - Phi_y) * E * Iy / (L * (1 + Phi_y));
-    k[2][2] = a_y; k[2][8] = -a_y; k[8][2] = -a_y; k[8][8] = a_y;
-    k[2][4] = -b_y; k[2][10] = -b_y; k[4][2] = -b_y; k[10][2] = -b_y;
-    k[8][4] = b_y; k[8][10] = b_y; k[4][8] = b_y; k[10][8] = b_y;
-    k[4][4] = c_y; k[4][10] = d_y; k[10][4] = d_y; k[10][10] = c_y;
-    double a_z = 12 * E * Iz / (L * L * L * (1 + Phi_z)), b_z = 6 * E * Iz / (L * L * (1 + Phi_z));
-    double c_z = (4 + Phi_z) * E * Iz / (L * (1 + Phi_z)), d_z = (2 - Phi_z) * E * Iz / (L * (1 + Phi_z));
-    k[1][1] = a_z; k[1][7] = -a_z; k[7][1] = -a_z; k[7][7] = a_z;
-    k[1][5] = b_z; k[1][11] = b_z; k[5][1] = b_z; k[11][1] = b_z;
-    k[7][5] = -b_z; k[7][11] = -b_z; k[5][7] = -b_z; k[11][7] = -b_z;
-    k[5][5] = c_z; k[5][11] = d_z; k[11][5] = d_z; k[11][11] = c_z;
+    c.ay = 12 * E * Iy / (L * L * L * (1 + Phi_y)); c.by = 6 * E * Iy / (L * L * (1 + Phi_y));
+    c.cy = (4 + Phi_y) * E * Iy / (L * (1 + Phi_y)); c.dy = (2 - Phi_y) * E * Iy / (L * (1 + Phi_y));
+    c.az = 12 * E * Iz / (L * L * L * (1 + Phi_z)); c.bz = 6 * E * Iz / (L * L * (1 + Phi_z));
+    c.cz = (4 + Phi_z) * E * Iz / (L * (1 + Phi_z)); c.dz = (2 - Phi_z) * E * Iz / (L * (1 + Phi_z));
     if (fabs(I12) > 0.0) {
-        double a = 12 * E * I12 / (L * L * L), b = 6 * E * I12 / (L * L), c = 4 * E * I12 / L, d = 2 * E * I12 / L;
-        k[1][2] += a; k[2][1] += a; k[1][8] += -a; k[8][1] += -a;
-        k[7][2] += -a; k[2][7] += -a; k[7][8] += a; k[8][7] += a;
-        k[1][4] += -b; k[4][1] += -b; k[1][10] += -b; k[10][1] += -b;
-        k[7][4] += b; k[4][7] += b; k[7][10] += b; k[10][7] += b;
-        k[2][5] += b; k[5][2] += b; k[2][11] += b; k[11][2] += b;
-        k[8][5] += -b; k[5][8] += -b; k[8][11] += -b; k[11][8] += -b;
-        k[4][5] += -c; k[5][4] += -c; k[4][11] += -d; k[11][4] += -d;
-        k[10][5] += -d; k[5][10] += -d; k[10][11] += -c; k[11][10] += -c;
+        c.a12 = 12 * E * I12 / (L * L * L); c.b12 = 6 * E * I12 / (L * L);
+        c.c12 = 4 * E * I12 / L; c.d12 = 2 * E * I12 / L;
+    } else {
+        c.a12 = c.b12 = c.c12 = c.d12 = 0.0;
     }
+    return c;
 }
 
-// Write T' k T (upper triangle) for one bar.
-__device__ __forceinline__ void bar_write(const ElemOut &o, int64_t e, const BarFrame &F, const double k[12][12],
-                                          const int32_t nd[2], double &lmax) {
-    double KT[12][12];
-    for (int i = 0; i < 12; ++i)
-        for (int j = 0; j < 12; ++j) {
-            double s = 0.0;
-            for (int l = 0; l < 12; ++l) s += k[i][l] * bar_T(F, l, j);
-            KT[i][j] = s;
-        }
-    double G[12][12];
-    for (int i = 0; i < 12; ++i)
-        for (int j = 0; j < 12; ++j) {
-            double s = 0.0;
-            for (int l = 0; l < 12; ++l) s += bar_T(F, l, i) * KT[l][j];
-            G[i][j] = s;
-            lmax = fmax(lmax, fabs(s));
-        }
-    const int pa[3] = {0, 0, 1}, pb[3] = {0, 1, 1};
-    for (int p = 0; p < 3; ++p) {
-        const int32_t s = __ldg(o.blk_slot + e * 3 + p);
-        for (int i = 0; i < 6; ++i)
-            for (int j = 0; j < 6; ++j) *blk_entry(o, s, i, j) = G[6 * pa[p] + i][6 * pb[p] + j];
+// Beam-column geometric stiffness in the same closed form (axial force P).
+__device__ __forceinline__ FrameK frame3d_kg(double L, double P) {
+    FrameK c;
+    c.X = c.T = 0.0;
+    c.a12 = c.b12 = c.c12 = c.d12 = 0.0;
+    if (L < 1e-9 || fabs(P) < 1e-30) {
+        c.ay = c.by = c.cy = c.dy = c.az = c.bz = c.cz = c.dz = 0.0;
+        return c;
     }
-    if (o.diag_staging)
-        for (int i = 0; i < 12; ++i) o.diag_staging[__ldg(o.diag_slot + e * 12 + i)] = G[i][i];
+    double c1 = 6.0 * P / (5.0 * L), c2 = P / 10.0, c3 = 2.0 * P * L / 15.0, c4 = -P * L / 30.0;
+    c.ay = c.az = c1; c.by = c.bz = c2; c.cy = c.cz = c3; c.dy = c.dz = c4;
+    return c;
 }
 
-__global__ void __launch_bounds__(128) bar_k_kernel(int64_t nb, const int32_t *__restrict__ nodes,
-                                                   const double *__restrict__ prop, const double *__restrict__ coords,
-                                                   const double *__restrict__ nodeR, ElemOut o) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+// out = k^{xy}_{AB} M: the 3x3 local sub-block (node A part x, node B part
+// y; part 0 = translations, 1 = rotations) times a 3x3 matrix.
+template <int A, int B, int X, int Y>
+__device__ __forceinline__ void kmul(const FrameK &c, const double *M, double out[3][3]) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            double s = 0.0;
+#pragma unroll
+            for (int l = 0; l < 3; ++l)
+                if (frame_nz(6 * A + 3 * X + i, 6 * B + 3 * Y + l))
+                    s += frame_k(c, 6 * A + 3 * X + i, 6 * B + 3 * Y + l) * M[3 * l + j];
+            out[i][j] = s;
+        }
+}
+
+// acc (+)= P^T W for a 3x3 P (row-major) and W.
+__device__ __forceinline__ void tmul(const double *P, const double W[3][3], double acc[3][3], bool add) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            double s = P[i] * W[0][j] + P[3 + i] * W[1][j] + P[6 + i] * W[2][j];
+            acc[i][j] = add ? acc[i][j] + s : s;
+        }
+}
+
+__device__ __forceinline__ void bar_store(const ElemOut &o, int64_t e, int32_t sl, int bi, int bj, const double G[3][3],
+                                          bool diag, int node, double &lmax) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            lmax = fmax(lmax, fabs(G[i][j]));
+            *blk_entry(o, sl, 3 * bi + i, 3 * bj + j) = G[i][j];
+        }
+    if (diag && o.diag_staging && bi == bj)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) o.diag_staging[__ldg(o.diag_slot + e * 12 + 6 * node + 3 * bi + i)] = G[i][i];
+}
+
+// Global node-pair block (A, B) of T' k T with T_n = [[R_n, O_n], [0, R_n]]
+// (R_n = Rel node_R_n, O_n = -Rel skew(w_n) node_R_n):
+//   G_tt = R_A' k_tt R_B               G_tr = R_A' (k_tt O_B + k_tr R_B)
+//   G_rt = O_A' k_tt R_B + R_A' k_rt R_B
+//   G_rr = O_A' (k_tt O_B + k_tr R_B) + R_A' (k_rt O_B + k_rr R_B)
+template <int A, int B>
+__device__ __forceinline__ void bar_pair(const ElemOut &o, int64_t e, int p, const BarFrame &F, const FrameK &c,
+                                         double &lmax) {
+    const int32_t sl = __ldg(o.blk_slot + e * 3 + p);
+    const bool off = F.off;
+    const double *RA = F.TR[A], *RB = F.TR[B], *OA = F.Toff[A], *OB = F.Toff[B];
+    double W[3][3], W2[3][3], G[3][3];
+    // tt
+    kmul<A, B, 0, 0>(c, RB, W);
+    tmul(RA, W, G, false);
+    bar_store(o, e, sl, 0, 0, G, A == B, A, lmax);
+    // rt (W = k_tt R_B)
+    kmul<A, B, 1, 0>(c, RB, W2);
+    tmul(RA, W2, G, false);
+    if (off) tmul(OA, W, G, true);
+    bar_store(o, e, sl, 1, 0, G, false, A, lmax);
+    // tr: W = k_tt O_B + k_tr R_B
+    kmul<A, B, 0, 1>(c, RB, W);
+    if (off) {
+        kmul<A, B, 0, 0>(c, OB, W2);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) W[i][j] = W2[i][j] + W[i][j];
+    }
+    tmul(RA, W, G, false);
+    bar_store(o, e, sl, 0, 1, G, false, A, lmax);
+    // rr: R_A' (k_rt O_B + k_rr R_B) + O_A' W
+    kmul<A, B, 1, 1>(c, RB, W2);
+    if (off) {
+        double W3[3][3];
+        kmul<A, B, 1, 0>(c, OB, W3);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) W2[i][j] = W3[i][j] + W2[i][j];
+    }
+    tmul(RA, W2, G, false);
+    if (off) tmul(OA, W, G, true);
+    bar_store(o, e, sl, 1, 1, G, A == B, A, lmax);
+}
+
+// One (bar, node pair) per thread, pair-major so that a warp runs one
+// compile-time pair; each of the three threads recomputes the bar frame.
+__global__ void __launch_bounds__(128, 3) bar_k_kernel(int64_t nb, const int32_t *__restrict__ nodes,
+                                                      const double *__restrict__ prop, const double *__restrict__ coords,
+                                                      const double *__restrict__ nodeR, ElemOut o) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int pair = (int)(t / nb);
+    const int64_t e = t - (int64_t)pair * nb;
     double lmax = 0.0;
-    if (e < nb) {
+    if (pair < 3) {
         BarFrame F;
         int32_t nd[2];
         if (bar_frame(e, nodes, prop, coords, nodeR, F, nd)) {
-            double k[12][12];
-            frame3d_k(prop + 18 * e, F.L, k);
-            bar_write(o, e, F, k, nd, lmax);
+            const FrameK c = frame3d_k(prop + 18 * e, F.L);
+            if (pair == 0) bar_pair<0, 0>(o, e, 0, F, c, lmax);
+            else if (pair == 1) bar_pair<0, 1>(o, e, 1, F, c, lmax);
+            else bar_pair<1, 1>(o, e, 2, F, c, lmax);
         }
     }
     if (o.maxabs) {
@@ -170,46 +266,39 @@ __global__ void __launch_bounds__(128) bar_k_kernel(int64_t nb, const int32_t *_
     }
 }
 
-__global__ void __launch_bounds__(128) bar_kg_kernel(int64_t nb, const int32_t *__restrict__ nodes,
-                                                    const double *__restrict__ prop, const double *__restrict__ coords,
-                                                    const double *__restrict__ nodeR, const double *__restrict__ u,
-                                                    ElemOut o) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nb) return;
+__global__ void __launch_bounds__(128, 3) bar_kg_kernel(int64_t nb, const int32_t *__restrict__ nodes,
+                                                       const double *__restrict__ prop, const double *__restrict__ coords,
+                                                       const double *__restrict__ nodeR, const double *__restrict__ u,
+                                                       ElemOut o) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int pair = (int)(t / nb);
+    const int64_t e = t - (int64_t)pair * nb;
+    if (pair >= 3) return;
     BarFrame F;
     int32_t nd[2];
     if (!bar_frame(e, nodes, prop, coords, nodeR, F, nd)) return;
-    double ub[12];
+    // axial force P = (k u_bar)[7] (forces_frame3d): row 7 of k has only the
+    // axial entries, and u_bar's axial components are (R_n u_n + O_n theta_n)_x.
+    double ux[2];
+#pragma unroll
     for (int k = 0; k < 2; ++k) {
-        double ug[6];
-        for (int d = 0; d < 6; ++d) ug[d] = __ldg(u + 6 * (int64_t)nd[k] + d);
-        for (int dd = 0; dd < 6; ++dd) {
-            double s = 0.0;
-            for (int q = 0; q < 6; ++q) s += bar_T(F, 6 * k + dd, 6 * k + q) * ug[q];
-            ub[6 * k + dd] = s;
-        }
+        const double *ug = u + 6 * (int64_t)nd[k];
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) s += F.TR[k][q] * __ldg(ug + q);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) s += F.Toff[k][q] * __ldg(ug + 3 + q);
+        ux[k] = s;
     }
     const double *pr = prop + 18 * e;
     double A = __ldg(pr), E = __ldg(pr + 7);
     double X = E * A / F.L;
-    double P = -X * ub[0] + X * ub[6];
-    double kg[12][12];
-    for (int i = 0; i < 12; ++i)
-        for (int j = 0; j < 12; ++j) kg[i][j] = 0.0;
-    double L = F.L;
-    if (!(L < 1e-9 || fabs(P) < 1e-30)) {
-        double c1 = 6.0 * P / (5.0 * L), c2 = P / 10.0, c3 = 2.0 * P * L / 15.0, c4 = -P * L / 30.0;
-        kg[1][1] = c1; kg[7][7] = c1; kg[1][7] = -c1; kg[7][1] = -c1;
-        kg[1][5] = c2; kg[5][1] = c2; kg[1][11] = c2; kg[11][1] = c2;
-        kg[5][5] = c3; kg[11][11] = c3; kg[5][11] = c4; kg[11][5] = c4;
-        kg[7][5] = -c2; kg[5][7] = -c2; kg[7][11] = -c2; kg[11][7] = -c2;
-        kg[2][2] = c1; kg[8][8] = c1; kg[2][8] = -c1; kg[8][2] = -c1;
-        kg[2][4] = -c2; kg[4][2] = -c2; kg[2][10] = -c2; kg[10][2] = -c2;
-        kg[4][4] = c3; kg[10][10] = c3; kg[4][10] = c4; kg[10][4] = c4;
-        kg[8][4] = c2; kg[4][8] = c2; kg[8][10] = c2; kg[10][8] = c2;
-    }
+    double P = -X * ux[0] + X * ux[1];
+    const FrameK c = frame3d_kg(F.L, P);
     double lmax = 0.0;
-    bar_write(o, e, F, kg, nd, lmax);
+    if (pair == 0) bar_pair<0, 0>(o, e, 0, F, c, lmax);
+    else if (pair == 1) bar_pair<0, 1>(o, e, 1, F, c, lmax);
+    else bar_pair<1, 1>(o, e, 2, F, c, lmax);
 }
 
 }  // namespace jfg

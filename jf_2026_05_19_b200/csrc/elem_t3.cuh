@@ -18,7 +18,7 @@
 // first position on ties); eliminating above the pivot as well replaces the
 // back substitution.
 //
-// KG: one thread per element.  CST membrane resultant of stress_strain_tria3
+// KG: one thread per (element, node pair).  CST membrane resultant of stress_strain_tria3
 // (FEMKernels.jl:7391-7404) and geometric_stiffness_tria3's non-curvature
 // branch (:8083-8097), which the default principal-transverse mode falls
 // into; T'KgT and drill zeroing as in assembly.jl:6019-6157.
@@ -366,13 +366,13 @@ __global__ void __launch_bounds__(T3_THREADS) t3_k_kernel(int64_t nt, const int3
     }
 }
 
-__global__ void __launch_bounds__(128) t3_kg_kernel(int64_t nt, const int32_t *__restrict__ nodes,
-                                                   const double *__restrict__ prop,
-                                                   const double *__restrict__ coords,
-                                                   const double *__restrict__ nodeR,
-                                                   const double *__restrict__ u, ElemOut o) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nt) return;
+// One (element, node pair) per thread, laid out pair-major so that a warp
+// runs one compile-time pair; each thread recomputes the element's frame and
+// membrane stress (cheap) and writes its own pair block.
+template <int PA, int PB>
+__device__ __forceinline__ void t3_kg_pair(int64_t e, const int32_t *__restrict__ nodes, const double *__restrict__ prop,
+                                           const double *__restrict__ coords, const double *__restrict__ nodeR,
+                                           const double *__restrict__ u, const ElemOut &o) {
     int32_t nd[3];
     double p[3][3];
     for (int k = 0; k < 3; ++k) {
@@ -423,16 +423,33 @@ __global__ void __launch_bounds__(128) t3_kg_kernel(int64_t nt, const int32_t *_
             for (int j = 0; j < 3; ++j)
                 val[i][j] = h * A * (sxx * b[i] * b[j] + syy * cv[i] * cv[j] + sxy * (b[i] * cv[j] + cv[i] * b[j]));
     }
-    int pair = 0;
-    for (int a = 0; a < 3; ++a)
-        for (int bb = a; bb < 3; ++bb, ++pair) {
-            double L[3][3] = {{val[a][bb], 0, 0}, {0, val[a][bb], 0}, {0, 0, val[a][bb]}};
-            double O[3][3];
-            rot_block(Q[a], L, Q[bb], O);
-            const int32_t s = __ldg(o.blk_slot + e * 6 + pair);
-            for (int i = 0; i < 6; ++i)
-                for (int j = 0; j < 6; ++j) *blk_entry(o, s, i, j) = (i < 3 && j < 3) ? O[i][j] : 0.0;
-        }
+    double L[3][3] = {{val[PA][PB], 0, 0}, {0, val[PA][PB], 0}, {0, 0, val[PA][PB]}};
+    double O[3][3];
+    rot_block(Q[PA], L, Q[PB], O);
+    const int32_t s = __ldg(o.blk_slot + e * 6 + packed_index(PA, PB, 3));
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+        for (int j = 0; j < 6; ++j) *blk_entry(o, s, i, j) = (i < 3 && j < 3) ? O[i][j] : 0.0;
+}
+
+__global__ void __launch_bounds__(128) t3_kg_kernel(int64_t nt, const int32_t *__restrict__ nodes,
+                                                   const double *__restrict__ prop,
+                                                   const double *__restrict__ coords,
+                                                   const double *__restrict__ nodeR,
+                                                   const double *__restrict__ u, ElemOut o) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int pair = (int)(t / nt);
+    const int64_t e = t - (int64_t)pair * nt;
+    switch (pair) {
+        case 0: t3_kg_pair<0, 0>(e, nodes, prop, coords, nodeR, u, o); break;
+        case 1: t3_kg_pair<0, 1>(e, nodes, prop, coords, nodeR, u, o); break;
+        case 2: t3_kg_pair<0, 2>(e, nodes, prop, coords, nodeR, u, o); break;
+        case 3: t3_kg_pair<1, 1>(e, nodes, prop, coords, nodeR, u, o); break;
+        case 4: t3_kg_pair<1, 2>(e, nodes, prop, coords, nodeR, u, o); break;
+        case 5: t3_kg_pair<2, 2>(e, nodes, prop, coords, nodeR, u, o); break;
+        default: break;
+    }
 }
 
 }  // namespace jfg

@@ -1139,7 +1139,7 @@ jfg_status launch_elements(jfg_model *m, bool kg, const double *du, double *dmax
         o.blk_slot = m->d_blk_slot + m->pair_t3;
         o.diag_slot = m->d_dslot + m->dslot_t3;
         if (kg)
-            t3_kg_kernel<<<(unsigned)cdiv(m->nt, 128), 128, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords, m->d_nodeR,
+            t3_kg_kernel<<<(unsigned)cdiv(6 * m->nt, 128), 128, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords, m->d_nodeR,
                                                                             du, o);
         else
             t3_k_kernel<<<(unsigned)cdiv(m->nt, T3_ELEMS_PER_BLOCK), T3_THREADS, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords,
@@ -1151,10 +1151,10 @@ jfg_status launch_elements(jfg_model *m, bool kg, const double *du, double *dmax
         o.blk_slot = m->d_blk_slot + m->pair_bar;
         o.diag_slot = m->d_dslot + m->dslot_bar;
         if (kg)
-            bar_kg_kernel<<<(unsigned)cdiv(m->nb, 128), 128, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR,
+            bar_kg_kernel<<<(unsigned)cdiv(3 * m->nb, 128), 128, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR,
                                                                              du, o);
         else
-            bar_k_kernel<<<(unsigned)cdiv(m->nb, 128), 128, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, o);
+            bar_k_kernel<<<(unsigned)cdiv(3 * m->nb, 128), 128, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, o);
         CK(cudaGetLastError());
     }
     CK(cudaEventRecord(m->ev[3], m->stream));
