@@ -158,6 +158,92 @@ jfg_status jfg_timing_accumulated(jfg_model *m, int kind, double *ms6_sum, int64
  * orig_diag entries, device bytes in use}. */
 jfg_status jfg_model_stats(jfg_model *m, int64_t *out8);
 
+/* Element and node counts of a handle: out4 = {n_nodes, n_quad4, n_tria3, n_bar}. */
+jfg_status jfg_model_counts(jfg_model *m, int64_t *out4);
+
+/* ---- Batched variants of one model ---------------------------------------
+ * Design variants (one mesh, many property sets) and the requests of one
+ * model family in the serving loop run as one launch per kernel: the
+ * variants share the handle's mesh, CSC pattern and scatter maps; each has
+ * its own shell thicknesses, optionally its own bar records, its own
+ * displacement field and its own output values.  This is the batched form
+ * of assemble_stiffness / assemble_geometric_stiffness
+ * (src/solver/assembly.jl:1953-4375, 4382-6634) over n_var property sets;
+ * the reference has no batched call (it assembles one model per call).
+ */
+
+/* Device bytes of batch workspace (block staging, raw RBE2 blocks, chunk
+ * partials, diagonal staging) that n_var variants need. */
+jfg_status jfg_batch_workspace_bytes(jfg_model *m, int32_t n_var, int64_t *bytes);
+
+/* Grow the handle's batch workspace to hold n_var variants (1..65535).  It
+ * allocates device memory, so call it before any stream capture. */
+jfg_status jfg_batch_reserve(jfg_model *m, int32_t n_var);
+
+/* Assemble K and/or KG for n_var variants (device pointers, the handle's
+ * stream, returns without synchronising; n_var <= the reserved count):
+ *   h_dev         [n_var][n_quad4 + n_tria3] shell thicknesses (> 0, not
+ *                 checked on the device), or NULL for the handle's own;
+ *   bar_prop_dev  [n_var][n_bar][JFG_BAR_PROP] bar records with the handle's
+ *                 offsets and orientation vectors, or NULL for the handle's;
+ *   u_dev         displacements for KG: [n_var][ndof] with u_stride = ndof,
+ *                 or one field shared by every variant with u_stride = 0;
+ *   nzk_dev       [n_var][nnz] K values, or NULL to skip K;
+ *   max_dev       [n_var] max_elem_stiff, or NULL (needs nzk_dev);
+ *   diag_dev      [n_var][ndof] orig_diag, or NULL (needs nzk_dev);
+ *   nzkg_dev      [n_var][nnz] KG values, or NULL to skip KG.
+ * Variant v's outputs equal, bit for bit, a single-model call with variant
+ * v's properties.  KG refuses bars with offsets as jfg_assemble_kg does. */
+jfg_status jfg_assemble_batch_device(jfg_model *m, int32_t n_var, const double *h_dev, const double *bar_prop_dev,
+                                     const double *u_dev, int64_t u_stride, double *nzk_dev, double *max_dev,
+                                     double *diag_dev, double *nzkg_dev);
+
+/* ---- Serving: a device-resident request loop over model families --------
+ * Replaces the reference's optimisation worker loop
+ * (tools/jfem_worker_jsonl.jl:132-148, manifest_batch_core.jl:283-409), which
+ * reassembles a model per JSONL request: here each family's mesh, CSC pattern
+ * and scatter maps stay on the GPU (its jfg_model handle), and a request
+ * carries a new shell-thickness vector (n_quad4 + n_tria3 values, > 0) and
+ * gets K and, when the family has a displacement field, KG of that family.
+ * While a server lives it owns its families' handles (their streams are its
+ * own); results stay on the device until released.
+ *   JFG_SERVE_BATCHED  continuous batching: requests that wait when a result
+ *                      slot frees up run together in one batched launch;
+ *                      families run on their own streams and overlap.
+ *   JFG_SERVE_SERIAL   one request per launch, in arrival order, each
+ *                      finished before the next starts (the plain path).
+ * Admission: every family gets batch workspace and two result slots sized to
+ * an equal share of hbm_budget_bytes (batch limit <= max_batch); requests
+ * wait in their family's queue until a slot is free.  Results of a batched
+ * request equal, bit for bit, the same request served alone. */
+#define JFG_SERVE_BATCHED 0
+#define JFG_SERVE_SERIAL 1
+typedef struct jfg_server jfg_server;
+
+/* families[n_families] handles; u_host[n_families] displacement fields (ndof
+ * each) for KG, or NULL entries / NULL array for K only. */
+jfg_status jfg_server_create(jfg_model *const *families, const double *const *u_host, int32_t n_families,
+                             int64_t hbm_budget_bytes, int32_t max_batch, int32_t policy, jfg_server **out);
+/* Queue a request (the thickness vector is copied); keep = 0 drops the
+ * results as soon as they are computed (timing only). */
+jfg_status jfg_server_submit(jfg_server *s, int32_t family, const double *h_host, int32_t keep, int64_t *ticket);
+/* Wait until the request is done (timeout_s < 0: no limit); *done = 1 when finished. */
+jfg_status jfg_server_wait(jfg_server *s, int64_t ticket, double timeout_s, int32_t *done);
+/* Device pointers to a finished request's K values, KG values (NULL if the
+ * family has no u) and max_elem_stiff, valid until jfg_server_release;
+ * times3 = {submitted, launched, finished} in seconds since creation. */
+jfg_status jfg_server_result(jfg_server *s, int64_t ticket, double **nzk_dev, double **nzkg_dev, double **max_dev,
+                             double *times3);
+jfg_status jfg_server_release(jfg_server *s, int64_t ticket);
+/* out6 = {submitted, completed, batches launched, largest batch, reserved device bytes, queued}. */
+jfg_status jfg_server_stats(jfg_server *s, int64_t *out6);
+jfg_status jfg_server_family_batch(jfg_server *s, int32_t family, int32_t *batch_limit);
+/* hold != 0: queue new requests without launching them; hold = 0 admits the
+ * queue (a burst submitted under hold is batched as a whole). */
+jfg_status jfg_server_hold(jfg_server *s, int32_t hold);
+const char *jfg_server_last_error(jfg_server *s);
+void jfg_server_destroy(jfg_server *s);
+
 /* ---- Allocation-free CQUAD4 stiffness assembly ---------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory where they need a stiffness matrix (inside a CUDA graph capture, or

@@ -6,6 +6,7 @@ repository snapshot.
 """
 from __future__ import annotations
 
+import hashlib
 import os
 import shutil
 import subprocess
@@ -14,8 +15,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libjfemgpu.so")
-SOURCES = ["jfg_api.cu"]
-HEADERS = ["jfg_common.cuh", "elem_q4.cuh", "elem_t3.cuh", "elem_bar.cuh"]
+SOURCES = ["jfg_api.cu", "jfg_server.cu"]
+HEADERS = ["jfg_common.cuh", "elem_q4.cuh", "elem_t3.cuh", "elem_bar.cuh"]  # plus the SOURCES
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -30,24 +31,50 @@ def host_compiler() -> list:
     return ["-ccbin", "/usr/bin/g++"] if os.path.exists("/usr/bin/g++") else []
 
 
+def deps() -> list:
+    return [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "jfem_gpu.h")]
+
+
+def source_hash() -> str:
+    """Content hash of every source and header the library is built from.
+
+    It is compiled into the library (reported by jfg_version) so that a
+    library built from other sources -- whose entry points may have other
+    signatures -- is never loaded by mistake, whatever the file times are."""
+    h = hashlib.sha256()
+    for p in deps():
+        h.update(os.path.basename(p).encode())
+        with open(p, "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()[:16]
+
+
+def built_hash() -> str:
+    """Source hash recorded beside the built library, or '' when absent."""
+    try:
+        with open(LIB + ".srchash") as f:
+            return f.read().strip()
+    except OSError:
+        return ""
+
+
 def needs_build() -> bool:
-    if not os.path.exists(LIB):
-        return True
-    t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "jfem_gpu.h")]
-    return any(os.path.getmtime(p) > t for p in deps)
+    return not os.path.exists(LIB) or built_hash() != source_hash()
 
 
 def build(force: bool = False, verbose: bool = False, extra=None) -> str:
     if not force and not needs_build():
         return LIB
+    sh = source_hash()
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
            "--expt-relaxed-constexpr", *host_compiler(), "-I", os.path.join(ROOT, "include"),
-           *(extra or []), "-o", LIB + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES]]
+           f"-DJFG_SRC_HASH=\"{sh}\"", *(extra or []), "-o", LIB + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES]]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
     os.replace(LIB + ".tmp", LIB)
+    with open(LIB + ".srchash", "w") as f:
+        f.write(sh + "\n")
     return LIB
 
 

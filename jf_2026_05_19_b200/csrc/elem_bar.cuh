@@ -249,6 +249,8 @@ __global__ void __launch_bounds__(128, 3) bar_k_kernel(int64_t nb, const int32_t
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int pair = (int)(t / nb);
     const int64_t e = t - (int64_t)pair * nb;
+    o = o.at(blockIdx.y);
+    if (o.bprop) prop = o.bprop;
     double lmax = 0.0;
     if (pair < 3) {
         BarFrame F;
@@ -274,6 +276,9 @@ __global__ void __launch_bounds__(128, 3) bar_kg_kernel(int64_t nb, const int32_
     const int pair = (int)(t / nb);
     const int64_t e = t - (int64_t)pair * nb;
     if (pair >= 3) return;
+    o = o.at(blockIdx.y);
+    if (o.bprop) prop = o.bprop;
+    u += (int64_t)blockIdx.y * o.u_stride;
     BarFrame F;
     int32_t nd[2];
     if (!bar_frame(e, nodes, prop, coords, nodeR, F, nd)) return;

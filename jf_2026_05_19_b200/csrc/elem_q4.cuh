@@ -48,13 +48,38 @@ __constant__ int c_pair_b[10] = {0, 1, 2, 3, 1, 2, 3, 2, 3, 3};
 //                  node);
 //   blk_slot <  0: the pair touches an RBE2 node; the raw block goes to
 //                  exc_raw[36 * (-slot - 1)] for the dof-level expansion.
+//
+// Batched variants: a launch may cover several variants of one model
+// (blockIdx.y = variant).  They share the mesh, the pattern and the maps;
+// each has its own staging, raw RBE2 blocks, diagonal staging and max, its
+// own displacement field, and optionally its own shell thicknesses and bar
+// records.  A single-model call is the one-variant case with zero strides.
 struct ElemOut {
-    double *staging;           // 36 doubles per sorted block slot
-    double *exc_raw;           // 36 doubles per constraint-touching pair
-    const int32_t *blk_slot;   // per element node pair
-    double *diag_staging;      // K only: raw element diagonal at sorted dof slots (or null)
-    const int32_t *diag_slot;  // per element local dof (or null)
-    double *maxabs;            // K only: max |value| (bit-pattern atomic), or null
+    double *staging = nullptr;           // 36 doubles per sorted block slot
+    double *exc_raw = nullptr;           // 36 doubles per constraint-touching pair
+    const int32_t *blk_slot = nullptr;   // per element node pair
+    double *diag_staging = nullptr;      // K only: raw element diagonal at sorted dof slots (or null)
+    const int32_t *diag_slot = nullptr;  // per element local dof (or null)
+    double *maxabs = nullptr;            // K only: max |value| (bit-pattern atomic), or null
+    int64_t staging_stride = 0, exc_stride = 0, dstage_stride = 0;  // per-variant output strides
+    const double *h = nullptr;           // per-variant shell thickness of this element type, or null
+    int64_t h_stride = 0;
+    const double *bprop = nullptr;       // per-variant bar records, or null
+    int64_t bprop_stride = 0;
+    int64_t u_stride = 0;                // per-variant displacement stride (ndof)
+
+    __device__ __forceinline__ ElemOut at(int v) const {
+        ElemOut r = *this;
+        r.staging += v * staging_stride;
+        r.exc_raw += v * exc_stride;
+        if (diag_staging) r.diag_staging += v * dstage_stride;
+        if (maxabs) r.maxabs += v;
+        if (h) r.h += v * h_stride;
+        if (bprop) r.bprop += v * bprop_stride;
+        return r;
+    }
+    // Shell thickness of element e: the variant's own, else the property record's.
+    __device__ __forceinline__ double thickness(int64_t e, const double *pr) const { return h ? __ldg(h + e) : __ldg(pr); }
 };
 
 constexpr int32_t kBlkTranspose = 1 << 30;
@@ -269,6 +294,7 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
                                                          const double *__restrict__ coords,
                                                          const double *__restrict__ nodeR, double k6rot, ElemOut o) {
     __shared__ Q4KShared sh[Q4_ELEMS_PER_BLOCK];
+    o = o.at(blockIdx.y);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int team = lane / Q4_TEAM, tl = lane - team * Q4_TEAM;
     const bool in_team = team < Q4_TEAMS_PER_WARP;
@@ -284,7 +310,7 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
     if (valid && tl == 9) {
         // constitutive build for isotropic PSHELL/MAT1 (assembly.jl:2460-2469)
         const double *pr = prop + 7 * e;
-        double h = __ldg(pr), E = __ldg(pr + 1), nu = __ldg(pr + 2), br = __ldg(pr + 4), tst = __ldg(pr + 5), Gs = __ldg(pr + 6);
+        double h = o.thickness(e, pr), E = __ldg(pr + 1), nu = __ldg(pr + 2), br = __ldg(pr + 4), tst = __ldg(pr + 5), Gs = __ldg(pr + 6);
         double cm = E * h / (1 - nu * nu);
         double cb = br * (E * h * h * h) / (12 * (1 - nu * nu));
         double base[9] = {1.0, nu, 0.0, nu, 1.0, 0.0, 0.0, 0.0, (1 - nu) / 2};
@@ -509,6 +535,8 @@ __global__ void __launch_bounds__(Q4_THREADS) q4_kg_kernel(int64_t nq, const int
                                                           const double *__restrict__ nodeR,
                                                           const double *__restrict__ u, ElemOut o) {
     __shared__ Q4GShared sh[Q4_ELEMS_PER_BLOCK];
+    o = o.at(blockIdx.y);
+    u += (int64_t)blockIdx.y * o.u_stride;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int team = lane / Q4_TEAM, tl = lane - team * Q4_TEAM;
     const bool in_team = team < Q4_TEAMS_PER_WARP;
@@ -523,7 +551,7 @@ __global__ void __launch_bounds__(Q4_THREADS) q4_kg_kernel(int64_t nq, const int
     q4_geometry(S.g, in_team ? tl : 99, valid, nd, coords, nodeR);
     if (valid && tl == 9) {
         const double *pr = prop + 7 * e;
-        double h = __ldg(pr), E = __ldg(pr + 1), nu = __ldg(pr + 2);
+        double h = o.thickness(e, pr), E = __ldg(pr + 1), nu = __ldg(pr + 2);
         double cm = E / (1 - nu * nu);
         double base[9] = {1.0, nu, 0.0, nu, 1.0, 0.0, 0.0, 0.0, (1 - nu) / 2};
         for (int i = 0; i < 9; ++i) S.Cm[i] = (cm * base[i]) * h;

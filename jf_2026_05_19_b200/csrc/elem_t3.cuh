@@ -68,6 +68,7 @@ __global__ void __launch_bounds__(T3_THREADS) t3_k_kernel(int64_t nt, const int3
                                                          const double *__restrict__ coords,
                                                          const double *__restrict__ nodeR, double k6rot, ElemOut o) {
     __shared__ T3KShared sh[T3_ELEMS_PER_BLOCK];
+    o = o.at(blockIdx.y);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int team = lane >> 4, tl = lane & 15;
     const unsigned tm = 0xFFFFu << (16 * team);
@@ -107,7 +108,7 @@ __global__ void __launch_bounds__(T3_THREADS) t3_k_kernel(int64_t nt, const int3
         S.pts[5][0] = (x[2] + x[0]) / 2; S.pts[5][1] = (y[2] + y[0]) / 2;
         S.pts[6][0] = (x[0] + x[1] + x[2]) / 3; S.pts[6][1] = (y[0] + y[1] + y[2]) / 3;
         const double *pr = prop + 7 * e;
-        double h = __ldg(pr), E = __ldg(pr + 1), nu = __ldg(pr + 2), br = __ldg(pr + 4), tst = __ldg(pr + 5), Gs = __ldg(pr + 6);
+        double h = o.thickness(e, pr), E = __ldg(pr + 1), nu = __ldg(pr + 2), br = __ldg(pr + 4), tst = __ldg(pr + 5), Gs = __ldg(pr + 6);
         double cm = E * h / (1 - nu * nu);
         double cb = br * (E * h * h * h) / (12 * (1 - nu * nu));
         double base[9] = {1.0, nu, 0.0, nu, 1.0, 0.0, 0.0, 0.0, (1 - nu) / 2};
@@ -397,7 +398,7 @@ __device__ __forceinline__ void t3_kg_pair(int64_t e, const int32_t *__restrict_
         node_block(v1, v2, v3, nodeR ? Rl : nullptr, Q[k]);
     }
     const double *pr = prop + 7 * e;
-    const double h = __ldg(pr), E = __ldg(pr + 1), nu = __ldg(pr + 2);
+    const double h = o.thickness(e, pr), E = __ldg(pr + 1), nu = __ldg(pr + 2);
     double x[3] = {lc[0][0], lc[1][0], lc[2][0]}, y[3] = {lc[0][1], lc[1][1], lc[2][1]};
     double A = 0.5 * fabs(x[0] * (y[1] - y[2]) + x[1] * (y[2] - y[0]) + x[2] * (y[0] - y[1]));
     double val[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
@@ -441,6 +442,8 @@ __global__ void __launch_bounds__(128) t3_kg_kernel(int64_t nt, const int32_t *_
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int pair = (int)(t / nt);
     const int64_t e = t - (int64_t)pair * nt;
+    o = o.at(blockIdx.y);
+    u += (int64_t)blockIdx.y * o.u_stride;
     switch (pair) {
         case 0: t3_kg_pair<0, 0>(e, nodes, prop, coords, nodeR, u, o); break;
         case 1: t3_kg_pair<0, 1>(e, nodes, prop, coords, nodeR, u, o); break;

@@ -89,6 +89,10 @@ struct jfg_model {
     int64_t n_dcontrib = 0;
     // work buffers
     double *d_nz = nullptr, *d_u = nullptr, *d_diag = nullptr, *d_max = nullptr, *d_h = nullptr;
+    // batched-variant workspace (jfg_batch_reserve): per variant one copy of
+    // the block staging, raw RBE2 blocks, RBE2 chunk partials and diagonal staging
+    int32_t b_cap = 0;
+    double *d_bw = nullptr;
     // constraint map (host, 0-based dofs)
     std::vector<int64_t> dep_dof, dep_ptr, dep_ind;
     std::vector<double> dep_coef;
@@ -429,9 +433,11 @@ __global__ void __launch_bounds__(256) block_reduce_kernel(int64_t n_blk, const 
                                                            const double *__restrict__ staging, const int32_t *__restrict__ A,
                                                            const int32_t *__restrict__ B, const int32_t *__restrict__ offAB,
                                                            const int32_t *__restrict__ offBA, const int64_t *__restrict__ rowptr,
-                                                           double *nz) {
+                                                           double *nz, int64_t staging_stride, int64_t nnz) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_blk * 6) return;
+    staging += (int64_t)blockIdx.y * staging_stride;  // batched variant
+    nz += (int64_t)blockIdx.y * nnz;
     const int64_t k = t / 6;
     const int i = (int)(t - 6 * k);
     const int32_t a = __ldg(seg + k), b = __ldg(seg + k + 1);
@@ -473,10 +479,13 @@ constexpr int kXChunk = 256;
 
 __global__ void __launch_bounds__(256) exc_chunk_kernel(int64_t n_chunk, const int32_t *__restrict__ cseg,
                                                         const int32_t *__restrict__ src, const double *__restrict__ w,
-                                                        const double *__restrict__ raw, double *__restrict__ part) {
+                                                        const double *__restrict__ raw, double *__restrict__ part,
+                                                        int64_t raw_stride, int64_t part_stride) {
     const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (t >= n_chunk) return;  // warp-uniform
+    raw += (int64_t)blockIdx.y * raw_stride;  // batched variant
+    part += (int64_t)blockIdx.y * part_stride;
     const int32_t q0 = __ldg(cseg + t), q1 = __ldg(cseg + t + 1);
     double s = 0.0;
 #pragma unroll
@@ -490,10 +499,12 @@ __global__ void __launch_bounds__(256) exc_chunk_kernel(int64_t n_chunk, const i
 
 __global__ void __launch_bounds__(256) exc_key_kernel(int64_t n, const int32_t *__restrict__ kchunk,
                                                       const double *__restrict__ part, const int64_t *__restrict__ pos,
-                                                      double *nz) {
+                                                      double *nz, int64_t part_stride, int64_t nnz) {
     const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (t >= n) return;  // warp-uniform
+    part += (int64_t)blockIdx.y * part_stride;  // batched variant
+    nz += (int64_t)blockIdx.y * nnz;
     const int32_t c0 = __ldg(kchunk + t), c1 = __ldg(kchunk + t + 1);
     double s = 0.0;
     for (int32_t c = c0 + lane; c < c1; c += 32) s += __ldg(part + c);
@@ -501,9 +512,12 @@ __global__ void __launch_bounds__(256) exc_key_kernel(int64_t n, const int32_t *
     if (lane == 0) nz[__ldg(pos + t)] = s;
 }
 
-__global__ void diag_reduce_kernel(int64_t ndof, const int32_t *__restrict__ seg, const double *__restrict__ st, double *out) {
+__global__ void diag_reduce_kernel(int64_t ndof, const int32_t *__restrict__ seg, const double *__restrict__ st, double *out,
+                                   int64_t st_stride) {
     int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= ndof) return;
+    st += (int64_t)blockIdx.y * st_stride;  // batched variant
+    out += (int64_t)blockIdx.y * ndof;
     double s = 0.0;
     for (int32_t q = seg[d]; q < seg[d + 1]; ++q) s += st[q];
     out[d] = s;
@@ -596,7 +610,10 @@ jfg_status validate(jfg_model *m, const jfg_model_desc *d) {
 
 extern "C" {
 
-const char *jfg_version(void) { return "jfem-b200 0.1 (sm_100a, fp64)"; }
+#ifndef JFG_SRC_HASH
+#define JFG_SRC_HASH "unknown"
+#endif
+const char *jfg_version(void) { return "jfem-b200 0.1 (sm_100a, fp64) src " JFG_SRC_HASH; }
 
 const char *jfg_last_error(jfg_model *m) { return m ? m->err.c_str() : "null handle"; }
 
@@ -604,6 +621,7 @@ void jfg_model_destroy(jfg_model *m) {
     if (!m) return;
     if (m->stream) cudaStreamSynchronize(m->stream);
     for (void *p : m->allocs) cudaFree(p);
+    if (m->d_bw) cudaFree(m->d_bw);
     for (auto &set : m->ring)
         for (auto &e : set.e)
             if (e) cudaEventDestroy(e);
@@ -1080,6 +1098,15 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
     return JFG_OK;
 }
 
+jfg_status jfg_model_counts(jfg_model *m, int64_t *out4) {
+    if (!m || !out4) return JFG_ERR_INVALID;
+    out4[0] = m->n_nodes;
+    out4[1] = m->nq;
+    out4[2] = m->nt;
+    out4[3] = m->nb;
+    return JFG_OK;
+}
+
 jfg_status jfg_set_stream(jfg_model *m, void *stream) {
     if (!m) return JFG_ERR_INVALID;
     m->stream = stream ? (cudaStream_t)stream : m->own;
@@ -1115,69 +1142,120 @@ namespace {
 
 jfg_status begin_set(jfg_model *m, int kind);
 
-jfg_status launch_elements(jfg_model *m, bool kg, const double *du, double *dmax, double *ddiag) {
+// One assembly launch sequence over n_var variants of the model (n_var = 1
+// and zero strides for a single-model call).
+struct Batch {
+    int n_var = 1;
+    double *staging = nullptr, *exc_raw = nullptr, *dstaging = nullptr, *x_part = nullptr;
+    int64_t staging_stride = 0, exc_stride = 0, dstage_stride = 0, part_stride = 0;
+    const double *h = nullptr;      // [n_var][nq + nt] shell thickness, or null
+    const double *bprop = nullptr;  // [n_var][nb * JFG_BAR_PROP], or null
+    const double *u = nullptr;      // [n_var][ndof] (KG), or one field shared by all variants
+    int64_t u_stride = -1;          // per-variant displacement stride; -1 = ndof
+    double *nz = nullptr;           // [n_var][nnz]
+    double *dmax = nullptr;         // [n_var] (K, or null)
+    double *ddiag = nullptr;        // [n_var][ndof] (K, or null)
+};
+
+Batch single_batch(jfg_model *m) {
+    Batch b;
+    b.staging = m->d_staging;
+    b.exc_raw = m->d_exc_raw;
+    b.dstaging = m->d_dstaging;
+    b.x_part = m->d_x_part;
+    return b;
+}
+
+// Per-variant sizes of the batch workspace, in doubles.
+struct BatchSizes { int64_t staging, exc, part, dstage, total; };
+BatchSizes batch_sizes(const jfg_model *m) {
+    auto up = [](int64_t n) { return (n + 31) / 32 * 32; };  // 256-byte aligned sub-buffers
+    BatchSizes z;
+    z.staging = up(36 * m->n_blk_contrib);
+    z.exc = up(36 * m->n_xpair);
+    z.part = up(m->n_xchunk);
+    z.dstage = up(m->n_dcontrib);
+    z.total = z.staging + z.exc + z.part + z.dstage;
+    return z;
+}
+
+jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
+    const unsigned nv = (unsigned)bt.n_var;
     ElemOut o;
-    o.staging = m->d_staging;
-    o.exc_raw = m->d_exc_raw;
-    o.diag_staging = ddiag ? m->d_dstaging : nullptr;
-    o.diag_slot = nullptr;
-    o.maxabs = dmax;
+    o.staging = bt.staging;
+    o.exc_raw = bt.exc_raw;
+    o.diag_staging = bt.ddiag ? bt.dstaging : nullptr;
+    o.maxabs = bt.dmax;
+    o.staging_stride = bt.staging_stride;
+    o.exc_stride = bt.exc_stride;
+    o.dstage_stride = bt.dstage_stride;
+    o.u_stride = bt.u_stride < 0 ? m->ndof : bt.u_stride;
+    const double *du = bt.u;
     CK(cudaEventRecord(m->ev[0], m->stream));
     if (m->nq) {
         o.blk_slot = m->d_blk_slot + m->pair_q4;
         o.diag_slot = m->d_dslot + m->dslot_q4;
+        o.h = bt.h;
+        o.h_stride = m->nq + m->nt;
+        dim3 grid((unsigned)cdiv(m->nq, Q4_ELEMS_PER_BLOCK), nv);
         if (kg)
-            q4_kg_kernel<<<(unsigned)cdiv(m->nq, Q4_ELEMS_PER_BLOCK), Q4_THREADS, 0, m->stream>>>(
-                m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, du, o);
+            q4_kg_kernel<<<grid, Q4_THREADS, 0, m->stream>>>(m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, du, o);
         else
-            q4_k_kernel<<<(unsigned)cdiv(m->nq, Q4_ELEMS_PER_BLOCK), Q4_THREADS, 0, m->stream>>>(
-                m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, m->k6rot, o);
+            q4_k_kernel<<<grid, Q4_THREADS, 0, m->stream>>>(m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, m->k6rot, o);
         CK(cudaGetLastError());
     }
     CK(cudaEventRecord(m->ev[1], m->stream));
     if (m->nt) {
         o.blk_slot = m->d_blk_slot + m->pair_t3;
         o.diag_slot = m->d_dslot + m->dslot_t3;
+        o.h = bt.h ? bt.h + m->nq : nullptr;
+        o.h_stride = m->nq + m->nt;
         if (kg)
-            t3_kg_kernel<<<(unsigned)cdiv(6 * m->nt, 128), 128, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords, m->d_nodeR,
-                                                                            du, o);
+            t3_kg_kernel<<<dim3((unsigned)cdiv(6 * m->nt, 128), nv), 128, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords,
+                                                                                     m->d_nodeR, du, o);
         else
-            t3_k_kernel<<<(unsigned)cdiv(m->nt, T3_ELEMS_PER_BLOCK), T3_THREADS, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords,
-                                                                                       m->d_nodeR, m->k6rot, o);
+            t3_k_kernel<<<dim3((unsigned)cdiv(m->nt, T3_ELEMS_PER_BLOCK), nv), T3_THREADS, 0, m->stream>>>(
+                m->nt, m->d_t3n, m->d_t3p, m->d_coords, m->d_nodeR, m->k6rot, o);
         CK(cudaGetLastError());
     }
     CK(cudaEventRecord(m->ev[2], m->stream));
     if (m->nb) {
         o.blk_slot = m->d_blk_slot + m->pair_bar;
         o.diag_slot = m->d_dslot + m->dslot_bar;
+        o.h = nullptr;
+        o.bprop = bt.bprop;
+        o.bprop_stride = JFG_BAR_PROP * m->nb;
+        dim3 grid((unsigned)cdiv(3 * m->nb, 128), nv);
         if (kg)
-            bar_kg_kernel<<<(unsigned)cdiv(3 * m->nb, 128), 128, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR,
-                                                                             du, o);
+            bar_kg_kernel<<<grid, 128, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, du, o);
         else
-            bar_k_kernel<<<(unsigned)cdiv(3 * m->nb, 128), 128, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, o);
+            bar_k_kernel<<<grid, 128, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, o);
         CK(cudaGetLastError());
     }
     CK(cudaEventRecord(m->ev[3], m->stream));
     return JFG_OK;
 }
 
-jfg_status launch_reduce(jfg_model *m, double *nz, double *ddiag) {
+jfg_status launch_reduce(jfg_model *m, const Batch &bt) {
+    const unsigned nv = (unsigned)bt.n_var;
     if (m->n_xkey) {
-        exc_chunk_kernel<<<(unsigned)cdiv(m->n_xchunk * 32, 256), 256, 0, m->stream>>>(m->n_xchunk, m->d_x_cseg, m->d_x_src,
-                                                                                  m->d_x_w, m->d_exc_raw, m->d_x_part);
+        exc_chunk_kernel<<<dim3((unsigned)cdiv(m->n_xchunk * 32, 256), nv), 256, 0, m->stream>>>(
+            m->n_xchunk, m->d_x_cseg, m->d_x_src, m->d_x_w, bt.exc_raw, bt.x_part, bt.exc_stride, bt.part_stride);
         CK(cudaGetLastError());
-        exc_key_kernel<<<(unsigned)cdiv(m->n_xkey * 32, 256), 256, 0, m->stream>>>(m->n_xkey, m->d_x_kchunk, m->d_x_part,
-                                                                              m->d_x_pos, nz);
+        exc_key_kernel<<<dim3((unsigned)cdiv(m->n_xkey * 32, 256), nv), 256, 0, m->stream>>>(
+            m->n_xkey, m->d_x_kchunk, bt.x_part, m->d_x_pos, bt.nz, bt.part_stride, m->nnz);
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(m->ev[4], m->stream));
     if (m->n_blk)
-        block_reduce_kernel<<<(unsigned)cdiv(m->n_blk * 6, 256), 256, 0, m->stream>>>(
-            m->n_blk, m->d_blk_seg, m->d_staging, m->d_blk_A, m->d_blk_B, m->d_blk_offAB, m->d_blk_offBA, m->d_rowptr, nz);
+        block_reduce_kernel<<<dim3((unsigned)cdiv(m->n_blk * 6, 256), nv), 256, 0, m->stream>>>(
+            m->n_blk, m->d_blk_seg, bt.staging, m->d_blk_A, m->d_blk_B, m->d_blk_offAB, m->d_blk_offBA, m->d_rowptr, bt.nz,
+            bt.staging_stride, m->nnz);
     CK(cudaGetLastError());
     CK(cudaEventRecord(m->ev[5], m->stream));
-    if (ddiag)
-        diag_reduce_kernel<<<(unsigned)cdiv(m->ndof, 256), 256, 0, m->stream>>>(m->ndof, m->d_dseg, m->d_dstaging, ddiag);
+    if (bt.ddiag)
+        diag_reduce_kernel<<<dim3((unsigned)cdiv(m->ndof, 256), nv), 256, 0, m->stream>>>(m->ndof, m->d_dseg, bt.dstaging, bt.ddiag,
+                                                                                     bt.dstage_stride);
     CK(cudaGetLastError());
     CK(cudaEventRecord(m->ev[6], m->stream));
     return JFG_OK;
@@ -1185,24 +1263,42 @@ jfg_status launch_reduce(jfg_model *m, double *nz, double *ddiag) {
 
 jfg_status begin_set(jfg_model *m, int kind);
 
-jfg_status launch_k(jfg_model *m, double *nz, double *dmax, double *ddiag) {
+jfg_status launch_k(jfg_model *m, const Batch &bt) {
     jfg_status st = begin_set(m, 0);
     if (st) return st;
-    if (dmax) CK(cudaMemsetAsync(dmax, 0, sizeof(double), m->stream));
-    st = launch_elements(m, false, nullptr, dmax, ddiag);
+    if (bt.dmax) CK(cudaMemsetAsync(bt.dmax, 0, sizeof(double) * bt.n_var, m->stream));
+    st = launch_elements(m, false, bt);
     if (st) return st;
-    return launch_reduce(m, nz, ddiag);
+    return launch_reduce(m, bt);
 }
 
-jfg_status launch_kg(jfg_model *m, const double *du, double *nz) {
+jfg_status launch_kg(jfg_model *m, const Batch &bt) {
     if (m->bar_offsets)
         return fail(m, JFG_ERR_REFERENCE_RAISES,
                     "assemble_geometric_stiffness raises BoundsError for CBAR/CBEAM with offsets (assembly.jl:6326)");
     jfg_status st = begin_set(m, 1);
     if (st) return st;
-    st = launch_elements(m, true, du, nullptr, nullptr);
+    Batch b = bt;
+    b.dmax = nullptr;
+    b.ddiag = nullptr;
+    st = launch_elements(m, true, b);
     if (st) return st;
-    return launch_reduce(m, nz, nullptr);
+    return launch_reduce(m, b);
+}
+
+jfg_status launch_k(jfg_model *m, double *nz, double *dmax, double *ddiag) {
+    Batch b = single_batch(m);
+    b.nz = nz;
+    b.dmax = dmax;
+    b.ddiag = ddiag;
+    return launch_k(m, b);
+}
+
+jfg_status launch_kg(jfg_model *m, const double *du, double *nz) {
+    Batch b = single_batch(m);
+    b.u = du;
+    b.nz = nz;
+    return launch_kg(m, b);
 }
 
 // Complete one event set: per-kernel times into the accumulators and "last".
@@ -1261,6 +1357,68 @@ jfg_status jfg_assemble_kg_device(jfg_model *m, const double *u_dev, double *nzv
     if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
     if (!u_dev || !nzval_dev) return fail(m, JFG_ERR_INVALID, "null pointer");
     return launch_kg(m, u_dev, nzval_dev);
+}
+
+jfg_status jfg_batch_workspace_bytes(jfg_model *m, int32_t n_var, int64_t *bytes) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    if (n_var < 0 || !bytes) return fail(m, JFG_ERR_INVALID, "bad arguments");
+    *bytes = 8 * batch_sizes(m).total * (int64_t)n_var;
+    return JFG_OK;
+}
+
+jfg_status jfg_batch_reserve(jfg_model *m, int32_t n_var) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    if (n_var < 1 || n_var > 65535) return fail(m, JFG_ERR_INVALID, "n_var must be in [1, 65535]");
+    if (n_var <= m->b_cap) return JFG_OK;
+    CK(cudaStreamSynchronize(m->stream));
+    if (m->d_bw) {
+        CK(cudaFree(m->d_bw));
+        m->d_bw = nullptr;
+        m->b_cap = 0;
+    }
+    const int64_t per = batch_sizes(m).total;
+    CK(cudaMalloc((void **)&m->d_bw, sizeof(double) * std::max<int64_t>(per * n_var, 1)));
+    m->b_cap = n_var;
+    return JFG_OK;
+}
+
+jfg_status jfg_assemble_batch_device(jfg_model *m, int32_t n_var, const double *h_dev, const double *bar_prop_dev,
+                                     const double *u_dev, int64_t u_stride, double *nzk_dev, double *max_dev, double *diag_dev,
+                                     double *nzkg_dev) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    if (n_var < 1 || n_var > m->b_cap)
+        return fail(m, JFG_ERR_INVALID, "n_var must be in [1, reserved variants]; call jfg_batch_reserve first");
+    if (nzkg_dev && !u_dev) return fail(m, JFG_ERR_INVALID, "KG needs u");
+    if (u_stride != 0 && u_stride != m->ndof) return fail(m, JFG_ERR_INVALID, "u_stride must be 0 (shared u) or ndof");
+    if (!nzk_dev && (max_dev || diag_dev)) return fail(m, JFG_ERR_INVALID, "max/diag outputs belong to K");
+    const BatchSizes z = batch_sizes(m);
+    Batch b;
+    b.n_var = n_var;
+    b.staging = m->d_bw;
+    b.exc_raw = b.staging + z.staging * n_var;
+    b.x_part = b.exc_raw + z.exc * n_var;
+    b.dstaging = b.x_part + z.part * n_var;
+    b.staging_stride = z.staging;
+    b.exc_stride = z.exc;
+    b.part_stride = z.part;
+    b.dstage_stride = z.dstage;
+    b.h = h_dev;
+    b.bprop = bar_prop_dev;
+    b.u = u_dev;
+    b.u_stride = u_stride;
+    jfg_status st = JFG_OK;
+    if (nzk_dev) {
+        b.nz = nzk_dev;
+        b.dmax = max_dev;
+        b.ddiag = diag_dev;
+        st = launch_k(m, b);
+        if (st) return st;
+    }
+    if (nzkg_dev) {
+        b.nz = nzkg_dev;
+        st = launch_kg(m, b);
+    }
+    return st;
 }
 
 jfg_status jfg_assemble_k(jfg_model *m, double *nzval, double *max_elem_stiff, double *orig_diag) {

@@ -21,7 +21,11 @@ LIB_PATH = os.path.join(PKG, "libjfemgpu.so")
 # every entry point declared in include/jfem_gpu.h
 EXPORTS = ("jfg_model_create", "jfg_pattern", "jfg_pattern_fill", "jfg_assemble_k", "jfg_assemble_kg",
            "jfg_assemble_k_device", "jfg_assemble_kg_device", "jfg_update_properties", "jfg_constraint_map",
-           "jfg_set_stream", "jfg_last_timing", "jfg_kernel_timing", "jfg_timing_accumulated", "jfg_model_stats", "jfg_assemble_k_quad4_noalloc", "jfg_model_destroy", "jfg_last_error", "jfg_version")
+           "jfg_set_stream", "jfg_last_timing", "jfg_kernel_timing", "jfg_timing_accumulated", "jfg_model_stats", "jfg_model_counts", "jfg_batch_workspace_bytes",
+           "jfg_batch_reserve", "jfg_assemble_batch_device", "jfg_server_create", "jfg_server_submit", "jfg_server_wait",
+           "jfg_server_result", "jfg_server_release", "jfg_server_stats", "jfg_server_family_batch",
+           "jfg_server_hold", "jfg_server_last_error", "jfg_server_destroy", "jfg_assemble_k_quad4_noalloc", "jfg_model_destroy", "jfg_last_error",
+           "jfg_version")
 
 _lib = None
 
@@ -43,13 +47,17 @@ def load(path: str = LIB_PATH):
     global _lib
     if _lib is not None:
         return _lib
-    if not os.path.exists(path):
+    from . import build as _b
+    if path == LIB_PATH and _b.needs_build():
         try:
-            from .build import build
-            build()
+            _b.build()
         except Exception as exc:  # pragma: no cover - reported loudly below
-            raise RuntimeError(f"CUDA library {path} missing and could not be built: {exc}") from exc
+            raise RuntimeError(f"CUDA library {path} is missing or stale and could not be built: {exc}") from exc
     L = C.CDLL(path)
+    L.jfg_version.restype = C.c_char_p
+    ver = L.jfg_version().decode()
+    if path == LIB_PATH and not ver.endswith("src " + _b.source_hash()):
+        raise RuntimeError(f"{path} was built from other sources ({ver}); rebuild it (jf_2026_05_19_b200/build.py --force)")
     L.jfg_model_create.argtypes = [C.POINTER(JfgModelDesc), C.POINTER(C.c_void_p)]
     L.jfg_model_create.restype = C.c_int32
     L.jfg_pattern.argtypes = [C.c_void_p, _pi64, _pi64]
@@ -67,6 +75,24 @@ def load(path: str = LIB_PATH):
     L.jfg_assemble_k_quad4_noalloc.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
                                                C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.jfg_timing_accumulated.argtypes = [C.c_void_p, C.c_int, _pd, _pi64, C.c_int]
+    L.jfg_batch_workspace_bytes.argtypes = [C.c_void_p, C.c_int32, _pi64]
+    L.jfg_batch_reserve.argtypes = [C.c_void_p, C.c_int32]
+    L.jfg_assemble_batch_device.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.jfg_model_counts.argtypes = [C.c_void_p, _pi64]
+    _pp = C.POINTER(C.c_void_p)
+    L.jfg_server_create.argtypes = [_pp, _pp, C.c_int32, C.c_int64, C.c_int32, C.c_int32, _pp]
+    L.jfg_server_submit.argtypes = [C.c_void_p, C.c_int32, _pd, C.c_int32, _pi64]
+    L.jfg_server_wait.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.POINTER(C.c_int32)]
+    L.jfg_server_result.argtypes = [C.c_void_p, C.c_int64, _pp, _pp, _pp, _pd]
+    L.jfg_server_release.argtypes = [C.c_void_p, C.c_int64]
+    L.jfg_server_stats.argtypes = [C.c_void_p, _pi64]
+    L.jfg_server_family_batch.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]
+    L.jfg_server_hold.argtypes = [C.c_void_p, C.c_int32]
+    L.jfg_server_last_error.argtypes = [C.c_void_p]
+    L.jfg_server_last_error.restype = C.c_char_p
+    L.jfg_server_destroy.argtypes = [C.c_void_p]
+    L.jfg_server_destroy.restype = None
     L.jfg_model_destroy.argtypes = [C.c_void_p]
     L.jfg_model_destroy.restype = None
     L.jfg_last_error.argtypes = [C.c_void_p]
@@ -75,7 +101,10 @@ def load(path: str = LIB_PATH):
     for name in ("jfg_pattern", "jfg_pattern_fill", "jfg_assemble_k", "jfg_assemble_kg", "jfg_assemble_k_device",
                  "jfg_assemble_kg_device", "jfg_update_properties", "jfg_constraint_map", "jfg_set_stream",
                  "jfg_last_timing", "jfg_kernel_timing", "jfg_timing_accumulated", "jfg_model_stats",
-                 "jfg_assemble_k_quad4_noalloc"):
+                 "jfg_assemble_k_quad4_noalloc", "jfg_model_counts", "jfg_batch_workspace_bytes", "jfg_batch_reserve",
+                 "jfg_assemble_batch_device", "jfg_server_create", "jfg_server_submit", "jfg_server_wait",
+                 "jfg_server_result", "jfg_server_release", "jfg_server_stats", "jfg_server_family_batch",
+                 "jfg_server_hold"):
         getattr(L, name).restype = C.c_int32
     _lib = L
     return L
@@ -109,6 +138,13 @@ class GpuModel:
     def _check(self, st: int):
         if st != 0:
             raise JfgError(st, self.L.jfg_last_error(self.h).decode())
+
+    @property
+    def counts(self) -> list:
+        """[n_nodes, n_quad4, n_tria3, n_bar] of this handle."""
+        o = np.zeros(4, np.int64)
+        self._check(self.L.jfg_model_counts(self.h, _ptr(o, _pi64)))
+        return o.tolist()
 
     def close(self):
         if self.h:
@@ -161,6 +197,24 @@ class GpuModel:
     def assemble_kg_device(self, u_ptr: int, nz_ptr: int):
         self._check(self.L.jfg_assemble_kg_device(self.h, C.c_void_p(u_ptr), C.c_void_p(nz_ptr)))
 
+    # -- batched variants (device pointers) --------------------------------
+    def batch_workspace_bytes(self, n_var: int) -> int:
+        b = C.c_int64()
+        self._check(self.L.jfg_batch_workspace_bytes(self.h, int(n_var), C.byref(b)))
+        return b.value
+
+    def batch_reserve(self, n_var: int):
+        self._check(self.L.jfg_batch_reserve(self.h, int(n_var)))
+
+    def assemble_batch_device(self, n_var: int, h_ptr: int = 0, bar_prop_ptr: int = 0, u_ptr: int = 0,
+                              u_stride: Optional[int] = None, nzk_ptr: int = 0, max_ptr: int = 0, diag_ptr: int = 0,
+                              nzkg_ptr: int = 0):
+        """K and/or KG for n_var variants sharing this model's mesh and pattern."""
+        us = self.ndof if u_stride is None else int(u_stride)
+        v = lambda p: C.c_void_p(p or None)
+        self._check(self.L.jfg_assemble_batch_device(self.h, int(n_var), v(h_ptr), v(bar_prop_ptr), v(u_ptr), us,
+                                                     v(nzk_ptr), v(max_ptr), v(diag_ptr), v(nzkg_ptr)))
+
     def set_stream(self, stream_ptr: int):
         self._check(self.L.jfg_set_stream(self.h, C.c_void_p(stream_ptr or None)))
 
@@ -204,3 +258,89 @@ class GpuModel:
 
 def version() -> str:
     return load().jfg_version().decode()
+
+
+SERVE_BATCHED, SERVE_SERIAL = 0, 1
+
+
+class Server:
+    """Device-resident request loop over model families (jfg_server_* in the C ABI).
+
+    Each request carries a new shell-thickness vector for one family and gets
+    that family's K (and KG when the family has a displacement field); the
+    results stay on the device until released.  The GpuModel handles must
+    outlive the server, which uses them exclusively while it runs.
+    """
+
+    def __init__(self, models, u=None, hbm_budget_bytes: int = 150 * 10**9, max_batch: int = 32,
+                 policy: int = SERVE_BATCHED):
+        self.L = load()
+        self.models = list(models)
+        n = len(self.models)
+        hs = (C.c_void_p * n)(*[m.h.value for m in self.models])
+        self._u = [None if (u is None or u[i] is None) else np.ascontiguousarray(u[i], np.float64) for i in range(n)]
+        us = (C.c_void_p * n)(*[None if a is None else a.ctypes.data for a in self._u])
+        out = C.c_void_p()
+        st = self.L.jfg_server_create(hs, us, n, int(hbm_budget_bytes), int(max_batch), int(policy), C.byref(out))
+        if st != 0:
+            raise JfgError(st, "jfg_server_create failed (status %d)" % st)
+        self.s = out.value
+        self.n_shell = [int(m.counts[1] + m.counts[2]) for m in self.models]
+
+    def _check(self, st: int):
+        if st != 0:
+            raise JfgError(st, self.L.jfg_server_last_error(self.s).decode())
+
+    def submit(self, family: int, h: np.ndarray, keep: bool = True) -> int:
+        h = np.ascontiguousarray(h, np.float64)
+        if h.shape != (self.n_shell[family],):
+            raise ValueError(f"family {family} takes {self.n_shell[family]} thicknesses")
+        t = C.c_int64()
+        self._check(self.L.jfg_server_submit(self.s, int(family), _ptr(h, _pd), int(keep), C.byref(t)))
+        return t.value
+
+    def wait(self, ticket: int, timeout: float = -1.0) -> bool:
+        d = C.c_int32()
+        self._check(self.L.jfg_server_wait(self.s, int(ticket), float(timeout), C.byref(d)))
+        return bool(d.value)
+
+    def result(self, ticket: int):
+        """(K ptr, KG ptr or None, max ptr, (t_submit, t_launch, t_done)) of a finished request."""
+        a, b, c = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        t = np.zeros(3)
+        self._check(self.L.jfg_server_result(self.s, int(ticket), C.byref(a), C.byref(b), C.byref(c), _ptr(t, _pd)))
+        return a.value, b.value, c.value, tuple(t.tolist())
+
+    def release(self, ticket: int):
+        self._check(self.L.jfg_server_release(self.s, int(ticket)))
+
+    def stats(self) -> dict:
+        o = np.zeros(6, np.int64)
+        self._check(self.L.jfg_server_stats(self.s, _ptr(o, _pi64)))
+        return dict(zip(("submitted", "completed", "batches", "max_batch", "reserved_bytes", "queued"), o.tolist()))
+
+    def hold(self, on: bool = True):
+        """Queue requests without launching them while on; off admits the queue."""
+        self._check(self.L.jfg_server_hold(self.s, int(on)))
+
+    def batch_limit(self, family: int) -> int:
+        b = C.c_int32()
+        self._check(self.L.jfg_server_family_batch(self.s, int(family), C.byref(b)))
+        return b.value
+
+    def close(self):
+        if getattr(self, "s", None):
+            self.L.jfg_server_destroy(self.s)
+            self.s = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
