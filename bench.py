@@ -47,7 +47,13 @@ def parse_args():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["barrel", "barrel_medium", "barrel_small", "panel", "plate"], default="barrel")
+    p.add_argument("--workload", choices=["barrel", "barrel_medium", "barrel_small", "panel", "plate", "serving"],
+                   default="barrel")
+    p.add_argument("--rates", type=str, default="100,1000,5000", help="serving: Poisson arrival rates, req/s")
+    p.add_argument("--requests", type=int, default=256, help="serving: requests per rate (server arms)")
+    p.add_argument("--plain-requests", type=int, default=48, help="serving: requests per rate (plain arm)")
+    p.add_argument("--max-batch", type=int, default=32, help="serving: batch limit per family")
+    p.add_argument("--hbm-budget-gb", type=float, default=150.0, help="serving: device memory budget")
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -267,8 +273,189 @@ def run_reference(args):
     return 0
 
 
+SERVE_METRIC = "served K+KG requests/s, mixed 8-family stream (p50/p99 latency beside)"
+
+
+def serving_setup(seed: int = 0):
+    """Eight families (1.6k-596k elements), their u fields and per-family thickness pools."""
+    from jf_2026_05_19_b200 import decks
+    fams = decks.serving_families(seed=seed)
+    us = [decks.smooth_displacement(m, seed=20 + i) for i, m in enumerate(fams)]
+    rng = np.random.default_rng(seed + 1)
+    pools = []
+    for m in fams:
+        base = np.concatenate([m.q4_prop[:, 0], m.t3_prop[:, 0]])
+        pools.append([base * np.exp(0.1 * rng.standard_normal(base.shape[0])) for _ in range(4)])
+    return fams, us, pools
+
+
+def serving_stream(rate: float, n: int, n_fam: int, seed: int):
+    """Poisson arrivals: (arrival s, family, pool index); identical for every arm at one rate."""
+    rng = np.random.default_rng(1000 + seed + int(rate))
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    return [(float(t[i]), int(rng.integers(n_fam)), int(rng.integers(4))) for i in range(n)]
+
+
+def latency_summary(lat, t_first, t_last, n):
+    lat = np.asarray(lat)
+    return {"requests": int(n), "throughput_req_s": n / max(t_last - t_first, 1e-9),
+            "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "mean_ms": float(lat.mean() * 1e3)}
+
+
+def run_server_stream(native, srv, stream, pools):
+    """Submit at the arrival times (open loop); a collector waits, reads times and releases."""
+    import queue
+    import threading
+    q = queue.Queue()
+    rec = []
+
+    def collect():
+        while True:
+            t = q.get()
+            if t is None:
+                return
+            srv.wait(t, -1.0)
+            rec.append(srv.result(t)[3])
+            srv.release(t)
+
+    th = threading.Thread(target=collect)
+    th.start()
+    t0 = time.perf_counter()
+    lag = 0.0
+    for (ta, f, k) in stream:
+        while True:
+            now = time.perf_counter() - t0
+            if now >= ta:
+                break
+            if ta - now > 2e-4:
+                time.sleep(min(ta - now - 1e-4, 0.01))
+        lag = max(lag, time.perf_counter() - t0 - ta)
+        q.put(srv.submit(f, pools[f][k], keep=False))
+    q.put(None)
+    th.join()
+    ts = np.array(rec)
+    out = latency_summary(ts[:, 2] - ts[:, 0], ts[:, 0].min(), ts[:, 2].max(), len(rec))
+    out["max_submit_lag_ms"] = lag * 1e3
+    return out
+
+
+def run_plain_stream(native, torch, fams, us_dev, pools, stream, nz_bufs):
+    """The plain one-deck-per-launch GPU path: per request, build the model on the GPU
+    (pattern and maps), assemble K and KG into device buffers, wait, free it."""
+    t0 = time.perf_counter()
+    lat, done = [], []
+    for (ta, f, k) in stream:
+        while time.perf_counter() - t0 < ta:
+            time.sleep(1e-4)
+        m = fams[f]
+        h = pools[f][k]
+        nq = m.q4_nodes.shape[0]
+        with native.GpuModel(m.with_thickness(h[:nq], h[nq:])) as g:
+            nzk, nzg = nz_bufs[f]
+            g.assemble_k_device(nzk.data_ptr())
+            g.assemble_kg_device(us_dev[f].data_ptr(), nzg.data_ptr())
+            torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+        lat.append(t - ta)
+        done.append(t)
+    return latency_summary(lat, stream[0][0], max(done), len(stream))
+
+
+def run_serving(args):
+    import torch
+    from jf_2026_05_19_b200 import native
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(0)
+    rates = [float(r) for r in args.rates.split(",")]
+    fams, us, pools = serving_setup()
+    sizes = [m.n_elements for m in fams]
+    models = [native.GpuModel(m) for m in fams]
+    launches_per_batch = [2 * (sum(1 for c in ("quad4", "tria3", "bar") if m.counts()[c]) + 1 +
+                               (2 if m.rbe2_master.shape[0] else 0)) for m in fams]
+    arms = {}
+    clocks = ClockSampler(uuid=device_uuid(torch, torch.device("cuda", 0)), index=0)
+    clocks.start()
+    for name, policy in (("batched", native.SERVE_BATCHED), ("serial_resident", native.SERVE_SERIAL)):
+        with native.Server(models, us, hbm_budget_bytes=int(args.hbm_budget_gb * 1e9), max_batch=args.max_batch,
+                           policy=policy) as srv:
+            warm = [srv.submit(f, pools[f][0], keep=False) for f in range(len(fams))]
+            for t in warm:
+                srv.wait(t, -1.0); srv.release(t)
+            res = {}
+            b0 = srv.stats()["batches"]
+            for r in rates:
+                res[f"{r:g}"] = run_server_stream(native, srv, serving_stream(r, args.requests, len(fams), 0), pools)
+            st = srv.stats()
+            res["batches"] = st["batches"] - b0
+            res["largest_batch"] = st["max_batch"]
+            res["reserved_gb"] = st["reserved_bytes"] / 1e9
+            res["batch_limits"] = [srv.batch_limit(f) for f in range(len(fams))]
+            arms[name] = res
+    for g in models:
+        g.close()
+    torch.cuda.synchronize()
+    us_dev = [torch.from_numpy(u).cuda() for u in us]
+    nz_bufs = []
+    for m in fams:
+        with native.GpuModel(m) as g:
+            nz_bufs.append((torch.empty(g.nnz, dtype=torch.float64, device="cuda"),
+                            torch.empty(g.nnz, dtype=torch.float64, device="cuda")))
+    plain = {}
+    for r in rates:
+        plain[f"{r:g}"] = run_plain_stream(native, torch, fams, us_dev, pools,
+                                           serving_stream(r, args.plain_requests, len(fams), 0), nz_bufs)
+    arms["plain_one_deck_per_launch"] = plain
+    clk = clocks.stop()
+    top = f"{max(rates):g}"
+    v = arms["batched"][top]["throughput_req_s"]
+    mean_shell = float(np.mean([p[0].shape[0] for p in pools]))
+    line = {"metric": SERVE_METRIC, "value": v, "unit": "req/s", "n_gpus": 1, "steps": args.requests,
+            "warmup": len(fams), "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded plate/panel/barrel families, Poisson arrivals, lognormal(0.1) thickness vectors",
+            "config": {"workload": "serving: 8 device-resident families, K+KG per request, uniform family choice",
+                       "family_elements": sizes, "rates_req_s": rates, "hbm_budget_gb": args.hbm_budget_gb,
+                       "max_batch": args.max_batch, "value_at_rate": float(top)},
+            "serving": arms,
+            "speedup_at_top_rate": {
+                "vs_plain_one_deck_per_launch": v / arms["plain_one_deck_per_launch"][top]["throughput_req_s"],
+                "vs_serial_resident": v / arms["serial_resident"][top]["throughput_req_s"]},
+            "e2e": {"value": v, "unit": "req/s", "h2d_bytes_per_step": 8 * mean_shell, "d2h_bytes_per_step": 0,
+                    "note": "submit-to-done wall clock through the server's C ABI; thickness vectors copied in, "
+                            "K and KG stay on the device"},
+            "gpu_launches": int(arms["batched"]["batches"] * float(np.mean(launches_per_batch))),
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_reference_serving(args):
+    """Oracle port, one request at a time: elements/s on the bounded barrel sample,
+    converted with the stream's mean request size."""
+    from jf_2026_05_19_b200 import decks
+    v_el, threads, sample = time_cpu_oracle(args.cpu_seconds)
+    fams = decks.serving_families()
+    mean_el = float(np.mean([m.n_elements for m in fams]))
+    v = v_el / mean_el
+    line = {"metric": SERVE_METRIC, "value": v, "unit": "req/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded families)",
+            "config": {"workload": "serving: 8 families, uniform family choice", "mean_request_elements": mean_el},
+            "cpu_baseline": {"value": v, "unit": "req/s", "cores": threads, "kind": "port",
+                             "sample": sample + f"; req/s = elements/s / {mean_el:.0f} mean elements per request"},
+            "e2e": {"value": v, "unit": "req/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
+    if args.workload == "serving":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return 0  # one GPU serves; other ranks have nothing to do
+        return run_reference_serving(args) if args.impl == "reference" else run_serving(args)
     if args.impl == "reference":
         return run_reference(args)
     import torch

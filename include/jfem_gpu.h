@@ -224,8 +224,10 @@ typedef struct jfg_server jfg_server;
  * each) for KG, or NULL entries / NULL array for K only. */
 jfg_status jfg_server_create(jfg_model *const *families, const double *const *u_host, int32_t n_families,
                              int64_t hbm_budget_bytes, int32_t max_batch, int32_t policy, jfg_server **out);
-/* Queue a request (the thickness vector is copied); keep = 0 drops the
- * results as soon as they are computed (timing only). */
+/* Queue a request (the thickness vector is copied).  keep = 0 returns the
+ * result slot as soon as the request is computed (timing only: its record
+ * and times stay readable until jfg_server_release, its result pointers are
+ * NULL). */
 jfg_status jfg_server_submit(jfg_server *s, int32_t family, const double *h_host, int32_t keep, int64_t *ticket);
 /* Wait until the request is done (timeout_s < 0: no limit); *done = 1 when finished. */
 jfg_status jfg_server_wait(jfg_server *s, int64_t ticket, double timeout_s, int32_t *done);

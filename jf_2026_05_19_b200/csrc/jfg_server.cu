@@ -48,6 +48,7 @@ struct SrvRequest {
     int family = 0;
     std::vector<double> h;      // thickness vector, copied at submit
     bool keep = true;           // results kept until jfg_server_release
+    bool freed = false;         // keep == false: its slot share was returned at completion
     int state = 0;              // 0 queued, 1 launched, 2 done
     int slot = -1, var = -1;
     double t_submit = 0, t_launch = 0, t_done = 0;
@@ -136,8 +137,8 @@ void CUDART_CB batch_done(void *p) {
             if (it == s->reqs.end()) continue;
             it->second.state = 2;
             it->second.t_done = t;
-            if (!it->second.keep) {
-                s->reqs.erase(it);
+            if (!it->second.keep) {  // results dropped now; the record (times) stays until released
+                it->second.freed = true;
                 sl.unreleased -= 1;
             }
         }
@@ -372,9 +373,9 @@ jfg_status jfg_server_result(jfg_server *s, int64_t ticket, double **nzk_dev, do
     if (r.state != 2) return sfail(s, JFG_ERR_STATE, "request not finished");
     const Family &f = s->fam[r.family];
     const Slot &sl = f.slots[r.slot];
-    if (nzk_dev) *nzk_dev = sl.nzk + (int64_t)r.var * f.nnz;
-    if (nzkg_dev) *nzkg_dev = sl.nzkg ? sl.nzkg + (int64_t)r.var * f.nnz : nullptr;
-    if (max_dev) *max_dev = sl.max + r.var;
+    if (nzk_dev) *nzk_dev = r.freed ? nullptr : sl.nzk + (int64_t)r.var * f.nnz;
+    if (nzkg_dev) *nzkg_dev = (r.freed || !sl.nzkg) ? nullptr : sl.nzkg + (int64_t)r.var * f.nnz;
+    if (max_dev) *max_dev = r.freed ? nullptr : sl.max + r.var;
     if (times3) { times3[0] = r.t_submit; times3[1] = r.t_launch; times3[2] = r.t_done; }
     return JFG_OK;
 }
@@ -387,9 +388,12 @@ jfg_status jfg_server_release(jfg_server *s, int64_t ticket) {
         if (it == s->reqs.end()) return sfail(s, JFG_ERR_INVALID, "unknown or released ticket");
         if (it->second.state != 2) return sfail(s, JFG_ERR_STATE, "request not finished");
         Slot &sl = s->fam[it->second.family].slots[it->second.slot];
+        const bool freed = it->second.freed;
         s->reqs.erase(it);
-        sl.unreleased -= 1;
-        if (sl.unreleased == 0 && !sl.batch) sl.busy = false;
+        if (!freed) {
+            sl.unreleased -= 1;
+            if (sl.unreleased == 0 && !sl.batch) sl.busy = false;
+        }
     }
     s->cv.notify_all();
     return JFG_OK;
