@@ -47,13 +47,14 @@ def parse_args():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["barrel", "barrel_medium", "barrel_small", "panel", "plate", "serving"],
+    p.add_argument("--workload", choices=["barrel", "barrel_medium", "barrel_small", "panel", "plate", "serving", "variants"],
                    default="barrel")
     p.add_argument("--rates", type=str, default="100,1000,5000", help="serving: Poisson arrival rates, req/s")
     p.add_argument("--requests", type=int, default=256, help="serving: requests per rate (server arms)")
     p.add_argument("--plain-requests", type=int, default=48, help="serving: requests per rate (plain arm)")
     p.add_argument("--max-batch", type=int, default=32, help="serving: batch limit per family")
     p.add_argument("--hbm-budget-gb", type=float, default=150.0, help="serving: device memory budget")
+    p.add_argument("--variants", type=int, default=256, help="variants: design variants in one batch")
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -431,6 +432,132 @@ def run_serving(args):
     return 0
 
 
+def run_variants(args):
+    """256 stiffened-panel design variants (own thickness vector and stringer section each)
+    assembled as one batch: K and KG for every variant per graph replay."""
+    import torch
+    from jf_2026_05_19_b200 import decks, native, roofline
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    nv = args.variants
+    ms = [decks.panel_variant_c3(v, no_offset=True) for v in range(nv)]
+    base = ms[0]
+    u = decks.smooth_displacement(base, seed=1)
+    H = np.stack([np.concatenate([m.q4_prop[:, 0], m.t3_prop[:, 0]]) for m in ms])
+    BP = np.stack([m.bar_prop for m in ms])
+    g = native.GpuModel(base)
+    g.batch_reserve(nv)
+    s = torch.cuda.Stream()
+    g.set_stream(s.cuda_stream)
+    Hd, BPd, ud = (torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in (H, BP, u))
+    nzk = torch.empty(nv, g.nnz, dtype=torch.float64, device=dev)
+    nzg = torch.empty_like(nzk)
+    mx = torch.zeros(nv, dtype=torch.float64, device=dev)
+
+    def call():
+        g.assemble_batch_device(nv, Hd.data_ptr(), BPd.data_ptr(), ud.data_ptr(), 0, nzk.data_ptr(), mx.data_ptr(), 0,
+                                nzg.data_ptr())
+
+    torch.cuda.synchronize()
+    for _ in range(2):
+        call()
+    s.synchronize()
+    # per-kernel split from timed direct calls
+    g.timing_accumulated("k", reset=True); g.timing_accumulated("kg", reset=True)
+    for _ in range(3):
+        call()
+    s.synchronize()
+    kt, kn = g.timing_accumulated("k", reset=True)
+    gt, gn = g.timing_accumulated("kg", reset=True)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=s):
+        call()
+    for _ in range(max(args.warmup, 3)):
+        graph.replay()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(uuid=device_uuid(torch, dev), index=0)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    with torch.cuda.stream(s):
+        for _ in range(args.steps):
+            graph.replay()
+    e1.record(s)
+    e1.synchronize()
+    clk = clocks.stop()
+    el = e0.elapsed_time(e1) / 1e3 / args.steps
+    # one launch sequence per variant (no batching, no graph)
+    p0 = torch.cuda.Event(enable_timing=True); p1 = torch.cuda.Event(enable_timing=True)
+    p0.record(s)
+    for v in range(nv):
+        g.assemble_batch_device(1, Hd[v].data_ptr(), BPd[v].data_ptr(), ud.data_ptr(), 0, nzk[v].data_ptr(),
+                                mx[v:].data_ptr(), 0, nzg[v].data_ptr())
+    p1.record(s)
+    p1.synchronize()
+    per_variant = p0.elapsed_time(p1) / 1e3
+    # end to end: inputs from pinned host memory, graph replay, per-variant max read back
+    Hp = torch.from_numpy(H).pin_memory(); BPp = torch.from_numpy(BP).pin_memory()
+    mxp = torch.empty(nv, dtype=torch.float64).pin_memory()
+    q0 = torch.cuda.Event(enable_timing=True); q1 = torch.cuda.Event(enable_timing=True)
+    q0.record(s)
+    with torch.cuda.stream(s):
+        for _ in range(args.e2e_steps):
+            Hd.copy_(Hp, non_blocking=True); BPd.copy_(BPp, non_blocking=True)
+            graph.replay()
+            mxp.copy_(mx, non_blocking=True)
+    q1.record(s)
+    q1.synchronize()
+    e2e_el = q0.elapsed_time(q1) / 1e3 / args.e2e_steps
+    # parity of two variants against their own handles
+    for v in (0, nv - 1):
+        with native.GpuModel(ms[v]) as gv:
+            assert np.array_equal(gv.assemble_k()[0], nzk[v].cpu().numpy()), f"variant {v} K differs"
+            assert np.array_equal(gv.assemble_kg(u), nzg[v].cpu().numpy()), f"variant {v} KG differs"
+    del graph
+    g.set_stream(0)
+    n_el = nv * base.n_elements
+    counts = {k: nv * c for k, c in base.counts().items()}
+    per_kernel = {}
+    for tag, tt, nn in (("k", kt, kn), ("kg", gt, gn)):
+        for name in ("quad4", "tria3", "bar", "dof_reduce", "block_reduce"):
+            per_kernel[f"{name}_{tag}"] = tt[name] / max(nn, 1)
+    dom = max(per_kernel, key=per_kernel.get)
+    fp64 = measure_fp64_peak(torch, dev)
+    roof = {"bound": "tensor", "unit": "TFLOP/s", "kernel": dom, "peak": fp64, "traffic": None,
+            "peak_source": "FP64 DGEMM (torch.matmul float64 8192^3) measured in this run"}
+    if dom.startswith(("quad4", "tria3", "bar")):
+        roof["achieved"] = roofline.kernel_flops(dom, counts[dom.split("_")[0]]) / (per_kernel[dom] / 1e3) / 1e12
+    else:
+        st = g.stats()
+        mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+        hbm = json.load(open(mp))["hbm_gbs"] if os.path.exists(mp) else 6650.0
+        roof = {"bound": "hbm", "unit": "GB/s", "kernel": dom, "peak": hbm, "traffic": None,
+                "achieved": nv * (8 * st["staging_values"] + 20 * st["n_blocks"] + 8 * st["nnz"]) / (per_kernel[dom] / 1e3) / 1e9}
+    roof["frac"] = roof["achieved"] / roof["peak"]
+    roof["launch_ms"] = per_kernel[dom]
+    g.close()
+    line = {"metric": METRIC, "value": n_el / el, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": el * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: 256 seeded stiffened-panel variants (lognormal thickness, stringer height U[15,25])",
+            "config": {"workload": f"{nv} stiffened-panel design variants, K+KG of all in one CUDA-graph replay",
+                       "elements_per_variant": int(base.n_elements), "variants": nv, "elements_per_step": int(n_el),
+                       "nnz_per_variant": int(nzk.shape[1]),
+                       "l2": "outputs larger than L2", "parallelism": "one GPU, variants batched on blockIdx.y"},
+            "variants": {"graph_replay_ms": el * 1e3, "one_launch_sequence_per_variant_ms": per_variant * 1e3,
+                         "speedup_vs_per_variant_launches": per_variant / el,
+                         "kernel_ms_direct_call": per_kernel},
+            "roofline": roof,
+            "e2e": {"value": n_el / e2e_el, "unit": UNIT, "h2d_bytes_per_step": int(H.nbytes + BP.nbytes),
+                    "d2h_bytes_per_step": 8 * nv},
+            "gpu_launches": args.steps * 2 * (sum(1 for c in ("quad4", "tria3", "bar") if base.counts()[c]) + 1 +
+                                              (2 if base.rbe2_master.shape[0] else 0)),
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference_serving(args):
     """Oracle port, one request at a time: elements/s on the bounded barrel sample,
     converted with the stream's mean request size."""
@@ -452,6 +579,12 @@ def run_reference_serving(args):
 
 def main():
     args = parse_args()
+    if args.workload == "variants":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return 0
+        if args.impl == "reference":
+            return run_reference(args)
+        return run_variants(args)
     if args.workload == "serving":
         if int(os.environ.get("RANK", "0")) != 0:
             return 0  # one GPU serves; other ranks have nothing to do

@@ -102,6 +102,7 @@ struct jfg_model {
     static constexpr int kRing = 64;
     EvSet ring[kRing];
     int ring_head = 0, last_set = -1;
+    bool capturing = false;              // the current call is being captured into a graph
     cudaEvent_t *ev = nullptr;
     float last_elem_ms = 0.f, last_reduce_ms = 0.f, last_total_ms = 0.f;
     float last_kernel_ms[6] = {0, 0, 0, 0, 0, 0};  // quad4, tria3, bar, expand, reduce, diag
@@ -1179,6 +1180,9 @@ BatchSizes batch_sizes(const jfg_model *m) {
     return z;
 }
 
+// Timing event i of the current set (skipped while the stream is captured).
+cudaError_t mark(jfg_model *m, int i) { return m->capturing ? cudaSuccess : cudaEventRecord(m->ev[i], m->stream); }
+
 jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
     const unsigned nv = (unsigned)bt.n_var;
     ElemOut o;
@@ -1191,7 +1195,7 @@ jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
     o.dstage_stride = bt.dstage_stride;
     o.u_stride = bt.u_stride < 0 ? m->ndof : bt.u_stride;
     const double *du = bt.u;
-    CK(cudaEventRecord(m->ev[0], m->stream));
+    CK(mark(m, 0));
     if (m->nq) {
         o.blk_slot = m->d_blk_slot + m->pair_q4;
         o.diag_slot = m->d_dslot + m->dslot_q4;
@@ -1204,7 +1208,7 @@ jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
             q4_k_kernel<<<grid, Q4_THREADS, 0, m->stream>>>(m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, m->k6rot, o);
         CK(cudaGetLastError());
     }
-    CK(cudaEventRecord(m->ev[1], m->stream));
+    CK(mark(m, 1));
     if (m->nt) {
         o.blk_slot = m->d_blk_slot + m->pair_t3;
         o.diag_slot = m->d_dslot + m->dslot_t3;
@@ -1218,7 +1222,7 @@ jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
                 m->nt, m->d_t3n, m->d_t3p, m->d_coords, m->d_nodeR, m->k6rot, o);
         CK(cudaGetLastError());
     }
-    CK(cudaEventRecord(m->ev[2], m->stream));
+    CK(mark(m, 2));
     if (m->nb) {
         o.blk_slot = m->d_blk_slot + m->pair_bar;
         o.diag_slot = m->d_dslot + m->dslot_bar;
@@ -1232,7 +1236,7 @@ jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
             bar_k_kernel<<<grid, 128, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, o);
         CK(cudaGetLastError());
     }
-    CK(cudaEventRecord(m->ev[3], m->stream));
+    CK(mark(m, 3));
     return JFG_OK;
 }
 
@@ -1246,18 +1250,18 @@ jfg_status launch_reduce(jfg_model *m, const Batch &bt) {
             m->n_xkey, m->d_x_kchunk, bt.x_part, m->d_x_pos, bt.nz, bt.part_stride, m->nnz);
     }
     CK(cudaGetLastError());
-    CK(cudaEventRecord(m->ev[4], m->stream));
+    CK(mark(m, 4));
     if (m->n_blk)
         block_reduce_kernel<<<dim3((unsigned)cdiv(m->n_blk * 6, 256), nv), 256, 0, m->stream>>>(
             m->n_blk, m->d_blk_seg, bt.staging, m->d_blk_A, m->d_blk_B, m->d_blk_offAB, m->d_blk_offBA, m->d_rowptr, bt.nz,
             bt.staging_stride, m->nnz);
     CK(cudaGetLastError());
-    CK(cudaEventRecord(m->ev[5], m->stream));
+    CK(mark(m, 5));
     if (bt.ddiag)
         diag_reduce_kernel<<<dim3((unsigned)cdiv(m->ndof, 256), nv), 256, 0, m->stream>>>(m->ndof, m->d_dseg, bt.dstaging, bt.ddiag,
                                                                                      bt.dstage_stride);
     CK(cudaGetLastError());
-    CK(cudaEventRecord(m->ev[6], m->stream));
+    CK(mark(m, 6));
     return JFG_OK;
 }
 
@@ -1332,6 +1336,12 @@ jfg_status finish_timing(jfg_model *m) {
 
 // Select the next event set for an assembly call of the given kind.
 jfg_status begin_set(jfg_model *m, int kind) {
+    // Inside a stream capture nothing is timed: no host wait on an old event
+    // set and no event records (a graph replays the kernels only).
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(m->stream, &cs));
+    m->capturing = cs != cudaStreamCaptureStatusNone;
+    if (m->capturing) return JFG_OK;
     int idx = m->ring_head;
     jfg_status st = finish_set(m, idx);  // waits only if 64 calls are still in flight
     if (st) return st;
