@@ -198,6 +198,33 @@ jfg_status jfg_assemble_batch_device(jfg_model *m, int32_t n_var, const double *
                                      const double *u_dev, int64_t u_stride, double *nzk_dev, double *max_dev,
                                      double *diag_dev, double *nzkg_dev);
 
+/* ---- Free-dof submatrices for the solver --------------------------------
+ * The step right after assembly in the SOL 105 consumer: A_ff = A[free,
+ * free] and its symmetric part 0.5 * (A_ff + A_ff') for K
+ * (src/solver/boundary_conditions.jl:113-114) and Kg
+ * (src/solver/solve_case.jl:1908-1927), with Kg's diagnostics max|Kg_ff| and
+ * max|Kg_ff - Kg_ff'|.  As with Julia's sparse +, entries whose sum is
+ * exactly zero are not stored.  Done on the device, so only the free-dof
+ * matrices need to cross to the host. */
+
+/* Set the free dofs (1-based, strictly increasing; the host computes them
+ * from SPC, RBE2 dependents and AUTOSPC).  The first call also finds, once
+ * per pattern, where each stored entry's transpose lives (allocates). */
+jfg_status jfg_ff_set_free(jfg_model *m, const int64_t *free_dofs, int64_t n_free);
+
+/* Extract from device values nz_dev (a K or KG of this handle, CSC order):
+ * nnz of the symmetrised free-dof matrix, max|A_ff| and max|A_ff - A_ff'|.
+ * Runs on the handle's stream and waits for it. */
+jfg_status jfg_ff_extract_device(jfg_model *m, const double *nz_dev, int64_t *nnz_ff, double *max_abs,
+                                 double *max_asym);
+
+/* Host copies of the last extraction: 1-based CSC colptr (n_free + 1),
+ * rowval and nzval (nnz_ff each). */
+jfg_status jfg_ff_fetch(jfg_model *m, int64_t *colptr, int64_t *rowval, double *nzval);
+
+/* Device pointers to the last extraction (valid until the next one). */
+jfg_status jfg_ff_device_arrays(jfg_model *m, const int64_t **colptr, const int64_t **rowval, const double **nzval);
+
 /* ---- Serving: a device-resident request loop over model families --------
  * Replaces the reference's optimisation worker loop
  * (tools/jfem_worker_jsonl.jl:132-148, manifest_batch_core.jl:283-409), which

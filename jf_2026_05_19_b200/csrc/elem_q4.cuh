@@ -303,14 +303,20 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
     const bool valid = in_team && e < nq;
     Q4KShared &S = sh[slot_id];
     int32_t nd[4] = {0, 0, 0, 0};
+    // property loads are issued before the geometry so that their latency
+    // overlaps the node and coordinate loads
+    double h = 0.0, E = 0.0, nu = 0.0, br = 0.0, tst = 0.0, Gs = 0.0;
+    if (valid && tl == 9) {
+        const double *pr = prop + 7 * e;
+        h = o.thickness(e, pr); E = __ldg(pr + 1); nu = __ldg(pr + 2); br = __ldg(pr + 4); tst = __ldg(pr + 5);
+        Gs = __ldg(pr + 6);
+    }
     if (valid)
         for (int k = 0; k < 4; ++k) nd[k] = __ldg(nodes + 4 * e + k);
 
     q4_geometry(S.g, in_team ? tl : 99, valid, nd, coords, nodeR);
     if (valid && tl == 9) {
         // constitutive build for isotropic PSHELL/MAT1 (assembly.jl:2460-2469)
-        const double *pr = prop + 7 * e;
-        double h = o.thickness(e, pr), E = __ldg(pr + 1), nu = __ldg(pr + 2), br = __ldg(pr + 4), tst = __ldg(pr + 5), Gs = __ldg(pr + 6);
         double cm = E * h / (1 - nu * nu);
         double cb = br * (E * h * h * h) / (12 * (1 - nu * nu));
         double base[9] = {1.0, nu, 0.0, nu, 1.0, 0.0, 0.0, 0.0, (1 - nu) / 2};

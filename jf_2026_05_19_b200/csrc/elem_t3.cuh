@@ -76,7 +76,14 @@ __global__ void __launch_bounds__(T3_THREADS) t3_k_kernel(int64_t nt, const int3
     if (e >= nt) return;  // the whole team leaves; syncs below are team-local
     T3KShared &S = sh[warp * T3_TEAMS_PER_WARP + team];
 
-    // Phase 0: connectivity and coordinates.
+    // Phase 0: connectivity and coordinates; the property record is loaded
+    // now so that its latency overlaps the coordinate loads.
+    double h = 0.0, E = 0.0, nu = 0.0, br = 0.0, tst = 0.0, Gs = 0.0;
+    if (tl == 0) {
+        const double *pr = prop + 7 * e;
+        h = o.thickness(e, pr); E = __ldg(pr + 1); nu = __ldg(pr + 2); br = __ldg(pr + 4); tst = __ldg(pr + 5);
+        Gs = __ldg(pr + 6);
+    }
     if (tl < 3) {
         const int32_t n = __ldg(nodes + 3 * e + tl);
         S.nd[tl] = n;
@@ -107,8 +114,6 @@ __global__ void __launch_bounds__(T3_THREADS) t3_k_kernel(int64_t nt, const int3
         S.pts[4][0] = (x[1] + x[2]) / 2; S.pts[4][1] = (y[1] + y[2]) / 2;
         S.pts[5][0] = (x[2] + x[0]) / 2; S.pts[5][1] = (y[2] + y[0]) / 2;
         S.pts[6][0] = (x[0] + x[1] + x[2]) / 3; S.pts[6][1] = (y[0] + y[1] + y[2]) / 3;
-        const double *pr = prop + 7 * e;
-        double h = o.thickness(e, pr), E = __ldg(pr + 1), nu = __ldg(pr + 2), br = __ldg(pr + 4), tst = __ldg(pr + 5), Gs = __ldg(pr + 6);
         double cm = E * h / (1 - nu * nu);
         double cb = br * (E * h * h * h) / (12 * (1 - nu * nu));
         double base[9] = {1.0, nu, 0.0, nu, 1.0, 0.0, 0.0, 0.0, (1 - nu) / 2};

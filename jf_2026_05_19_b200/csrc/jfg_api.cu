@@ -93,6 +93,13 @@ struct jfg_model {
     // the block staging, raw RBE2 blocks, RBE2 chunk partials and diagonal staging
     int32_t b_cap = 0;
     double *d_bw = nullptr;
+    // free-dof extraction (jfg_ff_*): transposed-entry offsets, dof map, output CSC
+    int32_t *d_tpos = nullptr;           // per stored entry: offset of its transpose in the mirrored row
+    int64_t *d_fmap = nullptr;           // per dof: index among the free dofs, or -1
+    int64_t n_free = -1, ff_nnz = -1;
+    int64_t *d_ff_cnt = nullptr, *d_ff_colptr = nullptr, *d_ff_rowval = nullptr;
+    double *d_ff_val = nullptr;
+    unsigned long long *d_ff_max = nullptr;   // max |A_ff|, max |A_ff - A_ff'| (bit patterns)
     // constraint map (host, 0-based dofs)
     std::vector<int64_t> dep_dof, dep_ptr, dep_ind;
     std::vector<double> dep_coef;
@@ -1706,3 +1713,166 @@ extern "C" jfg_status jfg_assemble_k_quad4_noalloc(int64_t n_nodes, const double
     if (cudaStreamSynchronize(s) != cudaSuccess) return JFG_ERR_CUDA;
     return err ? JFG_ERR_UNSUPPORTED : JFG_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Free-dof submatrix, symmetrised: the K_ff / Kg_ff step of the SOL 105
+// consumer.  The reference slices A_ff = A[free, free] and forms
+// 0.5 * (A_ff + A_ff') (boundary_conditions.jl:113-114 for K,
+// solve_case.jl:1908-1927 for Kg, after recording max|Kg_ff| and
+// max|Kg_ff - Kg_ff'|).  Julia's sparse + keeps only entries whose sum is
+// nonzero, so exact zeros (e.g. the zeroed drill rows of Kg) leave the
+// pattern.  The stored pattern is structurally symmetric, so the transpose of
+// entry (r, c) sits in row c; its offset there is found once per pattern.
+// ---------------------------------------------------------------------------
+namespace {
+
+__global__ void tpos_kernel(int64_t ndof, const int64_t *__restrict__ rowptr, const int64_t *__restrict__ colind,
+                            int32_t *tpos, int32_t *err) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ndof) return;
+    for (int64_t p = rowptr[c]; p < rowptr[c + 1]; ++p) {
+        const int64_t r = colind[p];
+        const int64_t t = find_col(rowptr, colind, r, c);
+        if (t < 0) { atomicExch(err, 1); tpos[p] = 0; continue; }
+        tpos[p] = (int32_t)(t - rowptr[r]);
+    }
+}
+
+__global__ void ff_map_kernel(int64_t n_free, const int64_t *__restrict__ free1, int64_t *fmap) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n_free) fmap[free1[k] - 1] = k;
+}
+
+// Column c of the stored CSC (values nz[p] = A[colind[p], c]); pass 0 counts
+// the kept entries of output column fmap[c], pass 1 writes them (1-based).
+template <int PASS>
+__global__ void ff_kernel(int64_t ndof, const int64_t *__restrict__ rowptr, const int64_t *__restrict__ colind,
+                          const int32_t *__restrict__ tpos, const int64_t *__restrict__ fmap, const double *__restrict__ nz,
+                          int64_t *cnt_or_colptr, int64_t *rowval, double *val, unsigned long long *mx) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ndof) return;
+    const int64_t nc = fmap[c];
+    if (nc < 0) return;
+    int64_t q = PASS == 0 ? 0 : cnt_or_colptr[nc] - 1;
+    double lmax = 0.0, lasym = 0.0;
+    for (int64_t p = rowptr[c]; p < rowptr[c + 1]; ++p) {
+        const int64_t r = colind[p];
+        const int64_t nr = fmap[r];
+        if (nr < 0) continue;
+        const double a = nz[p], b = nz[rowptr[r] + tpos[p]];
+        const double sum = a + b;
+        if (PASS == 0) {
+            lmax = fmax(lmax, fabs(a));
+            lasym = fmax(lasym, fabs(a - b));
+            if (sum != 0.0) ++q;
+        } else if (sum != 0.0) {
+            rowval[q] = nr + 1;
+            val[q] = 0.5 * sum;
+            ++q;
+        }
+    }
+    if (PASS == 0) {
+        cnt_or_colptr[nc] = q;
+        if (lmax > 0.0) atomicMax(mx, (unsigned long long)__double_as_longlong(lmax));
+        if (lasym > 0.0) atomicMax(mx + 1, (unsigned long long)__double_as_longlong(lasym));
+    }
+}
+
+__global__ void add_one_kernel(int64_t n, int64_t *a) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) a[k] += 1;
+}
+
+}  // namespace
+
+extern "C" {
+
+jfg_status jfg_ff_set_free(jfg_model *m, const int64_t *free_dofs, int64_t n_free) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    if (n_free < 0 || n_free > m->ndof || (n_free && !free_dofs)) return fail(m, JFG_ERR_INVALID, "bad free-dof list");
+    for (int64_t k = 0; k < n_free; ++k)
+        if (free_dofs[k] < 1 || free_dofs[k] > m->ndof || (k && free_dofs[k] <= free_dofs[k - 1]))
+            return fail(m, JFG_ERR_INVALID, "free dofs must be 1-based, in range and strictly increasing");
+    if (!m->d_tpos) {
+        int32_t *d_err = nullptr;
+        CK(dalloc(m, &m->d_tpos, m->nnz));
+        CK(dalloc(m, &d_err, 1));
+        CK(cudaMemsetAsync(d_err, 0, sizeof(int32_t), m->stream));
+        tpos_kernel<<<(unsigned)cdiv(m->ndof, 128), 128, 0, m->stream>>>(m->ndof, m->d_rowptr, m->d_colind, m->d_tpos, d_err);
+        CK(cudaGetLastError());
+        int32_t herr = 0;
+        CK(cudaMemcpyAsync(&herr, d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, m->stream));
+        CK(cudaStreamSynchronize(m->stream));
+        if (herr) return fail(m, JFG_ERR_STATE, "stored pattern is not structurally symmetric");
+        CK(dalloc(m, &m->d_fmap, m->ndof));
+        CK(dalloc(m, &m->d_ff_cnt, m->ndof + 1));
+        CK(dalloc(m, &m->d_ff_colptr, m->ndof + 1));
+        CK(dalloc(m, &m->d_ff_rowval, m->nnz));
+        CK(dalloc(m, &m->d_ff_val, m->nnz));
+        CK(dalloc(m, &m->d_ff_max, 2));
+    }
+    CK(cudaMemsetAsync(m->d_fmap, 0xff, sizeof(int64_t) * m->ndof, m->stream));  // -1
+    if (n_free) {
+        int64_t *d_free = nullptr;
+        CK(cudaMallocAsync(&d_free, sizeof(int64_t) * n_free, m->stream));
+        CK(cudaMemcpyAsync(d_free, free_dofs, sizeof(int64_t) * n_free, cudaMemcpyHostToDevice, m->stream));
+        ff_map_kernel<<<(unsigned)cdiv(n_free, 256), 256, 0, m->stream>>>(n_free, d_free, m->d_fmap);
+        CK(cudaGetLastError());
+        CK(cudaFreeAsync(d_free, m->stream));
+    }
+    CK(cudaStreamSynchronize(m->stream));
+    m->n_free = n_free;
+    m->ff_nnz = -1;
+    return JFG_OK;
+}
+
+jfg_status jfg_ff_extract_device(jfg_model *m, const double *nz_dev, int64_t *nnz_ff, double *max_abs, double *max_asym) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    if (m->n_free < 0) return fail(m, JFG_ERR_STATE, "call jfg_ff_set_free first");
+    if (!nz_dev) return fail(m, JFG_ERR_INVALID, "null values");
+    const int64_t nf = m->n_free;
+    CK(cudaMemsetAsync(m->d_ff_cnt, 0, sizeof(int64_t) * (nf + 1), m->stream));
+    CK(cudaMemsetAsync(m->d_ff_max, 0, 2 * sizeof(unsigned long long), m->stream));
+    const unsigned grid = (unsigned)cdiv(m->ndof, 128);
+    ff_kernel<0><<<grid, 128, 0, m->stream>>>(m->ndof, m->d_rowptr, m->d_colind, m->d_tpos, m->d_fmap, nz_dev,
+                                             m->d_ff_cnt, nullptr, nullptr, m->d_ff_max);
+    CK(cudaGetLastError());
+    CK(exclusive_sum(m, m->d_ff_cnt, m->d_ff_colptr, nf + 1));  // counts -> 0-based column starts
+    add_one_kernel<<<(unsigned)cdiv(nf + 1, 256), 256, 0, m->stream>>>(nf + 1, m->d_ff_colptr);  // 1-based
+    CK(cudaGetLastError());
+    ff_kernel<1><<<grid, 128, 0, m->stream>>>(m->ndof, m->d_rowptr, m->d_colind, m->d_tpos, m->d_fmap, nz_dev,
+                                             m->d_ff_colptr, m->d_ff_rowval, m->d_ff_val, nullptr);
+    CK(cudaGetLastError());
+    int64_t last = 0;
+    unsigned long long mx[2] = {0, 0};
+    CK(cudaMemcpyAsync(&last, m->d_ff_colptr + nf, sizeof(int64_t), cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaMemcpyAsync(mx, m->d_ff_max, sizeof(mx), cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    m->ff_nnz = last - 1;
+    if (nnz_ff) *nnz_ff = m->ff_nnz;
+    double a, b;
+    std::memcpy(&a, &mx[0], sizeof(double));
+    std::memcpy(&b, &mx[1], sizeof(double));
+    if (max_abs) *max_abs = a;
+    if (max_asym) *max_asym = b;
+    return JFG_OK;
+}
+
+jfg_status jfg_ff_fetch(jfg_model *m, int64_t *colptr, int64_t *rowval, double *nzval) {
+    if (!m || m->ff_nnz < 0) return fail(m, JFG_ERR_STATE, "no extraction yet");
+    if (colptr) CK(cudaMemcpyAsync(colptr, m->d_ff_colptr, sizeof(int64_t) * (m->n_free + 1), cudaMemcpyDeviceToHost, m->stream));
+    if (rowval) CK(cudaMemcpyAsync(rowval, m->d_ff_rowval, sizeof(int64_t) * m->ff_nnz, cudaMemcpyDeviceToHost, m->stream));
+    if (nzval) CK(cudaMemcpyAsync(nzval, m->d_ff_val, sizeof(double) * m->ff_nnz, cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    return JFG_OK;
+}
+
+jfg_status jfg_ff_device_arrays(jfg_model *m, const int64_t **colptr, const int64_t **rowval, const double **nzval) {
+    if (!m || m->ff_nnz < 0) return fail(m, JFG_ERR_STATE, "no extraction yet");
+    if (colptr) *colptr = m->d_ff_colptr;
+    if (rowval) *rowval = m->d_ff_rowval;
+    if (nzval) *nzval = m->d_ff_val;
+    return JFG_OK;
+}
+
+}  // extern "C"

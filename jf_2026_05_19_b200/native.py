@@ -22,7 +22,8 @@ LIB_PATH = os.path.join(PKG, "libjfemgpu.so")
 EXPORTS = ("jfg_model_create", "jfg_pattern", "jfg_pattern_fill", "jfg_assemble_k", "jfg_assemble_kg",
            "jfg_assemble_k_device", "jfg_assemble_kg_device", "jfg_update_properties", "jfg_constraint_map",
            "jfg_set_stream", "jfg_last_timing", "jfg_kernel_timing", "jfg_timing_accumulated", "jfg_model_stats", "jfg_model_counts", "jfg_batch_workspace_bytes",
-           "jfg_batch_reserve", "jfg_assemble_batch_device", "jfg_server_create", "jfg_server_submit", "jfg_server_wait",
+           "jfg_batch_reserve", "jfg_assemble_batch_device", "jfg_ff_set_free", "jfg_ff_extract_device",
+           "jfg_ff_fetch", "jfg_ff_device_arrays", "jfg_server_create", "jfg_server_submit", "jfg_server_wait",
            "jfg_server_result", "jfg_server_release", "jfg_server_stats", "jfg_server_family_batch",
            "jfg_server_hold", "jfg_server_last_error", "jfg_server_destroy", "jfg_assemble_k_quad4_noalloc", "jfg_model_destroy", "jfg_last_error",
            "jfg_version")
@@ -80,6 +81,10 @@ def load(path: str = LIB_PATH):
     L.jfg_assemble_batch_device.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.jfg_model_counts.argtypes = [C.c_void_p, _pi64]
+    L.jfg_ff_set_free.argtypes = [C.c_void_p, _pi64, C.c_int64]
+    L.jfg_ff_extract_device.argtypes = [C.c_void_p, C.c_void_p, _pi64, _pd, _pd]
+    L.jfg_ff_fetch.argtypes = [C.c_void_p, _pi64, _pi64, _pd]
+    L.jfg_ff_device_arrays.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
     _pp = C.POINTER(C.c_void_p)
     L.jfg_server_create.argtypes = [_pp, _pp, C.c_int32, C.c_int64, C.c_int32, C.c_int32, _pp]
     L.jfg_server_submit.argtypes = [C.c_void_p, C.c_int32, _pd, C.c_int32, _pi64]
@@ -104,7 +109,8 @@ def load(path: str = LIB_PATH):
                  "jfg_assemble_k_quad4_noalloc", "jfg_model_counts", "jfg_batch_workspace_bytes", "jfg_batch_reserve",
                  "jfg_assemble_batch_device", "jfg_server_create", "jfg_server_submit", "jfg_server_wait",
                  "jfg_server_result", "jfg_server_release", "jfg_server_stats", "jfg_server_family_batch",
-                 "jfg_server_hold"):
+                 "jfg_server_hold", "jfg_ff_set_free", "jfg_ff_extract_device", "jfg_ff_fetch",
+                 "jfg_ff_device_arrays"):
         getattr(L, name).restype = C.c_int32
     _lib = L
     return L
@@ -214,6 +220,23 @@ class GpuModel:
         v = lambda p: C.c_void_p(p or None)
         self._check(self.L.jfg_assemble_batch_device(self.h, int(n_var), v(h_ptr), v(bar_prop_ptr), v(u_ptr), us,
                                                      v(nzk_ptr), v(max_ptr), v(diag_ptr), v(nzkg_ptr)))
+
+    # -- free-dof submatrices (K_ff / Kg_ff) ----------------------------------
+    def ff_set_free(self, free0: np.ndarray):
+        """Free dofs as 0-based indices (sorted); stored 1-based by the library."""
+        f = np.ascontiguousarray(np.asarray(free0, np.int64) + 1)
+        self._check(self.L.jfg_ff_set_free(self.h, _ptr(f, _pi64), int(f.shape[0])))
+        self._n_free = int(f.shape[0])
+
+    def ff_extract(self, nz_ptr: int):
+        """0.5 (A_ff + A_ff') of device values; returns (colptr, rowval, nzval, max|A_ff|, max|A_ff - A_ff'|)."""
+        nnz = C.c_int64(); a = C.c_double(); b = C.c_double()
+        self._check(self.L.jfg_ff_extract_device(self.h, C.c_void_p(nz_ptr), C.byref(nnz), C.byref(a), C.byref(b)))
+        colptr = np.empty(self._n_free + 1, np.int64)
+        rowval = np.empty(nnz.value, np.int64)
+        val = np.empty(nnz.value)
+        self._check(self.L.jfg_ff_fetch(self.h, _ptr(colptr, _pi64), _ptr(rowval, _pi64), _ptr(val, _pd)))
+        return colptr, rowval, val, a.value, b.value
 
     def set_stream(self, stream_ptr: int):
         self._check(self.L.jfg_set_stream(self.h, C.c_void_p(stream_ptr or None)))
