@@ -63,7 +63,7 @@ struct T3KShared {
     double Pb[3][10][9];  // quad q, local node pair (a <= b): 3x3 over (w, theta_x, theta_y)
 };
 
-__global__ void __launch_bounds__(T3_THREADS) t3_k_kernel(int64_t nt, const int32_t *__restrict__ nodes,
+__global__ void __launch_bounds__(T3_THREADS, 5) t3_k_kernel(int64_t nt, const int32_t *__restrict__ nodes,
                                                          const double *__restrict__ prop,
                                                          const double *__restrict__ coords,
                                                          const double *__restrict__ nodeR, double k6rot, ElemOut o) {
