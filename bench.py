@@ -245,6 +245,16 @@ def load_traffic():
     return {}
 
 
+def max_over_ranks(seconds: float, dist, device) -> float:
+    """The slowest rank's time (every rank gets it); the value itself without a process group."""
+    if dist is None:
+        return seconds
+    import torch
+    t = torch.tensor([seconds], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -645,10 +655,7 @@ def main():
         dist.barrier()
     clk = clocks.stop()
     elapsed = start.elapsed_time(end) / 1e3
-    if dist:
-        t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    elapsed = max_over_ranks(elapsed, dist, dev)
     kt, kn = g.timing_accumulated("k", reset=True)
     gt, gn = g.timing_accumulated("kg", reset=True)
 
@@ -671,10 +678,7 @@ def main():
     e2.record(stream)
     e2.synchronize()
     e2e_el = s2.elapsed_time(e2) / 1e3
-    if dist:
-        t = torch.tensor([e2e_el], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_el = float(t.item())
+    e2e_el = max_over_ranks(e2e_el, dist, dev)
 
     n_el = m.n_elements
     value = world * n_el * args.steps / elapsed
