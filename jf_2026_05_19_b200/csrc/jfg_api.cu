@@ -436,20 +436,9 @@ __global__ void key_pos_kernel(int64_t n, const uint64_t *__restrict__ keys, int
 // every element block in global block k's segment, in slot order, and writes
 // it to row 6A+i (columns of B) and, for A != B, into column i of the
 // mirrored rows 6B+j.  Staging rows are 48-byte aligned, so they are read as
-// three double2 loads, two contributions per loop trip.
-__global__ void __launch_bounds__(256) block_reduce_kernel(int64_t n_blk, const int32_t *__restrict__ seg,
-                                                           const double *__restrict__ staging, const int32_t *__restrict__ A,
-                                                           const int32_t *__restrict__ B, const int32_t *__restrict__ offAB,
-                                                           const int32_t *__restrict__ offBA, const int64_t *__restrict__ rowptr,
-                                                           double *nz, int64_t staging_stride, int64_t nnz) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n_blk * 6) return;
-    staging += (int64_t)blockIdx.y * staging_stride;  // batched variant
-    nz += (int64_t)blockIdx.y * nnz;
-    const int64_t k = t / 6;
-    const int i = (int)(t - 6 * k);
-    const int32_t a = __ldg(seg + k), b = __ldg(seg + k + 1);
-    double s[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+// three double2 loads.  Each thread takes two blocks, k and k + half, whose
+// loads are issued together to keep more of them in flight.
+__device__ __forceinline__ void block_row_sum(const double *__restrict__ staging, int32_t a, int32_t b, int i, double s[6]) {
     int32_t q = a;
     for (; q + 1 < b; q += 2) {
         const double2 *p0 = reinterpret_cast<const double2 *>(staging + 36 * (int64_t)q + 6 * i);
@@ -464,6 +453,12 @@ __global__ void __launch_bounds__(256) block_reduce_kernel(int64_t n_blk, const 
         const double2 x0 = __ldg(p0), x1 = __ldg(p0 + 1), x2 = __ldg(p0 + 2);
         s[0] += x0.x; s[1] += x0.y; s[2] += x1.x; s[3] += x1.y; s[4] += x2.x; s[5] += x2.y;
     }
+}
+
+__device__ __forceinline__ void block_row_write(int64_t k, int i, const double s[6], const int32_t *__restrict__ A,
+                                                const int32_t *__restrict__ B, const int32_t *__restrict__ offAB,
+                                                const int32_t *__restrict__ offBA, const int64_t *__restrict__ rowptr,
+                                                double *nz) {
     const int64_t nA = __ldg(A + k), nB = __ldg(B + k);
     double *row = nz + __ldg(rowptr + 6 * nA + i) + __ldg(offAB + k);
 #pragma unroll
@@ -473,6 +468,28 @@ __global__ void __launch_bounds__(256) block_reduce_kernel(int64_t n_blk, const 
 #pragma unroll
         for (int j = 0; j < 6; ++j) nz[__ldg(rowptr + 6 * nB + j) + cb] = s[j];
     }
+}
+
+__global__ void __launch_bounds__(256) block_reduce_kernel(int64_t n_blk, const int32_t *__restrict__ seg,
+                                                           const double *__restrict__ staging, const int32_t *__restrict__ A,
+                                                           const int32_t *__restrict__ B, const int32_t *__restrict__ offAB,
+                                                           const int32_t *__restrict__ offBA, const int64_t *__restrict__ rowptr,
+                                                           double *nz, int64_t staging_stride, int64_t nnz) {
+    const int64_t half = (n_blk + 1) / 2;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= half * 6) return;
+    staging += (int64_t)blockIdx.y * staging_stride;  // batched variant
+    nz += (int64_t)blockIdx.y * nnz;
+    const int64_t k0 = t / 6, k1 = k0 + half;
+    const int i = (int)(t - 6 * k0);
+    const bool two = k1 < n_blk;
+    const int32_t a0 = __ldg(seg + k0), b0 = __ldg(seg + k0 + 1);
+    const int32_t a1 = two ? __ldg(seg + k1) : 0, b1 = two ? __ldg(seg + k1 + 1) : 0;
+    double s0[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, s1[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    block_row_sum(staging, a0, b0, i, s0);
+    block_row_sum(staging, a1, b1, i, s1);
+    block_row_write(k0, i, s0, A, B, offAB, offBA, rowptr, nz);
+    if (two) block_row_write(k1, i, s1, A, B, offAB, offBA, rowptr, nz);
 }
 
 // Dof-level path: each CSC position touched by an RBE2-expanded entry sums
@@ -1259,7 +1276,7 @@ jfg_status launch_reduce(jfg_model *m, const Batch &bt) {
     CK(cudaGetLastError());
     CK(mark(m, 4));
     if (m->n_blk)
-        block_reduce_kernel<<<dim3((unsigned)cdiv(m->n_blk * 6, 256), nv), 256, 0, m->stream>>>(
+        block_reduce_kernel<<<dim3((unsigned)cdiv((m->n_blk + 1) / 2 * 6, 256), nv), 256, 0, m->stream>>>(
             m->n_blk, m->d_blk_seg, bt.staging, m->d_blk_A, m->d_blk_B, m->d_blk_offAB, m->d_blk_offBA, m->d_rowptr, bt.nz,
             bt.staging_stride, m->nnz);
     CK(cudaGetLastError());
