@@ -180,10 +180,13 @@ class GpuModel:
         return self._pattern
 
     # -- host-buffer assembly (the reference-facing calls) -----------------
-    def assemble_k(self, nzval: Optional[np.ndarray] = None, want_diag: bool = True):
+    def assemble_k(self, nzval: Optional[np.ndarray] = None, want_diag: bool = True,
+                   diag_out: Optional[np.ndarray] = None):
+        """K values (and max_elem_stiff, orig_diag) into host arrays; pass pinned
+        arrays as nzval / diag_out to avoid pageable copies."""
         nz = np.empty(self.nnz) if nzval is None else nzval
         mx = np.zeros(1)
-        diag = np.empty(self.ndof) if want_diag else None
+        diag = (np.empty(self.ndof) if diag_out is None else diag_out) if want_diag else None
         self._check(self.L.jfg_assemble_k(self.h, _ptr(nz, _pd), _ptr(mx, _pd), _ptr(diag, _pd)))
         return nz, float(mx[0]), diag
 
