@@ -102,21 +102,29 @@ struct Q4Geo {
     double dphi[4][4];            // d1x, d1y, d2x, d2y per Gauss point
 };
 
+// Per-point data of one CQUAD4 shared by its team.
+struct Q4Pts {
+    double dNx[5][4], dNy[5][4];  // 4 Gauss points + centre (index 4)
+    double wdet[4];
+    double dphi[4][4];            // d1x, d1y, d2x, d2y per Gauss point
+};
+
+// K kernel state of one element.  The isotropic constitutive matrices are
+// scalar multiples of one plane-stress matrix P(nu): Cm = cm P, Cb = cb P.
+// The incompatible-mode blocks therefore factor as K_ab = cm Am, K_bb = cm B
+// (membrane) and K_abb = cb Ab S, K_bbb = cb S' B S (bending), where Am, Ab
+// and B hold geometry and P only and S is the signed permutation taking the
+// bending modes (-m1, -m3, m0, m2) to the membrane modes m0..m3.  Both
+// condensations K_ab K_bb^-1 K_ab' are then c A B^-1 A' with the one 4x4
+// symmetric positive definite B.
 struct Q4KShared {
-    Q4Geo g;
-    double Cm[9], Cb[9], Cs[4];
-    double h, alpha_d;
-    int skip_macneal, bend_cond;
-    double Kabm[8][4], Kbbm[16], Kabb[8][4], Kbbb[16];
-    double D[4][12], Jp[4];
-    MacNealZ mz;
-    union {
-        double P[2][4][4][3];  // phase 1: C b_l(g) for membrane (0) / bending (1) incompatible modes
-        struct {
-            double Xm[4][8], Xb[4][8];
-            double Y[4][12];
-        } x;                   // phases 3-4
-    } u;
+    Q4Pts g;
+    double Dd[4][4];            // MacNeal sampling rows: dN_k/dx (rows 0, 1), dN_k/dy (rows 2, 3)
+    double ivd[4];              // 1 / (sqrt(2 Jp)^2 cs) per sampling point
+    double W[6];                // Zx^-1 (w00, w01, w11), Zy^-1 (w22, w23, w33)
+    double Am[8][4], Ab[8][4];  // rows: (node, component) of the membrane / bending B
+    double B[10];               // packed upper triangle
+    double Xm[4][8], Xb[4][8];  // B^-1 Am', B^-1 Ab'
 };
 
 struct Q4GShared {
@@ -289,6 +297,117 @@ __device__ __forceinline__ void write_sub_block(const ElemOut &o, int64_t e, int
     }
 }
 
+// Element frame (q4_frame) and corner coordinates about the centroid
+// (assembly.jl:2693-2698), in registers.
+__device__ __forceinline__ void q4_local(const double p[4][3], double V[9], double lc[4][2]) {
+    double v1[3], v2[3], v3[3];
+    q4_frame(p[0], p[1], p[2], p[3], v1, v2, v3);
+    double c[3];
+    for (int i = 0; i < 3; ++i) c[i] = (p[0][i] + p[1][i] + p[2][i] + p[3][i]) / 4.0;
+    for (int k = 0; k < 4; ++k) {
+        double d[3];
+        sub3(p[k], c, d);
+        lc[k][0] = dot3(d, v1);
+        lc[k][1] = dot3(d, v2);
+    }
+    for (int i = 0; i < 3; ++i) { V[i] = v1[i]; V[3 + i] = v2[i]; V[6 + i] = v3[i]; }
+}
+
+// Natural coordinates of point pt: 0-3 the 2x2 Gauss points, 4 the centre,
+// 5-8 MacNeal's strain-sampling points (0, -p), (0, p), (-p, 0), (p, 0).
+__device__ __forceinline__ void q4_point_rs(int pt, double &r, double &s) {
+    const double p = 0.57735026918962576451;  // 1/sqrt(3)
+    r = pt < 4 ? ((pt == 0 || pt == 3) ? -p : p) : (pt == 7 ? -p : (pt == 8 ? p : 0.0));
+    s = pt < 4 ? (pt <= 1 ? -p : p) : (pt == 5 ? -p : (pt == 6 ? p : 0.0));
+}
+
+// Shape-function derivatives at (r, s): returns det J (clamped away from 0
+// to +-1e-14 when `clamp`, as the MacNeal sampling does) and writes
+// dN/dx, dN/dy and the inverse Jacobian (iJ11, iJ12, iJ21, iJ22).
+__device__ __forceinline__ double q4_point_derivs(const double lc[4][2], double r, double s, bool clamp,
+                                                  double dx[4], double dy[4], double iJ[4]) {
+    const double dNr[4] = {-0.25 * (1 - s), 0.25 * (1 - s), 0.25 * (1 + s), -0.25 * (1 + s)};
+    const double dNs[4] = {-0.25 * (1 - r), -0.25 * (1 + r), 0.25 * (1 + r), 0.25 * (1 - r)};
+    double J11 = 0, J12 = 0, J21 = 0, J22 = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        J11 += dNr[k] * lc[k][0]; J12 += dNr[k] * lc[k][1];
+        J21 += dNs[k] * lc[k][0]; J22 += dNs[k] * lc[k][1];
+    }
+    double det = J11 * J22 - J12 * J21;
+    if (clamp && fabs(det) < 1e-14) det = det < 0.0 ? -1e-14 : 1e-14;
+    const double inv = 1.0 / det;
+    iJ[0] = J22 * inv; iJ[1] = -J12 * inv; iJ[2] = -J21 * inv; iJ[3] = J11 * inv;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        dx[k] = iJ[0] * dNr[k] + iJ[1] * dNs[k];
+        dy[k] = iJ[2] * dNr[k] + iJ[3] * dNs[k];
+    }
+    return det;
+}
+
+// Node pair (a <= b) of team lane tl: (0,0) (0,1) (0,2) (0,3) (1,1) (1,2)
+// (1,3) (2,2) (2,3) (3,3).
+__device__ __forceinline__ void q4_pair(int tl, int &a, int &b) {
+    a = (tl >= 4) + (tl >= 7) + (tl >= 9);
+    b = a + tl - (a == 0 ? 0 : (a == 1 ? 4 : (a == 2 ? 7 : 9)));
+}
+
+// Out = Qa' M Qb for a 3x3 block M whose structural zeros are the clear bits
+// of NZ (bit 3 r + c set when M[r][c] may be nonzero).
+template <int NZ>
+__device__ __forceinline__ void rot_sparse(const double *Qa, const double M[3][3], const double *Qb, double out[3][3]) {
+    double W[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            double w = 0.0;
+            bool any = false;
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                if ((NZ >> (3 * r + c)) & 1) { w = any ? w + M[r][c] * Qb[3 * c + j] : M[r][c] * Qb[3 * c + j]; any = true; }
+            W[r][j] = w;
+        }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            double o = 0.0;
+            bool any = false;
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+                if ((NZ >> (3 * r)) & 7) { o = any ? o + Qa[3 * r + i] * W[r][j] : Qa[3 * r + i] * W[r][j]; any = true; }
+            out[i][j] = o;
+        }
+}
+
+// Solve B x = rhs with the LDL' factors of the packed SPD 4x4 B.
+struct Ldl4 {
+    double l10, l20, l30, l21, l31, l32, r0, r1, r2, r3;
+    __device__ __forceinline__ explicit Ldl4(const double *B) {
+        const double b00 = B[0], b01 = B[1], b02 = B[2], b03 = B[3], b11 = B[4], b12 = B[5], b13 = B[6];
+        const double b22 = B[7], b23 = B[8], b33 = B[9];
+        r0 = 1.0 / b00;
+        l10 = b01 * r0; l20 = b02 * r0; l30 = b03 * r0;
+        r1 = 1.0 / (b11 - l10 * b01);
+        const double u12 = b12 - l10 * b02, u13 = b13 - l10 * b03;
+        l21 = u12 * r1; l31 = u13 * r1;
+        r2 = 1.0 / (b22 - l20 * b02 - l21 * u12);
+        const double u23 = b23 - l20 * b03 - l21 * u13;
+        l32 = u23 * r2;
+        r3 = 1.0 / (b33 - l30 * b03 - l31 * u13 - l32 * u23);
+    }
+    __device__ __forceinline__ void solve(const double rhs[4], double x[4]) const {
+        const double y0 = rhs[0], y1 = rhs[1] - l10 * y0, y2 = rhs[2] - l20 * y0 - l21 * y1;
+        const double y3 = rhs[3] - l30 * y0 - l31 * y1 - l32 * y2;
+        x[3] = y3 * r3;
+        x[2] = y2 * r2 - l32 * x[3];
+        x[1] = y1 * r1 - l21 * x[2] - l31 * x[3];
+        x[0] = y0 * r0 - l10 * x[1] - l20 * x[2] - l30 * x[3];
+    }
+};
+
 __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const int32_t *__restrict__ nodes,
                                                          const double *__restrict__ prop,
                                                          const double *__restrict__ coords,
@@ -302,232 +421,261 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
     const int64_t e = (int64_t)blockIdx.x * Q4_ELEMS_PER_BLOCK + slot_id;
     const bool valid = in_team && e < nq;
     Q4KShared &S = sh[slot_id];
-    int32_t nd[4] = {0, 0, 0, 0};
-    // property loads are issued before the geometry so that their latency
-    // overlaps the node and coordinate loads
-    double h = 0.0, E = 0.0, nu = 0.0, br = 0.0, tst = 0.0, Gs = 0.0;
-    if (valid && tl == 9) {
+
+    // Phase 0, every lane of the team in registers: nodes, corners,
+    // property record, frame, local coordinates and the constitutive scalars
+    // of isotropic PSHELL/MAT1 (assembly.jl:2460-2469).
+    int nd[4] = {0, 0, 0, 0};
+    double V[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    double lc[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
+    double h = 1.0, E = 0.0, nu = 0.0, br = 0.0, tst = 0.0, Gs = 0.0;
+    if (valid) {
         const double *pr = prop + 7 * e;
         h = o.thickness(e, pr); E = __ldg(pr + 1); nu = __ldg(pr + 2); br = __ldg(pr + 4); tst = __ldg(pr + 5);
         Gs = __ldg(pr + 6);
-    }
-    if (valid)
+#pragma unroll
         for (int k = 0; k < 4; ++k) nd[k] = __ldg(nodes + 4 * e + k);
+        double p[4][3];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) p[k][i] = __ldg(coords + 3 * (int64_t)nd[k] + i);
+        q4_local(p, V, lc);
+    }
+    const double gam = (1 - nu) / 2;
+    const double cm = E * h / (1 - nu * nu);
+    const double cb = br * (E * h * h * h) / (12 * (1 - nu * nu));
+    const bool membrane_only = br <= 1e-12;
+    const double cs = membrane_only ? 0.0 : tst * h * Gs;
+    double G_drill = (cm * gam) / h;
+    if (G_drill < 1e-6) G_drill = E / (2 * 3.0);
+    const double ad = membrane_only ? 0.0 : (k6rot / 1e5) * G_drill * h;
+    const bool skip_mac = h < 1e-30 || fabs(cs) < 1e-30;
 
-    q4_geometry(S.g, in_team ? tl : 99, valid, nd, coords, nodeR);
-    if (valid && tl == 9) {
-        // constitutive build for isotropic PSHELL/MAT1 (assembly.jl:2460-2469)
-        double cm = E * h / (1 - nu * nu);
-        double cb = br * (E * h * h * h) / (12 * (1 - nu * nu));
-        double base[9] = {1.0, nu, 0.0, nu, 1.0, 0.0, 0.0, 0.0, (1 - nu) / 2};
-        for (int i = 0; i < 9; ++i) { S.Cm[i] = cm * base[i]; S.Cb[i] = cb * base[i]; }
-        bool membrane_only = br <= 1e-12;
-        double cs = membrane_only ? 0.0 : tst * h * Gs;
-        S.Cs[0] = cs; S.Cs[1] = 0.0; S.Cs[2] = 0.0; S.Cs[3] = cs;
-        S.h = h;
-        double G_drill = S.Cm[8] / h;
-        if (G_drill < 1e-6) G_drill = E / (2 * 3.0);
-        double k6 = membrane_only ? 0.0 : k6rot, ds = membrane_only ? 0.0 : 1.0;
-        S.alpha_d = ds * (k6 / 1e5) * G_drill * h;
-        S.skip_macneal = (h < 1e-30 || fabs(cs) < 1e-30) ? 1 : 0;
-    }
-    __syncwarp();
-
-    // Phase 1: MacNeal strain-sampling rows, incompatible-mode couplings.
-    if (valid && tl < 4) {
-        const double pt = 0.57735026918962576451;
-        const double xs[4] = {0.0, 0.0, -pt, pt}, es[4] = {-pt, pt, 0.0, 0.0};
-        double xi = xs[tl], eta = es[tl];
-        double dNr[4] = {-0.25 * (1 - eta), 0.25 * (1 - eta), 0.25 * (1 + eta), -0.25 * (1 + eta)};
-        double dNs[4] = {-0.25 * (1 - xi), -0.25 * (1 + xi), 0.25 * (1 + xi), 0.25 * (1 - xi)};
-        double J11 = 0, J12 = 0, J21 = 0, J22 = 0;
-        for (int k = 0; k < 4; ++k) {
-            J11 += dNr[k] * S.g.lc[k][0]; J12 += dNr[k] * S.g.lc[k][1];
-            J21 += dNs[k] * S.g.lc[k][0]; J22 += dNs[k] * S.g.lc[k][1];
-        }
-        double det = J11 * J22 - J12 * J21;
-        if (fabs(det) < 1e-14) det = det < 0.0 ? -1e-14 : 1e-14;
-        S.Jp[tl] = fabs(det);
-        double inv = 1.0 / det;
-        double iJ11 = J22 * inv, iJ12 = -J12 * inv, iJ21 = -J21 * inv, iJ22 = J11 * inv;
-        for (int k = 0; k < 4; ++k) {
-            double dx = iJ11 * dNr[k] + iJ12 * dNs[k];
-            double dy = iJ21 * dNr[k] + iJ22 * dNs[k];
-            double Nk = 0.25 * (1 + ((k == 1 || k == 2) ? xi : -xi)) * (1 + (k >= 2 ? eta : -eta));
-            if (tl < 2) { S.D[tl][3 * k] = dx; S.D[tl][3 * k + 1] = 0.0; S.D[tl][3 * k + 2] = Nk; }
-            else { S.D[tl][3 * k] = dy; S.D[tl][3 * k + 1] = -Nk; S.D[tl][3 * k + 2] = 0.0; }
-        }
-    }
-    // C b_l(g) of every incompatible-mode column (membrane, bending).
-    if (valid) {
-        for (int w = tl; w < 32; w += Q4_TEAM) {
-            const int kind = w >> 4, g = (w >> 2) & 3, l = w & 3;
-            double b[3];
-            if (kind == 0) q4_bi_col(S.g, g, l, b);
-            else q4_bib_col(S.g, g, l, b);
-            const double *C = kind == 0 ? S.Cm : S.Cb;
+    // Phase 1: point derivatives (lanes 0-8), MacNeal element scalars (lane 9).
+    double zs[4] = {0.0, 0.0, 0.0, 0.0};  // zxu + zxd, zxu - zxd, zyu + zyd, zyu - zyd
+    if (valid && tl < 9) {
+        double r, s, dx[4], dy[4], iJ[4];
+        q4_point_rs(tl, r, s);
+        const bool mac = tl >= 5;
+        const double det = q4_point_derivs(lc, r, s, mac, dx, dy, iJ);
+        if (!mac) {
 #pragma unroll
-            for (int r = 0; r < 3; ++r) S.u.P[kind][g][l][r] = C[3 * r] * b[0] + C[3 * r + 1] * b[1] + C[3 * r + 2] * b[2];
-        }
-    }
-    __syncwarp();
-    // K_ab / K_bb rows (membrane then bending): 8 + 4 + 8 + 4 row items,
-    // four independent accumulators each.
-    if (valid) {
-        for (int w = tl; w < 24; w += Q4_TEAM) {
-            const int kind = w >= 12 ? 1 : 0, r = w - 12 * kind;
-            double acc[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-            for (int g = 0; g < 4; ++g) {
-                double a[3];
-                if (r < 8) {
-                    if (kind == 0) q4_mem_col(S.g, g, r >> 1, r & 1, a);
-                    else q4_bend_col(S.g, g, r >> 1, r & 1, a);
-                } else {
-                    if (kind == 0) q4_bi_col(S.g, g, r - 8, a);
-                    else q4_bib_col(S.g, g, r - 8, a);
-                }
-                const double wd = S.g.wdet[g];
-#pragma unroll
-                for (int l = 0; l < 4; ++l) {
-                    const double *P = S.u.P[kind][g][l];
-                    acc[l] += wd * (a[0] * P[0] + a[1] * P[1] + a[2] * P[2]);
-                }
+            for (int k = 0; k < 4; ++k) { S.g.dNx[tl][k] = dx[k]; S.g.dNy[tl][k] = dy[k]; }
+            if (tl < 4) {
+                const double a = fabs(det);
+                S.g.wdet[tl] = a < 1e-12 ? 1e-12 : a;
+                S.g.dphi[tl][0] = iJ[0] * (-2.0 * r);
+                S.g.dphi[tl][1] = iJ[2] * (-2.0 * r);
+                S.g.dphi[tl][2] = iJ[1] * (-2.0 * s);
+                S.g.dphi[tl][3] = iJ[3] * (-2.0 * s);
             }
+        } else {
+            const int l = tl - 5;
 #pragma unroll
-            for (int l = 0; l < 4; ++l) {
-                if (r < 8) (kind == 0 ? S.Kabm : S.Kabb)[r][l] = acc[l];
-                else (kind == 0 ? S.Kbbm : S.Kbbb)[4 * (r - 8) + l] = acc[l];
-            }
+            for (int k = 0; k < 4; ++k) S.Dd[l][k] = l < 2 ? dx[k] : dy[k];
+            const double sq = sqrt(2.0 * fabs(det));
+            const double v = sq * sq * cs;
+            S.ivd[l] = 1.0 / (v < 1e-30 ? 1e-30 : v);
         }
+    } else if (valid && tl == 9) {
+        // residual bending flexibility (add_quad4_macneal_shear_rbf!,
+        // FEMKernels.jl:4803-4869: eps 0.04, zb 0.65, flex 1/Cb11, 1/Cb22)
+        const double Dx = 0.5 * (lc[1][0] + lc[2][0] - lc[0][0] - lc[3][0]);
+        const double Dy = 0.5 * (lc[2][1] + lc[3][1] - lc[0][1] - lc[1][1]);
+        const double Dx2 = Dx * Dx, Dy2 = Dy * Dy;
+        const double J11c = 0.25 * (-lc[0][0] + lc[1][0] + lc[2][0] - lc[3][0]);
+        const double J12c = 0.25 * (-lc[0][1] + lc[1][1] + lc[2][1] - lc[3][1]);
+        const double J21c = 0.25 * (-lc[0][0] - lc[1][0] + lc[2][0] + lc[3][0]);
+        const double J22c = 0.25 * (-lc[0][1] - lc[1][1] + lc[2][1] + lc[3][1]);
+        const double A_elem = 4.0 * fabs(J11c * J22c - J12c * J21c);
+        const double eps = 0.04;
+        const double ap = eps / (eps + (1.0 - eps) * Dx2 / fmax(Dy2, 1e-30));
+        const double bp = eps / (eps + (1.0 - eps) * Dy2 / fmax(Dx2, 1e-30));
+        const double flex = 1.0 / fmax(fabs(cb), 1e-30);
+        const double c12 = 0.65 * (1.0 / (12.0 * A_elem));
+        const double zxu = c12 * Dx2 * flex, zxd = c12 * ap * Dx2 * flex;
+        const double zyu = c12 * Dy2 * flex, zyd = c12 * bp * Dy2 * flex;
+        zs[0] = zxu + zxd; zs[1] = zxu - zxd; zs[2] = zyu + zyd; zs[3] = zyu - zyd;
     }
     __syncwarp();
 
-    // Phase 2: the two 4x4 inverses (lanes 0 and 1 in one code path) and the
-    // MacNeal compliance factors (lane 2).
-    if (valid && tl < 2) {
-        double *M = tl == 0 ? S.Kbbm : S.Kbbb;
-        bool inv = true;
-        if (tl == 1) {
-            double mx = 0.0;
-            for (int i = 0; i < 16; ++i) mx = fmax(mx, fabs(M[i]));
-            S.bend_cond = mx > 0.0 ? 1 : 0;
-            inv = mx > 0.0;
-        }
-        if (inv) inv4_inplace(M);
-    } else if (valid && tl == 2 && !S.skip_macneal) {
-        S.mz = macneal_z(S.g.lc, S.Jp, S.Cs[0], S.Cb[0], S.Cb[4]);
-    }
-    __syncwarp();
-
-    // Phase 3: X = Kbb^-1 Kab' for both condensations, Y = Z \ D by columns.
-    if (valid) {
-        for (int w = tl; w < 76; w += Q4_TEAM) {
-            if (w < 32) {
-                int l = w >> 3, r = w & 7;
-                double s = 0.0;
-                for (int q = 0; q < 4; ++q) s += S.Kbbm[4 * l + q] * S.Kabm[r][q];
-                S.u.x.Xm[l][r] = s;
-            } else if (w < 64) {
-                int l = (w - 32) >> 3, r = (w - 32) & 7;
-                double s = 0.0;
-                if (S.bend_cond)
-                    for (int q = 0; q < 4; ++q) s += S.Kbbb[4 * l + q] * S.Kabb[r][q];
-                S.u.x.Xb[l][r] = s;
-            } else if (!S.skip_macneal) {
-                int j = w - 64;
-                double d[4] = {S.D[0][j], S.D[1][j], S.D[2][j], S.D[3][j]}, y[4];
-                macneal_y(S.mz, d, y);
-                for (int l = 0; l < 4; ++l) S.u.x.Y[l][j] = y[l];
+    // Phase 2: rows of Am and Ab (lanes 0-7), B (lane 8), Z^-1 (lane 9).
+    double am[4] = {0.0, 0.0, 0.0, 0.0}, ab[4] = {0.0, 0.0, 0.0, 0.0};
+    if (valid && tl < 8) {
+        const int k = tl >> 1;
+        const bool c1 = tl & 1;
+        const double xc = S.g.dNx[4][k], yc = S.g.dNy[4][k];
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+            const double wd = S.g.wdet[g], x = S.g.dNx[g][k], y = S.g.dNy[g][k];
+            const double d1x = S.g.dphi[g][0], d1y = S.g.dphi[g][1], d2x = S.g.dphi[g][2], d2y = S.g.dphi[g][3];
+            // membrane column (x, 0, y) / (0, y, x); bending column with the
+            // MacNeal twist row (0, -y, 2(-x) + xc) / (x, 0, 2y - yc)
+            const double m0 = wd * (c1 ? 0.0 : x), m1 = wd * (c1 ? y : 0.0), m2 = wd * (c1 ? x : y);
+            const double t = c1 ? 2.0 * y - yc : 2.0 * (-x) - (-xc);
+            const double b0 = wd * (c1 ? x : 0.0), b1 = wd * (c1 ? 0.0 : -y), b2 = wd * t;
+            const double P[4][3] = {{d1x, nu * d1x, gam * d1y}, {nu * d1y, d1y, gam * d1x},
+                                    {d2x, nu * d2x, gam * d2y}, {nu * d2y, d2y, gam * d2x}};
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                am[m] += m0 * P[m][0] + m1 * P[m][1] + m2 * P[m][2];
+                ab[m] += b0 * P[m][0] + b1 * P[m][1] + b2 * P[m][2];
             }
         }
+#pragma unroll
+        for (int m = 0; m < 4; ++m) { S.Am[tl][m] = am[m]; S.Ab[tl][m] = ab[m]; }
+    } else if (valid && tl == 8) {
+        double Bs[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+            const double wd = S.g.wdet[g];
+            const double d1x = S.g.dphi[g][0], d1y = S.g.dphi[g][1], d2x = S.g.dphi[g][2], d2y = S.g.dphi[g][3];
+            const double P[4][3] = {{d1x, nu * d1x, gam * d1y}, {nu * d1y, d1y, gam * d1x},
+                                    {d2x, nu * d2x, gam * d2y}, {nu * d2y, d2y, gam * d2x}};
+            // modes m0 = (d1x, 0, d1y), m1 = (0, d1y, d1x), m2 = (d2x, 0, d2y), m3 = (0, d2y, d2x)
+            Bs[0] += wd * (d1x * P[0][0] + d1y * P[0][2]);
+            Bs[1] += wd * (d1x * P[1][0] + d1y * P[1][2]);
+            Bs[2] += wd * (d1x * P[2][0] + d1y * P[2][2]);
+            Bs[3] += wd * (d1x * P[3][0] + d1y * P[3][2]);
+            Bs[4] += wd * (d1y * P[1][1] + d1x * P[1][2]);
+            Bs[5] += wd * (d1y * P[2][1] + d1x * P[2][2]);
+            Bs[6] += wd * (d1y * P[3][1] + d1x * P[3][2]);
+            Bs[7] += wd * (d2x * P[2][0] + d2y * P[2][2]);
+            Bs[8] += wd * (d2x * P[3][0] + d2y * P[3][2]);
+            Bs[9] += wd * (d2y * P[3][1] + d2x * P[3][2]);
+        }
+#pragma unroll
+        for (int i = 0; i < 10; ++i) S.B[i] = Bs[i];
+    } else if (valid && tl == 9 && !skip_mac) {
+        // Z = sym(inv(VGV) + Zb) is block diagonal with 2x2 blocks on the
+        // xi-sampling rows (0, 1) and the eta-sampling rows (2, 3)
+        const double zx00 = S.ivd[0] + zs[0], zx11 = S.ivd[1] + zs[0], zx01 = zs[1];
+        const double zy00 = S.ivd[2] + zs[2], zy11 = S.ivd[3] + zs[2], zy01 = zs[3];
+        const double ix = 1.0 / (zx00 * zx11 - zx01 * zx01), iy = 1.0 / (zy00 * zy11 - zy01 * zy01);
+        S.W[0] = zx11 * ix; S.W[1] = -zx01 * ix; S.W[2] = zx00 * ix;
+        S.W[3] = zy11 * iy; S.W[4] = -zy01 * iy; S.W[5] = zy00 * iy;
     }
     __syncwarp();
 
-    // Phase 4: one node pair per lane.
+    // Phase 3: X = B^-1 A' for both condensations, one A row per lane.
+    if (valid && tl < 8) {
+        const Ldl4 f(S.B);
+        double x[4];
+        f.solve(am, x);
+#pragma unroll
+        for (int l = 0; l < 4; ++l) S.Xm[l][tl] = x[l];
+        f.solve(ab, x);
+#pragma unroll
+        for (int l = 0; l < 4; ++l) S.Xb[l][tl] = x[l];
+    }
+    __syncwarp();
+
+    // Phase 4: one node pair (a <= b) per lane.  Gauss-point sums, the
+    // 6x6 local block (18 structural nonzeros), then T'KT by 3x3 sub-blocks.
     double lmax = 0.0;
     if (valid) {
-        const int a = c_pair_a[tl], b = c_pair_b[tl];
-        double L[6][6];
-#pragma unroll
-        for (int i = 0; i < 6; ++i)
-#pragma unroll
-            for (int j = 0; j < 6; ++j) L[i][j] = 0.0;
-        const double ad = S.alpha_d;
+        int a, b;
+        q4_pair(tl, a, b);
+        double Pxx = 0, Pxy = 0, Pyx = 0, Pyy = 0, T00 = 0, T01 = 0, T10 = 0, T11 = 0;
+        double SxN = 0, SyN = 0, SNx = 0, SNy = 0, SNN = 0;
+        const double xca = S.g.dNx[4][a], yca = S.g.dNy[4][a], xcb = S.g.dNx[4][b], ycb = S.g.dNy[4][b];
 #pragma unroll
         for (int g = 0; g < 4; ++g) {
             double r, s;
             q4_shape_gp(g, r, s);
             const double wd = S.g.wdet[g];
-            double ma[2][3], mb[2][3], ba[2][3], bb[2][3];
-            q4_mem_col(S.g, g, a, 0, ma[0]); q4_mem_col(S.g, g, a, 1, ma[1]);
-            q4_mem_col(S.g, g, b, 0, mb[0]); q4_mem_col(S.g, g, b, 1, mb[1]);
-            q4_bend_col(S.g, g, a, 0, ba[0]); q4_bend_col(S.g, g, a, 1, ba[1]);
-            q4_bend_col(S.g, g, b, 0, bb[0]); q4_bend_col(S.g, g, b, 1, bb[1]);
-#pragma unroll
-            for (int be = 0; be < 2; ++be) {
-                double cm[3], cb[3];
-#pragma unroll
-                for (int r = 0; r < 3; ++r) {
-                    cm[r] = wd * (S.Cm[3 * r] * mb[be][0] + S.Cm[3 * r + 1] * mb[be][1] + S.Cm[3 * r + 2] * mb[be][2]);
-                    cb[r] = wd * (S.Cb[3 * r] * bb[be][0] + S.Cb[3 * r + 1] * bb[be][1] + S.Cb[3 * r + 2] * bb[be][2]);
-                }
-#pragma unroll
-                for (int al = 0; al < 2; ++al) {
-                    L[al][be] += ma[al][0] * cm[0] + ma[al][1] * cm[1] + ma[al][2] * cm[2];
-                    L[3 + al][3 + be] += ba[al][0] * cb[0] + ba[al][1] * cb[1] + ba[al][2] * cb[2];
-                }
-            }
-            // drilling: Bd = [0.5 dN/dy, -0.5 dN/dx, N] on (u, v, theta_z)
-            double da[3] = {0.5 * S.g.dNy[g][a], -0.5 * S.g.dNx[g][a], q4_N(a, r, s)};
-            double db[3] = {0.5 * S.g.dNy[g][b], -0.5 * S.g.dNx[g][b], q4_N(b, r, s)};
-            const int di[3] = {0, 1, 5};
-            double wda = wd * ad;
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) L[di[i]][di[j]] += wda * da[i] * db[j];
+            const double xa = S.g.dNx[g][a], ya = S.g.dNy[g][a], xb = S.g.dNx[g][b], yb = S.g.dNy[g][b];
+            const double t0a = 2.0 * (-xa) - (-xca), t1a = 2.0 * ya - yca;
+            const double t0b = 2.0 * (-xb) - (-xcb), t1b = 2.0 * yb - ycb;
+            const double Na = q4_N(a, r, s), Nb = q4_N(b, r, s);
+            const double wx = wd * xa, wy = wd * ya, w0 = wd * t0a, w1 = wd * t1a, wn = wd * Na;
+            Pxx += wx * xb; Pxy += wx * yb; Pyx += wy * xb; Pyy += wy * yb;
+            T00 += w0 * t0b; T01 += w0 * t1b; T10 += w1 * t0b; T11 += w1 * t1b;
+            SxN += wx * Nb; SyN += wy * Nb; SNx += wn * xb; SNy += wn * yb; SNN += wn * Nb;
         }
-        if (!S.skip_macneal) {
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    double s1 = 0.0, s2 = 0.0;
-                    for (int l = 0; l < 4; ++l) {
-                        s1 += S.D[l][3 * a + i] * S.u.x.Y[l][3 * b + j];
-                        s2 += S.D[l][3 * b + j] * S.u.x.Y[l][3 * a + i];
-                    }
-                    L[2 + i][2 + j] += 0.5 * (s1 + s2);
-                }
-        }
+        // incompatible-mode condensations
+        double cmm[2][2], cbb[2][2];
 #pragma unroll
         for (int al = 0; al < 2; ++al)
 #pragma unroll
             for (int be = 0; be < 2; ++be) {
                 double sm = 0.0, sb = 0.0;
+#pragma unroll
                 for (int l = 0; l < 4; ++l) {
-                    sm += S.Kabm[2 * a + al][l] * S.u.x.Xm[l][2 * b + be];
-                    sb += S.Kabb[2 * a + al][l] * S.u.x.Xb[l][2 * b + be];
+                    sm += S.Am[2 * a + al][l] * S.Xm[l][2 * b + be];
+                    sb += S.Ab[2 * a + al][l] * S.Xb[l][2 * b + be];
                 }
-                L[al][be] -= sm;
-                if (S.bend_cond) L[3 + al][3 + be] -= sb;
+                cmm[al][be] = sm;
+                cbb[al][be] = sb;
             }
-        // T'KT on the node pair, one 3x3 sub-block at a time (keeps the
-        // register footprint to the local 6x6 block)
+        // membrane + drilling on (u, v, theta_z): Bd = (dN/dy / 2, -dN/dx / 2, N)
+        const double q = 0.25 * ad, hq = 0.5 * ad;
+        double Lm[3][3];
+        Lm[0][0] = cm * (Pxx + gam * Pyy) + q * Pyy - cm * cmm[0][0];
+        Lm[0][1] = cm * (nu * Pxy + gam * Pyx) - q * Pyx - cm * cmm[0][1];
+        Lm[1][0] = cm * (nu * Pyx + gam * Pxy) - q * Pxy - cm * cmm[1][0];
+        Lm[1][1] = cm * (Pyy + gam * Pxx) + q * Pxx - cm * cmm[1][1];
+        Lm[0][2] = hq * SyN; Lm[1][2] = -hq * SxN;
+        Lm[2][0] = hq * SNy; Lm[2][1] = -hq * SNx; Lm[2][2] = ad * SNN;
+        // plate on (w, theta_x, theta_y): bending with the twist row, then
+        // MacNeal's shear D' Z^-1 D
+        double Lp[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+        Lp[1][1] = cb * (Pyy + gam * T00) - cb * cbb[0][0];
+        Lp[1][2] = cb * (gam * T01 - nu * Pyx) - cb * cbb[0][1];
+        Lp[2][1] = cb * (gam * T10 - nu * Pxy) - cb * cbb[1][0];
+        Lp[2][2] = cb * (Pxx + gam * T11) - cb * cbb[1][1];
+        if (!skip_mac) {
+            const double pt = 0.57735026918962576451;
+            // sampling-row parts of the w, theta_x, theta_y columns of D
+            const double cxa0 = S.Dd[0][a], cxa1 = S.Dd[1][a], cya0 = S.Dd[2][a], cya1 = S.Dd[3][a];
+            const double cxb0 = S.Dd[0][b], cxb1 = S.Dd[1][b], cyb0 = S.Dd[2][b], cyb1 = S.Dd[3][b];
+            const double nxa0 = q4_N(a, 0.0, -pt), nxa1 = q4_N(a, 0.0, pt);
+            const double nya0 = -q4_N(a, -pt, 0.0), nya1 = -q4_N(a, pt, 0.0);
+            const double nxb0 = q4_N(b, 0.0, -pt), nxb1 = q4_N(b, 0.0, pt);
+            const double nyb0 = -q4_N(b, -pt, 0.0), nyb1 = -q4_N(b, pt, 0.0);
+            const double w0 = S.W[0], w1 = S.W[1], w2 = S.W[2], w3 = S.W[3], w4 = S.W[4], w5 = S.W[5];
+            const double yx0 = w0 * cxb0 + w1 * cxb1, yx1 = w1 * cxb0 + w2 * cxb1;
+            const double ynx0 = w0 * nxb0 + w1 * nxb1, ynx1 = w1 * nxb0 + w2 * nxb1;
+            const double yy0 = w3 * cyb0 + w4 * cyb1, yy1 = w4 * cyb0 + w5 * cyb1;
+            const double yny0 = w3 * nyb0 + w4 * nyb1, yny1 = w4 * nyb0 + w5 * nyb1;
+            Lp[0][0] = (cxa0 * yx0 + cxa1 * yx1) + (cya0 * yy0 + cya1 * yy1);
+            Lp[0][1] = cya0 * yny0 + cya1 * yny1;
+            Lp[0][2] = cxa0 * ynx0 + cxa1 * ynx1;
+            Lp[1][0] = nya0 * yy0 + nya1 * yy1;
+            Lp[1][1] += nya0 * yny0 + nya1 * yny1;
+            Lp[2][0] = nxa0 * yx0 + nxa1 * yx1;
+            Lp[2][2] += nxa0 * ynx0 + nxa1 * ynx1;
+        }
+        double Qa[9], Qb[9];
+        if (nodeR) {
+            double Ra[9], Rb[9];
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                Ra[i] = __ldg(nodeR + 9 * (int64_t)nd[a] + i);
+                Rb[i] = __ldg(nodeR + 9 * (int64_t)nd[b] + i);
+            }
+            node_block(V, V + 3, V + 6, Ra, Qa);
+            node_block(V, V + 3, V + 6, Rb, Qb);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 9; ++i) { Qa[i] = V[i]; Qb[i] = V[i]; }
+        }
         const int32_t sl = __ldg(o.blk_slot + e * 10 + tl);
-#pragma unroll
-        for (int bi = 0; bi < 2; ++bi)
-#pragma unroll
-            for (int bj = 0; bj < 2; ++bj) {
-                double Ls[3][3], O[3][3];
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) Ls[i][j] = L[3 * bi + i][3 * bj + j];
-                rot_block(S.g.Q[a], Ls, S.g.Q[b], O);
-                write_sub_block(o, e, sl, a, b, bi, bj, O, lmax, 24);
-            }
+        double M[3][3], O[3][3];
+        // local dof order (u, v, w, theta_x, theta_y, theta_z)
+        M[0][0] = Lm[0][0]; M[0][1] = Lm[0][1]; M[1][0] = Lm[1][0]; M[1][1] = Lm[1][1]; M[2][2] = Lp[0][0];
+        rot_sparse<0b100011011>(Qa, M, Qb, O);
+        write_sub_block(o, e, sl, a, b, 0, 0, O, lmax, 24);
+        M[0][2] = Lm[0][2]; M[1][2] = Lm[1][2]; M[2][0] = Lp[0][1]; M[2][1] = Lp[0][2];
+        rot_sparse<0b011100100>(Qa, M, Qb, O);
+        write_sub_block(o, e, sl, a, b, 0, 1, O, lmax, 24);
+        M[0][2] = Lp[1][0]; M[1][2] = Lp[2][0]; M[2][0] = Lm[2][0]; M[2][1] = Lm[2][1];
+        rot_sparse<0b011100100>(Qa, M, Qb, O);
+        write_sub_block(o, e, sl, a, b, 1, 0, O, lmax, 24);
+        M[0][0] = Lp[1][1]; M[0][1] = Lp[1][2]; M[1][0] = Lp[2][1]; M[1][1] = Lp[2][2]; M[2][2] = Lm[2][2];
+        rot_sparse<0b100011011>(Qa, M, Qb, O);
+        write_sub_block(o, e, sl, a, b, 1, 1, O, lmax, 24);
     }
     if (o.maxabs) {
         for (int off = 16; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
