@@ -1,18 +1,21 @@
 // elem_q4.cuh -- CQUAD4 stiffness (K) and differential stiffness (KG) kernels.
 //
 // Mapping: a team of 10 lanes owns one element, three teams per warp
-// (lanes 30-31 only join the warp barriers).  Per-element intermediates live
-// in shared memory; the final phase gives each lane one node pair (a <= b)
-// of the symmetric 24x24 global matrix, so the 300 packed values are
-// produced without redundant work and written straight to their sorted
-// contribution slots (deterministic segmented reduction follows).
+// (lanes 30-31 only join the warp barriers).  Every lane of a team computes
+// the frame and local coordinates in registers; per-point and per-row
+// intermediates are spread over the lanes and meet in shared memory; the
+// final phase gives each lane one node pair (a <= b) of the symmetric 24x24
+// global matrix, so the 300 packed values are produced without redundant
+// work and written straight to their sorted contribution slots
+// (deterministic segmented reduction follows).
 //
 // K follows stiffness_quad4_matrices' default planar branch
 // (src/FEMKernels.jl:3185-4034): 2x2 Gauss membrane + bending with the
 // MacNeal twist row (:3670-3673), Hughes-Brezzi drilling (:3556-3559,
-// :3778-3779), Wilson incompatible modes condensed by 4x4 inverses
-// (:3790-3801, :3964-4011) and MacNeal's residual-bending-flexibility shear
-// (add_quad4_macneal_shear_rbf!, :4715-4978); then T'KT with T built from the
+// :3778-3779), Wilson incompatible modes condensed (:3790-3801, :3964-4011;
+// both condensations through one LDL' factorisation, see Q4KShared) and
+// MacNeal's residual-bending-flexibility shear (add_quad4_macneal_shear_rbf!,
+// :4715-4978); then T'KT with T built from the
 // element frame and node CD frames (src/solver/assembly.jl:3808-3837).
 //
 // KG follows the Q4 branch of the shell loop of assemble_geometric_stiffness
@@ -35,7 +38,6 @@ constexpr int Q4_TEAMS_PER_WARP = 3;
 constexpr int Q4_WARPS = 4;
 constexpr int Q4_THREADS = 32 * Q4_WARPS;
 constexpr int Q4_ELEMS_PER_BLOCK = Q4_TEAMS_PER_WARP * Q4_WARPS;
-constexpr int Q4_PACKED = 300;
 
 __constant__ int c_pair_a[10] = {0, 0, 0, 0, 1, 1, 1, 2, 2, 3};
 __constant__ int c_pair_b[10] = {0, 1, 2, 3, 1, 2, 3, 2, 3, 3};
@@ -92,16 +94,6 @@ __device__ __forceinline__ double *blk_entry(const ElemOut &o, int32_t s, int i,
     return (s & kBlkTranspose) ? base + 6 * j + i : base + 6 * i + j;
 }
 
-struct Q4Geo {
-    double p[4][3];
-    double v[3][3];
-    double lc[4][2];
-    double Q[4][9];
-    double dNx[5][4], dNy[5][4];  // 4 Gauss points + centre (index 4)
-    double wdet[4];
-    double dphi[4][4];            // d1x, d1y, d2x, d2y per Gauss point
-};
-
 // Per-point data of one CQUAD4 shared by its team.
 struct Q4Pts {
     double dNx[5][4], dNy[5][4];  // 4 Gauss points + centre (index 4)
@@ -127,14 +119,14 @@ struct Q4KShared {
     double Xm[4][8], Xb[4][8];  // B^-1 Am', B^-1 Ab'
 };
 
+// KG kernel state of one element (membrane incompatible modes only; the
+// condensation map is -B^-1 Am' with Am, B as in the K kernel).
 struct Q4GShared {
-    Q4Geo g;
-    double Cm[9], h;
-    double uuv[8];
-    double P[4][4][3];  // Cm b_l(g) of the membrane incompatible modes
-    double Kabm[8][4], Kbbm[16];
-    double Am[4][8];
-    double alpha[4];
+    Q4Pts g;
+    double uuv[8];        // local (u, v) of each node
+    double Am[8][4];
+    double B[10];
+    double map[4][8];     // -B^-1 Am'
     double t[8][8], gz[8][4], f[8];
 };
 
@@ -148,100 +140,6 @@ __device__ __forceinline__ double q4_N(int k, double r, double s) {
     return 0.25 * (1 + ((k == 1 || k == 2) ? r : -r)) * (1 + (k >= 2 ? s : -s));
 }
 
-// Phase 0 of both kernels: node loads, frame, local coordinates, node
-// transformation blocks and Gauss-point Jacobians.  Called by all lanes of
-// a team; `tl` is the lane index within the team, `valid` false for teams
-// past the end (they still reach every barrier).
-__device__ __forceinline__ void q4_geometry(Q4Geo &G, int tl, bool valid, const int32_t *nd,
-                                            const double *__restrict__ coords, const double *__restrict__ nodeR) {
-    if (valid && tl < 4) {
-        int n = nd[tl];
-        G.p[tl][0] = __ldg(coords + 3 * (int64_t)n);
-        G.p[tl][1] = __ldg(coords + 3 * (int64_t)n + 1);
-        G.p[tl][2] = __ldg(coords + 3 * (int64_t)n + 2);
-    }
-    __syncwarp();
-    if (valid && tl == 0) {
-        double v1[3], v2[3], v3[3];
-        q4_frame(G.p[0], G.p[1], G.p[2], G.p[3], v1, v2, v3);
-        double c[3];
-        for (int i = 0; i < 3; ++i) c[i] = (G.p[0][i] + G.p[1][i] + G.p[2][i] + G.p[3][i]) / 4.0;
-        for (int k = 0; k < 4; ++k) {
-            double d[3];
-            sub3(G.p[k], c, d);
-            G.lc[k][0] = dot3(d, v1);
-            G.lc[k][1] = dot3(d, v2);
-        }
-        for (int i = 0; i < 3; ++i) { G.v[0][i] = v1[i]; G.v[1][i] = v2[i]; G.v[2][i] = v3[i]; }
-    }
-    __syncwarp();
-    if (valid && tl < 4) {
-        const double *R = nodeR ? nodeR + 9 * (int64_t)nd[tl] : nullptr;
-        double Rl[9];
-        if (R)
-            for (int i = 0; i < 9; ++i) Rl[i] = __ldg(R + i);
-        node_block(G.v[0], G.v[1], G.v[2], R ? Rl : nullptr, G.Q[tl]);
-    } else if (valid && tl < 9) {
-        int g = tl - 4;  // 0..3 Gauss points, 4 = centre
-        double r = 0.0, s = 0.0;
-        if (g < 4) q4_shape_gp(g, r, s);
-        double dNr[4] = {-0.25 * (1 - s), 0.25 * (1 - s), 0.25 * (1 + s), -0.25 * (1 + s)};
-        double dNs[4] = {-0.25 * (1 - r), -0.25 * (1 + r), 0.25 * (1 + r), 0.25 * (1 - r)};
-        double J11 = 0, J12 = 0, J21 = 0, J22 = 0;
-        for (int k = 0; k < 4; ++k) {
-            J11 += dNr[k] * G.lc[k][0]; J12 += dNr[k] * G.lc[k][1];
-            J21 += dNs[k] * G.lc[k][0]; J22 += dNs[k] * G.lc[k][1];
-        }
-        double det = J11 * J22 - J12 * J21;
-        double inv = 1.0 / det;
-        double iJ11 = J22 * inv, iJ12 = -J12 * inv, iJ21 = -J21 * inv, iJ22 = J11 * inv;
-        for (int k = 0; k < 4; ++k) {
-            G.dNx[g][k] = iJ11 * dNr[k] + iJ12 * dNs[k];
-            G.dNy[g][k] = iJ21 * dNr[k] + iJ22 * dNs[k];
-        }
-        if (g < 4) {
-            double a = fabs(det);
-            G.wdet[g] = a < 1e-12 ? 1e-12 : a;
-            G.dphi[g][0] = iJ11 * (-2.0 * r);
-            G.dphi[g][1] = iJ21 * (-2.0 * r);
-            G.dphi[g][2] = iJ12 * (-2.0 * s);
-            G.dphi[g][3] = iJ22 * (-2.0 * s);
-        }
-    }
-}
-
-// Bending B column of local dof (theta_x: comp 0, theta_y: comp 1) of node k
-// at Gauss point g, with the MacNeal twist correction.
-__device__ __forceinline__ void q4_bend_col(const Q4Geo &G, int g, int k, int comp, double b[3]) {
-    double x = G.dNx[g][k], y = G.dNy[g][k];
-    if (comp == 0) { b[0] = 0.0; b[1] = -y; b[2] = 2.0 * (-x) - (-G.dNx[4][k]); }
-    else { b[0] = x; b[1] = 0.0; b[2] = 2.0 * y - G.dNy[4][k]; }
-}
-__device__ __forceinline__ void q4_mem_col(const Q4Geo &G, int g, int k, int comp, double b[3]) {
-    double x = G.dNx[g][k], y = G.dNy[g][k];
-    if (comp == 0) { b[0] = x; b[1] = 0.0; b[2] = y; }
-    else { b[0] = 0.0; b[1] = y; b[2] = x; }
-}
-// Membrane incompatible-mode column l (0..3) at Gauss point g.
-__device__ __forceinline__ void q4_bi_col(const Q4Geo &G, int g, int l, double b[3]) {
-    double d1x = G.dphi[g][0], d1y = G.dphi[g][1], d2x = G.dphi[g][2], d2y = G.dphi[g][3];
-    switch (l) {
-        case 0: b[0] = d1x; b[1] = 0.0; b[2] = d1y; break;
-        case 1: b[0] = 0.0; b[1] = d1y; b[2] = d1x; break;
-        case 2: b[0] = d2x; b[1] = 0.0; b[2] = d2y; break;
-        default: b[0] = 0.0; b[1] = d2y; b[2] = d2x; break;
-    }
-}
-// Bending incompatible-mode column l (0..3) at Gauss point g.
-__device__ __forceinline__ void q4_bib_col(const Q4Geo &G, int g, int l, double b[3]) {
-    double d1x = G.dphi[g][0], d1y = G.dphi[g][1], d2x = G.dphi[g][2], d2y = G.dphi[g][3];
-    switch (l) {
-        case 0: b[0] = 0.0; b[1] = -d1y; b[2] = -d1x; break;
-        case 1: b[0] = 0.0; b[1] = -d2y; b[2] = -d2x; break;
-        case 2: b[0] = d1x; b[1] = 0.0; b[2] = d1y; break;
-        default: b[0] = d2x; b[1] = 0.0; b[2] = d2y; break;
-    }
-}
 __device__ __forceinline__ double quad_form(const double a[3], const double C[9], const double b[3]) {
     double cb0 = C[0] * b[0] + C[1] * b[1] + C[2] * b[2];
     double cb1 = C[3] * b[0] + C[4] * b[1] + C[5] * b[2];
@@ -256,27 +154,6 @@ __device__ __forceinline__ void rot_block(const double *Qa, const double L[3][3]
         for (int j = 0; j < 3; ++j) W[i][j] = L[i][0] * Qb[j] + L[i][1] * Qb[3 + j] + L[i][2] * Qb[6 + j];
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) out[i][j] = Qa[i] * W[0][j] + Qa[3 + i] * W[1][j] + Qa[6 + i] * W[2][j];
-}
-
-// Write one global 6x6 node-pair block (a <= b, pair index p) of element e
-// with NP node pairs; diagonal entries of diagonal pairs also go to the
-// orig_diag staging (K only).
-template <int NN, int NP>
-__device__ __forceinline__ void write_pair_block(const ElemOut &o, int64_t e, int p, int a, int b, const double Gb[6][6],
-                                                 double &lmax) {
-    const int32_t s = __ldg(o.blk_slot + e * NP + p);
-#pragma unroll
-    for (int i = 0; i < 6; ++i)
-#pragma unroll
-        for (int j = 0; j < 6; ++j) {
-            double v = Gb[i][j];
-            lmax = fmax(lmax, fabs(v));
-            *blk_entry(o, s, i, j) = v;
-        }
-    if (o.diag_staging && a == b) {
-#pragma unroll
-        for (int i = 0; i < 6; ++i) o.diag_staging[__ldg(o.diag_slot + e * 6 * NN + 6 * a + i)] = Gb[i][i];
-    }
 }
 
 // Write one 3x3 sub-block (bi, bj) of the node-pair block (a, b) of element
@@ -698,104 +575,149 @@ __global__ void __launch_bounds__(Q4_THREADS) q4_kg_kernel(int64_t nq, const int
     const int64_t e = (int64_t)blockIdx.x * Q4_ELEMS_PER_BLOCK + slot_id;
     const bool valid = in_team && e < nq;
     Q4GShared &S = sh[slot_id];
-    int32_t nd[4] = {0, 0, 0, 0};
-    if (valid)
-        for (int k = 0; k < 4; ++k) nd[k] = __ldg(nodes + 4 * e + k);
 
-    q4_geometry(S.g, in_team ? tl : 99, valid, nd, coords, nodeR);
-    if (valid && tl == 9) {
+    // Phase 0, every lane in registers: nodes, corners, frame, local
+    // coordinates, membrane stiffness scalar.
+    int nd[4] = {0, 0, 0, 0};
+    double V[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    double lc[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
+    double h = 1.0, E = 0.0, nu = 0.0;
+    if (valid) {
         const double *pr = prop + 7 * e;
-        double h = o.thickness(e, pr), E = __ldg(pr + 1), nu = __ldg(pr + 2);
-        double cm = E / (1 - nu * nu);
-        double base[9] = {1.0, nu, 0.0, nu, 1.0, 0.0, 0.0, 0.0, (1 - nu) / 2};
-        for (int i = 0; i < 9; ++i) S.Cm[i] = (cm * base[i]) * h;
-        S.h = h;
+        h = o.thickness(e, pr); E = __ldg(pr + 1); nu = __ldg(pr + 2);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) nd[k] = __ldg(nodes + 4 * e + k);
+        double p[4][3];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) p[k][i] = __ldg(coords + 3 * (int64_t)nd[k] + i);
+        q4_local(p, V, lc);
     }
-    __syncwarp();
-    // local membrane displacements u_elem = T u_global (u, v of each node)
+    const double gam = (1 - nu) / 2;
+    const double cmh = (E / (1 - nu * nu)) * h;  // Cm = cmh P(nu)
+
+    // Phase 1: Gauss-point derivatives (lanes 0-3); local membrane
+    // displacements u_elem = T u_global (lanes 4-7, assembly.jl:5176-5185).
     if (valid && tl < 4) {
-        const double *ug = u + 6 * (int64_t)nd[tl];
-        double u0 = __ldg(ug), u1 = __ldg(ug + 1), u2 = __ldg(ug + 2);
-        const double *Q = S.g.Q[tl];
-        S.uuv[2 * tl] = Q[0] * u0 + Q[1] * u1 + Q[2] * u2;
-        S.uuv[2 * tl + 1] = Q[3] * u0 + Q[4] * u1 + Q[5] * u2;
-    }
-    // C b_l(g) of the membrane incompatible-mode columns, then K_ab / K_bb
-    // rows with four independent accumulators.
-    if (valid) {
-        for (int w = tl; w < 16; w += Q4_TEAM) {
-            const int g = w >> 2, l = w & 3;
-            double b[3];
-            q4_bi_col(S.g, g, l, b);
+        double r, s, dx[4], dy[4], iJ[4];
+        q4_shape_gp(tl, r, s);
+        const double det = q4_point_derivs(lc, r, s, false, dx, dy, iJ);
 #pragma unroll
-            for (int r = 0; r < 3; ++r) S.P[g][l][r] = S.Cm[3 * r] * b[0] + S.Cm[3 * r + 1] * b[1] + S.Cm[3 * r + 2] * b[2];
+        for (int k = 0; k < 4; ++k) { S.g.dNx[tl][k] = dx[k]; S.g.dNy[tl][k] = dy[k]; }
+        const double a = fabs(det);
+        S.g.wdet[tl] = a < 1e-12 ? 1e-12 : a;
+        S.g.dphi[tl][0] = iJ[0] * (-2.0 * r);
+        S.g.dphi[tl][1] = iJ[2] * (-2.0 * r);
+        S.g.dphi[tl][2] = iJ[1] * (-2.0 * s);
+        S.g.dphi[tl][3] = iJ[3] * (-2.0 * s);
+    } else if (valid && tl < 8) {
+        const int k = tl - 4;
+        double Q[9];
+        if (nodeR) {
+            double R[9];
+#pragma unroll
+            for (int i = 0; i < 9; ++i) R[i] = __ldg(nodeR + 9 * (int64_t)nd[k] + i);
+            node_block(V, V + 3, V + 6, R, Q);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 9; ++i) Q[i] = V[i];
         }
+        const double *ug = u + 6 * (int64_t)nd[k];
+        const double u0 = __ldg(ug), u1 = __ldg(ug + 1), u2 = __ldg(ug + 2);
+        S.uuv[2 * k] = Q[0] * u0 + Q[1] * u1 + Q[2] * u2;
+        S.uuv[2 * k + 1] = Q[3] * u0 + Q[4] * u1 + Q[5] * u2;
     }
     __syncwarp();
-    if (valid) {
-        for (int r = tl; r < 12; r += Q4_TEAM) {
-            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+
+    // Phase 2: membrane rows of Am (lanes 0-7) and B (lane 8).
+    double am[4] = {0.0, 0.0, 0.0, 0.0};
+    if (valid && tl < 8) {
+        const int k = tl >> 1;
+        const bool c1 = tl & 1;
 #pragma unroll
-            for (int g = 0; g < 4; ++g) {
-                double a[3];
-                if (r < 8) q4_mem_col(S.g, g, r >> 1, r & 1, a);
-                else q4_bi_col(S.g, g, r - 8, a);
-                const double wd = S.g.wdet[g];
+        for (int g = 0; g < 4; ++g) {
+            const double wd = S.g.wdet[g], x = S.g.dNx[g][k], y = S.g.dNy[g][k];
+            const double d1x = S.g.dphi[g][0], d1y = S.g.dphi[g][1], d2x = S.g.dphi[g][2], d2y = S.g.dphi[g][3];
+            const double m0 = wd * (c1 ? 0.0 : x), m1 = wd * (c1 ? y : 0.0), m2 = wd * (c1 ? x : y);
+            const double P[4][3] = {{d1x, nu * d1x, gam * d1y}, {nu * d1y, d1y, gam * d1x},
+                                    {d2x, nu * d2x, gam * d2y}, {nu * d2y, d2y, gam * d2x}};
 #pragma unroll
-                for (int l = 0; l < 4; ++l) {
-                    const double *P = S.P[g][l];
-                    acc[l] += wd * (a[0] * P[0] + a[1] * P[1] + a[2] * P[2]);
-                }
-            }
-#pragma unroll
-            for (int l = 0; l < 4; ++l) {
-                if (r < 8) S.Kabm[r][l] = acc[l];
-                else S.Kbbm[4 * (r - 8) + l] = acc[l];
-            }
+            for (int m = 0; m < 4; ++m) am[m] += m0 * P[m][0] + m1 * P[m][1] + m2 * P[m][2];
         }
-    }
-    __syncwarp();
-    if (valid && tl == 0) inv4_inplace(S.Kbbm);
-    __syncwarp();
-    // condensation map A = -Kbb^-1 Kab' on the membrane dofs
-    if (valid) {
-        for (int w = tl; w < 32; w += Q4_TEAM) {
-            int l = w >> 3, r = w & 7;
-            double s = 0.0;
-            for (int q = 0; q < 4; ++q) s += S.Kbbm[4 * l + q] * S.Kabm[r][q];
-            S.Am[l][r] = -s;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) S.Am[tl][m] = am[m];
+    } else if (valid && tl == 8) {
+        double Bs[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+            const double wd = S.g.wdet[g];
+            const double d1x = S.g.dphi[g][0], d1y = S.g.dphi[g][1], d2x = S.g.dphi[g][2], d2y = S.g.dphi[g][3];
+            const double P[4][3] = {{d1x, nu * d1x, gam * d1y}, {nu * d1y, d1y, gam * d1x},
+                                    {d2x, nu * d2x, gam * d2y}, {nu * d2y, d2y, gam * d2x}};
+            Bs[0] += wd * (d1x * P[0][0] + d1y * P[0][2]);
+            Bs[1] += wd * (d1x * P[1][0] + d1y * P[1][2]);
+            Bs[2] += wd * (d1x * P[2][0] + d1y * P[2][2]);
+            Bs[3] += wd * (d1x * P[3][0] + d1y * P[3][2]);
+            Bs[4] += wd * (d1y * P[1][1] + d1x * P[1][2]);
+            Bs[5] += wd * (d1y * P[2][1] + d1x * P[2][2]);
+            Bs[6] += wd * (d1y * P[3][1] + d1x * P[3][2]);
+            Bs[7] += wd * (d2x * P[2][0] + d2y * P[2][2]);
+            Bs[8] += wd * (d2x * P[3][0] + d2y * P[3][2]);
+            Bs[9] += wd * (d2y * P[3][1] + d2x * P[3][2]);
         }
+#pragma unroll
+        for (int i = 0; i < 10; ++i) S.B[i] = Bs[i];
     }
     __syncwarp();
-    if (valid && tl < 4) {
-        double s = 0.0;
-        for (int r = 0; r < 8; ++r) s += S.Am[tl][r] * S.uuv[r];
-        S.alpha[tl] = s;
+
+    // Phase 3 (lanes 0-7): column tl of the condensation map -B^-1 Am'
+    // (quad4_membrane_incompatible_condensation_map, FEMKernels.jl:6708-6785)
+    // and, in every one of these lanes, the mode amplitudes
+    // alpha = -B^-1 (Am' u) of quad4_membrane_force_field (:6366-6446).
+    double alpha[4] = {0.0, 0.0, 0.0, 0.0};
+    if (valid && tl < 8) {
+        const Ldl4 f(S.B);
+        double x[4];
+        f.solve(am, x);
+#pragma unroll
+        for (int l = 0; l < 4; ++l) S.map[l][tl] = -x[l];
+        double rhs[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const double ur = S.uuv[r];
+#pragma unroll
+            for (int l = 0; l < 4; ++l) rhs[l] += S.Am[r][l] * ur;
+        }
+        f.solve(rhs, x);
+#pragma unroll
+        for (int l = 0; l < 4; ++l) alpha[l] = -x[l];
     }
     __syncwarp();
-    // Gauss-point stresses, principal directions and gradient vectors:
-    // lane tl < 8 handles Gauss point g = tl / 2, principal direction tl % 2.
+
+    // Phase 4: Gauss-point stresses N/h, principal directions and gradient
+    // vectors; lane tl < 8 handles Gauss point g = tl / 2, direction tl % 2.
     if (valid && tl < 8) {
         const int g = tl >> 1, dir = tl & 1;
-        const Q4Geo &G = S.g;
         double exx = 0.0, eyy = 0.0, gxy = 0.0;
+#pragma unroll
         for (int k = 0; k < 4; ++k) {
-            double x = G.dNx[g][k], y = G.dNy[g][k];
-            exx += x * S.uuv[2 * k];
-            eyy += y * S.uuv[2 * k + 1];
-            gxy += y * S.uuv[2 * k] + x * S.uuv[2 * k + 1];
+            const double x = S.g.dNx[g][k], y = S.g.dNy[g][k], uk = S.uuv[2 * k], vk = S.uuv[2 * k + 1];
+            exx += x * uk;
+            eyy += y * vk;
+            gxy += y * uk + x * vk;
         }
-        double d1x = G.dphi[g][0], d1y = G.dphi[g][1], d2x = G.dphi[g][2], d2y = G.dphi[g][3];
-        exx += d1x * S.alpha[0] + d2x * S.alpha[2];
-        eyy += d1y * S.alpha[1] + d2y * S.alpha[3];
-        gxy += d1y * S.alpha[0] + d1x * S.alpha[1] + d2y * S.alpha[2] + d2x * S.alpha[3];
-        double h = S.h;
-        double sxx = (S.Cm[0] * exx + S.Cm[1] * eyy + S.Cm[2] * gxy) / h;
-        double syy = (S.Cm[3] * exx + S.Cm[4] * eyy + S.Cm[5] * gxy) / h;
-        double sxy = (S.Cm[6] * exx + S.Cm[7] * eyy + S.Cm[8] * gxy) / h;
+        const double d1x = S.g.dphi[g][0], d1y = S.g.dphi[g][1], d2x = S.g.dphi[g][2], d2y = S.g.dphi[g][3];
+        exx += d1x * alpha[0] + d2x * alpha[2];
+        eyy += d1y * alpha[1] + d2y * alpha[3];
+        gxy += d1y * alpha[0] + d1x * alpha[1] + d2y * alpha[2] + d2x * alpha[3];
+        const double ih = 1.0 / h;
+        const double sxx = (cmh * (exx + nu * eyy)) * ih;
+        const double syy = (cmh * (nu * exx + eyy)) * ih;
+        const double sxy = (cmh * (gam * gxy)) * ih;
         // principal_stress_2d_components (FEMKernels.jl:6891-6902)
-        double mean = 0.5 * (sxx + syy), hd = 0.5 * (sxx - syy);
-        double rad = sqrt(hd * hd + sxy * sxy);
+        const double mean = 0.5 * (sxx + syy), hd = 0.5 * (sxx - syy);
+        const double rad = sqrt(hd * hd + sxy * sxy);
         double lam, c, sn;
         if (rad <= 1e-30) {
             lam = mean;
@@ -807,45 +729,66 @@ __global__ void __launch_bounds__(Q4_THREADS) q4_kg_kernel(int64_t nq, const int
             // sin 2theta = sxy / rad by the half-angle identities, taking the
             // square root on the side without cancellation.
             double c1, s1;
+            const double i2r = 1.0 / (2.0 * rad);
             if (hd >= 0.0) {
-                c1 = sqrt((rad + hd) / (2.0 * rad));
-                s1 = sxy / (2.0 * c1 * rad);
+                c1 = sqrt((rad + hd) * i2r);
+                s1 = (sxy * i2r) / c1;
             } else {
-                s1 = copysign(sqrt((rad - hd) / (2.0 * rad)), sxy);
-                c1 = sxy / (2.0 * s1 * rad);
+                s1 = copysign(sqrt((rad - hd) * i2r), sxy);
+                c1 = (sxy * i2r) / s1;
             }
             if (dir == 0) { lam = mean + rad; c = c1; sn = s1; }
             else { lam = mean - rad; c = -s1; sn = c1; }
         }
-        double f = (fabs(lam) <= 1e-30) ? 0.0 : (h * G.wdet[g]) * lam;
-        S.f[tl] = f;
+        S.f[tl] = (fabs(lam) <= 1e-30) ? 0.0 : (h * S.g.wdet[g]) * lam;
+#pragma unroll
         for (int r = 0; r < 8; ++r) {
-            int k = r >> 1, comp = r & 1;
-            double ux_dx = d1x * S.Am[0][r] + d2x * S.Am[2][r];
-            double ux_dy = d1y * S.Am[0][r] + d2y * S.Am[2][r];
-            double uy_dx = d1x * S.Am[1][r] + d2x * S.Am[3][r];
-            double uy_dy = d1y * S.Am[1][r] + d2y * S.Am[3][r];
-            if (comp == 0) { ux_dx += G.dNx[g][k]; ux_dy += G.dNy[g][k]; }
-            else { uy_dx += G.dNx[g][k]; uy_dy += G.dNy[g][k]; }
-            double gx = c * ux_dx + sn * ux_dy, gy = c * uy_dx + sn * uy_dy;
+            const int k = r >> 1;
+            double ux_dx = d1x * S.map[0][r] + d2x * S.map[2][r];
+            double ux_dy = d1y * S.map[0][r] + d2y * S.map[2][r];
+            double uy_dx = d1x * S.map[1][r] + d2x * S.map[3][r];
+            double uy_dy = d1y * S.map[1][r] + d2y * S.map[3][r];
+            if ((r & 1) == 0) { ux_dx += S.g.dNx[g][k]; ux_dy += S.g.dNy[g][k]; }
+            else { uy_dx += S.g.dNx[g][k]; uy_dy += S.g.dNy[g][k]; }
+            const double gx = c * ux_dx + sn * ux_dy, gy = c * uy_dx + sn * uy_dy;
             S.t[tl][r] = sn * gx - c * gy;
         }
-        for (int k = 0; k < 4; ++k) S.gz[tl][k] = c * G.dNx[g][k] + sn * G.dNy[g][k];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) S.gz[tl][k] = c * S.g.dNx[g][k] + sn * S.g.dNy[g][k];
     }
     __syncwarp();
+
+    // Phase 5: one node pair per lane; translations only (the rotation
+    // sub-blocks of a flat shell's KG are zero).
     if (valid) {
-        const int a = c_pair_a[tl], b = c_pair_b[tl];
+        int a, b;
+        q4_pair(tl, a, b);
         double M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-            double f = S.f[q];
-            double ta0 = S.t[q][2 * a], ta1 = S.t[q][2 * a + 1], tb0 = S.t[q][2 * b], tb1 = S.t[q][2 * b + 1];
-            M[0][0] += f * ta0 * tb0; M[0][1] += f * ta0 * tb1;
-            M[1][0] += f * ta1 * tb0; M[1][1] += f * ta1 * tb1;
-            M[2][2] += f * S.gz[q][a] * S.gz[q][b];
+            const double f = S.f[q];
+            const double ta0 = S.t[q][2 * a], ta1 = S.t[q][2 * a + 1], tb0 = S.t[q][2 * b], tb1 = S.t[q][2 * b + 1];
+            const double fa0 = f * ta0, fa1 = f * ta1;
+            M[0][0] += fa0 * tb0; M[0][1] += fa0 * tb1;
+            M[1][0] += fa1 * tb0; M[1][1] += fa1 * tb1;
+            M[2][2] += (f * S.gz[q][a]) * S.gz[q][b];
+        }
+        double Qa[9], Qb[9];
+        if (nodeR) {
+            double Ra[9], Rb[9];
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                Ra[i] = __ldg(nodeR + 9 * (int64_t)nd[a] + i);
+                Rb[i] = __ldg(nodeR + 9 * (int64_t)nd[b] + i);
+            }
+            node_block(V, V + 3, V + 6, Ra, Qa);
+            node_block(V, V + 3, V + 6, Rb, Qb);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 9; ++i) { Qa[i] = V[i]; Qb[i] = V[i]; }
         }
         double O[3][3];
-        rot_block(S.g.Q[a], M, S.g.Q[b], O);
+        rot_sparse<0b100011011>(Qa, M, Qb, O);
         const int32_t sl = __ldg(o.blk_slot + e * 10 + tl);
         const double Z[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
         double lmax = 0.0;
