@@ -790,12 +790,16 @@ __global__ void __launch_bounds__(Q4_THREADS) q4_kg_kernel(int64_t nq, const int
         double O[3][3];
         rot_sparse<0b100011011>(Qa, M, Qb, O);
         const int32_t sl = __ldg(o.blk_slot + e * 10 + tl);
-        const double Z[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
         double lmax = 0.0;
         write_sub_block(o, e, sl, a, b, 0, 0, O, lmax, 24);
-        write_sub_block(o, e, sl, a, b, 0, 1, Z, lmax, 24);
-        write_sub_block(o, e, sl, a, b, 1, 0, Z, lmax, 24);
-        write_sub_block(o, e, sl, a, b, 1, 1, Z, lmax, 24);
+        if (sl < 0) {
+            // the dof-level RBE2 path reads whole raw blocks; staged shell
+            // blocks of KG are read as their translation 3x3 only
+            const double Z[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            write_sub_block(o, e, sl, a, b, 0, 1, Z, lmax, 24);
+            write_sub_block(o, e, sl, a, b, 1, 0, Z, lmax, 24);
+            write_sub_block(o, e, sl, a, b, 1, 1, Z, lmax, 24);
+        }
     }
 }
 

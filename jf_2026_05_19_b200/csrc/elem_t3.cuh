@@ -433,10 +433,14 @@ __device__ __forceinline__ void t3_kg_pair(int64_t e, const int32_t *__restrict_
     double O[3][3];
     rot_block(Q[PA], L, Q[PB], O);
     const int32_t s = __ldg(o.blk_slot + e * 6 + packed_index(PA, PB, 3));
+    // staged blocks of KG shells are read as their translation 3x3 only; the
+    // dof-level RBE2 path (s < 0) reads whole raw blocks
 #pragma unroll
     for (int i = 0; i < 6; ++i)
 #pragma unroll
-        for (int j = 0; j < 6; ++j) *blk_entry(o, s, i, j) = (i < 3 && j < 3) ? O[i][j] : 0.0;
+        for (int j = 0; j < 6; ++j)
+            if (i < 3 && j < 3) *blk_entry(o, s, i, j) = O[i][j];
+            else if (s < 0) *blk_entry(o, s, i, j) = 0.0;
 }
 
 __global__ void __launch_bounds__(128) t3_kg_kernel(int64_t nt, const int32_t *__restrict__ nodes,

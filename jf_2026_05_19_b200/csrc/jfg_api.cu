@@ -69,6 +69,7 @@ struct jfg_model {
     int64_t n_blk = 0, n_blk_contrib = 0, n_upper = 0, nnz = 0;
     int32_t *d_blk_seg = nullptr;       // n_blk + 1 segment bounds (in blocks)
     int32_t *d_blk_A = nullptr, *d_blk_B = nullptr, *d_blk_offAB = nullptr, *d_blk_offBA = nullptr;
+    int32_t *d_blk_rot = nullptr;       // first bar slot of each block's segment (segment end if none)
     double *d_staging = nullptr;        // 36 doubles per regular element pair
     int64_t *d_rowptr = nullptr, *d_colind = nullptr;   // 0-based symmetric CSR == CSC
     // dof-level path for pairs that touch RBE2 nodes
@@ -418,6 +419,17 @@ __global__ void blk_slot_kernel(int64_t nbc, const int32_t *__restrict__ vals, i
     slot[pid] = (int32_t)q | (A > B ? jfg::kBlkTranspose : 0);
 }
 
+// First bar contribution of every block.  Contributions of a block sort in
+// element-pair order (shell pairs before bar pairs), so the bar slots of a
+// block are the tail [rot, seg end); only they carry rotation terms in KG.
+__global__ void blk_rot_kernel(int64_t nbc, const int32_t *__restrict__ vals, const int32_t *__restrict__ flags,
+                               const int32_t *__restrict__ pos, int64_t pair_bar, int32_t *rot) {
+    int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nbc || vals[q] < pair_bar) return;
+    if (!flags[q] && vals[q - 1] >= pair_bar) return;
+    rot[pos[q] + flags[q] - 1] = (int32_t)q;
+}
+
 __global__ void key_pos_kernel(int64_t n, const uint64_t *__restrict__ keys, int64_t ndof, const int64_t *__restrict__ rowptr,
                                const int64_t *__restrict__ colind, int64_t *pos, int32_t *err) {
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -455,6 +467,42 @@ __device__ __forceinline__ void block_row_sum(const double *__restrict__ staging
     }
 }
 
+// KG rows: shell contributions hold only their translation 3x3 (written by
+// the shell kernels; the rest of their slot is not read), bar contributions
+// [r, b) hold the full block.  Row i < 3 sums columns 0-2 over every slot and
+// columns 3-5 over the bar slots; row i >= 3 sums the bar slots only.  The
+// order of the nonzero terms is the slot order, as in block_row_sum.
+__device__ __forceinline__ void block_row_sum_kg(const double *__restrict__ staging, int32_t a, int32_t r, int32_t b, int i,
+                                                 double s[6]) {
+    if (i < 3) {
+        // batches of four slots, loads issued together; slots past the end
+        // add +0.0
+        for (int32_t q = a; q < b; q += 4) {
+            double2 x[4];
+            double z[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                x[u] = make_double2(0.0, 0.0);
+                z[u] = 0.0;
+                if (q + u < b) {
+                    const double *p = staging + 36 * (int64_t)(q + u) + 6 * i;
+                    x[u] = __ldg(reinterpret_cast<const double2 *>(p));
+                    z[u] = __ldg(p + 2);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) { s[0] += x[u].x; s[1] += x[u].y; s[2] += z[u]; }
+        }
+        for (int32_t q = r; q < b; ++q) {
+            const double *p = staging + 36 * (int64_t)q + 6 * i;
+            const double2 x2 = __ldg(reinterpret_cast<const double2 *>(p + 4));
+            s[3] += __ldg(p + 3); s[4] += x2.x; s[5] += x2.y;
+        }
+    } else {
+        block_row_sum(staging, r, b, i, s);
+    }
+}
+
 __device__ __forceinline__ void block_row_write(int64_t k, int i, const double s[6], const int32_t *__restrict__ A,
                                                 const int32_t *__restrict__ B, const int32_t *__restrict__ offAB,
                                                 const int32_t *__restrict__ offBA, const int64_t *__restrict__ rowptr,
@@ -470,7 +518,9 @@ __device__ __forceinline__ void block_row_write(int64_t k, int i, const double s
     }
 }
 
+template <bool KG>
 __global__ void __launch_bounds__(256) block_reduce_kernel(int64_t n_blk, const int32_t *__restrict__ seg,
+                                                           const int32_t *__restrict__ rot,
                                                            const double *__restrict__ staging, const int32_t *__restrict__ A,
                                                            const int32_t *__restrict__ B, const int32_t *__restrict__ offAB,
                                                            const int32_t *__restrict__ offBA, const int64_t *__restrict__ rowptr,
@@ -486,8 +536,14 @@ __global__ void __launch_bounds__(256) block_reduce_kernel(int64_t n_blk, const 
     const int32_t a0 = __ldg(seg + k0), b0 = __ldg(seg + k0 + 1);
     const int32_t a1 = two ? __ldg(seg + k1) : 0, b1 = two ? __ldg(seg + k1 + 1) : 0;
     double s0[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, s1[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    block_row_sum(staging, a0, b0, i, s0);
-    block_row_sum(staging, a1, b1, i, s1);
+    if (KG) {
+        const int32_t r0 = __ldg(rot + k0), r1 = two ? __ldg(rot + k1) : 0;
+        block_row_sum_kg(staging, a0, r0, b0, i, s0);
+        block_row_sum_kg(staging, a1, r1, b1, i, s1);
+    } else {
+        block_row_sum(staging, a0, b0, i, s0);
+        block_row_sum(staging, a1, b1, i, s1);
+    }
     block_row_write(k0, i, s0, A, B, offAB, offBA, rowptr, nz);
     if (two) block_row_write(k1, i, s1, A, B, offAB, offBA, rowptr, nz);
 }
@@ -961,6 +1017,7 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
     CK(dalloc(m, &m->d_blk_B, m->n_blk));
     CK(dalloc(m, &m->d_blk_offAB, m->n_blk));
     CK(dalloc(m, &m->d_blk_offBA, m->n_blk));
+    CK(dalloc(m, &m->d_blk_rot, m->n_blk));
     CK(dalloc(m, &m->d_blk_slot, NP));
     CK(cudaMemsetAsync(m->d_blk_slot, 0, sizeof(int32_t) * std::max<int64_t>(NP, 1), m->stream));
     int32_t *d_err = nullptr;
@@ -977,6 +1034,9 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
         CK(cudaGetLastError());
         blk_slot_kernel<<<(unsigned)cdiv(nbc, 256), 256, 0, m->stream>>>(nbc, d_bv2, m->pair_t3, m->pair_bar, m->d_q4n, m->d_t3n,
                                                                          m->d_barn, m->d_blk_slot);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(m->d_blk_rot, m->d_blk_seg + 1, sizeof(int32_t) * m->n_blk, cudaMemcpyDeviceToDevice, m->stream));
+        blk_rot_kernel<<<(unsigned)cdiv(nbc, 256), 256, 0, m->stream>>>(nbc, d_bv2, d_bflags, d_bpos, m->pair_bar, m->d_blk_rot);
         CK(cudaGetLastError());
     }
     // exception pairs: raw blocks, then dof-level weighted contributions
@@ -1264,7 +1324,7 @@ jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
     return JFG_OK;
 }
 
-jfg_status launch_reduce(jfg_model *m, const Batch &bt) {
+jfg_status launch_reduce(jfg_model *m, const Batch &bt, bool kg) {
     const unsigned nv = (unsigned)bt.n_var;
     if (m->n_xkey) {
         exc_chunk_kernel<<<dim3((unsigned)cdiv(m->n_xchunk * 32, 256), nv), 256, 0, m->stream>>>(
@@ -1275,10 +1335,17 @@ jfg_status launch_reduce(jfg_model *m, const Batch &bt) {
     }
     CK(cudaGetLastError());
     CK(mark(m, 4));
-    if (m->n_blk)
-        block_reduce_kernel<<<dim3((unsigned)cdiv((m->n_blk + 1) / 2 * 6, 256), nv), 256, 0, m->stream>>>(
-            m->n_blk, m->d_blk_seg, bt.staging, m->d_blk_A, m->d_blk_B, m->d_blk_offAB, m->d_blk_offBA, m->d_rowptr, bt.nz,
-            bt.staging_stride, m->nnz);
+    if (m->n_blk) {
+        const dim3 grid((unsigned)cdiv((m->n_blk + 1) / 2 * 6, 256), nv);
+        if (kg)
+            block_reduce_kernel<true><<<grid, 256, 0, m->stream>>>(
+                m->n_blk, m->d_blk_seg, m->d_blk_rot, bt.staging, m->d_blk_A, m->d_blk_B, m->d_blk_offAB, m->d_blk_offBA,
+                m->d_rowptr, bt.nz, bt.staging_stride, m->nnz);
+        else
+            block_reduce_kernel<false><<<grid, 256, 0, m->stream>>>(
+                m->n_blk, m->d_blk_seg, m->d_blk_rot, bt.staging, m->d_blk_A, m->d_blk_B, m->d_blk_offAB, m->d_blk_offBA,
+                m->d_rowptr, bt.nz, bt.staging_stride, m->nnz);
+    }
     CK(cudaGetLastError());
     CK(mark(m, 5));
     if (bt.ddiag)
@@ -1297,7 +1364,7 @@ jfg_status launch_k(jfg_model *m, const Batch &bt) {
     if (bt.dmax) CK(cudaMemsetAsync(bt.dmax, 0, sizeof(double) * bt.n_var, m->stream));
     st = launch_elements(m, false, bt);
     if (st) return st;
-    return launch_reduce(m, bt);
+    return launch_reduce(m, bt, false);
 }
 
 jfg_status launch_kg(jfg_model *m, const Batch &bt) {
@@ -1311,7 +1378,7 @@ jfg_status launch_kg(jfg_model *m, const Batch &bt) {
     b.ddiag = nullptr;
     st = launch_elements(m, true, b);
     if (st) return st;
-    return launch_reduce(m, b);
+    return launch_reduce(m, b, true);
 }
 
 jfg_status launch_k(jfg_model *m, double *nz, double *dmax, double *ddiag) {
