@@ -285,6 +285,97 @@ struct Ldl4 {
     }
 };
 
+// MacNeal residual-bending-flexibility scalars of one (virtual) quad with
+// corner coordinates lc and isotropic bending stiffness cb
+// (add_quad4_macneal_shear_rbf!, FEMKernels.jl:4803-4869: eps 0.04, zb 0.65,
+// flex 1/Cb11 = 1/Cb22): zs = (zxu + zxd, zxu - zxd, zyu + zyd, zyu - zyd).
+__device__ __forceinline__ void macneal_zs(const double lc[4][2], double cb, double zs[4]) {
+    const double Dx = 0.5 * (lc[1][0] + lc[2][0] - lc[0][0] - lc[3][0]);
+    const double Dy = 0.5 * (lc[2][1] + lc[3][1] - lc[0][1] - lc[1][1]);
+    const double Dx2 = Dx * Dx, Dy2 = Dy * Dy;
+    const double J11c = 0.25 * (-lc[0][0] + lc[1][0] + lc[2][0] - lc[3][0]);
+    const double J12c = 0.25 * (-lc[0][1] + lc[1][1] + lc[2][1] - lc[3][1]);
+    const double J21c = 0.25 * (-lc[0][0] - lc[1][0] + lc[2][0] + lc[3][0]);
+    const double J22c = 0.25 * (-lc[0][1] - lc[1][1] + lc[2][1] + lc[3][1]);
+    const double A_elem = 4.0 * fabs(J11c * J22c - J12c * J21c);
+    const double eps = 0.04;
+    const double ap = eps / (eps + (1.0 - eps) * Dx2 / fmax(Dy2, 1e-30));
+    const double bp = eps / (eps + (1.0 - eps) * Dy2 / fmax(Dx2, 1e-30));
+    const double flex = 1.0 / fmax(fabs(cb), 1e-30);
+    const double c12 = 0.65 * (1.0 / (12.0 * A_elem));
+    const double zxu = c12 * Dx2 * flex, zxd = c12 * ap * Dx2 * flex;
+    const double zyu = c12 * Dy2 * flex, zyd = c12 * bp * Dy2 * flex;
+    zs[0] = zxu + zxd; zs[1] = zxu - zxd; zs[2] = zyu + zyd; zs[3] = zyu - zyd;
+}
+
+// 1 / (sqrt(2 |det J|)^2 cs) at a strain-sampling point (V G V of the
+// reference with an isotropic shear matrix cs I, floored at 1e-30).
+__device__ __forceinline__ double macneal_ivd(double det, double cs) {
+    const double sq = sqrt(2.0 * fabs(det));
+    const double v = sq * sq * cs;
+    return 1.0 / (v < 1e-30 ? 1e-30 : v);
+}
+
+// Z = sym(inv(VGV) + Zb) is block diagonal with 2x2 blocks on the
+// xi-sampling rows (0, 1) and the eta-sampling rows (2, 3); W holds the two
+// inverse blocks (w00, w01, w11, w22, w23, w33).
+__device__ __forceinline__ void macneal_w(const double ivd[4], const double zs[4], double W[6]) {
+    const double zx00 = ivd[0] + zs[0], zx11 = ivd[1] + zs[0], zx01 = zs[1];
+    const double zy00 = ivd[2] + zs[2], zy11 = ivd[3] + zs[2], zy01 = zs[3];
+    const double ix = 1.0 / (zx00 * zx11 - zx01 * zx01), iy = 1.0 / (zy00 * zy11 - zy01 * zy01);
+    W[0] = zx11 * ix; W[1] = -zx01 * ix; W[2] = zx00 * ix;
+    W[3] = zy11 * iy; W[4] = -zy01 * iy; W[5] = zy00 * iy;
+}
+
+// MacNeal's shear term D_a' Z^-1 D_b of node pair (a, b) on (w, theta_x,
+// theta_y), added to P.  D's columns for node k: w -> (dN/dx at the
+// xi-sampling rows, dN/dy at the eta-sampling rows), theta_x -> -N on the
+// eta rows, theta_y -> N on the xi rows; the theta_x-theta_y coupling is zero.
+__device__ __forceinline__ void macneal_pair(const double (*Dd)[4], const double *W, int a, int b, double P[3][3]) {
+    const double pt = 0.57735026918962576451;
+    const double cxa0 = Dd[0][a], cxa1 = Dd[1][a], cya0 = Dd[2][a], cya1 = Dd[3][a];
+    const double cxb0 = Dd[0][b], cxb1 = Dd[1][b], cyb0 = Dd[2][b], cyb1 = Dd[3][b];
+    const double nxa0 = q4_N(a, 0.0, -pt), nxa1 = q4_N(a, 0.0, pt);
+    const double nya0 = -q4_N(a, -pt, 0.0), nya1 = -q4_N(a, pt, 0.0);
+    const double nxb0 = q4_N(b, 0.0, -pt), nxb1 = q4_N(b, 0.0, pt);
+    const double nyb0 = -q4_N(b, -pt, 0.0), nyb1 = -q4_N(b, pt, 0.0);
+    const double w0 = W[0], w1 = W[1], w2 = W[2], w3 = W[3], w4 = W[4], w5 = W[5];
+    const double yx0 = w0 * cxb0 + w1 * cxb1, yx1 = w1 * cxb0 + w2 * cxb1;
+    const double ynx0 = w0 * nxb0 + w1 * nxb1, ynx1 = w1 * nxb0 + w2 * nxb1;
+    const double yy0 = w3 * cyb0 + w4 * cyb1, yy1 = w4 * cyb0 + w5 * cyb1;
+    const double yny0 = w3 * nyb0 + w4 * nyb1, yny1 = w4 * nyb0 + w5 * nyb1;
+    P[0][0] += (cxa0 * yx0 + cxa1 * yx1) + (cya0 * yy0 + cya1 * yy1);
+    P[0][1] += cya0 * yny0 + cya1 * yny1;
+    P[0][2] += cxa0 * ynx0 + cxa1 * ynx1;
+    P[1][0] += nya0 * yy0 + nya1 * yy1;
+    P[1][1] += nya0 * yny0 + nya1 * yny1;
+    P[2][0] += nxa0 * yx0 + nxa1 * yx1;
+    P[2][2] += nxa0 * ynx0 + nxa1 * ynx1;
+}
+
+// Bending stiffness with the MacNeal twist row (0, -y, 2(-x) + xc) /
+// (x, 0, 2y - yc) for node pair (a, b) over the 2x2 Gauss points, isotropic
+// Cb = cb P(nu): the (theta_x, theta_y) 2x2 block added to P[1..2][1..2].
+__device__ __forceinline__ void bend_pair(const double (*dNx)[4], const double (*dNy)[4], const double *wdet, int a, int b,
+                                          double cb, double nu, double gam, double P[3][3]) {
+    double Pxx = 0, Pxy = 0, Pyx = 0, Pyy = 0, T00 = 0, T01 = 0, T10 = 0, T11 = 0;
+    const double xca = dNx[4][a], yca = dNy[4][a], xcb = dNx[4][b], ycb = dNy[4][b];
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+        const double wd = wdet[g];
+        const double xa = dNx[g][a], ya = dNy[g][a], xb = dNx[g][b], yb = dNy[g][b];
+        const double t0a = 2.0 * (-xa) - (-xca), t1a = 2.0 * ya - yca;
+        const double t0b = 2.0 * (-xb) - (-xcb), t1b = 2.0 * yb - ycb;
+        const double wx = wd * xa, wy = wd * ya, w0 = wd * t0a, w1 = wd * t1a;
+        Pxx += wx * xb; Pxy += wx * yb; Pyx += wy * xb; Pyy += wy * yb;
+        T00 += w0 * t0b; T01 += w0 * t1b; T10 += w1 * t0b; T11 += w1 * t1b;
+    }
+    P[1][1] += cb * (Pyy + gam * T00);
+    P[1][2] += cb * (gam * T01 - nu * Pyx);
+    P[2][1] += cb * (gam * T10 - nu * Pxy);
+    P[2][2] += cb * (Pxx + gam * T11);
+}
+
 __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const int32_t *__restrict__ nodes,
                                                          const double *__restrict__ prop,
                                                          const double *__restrict__ coords,
@@ -351,29 +442,10 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
             const int l = tl - 5;
 #pragma unroll
             for (int k = 0; k < 4; ++k) S.Dd[l][k] = l < 2 ? dx[k] : dy[k];
-            const double sq = sqrt(2.0 * fabs(det));
-            const double v = sq * sq * cs;
-            S.ivd[l] = 1.0 / (v < 1e-30 ? 1e-30 : v);
+            S.ivd[l] = macneal_ivd(det, cs);
         }
     } else if (valid && tl == 9) {
-        // residual bending flexibility (add_quad4_macneal_shear_rbf!,
-        // FEMKernels.jl:4803-4869: eps 0.04, zb 0.65, flex 1/Cb11, 1/Cb22)
-        const double Dx = 0.5 * (lc[1][0] + lc[2][0] - lc[0][0] - lc[3][0]);
-        const double Dy = 0.5 * (lc[2][1] + lc[3][1] - lc[0][1] - lc[1][1]);
-        const double Dx2 = Dx * Dx, Dy2 = Dy * Dy;
-        const double J11c = 0.25 * (-lc[0][0] + lc[1][0] + lc[2][0] - lc[3][0]);
-        const double J12c = 0.25 * (-lc[0][1] + lc[1][1] + lc[2][1] - lc[3][1]);
-        const double J21c = 0.25 * (-lc[0][0] - lc[1][0] + lc[2][0] + lc[3][0]);
-        const double J22c = 0.25 * (-lc[0][1] - lc[1][1] + lc[2][1] + lc[3][1]);
-        const double A_elem = 4.0 * fabs(J11c * J22c - J12c * J21c);
-        const double eps = 0.04;
-        const double ap = eps / (eps + (1.0 - eps) * Dx2 / fmax(Dy2, 1e-30));
-        const double bp = eps / (eps + (1.0 - eps) * Dy2 / fmax(Dx2, 1e-30));
-        const double flex = 1.0 / fmax(fabs(cb), 1e-30);
-        const double c12 = 0.65 * (1.0 / (12.0 * A_elem));
-        const double zxu = c12 * Dx2 * flex, zxd = c12 * ap * Dx2 * flex;
-        const double zyu = c12 * Dy2 * flex, zyd = c12 * bp * Dy2 * flex;
-        zs[0] = zxu + zxd; zs[1] = zxu - zxd; zs[2] = zyu + zyd; zs[3] = zyu - zyd;
+        macneal_zs(lc, cb, zs);
     }
     __syncwarp();
 
@@ -425,13 +497,7 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
 #pragma unroll
         for (int i = 0; i < 10; ++i) S.B[i] = Bs[i];
     } else if (valid && tl == 9 && !skip_mac) {
-        // Z = sym(inv(VGV) + Zb) is block diagonal with 2x2 blocks on the
-        // xi-sampling rows (0, 1) and the eta-sampling rows (2, 3)
-        const double zx00 = S.ivd[0] + zs[0], zx11 = S.ivd[1] + zs[0], zx01 = zs[1];
-        const double zy00 = S.ivd[2] + zs[2], zy11 = S.ivd[3] + zs[2], zy01 = zs[3];
-        const double ix = 1.0 / (zx00 * zx11 - zx01 * zx01), iy = 1.0 / (zy00 * zy11 - zy01 * zy01);
-        S.W[0] = zx11 * ix; S.W[1] = -zx01 * ix; S.W[2] = zx00 * ix;
-        S.W[3] = zy11 * iy; S.W[4] = -zy01 * iy; S.W[5] = zy00 * iy;
+        macneal_w(S.ivd, zs, S.W);
     }
     __syncwarp();
 
@@ -502,28 +568,7 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
         Lp[1][2] = cb * (gam * T01 - nu * Pyx) - cb * cbb[0][1];
         Lp[2][1] = cb * (gam * T10 - nu * Pxy) - cb * cbb[1][0];
         Lp[2][2] = cb * (Pxx + gam * T11) - cb * cbb[1][1];
-        if (!skip_mac) {
-            const double pt = 0.57735026918962576451;
-            // sampling-row parts of the w, theta_x, theta_y columns of D
-            const double cxa0 = S.Dd[0][a], cxa1 = S.Dd[1][a], cya0 = S.Dd[2][a], cya1 = S.Dd[3][a];
-            const double cxb0 = S.Dd[0][b], cxb1 = S.Dd[1][b], cyb0 = S.Dd[2][b], cyb1 = S.Dd[3][b];
-            const double nxa0 = q4_N(a, 0.0, -pt), nxa1 = q4_N(a, 0.0, pt);
-            const double nya0 = -q4_N(a, -pt, 0.0), nya1 = -q4_N(a, pt, 0.0);
-            const double nxb0 = q4_N(b, 0.0, -pt), nxb1 = q4_N(b, 0.0, pt);
-            const double nyb0 = -q4_N(b, -pt, 0.0), nyb1 = -q4_N(b, pt, 0.0);
-            const double w0 = S.W[0], w1 = S.W[1], w2 = S.W[2], w3 = S.W[3], w4 = S.W[4], w5 = S.W[5];
-            const double yx0 = w0 * cxb0 + w1 * cxb1, yx1 = w1 * cxb0 + w2 * cxb1;
-            const double ynx0 = w0 * nxb0 + w1 * nxb1, ynx1 = w1 * nxb0 + w2 * nxb1;
-            const double yy0 = w3 * cyb0 + w4 * cyb1, yy1 = w4 * cyb0 + w5 * cyb1;
-            const double yny0 = w3 * nyb0 + w4 * nyb1, yny1 = w4 * nyb0 + w5 * nyb1;
-            Lp[0][0] = (cxa0 * yx0 + cxa1 * yx1) + (cya0 * yy0 + cya1 * yy1);
-            Lp[0][1] = cya0 * yny0 + cya1 * yny1;
-            Lp[0][2] = cxa0 * ynx0 + cxa1 * ynx1;
-            Lp[1][0] = nya0 * yy0 + nya1 * yy1;
-            Lp[1][1] += nya0 * yny0 + nya1 * yny1;
-            Lp[2][0] = nxa0 * yx0 + nxa1 * yx1;
-            Lp[2][2] += nxa0 * ynx0 + nxa1 * ynx1;
-        }
+        if (!skip_mac) macneal_pair(S.Dd, S.W, a, b, Lp);
         double Qa[9], Qb[9];
         if (nodeR) {
             double Ra[9], Rb[9];

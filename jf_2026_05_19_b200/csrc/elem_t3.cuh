@@ -42,26 +42,35 @@ __host__ __device__ constexpr int t3_quad_node(int q, int k) {
 __constant__ int c_t3_quads[3][4] = {{0, 3, 6, 5}, {1, 4, 6, 3}, {2, 5, 6, 4}};
 
 struct T3KShared {
-    double p[3][3];
-    double v[3][3];
-    double Q[3][9];
-    double pts[7][2];
-    double bv[3], cv[3], A;
-    double Cm[9], Cb[9], cs, alpha_d;
-    int nd[3], plate, skip_macneal;
+    double V[9];
+    double bv[3], cv[3], A, cm, ad;
+    int nd[3];
     union {
-        struct {  // virtual-quad data (phases 2-4)
+        struct {  // virtual-quad data (phases 1-3): Gauss points 0-3, centre 4
             double dNx[3][5][4], dNy[3][5][4], wdet[3][4];
-            double D[3][4][12], Jp[3][4];
-            MacNealZ mz[3];
+            double Dd[3][4][4], ivd[3][4], zs[3][4], W[3][6];
         } q;
-        struct {  // condensation (phases 5-7)
+        struct {  // condensation (phases 4-6)
             double X[12][9];
             double Kc[9][9];
         } c;
     } u;
     double Pb[3][10][9];  // quad q, local node pair (a <= b): 3x3 over (w, theta_x, theta_y)
 };
+
+// Corner coordinates of virtual quad q (corner q, midpoint to the next
+// corner, centroid, midpoint from the previous corner), as the macro points
+// (x_i + x_j) / 2 and (x_0 + x_1 + x_2) / 3 of tria3_plate_macro_data.
+__device__ __forceinline__ void t3_quad_coords(int q, const double x[3], const double y[3], double lq[4][2]) {
+    const int n = q == 2 ? 0 : q + 1, pv = q == 0 ? 2 : q - 1;
+    const double xc = q == 0 ? x[0] : (q == 1 ? x[1] : x[2]), yc = q == 0 ? y[0] : (q == 1 ? y[1] : y[2]);
+    const double xn = n == 0 ? x[0] : (n == 1 ? x[1] : x[2]), yn = n == 0 ? y[0] : (n == 1 ? y[1] : y[2]);
+    const double xp = pv == 0 ? x[0] : (pv == 1 ? x[1] : x[2]), yp = pv == 0 ? y[0] : (pv == 1 ? y[1] : y[2]);
+    lq[0][0] = xc; lq[0][1] = yc;
+    lq[1][0] = (xc + xn) / 2; lq[1][1] = (yc + yn) / 2;
+    lq[2][0] = (x[0] + x[1] + x[2]) / 3; lq[2][1] = (y[0] + y[1] + y[2]) / 3;
+    lq[3][0] = (xp + xc) / 2; lq[3][1] = (yp + yc) / 2;
+}
 
 __global__ void __launch_bounds__(T3_THREADS, 5) t3_k_kernel(int64_t nt, const int32_t *__restrict__ nodes,
                                                          const double *__restrict__ prop,
@@ -76,182 +85,97 @@ __global__ void __launch_bounds__(T3_THREADS, 5) t3_k_kernel(int64_t nt, const i
     if (e >= nt) return;  // the whole team leaves; syncs below are team-local
     T3KShared &S = sh[warp * T3_TEAMS_PER_WARP + team];
 
-    // Phase 0: connectivity and coordinates; the property record is loaded
-    // now so that its latency overlaps the coordinate loads.
-    double h = 0.0, E = 0.0, nu = 0.0, br = 0.0, tst = 0.0, Gs = 0.0;
-    if (tl == 0) {
+    // Phase 0, every lane in registers: nodes, corners, properties, frame,
+    // local coordinates, CST derivatives, constitutive scalars.
+    double x[3], y[3], A, cb, cs, nu, gam;
+    bool plate, macneal;
+    {
         const double *pr = prop + 7 * e;
-        h = o.thickness(e, pr); E = __ldg(pr + 1); nu = __ldg(pr + 2); br = __ldg(pr + 4); tst = __ldg(pr + 5);
-        Gs = __ldg(pr + 6);
-    }
-    if (tl < 3) {
-        const int32_t n = __ldg(nodes + 3 * e + tl);
-        S.nd[tl] = n;
-        for (int i = 0; i < 3; ++i) S.p[tl][i] = __ldg(coords + 3 * (int64_t)n + i);
-    }
-    __syncwarp(tm);
-    // Phase 1: frame, macro points, constitutive data (one lane).
-    if (tl == 0) {
+        const double h = o.thickness(e, pr), E = __ldg(pr + 1), br = __ldg(pr + 4), tst = __ldg(pr + 5), Gs = __ldg(pr + 6);
+        nu = __ldg(pr + 2);
+        int nd[3];
+        double p[3][3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            nd[k] = __ldg(nodes + 3 * e + k);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) p[k][i] = __ldg(coords + 3 * (int64_t)nd[k] + i);
+        }
         double v1[3], v2[3], v3[3];
-        t3_frame(S.p[0], S.p[1], S.p[2], v1, v2, v3);
-        double c[3], lc[3][2];
-        for (int i = 0; i < 3; ++i) c[i] = (S.p[0][i] + S.p[1][i] + S.p[2][i]) / 3.0;
+        t3_frame(p[0], p[1], p[2], v1, v2, v3);
+        double c[3];
+        for (int i = 0; i < 3; ++i) c[i] = (p[0][i] + p[1][i] + p[2][i]) / 3.0;
+#pragma unroll
         for (int k = 0; k < 3; ++k) {
             double d[3];
-            sub3(S.p[k], c, d);
-            lc[k][0] = dot3(d, v1);
-            lc[k][1] = dot3(d, v2);
+            sub3(p[k], c, d);
+            x[k] = dot3(d, v1);
+            y[k] = dot3(d, v2);
         }
-        for (int i = 0; i < 3; ++i) { S.v[0][i] = v1[i]; S.v[1][i] = v2[i]; S.v[2][i] = v3[i]; }
-        double x[3] = {lc[0][0], lc[1][0], lc[2][0]}, y[3] = {lc[0][1], lc[1][1], lc[2][1]};
-        double A2 = x[0] * (y[1] - y[2]) + x[1] * (y[2] - y[0]) + x[2] * (y[0] - y[1]);
-        double A = 0.5 * fabs(A2);
-        S.A = A;
-        S.bv[0] = (y[1] - y[2]) / (2 * A); S.bv[1] = (y[2] - y[0]) / (2 * A); S.bv[2] = (y[0] - y[1]) / (2 * A);
-        S.cv[0] = (x[2] - x[1]) / (2 * A); S.cv[1] = (x[0] - x[2]) / (2 * A); S.cv[2] = (x[1] - x[0]) / (2 * A);
-        for (int i = 0; i < 3; ++i) { S.pts[i][0] = x[i]; S.pts[i][1] = y[i]; }
-        S.pts[3][0] = (x[0] + x[1]) / 2; S.pts[3][1] = (y[0] + y[1]) / 2;
-        S.pts[4][0] = (x[1] + x[2]) / 2; S.pts[4][1] = (y[1] + y[2]) / 2;
-        S.pts[5][0] = (x[2] + x[0]) / 2; S.pts[5][1] = (y[2] + y[0]) / 2;
-        S.pts[6][0] = (x[0] + x[1] + x[2]) / 3; S.pts[6][1] = (y[0] + y[1] + y[2]) / 3;
-        double cm = E * h / (1 - nu * nu);
-        double cb = br * (E * h * h * h) / (12 * (1 - nu * nu));
-        double base[9] = {1.0, nu, 0.0, nu, 1.0, 0.0, 0.0, 0.0, (1 - nu) / 2};
-        for (int i = 0; i < 9; ++i) { S.Cm[i] = cm * base[i]; S.Cb[i] = cb * base[i]; }
-        bool membrane_only = br <= 1e-12;
-        double cs = membrane_only ? 0.0 : tst * h * Gs;
-        S.cs = cs;
-        S.plate = (!membrane_only && A >= 1e-12) ? 1 : 0;
-        S.skip_macneal = (h < 1e-30 || fabs(cs) < 1e-30) ? 1 : 0;
-        double k6 = membrane_only ? 0.0 : k6rot;
-        S.alpha_d = (k6 / 1e5) * Gs * h;  // G_ref = shear-material G (assembly.jl:2468)
-    }
-    __syncwarp(tm);
-    const bool plate = S.plate != 0, macneal = plate && !S.skip_macneal;
-
-    // Phase 2: node blocks (items 0-2), virtual-quad Jacobians (3-17) and
-    // MacNeal strain-sampling rows (18-29), two items per lane.
-    for (int it = tl; it < 30; it += T3_TEAM) {
-        if (it < 3) {
-            const double *R = nodeR ? nodeR + 9 * (int64_t)S.nd[it] : nullptr;
-            double Rl[9];
-            if (R)
-                for (int i = 0; i < 9; ++i) Rl[i] = __ldg(R + i);
-            node_block(S.v[0], S.v[1], S.v[2], R ? Rl : nullptr, S.Q[it]);
-        } else if (!plate) {
-        } else if (it < 18) {
-            int q = (it - 3) / 5, g = (it - 3) % 5;
-            double lq[4][2];
-            for (int k = 0; k < 4; ++k) { lq[k][0] = S.pts[c_t3_quads[q][k]][0]; lq[k][1] = S.pts[c_t3_quads[q][k]][1]; }
-            double r = 0.0, s = 0.0;
-            if (g < 4) q4_shape_gp(g, r, s);
-            double dNr[4] = {-0.25 * (1 - s), 0.25 * (1 - s), 0.25 * (1 + s), -0.25 * (1 + s)};
-            double dNs[4] = {-0.25 * (1 - r), -0.25 * (1 + r), 0.25 * (1 + r), 0.25 * (1 - r)};
-            double J11 = 0, J12 = 0, J21 = 0, J22 = 0;
-            for (int k = 0; k < 4; ++k) {
-                J11 += dNr[k] * lq[k][0]; J12 += dNr[k] * lq[k][1];
-                J21 += dNs[k] * lq[k][0]; J22 += dNs[k] * lq[k][1];
-            }
-            double det = J11 * J22 - J12 * J21;
-            double inv = 1.0 / det;
-            double iJ11 = J22 * inv, iJ12 = -J12 * inv, iJ21 = -J21 * inv, iJ22 = J11 * inv;
-            for (int k = 0; k < 4; ++k) {
-                S.u.q.dNx[q][g][k] = iJ11 * dNr[k] + iJ12 * dNs[k];
-                S.u.q.dNy[q][g][k] = iJ21 * dNr[k] + iJ22 * dNs[k];
-            }
-            if (g < 4) { double a = fabs(det); S.u.q.wdet[q][g] = a < 1e-12 ? 1e-12 : a; }
-        } else {
-            int q = (it - 18) >> 2, sp = (it - 18) & 3;
-            double lq[4][2];
-            for (int k = 0; k < 4; ++k) { lq[k][0] = S.pts[c_t3_quads[q][k]][0]; lq[k][1] = S.pts[c_t3_quads[q][k]][1]; }
-            const double pt = 0.57735026918962576451;
-            double xi = sp < 2 ? 0.0 : (sp == 2 ? -pt : pt), eta = sp >= 2 ? 0.0 : (sp == 0 ? -pt : pt);
-            double dNr[4] = {-0.25 * (1 - eta), 0.25 * (1 - eta), 0.25 * (1 + eta), -0.25 * (1 + eta)};
-            double dNs[4] = {-0.25 * (1 - xi), -0.25 * (1 + xi), 0.25 * (1 + xi), 0.25 * (1 - xi)};
-            double J11 = 0, J12 = 0, J21 = 0, J22 = 0;
-            for (int k = 0; k < 4; ++k) {
-                J11 += dNr[k] * lq[k][0]; J12 += dNr[k] * lq[k][1];
-                J21 += dNs[k] * lq[k][0]; J22 += dNs[k] * lq[k][1];
-            }
-            double det = J11 * J22 - J12 * J21;
-            if (fabs(det) < 1e-14) det = det < 0.0 ? -1e-14 : 1e-14;
-            S.u.q.Jp[q][sp] = fabs(det);
-            double inv = 1.0 / det;
-            double iJ11 = J22 * inv, iJ12 = -J12 * inv, iJ21 = -J21 * inv, iJ22 = J11 * inv;
-            for (int k = 0; k < 4; ++k) {
-                double dx = iJ11 * dNr[k] + iJ12 * dNs[k], dy = iJ21 * dNr[k] + iJ22 * dNs[k];
-                double Nk = 0.25 * (1 + ((k == 1 || k == 2) ? xi : -xi)) * (1 + (k >= 2 ? eta : -eta));
-                double *Dr = S.u.q.D[q][sp] + 3 * k;
-                if (sp < 2) { Dr[0] = dx; Dr[1] = 0.0; Dr[2] = Nk; }
-                else { Dr[0] = dy; Dr[1] = -Nk; Dr[2] = 0.0; }
-            }
+        A = 0.5 * fabs(x[0] * (y[1] - y[2]) + x[1] * (y[2] - y[0]) + x[2] * (y[0] - y[1]));
+        gam = (1 - nu) / 2;
+        const double cm = E * h / (1 - nu * nu);
+        cb = br * (E * h * h * h) / (12 * (1 - nu * nu));
+        const bool membrane_only = br <= 1e-12;
+        cs = membrane_only ? 0.0 : tst * h * Gs;
+        plate = !membrane_only && A >= 1e-12;
+        macneal = plate && !(h < 1e-30 || fabs(cs) < 1e-30);
+        if (tl == 0) {
+            for (int i = 0; i < 3; ++i) { S.V[i] = v1[i]; S.V[3 + i] = v2[i]; S.V[6 + i] = v3[i]; S.nd[i] = nd[i]; }
+            const double i2A = 1.0 / (2 * A);
+            S.bv[0] = (y[1] - y[2]) * i2A; S.bv[1] = (y[2] - y[0]) * i2A; S.bv[2] = (y[0] - y[1]) * i2A;
+            S.cv[0] = (x[2] - x[1]) * i2A; S.cv[1] = (x[0] - x[2]) * i2A; S.cv[2] = (x[1] - x[0]) * i2A;
+            S.A = A;
+            S.cm = cm;
+            // G_ref = shear-material G (assembly.jl:2468)
+            S.ad = ((membrane_only ? 0.0 : k6rot) / 1e5) * Gs * h;
         }
     }
-    __syncwarp(tm);
-    // Phase 3: MacNeal compliance factors per virtual quad.
-    if (macneal && tl < 3) {
-        double lq[4][2];
-        for (int k = 0; k < 4; ++k) { lq[k][0] = S.pts[c_t3_quads[tl][k]][0]; lq[k][1] = S.pts[c_t3_quads[tl][k]][1]; }
-        S.u.q.mz[tl] = macneal_z(lq, S.u.q.Jp[tl], S.cs, S.Cb[0], S.Cb[4]);
-    }
-    __syncwarp(tm);
 
     if (plate) {
-        // Phase 4: plate 3x3 block of every (virtual quad, node pair).
+        // Phase 1: virtual-quad points (27 items: quad q = it / 9, point
+        // it % 9 -- Gauss points, centre, MacNeal sampling points) and the
+        // MacNeal scalars of each quad (items 27-29).
+        for (int it = tl; it < 30; it += T3_TEAM) {
+            const int q = it < 27 ? it / 9 : it - 27, pt = it - 9 * (it / 9);
+            double lq[4][2];
+            t3_quad_coords(q, x, y, lq);
+            if (it < 27) {
+                double r, s, dx[4], dy[4], iJ[4];
+                q4_point_rs(pt, r, s);
+                const bool mac = pt >= 5;
+                const double det = q4_point_derivs(lq, r, s, mac, dx, dy, iJ);
+                if (!mac) {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) { S.u.q.dNx[q][pt][k] = dx[k]; S.u.q.dNy[q][pt][k] = dy[k]; }
+                    if (pt < 4) { const double a = fabs(det); S.u.q.wdet[q][pt] = a < 1e-12 ? 1e-12 : a; }
+                } else {
+                    const int l = pt - 5;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) S.u.q.Dd[q][l][k] = l < 2 ? dx[k] : dy[k];
+                    S.u.q.ivd[q][l] = macneal_ivd(det, cs);
+                }
+            } else {
+                double zs[4];
+                macneal_zs(lq, cb, zs);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) S.u.q.zs[q][i] = zs[i];
+            }
+        }
+        __syncwarp(tm);
+        if (macneal && tl < 3) macneal_w(S.u.q.ivd[tl], S.u.q.zs[tl], S.u.q.W[tl]);
+        __syncwarp(tm);
+
+        // Phase 2: plate 3x3 block of every (virtual quad, node pair):
+        // bending with the twist row (no bending incompatible modes in the
+        // macro quads) plus MacNeal's shear.
         for (int it = tl; it < 30; it += T3_TEAM) {
             const int q = it / 10, pp = it - 10 * q;
-            const int ka = c_pair_a[pp], kb = c_pair_b[pp];
+            int ka, kb;
+            q4_pair(pp, ka, kb);
             double v[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-            const double xca = S.u.q.dNx[q][4][ka], yca = S.u.q.dNy[q][4][ka];
-            const double xcb = S.u.q.dNx[q][4][kb], ycb = S.u.q.dNy[q][4][kb];
-#pragma unroll
-            for (int g = 0; g < 4; ++g) {
-                const double xa = S.u.q.dNx[q][g][ka], ya = S.u.q.dNy[q][g][ka];
-                const double xb = S.u.q.dNx[q][g][kb], yb = S.u.q.dNy[q][g][kb];
-                const double wd = S.u.q.wdet[q][g];
-                // bending columns (theta_x, theta_y) with the twist correction
-                const double ac[2][3] = {{0.0, -ya, 2.0 * (-xa) - (-xca)}, {xa, 0.0, 2.0 * ya - yca}};
-                const double bc[2][3] = {{0.0, -yb, 2.0 * (-xb) - (-xcb)}, {xb, 0.0, 2.0 * yb - ycb}};
-#pragma unroll
-                for (int cj = 0; cj < 2; ++cj) {
-                    double cbb[3];
-#pragma unroll
-                    for (int r = 0; r < 3; ++r)
-                        cbb[r] = S.Cb[3 * r] * bc[cj][0] + S.Cb[3 * r + 1] * bc[cj][1] + S.Cb[3 * r + 2] * bc[cj][2];
-#pragma unroll
-                    for (int ci = 0; ci < 2; ++ci)
-                        v[1 + ci][1 + cj] += wd * (ac[ci][0] * cbb[0] + ac[ci][1] * cbb[1] + ac[ci][2] * cbb[2]);
-                }
-            }
-            if (macneal) {
-                double Da[4][3], Db[4][3], Ya[4][3], Yb[4][3];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    double d[4], y[4];
-#pragma unroll
-                    for (int l = 0; l < 4; ++l) d[l] = Da[l][c] = S.u.q.D[q][l][3 * ka + c];
-                    macneal_y(S.u.q.mz[q], d, y);
-#pragma unroll
-                    for (int l = 0; l < 4; ++l) Ya[l][c] = y[l];
-#pragma unroll
-                    for (int l = 0; l < 4; ++l) d[l] = Db[l][c] = S.u.q.D[q][l][3 * kb + c];
-                    macneal_y(S.u.q.mz[q], d, y);
-#pragma unroll
-                    for (int l = 0; l < 4; ++l) Yb[l][c] = y[l];
-                }
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) {
-                        double s1 = 0.0, s2 = 0.0;
-#pragma unroll
-                        for (int l = 0; l < 4; ++l) {
-                            s1 += Da[l][i] * Yb[l][j];
-                            s2 += Db[l][j] * Ya[l][i];
-                        }
-                        v[i][j] += 0.5 * (s1 + s2);
-                    }
-            }
+            bend_pair(S.u.q.dNx[q], S.u.q.dNy[q], S.u.q.wdet[q], ka, kb, cb, nu, gam, v);
+            if (macneal) macneal_pair(S.u.q.Dd[q], S.u.q.W[q], ka, kb, v);
 #pragma unroll
             for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -259,7 +183,7 @@ __global__ void __launch_bounds__(T3_THREADS, 5) t3_k_kernel(int64_t nt, const i
         }
         __syncwarp(tm);
 
-        // Phase 5: lane r < 12 holds row r of [Kii | Kie] (internal dof r =
+        // Phase 3: lane r < 12 holds row r of [Kii | Kie] (internal dof r =
         // macro node 3 + r/3, component r%3), summed over quads in order.
         const bool act = tl < 12;
         const int nA = 3 + tl / 3, ci = tl - 3 * (tl / 3);
@@ -319,7 +243,7 @@ __global__ void __launch_bounds__(T3_THREADS, 5) t3_k_kernel(int64_t nt, const i
             for (int c = 0; c < 9; ++c) S.u.c.X[pos][c] = row[12 + c] / diag;
         __syncwarp(tm);
 
-        // Phase 6: Kcond = Kee - Kei X (Kee, Kei from the corner's own quad).
+        // Phase 4: Kcond = Kee - Kei X (Kee, Kei from the corner's own quad).
         for (int it = tl; it < 81; it += T3_TEAM) {
             const int r = it / 9, col = it - 9 * r;
             const int c = r / 3, i = r - 3 * c, c2 = col / 3, j = col - 3 * c2;
@@ -332,39 +256,63 @@ __global__ void __launch_bounds__(T3_THREADS, 5) t3_k_kernel(int64_t nt, const i
             }
             S.u.c.Kc[r][col] = kee - s;
         }
-        __syncwarp(tm);
     }
+    __syncwarp(tm);
 
-    // Phase 7: node-pair sub-blocks: item -> (pair 0..5, sub-block tt, tr, rt, rr)
+    // Phase 5: lane tl < 12 takes node pair tl / 2 and sub-block row bi =
+    // tl % 2 (translations, rotations) for both sub-block columns.  Local
+    // block: CST membrane and centroidal drill on (u, v, theta_z), condensed
+    // plate on (w, theta_x, theta_y).
     double lmax = 0.0;
-    const bool degenerate = S.A < 1e-12;
-    for (int it = tl; it < 24; it += T3_TEAM) {
-        const int pr_a[6] = {0, 0, 0, 1, 1, 2}, pr_b[6] = {0, 1, 2, 1, 2, 2};
-        const int pair = it >> 2, sub = it & 3;
-        const int a = pr_a[pair], b = pr_b[pair];
-        const int bi = sub >> 1, bj = sub & 1;
-        double L[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-        if (!degenerate) {
-            const double A = S.A;
-            // membrane CST (u, v) and drill (u, v, theta_z) terms
-            double Bd_a[6] = {0.5 * S.cv[a], -0.5 * S.bv[a], 0, 0, 0, 1.0 / 3.0};
-            double Bd_b[6] = {0.5 * S.cv[b], -0.5 * S.bv[b], 0, 0, 0, 1.0 / 3.0};
-            double ma[2][3] = {{S.bv[a], 0.0, S.cv[a]}, {0.0, S.cv[a], S.bv[a]}};
-            double mb[2][3] = {{S.bv[b], 0.0, S.cv[b]}, {0.0, S.cv[b], S.bv[b]}};
+    if (tl < 12) {
+        const int pair = tl >> 1, bi = tl & 1;
+        const int a = (pair >= 3) + (pair >= 5);
+        const int b = a + pair - (a == 0 ? 0 : (a == 1 ? 3 : 5));
+        double Lm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, Lp[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        if (A >= 1e-12) {
+            const double ba = S.bv[a], ca = S.cv[a], bb = S.bv[b], cb_ = S.cv[b], cm = S.cm, ad = S.ad;
+            const double da[3] = {0.5 * ca, -0.5 * ba, 1.0 / 3.0}, db[3] = {0.5 * cb_, -0.5 * bb, 1.0 / 3.0};
+#pragma unroll
             for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j) {
-                    int gi = 3 * bi + i, gj = 3 * bj + j;  // local dof index 0..5
-                    double v = S.alpha_d * (Bd_a[gi] * Bd_b[gj]) * A;
-                    if (gi < 2 && gj < 2) v += quad_form(ma[gi], S.Cm, mb[gj]) * A;
-                    // plate (w, theta_x, theta_y) = local 2, 3, 4
-                    if (plate && gi >= 2 && gi <= 4 && gj >= 2 && gj <= 4) v += S.u.c.Kc[3 * a + gi - 2][3 * b + gj - 2];
-                    L[i][j] = v;
-                }
+#pragma unroll
+                for (int j = 0; j < 3; ++j) Lm[i][j] = ad * (da[i] * db[j]) * A;
+            Lm[0][0] += (cm * (ba * bb + gam * (ca * cb_))) * A;
+            Lm[0][1] += (cm * (nu * (ba * cb_) + gam * (ca * bb))) * A;
+            Lm[1][0] += (cm * (nu * (ca * bb) + gam * (ba * cb_))) * A;
+            Lm[1][1] += (cm * (ca * cb_ + gam * (ba * bb))) * A;
+            if (plate)
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) Lp[i][j] = S.u.c.Kc[3 * a + i][3 * b + j];
         }
-        double O[3][3];
-        rot_block(S.Q[a], L, S.Q[b], O);
+        double Qa[9], Qb[9];
+        if (nodeR) {
+            double Ra[9], Rb[9];
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                Ra[i] = __ldg(nodeR + 9 * (int64_t)S.nd[a] + i);
+                Rb[i] = __ldg(nodeR + 9 * (int64_t)S.nd[b] + i);
+            }
+            node_block(S.V, S.V + 3, S.V + 6, Ra, Qa);
+            node_block(S.V, S.V + 3, S.V + 6, Rb, Qb);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 9; ++i) { Qa[i] = S.V[i]; Qb[i] = S.V[i]; }
+        }
         const int32_t sl = __ldg(o.blk_slot + e * 6 + pair);
-        write_sub_block(o, e, sl, a, b, bi, bj, O, lmax, 18);
+        double M[3][3], O[3][3];
+        // diagonal sub-block: (u, v, w) x (u, v, w) or (rx, ry, rz) x (rx, ry, rz)
+        M[0][0] = bi ? Lp[1][1] : Lm[0][0]; M[0][1] = bi ? Lp[1][2] : Lm[0][1];
+        M[1][0] = bi ? Lp[2][1] : Lm[1][0]; M[1][1] = bi ? Lp[2][2] : Lm[1][1];
+        M[2][2] = bi ? Lm[2][2] : Lp[0][0];
+        rot_sparse<0b100011011>(Qa, M, Qb, O);
+        write_sub_block(o, e, sl, a, b, bi, bi, O, lmax, 18);
+        // off-diagonal sub-block: (u, v, w) x (rx, ry, rz) or its mirror
+        M[0][2] = bi ? Lp[1][0] : Lm[0][2]; M[1][2] = bi ? Lp[2][0] : Lm[1][2];
+        M[2][0] = bi ? Lm[2][0] : Lp[0][1]; M[2][1] = bi ? Lm[2][1] : Lp[0][2];
+        rot_sparse<0b011100100>(Qa, M, Qb, O);
+        write_sub_block(o, e, sl, a, b, bi, 1 - bi, O, lmax, 18);
     }
     if (o.maxabs) {
         for (int off = 8; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_xor_sync(tm, lmax, off, 16));
