@@ -69,6 +69,7 @@ struct ElemOut {
     const double *bprop = nullptr;       // per-variant bar records, or null
     int64_t bprop_stride = 0;
     int64_t u_stride = 0;                // per-variant displacement stride (ndof)
+    bool kg_layout = false;              // staged blocks sub-block-major (KG), else row-major (K)
 
     __device__ __forceinline__ ElemOut at(int v) const {
         ElemOut r = *this;
@@ -87,11 +88,25 @@ struct ElemOut {
 constexpr int32_t kBlkTranspose = 1 << 30;
 constexpr int32_t kBlkIndexMask = kBlkTranspose - 1;
 
-// Address of entry (i, j) of a pair block given its slot.
+// Address of entry (i, j) of a pair block given its slot.  Raw RBE2 blocks
+// are row-major.  Staged K blocks are row-major; staged KG blocks are
+// sub-block-major (translation 3x3, then translation-rotation,
+// rotation-translation, rotation-rotation, each row-major), so a shell's
+// translation-only KG block fills the first 9 values of its slot.
 __device__ __forceinline__ double *blk_entry(const ElemOut &o, int32_t s, int i, int j) {
     if (s < 0) return o.exc_raw + 36 * (int64_t)(-(s + 1)) + 6 * i + j;
     double *base = o.staging + 36 * (int64_t)(s & kBlkIndexMask);
-    return (s & kBlkTranspose) ? base + 6 * j + i : base + 6 * i + j;
+    const int r = (s & kBlkTranspose) ? j : i, c = (s & kBlkTranspose) ? i : j;
+    return o.kg_layout ? base + 9 * (2 * (r / 3) + c / 3) + 3 * (r % 3) + (c % 3) : base + 6 * r + c;
+}
+
+// Completes the first 96 bytes (three 32-byte sectors) of a staged KG shell
+// slot after its translation 3x3, so that the slot's written sectors are whole
+// and are not read back from DRAM to merge a partial write.
+__device__ __forceinline__ void kg_shell_pad(const ElemOut &o, int32_t s) {
+    if (s < 0) return;
+    double *base = o.staging + 36 * (int64_t)(s & kBlkIndexMask);
+    base[9] = 0.0; base[10] = 0.0; base[11] = 0.0;
 }
 
 // Per-point data of one CQUAD4 shared by its team.
@@ -837,6 +852,7 @@ __global__ void __launch_bounds__(Q4_THREADS) q4_kg_kernel(int64_t nq, const int
         const int32_t sl = __ldg(o.blk_slot + e * 10 + tl);
         double lmax = 0.0;
         write_sub_block(o, e, sl, a, b, 0, 0, O, lmax, 24);
+        kg_shell_pad(o, sl);
         if (sl < 0) {
             // the dof-level RBE2 path reads whole raw blocks; staged shell
             // blocks of KG are read as their translation 3x3 only

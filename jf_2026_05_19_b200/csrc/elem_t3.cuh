@@ -389,6 +389,7 @@ __device__ __forceinline__ void t3_kg_pair(int64_t e, const int32_t *__restrict_
         for (int j = 0; j < 6; ++j)
             if (i < 3 && j < 3) *blk_entry(o, s, i, j) = O[i][j];
             else if (s < 0) *blk_entry(o, s, i, j) = 0.0;
+    kg_shell_pad(o, s);
 }
 
 __global__ void __launch_bounds__(128) t3_kg_kernel(int64_t nt, const int32_t *__restrict__ nodes,

@@ -467,39 +467,37 @@ __device__ __forceinline__ void block_row_sum(const double *__restrict__ staging
     }
 }
 
-// KG rows: shell contributions hold only their translation 3x3 (written by
-// the shell kernels; the rest of their slot is not read), bar contributions
-// [r, b) hold the full block.  Row i < 3 sums columns 0-2 over every slot and
-// columns 3-5 over the bar slots; row i >= 3 sums the bar slots only.  The
-// order of the nonzero terms is the slot order, as in block_row_sum.
+// KG rows (sub-block-major slots, see blk_entry): shell contributions hold
+// only their translation 3x3 (the rest of their slot is not read), bar
+// contributions [r, b) hold the full block.  Row i < 3 sums columns 0-2 over
+// every slot and columns 3-5 over the bar slots; row i >= 3 sums the bar
+// slots only.  The nonzero terms are added in slot order.
 __device__ __forceinline__ void block_row_sum_kg(const double *__restrict__ staging, int32_t a, int32_t r, int32_t b, int i,
                                                  double s[6]) {
+    const int i3 = i < 3 ? i : i - 3;
     if (i < 3) {
         // batches of four slots, loads issued together; slots past the end
         // add +0.0
         for (int32_t q = a; q < b; q += 4) {
-            double2 x[4];
-            double z[4];
+            double x[4][3];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                x[u] = make_double2(0.0, 0.0);
-                z[u] = 0.0;
+                x[u][0] = x[u][1] = x[u][2] = 0.0;
                 if (q + u < b) {
-                    const double *p = staging + 36 * (int64_t)(q + u) + 6 * i;
-                    x[u] = __ldg(reinterpret_cast<const double2 *>(p));
-                    z[u] = __ldg(p + 2);
+                    const double *p = staging + 36 * (int64_t)(q + u) + 3 * i3;
+                    x[u][0] = __ldg(p); x[u][1] = __ldg(p + 1); x[u][2] = __ldg(p + 2);
                 }
             }
 #pragma unroll
-            for (int u = 0; u < 4; ++u) { s[0] += x[u].x; s[1] += x[u].y; s[2] += z[u]; }
+            for (int u = 0; u < 4; ++u) { s[0] += x[u][0]; s[1] += x[u][1]; s[2] += x[u][2]; }
         }
-        for (int32_t q = r; q < b; ++q) {
-            const double *p = staging + 36 * (int64_t)q + 6 * i;
-            const double2 x2 = __ldg(reinterpret_cast<const double2 *>(p + 4));
-            s[3] += __ldg(p + 3); s[4] += x2.x; s[5] += x2.y;
-        }
-    } else {
-        block_row_sum(staging, r, b, i, s);
+    }
+    const int c0 = i < 3 ? 9 : 18, c1 = i < 3 ? -1 : 27;  // sub-blocks of columns 0-2 (rows >= 3) and 3-5
+    for (int32_t q = r; q < b; ++q) {
+        const double *p = staging + 36 * (int64_t)q + 3 * i3;
+        if (i >= 3) { s[0] += __ldg(p + c0); s[1] += __ldg(p + c0 + 1); s[2] += __ldg(p + c0 + 2); }
+        const int o3 = i < 3 ? c0 : c1;
+        s[3] += __ldg(p + o3); s[4] += __ldg(p + o3 + 1); s[5] += __ldg(p + o3 + 2);
     }
 }
 
@@ -1278,6 +1276,7 @@ jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
     o.exc_stride = bt.exc_stride;
     o.dstage_stride = bt.dstage_stride;
     o.u_stride = bt.u_stride < 0 ? m->ndof : bt.u_stride;
+    o.kg_layout = kg;
     const double *du = bt.u;
     CK(mark(m, 0));
     if (m->nq) {
