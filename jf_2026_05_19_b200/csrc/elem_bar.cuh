@@ -181,13 +181,13 @@ __device__ __forceinline__ void tmul(const double *P, const double W[3][3], doub
 }
 
 __device__ __forceinline__ void bar_store(const ElemOut &o, int64_t e, int32_t sl, int bi, int bj, const double G[3][3],
-                                          bool diag, int node, double &lmax) {
+                                          bool diag, int node, double &lmax, int64_t pair_id) {
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
             lmax = fmax(lmax, fabs(G[i][j]));
-            *blk_entry(o, sl, 3 * bi + i, 3 * bj + j) = G[i][j];
+            *blk_entry(o, sl, 3 * bi + i, 3 * bj + j, pair_id) = G[i][j];
         }
     if (diag && o.diag_staging && bi == bj)
 #pragma unroll
@@ -209,12 +209,12 @@ __device__ __forceinline__ void bar_pair(const ElemOut &o, int64_t e, int p, con
     // tt
     kmul<A, B, 0, 0>(c, RB, W);
     tmul(RA, W, G, false);
-    bar_store(o, e, sl, 0, 0, G, A == B, A, lmax);
+    bar_store(o, e, sl, 0, 0, G, A == B, A, lmax, 3 * e + p);
     // rt (W = k_tt R_B)
     kmul<A, B, 1, 0>(c, RB, W2);
     tmul(RA, W2, G, false);
     if (off) tmul(OA, W, G, true);
-    bar_store(o, e, sl, 1, 0, G, false, A, lmax);
+    bar_store(o, e, sl, 1, 0, G, false, A, lmax, 3 * e + p);
     // tr: W = k_tt O_B + k_tr R_B
     kmul<A, B, 0, 1>(c, RB, W);
     if (off) {
@@ -225,7 +225,7 @@ __device__ __forceinline__ void bar_pair(const ElemOut &o, int64_t e, int p, con
             for (int j = 0; j < 3; ++j) W[i][j] = W2[i][j] + W[i][j];
     }
     tmul(RA, W, G, false);
-    bar_store(o, e, sl, 0, 1, G, false, A, lmax);
+    bar_store(o, e, sl, 0, 1, G, false, A, lmax, 3 * e + p);
     // rr: R_A' (k_rt O_B + k_rr R_B) + O_A' W
     kmul<A, B, 1, 1>(c, RB, W2);
     if (off) {
@@ -238,7 +238,7 @@ __device__ __forceinline__ void bar_pair(const ElemOut &o, int64_t e, int p, con
     }
     tmul(RA, W2, G, false);
     if (off) tmul(OA, W, G, true);
-    bar_store(o, e, sl, 1, 1, G, A == B, A, lmax);
+    bar_store(o, e, sl, 1, 1, G, A == B, A, lmax, 3 * e + p);
 }
 
 // One (bar, node pair) per thread, pair-major so that a warp runs one

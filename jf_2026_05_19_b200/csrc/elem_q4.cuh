@@ -69,7 +69,8 @@ struct ElemOut {
     const double *bprop = nullptr;       // per-variant bar records, or null
     int64_t bprop_stride = 0;
     int64_t u_stride = 0;                // per-variant displacement stride (ndof)
-    bool kg_layout = false;              // staged blocks sub-block-major (KG), else row-major (K)
+    bool kg_layout = false;              // KG staging layout (see blk_entry), else K's
+    double *kg_rot = nullptr;            // KG: rotation sub-blocks of bar pairs (27 doubles per bar pair)
 
     __device__ __forceinline__ ElemOut at(int v) const {
         ElemOut r = *this;
@@ -79,6 +80,7 @@ struct ElemOut {
         if (maxabs) r.maxabs += v;
         if (h) r.h += v * h_stride;
         if (bprop) r.bprop += v * bprop_stride;
+        if (kg_rot) r.kg_rot += v * staging_stride;
         return r;
     }
     // Shell thickness of element e: the variant's own, else the property record's.
@@ -89,23 +91,25 @@ constexpr int32_t kBlkTranspose = 1 << 30;
 constexpr int32_t kBlkIndexMask = kBlkTranspose - 1;
 
 // Address of entry (i, j) of a pair block given its slot.  Raw RBE2 blocks
-// are row-major.  Staged K blocks are row-major; staged KG blocks are
-// sub-block-major (translation 3x3, then translation-rotation,
-// rotation-translation, rotation-rotation, each row-major), so a shell's
-// translation-only KG block fills the first 9 values of its slot.
-__device__ __forceinline__ double *blk_entry(const ElemOut &o, int32_t s, int i, int j) {
+// are row-major 6x6.  K stages 36 values per slot, row-major.  KG stages 12
+// values per slot: the translation 3x3 (row-major) and three values of
+// padding, so a shell's KG contribution (translations only) fills whole
+// 32-byte sectors; the other three 3x3 sub-blocks of a bar pair (translation-
+// rotation, rotation-translation, rotation-rotation) go to kg_rot at the bar
+// pair's index.
+__device__ __forceinline__ double *blk_entry(const ElemOut &o, int32_t s, int i, int j, int64_t bar_pair = 0) {
     if (s < 0) return o.exc_raw + 36 * (int64_t)(-(s + 1)) + 6 * i + j;
-    double *base = o.staging + 36 * (int64_t)(s & kBlkIndexMask);
+    const int64_t idx = s & kBlkIndexMask;
     const int r = (s & kBlkTranspose) ? j : i, c = (s & kBlkTranspose) ? i : j;
-    return o.kg_layout ? base + 9 * (2 * (r / 3) + c / 3) + 3 * (r % 3) + (c % 3) : base + 6 * r + c;
+    if (!o.kg_layout) return o.staging + 36 * idx + 6 * r + c;
+    if (r < 3 && c < 3) return o.staging + 12 * idx + 3 * r + c;
+    return o.kg_rot + 27 * bar_pair + 9 * (2 * (r / 3) + c / 3 - 1) + 3 * (r % 3) + (c % 3);
 }
 
-// Completes the first 96 bytes (three 32-byte sectors) of a staged KG shell
-// slot after its translation 3x3, so that the slot's written sectors are whole
-// and are not read back from DRAM to merge a partial write.
+// The padding of a staged KG shell slot (see blk_entry).
 __device__ __forceinline__ void kg_shell_pad(const ElemOut &o, int32_t s) {
     if (s < 0) return;
-    double *base = o.staging + 36 * (int64_t)(s & kBlkIndexMask);
+    double *base = o.staging + 12 * (int64_t)(s & kBlkIndexMask);
     base[9] = 0.0; base[10] = 0.0; base[11] = 0.0;
 }
 

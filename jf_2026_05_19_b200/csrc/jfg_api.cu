@@ -70,6 +70,8 @@ struct jfg_model {
     int32_t *d_blk_seg = nullptr;       // n_blk + 1 segment bounds (in blocks)
     int32_t *d_blk_A = nullptr, *d_blk_B = nullptr, *d_blk_offAB = nullptr, *d_blk_offBA = nullptr;
     int32_t *d_blk_rot = nullptr;       // first bar slot of each block's segment (segment end if none)
+    int32_t *d_slot_bar = nullptr;      // per slot: bar pair index (element pair - pair_bar), negative for shells
+    int64_t staging_len = 0;            // staging doubles per assembly: max(K 36 per slot, KG 12 per slot + 27 per bar pair)
     double *d_staging = nullptr;        // 36 doubles per regular element pair
     int64_t *d_rowptr = nullptr, *d_colind = nullptr;   // 0-based symmetric CSR == CSC
     // dof-level path for pairs that touch RBE2 nodes
@@ -430,6 +432,11 @@ __global__ void blk_rot_kernel(int64_t nbc, const int32_t *__restrict__ vals, co
     rot[pos[q] + flags[q] - 1] = (int32_t)q;
 }
 
+__global__ void slot_bar_kernel(int64_t nbc, const int32_t *__restrict__ vals, int64_t pair_bar, int32_t *slot_bar) {
+    int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < nbc) slot_bar[q] = (int32_t)(vals[q] - pair_bar);
+}
+
 __global__ void key_pos_kernel(int64_t n, const uint64_t *__restrict__ keys, int64_t ndof, const int64_t *__restrict__ rowptr,
                                const int64_t *__restrict__ colind, int64_t *pos, int32_t *err) {
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -467,13 +474,14 @@ __device__ __forceinline__ void block_row_sum(const double *__restrict__ staging
     }
 }
 
-// KG rows (sub-block-major slots, see blk_entry): shell contributions hold
-// only their translation 3x3 (the rest of their slot is not read), bar
-// contributions [r, b) hold the full block.  Row i < 3 sums columns 0-2 over
+// KG rows (12 values per slot plus 27 per bar pair, see blk_entry): shell
+// contributions hold only their translation 3x3, bar contributions [r, b)
+// also their three rotation sub-blocks.  Row i < 3 sums columns 0-2 over
 // every slot and columns 3-5 over the bar slots; row i >= 3 sums the bar
 // slots only.  The nonzero terms are added in slot order.
-__device__ __forceinline__ void block_row_sum_kg(const double *__restrict__ staging, int32_t a, int32_t r, int32_t b, int i,
-                                                 double s[6]) {
+__device__ __forceinline__ void block_row_sum_kg(const double *__restrict__ staging, const double *__restrict__ kg_rot,
+                                                 const int32_t *__restrict__ slot_bar, int32_t a, int32_t r, int32_t b,
+                                                 int i, double s[6]) {
     const int i3 = i < 3 ? i : i - 3;
     if (i < 3) {
         // batches of four slots, loads issued together; slots past the end
@@ -484,7 +492,7 @@ __device__ __forceinline__ void block_row_sum_kg(const double *__restrict__ stag
             for (int u = 0; u < 4; ++u) {
                 x[u][0] = x[u][1] = x[u][2] = 0.0;
                 if (q + u < b) {
-                    const double *p = staging + 36 * (int64_t)(q + u) + 3 * i3;
+                    const double *p = staging + 12 * (int64_t)(q + u) + 3 * i3;
                     x[u][0] = __ldg(p); x[u][1] = __ldg(p + 1); x[u][2] = __ldg(p + 2);
                 }
             }
@@ -492,11 +500,10 @@ __device__ __forceinline__ void block_row_sum_kg(const double *__restrict__ stag
             for (int u = 0; u < 4; ++u) { s[0] += x[u][0]; s[1] += x[u][1]; s[2] += x[u][2]; }
         }
     }
-    const int c0 = i < 3 ? 9 : 18, c1 = i < 3 ? -1 : 27;  // sub-blocks of columns 0-2 (rows >= 3) and 3-5
     for (int32_t q = r; q < b; ++q) {
-        const double *p = staging + 36 * (int64_t)q + 3 * i3;
-        if (i >= 3) { s[0] += __ldg(p + c0); s[1] += __ldg(p + c0 + 1); s[2] += __ldg(p + c0 + 2); }
-        const int o3 = i < 3 ? c0 : c1;
+        const double *p = kg_rot + 27 * (int64_t)__ldg(slot_bar + q) + 3 * i3;
+        if (i >= 3) { s[0] += __ldg(p + 9); s[1] += __ldg(p + 10); s[2] += __ldg(p + 11); }
+        const int o3 = i < 3 ? 0 : 18;  // translation-rotation / rotation-rotation rows
         s[3] += __ldg(p + o3); s[4] += __ldg(p + o3 + 1); s[5] += __ldg(p + o3 + 2);
     }
 }
@@ -519,6 +526,7 @@ __device__ __forceinline__ void block_row_write(int64_t k, int i, const double s
 template <bool KG>
 __global__ void __launch_bounds__(256) block_reduce_kernel(int64_t n_blk, const int32_t *__restrict__ seg,
                                                            const int32_t *__restrict__ rot,
+                                                           const int32_t *__restrict__ slot_bar, int64_t kg_rot_off,
                                                            const double *__restrict__ staging, const int32_t *__restrict__ A,
                                                            const int32_t *__restrict__ B, const int32_t *__restrict__ offAB,
                                                            const int32_t *__restrict__ offBA, const int64_t *__restrict__ rowptr,
@@ -536,8 +544,8 @@ __global__ void __launch_bounds__(256) block_reduce_kernel(int64_t n_blk, const 
     double s0[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, s1[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (KG) {
         const int32_t r0 = __ldg(rot + k0), r1 = two ? __ldg(rot + k1) : 0;
-        block_row_sum_kg(staging, a0, r0, b0, i, s0);
-        block_row_sum_kg(staging, a1, r1, b1, i, s1);
+        block_row_sum_kg(staging, staging + kg_rot_off, slot_bar, a0, r0, b0, i, s0);
+        block_row_sum_kg(staging, staging + kg_rot_off, slot_bar, a1, r1, b1, i, s1);
     } else {
         block_row_sum(staging, a0, b0, i, s0);
         block_row_sum(staging, a1, b1, i, s1);
@@ -1016,6 +1024,7 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
     CK(dalloc(m, &m->d_blk_offAB, m->n_blk));
     CK(dalloc(m, &m->d_blk_offBA, m->n_blk));
     CK(dalloc(m, &m->d_blk_rot, m->n_blk));
+    CK(dalloc(m, &m->d_slot_bar, nbc));
     CK(dalloc(m, &m->d_blk_slot, NP));
     CK(cudaMemsetAsync(m->d_blk_slot, 0, sizeof(int32_t) * std::max<int64_t>(NP, 1), m->stream));
     int32_t *d_err = nullptr;
@@ -1035,6 +1044,8 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(m->d_blk_rot, m->d_blk_seg + 1, sizeof(int32_t) * m->n_blk, cudaMemcpyDeviceToDevice, m->stream));
         blk_rot_kernel<<<(unsigned)cdiv(nbc, 256), 256, 0, m->stream>>>(nbc, d_bv2, d_bflags, d_bpos, m->pair_bar, m->d_blk_rot);
+        CK(cudaGetLastError());
+        slot_bar_kernel<<<(unsigned)cdiv(nbc, 256), 256, 0, m->stream>>>(nbc, d_bv2, m->pair_bar, m->d_slot_bar);
         CK(cudaGetLastError());
     }
     // exception pairs: raw blocks, then dof-level weighted contributions
@@ -1117,7 +1128,8 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
         cudaFreeAsync(d_uk, m->stream);
     }
     CK(dalloc(m, &m->d_exc_raw, 36 * m->n_xpair));
-    CK(dalloc(m, &m->d_staging, 36 * nbc));
+    m->staging_len = std::max<int64_t>(36 * nbc, 12 * nbc + 27 * 3 * m->nb);
+    CK(dalloc(m, &m->d_staging, m->staging_len));
     {
         int32_t herr = 0;
         CK(cudaMemcpyAsync(&herr, d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, m->stream));
@@ -1254,7 +1266,7 @@ struct BatchSizes { int64_t staging, exc, part, dstage, total; };
 BatchSizes batch_sizes(const jfg_model *m) {
     auto up = [](int64_t n) { return (n + 31) / 32 * 32; };  // 256-byte aligned sub-buffers
     BatchSizes z;
-    z.staging = up(36 * m->n_blk_contrib);
+    z.staging = up(m->staging_len);
     z.exc = up(36 * m->n_xpair);
     z.part = up(m->n_xchunk);
     z.dstage = up(m->n_dcontrib);
@@ -1277,6 +1289,7 @@ jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
     o.dstage_stride = bt.dstage_stride;
     o.u_stride = bt.u_stride < 0 ? m->ndof : bt.u_stride;
     o.kg_layout = kg;
+    o.kg_rot = kg ? bt.staging + 12 * m->n_blk_contrib : nullptr;
     const double *du = bt.u;
     CK(mark(m, 0));
     if (m->nq) {
@@ -1338,12 +1351,12 @@ jfg_status launch_reduce(jfg_model *m, const Batch &bt, bool kg) {
         const dim3 grid((unsigned)cdiv((m->n_blk + 1) / 2 * 6, 256), nv);
         if (kg)
             block_reduce_kernel<true><<<grid, 256, 0, m->stream>>>(
-                m->n_blk, m->d_blk_seg, m->d_blk_rot, bt.staging, m->d_blk_A, m->d_blk_B, m->d_blk_offAB, m->d_blk_offBA,
-                m->d_rowptr, bt.nz, bt.staging_stride, m->nnz);
+                m->n_blk, m->d_blk_seg, m->d_blk_rot, m->d_slot_bar, 12 * m->n_blk_contrib, bt.staging, m->d_blk_A, m->d_blk_B,
+                m->d_blk_offAB, m->d_blk_offBA, m->d_rowptr, bt.nz, bt.staging_stride, m->nnz);
         else
             block_reduce_kernel<false><<<grid, 256, 0, m->stream>>>(
-                m->n_blk, m->d_blk_seg, m->d_blk_rot, bt.staging, m->d_blk_A, m->d_blk_B, m->d_blk_offAB, m->d_blk_offBA,
-                m->d_rowptr, bt.nz, bt.staging_stride, m->nnz);
+                m->n_blk, m->d_blk_seg, m->d_blk_rot, m->d_slot_bar, 0, bt.staging, m->d_blk_A, m->d_blk_B,
+                m->d_blk_offAB, m->d_blk_offBA, m->d_rowptr, bt.nz, bt.staging_stride, m->nnz);
     }
     CK(cudaGetLastError());
     CK(mark(m, 5));
