@@ -452,11 +452,11 @@ __global__ void key_pos_kernel(int64_t n, const uint64_t *__restrict__ keys, int
 // ---------------------------------------------------------------------------
 
 // Deterministic block reduction: thread (k, i) sums row i (six values) of
-// every element block in global block k's segment, in slot order, and writes
-// it to row 6A+i (columns of B) and, for A != B, into column i of the
-// mirrored rows 6B+j.  Staging rows are 48-byte aligned, so they are read as
-// three double2 loads.  Each thread takes two blocks, k and k + half, whose
-// loads are issued together to keep more of them in flight.
+// every element block in global block k's segment, in slot order.  Staging
+// rows are 48-byte aligned, so they are read as three double2 loads.  Each
+// thread takes two blocks, k and k + half, whose loads are issued together to
+// keep more of them in flight.  The summed rows are then transposed through
+// shared memory and written with block_write.
 __device__ __forceinline__ void block_row_sum(const double *__restrict__ staging, int32_t a, int32_t b, int i, double s[6]) {
     int32_t q = a;
     for (; q + 1 < b; q += 2) {
@@ -508,50 +508,69 @@ __device__ __forceinline__ void block_row_sum_kg(const double *__restrict__ stag
     }
 }
 
-__device__ __forceinline__ void block_row_write(int64_t k, int i, const double s[6], const int32_t *__restrict__ A,
-                                                const int32_t *__restrict__ B, const int32_t *__restrict__ offAB,
-                                                const int32_t *__restrict__ offBA, const int64_t *__restrict__ rowptr,
-                                                double *nz) {
+// Writes of one summed block: column i goes to column i of the rows 6A+r,
+// row i to column i of the mirrored rows 6B+j, so in both writes the six
+// threads of a block store six consecutive values of one CSC row.
+__device__ __forceinline__ void block_write(int64_t k, int i, const double sr[6], const double sc[6],
+                                            const int32_t *__restrict__ A, const int32_t *__restrict__ B,
+                                            const int32_t *__restrict__ offAB, const int32_t *__restrict__ offBA,
+                                            const int64_t *__restrict__ rowptr, double *nz) {
     const int64_t nA = __ldg(A + k), nB = __ldg(B + k);
-    double *row = nz + __ldg(rowptr + 6 * nA + i) + __ldg(offAB + k);
+    const int64_t ca = __ldg(offAB + k) + i;
 #pragma unroll
-    for (int j = 0; j < 6; ++j) row[j] = s[j];
+    for (int r = 0; r < 6; ++r) nz[__ldg(rowptr + 6 * nA + r) + ca] = sc[r];
     if (nA != nB) {
         const int64_t cb = __ldg(offBA + k) + i;
 #pragma unroll
-        for (int j = 0; j < 6; ++j) nz[__ldg(rowptr + 6 * nB + j) + cb] = s[j];
+        for (int j = 0; j < 6; ++j) nz[__ldg(rowptr + 6 * nB + j) + cb] = sr[j];
     }
 }
 
+// Thread layout: warp w takes blocks 5w .. 5w+4 (lanes 6g .. 6g+5 for block
+// 5w+g, lanes 30-31 idle) and the same five blocks + half.  Each thread sums
+// row i of its blocks; the rows meet in shared memory so that every thread
+// also holds column i for the coalesced write above.
+constexpr int kRedWarps = 8;
+
 template <bool KG>
-__global__ void __launch_bounds__(256) block_reduce_kernel(int64_t n_blk, const int32_t *__restrict__ seg,
+__global__ void __launch_bounds__(32 * kRedWarps, 4) block_reduce_kernel(int64_t n_blk, const int32_t *__restrict__ seg,
                                                            const int32_t *__restrict__ rot,
                                                            const int32_t *__restrict__ slot_bar, int64_t kg_rot_off,
                                                            const double *__restrict__ staging, const int32_t *__restrict__ A,
                                                            const int32_t *__restrict__ B, const int32_t *__restrict__ offAB,
                                                            const int32_t *__restrict__ offBA, const int64_t *__restrict__ rowptr,
                                                            double *nz, int64_t staging_stride, int64_t nnz) {
+    __shared__ double tr[kRedWarps][2][5][36];
     const int64_t half = (n_blk + 1) / 2;
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= half * 6) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane / 6, i = lane - 6 * (lane / 6);
+    const int64_t k0 = ((int64_t)blockIdx.x * kRedWarps + warp) * 5 + g, k1 = k0 + half;
+    const bool one = g < 5 && k0 < half, two = one && k1 < n_blk;
     staging += (int64_t)blockIdx.y * staging_stride;  // batched variant
     nz += (int64_t)blockIdx.y * nnz;
-    const int64_t k0 = t / 6, k1 = k0 + half;
-    const int i = (int)(t - 6 * k0);
-    const bool two = k1 < n_blk;
-    const int32_t a0 = __ldg(seg + k0), b0 = __ldg(seg + k0 + 1);
-    const int32_t a1 = two ? __ldg(seg + k1) : 0, b1 = two ? __ldg(seg + k1 + 1) : 0;
     double s0[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, s1[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    if (KG) {
-        const int32_t r0 = __ldg(rot + k0), r1 = two ? __ldg(rot + k1) : 0;
-        block_row_sum_kg(staging, staging + kg_rot_off, slot_bar, a0, r0, b0, i, s0);
-        block_row_sum_kg(staging, staging + kg_rot_off, slot_bar, a1, r1, b1, i, s1);
-    } else {
-        block_row_sum(staging, a0, b0, i, s0);
-        block_row_sum(staging, a1, b1, i, s1);
+    if (one) {
+        const int32_t a0 = __ldg(seg + k0), b0 = __ldg(seg + k0 + 1);
+        const int32_t a1 = two ? __ldg(seg + k1) : 0, b1 = two ? __ldg(seg + k1 + 1) : 0;
+        if (KG) {
+            const int32_t r0 = __ldg(rot + k0), r1 = two ? __ldg(rot + k1) : 0;
+            block_row_sum_kg(staging, staging + kg_rot_off, slot_bar, a0, r0, b0, i, s0);
+            block_row_sum_kg(staging, staging + kg_rot_off, slot_bar, a1, r1, b1, i, s1);
+        } else {
+            block_row_sum(staging, a0, b0, i, s0);
+            block_row_sum(staging, a1, b1, i, s1);
+        }
+#pragma unroll
+        for (int c = 0; c < 6; ++c) { tr[warp][0][g][6 * i + c] = s0[c]; tr[warp][1][g][6 * i + c] = s1[c]; }
     }
-    block_row_write(k0, i, s0, A, B, offAB, offBA, rowptr, nz);
-    if (two) block_row_write(k1, i, s1, A, B, offAB, offBA, rowptr, nz);
+    __syncwarp();
+    if (one) {
+        double c0[6], c1[6];
+#pragma unroll
+        for (int r = 0; r < 6; ++r) { c0[r] = tr[warp][0][g][6 * r + i]; c1[r] = tr[warp][1][g][6 * r + i]; }
+        block_write(k0, i, s0, c0, A, B, offAB, offBA, rowptr, nz);
+        if (two) block_write(k1, i, s1, c1, A, B, offAB, offBA, rowptr, nz);
+    }
 }
 
 // Dof-level path: each CSC position touched by an RBE2-expanded entry sums
@@ -1348,13 +1367,13 @@ jfg_status launch_reduce(jfg_model *m, const Batch &bt, bool kg) {
     CK(cudaGetLastError());
     CK(mark(m, 4));
     if (m->n_blk) {
-        const dim3 grid((unsigned)cdiv((m->n_blk + 1) / 2 * 6, 256), nv);
+        const dim3 grid((unsigned)cdiv(cdiv((m->n_blk + 1) / 2, 5), kRedWarps), nv);
         if (kg)
-            block_reduce_kernel<true><<<grid, 256, 0, m->stream>>>(
+            block_reduce_kernel<true><<<grid, 32 * kRedWarps, 0, m->stream>>>(
                 m->n_blk, m->d_blk_seg, m->d_blk_rot, m->d_slot_bar, 12 * m->n_blk_contrib, bt.staging, m->d_blk_A, m->d_blk_B,
                 m->d_blk_offAB, m->d_blk_offBA, m->d_rowptr, bt.nz, bt.staging_stride, m->nnz);
         else
-            block_reduce_kernel<false><<<grid, 256, 0, m->stream>>>(
+            block_reduce_kernel<false><<<grid, 32 * kRedWarps, 0, m->stream>>>(
                 m->n_blk, m->d_blk_seg, m->d_blk_rot, m->d_slot_bar, 0, bt.staging, m->d_blk_A, m->d_blk_B,
                 m->d_blk_offAB, m->d_blk_offBA, m->d_rowptr, bt.nz, bt.staging_stride, m->nnz);
     }
