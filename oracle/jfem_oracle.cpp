@@ -888,6 +888,197 @@ void constrain_and_csc(const jfg_model_desc *d, Triplets &t, std::vector<int64_t
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// shell-thickness sensitivity element (dKdx.jl:218-250)
+// ---------------------------------------------------------------------------
+
+// stiffness_quad4_generic (FEMKernels.jl:1473-1490) over
+// stiffness_quad4_default_generic (:1496-1656), the element that
+// _shell_thickness_dKe_forward_ad differentiates: bend_ratio 1, ts_t 5/6,
+// k6rot 100, G = E / 2(1 + nu) (drill G_ref too), membrane with Wilson
+// incompatible modes at the Gauss-point Jacobian (no bending modes), bending
+// without the twist row, and transverse shear from the four tying points
+// (0, -+1), (-+1, 0) scaled by phi2 = min(1, 10 h^2 / max(4 |det Jc|, 1e-30))
+// (PHI2_ALPHA = 10, :10).  The parts are kept apart so that
+//   K      = Km + Kb + Kd + Ks - Kc
+//   dK/dh  = (Km + Kd - Kc + 3 Kb + s Ks) / h,   s = 3 while phi2 < 1, else 1,
+// which is what forward-mode AD of the reference returns: Cm, K_ab, K_bb and
+// the drill scale are linear in h, Cb cubic, and Cs linear times phi2 (h^2 on
+// the unsaturated branch ForwardDiff takes, constant on the saturated one).
+struct Q4GenericParts {
+    double Km[24][24], Kb[24][24], Kd[24][24], Ks[24][24], Kc[24][24];
+    bool phi2_saturated;
+};
+
+void q4_generic_parts(const double lc[4][2], double E, double nu, double h, Q4GenericParts &P) {
+    std::memset(&P, 0, sizeof(P));
+    const double cm = E * h / (1 - nu * nu), cb = 1.0 * (E * h * h * h) / (12 * (1 - nu * nu));
+    const double base[3][3] = {{1.0, nu, 0.0}, {nu, 1.0, 0.0}, {0.0, 0.0, (1 - nu) / 2}};
+    double Cm[3][3], Cb[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) { Cm[i][j] = cm * base[i][j]; Cb[i][j] = cb * base[i][j]; }
+    const double G = E / (2 * (1 + nu));
+    const double cs = (5.0 / 6.0) * G * h;
+    // tying-point rows (w, theta_x, theta_y of each node), :1510-1538
+    double Bs_tp[4][24] = {};
+    const double tp[4][2] = {{0.0, -1.0}, {0.0, 1.0}, {-1.0, 0.0}, {1.0, 0.0}};
+    for (int t = 0; t < 4; ++t) {
+        double dNr[4], dNs[4];
+        shape_derivs_quad(tp[t][0], tp[t][1], dNr, dNs);
+        Jac j = jacobian(lc, dNr, dNs);
+        const double xi = tp[t][0], eta = tp[t][1];
+        const double N[4] = {0.25 * (1.0 - xi) * (1.0 - eta), 0.25 * (1.0 + xi) * (1.0 - eta), 0.25 * (1.0 + xi) * (1.0 + eta),
+                             0.25 * (1.0 - xi) * (1.0 + eta)};
+        for (int k = 0; k < 4; ++k) {
+            if (t < 2) { Bs_tp[t][6 * k + 2] = dNr[k]; Bs_tp[t][6 * k + 3] = -j.J12 * N[k]; Bs_tp[t][6 * k + 4] = j.J11 * N[k]; }
+            else { Bs_tp[t][6 * k + 2] = dNs[k]; Bs_tp[t][6 * k + 3] = -j.J22 * N[k]; Bs_tp[t][6 * k + 4] = j.J21 * N[k]; }
+        }
+    }
+    const double dNr_c[4] = {-0.25, 0.25, 0.25, -0.25}, dNs_c[4] = {-0.25, -0.25, 0.25, 0.25};
+    Jac jc = jacobian(lc, dNr_c, dNs_c);
+    const double L_char_sq = std::max(4.0 * std::fabs(jc.det), 1e-30);
+    const double phi2_trial = 10.0 * h * h / L_char_sq;
+    P.phi2_saturated = !(phi2_trial < 1.0);
+    const double phi2 = P.phi2_saturated ? 1.0 : phi2_trial;
+    const double alpha_drill = (100.0 / 1e5) * G * h;
+    double K_ab[24][4] = {}, K_bb[4][4] = {};
+    const double pt = 1.0 / std::sqrt(3.0);
+    const double gp[4][2] = {{-pt, -pt}, {pt, -pt}, {pt, pt}, {-pt, pt}};
+    for (int g = 0; g < 4; ++g) {
+        const double r = gp[g][0], s = gp[g][1];
+        double dNr[4], dNs[4];
+        shape_derivs_quad(r, s, dNr, dNs);
+        Jac j = jacobian(lc, dNr, dNs);
+        double absdet = std::fabs(j.det);
+        if (absdet < 1e-12) absdet = 1e-12;
+        double Bm[3][24] = {}, Bb[3][24] = {}, Bd[1][24] = {}, Bi[3][4] = {};
+        for (int k = 0; k < 4; ++k) {
+            const double dx = j.iJ11 * dNr[k] + j.iJ12 * dNs[k], dy = j.iJ21 * dNr[k] + j.iJ22 * dNs[k];
+            const int idx = 6 * k;
+            const double Nk = 0.25 * (1 + ((k == 1 || k == 2) ? r : -r)) * (1 + (k >= 2 ? s : -s));
+            Bm[0][idx] = dx; Bm[1][idx + 1] = dy; Bm[2][idx] = dy; Bm[2][idx + 1] = dx;
+            Bb[0][idx + 4] = dx; Bb[1][idx + 3] = -dy; Bb[2][idx + 4] = dy; Bb[2][idx + 3] = -dx;
+            Bd[0][idx] = 0.5 * dy; Bd[0][idx + 1] = -0.5 * dx; Bd[0][idx + 5] = Nk;
+        }
+        const double d1x = j.iJ11 * (-2.0 * r), d1y = j.iJ21 * (-2.0 * r), d2x = j.iJ12 * (-2.0 * s), d2y = j.iJ22 * (-2.0 * s);
+        Bi[0][0] = d1x; Bi[2][0] = d1y; Bi[1][1] = d1y; Bi[2][1] = d1x;
+        Bi[0][2] = d2x; Bi[2][2] = d2y; Bi[1][3] = d2y; Bi[2][3] = d2x;
+        double t3x24[3 * 24], t3x4[3 * 4];
+        mul(t3x24, &Cm[0][0], &Bm[0][0], 3, 3, 24);
+        mul_At_add(&P.Km[0][0], &Bm[0][0], t3x24, 3, 24, 24, absdet);
+        mul(t3x24, &Cb[0][0], &Bb[0][0], 3, 3, 24);
+        mul_At_add(&P.Kb[0][0], &Bb[0][0], t3x24, 3, 24, 24, absdet);
+        mul_At_add(&P.Kd[0][0], &Bd[0][0], &Bd[0][0], 1, 24, 24, absdet * alpha_drill);
+        // covariant shear interpolation and Cs_cov = phi2 invJ' Cs invJ (:1620-1634)
+        const double wem = 0.5 * (1.0 - s), wep = 0.5 * (1.0 + s), wxm = 0.5 * (1.0 - r), wxp = 0.5 * (1.0 + r);
+        double Bs[2][24];
+        for (int c = 0; c < 24; ++c) {
+            Bs[0][c] = wem * Bs_tp[0][c] + wep * Bs_tp[1][c];
+            Bs[1][c] = wxm * Bs_tp[2][c] + wxp * Bs_tp[3][c];
+        }
+        const double iJ[2][2] = {{j.iJ11, j.iJ12}, {j.iJ21, j.iJ22}};
+        double Csc[2][2];
+        for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b) Csc[a][b] = phi2 * cs * (iJ[0][a] * iJ[0][b] + iJ[1][a] * iJ[1][b]);
+        double t2x24[2 * 24];
+        mul(t2x24, &Csc[0][0], &Bs[0][0], 2, 2, 24);
+        mul_At_add(&P.Ks[0][0], &Bs[0][0], t2x24, 2, 24, 24, absdet);
+        mul(t3x4, &Cm[0][0], &Bi[0][0], 3, 3, 4);
+        mul_At_add(&K_ab[0][0], &Bm[0][0], t3x4, 3, 24, 4, absdet);
+        mul_At_add(&K_bb[0][0], &Bi[0][0], t3x4, 3, 4, 4, absdet);
+    }
+    double kbbmax = 0.0;
+    for (int i = 0; i < 4; ++i)
+        for (int c = 0; c < 4; ++c) kbbmax = std::max(kbbmax, std::fabs(K_bb[i][c]));
+    if (kbbmax > 0.0) {
+        // K_ab (K_bb \ K_ab')
+        double A[16], X[4 * 24];
+        for (int i = 0; i < 4; ++i)
+            for (int c = 0; c < 4; ++c) A[4 * i + c] = K_bb[i][c];
+        for (int l = 0; l < 4; ++l)
+            for (int c = 0; c < 24; ++c) X[24 * l + c] = K_ab[c][l];
+        lu_solve(4, 24, A, X);
+        for (int i = 0; i < 24; ++i)
+            for (int c = 0; c < 24; ++c) {
+                double sm = 0.0;
+                for (int l = 0; l < 4; ++l) sm += K_ab[i][l] * X[24 * l + c];
+                P.Kc[i][c] = sm;
+            }
+    }
+}
+
+void q4_generic(const double lc[4][2], double E, double nu, double h, double Ke[24][24], double dKe[24][24]) {
+    static thread_local Q4GenericParts P;
+    q4_generic_parts(lc, E, nu, h, P);
+    const double sfac = P.phi2_saturated ? 1.0 : 3.0;
+    for (int i = 0; i < 24; ++i)
+        for (int c = 0; c < 24; ++c) {
+            if (Ke) Ke[i][c] = P.Km[i][c] + P.Kb[i][c] + P.Kd[i][c] + P.Ks[i][c] - P.Kc[i][c];
+            if (dKe) dKe[i][c] = (P.Km[i][c] + P.Kd[i][c] - P.Kc[i][c] + 3.0 * P.Kb[i][c] + sfac * P.Ks[i][c]) / h;
+        }
+}
+
+// stiffness_tria3_generic (FEMKernels.jl:7113-7123): the assembly's CTRIA3
+// with bend_ratio 1, ts_t 5/6, k6rot 100 and G = E / 2(1 + nu).
+void t3_generic(const double lc[3][2], double E, double nu, double h, double Ke[18][18]) {
+    const double G = E / (2 * (1 + nu));
+    const double base[3][3] = {{1.0, nu, 0.0}, {nu, 1.0, 0.0}, {0.0, 0.0, (1 - nu) / 2}};
+    double Dm[3][3], Db[3][3], Ds[2][2] = {{(5.0 / 6.0) * G * h, 0.0}, {0.0, (5.0 / 6.0) * G * h}};
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            Dm[i][j] = (E * h / (1 - nu * nu)) * base[i][j];
+            Db[i][j] = 1.0 * (E * h * h * h / (12 * (1 - nu * nu))) * base[i][j];
+        }
+    t3_stiffness(lc, Dm, Db, Ds, h, G, 1.0, 100.0, Ke);
+}
+
+// dK/dh of the CTRIA3 by central differences with one Richardson step
+// (step h / 256, error O(step^4)); the reference differentiates the same
+// function by forward-mode AD, which this matches to about 1e-10 relative.
+void t3_generic_dkdh(const double lc[3][2], double E, double nu, double h, double dKe[18][18]) {
+    double Kp[18][18], Km[18][18], Kp2[18][18], Km2[18][18];
+    const double d = h / 256.0;
+    t3_generic(lc, E, nu, h + d, Kp); t3_generic(lc, E, nu, h - d, Km);
+    t3_generic(lc, E, nu, h + 0.5 * d, Kp2); t3_generic(lc, E, nu, h - 0.5 * d, Km2);
+    for (int i = 0; i < 18; ++i)
+        for (int c = 0; c < 18; ++c) {
+            const double D1 = (Kp[i][c] - Km[i][c]) / (2 * d), D2 = (Kp2[i][c] - Km2[i][c]) / d;
+            dKe[i][c] = (4.0 * D2 - D1) / 3.0;
+        }
+}
+
+// Shell element setup of _shell_elem_local_data (dKdx.jl:128-176): frame
+// (shell_element_frame_fast: the :diag quad frame, the edge frame for a
+// triangle), centroid-relative local coordinates, node blocks Rel * node_R.
+void shell_setup(const jfg_model_desc *d, const int32_t *nd, int nn, double lc[4][2], double *Q) {
+    const double *p[4];
+    for (int k = 0; k < nn; ++k) p[k] = d->coords + 3 * (int64_t)nd[k];
+    double v1[3], v2[3], v3[3];
+    if (nn == 4) q4_frame(p[0], p[1], p[2], p[3], v1, v2, v3);
+    else t3_frame(p[0], p[1], p[2], v1, v2, v3);
+    double c[3] = {0.0, 0.0, 0.0};
+    for (int k = 0; k < nn; ++k)
+        for (int i = 0; i < 3; ++i) c[i] += p[k][i];
+    for (int i = 0; i < 3; ++i) c[i] /= nn;
+    for (int k = 0; k < nn; ++k) {
+        double dd[3];
+        sub3(p[k], c, dd);
+        lc[k][0] = dot3(dd, v1); lc[k][1] = dot3(dd, v2);
+    }
+    node_blocks(d, nd, nn, v1, v2, v3, Q);
+}
+
+// x_local = T x_elem (translations and rotations of node k by Q_k).
+void to_local(int nn, const double *Q, const double *xg, const int32_t *nd, double *xl) {
+    for (int k = 0; k < nn; ++k)
+        for (int half = 0; half < 2; ++half)
+            for (int r = 0; r < 3; ++r) {
+                double s = 0.0;
+                for (int c = 0; c < 3; ++c) s += Q[9 * k + 3 * r + c] * xg[6 * (int64_t)nd[k] + 3 * half + c];
+                xl[6 * k + 3 * half + r] = s;
+            }
+}
+
+// ---------------------------------------------------------------------------
 // exported oracle API (test infrastructure)
 // ---------------------------------------------------------------------------
 
@@ -916,6 +1107,80 @@ void oracle_t3_stiffness_local(const double *lc6, const double *prop7, double k6
     shell_constitutive(prop7, Cm, Cb, Cs);
     double br = prop7[4];
     t3_stiffness(lc, Cm, Cb, Cs, prop7[0], prop7[6], br, br <= 1e-12 ? 0.0 : k6rot, (double(*)[18])Ke324);
+}
+
+// Element-level shell-thickness derivatives (local frame).
+void oracle_q4_generic_local(const double *lc8, double E, double nu, double h, double *Ke576, double *dKe576) {
+    double lc[4][2];
+    for (int k = 0; k < 4; ++k) { lc[k][0] = lc8[2 * k]; lc[k][1] = lc8[2 * k + 1]; }
+    q4_generic(lc, E, nu, h, (double(*)[24])Ke576, (double(*)[24])dKe576);
+}
+void oracle_t3_generic_local(const double *lc6, double E, double nu, double h, double *Ke324, double *dKe324) {
+    double lc[3][2];
+    for (int k = 0; k < 3; ++k) { lc[k][0] = lc6[2 * k]; lc[k][1] = lc6[2 * k + 1]; }
+    if (Ke324) t3_generic(lc, E, nu, h, (double(*)[18])Ke324);
+    if (dKe324) t3_generic_dkdh(lc, E, nu, h, (double(*)[18])dKe324);
+}
+
+// Shell-thickness sensitivities over a model (dKdx.jl:193-250), element
+// thickness, E and nu from each element's property record:
+//   c_q4[e] / c_t3[e] = a_e' T_e' dK_e/dh T_e b_e          (a, b: ndof)
+//   load += T_e' dK_e/dh T_e u_e over elements with mask != 0 (load: ndof,
+//   zeroed here; null masks select nothing).
+// Any output or input pointer may be null to skip that part.
+void oracle_dkdh(const jfg_model_desc *d, const double *a, const double *b, double *c_q4, double *c_t3, const double *u,
+                 const uint8_t *mask_q4, const uint8_t *mask_t3, double *load) {
+    const int64_t ndof = 6 * d->n_nodes;
+    if (load) std::fill(load, load + ndof, 0.0);
+    for (int type = 0; type < 2; ++type) {
+        const int nn = type == 0 ? 4 : 3, nd6 = 6 * nn;
+        const int64_t ne = type == 0 ? d->n_quad4 : d->n_tria3;
+        const int32_t *nodes = type == 0 ? d->quad4_nodes : d->tria3_nodes;
+        const double *prop = type == 0 ? d->quad4_prop : d->tria3_prop;
+        double *cout = type == 0 ? c_q4 : c_t3;
+        const uint8_t *mask = type == 0 ? mask_q4 : mask_t3;
+        for (int64_t e = 0; e < ne; ++e) {
+            const bool want_c = cout && a && b, want_f = load && u && mask && mask[e];
+            if (!want_c && !want_f) continue;
+            const int32_t *nd = nodes + nn * e;
+            const double *pr = prop + JFG_SHELL_PROP * e;
+            double lc[4][2], Q[36], dK[24 * 24];
+            shell_setup(d, nd, nn, lc, Q);
+            if (nn == 4) q4_generic(lc, pr[1], pr[2], pr[0], nullptr, (double(*)[24])dK);
+            else {
+                double lc3[3][2] = {{lc[0][0], lc[0][1]}, {lc[1][0], lc[1][1]}, {lc[2][0], lc[2][1]}};
+                t3_generic_dkdh(lc3, pr[1], pr[2], pr[0], (double(*)[18])dK);
+            }
+            if (want_c) {
+                double al[24], bl[24], s = 0.0;
+                to_local(nn, Q, a, nd, al);
+                to_local(nn, Q, b, nd, bl);
+                for (int i = 0; i < nd6; ++i) {
+                    double t = 0.0;
+                    for (int c = 0; c < nd6; ++c) t += dK[nd6 * i + c] * bl[c];
+                    s += al[i] * t;
+                }
+                cout[e] = s;
+            }
+            if (want_f) {
+                double ul[24], fl[24];
+                to_local(nn, Q, u, nd, ul);
+                for (int i = 0; i < nd6; ++i) {
+                    double t = 0.0;
+                    for (int c = 0; c < nd6; ++c) t += dK[nd6 * i + c] * ul[c];
+                    fl[i] = t;
+                }
+                // f_global = T' f_local, scattered to the element's dofs
+                for (int k = 0; k < nn; ++k)
+                    for (int half = 0; half < 2; ++half)
+                        for (int c = 0; c < 3; ++c) {
+                            double s = 0.0;
+                            for (int r = 0; r < 3; ++r) s += Q[9 * k + 3 * r + c] * fl[6 * k + 3 * half + r];
+                            load[6 * (int64_t)nd[k] + 3 * half + c] += s;
+                        }
+            }
+        }
+    }
 }
 
 int oracle_num_threads(void) {

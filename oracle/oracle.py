@@ -50,6 +50,10 @@ def lib():
         L.oracle_constraint_map.restype = C.c_int64
         L.oracle_num_threads.restype = C.c_int
         L.oracle_set_threads.argtypes = [C.c_int]
+        L.oracle_q4_generic_local.argtypes = [pd, C.c_double, C.c_double, C.c_double, pd, pd]
+        L.oracle_t3_generic_local.argtypes = [pd, C.c_double, C.c_double, C.c_double, pd, pd]
+        pu8 = C.POINTER(C.c_uint8)
+        L.oracle_dkdh.argtypes = [C.POINTER(JfgModelDesc), pd, pd, pd, pd, pd, pu8, pu8, pd]
         _lib = L
     return _lib
 
@@ -134,6 +138,49 @@ def t3_local(lc: np.ndarray, prop: np.ndarray, k6rot: float = 100.0) -> np.ndarr
     pd = C.POINTER(C.c_double)
     L.oracle_t3_stiffness_local(lc.ctypes.data_as(pd), prop.ctypes.data_as(pd), k6rot, out.ctypes.data_as(pd))
     return out
+
+
+def q4_generic_local(lc: np.ndarray, E: float, nu: float, h: float):
+    """(K, dK/dh) of stiffness_quad4_generic in the element frame (24 x 24 each)."""
+    L = lib()
+    lc = np.ascontiguousarray(lc, np.float64).reshape(8)
+    K, dK = np.empty((24, 24)), np.empty((24, 24))
+    pd = C.POINTER(C.c_double)
+    L.oracle_q4_generic_local(lc.ctypes.data_as(pd), E, nu, h, K.ctypes.data_as(pd), dK.ctypes.data_as(pd))
+    return K, dK
+
+
+def t3_generic_local(lc: np.ndarray, E: float, nu: float, h: float):
+    """(K, dK/dh) of stiffness_tria3_generic in the element frame (18 x 18 each)."""
+    L = lib()
+    lc = np.ascontiguousarray(lc, np.float64).reshape(6)
+    K, dK = np.empty((18, 18)), np.empty((18, 18))
+    pd = C.POINTER(C.c_double)
+    L.oracle_t3_generic_local(lc.ctypes.data_as(pd), E, nu, h, K.ctypes.data_as(pd), dK.ctypes.data_as(pd))
+    return K, dK
+
+
+def dkdh(m: ModelArrays, a=None, b=None, u=None, mask_q4=None, mask_t3=None):
+    """Shell-thickness sensitivities of the model (see oracle_dkdh): per-element
+    contractions a_e' dK_e/dh b_e (CQUAD4, CTRIA3) when a and b are given, and
+    the pseudo-load dK/dh u over the masked elements (all when no mask) when u
+    is given."""
+    L = lib()
+    desc, keep = make_desc(m)
+    pd, pu8 = C.POINTER(C.c_double), C.POINTER(C.c_uint8)
+    nq, nt, ndof = m.q4_nodes.shape[0], m.t3_nodes.shape[0], 6 * m.coords.shape[0]
+    arr = lambda x, dt: None if x is None else np.ascontiguousarray(x, dt)
+    a, b, u = arr(a, np.float64), arr(b, np.float64), arr(u, np.float64)
+    mq = arr(mask_q4 if mask_q4 is not None or u is None else np.ones(nq), np.uint8)
+    mt = arr(mask_t3 if mask_t3 is not None or u is None else np.ones(nt), np.uint8)
+    cq = np.zeros(nq) if a is not None else None
+    ct = np.zeros(nt) if a is not None else None
+    load = np.zeros(ndof) if u is not None else None
+    ptr = lambda x, t: None if x is None else x.ctypes.data_as(t)
+    L.oracle_dkdh(C.byref(desc), ptr(a, pd), ptr(b, pd), ptr(cq, pd), ptr(ct, pd), ptr(u, pd), ptr(mq, pu8), ptr(mt, pu8),
+                  ptr(load, pd))
+    del keep
+    return cq, ct, load
 
 
 def to_scipy(colptr, rowval, nzval, ndof):
