@@ -225,6 +225,36 @@ jfg_status jfg_ff_fetch(jfg_model *m, int64_t *colptr, int64_t *rowval, double *
 /* Device pointers to the last extraction (valid until the next one). */
 jfg_status jfg_ff_device_arrays(jfg_model *m, const int64_t **colptr, const int64_t **rowval, const double **nzval);
 
+/* ---- Shell-thickness sensitivities dK/dh ---------------------------------
+ * Replace the shell_thickness branch of compute_dKdx_u
+ * (src/solver/dKdx.jl:193-250, _dKdx_u_shell_thickness_ad_forward and
+ * _shell_thickness_dKe_forward_ad) and the per-element loop of
+ * _compliance_and_sensitivity (src/solver/optimize_thickness.jl:420-441).
+ * The element is the reference's sensitivity element, stiffness_quad4_generic
+ * / stiffness_tria3_generic (src/FEMKernels.jl:1473-1656, :7113-7123: bend
+ * ratio 1, TS/T 5/6, K6ROT 100, G = E / 2(1 + nu)), with each element's own
+ * thickness, E and nu; the derivative is exact (what forward-mode AD gives),
+ * not a difference quotient.  Vectors are ndof long (6 dofs per node, the
+ * handle's node order); T_e holds the element frame and node CD frames.
+ *
+ * jfg_dkdh_contract: for every CQUAD4 e, c_q4[e] = a_e' T_e' dK_e/dh T_e b_e,
+ * and likewise c_t3 for every CTRIA3 (a = b = u gives u' dK_e/dh u, the
+ * compliance sensitivity -dC/dh_e; a = b = phi the buckling one).  Either
+ * output may be NULL.
+ * jfg_dkdh_load: the pseudo-load sum_e T_e' dK_e/dh T_e u_e over the elements
+ * whose mask byte is nonzero (one byte per element; a NULL mask selects every
+ * element of that type), summed per dof in a fixed order.
+ * The _device forms take device pointers and run asynchronously on the
+ * handle's stream (jfg_set_stream); jfg_dkdh_load_device reuses the handle's
+ * orig_diag staging, so it must not overlap a K assembly of the same handle.
+ * The host forms copy in and out and return when done. */
+jfg_status jfg_dkdh_contract(jfg_model *m, const double *a, const double *b, double *c_q4, double *c_t3);
+jfg_status jfg_dkdh_load(jfg_model *m, const double *u, const uint8_t *mask_q4, const uint8_t *mask_t3, double *load);
+jfg_status jfg_dkdh_contract_device(jfg_model *m, const double *a_dev, const double *b_dev, double *c_q4_dev,
+                                    double *c_t3_dev);
+jfg_status jfg_dkdh_load_device(jfg_model *m, const double *u_dev, const uint8_t *mask_q4_dev, const uint8_t *mask_t3_dev,
+                                double *load_dev);
+
 /* ---- Serving: a device-resident request loop over model families --------
  * Replaces the reference's optimisation worker loop
  * (tools/jfem_worker_jsonl.jl:132-148, manifest_batch_core.jl:283-409), which

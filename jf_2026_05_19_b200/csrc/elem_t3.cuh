@@ -72,6 +72,130 @@ __device__ __forceinline__ void t3_quad_coords(int q, const double x[3], const d
     lq[3][0] = (xp + xc) / 2; lq[3][1] = (yp + yc) / 2;
 }
 
+// Plate phases of the CTRIA3 kernels (team of 16 lanes, mask tm), shared by
+// the stiffness and the thickness-sensitivity kernels.
+
+// Virtual-quad point data and the MacNeal compliance blocks W of each quad.
+__device__ __forceinline__ void t3_plate_points(T3KShared &S, int tl, unsigned tm, const double x[3], const double y[3],
+                                                double cs, double cb, bool macneal) {
+    // Phase 1: virtual-quad points (27 items: quad q = it / 9, point
+    // it % 9 -- Gauss points, centre, MacNeal sampling points) and the
+    // MacNeal scalars of each quad (items 27-29).
+    for (int it = tl; it < 30; it += T3_TEAM) {
+        const int q = it < 27 ? it / 9 : it - 27, pt = it - 9 * (it / 9);
+        double lq[4][2];
+        t3_quad_coords(q, x, y, lq);
+        if (it < 27) {
+            double r, s, dx[4], dy[4], iJ[4];
+            q4_point_rs(pt, r, s);
+            const bool mac = pt >= 5;
+            const double det = q4_point_derivs(lq, r, s, mac, dx, dy, iJ);
+            if (!mac) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) { S.u.q.dNx[q][pt][k] = dx[k]; S.u.q.dNy[q][pt][k] = dy[k]; }
+                if (pt < 4) { const double a = fabs(det); S.u.q.wdet[q][pt] = a < 1e-12 ? 1e-12 : a; }
+            } else {
+                const int l = pt - 5;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) S.u.q.Dd[q][l][k] = l < 2 ? dx[k] : dy[k];
+                S.u.q.ivd[q][l] = macneal_ivd(det, cs);
+            }
+        } else {
+            double zs[4];
+            macneal_zs(lq, cb, zs);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) S.u.q.zs[q][i] = zs[i];
+        }
+    }
+    __syncwarp(tm);
+    if (macneal && tl < 3) macneal_w(S.u.q.ivd[tl], S.u.q.zs[tl], S.u.q.W[tl]);
+    __syncwarp(tm);
+}
+
+// Plate 3x3 block of every (virtual quad, node pair) into S.Pb.
+__device__ __forceinline__ void t3_plate_blocks(T3KShared &S, int tl, unsigned tm, double cb, double nu, double gam,
+                                                bool macneal) {
+    // Phase 2: plate 3x3 block of every (virtual quad, node pair):
+    // bending with the twist row (no bending incompatible modes in the
+    // macro quads) plus MacNeal's shear.
+    for (int it = tl; it < 30; it += T3_TEAM) {
+        const int q = it / 10, pp = it - 10 * q;
+        int ka, kb;
+        q4_pair(pp, ka, kb);
+        double v[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        bend_pair(S.u.q.dNx[q], S.u.q.dNy[q], S.u.q.wdet[q], ka, kb, cb, nu, gam, v);
+        if (macneal) macneal_pair(S.u.q.Dd[q], S.u.q.W[q], ka, kb, v);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) S.Pb[q][pp][3 * i + j] = v[i][j];
+    }
+    __syncwarp(tm);
+}
+
+// Condensation of the internal dofs: X = Kii^-1 Kie into S.u.c.X.
+__device__ __forceinline__ void t3_condense(T3KShared &S, int tl, unsigned tm) {
+    // Phase 3: lane r < 12 holds row r of [Kii | Kie] (internal dof r =
+    // macro node 3 + r/3, component r%3), summed over quads in order.
+    const bool act = tl < 12;
+    const int nA = 3 + tl / 3, ci = tl - 3 * (tl / 3);
+    double row[21];
+#pragma unroll
+    for (int c = 0; c < 21; ++c) row[c] = 0.0;
+    if (act) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            int la = -1;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (t3_quad_node(q, k) == nA) la = k;
+            if (la >= 0) {
+#pragma unroll
+                for (int kb = 0; kb < 4; ++kb) {
+                    const int nB = t3_quad_node(q, kb);
+                    const int cb0 = nB >= 3 ? 3 * (nB - 3) : 12 + 3 * nB;
+                    const bool tr = la > kb;
+                    const int pid = tr ? packed_index(kb, la, 4) : packed_index(la, kb, 4);
+#pragma unroll
+                    for (int cj = 0; cj < 3; ++cj) row[cb0 + cj] += S.Pb[q][pid][tr ? 3 * cj + ci : 3 * ci + cj];
+                }
+            }
+        }
+    }
+    int pos = act ? tl : 64;
+    double diag = 1.0;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+        const bool cand_ok = act && pos >= k;
+        double cv = cand_ok ? fabs(row[k]) : -1.0;
+        int cp = cand_ok ? pos : 64;
+#pragma unroll
+        for (int off = 8; off > 0; off >>= 1) {
+            const double ov = __shfl_xor_sync(tm, cv, off, 16);
+            const int op = __shfl_xor_sync(tm, cp, off, 16);
+            if (ov > cv || (ov == cv && op < cp)) { cv = ov; cp = op; }
+        }
+        const bool is_piv = act && pos == cp;
+        const unsigned bal = __ballot_sync(tm, is_piv) & tm;
+        const int src = (__ffs(bal) - 1) & 15;
+        if (act && pos == k) pos = cp;  // LU row swap of positions k and cp
+        if (is_piv) pos = k;
+        const double akk = __shfl_sync(tm, row[k], src, 16);
+        if (is_piv) diag = akk;
+        const double f = (act && !is_piv) ? row[k] / akk : 0.0;
+#pragma unroll
+        for (int j = k + 1; j < 21; ++j) {
+            const double pj = __shfl_sync(tm, row[j], src, 16);
+            row[j] -= f * pj;
+        }
+    }
+    __syncwarp(tm);  // every lane is past its last read of the quad data
+    if (act && pos < 12)
+#pragma unroll
+        for (int c = 0; c < 9; ++c) S.u.c.X[pos][c] = row[12 + c] / diag;
+    __syncwarp(tm);
+}
+
 __global__ void __launch_bounds__(T3_THREADS, 5) t3_k_kernel(int64_t nt, const int32_t *__restrict__ nodes,
                                                          const double *__restrict__ prop,
                                                          const double *__restrict__ coords,
@@ -133,115 +257,9 @@ __global__ void __launch_bounds__(T3_THREADS, 5) t3_k_kernel(int64_t nt, const i
     }
 
     if (plate) {
-        // Phase 1: virtual-quad points (27 items: quad q = it / 9, point
-        // it % 9 -- Gauss points, centre, MacNeal sampling points) and the
-        // MacNeal scalars of each quad (items 27-29).
-        for (int it = tl; it < 30; it += T3_TEAM) {
-            const int q = it < 27 ? it / 9 : it - 27, pt = it - 9 * (it / 9);
-            double lq[4][2];
-            t3_quad_coords(q, x, y, lq);
-            if (it < 27) {
-                double r, s, dx[4], dy[4], iJ[4];
-                q4_point_rs(pt, r, s);
-                const bool mac = pt >= 5;
-                const double det = q4_point_derivs(lq, r, s, mac, dx, dy, iJ);
-                if (!mac) {
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) { S.u.q.dNx[q][pt][k] = dx[k]; S.u.q.dNy[q][pt][k] = dy[k]; }
-                    if (pt < 4) { const double a = fabs(det); S.u.q.wdet[q][pt] = a < 1e-12 ? 1e-12 : a; }
-                } else {
-                    const int l = pt - 5;
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) S.u.q.Dd[q][l][k] = l < 2 ? dx[k] : dy[k];
-                    S.u.q.ivd[q][l] = macneal_ivd(det, cs);
-                }
-            } else {
-                double zs[4];
-                macneal_zs(lq, cb, zs);
-#pragma unroll
-                for (int i = 0; i < 4; ++i) S.u.q.zs[q][i] = zs[i];
-            }
-        }
-        __syncwarp(tm);
-        if (macneal && tl < 3) macneal_w(S.u.q.ivd[tl], S.u.q.zs[tl], S.u.q.W[tl]);
-        __syncwarp(tm);
-
-        // Phase 2: plate 3x3 block of every (virtual quad, node pair):
-        // bending with the twist row (no bending incompatible modes in the
-        // macro quads) plus MacNeal's shear.
-        for (int it = tl; it < 30; it += T3_TEAM) {
-            const int q = it / 10, pp = it - 10 * q;
-            int ka, kb;
-            q4_pair(pp, ka, kb);
-            double v[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-            bend_pair(S.u.q.dNx[q], S.u.q.dNy[q], S.u.q.wdet[q], ka, kb, cb, nu, gam, v);
-            if (macneal) macneal_pair(S.u.q.Dd[q], S.u.q.W[q], ka, kb, v);
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) S.Pb[q][pp][3 * i + j] = v[i][j];
-        }
-        __syncwarp(tm);
-
-        // Phase 3: lane r < 12 holds row r of [Kii | Kie] (internal dof r =
-        // macro node 3 + r/3, component r%3), summed over quads in order.
-        const bool act = tl < 12;
-        const int nA = 3 + tl / 3, ci = tl - 3 * (tl / 3);
-        double row[21];
-#pragma unroll
-        for (int c = 0; c < 21; ++c) row[c] = 0.0;
-        if (act) {
-#pragma unroll
-            for (int q = 0; q < 3; ++q) {
-                int la = -1;
-#pragma unroll
-                for (int k = 0; k < 4; ++k)
-                    if (t3_quad_node(q, k) == nA) la = k;
-                if (la >= 0) {
-#pragma unroll
-                    for (int kb = 0; kb < 4; ++kb) {
-                        const int nB = t3_quad_node(q, kb);
-                        const int cb0 = nB >= 3 ? 3 * (nB - 3) : 12 + 3 * nB;
-                        const bool tr = la > kb;
-                        const int pid = tr ? packed_index(kb, la, 4) : packed_index(la, kb, 4);
-#pragma unroll
-                        for (int cj = 0; cj < 3; ++cj) row[cb0 + cj] += S.Pb[q][pid][tr ? 3 * cj + ci : 3 * ci + cj];
-                    }
-                }
-            }
-        }
-        int pos = act ? tl : 64;
-        double diag = 1.0;
-#pragma unroll
-        for (int k = 0; k < 12; ++k) {
-            const bool cand_ok = act && pos >= k;
-            double cv = cand_ok ? fabs(row[k]) : -1.0;
-            int cp = cand_ok ? pos : 64;
-#pragma unroll
-            for (int off = 8; off > 0; off >>= 1) {
-                const double ov = __shfl_xor_sync(tm, cv, off, 16);
-                const int op = __shfl_xor_sync(tm, cp, off, 16);
-                if (ov > cv || (ov == cv && op < cp)) { cv = ov; cp = op; }
-            }
-            const bool is_piv = act && pos == cp;
-            const unsigned bal = __ballot_sync(tm, is_piv) & tm;
-            const int src = (__ffs(bal) - 1) & 15;
-            if (act && pos == k) pos = cp;  // LU row swap of positions k and cp
-            if (is_piv) pos = k;
-            const double akk = __shfl_sync(tm, row[k], src, 16);
-            if (is_piv) diag = akk;
-            const double f = (act && !is_piv) ? row[k] / akk : 0.0;
-#pragma unroll
-            for (int j = k + 1; j < 21; ++j) {
-                const double pj = __shfl_sync(tm, row[j], src, 16);
-                row[j] -= f * pj;
-            }
-        }
-        __syncwarp(tm);  // every lane is past its last read of the quad data
-        if (act && pos < 12)
-#pragma unroll
-            for (int c = 0; c < 9; ++c) S.u.c.X[pos][c] = row[12 + c] / diag;
-        __syncwarp(tm);
+        t3_plate_points(S, tl, tm, x, y, cs, cb, macneal);
+        t3_plate_blocks(S, tl, tm, cb, nu, gam, macneal);
+        t3_condense(S, tl, tm);
 
         // Phase 4: Kcond = Kee - Kei X (Kee, Kei from the corner's own quad).
         for (int it = tl; it < 81; it += T3_TEAM) {

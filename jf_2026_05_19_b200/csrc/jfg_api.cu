@@ -35,6 +35,7 @@
 #include "elem_bar.cuh"
 #include "elem_q4.cuh"
 #include "elem_t3.cuh"
+#include "elem_dkdh.cuh"
 
 using namespace jfg;
 
@@ -89,6 +90,8 @@ struct jfg_model {
     int64_t dslot_q4 = 0, dslot_t3 = 0, dslot_bar = 0;
     int32_t *d_dseg = nullptr;           // ndof + 1
     double *d_dstaging = nullptr;
+    double *d_dk = nullptr;             // host-buffer dK/dh calls: a, b (or u, load), c_q4, c_t3
+    uint8_t *d_dk_mask = nullptr;
     int64_t n_dcontrib = 0;
     // work buffers
     double *d_nz = nullptr, *d_u = nullptr, *d_diag = nullptr, *d_max = nullptr, *d_h = nullptr;
@@ -1576,6 +1579,89 @@ jfg_status jfg_assemble_kg(jfg_model *m, const double *u_global, double *nzval) 
     if (nzval) CK(cudaMemcpyAsync(nzval, m->d_nz, sizeof(double) * m->nnz, cudaMemcpyDeviceToHost, m->stream));
     CK(cudaStreamSynchronize(m->stream));
     return finish_timing(m);
+}
+
+// ---------------------------------------------------------------------------
+// shell-thickness sensitivities (dKdx.jl:193-250)
+// ---------------------------------------------------------------------------
+
+jfg_status jfg_dkdh_contract_device(jfg_model *m, const double *a_dev, const double *b_dev, double *c_q4_dev,
+                                    double *c_t3_dev) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    if (!a_dev || !b_dev) return fail(m, JFG_ERR_INVALID, "null vector");
+    if (m->nq && c_q4_dev) {
+        q4_dkdh_contract_kernel<<<(unsigned)cdiv(m->nq, 128), 128, 0, m->stream>>>(m->nq, m->d_q4n, m->d_q4p, m->d_coords,
+                                                                                  m->d_nodeR, a_dev, b_dev, c_q4_dev);
+        CK(cudaGetLastError());
+    }
+    if (m->nt && c_t3_dev) {
+        t3_dkdh_kernel<false><<<(unsigned)cdiv(m->nt, T3D_ELEMS), 32 * T3D_WARPS, 0, m->stream>>>(
+            m->nt, m->d_t3n, m->d_t3p, m->d_coords, m->d_nodeR, a_dev, b_dev, c_t3_dev, nullptr, nullptr, nullptr);
+        CK(cudaGetLastError());
+    }
+    return JFG_OK;
+}
+
+jfg_status jfg_dkdh_load_device(jfg_model *m, const double *u_dev, const uint8_t *mask_q4_dev, const uint8_t *mask_t3_dev,
+                                double *load_dev) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    if (!u_dev || !load_dev) return fail(m, JFG_ERR_INVALID, "null vector");
+    // element contributions go to the orig_diag staging (one slot per element
+    // dof, bars left at zero) and are summed per dof in slot order
+    if (m->n_dcontrib) CK(cudaMemsetAsync(m->d_dstaging, 0, sizeof(double) * m->n_dcontrib, m->stream));
+    if (m->nq) {
+        q4_dkdh_load_kernel<<<(unsigned)cdiv(m->nq, 128), 128, 0, m->stream>>>(
+            m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, u_dev, mask_q4_dev, m->d_dslot + m->dslot_q4, m->d_dstaging);
+        CK(cudaGetLastError());
+    }
+    if (m->nt) {
+        t3_dkdh_kernel<true><<<(unsigned)cdiv(m->nt, T3D_ELEMS), 32 * T3D_WARPS, 0, m->stream>>>(
+            m->nt, m->d_t3n, m->d_t3p, m->d_coords, m->d_nodeR, u_dev, nullptr, nullptr, mask_t3_dev, m->d_dslot + m->dslot_t3,
+            m->d_dstaging);
+        CK(cudaGetLastError());
+    }
+    diag_reduce_kernel<<<(unsigned)cdiv(m->ndof, 256), 256, 0, m->stream>>>(m->ndof, m->d_dseg, m->d_dstaging, load_dev, 0);
+    CK(cudaGetLastError());
+    return JFG_OK;
+}
+
+static jfg_status dk_buffers(jfg_model *m) {
+    if (!m->d_dk) CK(dalloc(m, &m->d_dk, 2 * m->ndof + m->nq + m->nt));
+    if (!m->d_dk_mask) CK(dalloc(m, &m->d_dk_mask, std::max<int64_t>(m->nq + m->nt, 1)));
+    return JFG_OK;
+}
+
+jfg_status jfg_dkdh_contract(jfg_model *m, const double *a, const double *b, double *c_q4, double *c_t3) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    if (!a || !b) return fail(m, JFG_ERR_INVALID, "null vector");
+    jfg_status st = dk_buffers(m);
+    if (st) return st;
+    double *da = m->d_dk, *db = da + m->ndof, *dc = db + m->ndof;
+    CK(cudaMemcpyAsync(da, a, sizeof(double) * m->ndof, cudaMemcpyHostToDevice, m->stream));
+    CK(cudaMemcpyAsync(db, b, sizeof(double) * m->ndof, cudaMemcpyHostToDevice, m->stream));
+    st = jfg_dkdh_contract_device(m, da, db, dc, dc + m->nq);
+    if (st) return st;
+    if (c_q4 && m->nq) CK(cudaMemcpyAsync(c_q4, dc, sizeof(double) * m->nq, cudaMemcpyDeviceToHost, m->stream));
+    if (c_t3 && m->nt) CK(cudaMemcpyAsync(c_t3, dc + m->nq, sizeof(double) * m->nt, cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    return JFG_OK;
+}
+
+jfg_status jfg_dkdh_load(jfg_model *m, const double *u, const uint8_t *mask_q4, const uint8_t *mask_t3, double *load) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    if (!u || !load) return fail(m, JFG_ERR_INVALID, "null vector");
+    jfg_status st = dk_buffers(m);
+    if (st) return st;
+    double *du = m->d_dk, *dl = du + m->ndof;
+    uint8_t *mq = m->d_dk_mask, *mt = m->d_dk_mask + m->nq;
+    CK(cudaMemcpyAsync(du, u, sizeof(double) * m->ndof, cudaMemcpyHostToDevice, m->stream));
+    if (mask_q4 && m->nq) CK(cudaMemcpyAsync(mq, mask_q4, m->nq, cudaMemcpyHostToDevice, m->stream));
+    if (mask_t3 && m->nt) CK(cudaMemcpyAsync(mt, mask_t3, m->nt, cudaMemcpyHostToDevice, m->stream));
+    st = jfg_dkdh_load_device(m, du, mask_q4 ? mq : nullptr, mask_t3 ? mt : nullptr, dl);
+    if (st) return st;
+    CK(cudaMemcpyAsync(load, dl, sizeof(double) * m->ndof, cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    return JFG_OK;
 }
 
 jfg_status jfg_update_properties(jfg_model *m, const double *quad4_h, const double *tria3_h) {

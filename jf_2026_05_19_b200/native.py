@@ -23,7 +23,8 @@ EXPORTS = ("jfg_model_create", "jfg_pattern", "jfg_pattern_fill", "jfg_assemble_
            "jfg_assemble_k_device", "jfg_assemble_kg_device", "jfg_update_properties", "jfg_constraint_map",
            "jfg_set_stream", "jfg_last_timing", "jfg_kernel_timing", "jfg_timing_accumulated", "jfg_model_stats", "jfg_model_counts", "jfg_batch_workspace_bytes",
            "jfg_batch_reserve", "jfg_assemble_batch_device", "jfg_ff_set_free", "jfg_ff_extract_device",
-           "jfg_ff_fetch", "jfg_ff_device_arrays", "jfg_server_create", "jfg_server_submit", "jfg_server_wait",
+           "jfg_ff_fetch", "jfg_ff_device_arrays", "jfg_dkdh_contract", "jfg_dkdh_load",
+           "jfg_dkdh_contract_device", "jfg_dkdh_load_device", "jfg_server_create", "jfg_server_submit", "jfg_server_wait",
            "jfg_server_result", "jfg_server_release", "jfg_server_stats", "jfg_server_family_batch",
            "jfg_server_hold", "jfg_server_last_error", "jfg_server_destroy", "jfg_assemble_k_quad4_noalloc", "jfg_model_destroy", "jfg_last_error",
            "jfg_version")
@@ -82,6 +83,11 @@ def load(path: str = LIB_PATH):
                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.jfg_model_counts.argtypes = [C.c_void_p, _pi64]
     L.jfg_ff_set_free.argtypes = [C.c_void_p, _pi64, C.c_int64]
+    _pu8 = C.POINTER(C.c_uint8)
+    L.jfg_dkdh_contract.argtypes = [C.c_void_p, _pd, _pd, _pd, _pd]
+    L.jfg_dkdh_load.argtypes = [C.c_void_p, _pd, _pu8, _pu8, _pd]
+    L.jfg_dkdh_contract_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.jfg_dkdh_load_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.jfg_ff_extract_device.argtypes = [C.c_void_p, C.c_void_p, _pi64, _pd, _pd]
     L.jfg_ff_fetch.argtypes = [C.c_void_p, _pi64, _pi64, _pd]
     L.jfg_ff_device_arrays.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
@@ -240,6 +246,35 @@ class GpuModel:
         val = np.empty(nnz.value)
         self._check(self.L.jfg_ff_fetch(self.h, _ptr(colptr, _pi64), _ptr(rowval, _pi64), _ptr(val, _pd)))
         return colptr, rowval, val, a.value, b.value
+
+    def dkdh_contract(self, a: np.ndarray, b: np.ndarray):
+        """Per-element a_e' dK_e/dh b_e of the shell-thickness sensitivity element:
+        (c_q4, c_t3) arrays (jfg_dkdh_contract)."""
+        a = np.ascontiguousarray(a, np.float64)
+        b = np.ascontiguousarray(b, np.float64)
+        nq, nt = self.counts[1], self.counts[2]
+        cq, ct = np.zeros(nq), np.zeros(nt)
+        self._check(self.L.jfg_dkdh_contract(self.h, _ptr(a, _pd), _ptr(b, _pd), _ptr(cq, _pd), _ptr(ct, _pd)))
+        return cq, ct
+
+    def dkdh_load(self, u: np.ndarray, mask_q4: Optional[np.ndarray] = None, mask_t3: Optional[np.ndarray] = None):
+        """Pseudo-load sum_e T' dK_e/dh T u_e over the masked elements (None = all of that type)."""
+        u = np.ascontiguousarray(u, np.float64)
+        pu8 = C.POINTER(C.c_uint8)
+        mq = None if mask_q4 is None else np.ascontiguousarray(mask_q4, np.uint8)
+        mt = None if mask_t3 is None else np.ascontiguousarray(mask_t3, np.uint8)
+        out = np.empty(self.ndof)
+        self._check(self.L.jfg_dkdh_load(self.h, _ptr(u, _pd), None if mq is None else mq.ctypes.data_as(pu8),
+                                         None if mt is None else mt.ctypes.data_as(pu8), _ptr(out, _pd)))
+        return out
+
+    def dkdh_contract_device(self, a_ptr: int, b_ptr: int, cq_ptr: Optional[int], ct_ptr: Optional[int]):
+        self._check(self.L.jfg_dkdh_contract_device(self.h, C.c_void_p(a_ptr), C.c_void_p(b_ptr), C.c_void_p(cq_ptr or None),
+                                                    C.c_void_p(ct_ptr or None)))
+
+    def dkdh_load_device(self, u_ptr: int, mq_ptr: Optional[int], mt_ptr: Optional[int], out_ptr: int):
+        self._check(self.L.jfg_dkdh_load_device(self.h, C.c_void_p(u_ptr), C.c_void_p(mq_ptr or None),
+                                                C.c_void_p(mt_ptr or None), C.c_void_p(out_ptr)))
 
     def set_stream(self, stream_ptr: int):
         self._check(self.L.jfg_set_stream(self.h, C.c_void_p(stream_ptr or None)))
