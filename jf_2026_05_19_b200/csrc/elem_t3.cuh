@@ -13,10 +13,11 @@
 // centroid 6.  No virtual quad holds two corners, so Kee is block diagonal
 // and every Kei entry comes from the one quad that holds the corner.  The
 // internal solve lu(Kii) \ Kie runs as Gauss-Jordan elimination with one row
-// of [Kii | Kie] per lane in registers: pivot choice, row positions and the
-// forward elimination are those of LU with partial pivoting (max |a_ik|,
-// first position on ties); eliminating above the pivot as well replaces the
-// back substitution.
+// of [Kii | Kie] per lane in registers, pivoting on the diagonal: Kii, the
+// plate stiffness of the midside and centroid dofs with the corners held, is
+// symmetric positive definite, so the reference's row exchanges change only
+// the rounding.  Eliminating above the pivot as well replaces the back
+// substitution.
 //
 // KG: one thread per (element, node pair).  CST membrane resultant of stress_strain_tria3
 // (FEMKernels.jl:7391-7404) and geometric_stiffness_tria3's non-curvature
@@ -162,37 +163,23 @@ __device__ __forceinline__ void t3_condense(T3KShared &S, int tl, unsigned tm) {
             }
         }
     }
-    int pos = act ? tl : 64;
     double diag = 1.0;
 #pragma unroll
     for (int k = 0; k < 12; ++k) {
-        const bool cand_ok = act && pos >= k;
-        double cv = cand_ok ? fabs(row[k]) : -1.0;
-        int cp = cand_ok ? pos : 64;
-#pragma unroll
-        for (int off = 8; off > 0; off >>= 1) {
-            const double ov = __shfl_xor_sync(tm, cv, off, 16);
-            const int op = __shfl_xor_sync(tm, cp, off, 16);
-            if (ov > cv || (ov == cv && op < cp)) { cv = ov; cp = op; }
-        }
-        const bool is_piv = act && pos == cp;
-        const unsigned bal = __ballot_sync(tm, is_piv) & tm;
-        const int src = (__ffs(bal) - 1) & 15;
-        if (act && pos == k) pos = cp;  // LU row swap of positions k and cp
-        if (is_piv) pos = k;
-        const double akk = __shfl_sync(tm, row[k], src, 16);
+        const bool is_piv = tl == k;  // diagonal pivot: the row of lane k
+        const double akk = __shfl_sync(tm, row[k], k, 16);
         if (is_piv) diag = akk;
         const double f = (act && !is_piv) ? row[k] / akk : 0.0;
 #pragma unroll
         for (int j = k + 1; j < 21; ++j) {
-            const double pj = __shfl_sync(tm, row[j], src, 16);
+            const double pj = __shfl_sync(tm, row[j], k, 16);
             row[j] -= f * pj;
         }
     }
     __syncwarp(tm);  // every lane is past its last read of the quad data
-    if (act && pos < 12)
+    if (act)
 #pragma unroll
-        for (int c = 0; c < 9; ++c) S.u.c.X[pos][c] = row[12 + c] / diag;
+        for (int c = 0; c < 9; ++c) S.u.c.X[tl][c] = row[12 + c] / diag;
     __syncwarp(tm);
 }
 
