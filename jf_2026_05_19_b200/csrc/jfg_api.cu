@@ -477,43 +477,48 @@ __device__ __forceinline__ void block_row_sum(const double *__restrict__ staging
     }
 }
 
-// KG rows (12 values per slot plus 27 per bar pair, see blk_entry): shell
-// contributions hold only their translation 3x3, bar contributions [r, b)
-// also their three rotation sub-blocks.  Row i < 3 sums columns 0-2 over
-// every slot and columns 3-5 over the bar slots; row i >= 3 sums the bar
-// slots only.  The nonzero terms are added in slot order.
-__device__ __forceinline__ void block_row_sum_kg(const double *__restrict__ staging, const double *__restrict__ kg_rot,
-                                                 const int32_t *__restrict__ slot_bar, int32_t a, int32_t r, int32_t b,
-                                                 int i, double s[6]) {
+// KG rows (12 values per slot plus 27 per bar pair, see blk_entry) of two
+// blocks at once: shell contributions hold only their translation 3x3, bar
+// contributions [rb, b) also their three rotation sub-blocks.  Row i < 3
+// sums columns 0-2 over every slot and columns 3-5 over the bar slots; row
+// i >= 3 sums the bar slots only.  The translation rows of both blocks are
+// read in interleaved batches of four slots (loads issued together, slots
+// past a block's end add +0.0); each block's terms are added in slot order.
+__device__ __forceinline__ void block_rows_sum_kg(const double *__restrict__ staging, const double *__restrict__ kg_rot,
+                                                  const int32_t *__restrict__ slot_bar, const int32_t a[2], const int32_t rb[2],
+                                                  const int32_t b[2], int i, double s[2][6]) {
     const int i3 = i < 3 ? i : i - 3;
     if (i < 3) {
-        // batches of four slots, loads issued together; slots past the end
-        // add +0.0
-        for (int32_t q = a; q < b; q += 4) {
-            double x[4][3];
+        const int32_t len = max(b[0] - a[0], b[1] - a[1]);
+        for (int32_t t = 0; t < len; t += 4) {
+            double x[2][4][3];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                x[u][0] = x[u][1] = x[u][2] = 0.0;
-                if (q + u < b) {
-                    const double *p = staging + 12 * (int64_t)(q + u) + 3 * i3;
-                    x[u][0] = __ldg(p); x[u][1] = __ldg(p + 1); x[u][2] = __ldg(p + 2);
+            for (int m = 0; m < 2; ++m)
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int32_t q = a[m] + t + u;
+                    x[m][u][0] = x[m][u][1] = x[m][u][2] = 0.0;
+                    if (q < b[m]) {
+                        const double *p = staging + 12 * (int64_t)q + 3 * i3;
+                        x[m][u][0] = __ldg(p); x[m][u][1] = __ldg(p + 1); x[m][u][2] = __ldg(p + 2);
+                    }
                 }
-            }
 #pragma unroll
-            for (int u = 0; u < 4; ++u) { s[0] += x[u][0]; s[1] += x[u][1]; s[2] += x[u][2]; }
+            for (int m = 0; m < 2; ++m)
+#pragma unroll
+                for (int u = 0; u < 4; ++u) { s[m][0] += x[m][u][0]; s[m][1] += x[m][u][1]; s[m][2] += x[m][u][2]; }
         }
     }
-    for (int32_t q = r; q < b; ++q) {
-        const double *p = kg_rot + 27 * (int64_t)__ldg(slot_bar + q) + 3 * i3;
-        if (i >= 3) { s[0] += __ldg(p + 9); s[1] += __ldg(p + 10); s[2] += __ldg(p + 11); }
-        const int o3 = i < 3 ? 0 : 18;  // translation-rotation / rotation-rotation rows
-        s[3] += __ldg(p + o3); s[4] += __ldg(p + o3 + 1); s[5] += __ldg(p + o3 + 2);
-    }
+#pragma unroll
+    for (int m = 0; m < 2; ++m)
+        for (int32_t q = rb[m]; q < b[m]; ++q) {
+            const double *p = kg_rot + 27 * (int64_t)__ldg(slot_bar + q) + 3 * i3;
+            if (i >= 3) { s[m][0] += __ldg(p + 9); s[m][1] += __ldg(p + 10); s[m][2] += __ldg(p + 11); }
+            const int o3 = i < 3 ? 0 : 18;  // translation-rotation / rotation-rotation rows
+            s[m][3] += __ldg(p + o3); s[m][4] += __ldg(p + o3 + 1); s[m][5] += __ldg(p + o3 + 2);
+        }
 }
 
-// Writes of one summed block: column i goes to column i of the rows 6A+r,
-// row i to column i of the mirrored rows 6B+j, so in both writes the six
-// threads of a block store six consecutive values of one CSC row.
 __device__ __forceinline__ void block_write(int64_t k, int i, const double sr[6], const double sc[6],
                                             const int32_t *__restrict__ A, const int32_t *__restrict__ B,
                                             const int32_t *__restrict__ offAB, const int32_t *__restrict__ offBA,
@@ -556,9 +561,11 @@ __global__ void __launch_bounds__(32 * kRedWarps, 4) block_reduce_kernel(int64_t
         const int32_t a0 = __ldg(seg + k0), b0 = __ldg(seg + k0 + 1);
         const int32_t a1 = two ? __ldg(seg + k1) : 0, b1 = two ? __ldg(seg + k1 + 1) : 0;
         if (KG) {
-            const int32_t r0 = __ldg(rot + k0), r1 = two ? __ldg(rot + k1) : 0;
-            block_row_sum_kg(staging, staging + kg_rot_off, slot_bar, a0, r0, b0, i, s0);
-            block_row_sum_kg(staging, staging + kg_rot_off, slot_bar, a1, r1, b1, i, s1);
+            const int32_t aa[2] = {a0, a1}, bb[2] = {b0, b1}, rr[2] = {__ldg(rot + k0), two ? __ldg(rot + k1) : 0};
+            double ss[2][6] = {{0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}};
+            block_rows_sum_kg(staging, staging + kg_rot_off, slot_bar, aa, rr, bb, i, ss);
+#pragma unroll
+            for (int c = 0; c < 6; ++c) { s0[c] = ss[0][c]; s1[c] = ss[1][c]; }
         } else {
             block_row_sum(staging, a0, b0, i, s0);
             block_row_sum(staging, a1, b1, i, s1);
