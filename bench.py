@@ -273,10 +273,14 @@ def run_reference(args):
     el = time.perf_counter() - t0
     v = m.n_elements * args.steps / el
     sample = f"{m.name}: {m.n_elements} elements per step, barrel element mix"
+    # the config is the GPU arm's workload; each timed step is the bounded sample above
+    full = make_model(args.workload, seed=0)
+    config = dict(workload_config(full, args.workload, args.gpus), parallelism=f"replicas x{args.gpus}",
+                  timed_sample=m.name)
     line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded barrel deck)",
-            "config": workload_config(m, "barrel_sample", 1),
+            "config": config,
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
                              "note": "reference is Julia 1.12 (absent here); C++ restatement of its algorithm"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
