@@ -93,3 +93,19 @@ def test_load_and_contraction_agree_and_device_forms_match(cuda_device):
         torch.cuda.synchronize()
         assert np.array_equal(dcq.cpu().numpy(), cq) and np.array_equal(dct.cpu().numpy(), ct)
         assert np.array_equal(dl.cpu().numpy(), load)
+
+
+def test_sensitivities_follow_thickness_updates(cuda_device):
+    """After jfg_update_properties (the optimiser's thickness step) the contractions use the
+    new thicknesses, as a handle built from the updated deck does."""
+    m = DECKS["barrel_small"]
+    rng = np.random.default_rng(21)
+    hq = rng.uniform(0.8, 3.0, m.q4_nodes.shape[0])
+    ht = rng.uniform(0.8, 3.0, m.t3_nodes.shape[0])
+    u = decks.smooth_displacement(m, seed=22)
+    oq, ot, _ = O.dkdh(m.with_thickness(hq, ht), a=u, b=u)
+    with native.GpuModel(m) as g:
+        g.dkdh_contract(u, u)
+        g.update_thickness(hq, ht)
+        cq, ct = g.dkdh_contract(u, u)
+    assert _close(cq, oq, Q4_TOL) and _close(ct, ot, T3_TOL)
