@@ -538,10 +538,10 @@ __device__ __forceinline__ void block_write(int64_t k, int i, const double sr[6]
 // 5w+g, lanes 30-31 idle) and the same five blocks + half.  Each thread sums
 // row i of its blocks; the rows meet in shared memory so that every thread
 // also holds column i for the coalesced write above.
-constexpr int kRedWarps = 8;
+constexpr int kRedWarps = 4;
 
 template <bool KG>
-__global__ void __launch_bounds__(32 * kRedWarps, 4) block_reduce_kernel(int64_t n_blk, const int32_t *__restrict__ seg,
+__global__ void __launch_bounds__(32 * kRedWarps, 8) block_reduce_kernel(int64_t n_blk, const int32_t *__restrict__ seg,
                                                            const int32_t *__restrict__ rot,
                                                            const int32_t *__restrict__ slot_bar, int64_t kg_rot_off,
                                                            const double *__restrict__ staging, const int32_t *__restrict__ A,
