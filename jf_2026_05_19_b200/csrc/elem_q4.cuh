@@ -128,7 +128,7 @@ struct Q4Pts {
 // bending modes (-m1, -m3, m0, m2) to the membrane modes m0..m3.  Both
 // condensations K_ab K_bb^-1 K_ab' are then c A B^-1 A' with the one 4x4
 // symmetric positive definite B.
-struct Q4KShared {
+struct __align__(16) Q4KShared {
     Q4Pts g;
     double Dd[4][4];            // MacNeal sampling rows: dN_k/dx (rows 0, 1), dN_k/dy (rows 2, 3)
     double ivd[4];              // 1 / (sqrt(2 Jp)^2 cs) per sampling point
@@ -136,6 +136,7 @@ struct Q4KShared {
     double Am[8][4], Ab[8][4];  // rows: (node, component) of the membrane / bending B
     double B[10];               // packed upper triangle
     double Xm[4][8], Xb[4][8];  // B^-1 Am', B^-1 Ab'
+    int32_t slot[10];           // node-pair slots, for the warp's copy of the staged blocks
 };
 
 // KG kernel state of one element (membrane incompatible modes only; the
@@ -533,11 +534,14 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
     }
     __syncwarp();
 
-    // Phase 4: one node pair (a <= b) per lane.  Gauss-point sums, the
-    // 6x6 local block (18 structural nonzeros), then T'KT by 3x3 sub-blocks.
+    // Phase 4: one node pair (a <= b) per lane.  Gauss-point sums and the
+    // 6x6 local block (18 structural nonzeros).
     double lmax = 0.0;
+    int a = 0, b = 0;
+    int32_t sl = -1;
+    double Lm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, Lp[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    double Qa[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, Qb[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
     if (valid) {
-        int a, b;
         q4_pair(tl, a, b);
         double Pxx = 0, Pxy = 0, Pyx = 0, Pyy = 0, T00 = 0, T01 = 0, T10 = 0, T11 = 0;
         double SxN = 0, SyN = 0, SNx = 0, SNy = 0, SNN = 0;
@@ -573,7 +577,6 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
             }
         // membrane + drilling on (u, v, theta_z): Bd = (dN/dy / 2, -dN/dx / 2, N)
         const double q = 0.25 * ad, hq = 0.5 * ad;
-        double Lm[3][3];
         Lm[0][0] = cm * (Pxx + gam * Pyy) + q * Pyy - cm * cmm[0][0];
         Lm[0][1] = cm * (nu * Pxy + gam * Pyx) - q * Pyx - cm * cmm[0][1];
         Lm[1][0] = cm * (nu * Pyx + gam * Pxy) - q * Pxy - cm * cmm[1][0];
@@ -582,13 +585,11 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
         Lm[2][0] = hq * SNy; Lm[2][1] = -hq * SNx; Lm[2][2] = ad * SNN;
         // plate on (w, theta_x, theta_y): bending with the twist row, then
         // MacNeal's shear D' Z^-1 D
-        double Lp[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
         Lp[1][1] = cb * (Pyy + gam * T00) - cb * cbb[0][0];
         Lp[1][2] = cb * (gam * T01 - nu * Pyx) - cb * cbb[0][1];
         Lp[2][1] = cb * (gam * T10 - nu * Pxy) - cb * cbb[1][0];
         Lp[2][2] = cb * (Pxx + gam * T11) - cb * cbb[1][1];
         if (!skip_mac) macneal_pair(S.Dd, S.W, a, b, Lp);
-        double Qa[9], Qb[9];
         if (nodeR) {
             double Ra[9], Rb[9];
 #pragma unroll
@@ -602,21 +603,70 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
 #pragma unroll
             for (int i = 0; i < 9; ++i) { Qa[i] = V[i]; Qb[i] = V[i]; }
         }
-        const int32_t sl = __ldg(o.blk_slot + e * 10 + tl);
-        double M[3][3], O[3][3];
-        // local dof order (u, v, w, theta_x, theta_y, theta_z)
-        M[0][0] = Lm[0][0]; M[0][1] = Lm[0][1]; M[1][0] = Lm[1][0]; M[1][1] = Lm[1][1]; M[2][2] = Lp[0][0];
-        rot_sparse<0b100011011>(Qa, M, Qb, O);
-        write_sub_block(o, e, sl, a, b, 0, 0, O, lmax, 24);
-        M[0][2] = Lm[0][2]; M[1][2] = Lm[1][2]; M[2][0] = Lp[0][1]; M[2][1] = Lp[0][2];
-        rot_sparse<0b011100100>(Qa, M, Qb, O);
-        write_sub_block(o, e, sl, a, b, 0, 1, O, lmax, 24);
-        M[0][2] = Lp[1][0]; M[1][2] = Lp[2][0]; M[2][0] = Lm[2][0]; M[2][1] = Lm[2][1];
-        rot_sparse<0b011100100>(Qa, M, Qb, O);
-        write_sub_block(o, e, sl, a, b, 1, 0, O, lmax, 24);
-        M[0][0] = Lp[1][1]; M[0][1] = Lp[1][2]; M[1][0] = Lp[2][1]; M[1][1] = Lp[2][2]; M[2][2] = Lm[2][2];
-        rot_sparse<0b100011011>(Qa, M, Qb, O);
-        write_sub_block(o, e, sl, a, b, 1, 1, O, lmax, 24);
+        sl = __ldg(o.blk_slot + e * 10 + tl);
+        S.slot[tl] = sl;
+    }
+    // Phase 5: T'KT and the writes.  The block of a pair is stored with
+    // rows of the lower-numbered global node (transposed when the slot says
+    // so).  Each half (stored rows 0-2, then 3-5) is rotated by sub-blocks,
+    // staged in the element's shared record -- no lane reads it any more --
+    // and copied out by the whole warp as 16-byte stores, 9 per half-slot,
+    // so a slot is written as whole contiguous lines instead of 36 scattered
+    // 8-byte stores.  Pairs on the RBE2 path are written directly.
+    __syncwarp();
+    const bool t = valid && sl >= 0 && (sl & kBlkTranspose);
+    double *buf = reinterpret_cast<double *>(&S) + 18 * tl;
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+        if (valid) {
+            // local dof order (u, v, w, theta_x, theta_y, theta_z); the
+            // translation-rotation and rotation-translation sub-blocks share
+            // one zero pattern, the two diagonal sub-blocks another
+            double M[3][3], Of[3][3], Os[3][3];
+            const bool off_tr = (half == 0) != t;  // off-diagonal sub-block of this half: TR, else RT
+            M[0][2] = off_tr ? Lm[0][2] : Lp[1][0]; M[1][2] = off_tr ? Lm[1][2] : Lp[2][0];
+            M[2][0] = off_tr ? Lp[0][1] : Lm[2][0]; M[2][1] = off_tr ? Lp[0][2] : Lm[2][1];
+            if (half == 0) {
+                rot_sparse<0b011100100>(Qa, M, Qb, Os);
+                M[0][0] = Lm[0][0]; M[0][1] = Lm[0][1]; M[1][0] = Lm[1][0]; M[1][1] = Lm[1][1]; M[2][2] = Lp[0][0];
+                rot_sparse<0b100011011>(Qa, M, Qb, Of);
+            } else {
+                rot_sparse<0b011100100>(Qa, M, Qb, Of);
+                M[0][0] = Lp[1][1]; M[0][1] = Lp[1][2]; M[1][0] = Lp[2][1]; M[1][1] = Lp[2][2]; M[2][2] = Lm[2][2];
+                rot_sparse<0b100011011>(Qa, M, Qb, Os);
+            }
+            if (sl < 0) {
+                write_sub_block(o, e, sl, a, b, half, 0, Of, lmax, 24);
+                write_sub_block(o, e, sl, a, b, half, 1, Os, lmax, 24);
+            } else {
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const double vf = t ? Of[c][r] : Of[r][c], vs = t ? Os[c][r] : Os[r][c];
+                        lmax = fmax(lmax, fmax(fabs(vf), fabs(vs)));
+                        buf[6 * r + c] = vf;
+                        buf[6 * r + 3 + c] = vs;
+                    }
+                if (o.diag_staging && a == b) {
+                    // diagonal pair (never transposed): TT in the first, RR in the second column band
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+                        o.diag_staging[__ldg(o.diag_slot + e * 24 + 6 * a + 3 * half + i)] = half == 0 ? Of[i][i] : Os[i][i];
+                }
+            }
+        }
+        __syncwarp();
+        for (int ch = lane; ch < Q4_TEAMS_PER_WARP * 10 * 9; ch += 32) {
+            const int tm = ch / 90, rem = ch - 90 * tm, pl = rem / 9, part = rem - 9 * pl;
+            const int sid = warp * Q4_TEAMS_PER_WARP + tm;
+            if ((int64_t)blockIdx.x * Q4_ELEMS_PER_BLOCK + sid >= nq) continue;
+            const int32_t st = sh[sid].slot[pl];
+            if (st < 0) continue;
+            const double2 v2 = reinterpret_cast<const double2 *>(reinterpret_cast<const double *>(&sh[sid]) + 18 * pl)[part];
+            reinterpret_cast<double2 *>(o.staging + 36 * (int64_t)(st & kBlkIndexMask) + 18 * half)[part] = v2;
+        }
+        __syncwarp();
     }
     if (o.maxabs) {
         for (int off = 16; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
