@@ -141,13 +141,14 @@ struct __align__(16) Q4KShared {
 
 // KG kernel state of one element (membrane incompatible modes only; the
 // condensation map is -B^-1 Am' with Am, B as in the K kernel).
-struct Q4GShared {
+struct __align__(16) Q4GShared {
     Q4Pts g;
     double uuv[8];        // local (u, v) of each node
     double Am[8][4];
     double B[10];
     double map[4][8];     // -B^-1 Am'
     double t[8][8], gz[8][4], f[8];
+    int32_t slot[10];     // node-pair slots, for the warp's copy of the staged blocks
 };
 
 __device__ __forceinline__ void q4_shape_gp(int g, double &r, double &s) {
@@ -873,9 +874,14 @@ __global__ void __launch_bounds__(Q4_THREADS) q4_kg_kernel(int64_t nq, const int
     __syncwarp();
 
     // Phase 5: one node pair per lane; translations only (the rotation
-    // sub-blocks of a flat shell's KG are zero).
+    // sub-blocks of a flat shell's KG are zero).  A staged slot holds the
+    // translation 3x3 and three zeros of padding: each lane stages its slot in
+    // the element's shared record, then the warp copies the slots out as
+    // 16-byte stores, 6 per slot.  Pairs on the RBE2 path are written directly.
+    double O[3][3];
+    int a = 0, b = 0;
+    int32_t sl = -1;
     if (valid) {
-        int a, b;
         q4_pair(tl, a, b);
         double M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
 #pragma unroll
@@ -901,20 +907,40 @@ __global__ void __launch_bounds__(Q4_THREADS) q4_kg_kernel(int64_t nq, const int
 #pragma unroll
             for (int i = 0; i < 9; ++i) { Qa[i] = V[i]; Qb[i] = V[i]; }
         }
-        double O[3][3];
         rot_sparse<0b100011011>(Qa, M, Qb, O);
-        const int32_t sl = __ldg(o.blk_slot + e * 10 + tl);
+        sl = __ldg(o.blk_slot + e * 10 + tl);
+    }
+    __syncwarp();  // every lane is past its last read of the element's record
+    if (valid) {
         double lmax = 0.0;
-        write_sub_block(o, e, sl, a, b, 0, 0, O, lmax, 24);
-        kg_shell_pad(o, sl);
         if (sl < 0) {
             // the dof-level RBE2 path reads whole raw blocks; staged shell
             // blocks of KG are read as their translation 3x3 only
             const double Z[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            write_sub_block(o, e, sl, a, b, 0, 0, O, lmax, 24);
             write_sub_block(o, e, sl, a, b, 0, 1, Z, lmax, 24);
             write_sub_block(o, e, sl, a, b, 1, 0, Z, lmax, 24);
             write_sub_block(o, e, sl, a, b, 1, 1, Z, lmax, 24);
+        } else {
+            const bool t = sl & kBlkTranspose;
+            double *buf = reinterpret_cast<double *>(&S) + 12 * tl;
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) buf[3 * r + c] = t ? O[c][r] : O[r][c];
+            buf[9] = 0.0; buf[10] = 0.0; buf[11] = 0.0;
         }
+        S.slot[tl] = sl;
+    }
+    __syncwarp();
+    for (int ch = lane; ch < Q4_TEAMS_PER_WARP * 10 * 6; ch += 32) {
+        const int tm = ch / 60, rem = ch - 60 * tm, pl = rem / 6, part = rem - 6 * pl;
+        const int sid = warp * Q4_TEAMS_PER_WARP + tm;
+        if ((int64_t)blockIdx.x * Q4_ELEMS_PER_BLOCK + sid >= nq) continue;
+        const int32_t st = sh[sid].slot[pl];
+        if (st < 0) continue;
+        const double2 v2 = reinterpret_cast<const double2 *>(reinterpret_cast<const double *>(&sh[sid]) + 12 * pl)[part];
+        reinterpret_cast<double2 *>(o.staging + 12 * (int64_t)(st & kBlkIndexMask))[part] = v2;
     }
 }
 

@@ -42,7 +42,7 @@ __host__ __device__ constexpr int t3_quad_node(int q, int k) {
 }
 __constant__ int c_t3_quads[3][4] = {{0, 3, 6, 5}, {1, 4, 6, 3}, {2, 5, 6, 4}};
 
-struct T3KShared {
+struct __align__(16) T3KShared {
     double V[9];
     double bv[3], cv[3], A, cm, ad;
     int nd[3];
@@ -56,7 +56,10 @@ struct T3KShared {
             double Kc[9][9];
         } c;
     } u;
-    double Pb[3][10][9];  // quad q, local node pair (a <= b): 3x3 over (w, theta_x, theta_y)
+    // quad q, local node pair (a <= b): 3x3 over (w, theta_x, theta_y);
+    // the K kernel's write phase reuses it for the six staged 6x6 blocks
+    alignas(16) double Pb[3][10][9];
+    int32_t slot[6];
 };
 
 // Corner coordinates of virtual quad q (corner q, midpoint to the next
@@ -183,6 +186,20 @@ __device__ __forceinline__ void t3_condense(T3KShared &S, int tl, unsigned tm) {
     __syncwarp(tm);
 }
 
+// Sub-block (bi, bj) of a node-pair 6x6 block into a staged slot buffer of
+// 36 values in stored orientation (transposed when the slot says so).
+__device__ __forceinline__ void stage_sub_block(double *buf, bool t, int bi, int bj, const double O[3][3], double &lmax) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const double v = O[i][j];
+            lmax = fmax(lmax, fabs(v));
+            const int r = 3 * bi + i, c = 3 * bj + j;
+            buf[t ? 6 * c + r : 6 * r + c] = v;
+        }
+}
+
 __global__ void __launch_bounds__(T3_THREADS, 5) t3_k_kernel(int64_t nt, const int32_t *__restrict__ nodes,
                                                          const double *__restrict__ prop,
                                                          const double *__restrict__ coords,
@@ -306,18 +323,41 @@ __global__ void __launch_bounds__(T3_THREADS, 5) t3_k_kernel(int64_t nt, const i
             for (int i = 0; i < 9; ++i) { Qa[i] = S.V[i]; Qb[i] = S.V[i]; }
         }
         const int32_t sl = __ldg(o.blk_slot + e * 6 + pair);
+        // Regular slots are staged in S.Pb (free after phase 4) in their
+        // stored orientation and copied out by the team below; pairs on the
+        // RBE2 path are written directly.
+        double *buf = &S.Pb[0][0][0] + 36 * pair;
+        const bool t = sl >= 0 && (sl & kBlkTranspose);
         double M[3][3], O[3][3];
         // diagonal sub-block: (u, v, w) x (u, v, w) or (rx, ry, rz) x (rx, ry, rz)
         M[0][0] = bi ? Lp[1][1] : Lm[0][0]; M[0][1] = bi ? Lp[1][2] : Lm[0][1];
         M[1][0] = bi ? Lp[2][1] : Lm[1][0]; M[1][1] = bi ? Lp[2][2] : Lm[1][1];
         M[2][2] = bi ? Lm[2][2] : Lp[0][0];
         rot_sparse<0b100011011>(Qa, M, Qb, O);
-        write_sub_block(o, e, sl, a, b, bi, bi, O, lmax, 18);
+        if (sl < 0) {
+            write_sub_block(o, e, sl, a, b, bi, bi, O, lmax, 18);
+        } else {
+            stage_sub_block(buf, t, bi, bi, O, lmax);
+            if (o.diag_staging && a == b)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) o.diag_staging[__ldg(o.diag_slot + e * 18 + 6 * a + 3 * bi + i)] = O[i][i];
+        }
         // off-diagonal sub-block: (u, v, w) x (rx, ry, rz) or its mirror
         M[0][2] = bi ? Lp[1][0] : Lm[0][2]; M[1][2] = bi ? Lp[2][0] : Lm[1][2];
         M[2][0] = bi ? Lm[2][0] : Lp[0][1]; M[2][1] = bi ? Lm[2][1] : Lp[0][2];
         rot_sparse<0b011100100>(Qa, M, Qb, O);
-        write_sub_block(o, e, sl, a, b, bi, 1 - bi, O, lmax, 18);
+        if (sl < 0) write_sub_block(o, e, sl, a, b, bi, 1 - bi, O, lmax, 18);
+        else stage_sub_block(buf, t, bi, 1 - bi, O, lmax);
+        if (bi == 0) S.slot[pair] = sl;
+    }
+    __syncwarp(tm);
+    // the team copies the staged slots as 16-byte stores, 18 per slot
+    for (int ch = tl; ch < 6 * 18; ch += T3_TEAM) {
+        const int pair = ch / 18, part = ch - 18 * pair;
+        const int32_t st = S.slot[pair];
+        if (st < 0) continue;
+        const double2 v2 = reinterpret_cast<const double2 *>(&S.Pb[0][0][0] + 36 * pair)[part];
+        reinterpret_cast<double2 *>(o.staging + 36 * (int64_t)(st & kBlkIndexMask))[part] = v2;
     }
     if (o.maxabs) {
         for (int off = 8; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_xor_sync(tm, lmax, off, 16));
