@@ -255,6 +255,54 @@ jfg_status jfg_dkdh_contract_device(jfg_model *m, const double *a_dev, const dou
 jfg_status jfg_dkdh_load_device(jfg_model *m, const double *u_dev, const uint8_t *mask_q4_dev, const uint8_t *mask_t3_dev,
                                 double *load_dev);
 
+/* ---- SOL 101 output recovery ----------------------------------------------
+ * Replace the per-element loops of recover_shell_stresses! and
+ * recover_bar_stresses! (src/solver/stress_recovery.jl:163-430, :432-593) on
+ * their default branch (isotropic PSHELL/MAT1, no SNORM, no curvature
+ * membrane): stress_strain_quad4 + quad4_bilinear_corner_forces
+ * (src/FEMKernels.jl:6003-6338) with the equilibrium-shear blend and the
+ * pressure-moment scale of CQUAD4, stress_strain_tria3 (:7391-7432) with its
+ * macro shear and the shared-edge macro-moment blend of CTRIA3, and
+ * forces_frame3d (:215-229) with the four section points of CBAR/CBEAM.
+ * u_global holds ndof values in the handle's dof order.
+ *
+ * Shell record, JFG_SHELL_REC doubles per element, CQUAD4s then CTRIA3s in
+ * handle order (the results_json "forces", "stresses", "strains" and
+ * "forces_bilin" entries):
+ *   0-2   fx fy fxy          membrane forces N
+ *   3-5   mx my mxy          bending moments M (CQUAD4: pressure scale applied)
+ *   6-7   qx qy              transverse shear (CQUAD4: equilibrium blend applied)
+ *   8-10  z1 stress          normal_x normal_y shear_xy at fibre -T/2
+ *   11-13 z2 stress          at +T/2
+ *   14-16 z1 strain, 17-19 z2 strain
+ *   20    stresses[eid]      max principal of the z1 stress
+ *   21    status             1 recovered; 0 where the reference's try block fails
+ *   22-33 corner forces N    CQUAD4 GA..GD (3 each, bilinear rows); 0 for CTRIA3
+ *   34-45 corner moments M   same layout, mxy constant across corners
+ *   46-47 von Mises z1, z2
+ * Bar record, JFG_BAR_REC doubles per CBAR/CBEAM in handle order:
+ *   0-7   axial shear_1 shear_2 torque moment_a1 moment_a2 moment_b1 moment_b2
+ *   8     axial stress (stresses[eid] is its absolute value)
+ *   9-12  end A stress at section points C D E F, 13-16 end B
+ *   17    status             1 recovered; 0 for a zero-length bar (skipped)
+ * bar_points (may be NULL: section stresses 0) holds JFG_BAR_POINTS doubles
+ * per bar: C1 C2 D1 D2 E1 E2 F1 F2 of the PBARL, then +1 for ROD/TUBE/TUBE2
+ * sections and -1 otherwise (surface_stress_sign).
+ * flags: JFG_RECOVER_PRESSURE_DECK declares that the deck has at least four
+ * PLOAD4 cards and no RBE3, RSPLINE, MPC, CROD or CONROD and at least four
+ * CSHELLs -- the model-level conditions of _quad4_pressure_resultant_moment_scale
+ * (stress_recovery.jl:131-161) that the handle cannot see; the handle adds
+ * "no bars, no RBE2" itself.  Either output may be NULL.  The _device form
+ * takes device pointers and runs on the handle's stream without waiting. */
+#define JFG_SHELL_REC 48
+#define JFG_BAR_REC 18
+#define JFG_BAR_POINTS 9
+#define JFG_RECOVER_PRESSURE_DECK 1
+jfg_status jfg_recover_stresses(jfg_model *m, const double *u_global, const double *bar_points, int32_t flags,
+                                double *shell_out, double *bar_out);
+jfg_status jfg_recover_stresses_device(jfg_model *m, const double *u_dev, const double *bar_points_dev, int32_t flags,
+                                       double *shell_out_dev, double *bar_out_dev);
+
 /* ---- Serving: a device-resident request loop over model families --------
  * Replaces the reference's optimisation worker loop
  * (tools/jfem_worker_jsonl.jl:132-148, manifest_batch_core.jl:283-409), which

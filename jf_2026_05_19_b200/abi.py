@@ -21,6 +21,12 @@ JFG_ERR_STATE = 5
 JFG_ERR_NOMEM = 6
 JFG_ERR_REFERENCE_RAISES = 7
 
+# output recovery records (jfg_recover_stresses)
+SHELL_REC = 48
+BAR_REC = 18
+BAR_POINTS = 9
+RECOVER_PRESSURE_DECK = 1
+
 STATUS_NAMES = {0: "OK", 1: "INVALID", 2: "UNSUPPORTED", 3: "CUDA", 4: "TIMEOUT",
                 5: "STATE", 6: "NOMEM", 7: "REFERENCE_RAISES"}
 

@@ -36,6 +36,7 @@
 #include "elem_q4.cuh"
 #include "elem_t3.cuh"
 #include "elem_dkdh.cuh"
+#include "elem_recover.cuh"
 
 using namespace jfg;
 
@@ -92,6 +93,10 @@ struct jfg_model {
     double *d_dstaging = nullptr;
     double *d_dk = nullptr;             // host-buffer dK/dh calls: a, b (or u, load), c_q4, c_t3
     uint8_t *d_dk_mask = nullptr;
+    // output recovery: CTRIA3 shared-edge macro weights (built at the first call), RBE2 count
+    double *d_t3_mw = nullptr;
+    double *d_rec = nullptr;            // host-form recovery buffers: u, bar points, records
+    int64_t n_rbe2 = 0;
     int64_t n_dcontrib = 0;
     // work buffers
     double *d_nz = nullptr, *d_u = nullptr, *d_diag = nullptr, *d_max = nullptr, *d_h = nullptr;
@@ -769,6 +774,7 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
     m->nq = d->n_quad4;
     m->nt = d->n_tria3;
     m->nb = d->n_bar;
+    m->n_rbe2 = d->n_rbe2;
     m->k6rot = d->k6rot;
     m->has_nodeR = d->node_R != nullptr;
     const int64_t ndof = m->ndof;
@@ -1667,6 +1673,83 @@ jfg_status jfg_dkdh_load(jfg_model *m, const double *u, const uint8_t *mask_q4, 
     st = jfg_dkdh_load_device(m, du, mask_q4 ? mq : nullptr, mask_t3 ? mt : nullptr, dl);
     if (st) return st;
     CK(cudaMemcpyAsync(load, dl, sizeof(double) * m->ndof, cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    return JFG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// SOL 101 output recovery (stress_recovery.jl:163-593)
+// ---------------------------------------------------------------------------
+
+// CTRIA3 shared-edge weights of _tria3_shell_macro_blend_weights
+// (stress_recovery.jl:20-51): every shell edge as a sorted-node key, sorted
+// once; each CTRIA3 counts its edges that occur more than once.
+static jfg_status build_t3_macro_weights(jfg_model *m) {
+    CK(dalloc(m, &m->d_t3_mw, m->nt));
+    const int64_t n = 4 * m->nq + 3 * m->nt;
+    unsigned long long *keys = nullptr;
+    CK(cudaMallocAsync(&keys, sizeof(unsigned long long) * 2 * n, m->stream));
+    shell_edge_keys_kernel<<<(unsigned)cdiv(n, 256), 256, 0, m->stream>>>(m->nq, m->nt, m->d_q4n, m->d_t3n, keys);
+    cudaError_t e = cudaGetLastError();
+    size_t tmp = 0;
+    void *d_tmp = nullptr;
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortKeys(nullptr, tmp, keys, keys + n, n, 0, 64, m->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d_tmp, tmp, m->stream);
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortKeys(d_tmp, tmp, keys, keys + n, n, 0, 64, m->stream);
+    if (e == cudaSuccess) {
+        t3_macro_weight_kernel<<<(unsigned)cdiv(m->nt, 256), 256, 0, m->stream>>>(m->nt, m->d_t3n, keys + n, n, m->d_t3_mw);
+        e = cudaGetLastError();
+    }
+    if (d_tmp) cudaFreeAsync(d_tmp, m->stream);
+    cudaFreeAsync(keys, m->stream);
+    CK(e);
+    return JFG_OK;
+}
+
+jfg_status jfg_recover_stresses_device(jfg_model *m, const double *u_dev, const double *bar_points_dev, int32_t flags,
+                                       double *shell_out_dev, double *bar_out_dev) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    if (!u_dev) return fail(m, JFG_ERR_INVALID, "null u_global");
+    if (flags & ~JFG_RECOVER_PRESSURE_DECK) return fail(m, JFG_ERR_INVALID, "unknown recovery flag");
+    if (shell_out_dev && m->nt && !m->d_t3_mw) {
+        jfg_status st = build_t3_macro_weights(m);
+        if (st) return st;
+    }
+    // the model-level conditions of _quad4_pressure_resultant_moment_scale the handle sees itself
+    const bool pressure_deck = (flags & JFG_RECOVER_PRESSURE_DECK) && m->nb == 0 && m->n_rbe2 == 0;
+    if (shell_out_dev && m->nq) {
+        q4_recover_kernel<<<(unsigned)cdiv(m->nq, 128), 128, 0, m->stream>>>(m->nq, m->d_q4n, m->d_q4p, m->d_coords,
+                                                                            m->d_nodeR, u_dev, pressure_deck, shell_out_dev);
+        CK(cudaGetLastError());
+    }
+    if (shell_out_dev && m->nt) {
+        t3_recover_kernel<<<(unsigned)cdiv(m->nt, T3_ELEMS_PER_BLOCK), T3_THREADS, 0, m->stream>>>(
+            m->nt, m->d_t3n, m->d_t3p, m->d_coords, m->d_nodeR, u_dev, m->d_t3_mw, shell_out_dev + REC_SHELL * m->nq);
+        CK(cudaGetLastError());
+    }
+    if (bar_out_dev && m->nb) {
+        bar_recover_kernel<<<(unsigned)cdiv(m->nb, 128), 128, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords,
+                                                                             m->d_nodeR, u_dev, bar_points_dev, bar_out_dev);
+        CK(cudaGetLastError());
+    }
+    return JFG_OK;
+}
+
+jfg_status jfg_recover_stresses(jfg_model *m, const double *u_global, const double *bar_points, int32_t flags,
+                                double *shell_out, double *bar_out) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    if (!u_global) return fail(m, JFG_ERR_INVALID, "null u_global");
+    const int64_t ns = m->nq + m->nt;
+    if (!m->d_rec) CK(dalloc(m, &m->d_rec, m->ndof + JFG_BAR_POINTS * m->nb + REC_SHELL * ns + REC_BAR * m->nb));
+    double *du = m->d_rec, *dp = du + m->ndof, *dsh = dp + JFG_BAR_POINTS * m->nb, *dbar = dsh + REC_SHELL * ns;
+    CK(cudaMemcpyAsync(du, u_global, sizeof(double) * m->ndof, cudaMemcpyHostToDevice, m->stream));
+    if (bar_points && m->nb)
+        CK(cudaMemcpyAsync(dp, bar_points, sizeof(double) * JFG_BAR_POINTS * m->nb, cudaMemcpyHostToDevice, m->stream));
+    jfg_status st = jfg_recover_stresses_device(m, du, bar_points ? dp : nullptr, flags, shell_out ? dsh : nullptr,
+                                                bar_out ? dbar : nullptr);
+    if (st) return st;
+    if (shell_out && ns) CK(cudaMemcpyAsync(shell_out, dsh, sizeof(double) * REC_SHELL * ns, cudaMemcpyDeviceToHost, m->stream));
+    if (bar_out && m->nb) CK(cudaMemcpyAsync(bar_out, dbar, sizeof(double) * REC_BAR * m->nb, cudaMemcpyDeviceToHost, m->stream));
     CK(cudaStreamSynchronize(m->stream));
     return JFG_OK;
 }

@@ -62,6 +62,14 @@ class ModelArrays:
     # Loads/BCs for a static preload (used by the SOL 105 consumer in tests)
     spc_dofs: Optional[np.ndarray] = None   # 0-based constrained dof indices
     force: Optional[np.ndarray] = None      # (ndof,) f64
+    # Element IDs in handle order and PBARL stress-recovery points (C1 C2 D1 D2
+    # E1 E2 F1 F2, then +1 for ROD/TUBE/TUBE2 sections, else -1), when the deck
+    # came from a model dictionary
+    q4_eid: Optional[np.ndarray] = None
+    t3_eid: Optional[np.ndarray] = None
+    bar_eid: Optional[np.ndarray] = None
+    bar_points: Optional[np.ndarray] = None  # (nb, 9) f64
+    shell_order: Optional[np.ndarray] = None  # shell record index (CQUAD4s, then CTRIA3s) in dictionary order
 
     @property
     def n_nodes(self) -> int:

@@ -12,7 +12,7 @@ from typing import Optional
 import numpy as np
 
 from . import abi
-from .abi import JfgModelDesc, make_desc
+from .abi import BAR_POINTS, BAR_REC, RECOVER_PRESSURE_DECK, SHELL_REC, JfgModelDesc, make_desc
 from .decks import ModelArrays
 
 PKG = os.path.dirname(os.path.abspath(__file__))
@@ -24,7 +24,8 @@ EXPORTS = ("jfg_model_create", "jfg_pattern", "jfg_pattern_fill", "jfg_assemble_
            "jfg_set_stream", "jfg_last_timing", "jfg_kernel_timing", "jfg_timing_accumulated", "jfg_model_stats", "jfg_model_counts", "jfg_batch_workspace_bytes",
            "jfg_batch_reserve", "jfg_assemble_batch_device", "jfg_ff_set_free", "jfg_ff_extract_device",
            "jfg_ff_fetch", "jfg_ff_device_arrays", "jfg_dkdh_contract", "jfg_dkdh_load",
-           "jfg_dkdh_contract_device", "jfg_dkdh_load_device", "jfg_server_create", "jfg_server_submit", "jfg_server_wait",
+           "jfg_dkdh_contract_device", "jfg_dkdh_load_device", "jfg_recover_stresses",
+           "jfg_recover_stresses_device", "jfg_server_create", "jfg_server_submit", "jfg_server_wait",
            "jfg_server_result", "jfg_server_release", "jfg_server_stats", "jfg_server_family_batch",
            "jfg_server_hold", "jfg_server_last_error", "jfg_server_destroy", "jfg_assemble_k_quad4_noalloc", "jfg_model_destroy", "jfg_last_error",
            "jfg_version")
@@ -88,6 +89,8 @@ def load(path: str = LIB_PATH):
     L.jfg_dkdh_load.argtypes = [C.c_void_p, _pd, _pu8, _pu8, _pd]
     L.jfg_dkdh_contract_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.jfg_dkdh_load_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.jfg_recover_stresses.argtypes = [C.c_void_p, _pd, _pd, C.c_int32, _pd, _pd]
+    L.jfg_recover_stresses_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
     L.jfg_ff_extract_device.argtypes = [C.c_void_p, C.c_void_p, _pi64, _pd, _pd]
     L.jfg_ff_fetch.argtypes = [C.c_void_p, _pi64, _pi64, _pd]
     L.jfg_ff_device_arrays.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
@@ -275,6 +278,23 @@ class GpuModel:
     def dkdh_load_device(self, u_ptr: int, mq_ptr: Optional[int], mt_ptr: Optional[int], out_ptr: int):
         self._check(self.L.jfg_dkdh_load_device(self.h, C.c_void_p(u_ptr), C.c_void_p(mq_ptr or None),
                                                 C.c_void_p(mt_ptr or None), C.c_void_p(out_ptr)))
+
+    def recover_stresses(self, u: np.ndarray, bar_points: Optional[np.ndarray] = None, pressure_deck: bool = False):
+        """SOL 101 output recovery (jfg_recover_stresses): shell records
+        (n_quad4 + n_tria3, SHELL_REC) and bar records (n_bar, BAR_REC)."""
+        u = np.ascontiguousarray(u, np.float64)
+        nq, nt, nb = self.counts[1], self.counts[2], self.counts[3]
+        pts = None if bar_points is None else np.ascontiguousarray(bar_points, np.float64).reshape(nb, BAR_POINTS)
+        shell = np.empty((nq + nt, SHELL_REC))
+        bar = np.empty((nb, BAR_REC))
+        self._check(self.L.jfg_recover_stresses(self.h, _ptr(u, _pd), _ptr(pts, _pd), RECOVER_PRESSURE_DECK if pressure_deck else 0,
+                                                _ptr(shell, _pd), _ptr(bar, _pd)))
+        return shell, bar
+
+    def recover_stresses_device(self, u_ptr: int, points_ptr: Optional[int], flags: int, shell_ptr: Optional[int],
+                                bar_ptr: Optional[int]):
+        self._check(self.L.jfg_recover_stresses_device(self.h, C.c_void_p(u_ptr), C.c_void_p(points_ptr or None), int(flags),
+                                                       C.c_void_p(shell_ptr or None), C.c_void_p(bar_ptr or None)))
 
     def set_stream(self, stream_ptr: int):
         self._check(self.L.jfg_set_stream(self.h, C.c_void_p(stream_ptr or None)))

@@ -20,6 +20,8 @@ raises raise ``RuntimeError`` with the reference location.
 """
 from __future__ import annotations
 
+import re
+
 import numpy as np
 import scipy.sparse as sp
 
@@ -36,6 +38,21 @@ def _raise(err: JfgError):
     if err.status == JFG_ERR_REFERENCE_RAISES:
         raise RuntimeError(err.msg) from err
     raise err
+
+
+def public_id(key, entry) -> int:
+    """Element ID of a model-dictionary entry (_stress_entry_public_id,
+    stress_recovery.jl:3-14): its "ID", else the key, else the key's leading integer."""
+    if isinstance(entry, dict) and "ID" in entry:
+        try:
+            return int(str(entry["ID"]))
+        except ValueError:
+            pass
+    try:
+        return int(str(key))
+    except ValueError:
+        m = re.match(r"^-?\d+", str(key))
+        return int(m.group(0)) if m else 0
 
 
 def model_arrays_from_dict(model: dict) -> tuple:
@@ -75,8 +92,8 @@ def model_arrays_from_dict(model: dict) -> tuple:
             Gs = Es / (2 * (1 + nus)) if Es > 0 else 0.0
         return [prop["T"], E, nu, G, prop.get("BEND_RATIO", 1.0), prop.get("TS_T", 5.0 / 6.0), Gs]
 
-    q4n, q4p, t3n, t3p = [], [], [], []
-    for el in model.get("CSHELLs", {}).values():
+    q4n, q4p, t3n, t3p, q4e, t3e, order = [], [], [], [], [], [], []
+    for key, el in model.get("CSHELLs", {}).items():
         if str(el["PID"]) not in pshells or str(pshells[str(el["PID"])]["MID"]) not in mats:
             continue
         nids = el["NODES"]
@@ -88,10 +105,12 @@ def model_arrays_from_dict(model: dict) -> tuple:
         idx = [id_map[nid] - 1 for nid in nids]
         (q4n if len(nids) == 4 else t3n).append(idx)
         (q4p if len(nids) == 4 else t3p).append(row)
+        (q4e if len(nids) == 4 else t3e).append(public_id(key, el))
+        order.append((len(nids) == 4, len(q4e if len(nids) == 4 else t3e) - 1))
     pbarls = model.get("PBARLs", {})
-    bn, bp, bpin = [], [], []
+    bn, bp, bpin, be, bpts = [], [], [], [], []
     for group in ("CBARs", "CBEAMs"):
-        for bar in model.get(group, {}).values():
+        for key, bar in model.get(group, {}).items():
             pid = str(bar["PID"])
             if pid not in pbarls:
                 continue
@@ -114,6 +133,9 @@ def model_arrays_from_dict(model: dict) -> tuple:
                        E, G, *v, *bar.get("WA", [0.0, 0.0, 0.0]), *bar.get("WB", [0.0, 0.0, 0.0])])
             bn.append([ga, id_map[bar["GB"]] - 1])
             bpin.append([int(bar.get("PA", 0) or 0), int(bar.get("PB", 0) or 0)])
+            be.append(public_id(key, bar))
+            sign = 1.0 if str(prop.get("TYPE", "")).upper() in ("ROD", "TUBE", "TUBE2") else -1.0
+            bpts.append([float(prop.get(k, 0.0)) for k in ("C1", "C2", "D1", "D2", "E1", "E2", "F1", "F2")] + [sign])
     masters, cms, sptr, slaves = [], [], [0], []
     for rbe in model.get("RBE2s", {}).values():
         if rbe["GN"] not in id_map:
@@ -133,7 +155,10 @@ def model_arrays_from_dict(model: dict) -> tuple:
         bar_pin=np.array(bpin, np.int32).reshape(-1, 2), rbe2_master=np.array(masters, np.int32),
         rbe2_cm=np.array(cms, np.int32), rbe2_slave_ptr=np.array(sptr, np.int64), rbe2_slaves=np.array(slaves, np.int32),
         node_R=node_R if any_cd else None, node_ids=np.array(ids, np.int64),
-        k6rot=float(model.get("PARAM_K6ROT", 100.0)), param_snorm=float(model.get("PARAM_SNORM", 0.0)))
+        k6rot=float(model.get("PARAM_K6ROT", 100.0)), param_snorm=float(model.get("PARAM_SNORM", 0.0)),
+        q4_eid=np.array(q4e, np.int64), t3_eid=np.array(t3e, np.int64), bar_eid=np.array(be, np.int64),
+        bar_points=np.array(bpts, float).reshape(-1, 9),
+        shell_order=np.array([i if quad else len(q4e) + i for quad, i in order], np.int64))
     return m, id_map, coords, [node_R[i] for i in range(n)]
 
 
@@ -220,6 +245,102 @@ def assemble_geometric_stiffness(model, id_map, node_coords, node_R, ndof, u_glo
         timings.clear()
         timings.update({"shells": el / 1e3, "sparse_build": red / 1e3, "total": tot / 1e3})
     return _csc(g, nz)
+
+
+def _recovery_inputs(model, u_global):
+    m, _, _, _ = model_arrays_from_dict(model)
+    g = _handle(model, m)
+    u = np.asarray(u_global, np.float64)
+    if u.shape != (g.ndof,):
+        raise ValueError("u_global does not match the model's dof count")
+    return m, g, u
+
+
+def _pressure_deck(model) -> bool:
+    """Model-level conditions of _quad4_pressure_resultant_moment_scale
+    (stress_recovery.jl:131-161) that the library cannot see; it adds "no bars,
+    no RBE2" itself.  MAT1 entries are taken as carrying E and NU (the parser
+    completes them)."""
+    if len(model.get("PLOAD4s", []) or []) < 4 or len(model.get("CSHELLs", {}) or {}) < 4:
+        return False
+    return not any(model.get(k) for k in ("RBE3s", "RSPLINEs", "MPCs", "CRODs", "CONRODs"))
+
+
+def recover_shell_stresses(model, id_map, X, node_R, u_global, snorm_normals, stresses, results_json):
+    """recover_shell_stresses! (stress_recovery.jl:163-430): per CQUAD4/CTRIA3 the
+    max principal z1 stress into ``stresses[eid]`` and the "forces", "forces_bilin",
+    "stresses" and "strains" rows into ``results_json``, in the dictionary's order."""
+    del id_map, X, node_R
+    if snorm_normals:
+        raise NotImplementedError("SNORM normals leave the default branch")
+    m, g, u = _recovery_inputs(model, u_global)
+    try:
+        shell, _ = g.recover_stresses(u, None, _pressure_deck(model))
+    except JfgError as err:
+        _raise(err)
+    nq = m.q4_nodes.shape[0]
+    forces = results_json.setdefault("forces", {})
+    bilin = results_json.setdefault("forces_bilin", {})
+    sres = results_json.setdefault("stresses", {})
+    eres = results_json.setdefault("strains", {})
+    ids = m.node_ids if m.node_ids is not None else np.arange(1, m.n_nodes + 1)
+    f = lambda v: float(v)
+    for i in m.shell_order:
+        r = shell[i]
+        if r[21] == 0.0:
+            continue  # the reference's try block failed: no entries
+        quad = i < nq
+        j = i if quad else i - nq
+        eid = int(m.q4_eid[j] if quad else m.t3_eid[j])
+        T = float((m.q4_prop if quad else m.t3_prop)[j, 0])
+        key = "quad4" if quad else "tria3"
+        stresses[eid] = f(r[20])
+        row = {"eid": eid, "fx": f(r[0]), "fy": f(r[1]), "fxy": f(r[2]), "mx": f(r[3]), "my": f(r[4]), "mxy": f(r[5]),
+               "qx": f(r[6]), "qy": f(r[7])}
+        forces.setdefault(key, []).append(row)
+        if quad:
+            rows = [dict(row, grid_id="CEN/4")]
+            for k in range(4):
+                rows.append({"eid": eid, "grid_id": int(ids[m.q4_nodes[j, k]]),
+                             "fx": f(r[22 + 3 * k]), "fy": f(r[23 + 3 * k]), "fxy": f(r[24 + 3 * k]),
+                             "mx": f(r[34 + 3 * k]), "my": f(r[35 + 3 * k]), "mxy": f(r[36 + 3 * k]),
+                             "qx": f(r[6]), "qy": f(r[7])})
+            bilin.setdefault("quad4", []).extend(rows)
+        sz1, sz2, ez1, ez2 = r[8:11], r[11:14], r[14:17], r[17:20]
+
+        def st(s, t, vm):
+            return {"fiber_dist": t, "normal_x": f(s[0]), "normal_y": f(s[1]), "shear_xy": f(s[2]), "von_mises": f(vm),
+                    "major": 0.0, "minor": 0.0}
+
+        def sn(e, t):
+            return {"fiber_dist": t, "normal_x": f(e[0]), "normal_y": f(e[1]), "shear_xy": f(e[2]), "major": 0.0, "minor": 0.0}
+
+        sres.setdefault(key, []).append({"eid": eid, "z1": st(sz1, -T / 2, r[46]), "z2": st(sz2, T / 2, r[47])})
+        eres.setdefault(key, []).append({"eid": eid, "z1": sn((ez1 + ez2) / 2.0, 0.0), "z2": sn((ez1 - ez2) / T, -1.0)})
+
+
+def recover_bar_stresses(model, id_map, X, node_R, u_global, stresses, results_json):
+    """recover_bar_stresses! (stress_recovery.jl:432-593): CBAR then CBEAM end
+    forces into results_json["forces"]["cbar"], section-point stresses into
+    results_json["stresses"]["cbar"] and |axial stress| into ``stresses[eid]``."""
+    del id_map, X, node_R
+    m, g, u = _recovery_inputs(model, u_global)
+    try:
+        _, bar = g.recover_stresses(u, m.bar_points)
+    except JfgError as err:
+        _raise(err)
+    forces = results_json.setdefault("forces", {}).setdefault("cbar", [])
+    sres = results_json.setdefault("stresses", {}).setdefault("cbar", [])
+    names = ("axial", "shear_1", "shear_2", "torque", "moment_a1", "moment_a2", "moment_b1", "moment_b2")
+    for i in range(bar.shape[0]):
+        r = bar[i]
+        if r[17] == 0.0:
+            continue  # zero-length bar
+        eid = int(m.bar_eid[i])
+        stresses[eid] = abs(float(r[8]))
+        forces.append({"eid": eid, **{n: float(r[k]) for k, n in enumerate(names)}})
+        sres.append({"eid": eid, "end_a": {f"p{j + 1}": float(r[9 + j]) for j in range(4)},
+                     "end_b": {f"p{j + 1}": float(r[13 + j]) for j in range(4)}, "axial": float(r[8])})
 
 
 def release(model=None):

@@ -1079,6 +1079,447 @@ void to_local(int nn, const double *Q, const double *xg, const int32_t *nd, doub
 }
 
 // ---------------------------------------------------------------------------
+// SOL 101 output recovery (stress_recovery.jl:163-593), default branch:
+// isotropic PSHELL/MAT1, no SNORM normals, no curvature membrane (scale 0),
+// Wilson modes with each Gauss point's own Jacobian, frame mode :diag.
+// ---------------------------------------------------------------------------
+
+// The Gauss-point loops shared by stress_strain_quad4 (FEMKernels.jl:6003-6195)
+// and quad4_bilinear_corner_forces (:6197-6338): membrane strain Bm u + Bi alpha
+// with alpha = -(K_bb \ K_ab' u), curvature Bb u, and the clamped |det J|.
+// Returns false where the reference's LU of K_bb raises (exactly singular).
+bool q4_gp_fields(const double lc[4][2], const double u[24], const double Cm[3][3], double eps[4][3], double kap[4][3],
+                  double wdet[4]) {
+    const double pt = 1.0 / std::sqrt(3.0);
+    const double gp[4][2] = {{-pt, -pt}, {pt, -pt}, {pt, pt}, {-pt, pt}};
+    double K_ab[24][4] = {}, K_bb[4][4] = {};
+    double Bm_g[4][3][24] = {}, Bb_g[4][3][24] = {}, Bi_g[4][3][4] = {};
+    for (int g = 0; g < 4; ++g) {
+        double r = gp[g][0], s = gp[g][1];
+        double dNr[4], dNs[4];
+        shape_derivs_quad(r, s, dNr, dNs);
+        Jac j = jacobian(lc, dNr, dNs);
+        double detg = std::fabs(j.det);
+        if (detg < 1e-12) detg = 1e-12;
+        wdet[g] = detg;
+        for (int k = 0; k < 4; ++k) {
+            double dx = j.iJ11 * dNr[k] + j.iJ12 * dNs[k];
+            double dy = j.iJ21 * dNr[k] + j.iJ22 * dNs[k];
+            Bm_g[g][0][6 * k] = dx; Bm_g[g][1][6 * k + 1] = dy; Bm_g[g][2][6 * k] = dy; Bm_g[g][2][6 * k + 1] = dx;
+            Bb_g[g][0][6 * k + 4] = dx; Bb_g[g][1][6 * k + 3] = -dy;
+            Bb_g[g][2][6 * k + 4] = dy; Bb_g[g][2][6 * k + 3] = -dx;
+        }
+        // fill_quad4_membrane_incompatible_B! (FEMKernels.jl:1831-1857)
+        double d1x = j.iJ11 * (-2.0 * r), d1y = j.iJ21 * (-2.0 * r), d2x = j.iJ12 * (-2.0 * s), d2y = j.iJ22 * (-2.0 * s);
+        Bi_g[g][0][0] = d1x; Bi_g[g][2][0] = d1y; Bi_g[g][1][1] = d1y; Bi_g[g][2][1] = d1x;
+        Bi_g[g][0][2] = d2x; Bi_g[g][2][2] = d2y; Bi_g[g][1][3] = d2y; Bi_g[g][2][3] = d2x;
+        double CBi[12];
+        mul(CBi, &Cm[0][0], &Bi_g[g][0][0], 3, 3, 4);
+        mul_At_add(&K_ab[0][0], &Bm_g[g][0][0], CBi, 3, 24, 4, detg);
+        mul_At_add(&K_bb[0][0], &Bi_g[g][0][0], CBi, 3, 4, 4, detg);
+    }
+    double rhs[4], A[16];
+    for (int l = 0; l < 4; ++l) {
+        double s = 0.0;
+        for (int i = 0; i < 24; ++i) s += K_ab[i][l] * u[i];
+        rhs[l] = s;
+    }
+    for (int i = 0; i < 4; ++i)
+        for (int jj = 0; jj < 4; ++jj) A[i * 4 + jj] = K_bb[i][jj];
+    if (!lu_solve(4, 1, A, rhs)) return false;
+    for (int g = 0; g < 4; ++g)
+        for (int c = 0; c < 3; ++c) {
+            double se = 0.0, sk = 0.0;
+            for (int i = 0; i < 24; ++i) { se += Bm_g[g][c][i] * u[i]; sk += Bb_g[g][c][i] * u[i]; }
+            for (int l = 0; l < 4; ++l) se += Bi_g[g][c][l] * (-rhs[l]);
+            eps[g][c] = se;
+            kap[g][c] = sk;
+        }
+    return true;
+}
+
+// quad4_mitc4_center_shear_resultant (FEMKernels.jl:5927-6001) with
+// PHI2_ALPHA = 10 (FEMKernels.jl:10) and ts_t = 5/6.
+void q4_mitc4_center_shear(const double lc[4][2], const double u[24], double G, double h, double Q[2]) {
+    const double tp[4][2] = {{0.0, -1.0}, {0.0, 1.0}, {-1.0, 0.0}, {1.0, 0.0}};
+    double Bs[4][24] = {};
+    for (int t = 0; t < 4; ++t) {
+        double xi = tp[t][0], eta = tp[t][1];
+        double dNr[4], dNs[4];
+        shape_derivs_quad(xi, eta, dNr, dNs);
+        Jac j = jacobian(lc, dNr, dNs);
+        double Nt[4] = {0.25 * (1 - xi) * (1 - eta), 0.25 * (1 + xi) * (1 - eta), 0.25 * (1 + xi) * (1 + eta),
+                        0.25 * (1 - xi) * (1 + eta)};
+        for (int k = 0; k < 4; ++k) {
+            if (t < 2) { Bs[t][6 * k + 2] = dNr[k]; Bs[t][6 * k + 3] = -j.J12 * Nt[k]; Bs[t][6 * k + 4] = j.J11 * Nt[k]; }
+            else { Bs[t][6 * k + 2] = dNs[k]; Bs[t][6 * k + 3] = -j.J22 * Nt[k]; Bs[t][6 * k + 4] = j.J21 * Nt[k]; }
+        }
+    }
+    double dNr[4], dNs[4];
+    shape_derivs_quad(0.0, 0.0, dNr, dNs);
+    Jac c = jacobian(lc, dNr, dNs);
+    double absdet = std::max(std::fabs(c.det), 1e-30);
+    double gam[2] = {0.0, 0.0};
+    for (int jx = 0; jx < 24; ++jx) {
+        gam[0] += 0.5 * (Bs[0][jx] + Bs[1][jx]) * u[jx];
+        gam[1] += 0.5 * (Bs[2][jx] + Bs[3][jx]) * u[jx];
+    }
+    double phi2 = std::min(1.0, 10.0 * h * h / std::max(4.0 * absdet, 1e-30));
+    double k = 5.0 / 6.0 * G * h;
+    double t11 = k * c.iJ11, t12 = k * c.iJ12, t21 = k * c.iJ21, t22 = k * c.iJ22;
+    double M11 = c.iJ11 * t11 + c.iJ21 * t21, M12 = c.iJ11 * t12 + c.iJ21 * t22;
+    double M21 = c.iJ12 * t11 + c.iJ22 * t21, M22 = c.iJ12 * t12 + c.iJ22 * t22;
+    double q1 = phi2 * (M11 * gam[0] + M12 * gam[1]), q2 = phi2 * (M21 * gam[0] + M22 * gam[1]);
+    Q[0] = c.J11 * q1 + c.J21 * q2;
+    Q[1] = c.J12 * q1 + c.J22 * q2;
+}
+
+inline void plane_stress_D(double E, double nu, double D[3][3]) {
+    double c = E / (1 - nu * nu);
+    double b[3][3] = {{1.0, nu, 0.0}, {nu, 1.0, 0.0}, {0.0, 0.0, (1 - nu) / 2}};
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) D[i][j] = c * b[i][j];
+}
+inline void mv3(const double A[3][3], const double x[3], double y[3]) {
+    for (int i = 0; i < 3; ++i) y[i] = A[i][0] * x[0] + A[i][1] * x[1] + A[i][2] * x[2];
+}
+
+// One element's recovered quantities (the record layout of JFG_SHELL_REC).
+struct ShellRec {
+    double N[3] = {}, M[3] = {}, Q[2] = {}, sz1[3] = {}, sz2[3] = {}, ez1[3] = {}, ez2[3] = {};
+    double Nc[4][3] = {}, Mc[4][3] = {};
+    bool ok = true;
+};
+
+// stress_strain_quad4 (for_kg = false), returning also the Gauss fields for
+// the bilinear corner forces.
+bool q4_stress_strain(const double lc[4][2], const double u[24], double E, double nu, double h, double br, ShellRec &R,
+                      double eps[4][3], double kap[4][3]) {
+    double D[3][3], Cm[3][3];
+    plane_stress_D(E, nu, D);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Cm[i][j] = D[i][j] * h;
+    double dNr[4], dNs[4];
+    shape_derivs_quad(0.0, 0.0, dNr, dNs);
+    if (jacobian(lc, dNr, dNs).det == 0.0) return false;  // inv(J) at the centre raises
+    double wdet[4];
+    if (!q4_gp_fields(lc, u, Cm, eps, kap, wdet)) return false;
+    double ea[3] = {0, 0, 0}, ka[3] = {0, 0, 0}, area = 0.0;
+    for (int g = 0; g < 4; ++g) {
+        for (int c = 0; c < 3; ++c) { ea[c] += eps[g][c] * wdet[g]; ka[c] += kap[g][c] * wdet[g]; }
+        area += wdet[g];
+    }
+    for (int c = 0; c < 3; ++c) { ea[c] /= area; ka[c] /= area; }
+    mv3(Cm, ea, R.N);
+    double Dk[3];
+    mv3(D, ka, Dk);
+    for (int c = 0; c < 3; ++c) R.M[c] = -br * Dk[c] * (h * h * h / 12.0);
+    double G = E / (2 * (1 + nu));
+    if (br <= 1e-12) R.Q[0] = R.Q[1] = 0.0;
+    else q4_mitc4_center_shear(lc, u, G, h, R.Q);
+    for (int c = 0; c < 3; ++c) { R.ez1[c] = ea[c] + (-h / 2.0) * ka[c]; R.ez2[c] = ea[c] + (h / 2.0) * ka[c]; }
+    mv3(D, R.ez1, R.sz1);
+    mv3(D, R.ez2, R.sz2);
+    return true;
+}
+
+// quad4_bilinear_corner_forces: Gauss values N = Cm eps, M = -Cb kappa
+// extrapolated to the corners (interp_2x2_gauss_sigma, FEMKernels.jl:5210-5227).
+void q4_corner_forces(double E, double nu, double h, double br, const double eps[4][3], const double kap[4][3],
+                      double Nc[4][3], double Mc[4][3]) {
+    double D[3][3], Cm[3][3], Cb[3][3];
+    plane_stress_D(E, nu, D);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) { Cm[i][j] = D[i][j] * h; Cb[i][j] = br * D[i][j] * (h * h * h / 12.0); }
+    double Ng[4][3], Mg[4][3];
+    for (int g = 0; g < 4; ++g) {
+        mv3(Cm, eps[g], Ng[g]);
+        double t[3];
+        mv3(Cb, kap[g], t);
+        for (int c = 0; c < 3; ++c) Mg[g][c] = -t[c];
+    }
+    const double pt = 1.0 / std::sqrt(3.0);
+    const double cp[4][2] = {{-1.0, -1.0}, {1.0, -1.0}, {1.0, 1.0}, {-1.0, 1.0}};
+    for (int i = 0; i < 4; ++i) {
+        double xi = cp[i][0], eta = cp[i][1];
+        double lx1 = (pt - xi) / (2.0 * pt), lx2 = (xi + pt) / (2.0 * pt), ly1 = (pt - eta) / (2.0 * pt), ly2 = (eta + pt) / (2.0 * pt);
+        double w[4] = {lx1 * ly1, lx2 * ly1, lx2 * ly2, lx1 * ly2};
+        for (int c = 0; c < 3; ++c) {
+            Nc[i][c] = w[0] * Ng[0][c] + w[1] * Ng[1][c] + w[2] * Ng[2][c] + w[3] * Ng[3][c];
+            Mc[i][c] = w[0] * Mg[0][c] + w[1] * Mg[1][c] + w[2] * Mg[2][c] + w[3] * Mg[3][c];
+        }
+    }
+}
+
+// _quad4_equilibrium_shear_from_bending + _quad4_blend_recovered_shear
+// (stress_recovery.jl:88-130).
+void q4_equilibrium_blend(const double lc[4][2], const double Mc[4][3], double Q[2]) {
+    const double dNr[4] = {-0.25, 0.25, 0.25, -0.25}, dNs[4] = {-0.25, -0.25, 0.25, 0.25};
+    double J11 = 0, J12 = 0, J21 = 0, J22 = 0;
+    for (int k = 0; k < 4; ++k) { J11 += dNr[k] * lc[k][0]; J12 += dNr[k] * lc[k][1]; J21 += dNs[k] * lc[k][0]; J22 += dNs[k] * lc[k][1]; }
+    double det = J11 * J22 - J12 * J21;
+    if (std::fabs(det) < 1e-12) return;
+    double i11 = J22 / det, i12 = -J12 / det, i21 = -J21 / det, i22 = J11 / det;
+    double rx = 0, sx = 0, ry = 0, sy = 0;
+    for (int k = 0; k < 4; ++k) { rx += dNr[k] * Mc[k][0]; sx += dNs[k] * Mc[k][0]; ry += dNr[k] * Mc[k][1]; sy += dNs[k] * Mc[k][1]; }
+    double eq[2] = {i11 * rx + i12 * sx, i21 * ry + i22 * sy};
+    for (int i = 0; i < 2; ++i)
+        if (std::isfinite(eq[i]) && std::fabs(eq[i]) < std::fabs(Q[i])) Q[i] = eq[i];
+}
+
+// quad4_is_axis_aligned_rectangle (FEMKernels.jl:5050-5077), tol 1e-8.
+bool q4_is_rectangle(const double lc[4][2]) {
+    const double tol = 1e-8;
+    double e[4][2];
+    for (int k = 0; k < 4; ++k) { int n = (k + 1) % 4; e[k][0] = lc[n][0] - lc[k][0]; e[k][1] = lc[n][1] - lc[k][1]; }
+    double L[4], Lmax = 1e-12;
+    for (int k = 0; k < 4; ++k) { L[k] = std::sqrt(e[k][0] * e[k][0] + e[k][1] * e[k][1]); Lmax = std::max(Lmax, L[k]); }
+    double as = Lmax * Lmax;
+    auto cr = [&](int a, int b) { return e[a][0] * e[b][1] - e[a][1] * e[b][0]; };
+    auto dt = [&](int a, int b) { return e[a][0] * e[b][0] + e[a][1] * e[b][1]; };
+    if (std::fabs(cr(0, 2)) > tol * as || std::fabs(cr(1, 3)) > tol * as) return false;
+    if (std::fabs(dt(0, 1)) > tol * as || std::fabs(dt(1, 2)) > tol * as || std::fabs(dt(2, 3)) > tol * as ||
+        std::fabs(dt(3, 0)) > tol * as)
+        return false;
+    if (std::fabs(L[0] - L[2]) > tol * Lmax || std::fabs(L[1] - L[3]) > tol * Lmax) return false;
+    return true;
+}
+
+// CQUAD4 branch of recover_shell_stresses! (stress_recovery.jl:179-302).
+void q4_recover(const double lc[4][2], const double u[24], double E, double nu, double h, double br, bool pressure_deck,
+                ShellRec &R) {
+    double eps[4][3], kap[4][3];
+    if (!q4_stress_strain(lc, u, E, nu, h, br, R, eps, kap)) { R = ShellRec(); R.ok = false; return; }
+    q4_corner_forces(E, nu, h, br, eps, kap, R.Nc, R.Mc);
+    double Qo[2] = {R.Q[0], R.Q[1]};
+    if (std::fabs(br) > 1e-12) q4_equilibrium_blend(lc, R.Mc, Qo);
+    // _quad4_pressure_resultant_moment_scale (stress_recovery.jl:131-161)
+    double scale = 1.0;
+    if (pressure_deck && std::fabs(br) > 1e-12 && q4_is_rectangle(lc)) {
+        double mq = std::max(std::fabs(Qo[0]), std::fabs(Qo[1]));
+        double mn = std::max(std::fabs(R.N[0]), std::max(std::fabs(R.N[1]), std::fabs(R.N[2])));
+        if (mq > 1e-8 && !(mn > std::max(1e-6, 1e-4 * mq))) scale = 0.99;
+    }
+    if (scale != 1.0)
+        for (int c = 0; c < 3; ++c) {
+            R.M[c] *= scale;
+            for (int k = 0; k < 4; ++k) R.Mc[k][c] *= scale;
+        }
+    for (int k = 0; k < 4; ++k) R.Mc[k][2] = R.M[2];
+    R.Q[0] = Qo[0];
+    R.Q[1] = Qo[1];
+}
+
+// CTRIA3 macro recovery: tria3_plate_macro_data (FEMKernels.jl:7157-7209) with
+// the recovery constitutive set of tria3_plate_macro_shear_resultant /
+// tria3_plate_macro_average_moment (:7225-7305: Cm = D h, Cb = D h^3/12,
+// Cs = 5/6 G h, G = E / 2(1 + nu), k6rot 100), then stress_strain_quad4 on each
+// virtual quad with only its plate dofs.  Area-weighted sums of the quads'
+// moments and shears; false where a factorisation raises.
+bool t3_macro_fields(const double lc[3][2], const double u[18], double E, double nu, double h, double br, double Msum[3],
+                     double Qsum[2], double &Asum) {
+    double x[3] = {lc[0][0], lc[1][0], lc[2][0]}, y[3] = {lc[0][1], lc[1][1], lc[2][1]};
+    double pts[7][2];
+    for (int i = 0; i < 3; ++i) { pts[i][0] = x[i]; pts[i][1] = y[i]; }
+    pts[3][0] = (x[0] + x[1]) / 2; pts[3][1] = (y[0] + y[1]) / 2;
+    pts[4][0] = (x[1] + x[2]) / 2; pts[4][1] = (y[1] + y[2]) / 2;
+    pts[5][0] = (x[2] + x[0]) / 2; pts[5][1] = (y[2] + y[0]) / 2;
+    pts[6][0] = (x[0] + x[1] + x[2]) / 3; pts[6][1] = (y[0] + y[1] + y[2]) / 3;
+    const int quads[3][4] = {{0, 3, 6, 5}, {1, 4, 6, 3}, {2, 5, 6, 4}};
+    const int pd[12] = {2, 3, 4, 8, 9, 10, 14, 15, 16, 20, 21, 22};
+    double D[3][3], Cm[3][3], Cb[3][3], Cs[2][2];
+    plane_stress_D(E, nu, D);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) { Cm[i][j] = D[i][j] * h; Cb[i][j] = D[i][j] * (h * h * h / 12.0); }
+    double G = E / (2.0 * (1.0 + nu));
+    Cs[0][0] = Cs[1][1] = 5.0 / 6.0 * G * h;
+    Cs[0][1] = Cs[1][0] = 0.0;
+    double K21[21][21] = {};
+    for (int q = 0; q < 3; ++q) {
+        double qc[4][2];
+        for (int k = 0; k < 4; ++k) { qc[k][0] = pts[quads[q][k]][0]; qc[k][1] = pts[quads[q][k]][1]; }
+        double Kq[24][24];
+        q4_stiffness(qc, Cm, Cb, Cs, h, G, 100.0, 1.0, /*bending_incomp=*/false, /*membrane_incomp=*/true, Kq);
+        int ed[12];
+        for (int k = 0; k < 4; ++k)
+            for (int dd = 0; dd < 3; ++dd) ed[3 * k + dd] = 3 * quads[q][k] + dd;
+        for (int i = 0; i < 12; ++i)
+            for (int j = 0; j < 12; ++j) K21[ed[i]][ed[j]] += Kq[pd[i]][pd[j]];
+    }
+    double Kii[144], Aint[12 * 9];
+    for (int i = 0; i < 12; ++i) {
+        for (int j = 0; j < 12; ++j) Kii[i * 12 + j] = K21[9 + i][9 + j];
+        for (int j = 0; j < 9; ++j) Aint[i * 9 + j] = K21[9 + i][j];
+    }
+    if (!lu_solve(12, 9, Kii, Aint)) return false;
+    const int up[9] = {2, 3, 4, 8, 9, 10, 14, 15, 16};
+    double ua[21];
+    for (int i = 0; i < 9; ++i) ua[i] = u[up[i]];
+    for (int i = 0; i < 12; ++i) {
+        double s = 0.0;
+        for (int j = 0; j < 9; ++j) s += -Aint[i * 9 + j] * ua[j];
+        ua[9 + i] = s;
+    }
+    Msum[0] = Msum[1] = Msum[2] = 0.0;
+    Qsum[0] = Qsum[1] = 0.0;
+    Asum = 0.0;
+    for (int q = 0; q < 3; ++q) {
+        double qc[4][2], uq[24] = {};
+        for (int k = 0; k < 4; ++k) {
+            qc[k][0] = pts[quads[q][k]][0]; qc[k][1] = pts[quads[q][k]][1];
+            for (int dd = 0; dd < 3; ++dd) uq[pd[3 * k + dd]] = ua[3 * quads[q][k] + dd];
+        }
+        ShellRec Rq;
+        double eps[4][3], kap[4][3];
+        if (!q4_stress_strain(qc, uq, E, nu, h, br, Rq, eps, kap)) return false;
+        // _tria3_virtual_quad_area (FEMKernels.jl:7151-7155)
+        double a1 = (qc[1][0] - qc[0][0]) * (qc[3][1] - qc[0][1]) - (qc[3][0] - qc[0][0]) * (qc[1][1] - qc[0][1]);
+        double a2 = (qc[2][0] - qc[1][0]) * (qc[3][1] - qc[1][1]) - (qc[3][0] - qc[1][0]) * (qc[2][1] - qc[1][1]);
+        double area = (std::fabs(a1) + std::fabs(a2)) / 2;
+        for (int c = 0; c < 3; ++c) Msum[c] += area * Rq.M[c];
+        for (int c = 0; c < 2; ++c) Qsum[c] += area * Rq.Q[c];
+        Asum += area;
+    }
+    return true;
+}
+
+// CTRIA3 branch of recover_shell_stresses! (stress_recovery.jl:303-354):
+// stress_strain_tria3 (FEMKernels.jl:7391-7432) and, for macro weight w > 0,
+// _blend_tria3_macro_bending_iso! (stress_recovery.jl:53-86).
+void t3_recover(const double lc[3][2], const double u[18], double E, double nu, double h, double br, double w, ShellRec &R) {
+    R = ShellRec();
+    double x[3] = {lc[0][0], lc[1][0], lc[2][0]}, y[3] = {lc[0][1], lc[1][1], lc[2][1]};
+    double A = 0.5 * std::fabs(x[0] * (y[1] - y[2]) + x[1] * (y[2] - y[0]) + x[2] * (y[0] - y[1]));
+    if (A < 1e-12) return;  // the reference returns zeros for a degenerate triangle
+    double b[3] = {(y[1] - y[2]) / (2 * A), (y[2] - y[0]) / (2 * A), (y[0] - y[1]) / (2 * A)};
+    double c[3] = {(x[2] - x[1]) / (2 * A), (x[0] - x[2]) / (2 * A), (x[1] - x[0]) / (2 * A)};
+    double eps[3] = {0, 0, 0}, kap[3] = {0, 0, 0};
+    for (int i = 0; i < 3; ++i) {
+        double ux = u[6 * i], uy = u[6 * i + 1], rx = u[6 * i + 3], ry = u[6 * i + 4];
+        eps[0] += b[i] * ux; eps[1] += c[i] * uy; eps[2] += c[i] * ux + b[i] * uy;
+        kap[0] += b[i] * ry; kap[1] += -c[i] * rx; kap[2] += c[i] * ry - b[i] * rx;
+    }
+    double D[3][3], De[3], Dk[3];
+    plane_stress_D(E, nu, D);
+    mv3(D, eps, De);
+    mv3(D, kap, Dk);
+    for (int k = 0; k < 3; ++k) { R.N[k] = De[k] * h; R.M[k] = -br * Dk[k] * (h * h * h / 12.0); }
+    double Msum[3] = {0, 0, 0}, Qsum[2] = {0, 0}, Asum = 0.0;
+    bool have_macro = false;
+    if (br > 1e-12) {
+        if (!t3_macro_fields(lc, u, E, nu, h, br, Msum, Qsum, Asum)) { R = ShellRec(); R.ok = false; return; }
+        have_macro = true;
+        if (Asum > 1e-12) { R.Q[0] = Qsum[0] / Asum; R.Q[1] = Qsum[1] / Asum; }
+    }
+    for (int k = 0; k < 3; ++k) { R.ez1[k] = eps[k] + (-h / 2.0) * kap[k]; R.ez2[k] = eps[k] + (h / 2.0) * kap[k]; }
+    mv3(D, R.ez1, R.sz1);
+    mv3(D, R.ez2, R.sz2);
+    if (w > 0.0 && std::fabs(br) > 1e-12 && have_macro) {
+        double Mm[3] = {0, 0, 0};
+        if (Asum > 1e-12)
+            for (int k = 0; k < 3; ++k) Mm[k] = Msum[k] / Asum;
+        if (std::isfinite(Mm[0]) && std::isfinite(Mm[1]) && std::isfinite(Mm[2])) {
+            double Mb[3], Dm[9], rhs[3];
+            for (int k = 0; k < 3; ++k) Mb[k] = (1.0 - w) * R.M[k] + w * Mm[k];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) Dm[3 * i + j] = D[i][j];
+            for (int k = 0; k < 3; ++k) rhs[k] = Mb[k];
+            lu_solve(3, 1, Dm, rhs);
+            double kb[3], em[3];
+            for (int k = 0; k < 3; ++k) {
+                kb[k] = -(12.0 / (br * h * h * h)) * rhs[k];
+                em[k] = (R.ez1[k] + R.ez2[k]) / 2.0;
+            }
+            for (int k = 0; k < 3; ++k) {
+                R.M[k] = Mb[k];
+                R.ez1[k] = em[k] + (-h / 2.0) * kb[k];
+                R.ez2[k] = em[k] + (h / 2.0) * kb[k];
+            }
+            mv3(D, R.ez1, R.sz1);
+            mv3(D, R.ez2, R.sz2);
+        }
+    }
+}
+
+// _tria3_shell_macro_blend_weights (stress_recovery.jl:20-51): edges counted
+// over every CQUAD4 and CTRIA3; w = clamp((shared edges - 1) / 2, 0, 1).
+void t3_macro_weights(const jfg_model_desc *d, std::vector<double> &w) {
+    std::map<std::pair<int32_t, int32_t>, int> cnt;
+    auto key = [](int32_t a, int32_t b) { return a < b ? std::make_pair(a, b) : std::make_pair(b, a); };
+    for (int64_t e = 0; e < d->n_quad4; ++e)
+        for (int k = 0; k < 4; ++k) cnt[key(d->quad4_nodes[4 * e + k], d->quad4_nodes[4 * e + (k + 1) % 4])] += 1;
+    for (int64_t e = 0; e < d->n_tria3; ++e)
+        for (int k = 0; k < 3; ++k) cnt[key(d->tria3_nodes[3 * e + k], d->tria3_nodes[3 * e + (k + 1) % 3])] += 1;
+    w.assign(d->n_tria3, 0.0);
+    for (int64_t e = 0; e < d->n_tria3; ++e) {
+        int shared = 0;
+        for (int k = 0; k < 3; ++k) shared += cnt[key(d->tria3_nodes[3 * e + k], d->tria3_nodes[3 * e + (k + 1) % 3])] > 1;
+        w[e] = std::min(1.0, std::max(0.0, (shared - 1) / 2.0));
+    }
+}
+
+void write_shell_rec(const ShellRec &R, double *o) {
+    std::fill(o, o + JFG_SHELL_REC, 0.0);
+    if (!R.ok) return;
+    for (int k = 0; k < 3; ++k) {
+        o[k] = R.N[k]; o[3 + k] = R.M[k]; o[8 + k] = R.sz1[k]; o[11 + k] = R.sz2[k]; o[14 + k] = R.ez1[k]; o[17 + k] = R.ez2[k];
+    }
+    o[6] = R.Q[0]; o[7] = R.Q[1];
+    // compute_principal_2d (FEMKernels.jl:5921-5925), first root
+    double s11 = R.sz1[0], s22 = R.sz1[1], s12 = R.sz1[2];
+    o[20] = (s11 + s22) / 2.0 + std::sqrt(((s11 - s22) / 2.0) * ((s11 - s22) / 2.0) + s12 * s12);
+    o[21] = 1.0;
+    for (int k = 0; k < 4; ++k)
+        for (int c = 0; c < 3; ++c) { o[22 + 3 * k + c] = R.Nc[k][c]; o[34 + 3 * k + c] = R.Mc[k][c]; }
+    auto vm = [](const double *s) { return std::sqrt(s[0] * s[0] - s[0] * s[1] + s[1] * s[1] + 3 * s[2] * s[2]); };
+    o[46] = vm(R.sz1);
+    o[47] = vm(R.sz2);
+}
+
+// CBAR/CBEAM loop body of recover_bar_stresses! (stress_recovery.jl:446-503):
+// forces_frame3d (FEMKernels.jl:215-229) on the offset-aware local
+// displacements, axial stress and the section-point stresses.
+void bar_recover(const jfg_model_desc *d, int64_t e, const double *u, const double *pts, double *o) {
+    std::fill(o, o + JFG_BAR_REC, 0.0);
+    double L, T12[12][12];
+    bool off;
+    if (!bar_setup(d, e, L, T12, off)) return;
+    const int32_t *nd = d->bar_nodes + 2 * e;
+    double ub[12] = {};
+    for (int k = 0; k < 2; ++k) {
+        const double *ug = u + 6 * (int64_t)nd[k];
+        for (int dd = 0; dd < 6; ++dd)
+            for (int q = 0; q < 6; ++q) ub[6 * k + dd] += T12[6 * k + dd][6 * k + q] * ug[q];
+    }
+    double A, Iy, Iz, I12, J, E, G, Asy, Asz;
+    bar_section(d->bar_prop + JFG_BAR_PROP * e, A, Iy, Iz, I12, J, E, G, Asy, Asz);
+    double k[12][12], f[12];
+    frame3d_stiffness(L, A, Iy, Iz, J, E, G, Asy, Asz, I12, k);
+    for (int i = 0; i < 12; ++i) {
+        double s = 0.0;
+        for (int q = 0; q < 12; ++q) s += k[i][q] * ub[q];
+        f[i] = s;
+    }
+    o[0] = f[6]; o[1] = -f[1]; o[2] = -f[2]; o[3] = -f[3];
+    o[4] = -f[5]; o[5] = f[4]; o[6] = f[11]; o[7] = -f[10];
+    o[8] = std::fabs(A) > 1e-30 ? f[6] / A : 0.0;
+    if (pts) {
+        const double *p = pts + JFG_BAR_POINTS * e;
+        double den = Iz * Iy - I12 * I12;
+        for (int end = 0; end < 2; ++end) {
+            double m1 = end == 0 ? o[4] : o[6], m2 = end == 0 ? o[5] : o[7];
+            for (int j = 0; j < 4; ++j) {
+                double yj = p[2 * j], zj = p[2 * j + 1];
+                double s = std::fabs(den) > 1e-30 ? ((m1 * Iy - m2 * I12) * yj + (m2 * Iz - m1 * I12) * zj) / den
+                                                  : m1 * yj / std::max(Iz, 1e-30) + m2 * zj / std::max(Iy, 1e-30);
+                o[9 + 4 * end + j] = p[8] * s;
+            }
+        }
+    }
+    o[17] = 1.0;
+}
+
+// ---------------------------------------------------------------------------
 // exported oracle API (test infrastructure)
 // ---------------------------------------------------------------------------
 
@@ -1181,6 +1622,37 @@ void oracle_dkdh(const jfg_model_desc *d, const double *a, const double *b, doub
             }
         }
     }
+}
+
+// SOL 101 output recovery over a model (records as in jfem_gpu.h,
+// JFG_SHELL_REC per shell -- CQUAD4s then CTRIA3s -- and JFG_BAR_REC per bar).
+void oracle_recover(const jfg_model_desc *d, const double *u, const double *bar_points, int32_t flags,
+                    double *shell_out, double *bar_out) {
+    const bool pressure_deck = (flags & JFG_RECOVER_PRESSURE_DECK) && d->n_bar == 0 && d->n_rbe2 == 0;
+    if (shell_out) {
+        std::vector<double> w;
+        t3_macro_weights(d, w);
+#pragma omp parallel for schedule(dynamic, 64)
+        for (int64_t i = 0; i < d->n_quad4 + d->n_tria3; ++i) {
+            const bool quad = i < d->n_quad4;
+            const int64_t e = quad ? i : i - d->n_quad4;
+            const int nn = quad ? 4 : 3;
+            const int32_t *nd = (quad ? d->quad4_nodes : d->tria3_nodes) + nn * e;
+            const double *pr = (quad ? d->quad4_prop : d->tria3_prop) + JFG_SHELL_PROP * e;
+            double lc[4][2], Q[36], ul[24];
+            shell_setup(d, nd, nn, lc, Q);
+            to_local(nn, Q, u, nd, ul);
+            ShellRec R;
+            if (quad) q4_recover(lc, ul, pr[1], pr[2], pr[0], pr[4], pressure_deck, R);
+            else {
+                double lc3[3][2] = {{lc[0][0], lc[0][1]}, {lc[1][0], lc[1][1]}, {lc[2][0], lc[2][1]}};
+                t3_recover(lc3, ul, pr[1], pr[2], pr[0], pr[4], w[e], R);
+            }
+            write_shell_rec(R, shell_out + JFG_SHELL_REC * i);
+        }
+    }
+    if (bar_out)
+        for (int64_t e = 0; e < d->n_bar; ++e) bar_recover(d, e, u, bar_points, bar_out + JFG_BAR_REC * e);
 }
 
 int oracle_num_threads(void) {

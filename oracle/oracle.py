@@ -54,6 +54,7 @@ def lib():
         L.oracle_t3_generic_local.argtypes = [pd, C.c_double, C.c_double, C.c_double, pd, pd]
         pu8 = C.POINTER(C.c_uint8)
         L.oracle_dkdh.argtypes = [C.POINTER(JfgModelDesc), pd, pd, pd, pd, pd, pu8, pu8, pd]
+        L.oracle_recover.argtypes = [C.POINTER(JfgModelDesc), pd, pd, C.c_int32, pd, pd]
         _lib = L
     return _lib
 
@@ -181,6 +182,28 @@ def dkdh(m: ModelArrays, a=None, b=None, u=None, mask_q4=None, mask_t3=None):
                   ptr(load, pd))
     del keep
     return cq, ct, load
+
+
+SHELL_REC, BAR_REC, BAR_POINTS = 48, 18, 9
+RECOVER_PRESSURE_DECK = 1
+
+
+def recover(m: ModelArrays, u, bar_points=None, flags: int = 0):
+    """SOL 101 output recovery of the model (see oracle_recover): the shell
+    records (CQUAD4s then CTRIA3s, SHELL_REC values each) and the bar records
+    (BAR_REC values each) for displacement u (ndof)."""
+    L = lib()
+    desc, keep = make_desc(m)
+    pd = C.POINTER(C.c_double)
+    ns, nb = m.q4_nodes.shape[0] + m.t3_nodes.shape[0], m.bar_nodes.shape[0]
+    u = np.ascontiguousarray(u, np.float64)
+    pts = None if bar_points is None else np.ascontiguousarray(bar_points, np.float64).reshape(nb, BAR_POINTS)
+    shell = np.zeros((ns, SHELL_REC))
+    bar = np.zeros((nb, BAR_REC))
+    L.oracle_recover(C.byref(desc), u.ctypes.data_as(pd), None if pts is None else pts.ctypes.data_as(pd), int(flags),
+                     shell.ctypes.data_as(pd), bar.ctypes.data_as(pd))
+    del keep
+    return shell, bar
 
 
 def to_scipy(colptr, rowval, nzval, ndof):
