@@ -110,6 +110,21 @@ def time_cpu_oracle(seconds: float, reps_max: int = 50):
     return m.n_elements * reps / el, threads, f"{m.name}: {m.n_elements} elements, {reps} K+KG passes, {el:.1f} s"
 
 
+def time_cpu_recovery(reps: int = 3):
+    """Oracle SOL 101 output recovery on the same bounded sample (elements/s)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # CPU restatement: reported baseline only
+    from jf_2026_05_19_b200 import decks
+    m = cpu_sample_model()
+    u = decks.smooth_displacement(m, seed=1)
+    O.recover(m, u)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        O.recover(m, u)
+    el = time.perf_counter() - t0
+    return m.n_elements * reps / el
+
+
 class ClockSampler:
     """SM clock and clock-event reasons sampled during the timed region.
 
@@ -684,10 +699,29 @@ def main():
     e2e_el = s2.elapsed_time(e2) / 1e3
     e2e_el = max_over_ranks(e2e_el, dist, dev)
 
+    # SOL 101 output recovery of the same model and displacement, timed on its
+    # own after the step (it follows the static solve, not the assembly)
+    counts = m.counts()
+    rec_sh = torch.empty((counts["quad4"] + counts["tria3"], 48), dtype=torch.float64, device=dev)
+    rec_bar = torch.empty((max(counts["bar"], 1), 18), dtype=torch.float64, device=dev)
+
+    def recover():
+        g.recover_stresses_device(u_dev.data_ptr(), None, 0, rec_sh.data_ptr(), rec_bar.data_ptr() if counts["bar"] else None)
+
+    for _ in range(3):
+        recover()
+    torch.cuda.synchronize()
+    s3 = torch.cuda.Event(enable_timing=True); e3 = torch.cuda.Event(enable_timing=True)
+    s3.record(stream)
+    for _ in range(5):
+        recover()
+    e3.record(stream)
+    e3.synchronize()
+    rec_ms = s3.elapsed_time(e3) / 5
+
     n_el = m.n_elements
     value = world * n_el * args.steps / elapsed
     e2e_value = world * n_el * e2e_steps / e2e_el
-    counts = m.counts()
     # dominant kernel over the timed region
     per_kernel = {}
     for tag, tt, nn in (("k", kt, kn), ("kg", gt, gn)):
@@ -728,10 +762,14 @@ def main():
                     "steps": e2e_steps},
             "roofline": roof, "gpu_launches": launches_per_step * args.steps, "clocks": clk,
             "kernel_ms": per_kernel, "fp64_dgemm_tflops": fp64_peak, "model_stats": st,
-            "whole_step_roofline": {"flops": roofline.flops_per_step(counts), "bytes": roofline.bytes_per_step(counts, g.nnz)}}
+            "whole_step_roofline": {"flops": roofline.flops_per_step(counts), "bytes": roofline.bytes_per_step(counts, g.nnz)},
+            "recovery": {"ms": rec_ms, "elements_per_s": n_el / rec_ms * 1e3, "timed_calls": 5,
+                         "output_bytes": 8 * (rec_sh.numel() + (rec_bar.numel() if counts["bar"] else 0)),
+                         "note": "jfg_recover_stresses_device on the same model and u, outside the timed step"}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, thr, sample = time_cpu_oracle(args.cpu_seconds)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample}
+        line["recovery"]["cpu_port_elements_per_s"] = time_cpu_recovery()
     if rank == 0:
         print(json.dumps(line), flush=True)
     g.close()

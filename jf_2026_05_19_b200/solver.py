@@ -1,6 +1,6 @@
-"""Host-side mirror of the reference's two assembly calls, backed by the CUDA library.
+"""Host-side mirror of the reference's assembly and output-recovery calls, backed by the CUDA library.
 
-Same names, arguments and return values as OpenJFEM's
+Same names, arguments and return values (or filled dictionaries) as OpenJFEM's
 
     Solver.assemble_stiffness(model; bending_incomp, shear_center_only,
         membrane_incomp, pcomp_membrane_incomp, snorm_angle_override,
@@ -8,6 +8,14 @@ Same names, arguments and return values as OpenJFEM's
     Solver.assemble_geometric_stiffness(model, id_map, node_coords, node_R,
         ndof, u_global, snorm_normals, rbe3_map; snorm_angle_override,
         buckling_subcase, static_load_id, timings)       src/solver/assembly.jl:4382-4386
+
+and the per-element loops of the SOL 101 output recovery that follows the
+static solve,
+
+    recover_shell_stresses!(model, id_map, X, node_R, u_global, snorm_normals,
+        stresses, results_json)                          src/solver/stress_recovery.jl:163-430
+    recover_bar_stresses!(model, id_map, X, node_R, u_global, stresses,
+        results_json)                                    src/solver/stress_recovery.jl:432-593
 
 ``model`` is the nested dictionary the reference's model builder produces
 (``GRIDs``, ``CORDs``, ``CSHELLs``, ``PSHELLs``, ``MATs``, ``CBARs``,
