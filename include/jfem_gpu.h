@@ -10,7 +10,10 @@
  * :1452-1457.  The caller keeps its own model build, SPC/MPC reduction,
  * factorization and eigensolve; this library only produces the same sparse
  * matrices (Julia SparseMatrixCSC{Float64,Int64} arrays: 1-based colptr,
- * rowval, nzval) that those two functions return.
+ * rowval, nzval) that those two functions return.  On the same element
+ * kernels it also serves the steps either side: the free-dof extraction,
+ * shell-thickness sensitivities of K and KG, SOL 101 output recovery, and a
+ * device-resident request loop.
  *
  * Every entry point takes plain pointers and sizes.  Host arrays are owned by
  * the caller; the library copies what it needs and keeps no pointer into
@@ -254,6 +257,23 @@ jfg_status jfg_dkdh_contract_device(jfg_model *m, const double *a_dev, const dou
                                     double *c_t3_dev);
 jfg_status jfg_dkdh_load_device(jfg_model *m, const double *u_dev, const uint8_t *mask_q4_dev, const uint8_t *mask_t3_dev,
                                 double *load_dev);
+
+/* ---- Per-element KG contractions (buckling sensitivities) ----------------
+ * c_q4[e] = a_e' T_e' KG_e(u) T_e b_e for every CQUAD4, likewise c_t3, with KG_e
+ * the element matrix of jfg_assemble_kg (before constraints).  With a = b =
+ * phi and divided by the element thickness this is phi' dKG_e/dh phi, the
+ * per-element term of _dKg_dx_phi_thickness (src/solver/adjoint_buckling.jl:
+ * 2079-2150): at fixed u the membrane stress does not depend on h, and KG is
+ * linear in h.  That function's flat-isotropic context uses the assembly's
+ * KG formulation when the deck has line elements; for shell-only decks it
+ * switches to the enhanced membrane modes (:930-951), which this library does
+ * not build.  Decks whose KG assembly raises (offset bars) raise here too.
+ * The _device form runs asynchronously on the handle's stream and uses the
+ * handle's staging, so it must not overlap an assembly of the same handle. */
+jfg_status jfg_kg_contract(jfg_model *m, const double *u_global, const double *a, const double *b, double *c_q4,
+                           double *c_t3);
+jfg_status jfg_kg_contract_device(jfg_model *m, const double *u_dev, const double *a_dev, const double *b_dev,
+                                  double *c_q4_dev, double *c_t3_dev);
 
 /* ---- SOL 101 output recovery ----------------------------------------------
  * Replace the per-element loops of recover_shell_stresses! and

@@ -630,4 +630,64 @@ __global__ void __launch_bounds__(32 * T3D_WARPS) t3_dkdh_kernel(int64_t nt, con
     }
 }
 
+// Per-element a_e' KG_e b_e from the staged KG blocks of one shell type (the
+// KG element kernels' output before the reduction; the element matrices of
+// the KG assembly before constraints).  NN nodes, NN(NN+1)/2 node pairs per
+// element in slot-map order; a regular slot holds the translation 3x3 in
+// stored orientation, an RBE2-path pair its raw 6x6 block.  With a = b = phi
+// this is phi' KG_e phi, and divided by h_e the thickness sensitivity of
+// _dKg_dx_phi_thickness (src/solver/adjoint_buckling.jl:2079-2150): KG is
+// linear in h at fixed u.
+template <int NN>
+__global__ void __launch_bounds__(128) kg_contract_kernel(int64_t ne, const int32_t *__restrict__ nodes,
+                                                          const int32_t *__restrict__ blk_slot,
+                                                          const double *__restrict__ staging,
+                                                          const double *__restrict__ exc_raw,
+                                                          const double *__restrict__ a, const double *__restrict__ b,
+                                                          double *__restrict__ c) {
+    constexpr int NP = NN * (NN + 1) / 2;
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    int32_t nd[NN];
+#pragma unroll
+    for (int k = 0; k < NN; ++k) nd[k] = __ldg(nodes + NN * e + k);
+    double s = 0.0;
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+        int pa, pb;
+        if (NN == 4) {
+            q4_pair(p, pa, pb);
+        } else {
+            pa = (p >= 3) + (p >= 5);
+            pb = pa + p - (pa == 0 ? 0 : (pa == 1 ? 3 : 5));
+        }
+        const int32_t sl = __ldg(blk_slot + NP * e + p);
+        const double *ua = a + 6 * (int64_t)nd[pa], *ub = b + 6 * (int64_t)nd[pb];
+        const double *va = a + 6 * (int64_t)nd[pb], *vb = b + 6 * (int64_t)nd[pa];
+        if (sl >= 0) {
+            const double *S = staging + 12 * (int64_t)(sl & kBlkIndexMask);
+            const bool t = sl & kBlkTranspose;
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const double g = t ? __ldg(S + 3 * j + i) : __ldg(S + 3 * i + j);
+                    s += __ldg(ua + i) * g * __ldg(ub + j);
+                    if (pa != pb) s += __ldg(va + j) * g * __ldg(vb + i);
+                }
+        } else {
+            const double *R = exc_raw + 36 * (int64_t)(-(sl + 1));
+#pragma unroll
+            for (int i = 0; i < 6; ++i)
+#pragma unroll
+                for (int j = 0; j < 6; ++j) {
+                    const double g = __ldg(R + 6 * i + j);
+                    s += __ldg(ua + i) * g * __ldg(ub + j);
+                    if (pa != pb) s += __ldg(va + j) * g * __ldg(vb + i);
+                }
+        }
+    }
+    c[e] = s;
+}
+
 }  // namespace jfg

@@ -124,8 +124,8 @@ struct jfg_model {
     cudaEvent_t *ev = nullptr;
     float last_elem_ms = 0.f, last_reduce_ms = 0.f, last_total_ms = 0.f;
     float last_kernel_ms[6] = {0, 0, 0, 0, 0, 0};  // quad4, tria3, bar, expand, reduce, diag
-    double acc_ms[2][6] = {{0, 0, 0, 0, 0, 0}, {0, 0, 0, 0, 0, 0}};
-    int64_t acc_calls[2] = {0, 0};
+    double acc_ms[3][6] = {{0, 0, 0, 0, 0, 0}, {0, 0, 0, 0, 0, 0}, {0, 0, 0, 0, 0, 0}};  // K, KG, KG contractions
+    int64_t acc_calls[3] = {0, 0, 0};
     std::vector<void *> allocs;
 };
 
@@ -1675,6 +1675,54 @@ jfg_status jfg_dkdh_load(jfg_model *m, const double *u, const uint8_t *mask_q4, 
     CK(cudaMemcpyAsync(load, dl, sizeof(double) * m->ndof, cudaMemcpyDeviceToHost, m->stream));
     CK(cudaStreamSynchronize(m->stream));
     return JFG_OK;
+}
+
+// Per-element KG contractions: the KG element kernels (no reduction), then
+// a' KG_e b from their staged blocks.  Timed as its own kind of event set.
+jfg_status jfg_kg_contract_device(jfg_model *m, const double *u_dev, const double *a_dev, const double *b_dev,
+                                  double *c_q4_dev, double *c_t3_dev) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    if (!u_dev || !a_dev || !b_dev) return fail(m, JFG_ERR_INVALID, "null vector");
+    if (m->bar_offsets)
+        return fail(m, JFG_ERR_REFERENCE_RAISES,
+                    "assemble_geometric_stiffness raises BoundsError for CBAR/CBEAM with offsets (assembly.jl:6326)");
+    jfg_status st = begin_set(m, 2);
+    if (st) return st;
+    Batch bt = single_batch(m);
+    bt.u = u_dev;
+    st = launch_elements(m, true, bt);
+    if (st) return st;
+    if (m->nq && c_q4_dev) {
+        kg_contract_kernel<4><<<(unsigned)cdiv(m->nq, 128), 128, 0, m->stream>>>(
+            m->nq, m->d_q4n, m->d_blk_slot + m->pair_q4, m->d_staging, m->d_exc_raw, a_dev, b_dev, c_q4_dev);
+        CK(cudaGetLastError());
+    }
+    if (m->nt && c_t3_dev) {
+        kg_contract_kernel<3><<<(unsigned)cdiv(m->nt, 128), 128, 0, m->stream>>>(
+            m->nt, m->d_t3n, m->d_blk_slot + m->pair_t3, m->d_staging, m->d_exc_raw, a_dev, b_dev, c_t3_dev);
+        CK(cudaGetLastError());
+    }
+    CK(mark(m, 4));
+    CK(mark(m, 5));
+    CK(mark(m, 6));
+    return JFG_OK;
+}
+
+jfg_status jfg_kg_contract(jfg_model *m, const double *u, const double *a, const double *b, double *c_q4, double *c_t3) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    if (!u || !a || !b) return fail(m, JFG_ERR_INVALID, "null vector");
+    jfg_status st = dk_buffers(m);
+    if (st) return st;
+    double *da = m->d_dk, *db = da + m->ndof, *dc = db + m->ndof;
+    CK(cudaMemcpyAsync(m->d_u, u, sizeof(double) * m->ndof, cudaMemcpyHostToDevice, m->stream));
+    CK(cudaMemcpyAsync(da, a, sizeof(double) * m->ndof, cudaMemcpyHostToDevice, m->stream));
+    CK(cudaMemcpyAsync(db, b, sizeof(double) * m->ndof, cudaMemcpyHostToDevice, m->stream));
+    st = jfg_kg_contract_device(m, m->d_u, da, db, dc, dc + m->nq);
+    if (st) return st;
+    if (c_q4 && m->nq) CK(cudaMemcpyAsync(c_q4, dc, sizeof(double) * m->nq, cudaMemcpyDeviceToHost, m->stream));
+    if (c_t3 && m->nt) CK(cudaMemcpyAsync(c_t3, dc + m->nq, sizeof(double) * m->nt, cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    return finish_timing(m);
 }
 
 // ---------------------------------------------------------------------------

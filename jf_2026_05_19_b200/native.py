@@ -25,7 +25,7 @@ EXPORTS = ("jfg_model_create", "jfg_pattern", "jfg_pattern_fill", "jfg_assemble_
            "jfg_batch_reserve", "jfg_assemble_batch_device", "jfg_ff_set_free", "jfg_ff_extract_device",
            "jfg_ff_fetch", "jfg_ff_device_arrays", "jfg_dkdh_contract", "jfg_dkdh_load",
            "jfg_dkdh_contract_device", "jfg_dkdh_load_device", "jfg_recover_stresses",
-           "jfg_recover_stresses_device", "jfg_server_create", "jfg_server_submit", "jfg_server_wait",
+           "jfg_recover_stresses_device", "jfg_kg_contract", "jfg_kg_contract_device", "jfg_server_create", "jfg_server_submit", "jfg_server_wait",
            "jfg_server_result", "jfg_server_release", "jfg_server_stats", "jfg_server_family_batch",
            "jfg_server_hold", "jfg_server_last_error", "jfg_server_destroy", "jfg_assemble_k_quad4_noalloc", "jfg_model_destroy", "jfg_last_error",
            "jfg_version")
@@ -90,6 +90,8 @@ def load(path: str = LIB_PATH):
     L.jfg_dkdh_contract_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.jfg_dkdh_load_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.jfg_recover_stresses.argtypes = [C.c_void_p, _pd, _pd, C.c_int32, _pd, _pd]
+    L.jfg_kg_contract.argtypes = [C.c_void_p, _pd, _pd, _pd, _pd, _pd]
+    L.jfg_kg_contract_device.argtypes = [C.c_void_p] + [C.c_void_p] * 5
     L.jfg_recover_stresses_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
     L.jfg_ff_extract_device.argtypes = [C.c_void_p, C.c_void_p, _pi64, _pd, _pd]
     L.jfg_ff_fetch.argtypes = [C.c_void_p, _pi64, _pi64, _pd]
@@ -278,6 +280,20 @@ class GpuModel:
     def dkdh_load_device(self, u_ptr: int, mq_ptr: Optional[int], mt_ptr: Optional[int], out_ptr: int):
         self._check(self.L.jfg_dkdh_load_device(self.h, C.c_void_p(u_ptr), C.c_void_p(mq_ptr or None),
                                                 C.c_void_p(mt_ptr or None), C.c_void_p(out_ptr)))
+
+    def kg_contract(self, u: np.ndarray, a: np.ndarray, b: np.ndarray):
+        """Per-element a_e' KG_e(u) b_e of every CQUAD4 and CTRIA3 (jfg_kg_contract);
+        divided by the element thickness, with a = b = phi, the buckling thickness
+        sensitivity phi' dKG_e/dh phi."""
+        u, a, b = (np.ascontiguousarray(x, np.float64) for x in (u, a, b))
+        nq, nt = self.counts[1], self.counts[2]
+        cq, ct = np.zeros(nq), np.zeros(nt)
+        self._check(self.L.jfg_kg_contract(self.h, _ptr(u, _pd), _ptr(a, _pd), _ptr(b, _pd), _ptr(cq, _pd), _ptr(ct, _pd)))
+        return cq, ct
+
+    def kg_contract_device(self, u_ptr: int, a_ptr: int, b_ptr: int, cq_ptr: Optional[int], ct_ptr: Optional[int]):
+        self._check(self.L.jfg_kg_contract_device(self.h, C.c_void_p(u_ptr), C.c_void_p(a_ptr), C.c_void_p(b_ptr),
+                                                  C.c_void_p(cq_ptr or None), C.c_void_p(ct_ptr or None)))
 
     def recover_stresses(self, u: np.ndarray, bar_points: Optional[np.ndarray] = None, pressure_deck: bool = False):
         """SOL 101 output recovery (jfg_recover_stresses): shell records

@@ -1530,6 +1530,200 @@ struct OracleCSC {
     std::string err;
 };
 
+// Element triplets of KG before constraints (assembly.jl:4382-6634), element
+// order quads (576 each), trias (324 each), bars (144 each, zero-length bars
+// dropped).  Returns nonzero where the reference raises.
+int kg_element_triplets(const jfg_model_desc *d, const double *u, Triplets &t, std::string &err) {
+    int st = check_predicates(d, err);
+    if (st) return st;
+    int64_t nq = d->n_quad4, nt = d->n_tria3, nb = d->n_bar;
+    // CBAR/CBEAM with offsets: the reference's u_bar extraction indexes
+    // T12[6+dd, 9+d] for d = 4..6, which is out of bounds for the 12x12 T12
+    // and raises a BoundsError (assembly.jl:6322-6327, :6398-6403).
+    for (int64_t e = 0; e < nb; ++e) {
+        double L, T12[12][12];
+        bool off;
+        if (bar_setup(d, e, L, T12, off) && off) {
+            err = "assemble_geometric_stiffness raises BoundsError for CBAR/CBEAM with offsets (assembly.jl:6326)";
+            return JFG_ERR_REFERENCE_RAISES;
+        }
+    }
+    size_t total = (size_t)nq * 576 + (size_t)nt * 324 + (size_t)nb * 144;
+    t.I.resize(total); t.J.resize(total); t.V.resize(total);
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < nq; ++e) {
+        const int32_t *nd = d->quad4_nodes + 4 * e;
+        const double *p[4];
+        for (int k = 0; k < 4; ++k) p[k] = d->coords + 3 * nd[k];
+        double v1[3], v2[3], v3[3];
+        q4_frame(p[0], p[1], p[2], p[3], v1, v2, v3);
+        double c[3];
+        for (int i = 0; i < 3; ++i) c[i] = (p[0][i] + p[1][i] + p[2][i] + p[3][i]) / 4.0;
+        double lc[4][2];
+        for (int k = 0; k < 4; ++k) {
+            double dd[3];
+            sub3(p[k], c, dd);
+            lc[k][0] = dot3(dd, v1); lc[k][1] = dot3(dd, v2);
+        }
+        double Q[36];
+        node_blocks(d, nd, 4, v1, v2, v3, Q);
+        // u_elem = T u_global (assembly.jl:5176-5185)
+        double ue[24];
+        for (int k = 0; k < 4; ++k) {
+            const double *ug = u + 6 * (int64_t)nd[k];
+            for (int dd = 0; dd < 3; ++dd) {
+                ue[6 * k + dd] = Q[9 * k + 3 * dd] * ug[0] + Q[9 * k + 3 * dd + 1] * ug[1] + Q[9 * k + 3 * dd + 2] * ug[2];
+                ue[6 * k + 3 + dd] = Q[9 * k + 3 * dd] * ug[3] + Q[9 * k + 3 * dd + 1] * ug[4] + Q[9 * k + 3 * dd + 2] * ug[5];
+            }
+        }
+        const double *pr = d->quad4_prop + JFG_SHELL_PROP * e;
+        double h = pr[0], E = pr[1], nu = pr[2];
+        double cm = E / (1 - nu * nu);
+        double Cm[3][3] = {{cm * 1.0 * h, cm * nu * h, 0.0}, {cm * nu * h, cm * 1.0 * h, 0.0}, {0.0, 0.0, cm * ((1 - nu) / 2) * h}};
+        double Ngp[4][3], sig[4][3];
+        q4_membrane_force_field(lc, ue, Cm, Ngp);
+        for (int g = 0; g < 4; ++g)
+            for (int cc = 0; cc < 3; ++cc) sig[g][cc] = Ngp[g][cc] / h;
+        double Kl[24][24], G[576];
+        q4_geometric_stiffness(lc, sig, h, Cm, Kl);
+        transform_sym(4, Q, &Kl[0][0], G);
+        for (int k = 0; k < 4; ++k) {
+            int dd = 6 * k + 5;
+            for (int r = 0; r < 24; ++r) { G[r * 24 + dd] = 0.0; G[dd * 24 + r] = 0.0; }
+        }
+        size_t base = (size_t)e * 576;
+        int cnt = 0;
+        for (int cc = 0; cc < 24; ++cc)
+            for (int rr = 0; rr < 24; ++rr) {
+                t.I[base + cnt] = 6 * (int64_t)nd[rr / 6] + rr % 6;
+                t.J[base + cnt] = 6 * (int64_t)nd[cc / 6] + cc % 6;
+                t.V[base + cnt] = G[rr * 24 + cc];
+                ++cnt;
+            }
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < nt; ++e) {
+        const int32_t *nd = d->tria3_nodes + 3 * e;
+        const double *p1 = d->coords + 3 * nd[0], *p2 = d->coords + 3 * nd[1], *p3 = d->coords + 3 * nd[2];
+        double v1[3], v2[3], v3[3];
+        t3_frame(p1, p2, p3, v1, v2, v3);
+        double c[3];
+        for (int i = 0; i < 3; ++i) c[i] = (p1[i] + p2[i] + p3[i]) / 3.0;
+        const double *ps[3] = {p1, p2, p3};
+        double lc[3][2];
+        for (int k = 0; k < 3; ++k) {
+            double dd[3];
+            sub3(ps[k], c, dd);
+            lc[k][0] = dot3(dd, v1); lc[k][1] = dot3(dd, v2);
+        }
+        double Q[27];
+        node_blocks(d, nd, 3, v1, v2, v3, Q);
+        double ue[18];
+        for (int k = 0; k < 3; ++k) {
+            const double *ug = u + 6 * (int64_t)nd[k];
+            for (int dd = 0; dd < 3; ++dd) {
+                ue[6 * k + dd] = Q[9 * k + 3 * dd] * ug[0] + Q[9 * k + 3 * dd + 1] * ug[1] + Q[9 * k + 3 * dd + 2] * ug[2];
+                ue[6 * k + 3 + dd] = Q[9 * k + 3 * dd] * ug[3] + Q[9 * k + 3 * dd + 1] * ug[4] + Q[9 * k + 3 * dd + 2] * ug[5];
+            }
+        }
+        const double *pr = d->tria3_prop + JFG_SHELL_PROP * e;
+        double h = pr[0], E = pr[1], nu = pr[2];
+        double Kl[18][18] = {};
+        double x[3] = {lc[0][0], lc[1][0], lc[2][0]}, y[3] = {lc[0][1], lc[1][1], lc[2][1]};
+        double A = 0.5 * std::fabs(x[0] * (y[1] - y[2]) + x[1] * (y[2] - y[0]) + x[2] * (y[0] - y[1]));
+        if (A >= 1e-12 && h >= 1e-30) {
+            // stress_strain_tria3 membrane part (FEMKernels.jl:7391-7404)
+            double b[3] = {(y[1] - y[2]) / (2 * A), (y[2] - y[0]) / (2 * A), (y[0] - y[1]) / (2 * A)};
+            double cv[3] = {(x[2] - x[1]) / (2 * A), (x[0] - x[2]) / (2 * A), (x[1] - x[0]) / (2 * A)};
+            double um[6] = {ue[0], ue[1], ue[6], ue[7], ue[12], ue[13]};
+            double eps[3] = {0, 0, 0};
+            for (int i = 0; i < 3; ++i) {
+                eps[0] += b[i] * um[2 * i];
+                eps[1] += cv[i] * um[2 * i + 1];
+                eps[2] += cv[i] * um[2 * i] + b[i] * um[2 * i + 1];
+            }
+            double cm = E / (1 - nu * nu);
+            double D[3][3] = {{cm, cm * nu, 0.0}, {cm * nu, cm, 0.0}, {0.0, 0.0, cm * (1 - nu) / 2}};
+            double N[3];
+            for (int i = 0; i < 3; ++i) N[i] = (D[i][0] * eps[0] + D[i][1] * eps[1] + D[i][2] * eps[2]) * h;
+            double sxx = N[0] / h, syy = N[1] / h, sxy = N[2] / h;
+            // geometric_stiffness_tria3, non-curvature branch (FEMKernels.jl:8083-8097)
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    double val = h * A * (sxx * b[i] * b[j] + syy * cv[i] * cv[j] + sxy * (b[i] * cv[j] + cv[i] * b[j]));
+                    for (int dd = 0; dd < 3; ++dd) Kl[6 * i + dd][6 * j + dd] += val;
+                }
+        }
+        double G[324];
+        transform_sym(3, Q, &Kl[0][0], G);
+        for (int k = 0; k < 3; ++k) {
+            int dd = 6 * k + 5;
+            for (int r = 0; r < 18; ++r) { G[r * 18 + dd] = 0.0; G[dd * 18 + r] = 0.0; }
+        }
+        size_t base = (size_t)nq * 576 + (size_t)e * 324;
+        int cnt = 0;
+        for (int cc = 0; cc < 18; ++cc)
+            for (int rr = 0; rr < 18; ++rr) {
+                t.I[base + cnt] = 6 * (int64_t)nd[rr / 6] + rr % 6;
+                t.J[base + cnt] = 6 * (int64_t)nd[cc / 6] + cc % 6;
+                t.V[base + cnt] = G[rr * 18 + cc];
+                ++cnt;
+            }
+    }
+    std::vector<char> bar_ok(nb, 1);
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < nb; ++e) {
+        double L, T12[12][12];
+        bool off;
+        if (!bar_setup(d, e, L, T12, off)) { bar_ok[e] = 0; continue; }
+        const int32_t *nd = d->bar_nodes + 2 * e;
+        double ub[12] = {};
+        for (int k = 0; k < 2; ++k) {
+            const double *ug = u + 6 * (int64_t)nd[k];
+            for (int dd = 0; dd < 6; ++dd)
+                for (int q = 0; q < 6; ++q) ub[6 * k + dd] += T12[6 * k + dd][6 * k + q] * ug[q];
+        }
+        double A, Iy, Iz, I12, J, E, G, Asy, Asz;
+        bar_section(d->bar_prop + JFG_BAR_PROP * e, A, Iy, Iz, I12, J, E, G, Asy, Asz);
+        double k[12][12];
+        frame3d_stiffness(L, A, Iy, Iz, J, E, G, Asy, Asz, I12, k);
+        double P = 0.0;
+        for (int q = 0; q < 12; ++q) P += k[6][q] * ub[q];
+        double kg[12][12], tmp[144], Kb[144];
+        frame3d_geometric(L, P, kg);
+        mul(tmp, &kg[0][0], &T12[0][0], 12, 12, 12);
+        for (int i = 0; i < 12; ++i)
+            for (int j = 0; j < 12; ++j) {
+                double s = 0.0;
+                for (int l = 0; l < 12; ++l) s += T12[l][i] * tmp[l * 12 + j];
+                Kb[i * 12 + j] = s;
+            }
+        size_t base = (size_t)nq * 576 + (size_t)nt * 324 + (size_t)e * 144;
+        int cnt = 0;
+        for (int cc = 0; cc < 12; ++cc)
+            for (int rr = 0; rr < 12; ++rr) {
+                t.I[base + cnt] = 6 * (int64_t)nd[rr / 6] + rr % 6;
+                t.J[base + cnt] = 6 * (int64_t)nd[cc / 6] + cc % 6;
+                t.V[base + cnt] = Kb[rr * 12 + cc];
+                ++cnt;
+            }
+    }
+    {
+        size_t nbase = (size_t)nq * 576 + (size_t)nt * 324;
+        bool any = false;
+        for (int64_t e = 0; e < nb; ++e) any |= !bar_ok[e];
+        if (any) {
+            Triplets u2;
+            u2.I.assign(t.I.begin(), t.I.begin() + nbase); u2.J.assign(t.J.begin(), t.J.begin() + nbase); u2.V.assign(t.V.begin(), t.V.begin() + nbase);
+            for (int64_t e = 0; e < nb; ++e)
+                if (bar_ok[e])
+                    for (int q = 0; q < 144; ++q) { size_t s = nbase + e * 144 + q; u2.I.push_back(t.I[s]); u2.J.push_back(t.J[s]); u2.V.push_back(t.V[s]); }
+            t = std::move(u2);
+        }
+    }
+    return 0;
+}
+
 extern "C" {
 
 // Element-level entry points (local frame), used by tests on single elements.
@@ -1812,195 +2006,35 @@ int oracle_assemble_k(const jfg_model_desc *d, void **handle) {
 int oracle_assemble_kg(const jfg_model_desc *d, const double *u, void **handle) {
     auto *out = new OracleCSC();
     *handle = out;
-    int st = check_predicates(d, out->err);
-    if (st) return st;
-    int64_t nq = d->n_quad4, nt = d->n_tria3, nb = d->n_bar;
-    // CBAR/CBEAM with offsets: the reference's u_bar extraction indexes
-    // T12[6+dd, 9+d] for d = 4..6, which is out of bounds for the 12x12 T12
-    // and raises a BoundsError (assembly.jl:6322-6327, :6398-6403).
-    for (int64_t e = 0; e < nb; ++e) {
-        double L, T12[12][12];
-        bool off;
-        if (bar_setup(d, e, L, T12, off) && off) {
-            out->err = "assemble_geometric_stiffness raises BoundsError for CBAR/CBEAM with offsets (assembly.jl:6326)";
-            return JFG_ERR_REFERENCE_RAISES;
-        }
-    }
     Triplets t;
-    size_t total = (size_t)nq * 576 + (size_t)nt * 324 + (size_t)nb * 144;
-    t.I.resize(total); t.J.resize(total); t.V.resize(total);
-#pragma omp parallel for schedule(static)
-    for (int64_t e = 0; e < nq; ++e) {
-        const int32_t *nd = d->quad4_nodes + 4 * e;
-        const double *p[4];
-        for (int k = 0; k < 4; ++k) p[k] = d->coords + 3 * nd[k];
-        double v1[3], v2[3], v3[3];
-        q4_frame(p[0], p[1], p[2], p[3], v1, v2, v3);
-        double c[3];
-        for (int i = 0; i < 3; ++i) c[i] = (p[0][i] + p[1][i] + p[2][i] + p[3][i]) / 4.0;
-        double lc[4][2];
-        for (int k = 0; k < 4; ++k) {
-            double dd[3];
-            sub3(p[k], c, dd);
-            lc[k][0] = dot3(dd, v1); lc[k][1] = dot3(dd, v2);
-        }
-        double Q[36];
-        node_blocks(d, nd, 4, v1, v2, v3, Q);
-        // u_elem = T u_global (assembly.jl:5176-5185)
-        double ue[24];
-        for (int k = 0; k < 4; ++k) {
-            const double *ug = u + 6 * (int64_t)nd[k];
-            for (int dd = 0; dd < 3; ++dd) {
-                ue[6 * k + dd] = Q[9 * k + 3 * dd] * ug[0] + Q[9 * k + 3 * dd + 1] * ug[1] + Q[9 * k + 3 * dd + 2] * ug[2];
-                ue[6 * k + 3 + dd] = Q[9 * k + 3 * dd] * ug[3] + Q[9 * k + 3 * dd + 1] * ug[4] + Q[9 * k + 3 * dd + 2] * ug[5];
-            }
-        }
-        const double *pr = d->quad4_prop + JFG_SHELL_PROP * e;
-        double h = pr[0], E = pr[1], nu = pr[2];
-        double cm = E / (1 - nu * nu);
-        double Cm[3][3] = {{cm * 1.0 * h, cm * nu * h, 0.0}, {cm * nu * h, cm * 1.0 * h, 0.0}, {0.0, 0.0, cm * ((1 - nu) / 2) * h}};
-        double Ngp[4][3], sig[4][3];
-        q4_membrane_force_field(lc, ue, Cm, Ngp);
-        for (int g = 0; g < 4; ++g)
-            for (int cc = 0; cc < 3; ++cc) sig[g][cc] = Ngp[g][cc] / h;
-        double Kl[24][24], G[576];
-        q4_geometric_stiffness(lc, sig, h, Cm, Kl);
-        transform_sym(4, Q, &Kl[0][0], G);
-        for (int k = 0; k < 4; ++k) {
-            int dd = 6 * k + 5;
-            for (int r = 0; r < 24; ++r) { G[r * 24 + dd] = 0.0; G[dd * 24 + r] = 0.0; }
-        }
-        size_t base = (size_t)e * 576;
-        int cnt = 0;
-        for (int cc = 0; cc < 24; ++cc)
-            for (int rr = 0; rr < 24; ++rr) {
-                t.I[base + cnt] = 6 * (int64_t)nd[rr / 6] + rr % 6;
-                t.J[base + cnt] = 6 * (int64_t)nd[cc / 6] + cc % 6;
-                t.V[base + cnt] = G[rr * 24 + cc];
-                ++cnt;
-            }
-    }
-#pragma omp parallel for schedule(static)
-    for (int64_t e = 0; e < nt; ++e) {
-        const int32_t *nd = d->tria3_nodes + 3 * e;
-        const double *p1 = d->coords + 3 * nd[0], *p2 = d->coords + 3 * nd[1], *p3 = d->coords + 3 * nd[2];
-        double v1[3], v2[3], v3[3];
-        t3_frame(p1, p2, p3, v1, v2, v3);
-        double c[3];
-        for (int i = 0; i < 3; ++i) c[i] = (p1[i] + p2[i] + p3[i]) / 3.0;
-        const double *ps[3] = {p1, p2, p3};
-        double lc[3][2];
-        for (int k = 0; k < 3; ++k) {
-            double dd[3];
-            sub3(ps[k], c, dd);
-            lc[k][0] = dot3(dd, v1); lc[k][1] = dot3(dd, v2);
-        }
-        double Q[27];
-        node_blocks(d, nd, 3, v1, v2, v3, Q);
-        double ue[18];
-        for (int k = 0; k < 3; ++k) {
-            const double *ug = u + 6 * (int64_t)nd[k];
-            for (int dd = 0; dd < 3; ++dd) {
-                ue[6 * k + dd] = Q[9 * k + 3 * dd] * ug[0] + Q[9 * k + 3 * dd + 1] * ug[1] + Q[9 * k + 3 * dd + 2] * ug[2];
-                ue[6 * k + 3 + dd] = Q[9 * k + 3 * dd] * ug[3] + Q[9 * k + 3 * dd + 1] * ug[4] + Q[9 * k + 3 * dd + 2] * ug[5];
-            }
-        }
-        const double *pr = d->tria3_prop + JFG_SHELL_PROP * e;
-        double h = pr[0], E = pr[1], nu = pr[2];
-        double Kl[18][18] = {};
-        double x[3] = {lc[0][0], lc[1][0], lc[2][0]}, y[3] = {lc[0][1], lc[1][1], lc[2][1]};
-        double A = 0.5 * std::fabs(x[0] * (y[1] - y[2]) + x[1] * (y[2] - y[0]) + x[2] * (y[0] - y[1]));
-        if (A >= 1e-12 && h >= 1e-30) {
-            // stress_strain_tria3 membrane part (FEMKernels.jl:7391-7404)
-            double b[3] = {(y[1] - y[2]) / (2 * A), (y[2] - y[0]) / (2 * A), (y[0] - y[1]) / (2 * A)};
-            double cv[3] = {(x[2] - x[1]) / (2 * A), (x[0] - x[2]) / (2 * A), (x[1] - x[0]) / (2 * A)};
-            double um[6] = {ue[0], ue[1], ue[6], ue[7], ue[12], ue[13]};
-            double eps[3] = {0, 0, 0};
-            for (int i = 0; i < 3; ++i) {
-                eps[0] += b[i] * um[2 * i];
-                eps[1] += cv[i] * um[2 * i + 1];
-                eps[2] += cv[i] * um[2 * i] + b[i] * um[2 * i + 1];
-            }
-            double cm = E / (1 - nu * nu);
-            double D[3][3] = {{cm, cm * nu, 0.0}, {cm * nu, cm, 0.0}, {0.0, 0.0, cm * (1 - nu) / 2}};
-            double N[3];
-            for (int i = 0; i < 3; ++i) N[i] = (D[i][0] * eps[0] + D[i][1] * eps[1] + D[i][2] * eps[2]) * h;
-            double sxx = N[0] / h, syy = N[1] / h, sxy = N[2] / h;
-            // geometric_stiffness_tria3, non-curvature branch (FEMKernels.jl:8083-8097)
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j) {
-                    double val = h * A * (sxx * b[i] * b[j] + syy * cv[i] * cv[j] + sxy * (b[i] * cv[j] + cv[i] * b[j]));
-                    for (int dd = 0; dd < 3; ++dd) Kl[6 * i + dd][6 * j + dd] += val;
-                }
-        }
-        double G[324];
-        transform_sym(3, Q, &Kl[0][0], G);
-        for (int k = 0; k < 3; ++k) {
-            int dd = 6 * k + 5;
-            for (int r = 0; r < 18; ++r) { G[r * 18 + dd] = 0.0; G[dd * 18 + r] = 0.0; }
-        }
-        size_t base = (size_t)nq * 576 + (size_t)e * 324;
-        int cnt = 0;
-        for (int cc = 0; cc < 18; ++cc)
-            for (int rr = 0; rr < 18; ++rr) {
-                t.I[base + cnt] = 6 * (int64_t)nd[rr / 6] + rr % 6;
-                t.J[base + cnt] = 6 * (int64_t)nd[cc / 6] + cc % 6;
-                t.V[base + cnt] = G[rr * 18 + cc];
-                ++cnt;
-            }
-    }
-    std::vector<char> bar_ok(nb, 1);
-#pragma omp parallel for schedule(static)
-    for (int64_t e = 0; e < nb; ++e) {
-        double L, T12[12][12];
-        bool off;
-        if (!bar_setup(d, e, L, T12, off)) { bar_ok[e] = 0; continue; }
-        const int32_t *nd = d->bar_nodes + 2 * e;
-        double ub[12] = {};
-        for (int k = 0; k < 2; ++k) {
-            const double *ug = u + 6 * (int64_t)nd[k];
-            for (int dd = 0; dd < 6; ++dd)
-                for (int q = 0; q < 6; ++q) ub[6 * k + dd] += T12[6 * k + dd][6 * k + q] * ug[q];
-        }
-        double A, Iy, Iz, I12, J, E, G, Asy, Asz;
-        bar_section(d->bar_prop + JFG_BAR_PROP * e, A, Iy, Iz, I12, J, E, G, Asy, Asz);
-        double k[12][12];
-        frame3d_stiffness(L, A, Iy, Iz, J, E, G, Asy, Asz, I12, k);
-        double P = 0.0;
-        for (int q = 0; q < 12; ++q) P += k[6][q] * ub[q];
-        double kg[12][12], tmp[144], Kb[144];
-        frame3d_geometric(L, P, kg);
-        mul(tmp, &kg[0][0], &T12[0][0], 12, 12, 12);
-        for (int i = 0; i < 12; ++i)
-            for (int j = 0; j < 12; ++j) {
-                double s = 0.0;
-                for (int l = 0; l < 12; ++l) s += T12[l][i] * tmp[l * 12 + j];
-                Kb[i * 12 + j] = s;
-            }
-        size_t base = (size_t)nq * 576 + (size_t)nt * 324 + (size_t)e * 144;
-        int cnt = 0;
-        for (int cc = 0; cc < 12; ++cc)
-            for (int rr = 0; rr < 12; ++rr) {
-                t.I[base + cnt] = 6 * (int64_t)nd[rr / 6] + rr % 6;
-                t.J[base + cnt] = 6 * (int64_t)nd[cc / 6] + cc % 6;
-                t.V[base + cnt] = Kb[rr * 12 + cc];
-                ++cnt;
-            }
-    }
-    {
-        size_t nbase = (size_t)nq * 576 + (size_t)nt * 324;
-        bool any = false;
-        for (int64_t e = 0; e < nb; ++e) any |= !bar_ok[e];
-        if (any) {
-            Triplets u2;
-            u2.I.assign(t.I.begin(), t.I.begin() + nbase); u2.J.assign(t.J.begin(), t.J.begin() + nbase); u2.V.assign(t.V.begin(), t.V.begin() + nbase);
-            for (int64_t e = 0; e < nb; ++e)
-                if (bar_ok[e])
-                    for (int q = 0; q < 144; ++q) { size_t s = nbase + e * 144 + q; u2.I.push_back(t.I[s]); u2.J.push_back(t.J[s]); u2.V.push_back(t.V[s]); }
-            t = std::move(u2);
-        }
-    }
+    int st = kg_element_triplets(d, u, t, out->err);
+    if (st) return st;
     constrain_and_csc(d, t, out->colptr, out->rowval, out->nzval);
+    return 0;
+}
+
+// Per-element contractions a_e' KG_e(u) b_e of every CQUAD4 and CTRIA3: the
+// element matrices of the KG assembly before constraints.  With a = b = phi,
+// c_e / h_e is the thickness sensitivity phi' dKG_e/dh phi of the reference's
+// _dKg_dx_phi_thickness (adjoint_buckling.jl:2079-2150; KG is linear in h at
+// fixed u).  Returns nonzero where the KG assembly raises.
+int oracle_kg_contract(const jfg_model_desc *d, const double *u, const double *a, const double *b, double *c_q4,
+                       double *c_t3) {
+    Triplets t;
+    std::string err;
+    int st = kg_element_triplets(d, u, t, err);
+    if (st) return st;
+    for (int64_t e = 0; e < d->n_quad4; ++e) {
+        double s = 0.0;
+        for (size_t q = 576 * (size_t)e; q < 576 * (size_t)(e + 1); ++q) s += a[t.I[q]] * t.V[q] * b[t.J[q]];
+        if (c_q4) c_q4[e] = s;
+    }
+    const size_t base = 576 * (size_t)d->n_quad4;
+    for (int64_t e = 0; e < d->n_tria3; ++e) {
+        double s = 0.0;
+        for (size_t q = base + 324 * (size_t)e; q < base + 324 * (size_t)(e + 1); ++q) s += a[t.I[q]] * t.V[q] * b[t.J[q]];
+        if (c_t3) c_t3[e] = s;
+    }
     return 0;
 }
 

@@ -55,6 +55,8 @@ def lib():
         pu8 = C.POINTER(C.c_uint8)
         L.oracle_dkdh.argtypes = [C.POINTER(JfgModelDesc), pd, pd, pd, pd, pd, pu8, pu8, pd]
         L.oracle_recover.argtypes = [C.POINTER(JfgModelDesc), pd, pd, C.c_int32, pd, pd]
+        L.oracle_kg_contract.argtypes = [C.POINTER(JfgModelDesc), pd, pd, pd, pd, pd]
+        L.oracle_kg_contract.restype = C.c_int
         _lib = L
     return _lib
 
@@ -204,6 +206,21 @@ def recover(m: ModelArrays, u, bar_points=None, flags: int = 0):
                      shell.ctypes.data_as(pd), bar.ctypes.data_as(pd))
     del keep
     return shell, bar
+
+
+def kg_contract(m: ModelArrays, u, a, b):
+    """Per-element a_e' KG_e(u) b_e of every CQUAD4 and CTRIA3 (see oracle_kg_contract)."""
+    L = lib()
+    desc, keep = make_desc(m)
+    pd = C.POINTER(C.c_double)
+    u, a, b = (np.ascontiguousarray(x, np.float64) for x in (u, a, b))
+    cq, ct = np.zeros(m.q4_nodes.shape[0]), np.zeros(m.t3_nodes.shape[0])
+    st = L.oracle_kg_contract(C.byref(desc), u.ctypes.data_as(pd), a.ctypes.data_as(pd), b.ctypes.data_as(pd),
+                              cq.ctypes.data_as(pd), ct.ctypes.data_as(pd))
+    del keep
+    if st:
+        raise RuntimeError(f"oracle_kg_contract status {st}")
+    return cq, ct
 
 
 def to_scipy(colptr, rowval, nzval, ndof):

@@ -109,3 +109,19 @@ def test_sensitivities_follow_thickness_updates(cuda_device):
         g.update_thickness(hq, ht)
         cq, ct = g.dkdh_contract(u, u)
     assert _close(cq, oq, Q4_TOL) and _close(ct, ot, T3_TOL)
+
+
+@pytest.mark.parametrize("name", sorted(DECKS))
+def test_kg_contractions_match_oracle(name, cuda_device):
+    """Per-element phi' KG_e phi (jfg_kg_contract) against the oracle's element
+    KG triplets; the call does not count as a KG assembly in the timing."""
+    m = DECKS[name]
+    u = decks.smooth_displacement(m, seed=31)
+    phi = decks.smooth_displacement(m, seed=32)
+    oq, ot = O.kg_contract(m, u, phi, phi)
+    with native.GpuModel(m) as g:
+        cq, ct = g.kg_contract(u, phi, phi)
+        _, n_kg = g.timing_accumulated("kg")
+    assert n_kg == 0
+    assert _close(cq, oq, 1e-10), np.abs(cq - oq).max()
+    assert _close(ct, ot, 1e-10), np.abs(ct - ot).max()

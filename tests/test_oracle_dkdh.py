@@ -101,3 +101,26 @@ def test_membrane_field_sensitivity_does_not_depend_on_thickness():
     m2.q4_prop[:, 0] *= 2.0
     c2, _, _ = O.dkdh(m2, a=u, b=u)
     assert np.allclose(c2, c1, rtol=1e-10)
+
+
+def test_kg_contractions_sum_to_assembled_quadratic_form():
+    """sum_e phi' KG_e phi equals phi' KG phi of the assembled KG on a shell deck
+    without RBE2 (no constraint redistribution, no bars); KG_e is linear in the thickness at fixed u,
+    so c_e / h_e is phi' dKG_e/dh phi."""
+    import dataclasses
+    from decks_extra import skewed_plane
+    m = skewed_plane(seed=4)
+    m = dataclasses.replace(m, rbe2_master=m.rbe2_master[:0], rbe2_cm=m.rbe2_cm[:0],
+                            rbe2_slave_ptr=m.rbe2_slave_ptr[:1], rbe2_slaves=m.rbe2_slaves[:0],
+                            bar_nodes=m.bar_nodes[:0], bar_prop=m.bar_prop[:0], bar_pin=m.bar_pin[:0])
+    u = decks.smooth_displacement(m, seed=5)
+    phi = decks.smooth_displacement(m, seed=6)
+    cq, ct = O.kg_contract(m, u, phi, phi)
+    colptr, rowval, nz = O.assemble_kg(m, u)
+    K = O.to_scipy(colptr, rowval, nz, m.ndof)
+    total = phi @ (K @ phi)
+    assert abs(cq.sum() + ct.sum() - total) <= 1e-10 * (np.abs(cq).sum() + np.abs(ct).sum())
+    m2 = m.with_thickness(2.0 * m.q4_prop[:, 0], 2.0 * m.t3_prop[:, 0])
+    cq2, ct2 = O.kg_contract(m2, u, phi, phi)
+    assert np.allclose(cq2, 2.0 * cq, rtol=1e-11, atol=1e-14 * np.abs(cq).max())
+    assert np.allclose(ct2, 2.0 * ct, rtol=1e-11, atol=1e-14 * np.abs(ct).max())
