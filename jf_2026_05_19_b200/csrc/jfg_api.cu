@@ -482,46 +482,61 @@ __device__ __forceinline__ void block_row_sum(const double *__restrict__ staging
     }
 }
 
-// KG rows (12 values per slot plus 27 per bar pair, see blk_entry) of two
-// blocks at once: shell contributions hold only their translation 3x3, bar
-// contributions [rb, b) also their three rotation sub-blocks.  Row i < 3
-// sums columns 0-2 over every slot and columns 3-5 over the bar slots; row
-// i >= 3 sums the bar slots only.  The translation rows of both blocks are
-// read in interleaved batches of four slots (loads issued together, slots
-// past a block's end add +0.0); each block's terms are added in slot order.
-__device__ __forceinline__ void block_rows_sum_kg(const double *__restrict__ staging, const double *__restrict__ kg_rot,
-                                                  const int32_t *__restrict__ slot_bar, const int32_t a[2], const int32_t rb[2],
-                                                  const int32_t b[2], int i, double s[2][6]) {
-    const int i3 = i < 3 ? i : i - 3;
-    if (i < 3) {
+// KG sums of two blocks (12 values per slot plus 27 per bar pair, see
+// blk_entry) into their 6x6 tiles t0, t1 in shared memory.  Lane i < 5 of a
+// block reads the i-th 16-byte chunk (values 2i, 2i+1) of every slot, so a
+// slot's translation 3x3 is five 16-byte loads spread over the block's lanes;
+// the two blocks' slots are read in interleaved batches of four (loads issued
+// together, slots past a block's end add +0.0), each value summed in slot
+// order.  Bar contributions [rb, b) also carry three rotation sub-blocks:
+// row i < 3 adds them to columns 3-5, row i >= 3 to all six columns.  Shell-only
+// blocks leave zeros there.
+__device__ __forceinline__ void block_kg_sums(const double *__restrict__ staging, const double *__restrict__ kg_rot,
+                                              const int32_t *__restrict__ slot_bar, const int32_t a[2], const int32_t rb[2],
+                                              const int32_t b[2], int i, double *t0, double *t1) {
+    double ch[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    if (i < 5) {
         const int32_t len = max(b[0] - a[0], b[1] - a[1]);
         for (int32_t t = 0; t < len; t += 4) {
-            double x[2][4][3];
+            double2 x[2][4];
 #pragma unroll
             for (int m = 0; m < 2; ++m)
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int32_t q = a[m] + t + u;
-                    x[m][u][0] = x[m][u][1] = x[m][u][2] = 0.0;
-                    if (q < b[m]) {
-                        const double *p = staging + 12 * (int64_t)q + 3 * i3;
-                        x[m][u][0] = __ldg(p); x[m][u][1] = __ldg(p + 1); x[m][u][2] = __ldg(p + 2);
-                    }
+                    x[m][u] = q < b[m] ? __ldg(reinterpret_cast<const double2 *>(staging + 12 * (int64_t)q) + i)
+                                       : make_double2(0.0, 0.0);
                 }
 #pragma unroll
             for (int m = 0; m < 2; ++m)
 #pragma unroll
-                for (int u = 0; u < 4; ++u) { s[m][0] += x[m][u][0]; s[m][1] += x[m][u][1]; s[m][2] += x[m][u][2]; }
+                for (int u = 0; u < 4; ++u) { ch[m][0] += x[m][u].x; ch[m][1] += x[m][u].y; }
         }
     }
+    const int i3 = i < 3 ? i : i - 3;
 #pragma unroll
-    for (int m = 0; m < 2; ++m)
+    for (int m = 0; m < 2; ++m) {
+        double s[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         for (int32_t q = rb[m]; q < b[m]; ++q) {
             const double *p = kg_rot + 27 * (int64_t)__ldg(slot_bar + q) + 3 * i3;
-            if (i >= 3) { s[m][0] += __ldg(p + 9); s[m][1] += __ldg(p + 10); s[m][2] += __ldg(p + 11); }
+            if (i >= 3) { s[0] += __ldg(p + 9); s[1] += __ldg(p + 10); s[2] += __ldg(p + 11); }
             const int o3 = i < 3 ? 0 : 18;  // translation-rotation / rotation-rotation rows
-            s[m][3] += __ldg(p + o3); s[m][4] += __ldg(p + o3 + 1); s[m][5] += __ldg(p + o3 + 2);
+            s[3] += __ldg(p + o3); s[4] += __ldg(p + o3 + 1); s[5] += __ldg(p + o3 + 2);
         }
+        double *tt = m == 0 ? t0 : t1;
+        // translation values 2i, 2i+1 (value v sits at row v / 3, column v % 3; 9-11 are padding)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int v = 2 * i + e;
+            if (v < 9) tt[6 * (v / 3) + v % 3] = ch[m][e];
+        }
+        if (i < 3) {
+            tt[6 * i + 3] = s[3]; tt[6 * i + 4] = s[4]; tt[6 * i + 5] = s[5];
+        } else {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) tt[6 * i + c] = s[c];
+        }
+    }
 }
 
 __device__ __forceinline__ void block_write(int64_t k, int i, const double sr[6], const double sc[6],
@@ -567,19 +582,20 @@ __global__ void __launch_bounds__(32 * kRedWarps, 8) block_reduce_kernel(int64_t
         const int32_t a1 = two ? __ldg(seg + k1) : 0, b1 = two ? __ldg(seg + k1 + 1) : 0;
         if (KG) {
             const int32_t aa[2] = {a0, a1}, bb[2] = {b0, b1}, rr[2] = {__ldg(rot + k0), two ? __ldg(rot + k1) : 0};
-            double ss[2][6] = {{0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}};
-            block_rows_sum_kg(staging, staging + kg_rot_off, slot_bar, aa, rr, bb, i, ss);
-#pragma unroll
-            for (int c = 0; c < 6; ++c) { s0[c] = ss[0][c]; s1[c] = ss[1][c]; }
+            block_kg_sums(staging, staging + kg_rot_off, slot_bar, aa, rr, bb, i, tr[warp][0][g], tr[warp][1][g]);
         } else {
             block_row_sum(staging, a0, b0, i, s0);
             block_row_sum(staging, a1, b1, i, s1);
-        }
 #pragma unroll
-        for (int c = 0; c < 6; ++c) { tr[warp][0][g][6 * i + c] = s0[c]; tr[warp][1][g][6 * i + c] = s1[c]; }
+            for (int c = 0; c < 6; ++c) { tr[warp][0][g][6 * i + c] = s0[c]; tr[warp][1][g][6 * i + c] = s1[c]; }
+        }
     }
     __syncwarp();
     if (one) {
+        if (KG) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) { s0[c] = tr[warp][0][g][6 * i + c]; s1[c] = tr[warp][1][g][6 * i + c]; }
+        }
         double c0[6], c1[6];
 #pragma unroll
         for (int r = 0; r < 6; ++r) { c0[r] = tr[warp][0][g][6 * r + i]; c1[r] = tr[warp][1][g][6 * r + i]; }

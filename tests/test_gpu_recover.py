@@ -152,3 +152,33 @@ def test_reference_style_results(cuda_device):
     jb = int(np.nonzero(m2.bar_eid == b["eid"])[0][0])
     assert abs(b["axial"] - bo[jb, 8]) <= TOL * np.abs(bo[:, 8]).max()
     assert stresses[b["eid"]] == abs(b["axial"])
+
+
+def test_edge_cases(cuda_device):
+    """A zero-length bar (skipped, status 0), a deck with shells only and one
+    with bars only: records and status columns as the oracle's."""
+    from decks_extra import skewed_plane
+    m = DECKS["barrel_small"]
+    z = DECKS["skewed_cd_frames"]  # carries one zero-length bar
+    u = decks.smooth_displacement(z, seed=41)
+    so, bo = O.recover(z, u)
+    with native.GpuModel(z) as g:
+        sg, bg = g.recover_stresses(u)
+    assert (bo[:, 17] == 0).sum() == 1 and np.array_equal(bg[:, 17], bo[:, 17])
+    _assert_records(sg, so, bg, bo)
+    shells = dataclasses.replace(skewed_plane(seed=5), bar_nodes=np.zeros((0, 2), np.int32),
+                                 bar_prop=np.zeros((0, 18)), bar_pin=np.zeros((0, 2), np.int32))
+    u = decks.smooth_displacement(shells, seed=42)
+    so, bo = O.recover(shells, u)
+    with native.GpuModel(shells) as g:
+        sg, bg = g.recover_stresses(u)
+    assert bg.shape == (0, 18)
+    _assert_records(sg, so)
+    bars = dataclasses.replace(m, q4_nodes=np.zeros((0, 4), np.int32), q4_prop=np.zeros((0, 7)),
+                               t3_nodes=np.zeros((0, 3), np.int32), t3_prop=np.zeros((0, 7)))
+    u = decks.smooth_displacement(bars, seed=43)
+    so, bo = O.recover(bars, u, bar_points=_bar_points(bars))
+    with native.GpuModel(bars) as g:
+        sg, bg = g.recover_stresses(u, _bar_points(bars))
+    assert sg.shape == (0, 48)
+    _assert_records(sg, so, bg, bo)
