@@ -617,6 +617,9 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
     __syncwarp();
     const bool t = valid && sl >= 0 && (sl & kBlkTranspose);
     double *buf = reinterpret_cast<double *>(&S) + 18 * tl;
+    const int64_t e_warp = (int64_t)blockIdx.x * Q4_ELEMS_PER_BLOCK + warp * Q4_TEAMS_PER_WARP;
+    const int64_t n_left = nq - e_warp;
+    const int nv = n_left <= 0 ? 0 : (n_left >= Q4_TEAMS_PER_WARP ? Q4_TEAMS_PER_WARP : (int)n_left);
 #pragma unroll
     for (int half = 0; half < 2; ++half) {
         if (valid) {
@@ -658,14 +661,19 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
             }
         }
         __syncwarp();
-        for (int ch = lane; ch < Q4_TEAMS_PER_WARP * 10 * 9; ch += 32) {
-            const int tm = ch / 90, rem = ch - 90 * tm, pl = rem / 9, part = rem - 9 * pl;
-            const int sid = warp * Q4_TEAMS_PER_WARP + tm;
-            if ((int64_t)blockIdx.x * Q4_ELEMS_PER_BLOCK + sid >= nq) continue;
-            const int32_t st = sh[sid].slot[pl];
-            if (st < 0) continue;
-            const double2 v2 = reinterpret_cast<const double2 *>(reinterpret_cast<const double *>(&sh[sid]) + 18 * pl)[part];
-            reinterpret_cast<double2 *>(o.staging + 36 * (int64_t)(st & kBlkIndexMask) + 18 * half)[part] = v2;
+        // chunk ch = 90 team + 9 pair + part; lanes step by 32 = 3 pairs + 5 parts.
+        // The warp's valid teams are a prefix (elements are consecutive).
+        for (int tm = 0, pl = lane / 9, part = lane % 9; tm < nv;) {
+            const Q4KShared &R = sh[warp * Q4_TEAMS_PER_WARP + tm];
+            const int32_t st = R.slot[pl];
+            if (st >= 0) {
+                const double2 v2 = reinterpret_cast<const double2 *>(reinterpret_cast<const double *>(&R) + 18 * pl)[part];
+                reinterpret_cast<double2 *>(o.staging + 36 * (int64_t)(st & kBlkIndexMask) + 18 * half)[part] = v2;
+            }
+            part += 5;
+            pl += 3;
+            if (part >= 9) { part -= 9; ++pl; }
+            if (pl >= 10) { pl -= 10; ++tm; }
         }
         __syncwarp();
     }
@@ -933,14 +941,21 @@ __global__ void __launch_bounds__(Q4_THREADS) q4_kg_kernel(int64_t nq, const int
         S.slot[tl] = sl;
     }
     __syncwarp();
-    for (int ch = lane; ch < Q4_TEAMS_PER_WARP * 10 * 6; ch += 32) {
-        const int tm = ch / 60, rem = ch - 60 * tm, pl = rem / 6, part = rem - 6 * pl;
-        const int sid = warp * Q4_TEAMS_PER_WARP + tm;
-        if ((int64_t)blockIdx.x * Q4_ELEMS_PER_BLOCK + sid >= nq) continue;
-        const int32_t st = sh[sid].slot[pl];
-        if (st < 0) continue;
-        const double2 v2 = reinterpret_cast<const double2 *>(reinterpret_cast<const double *>(&sh[sid]) + 12 * pl)[part];
-        reinterpret_cast<double2 *>(o.staging + 12 * (int64_t)(st & kBlkIndexMask))[part] = v2;
+    // chunk ch = 60 team + 6 pair + part; lanes step by 32 = 5 pairs + 2 parts
+    const int64_t e_warp = (int64_t)blockIdx.x * Q4_ELEMS_PER_BLOCK + warp * Q4_TEAMS_PER_WARP;
+    const int64_t n_left = nq - e_warp;
+    const int nv = n_left <= 0 ? 0 : (n_left >= Q4_TEAMS_PER_WARP ? Q4_TEAMS_PER_WARP : (int)n_left);
+    for (int tm = 0, pl = lane / 6, part = lane % 6; tm < nv;) {
+        const Q4GShared &R = sh[warp * Q4_TEAMS_PER_WARP + tm];
+        const int32_t st = R.slot[pl];
+        if (st >= 0) {
+            const double2 v2 = reinterpret_cast<const double2 *>(reinterpret_cast<const double *>(&R) + 12 * pl)[part];
+            reinterpret_cast<double2 *>(o.staging + 12 * (int64_t)(st & kBlkIndexMask))[part] = v2;
+        }
+        part += 2;
+        pl += 5;
+        if (part >= 6) { part -= 6; ++pl; }
+        if (pl >= 10) { pl -= 10; ++tm; }
     }
 }
 

@@ -352,12 +352,15 @@ __global__ void __launch_bounds__(T3_THREADS, 5) t3_k_kernel(int64_t nt, const i
     }
     __syncwarp(tm);
     // the team copies the staged slots as 16-byte stores, 18 per slot
-    for (int ch = tl; ch < 6 * 18; ch += T3_TEAM) {
-        const int pair = ch / 18, part = ch - 18 * pair;
+    // (chunk 18 pair + part; lanes step by 16 parts)
+    for (int pair = 0, part = tl; pair < 6;) {
         const int32_t st = S.slot[pair];
-        if (st < 0) continue;
-        const double2 v2 = reinterpret_cast<const double2 *>(&S.Pb[0][0][0] + 36 * pair)[part];
-        reinterpret_cast<double2 *>(o.staging + 36 * (int64_t)(st & kBlkIndexMask))[part] = v2;
+        if (st >= 0) {
+            const double2 v2 = reinterpret_cast<const double2 *>(&S.Pb[0][0][0] + 36 * pair)[part];
+            reinterpret_cast<double2 *>(o.staging + 36 * (int64_t)(st & kBlkIndexMask))[part] = v2;
+        }
+        part += T3_TEAM;
+        if (part >= 18) { part -= 18; ++pair; }
     }
     if (o.maxabs) {
         for (int off = 8; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_xor_sync(tm, lmax, off, 16));
