@@ -73,6 +73,11 @@ struct jfg_model {
     int32_t *d_blk_A = nullptr, *d_blk_B = nullptr, *d_blk_offAB = nullptr, *d_blk_offBA = nullptr;
     int32_t *d_blk_rot = nullptr;       // first bar slot of each block's segment (segment end if none)
     int32_t *d_slot_bar = nullptr;      // per slot: bar pair index (element pair - pair_bar), negative for shells
+    // per block: CSC position of its first entry in row 6A and in row 6B (-1 for A == B) and the
+    // row lengths of A and of B; used when every node's six rows are evenly spaced (blk_even)
+    int64_t *d_blk_pa = nullptr, *d_blk_pb = nullptr;
+    int2 *d_blk_len = nullptr;
+    bool blk_even = false;
     int64_t staging_len = 0;            // staging doubles per assembly: max(K 36 per slot, KG 12 per slot + 27 per bar pair)
     double *d_staging = nullptr;        // 36 doubles per regular element pair
     int64_t *d_rowptr = nullptr, *d_colind = nullptr;   // 0-based symmetric CSR == CSC
@@ -407,6 +412,25 @@ __global__ void blk_offsets_kernel(int64_t n_blk, const int32_t *__restrict__ A,
     offBA[k] = (int32_t)(pb - rowptr[6 * b]);
 }
 
+// CSC positions of each block's entries: row 6A + r starts r * L_A after row
+// 6A when the six rows of A have one length, so (6A + r, 6B + i) sits at
+// pa + r * L_A + i.  Flags a block whose nodes' rows are not evenly spaced.
+__global__ void blk_pos_kernel(int64_t n_blk, const int32_t *__restrict__ A, const int32_t *__restrict__ B,
+                               const int32_t *__restrict__ offAB, const int32_t *__restrict__ offBA,
+                               const int64_t *__restrict__ rowptr, int64_t *pa, int64_t *pb, int2 *len, int32_t *uneven) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n_blk) return;
+    const int64_t a = A[k], b = B[k];
+    const int64_t ra = rowptr[6 * a], rb = rowptr[6 * b];
+    const int64_t la = rowptr[6 * a + 1] - ra, lb = rowptr[6 * b + 1] - rb;
+    bool even = true;
+    for (int r = 2; r <= 6; ++r) even = even && rowptr[6 * a + r] - ra == r * la && rowptr[6 * b + r] - rb == r * lb;
+    if (!even) atomicExch(uneven, 1);
+    pa[k] = ra + offAB[k];
+    pb[k] = a == b ? -1 : rb + offBA[k];
+    len[k] = make_int2((int)la, (int)lb);
+}
+
 // Element pair -> sorted block slot, with the transpose bit when the pair's
 // local orientation (a <= b) maps to global node order A > B.
 __global__ void blk_slot_kernel(int64_t nbc, const int32_t *__restrict__ vals, int64_t pair_t3, int64_t pair_bar,
@@ -554,20 +578,39 @@ __device__ __forceinline__ void block_write(int64_t k, int i, const double sr[6]
     }
 }
 
+// The same writes from the block's precomputed CSC positions (blk_pos_kernel):
+// one load of the positions instead of the nodes, offsets and six row starts
+// per node, which takes a dependent memory round trip off each thread.
+__device__ __forceinline__ void block_write_pos(int64_t k, int i, const double sr[6], const double sc[6],
+                                                const int64_t *__restrict__ pa, const int64_t *__restrict__ pb,
+                                                const int2 *__restrict__ len, double *nz) {
+    const int64_t a0 = __ldg(pa + k) + i, b0 = __ldg(pb + k);
+    const int2 l = __ldg(len + k);
+#pragma unroll
+    for (int r = 0; r < 6; ++r) nz[a0 + (int64_t)r * l.x] = sc[r];
+    if (b0 >= 0) {
+        const int64_t bb = b0 + i;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) nz[bb + (int64_t)j * l.y] = sr[j];
+    }
+}
+
 // Thread layout: warp w takes blocks 5w .. 5w+4 (lanes 6g .. 6g+5 for block
 // 5w+g, lanes 30-31 idle) and the same five blocks + half.  Each thread sums
 // row i of its blocks; the rows meet in shared memory so that every thread
 // also holds column i for the coalesced write above.
 constexpr int kRedWarps = 4;
 
-template <bool KG>
+template <bool KG, bool POS>
 __global__ void __launch_bounds__(32 * kRedWarps, 8) block_reduce_kernel(int64_t n_blk, const int32_t *__restrict__ seg,
                                                            const int32_t *__restrict__ rot,
                                                            const int32_t *__restrict__ slot_bar, int64_t kg_rot_off,
                                                            const double *__restrict__ staging, const int32_t *__restrict__ A,
                                                            const int32_t *__restrict__ B, const int32_t *__restrict__ offAB,
                                                            const int32_t *__restrict__ offBA, const int64_t *__restrict__ rowptr,
-                                                           double *nz, int64_t staging_stride, int64_t nnz) {
+                                                           const int64_t *__restrict__ pa, const int64_t *__restrict__ pb,
+                                                           const int2 *__restrict__ len, double *nz, int64_t staging_stride,
+                                                           int64_t nnz) {
     __shared__ double tr[kRedWarps][2][5][36];
     const int64_t half = (n_blk + 1) / 2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -599,8 +642,13 @@ __global__ void __launch_bounds__(32 * kRedWarps, 8) block_reduce_kernel(int64_t
         double c0[6], c1[6];
 #pragma unroll
         for (int r = 0; r < 6; ++r) { c0[r] = tr[warp][0][g][6 * r + i]; c1[r] = tr[warp][1][g][6 * r + i]; }
-        block_write(k0, i, s0, c0, A, B, offAB, offBA, rowptr, nz);
-        if (two) block_write(k1, i, s1, c1, A, B, offAB, offBA, rowptr, nz);
+        if (POS) {
+            block_write_pos(k0, i, s0, c0, pa, pb, len, nz);
+            if (two) block_write_pos(k1, i, s1, c1, pa, pb, len, nz);
+        } else {
+            block_write(k0, i, s0, c0, A, B, offAB, offBA, rowptr, nz);
+            if (two) block_write(k1, i, s1, c1, A, B, offAB, offBA, rowptr, nz);
+        }
     }
 }
 
@@ -1090,6 +1138,21 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
         blk_offsets_kernel<<<(unsigned)cdiv(m->n_blk, 256), 256, 0, m->stream>>>(m->n_blk, m->d_blk_A, m->d_blk_B, m->d_rowptr,
                                                                                  m->d_colind, m->d_blk_offAB, m->d_blk_offBA, d_err);
         CK(cudaGetLastError());
+        CK(dalloc(m, &m->d_blk_pa, m->n_blk));
+        CK(dalloc(m, &m->d_blk_pb, m->n_blk));
+        CK(dalloc(m, &m->d_blk_len, m->n_blk));
+        int32_t *d_uneven = nullptr;
+        CK(cudaMallocAsync(&d_uneven, sizeof(int32_t), m->stream));
+        CK(cudaMemsetAsync(d_uneven, 0, sizeof(int32_t), m->stream));
+        blk_pos_kernel<<<(unsigned)cdiv(m->n_blk, 256), 256, 0, m->stream>>>(m->n_blk, m->d_blk_A, m->d_blk_B, m->d_blk_offAB,
+                                                                             m->d_blk_offBA, m->d_rowptr, m->d_blk_pa, m->d_blk_pb,
+                                                                             m->d_blk_len, d_uneven);
+        CK(cudaGetLastError());
+        int32_t uneven = 1;
+        CK(cudaMemcpyAsync(&uneven, d_uneven, sizeof(int32_t), cudaMemcpyDeviceToHost, m->stream));
+        CK(cudaStreamSynchronize(m->stream));
+        cudaFreeAsync(d_uneven, m->stream);
+        m->blk_even = uneven == 0;
         blk_slot_kernel<<<(unsigned)cdiv(nbc, 256), 256, 0, m->stream>>>(nbc, d_bv2, m->pair_t3, m->pair_bar, m->d_q4n, m->d_t3n,
                                                                          m->d_barn, m->d_blk_slot);
         CK(cudaGetLastError());
@@ -1400,14 +1463,16 @@ jfg_status launch_reduce(jfg_model *m, const Batch &bt, bool kg) {
     CK(mark(m, 4));
     if (m->n_blk) {
         const dim3 grid((unsigned)cdiv(cdiv((m->n_blk + 1) / 2, 5), kRedWarps), nv);
-        if (kg)
-            block_reduce_kernel<true><<<grid, 32 * kRedWarps, 0, m->stream>>>(
-                m->n_blk, m->d_blk_seg, m->d_blk_rot, m->d_slot_bar, 12 * m->n_blk_contrib, bt.staging, m->d_blk_A, m->d_blk_B,
-                m->d_blk_offAB, m->d_blk_offBA, m->d_rowptr, bt.nz, bt.staging_stride, m->nnz);
-        else
-            block_reduce_kernel<false><<<grid, 32 * kRedWarps, 0, m->stream>>>(
-                m->n_blk, m->d_blk_seg, m->d_blk_rot, m->d_slot_bar, 0, bt.staging, m->d_blk_A, m->d_blk_B,
-                m->d_blk_offAB, m->d_blk_offBA, m->d_rowptr, bt.nz, bt.staging_stride, m->nnz);
+        auto launch = [&](auto kernel, int64_t rot_off) {
+            kernel<<<grid, 32 * kRedWarps, 0, m->stream>>>(m->n_blk, m->d_blk_seg, m->d_blk_rot, m->d_slot_bar, rot_off, bt.staging,
+                                                        m->d_blk_A, m->d_blk_B, m->d_blk_offAB, m->d_blk_offBA, m->d_rowptr,
+                                                        m->d_blk_pa, m->d_blk_pb, m->d_blk_len, bt.nz, bt.staging_stride, m->nnz);
+        };
+        const int64_t rot_off = 12 * m->n_blk_contrib;
+        if (kg && m->blk_even) launch(block_reduce_kernel<true, true>, rot_off);
+        else if (kg) launch(block_reduce_kernel<true, false>, rot_off);
+        else if (m->blk_even) launch(block_reduce_kernel<false, true>, 0);
+        else launch(block_reduce_kernel<false, false>, 0);
     }
     CK(cudaGetLastError());
     CK(mark(m, 5));
