@@ -164,34 +164,37 @@ def test_unsupported_and_invalid_inputs(cuda_device):
 
 
 def test_plate_load_factors_match(cuda_device):
-    """SOL 105 consumer fed oracle vs GPU matrices: first 5 load factors within 1e-9."""
+    """SOL 105 consumer fed oracle vs GPU matrices: first 10 load factors within 1e-9."""
     m = decks.plate_c1()
     ocp, orv, onz, _, _ = O.assemble_k(m)
     Ko = to_csc(ocp, orv, onz, m.ndof)
     u, free = static_solution(m, Ko, O.constraint_map(m))
     _, _, ognz = O.assemble_kg(m, u)
-    lam_o = load_factors(Ko, to_csc(ocp, orv, ognz, m.ndof), free)
+    lam_o = load_factors(Ko, to_csc(ocp, orv, ognz, m.ndof), free, k=10)
     with native.GpuModel(m) as g:
         cp, rv = g.pattern()
         Kg_ = to_csc(cp, rv, g.assemble_k()[0], m.ndof)
-        lam_g = load_factors(Kg_, to_csc(cp, rv, g.assemble_kg(u), m.ndof), free)
+        lam_g = load_factors(Kg_, to_csc(cp, rv, g.assemble_kg(u), m.ndof), free, k=10)
+    assert lam_o.size == 10 and lam_g.size == 10
     assert np.all(np.abs(lam_g - lam_o) <= LAMBDA_TOL * np.abs(lam_o))
     D = 70000 * 8 / (12 * (1 - 0.33 ** 2))
     assert abs(lam_g[0] / (4 * np.pi ** 2 * D / 400.0 ** 2) - 1) < 0.01
 
 
 def test_barrel_load_factors_match(cuda_device):
+    """The barrel with bars and the RBE2 end ring: first 10 load factors within 1e-9."""
     m = decks.barrel_small(seed=1, n_circ=48, n_axial=12)
     ocp, orv, onz, _, _ = O.assemble_k(m)
     Ko = to_csc(ocp, orv, onz, m.ndof)
     cmap = O.constraint_map(m)
     u, free = static_solution(m, Ko, cmap)
     _, _, ognz = O.assemble_kg(m, u)
-    lam_o = load_factors(Ko, to_csc(ocp, orv, ognz, m.ndof), free, k=6, sigma=0.0)
+    lam_o = load_factors(Ko, to_csc(ocp, orv, ognz, m.ndof), free, k=10, sigma=0.0)
     with native.GpuModel(m) as g:
         cp, rv = g.pattern()
         Kg_ = to_csc(cp, rv, g.assemble_k()[0], m.ndof)
-        lam_g = load_factors(Kg_, to_csc(cp, rv, g.assemble_kg(u), m.ndof), free, k=6, sigma=0.0)
+        lam_g = load_factors(Kg_, to_csc(cp, rv, g.assemble_kg(u), m.ndof), free, k=10, sigma=0.0)
+    assert lam_o.size == 10 and lam_g.size == 10
     assert np.all(np.abs(lam_g - lam_o) <= LAMBDA_TOL * np.abs(lam_o))
 
 
