@@ -11,7 +11,7 @@ import numpy as np
 import scipy.sparse as sp
 import scipy.sparse.linalg as sla
 
-ROW_TOL = 1e-12      # |K_gpu - K_oracle| per nonzero / max |K| of its row
+ROW_TOL = 1e-12      # |K_gpu - K_oracle| per nonzero / max |K| of its row (the parity bound)
 LAMBDA_TOL = 1e-9    # relative, first buckling load factors
 
 
