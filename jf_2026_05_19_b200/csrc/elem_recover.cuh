@@ -184,15 +184,12 @@ __device__ __forceinline__ bool q4_is_rectangle(const double lc[4][2]) {
     return !(fabs(L[0] - L[2]) > tol * Lmax || fabs(L[1] - L[3]) > tol * Lmax);
 }
 
-// CQUAD4 branch of recover_shell_stresses! (stress_recovery.jl:179-302).
-__global__ void __launch_bounds__(128) q4_recover_kernel(int64_t nq, const int32_t *__restrict__ nodes,
-                                                         const double *__restrict__ prop,
-                                                         const double *__restrict__ coords,
-                                                         const double *__restrict__ nodeR, const double *__restrict__ u,
-                                                         bool pressure_deck, double *__restrict__ out) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nq) return;
-    double *o = out + REC_SHELL * e;
+// CQUAD4 branch of recover_shell_stresses! (stress_recovery.jl:179-302):
+// element e's record into o.
+__device__ __forceinline__ void q4_recover_element(int64_t e, const int32_t *__restrict__ nodes,
+                                                   const double *__restrict__ prop, const double *__restrict__ coords,
+                                                   const double *__restrict__ nodeR, const double *__restrict__ u,
+                                                   bool pressure_deck, double *o) {
     const double *pr = prop + 7 * e;
     const double h = __ldg(pr), E = __ldg(pr + 1), nu = __ldg(pr + 2), br = __ldg(pr + 4);
     int32_t nd[4];
@@ -352,6 +349,36 @@ __global__ void __launch_bounds__(128) q4_recover_kernel(int64_t nq, const int32
         Mc[i][2] = M[2];
 #pragma unroll
         for (int k = 0; k < 3; ++k) { o[22 + 3 * i + k] = Nc[i][k]; o[34 + 3 * i + k] = Mc[i][k]; }
+    }
+}
+
+// One thread per CQUAD4.  Records are built in shared memory (a row of 50
+// doubles per thread, 16-byte aligned) and the block writes its contiguous
+// records out as 16-byte stores; 8-byte stores when out is not 16-byte aligned.
+constexpr int Q4R_THREADS = 64, Q4R_ROW = 50;
+__global__ void __launch_bounds__(Q4R_THREADS) q4_recover_kernel(int64_t nq, const int32_t *__restrict__ nodes,
+                                                                 const double *__restrict__ prop,
+                                                                 const double *__restrict__ coords,
+                                                                 const double *__restrict__ nodeR,
+                                                                 const double *__restrict__ u, bool pressure_deck,
+                                                                 double *__restrict__ out) {
+    __shared__ __align__(16) double rec[Q4R_THREADS][Q4R_ROW];
+    const int64_t e0 = (int64_t)blockIdx.x * Q4R_THREADS;
+    const int t = threadIdx.x;
+    if (e0 + t < nq) q4_recover_element(e0 + t, nodes, prop, coords, nodeR, u, pressure_deck, rec[t]);
+    __syncthreads();
+    const int n = (int)(nq - e0 < Q4R_THREADS ? nq - e0 : Q4R_THREADS);
+    double *dst = out + REC_SHELL * e0;
+    if ((reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+        // chunk c = 24 record + part; threads step by 64 = 2 records + 16 parts
+        for (int j = t / 24, part = t % 24; j < n;) {
+            reinterpret_cast<double2 *>(dst + REC_SHELL * j)[part] = reinterpret_cast<const double2 *>(rec[j])[part];
+            part += 16;
+            j += 2;
+            if (part >= 24) { part -= 24; ++j; }
+        }
+    } else {
+        for (int c = t; c < n * REC_SHELL; c += Q4R_THREADS) dst[c] = rec[c / REC_SHELL][c % REC_SHELL];
     }
 }
 

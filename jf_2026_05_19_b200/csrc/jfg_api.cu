@@ -1847,8 +1847,8 @@ jfg_status jfg_recover_stresses_device(jfg_model *m, const double *u_dev, const 
     // the model-level conditions of _quad4_pressure_resultant_moment_scale the handle sees itself
     const bool pressure_deck = (flags & JFG_RECOVER_PRESSURE_DECK) && m->nb == 0 && m->n_rbe2 == 0;
     if (shell_out_dev && m->nq) {
-        q4_recover_kernel<<<(unsigned)cdiv(m->nq, 128), 128, 0, m->stream>>>(m->nq, m->d_q4n, m->d_q4p, m->d_coords,
-                                                                            m->d_nodeR, u_dev, pressure_deck, shell_out_dev);
+        q4_recover_kernel<<<(unsigned)cdiv(m->nq, Q4R_THREADS), Q4R_THREADS, 0, m->stream>>>(
+            m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, u_dev, pressure_deck, shell_out_dev);
         CK(cudaGetLastError());
     }
     if (shell_out_dev && m->nt) {
