@@ -515,16 +515,21 @@ __device__ __forceinline__ void block_row_sum(const double *__restrict__ staging
 // order.  Bar contributions [rb, b) also carry three rotation sub-blocks:
 // row i < 3 adds them to columns 3-5, row i >= 3 to all six columns.  Shell-only
 // blocks leave zeros there.
+template <int NB>
 __device__ __forceinline__ void block_kg_sums(const double *__restrict__ staging, const double *__restrict__ kg_rot,
-                                              const int32_t *__restrict__ slot_bar, const int32_t a[2], const int32_t rb[2],
-                                              const int32_t b[2], int i, double *t0, double *t1) {
-    double ch[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
-    if (i < 5) {
-        const int32_t len = max(b[0] - a[0], b[1] - a[1]);
-        for (int32_t t = 0; t < len; t += 4) {
-            double2 x[2][4];
+                                              const int32_t *__restrict__ slot_bar, const int32_t a[NB], const int32_t rb[NB],
+                                              const int32_t b[NB], int i, double *const tt_out[NB]) {
+    double ch[NB][2];
 #pragma unroll
-            for (int m = 0; m < 2; ++m)
+    for (int m = 0; m < NB; ++m) ch[m][0] = ch[m][1] = 0.0;
+    if (i < 5) {
+        int32_t len = b[0] - a[0];
+#pragma unroll
+        for (int m = 1; m < NB; ++m) len = max(len, b[m] - a[m]);
+        for (int32_t t = 0; t < len; t += 4) {
+            double2 x[NB][4];
+#pragma unroll
+            for (int m = 0; m < NB; ++m)
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int32_t q = a[m] + t + u;
@@ -532,14 +537,14 @@ __device__ __forceinline__ void block_kg_sums(const double *__restrict__ staging
                                        : make_double2(0.0, 0.0);
                 }
 #pragma unroll
-            for (int m = 0; m < 2; ++m)
+            for (int m = 0; m < NB; ++m)
 #pragma unroll
                 for (int u = 0; u < 4; ++u) { ch[m][0] += x[m][u].x; ch[m][1] += x[m][u].y; }
         }
     }
     const int i3 = i < 3 ? i : i - 3;
 #pragma unroll
-    for (int m = 0; m < 2; ++m) {
+    for (int m = 0; m < NB; ++m) {
         double s[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         for (int32_t q = rb[m]; q < b[m]; ++q) {
             const double *p = kg_rot + 27 * (int64_t)__ldg(slot_bar + q) + 3 * i3;
@@ -547,7 +552,7 @@ __device__ __forceinline__ void block_kg_sums(const double *__restrict__ staging
             const int o3 = i < 3 ? 0 : 18;  // translation-rotation / rotation-rotation rows
             s[3] += __ldg(p + o3); s[4] += __ldg(p + o3 + 1); s[5] += __ldg(p + o3 + 2);
         }
-        double *tt = m == 0 ? t0 : t1;
+        double *tt = tt_out[m];
         // translation values 2i, 2i+1 (value v sits at row v / 3, column v % 3; 9-11 are padding)
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
@@ -578,20 +583,56 @@ __device__ __forceinline__ void block_write(int64_t k, int i, const double sr[6]
     }
 }
 
-// The same writes from the block's precomputed CSC positions (blk_pos_kernel):
-// one load of the positions instead of the nodes, offsets and six row starts
-// per node, which takes a dependent memory round trip off each thread.
-__device__ __forceinline__ void block_write_pos(int64_t k, int i, const double sr[6], const double sc[6],
-                                                const int64_t *__restrict__ pa, const int64_t *__restrict__ pb,
-                                                const int2 *__restrict__ len, double *nz) {
-    const int64_t a0 = __ldg(pa + k) + i, b0 = __ldg(pb + k);
-    const int2 l = __ldg(len + k);
+// One block per thread, for patterns whose node rows are evenly spaced
+// (blk_pos_kernel): (6A + r, 6B + i) sits at pa + r * L_A + i, so the
+// block's CSC positions are loaded together with its segment bounds and the
+// path to the stores is two dependent memory round trips (positions and
+// bounds, then the staged rows).  Thread (g, i) of a warp sums row i of block
+// 5w + g; the rows meet in shared memory for the column writes.
+template <bool KG>
+__global__ void __launch_bounds__(128, 8) block_reduce1_kernel(int64_t n_blk, const int32_t *__restrict__ seg,
+                                                               const int32_t *__restrict__ rot,
+                                                               const int32_t *__restrict__ slot_bar, int64_t kg_rot_off,
+                                                               const double *__restrict__ staging,
+                                                               const int64_t *__restrict__ pa, const int64_t *__restrict__ pb,
+                                                               const int2 *__restrict__ len, double *nz, int64_t staging_stride,
+                                                               int64_t nnz) {
+    __shared__ double tr[4][5][36];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane / 6, i = lane - 6 * (lane / 6);
+    const int64_t k = ((int64_t)blockIdx.x * 4 + warp) * 5 + g;
+    const bool one = g < 5 && k < n_blk;
+    staging += (int64_t)blockIdx.y * staging_stride;  // batched variant
+    nz += (int64_t)blockIdx.y * nnz;
+    double *tile = tr[warp][g];
+    int64_t p_a = 0, p_b = -1;
+    int2 l = make_int2(0, 0);
+    if (one) {
+        p_a = __ldg(pa + k);
+        p_b = __ldg(pb + k);
+        l = __ldg(len + k);
+        const int32_t a0 = __ldg(seg + k), b0 = __ldg(seg + k + 1);
+        if (KG) {
+            const int32_t aa[1] = {a0}, bb[1] = {b0}, rr[1] = {__ldg(rot + k)};
+            double *const tt[1] = {tile};
+            block_kg_sums<1>(staging, staging + kg_rot_off, slot_bar, aa, rr, bb, i, tt);
+        } else {
+            double s[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            block_row_sum(staging, a0, b0, i, s);
 #pragma unroll
-    for (int r = 0; r < 6; ++r) nz[a0 + (int64_t)r * l.x] = sc[r];
-    if (b0 >= 0) {
-        const int64_t bb = b0 + i;
+            for (int c = 0; c < 6; ++c) tile[6 * i + c] = s[c];
+        }
+    }
+    __syncwarp();
+    if (one) {
+        const int64_t ca = p_a + i;
 #pragma unroll
-        for (int j = 0; j < 6; ++j) nz[bb + (int64_t)j * l.y] = sr[j];
+        for (int r = 0; r < 6; ++r) nz[ca + (int64_t)r * l.x] = tile[6 * r + i];
+        if (p_b >= 0) {
+            const int64_t cb = p_b + i;
+#pragma unroll
+            for (int j = 0; j < 6; ++j) nz[cb + (int64_t)j * l.y] = tile[6 * i + j];
+        }
     }
 }
 
@@ -601,16 +642,14 @@ __device__ __forceinline__ void block_write_pos(int64_t k, int i, const double s
 // also holds column i for the coalesced write above.
 constexpr int kRedWarps = 4;
 
-template <bool KG, bool POS>
+template <bool KG>
 __global__ void __launch_bounds__(32 * kRedWarps, 8) block_reduce_kernel(int64_t n_blk, const int32_t *__restrict__ seg,
                                                            const int32_t *__restrict__ rot,
                                                            const int32_t *__restrict__ slot_bar, int64_t kg_rot_off,
                                                            const double *__restrict__ staging, const int32_t *__restrict__ A,
                                                            const int32_t *__restrict__ B, const int32_t *__restrict__ offAB,
                                                            const int32_t *__restrict__ offBA, const int64_t *__restrict__ rowptr,
-                                                           const int64_t *__restrict__ pa, const int64_t *__restrict__ pb,
-                                                           const int2 *__restrict__ len, double *nz, int64_t staging_stride,
-                                                           int64_t nnz) {
+                                                           double *nz, int64_t staging_stride, int64_t nnz) {
     __shared__ double tr[kRedWarps][2][5][36];
     const int64_t half = (n_blk + 1) / 2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -625,7 +664,8 @@ __global__ void __launch_bounds__(32 * kRedWarps, 8) block_reduce_kernel(int64_t
         const int32_t a1 = two ? __ldg(seg + k1) : 0, b1 = two ? __ldg(seg + k1 + 1) : 0;
         if (KG) {
             const int32_t aa[2] = {a0, a1}, bb[2] = {b0, b1}, rr[2] = {__ldg(rot + k0), two ? __ldg(rot + k1) : 0};
-            block_kg_sums(staging, staging + kg_rot_off, slot_bar, aa, rr, bb, i, tr[warp][0][g], tr[warp][1][g]);
+            double *const tt[2] = {tr[warp][0][g], tr[warp][1][g]};
+            block_kg_sums<2>(staging, staging + kg_rot_off, slot_bar, aa, rr, bb, i, tt);
         } else {
             block_row_sum(staging, a0, b0, i, s0);
             block_row_sum(staging, a1, b1, i, s1);
@@ -642,13 +682,8 @@ __global__ void __launch_bounds__(32 * kRedWarps, 8) block_reduce_kernel(int64_t
         double c0[6], c1[6];
 #pragma unroll
         for (int r = 0; r < 6; ++r) { c0[r] = tr[warp][0][g][6 * r + i]; c1[r] = tr[warp][1][g][6 * r + i]; }
-        if (POS) {
-            block_write_pos(k0, i, s0, c0, pa, pb, len, nz);
-            if (two) block_write_pos(k1, i, s1, c1, pa, pb, len, nz);
-        } else {
-            block_write(k0, i, s0, c0, A, B, offAB, offBA, rowptr, nz);
-            if (two) block_write(k1, i, s1, c1, A, B, offAB, offBA, rowptr, nz);
-        }
+        block_write(k0, i, s0, c0, A, B, offAB, offBA, rowptr, nz);
+        if (two) block_write(k1, i, s1, c1, A, B, offAB, offBA, rowptr, nz);
     }
 }
 
@@ -1463,16 +1498,26 @@ jfg_status launch_reduce(jfg_model *m, const Batch &bt, bool kg) {
     CK(mark(m, 4));
     if (m->n_blk) {
         const dim3 grid((unsigned)cdiv(cdiv((m->n_blk + 1) / 2, 5), kRedWarps), nv);
-        auto launch = [&](auto kernel, int64_t rot_off) {
-            kernel<<<grid, 32 * kRedWarps, 0, m->stream>>>(m->n_blk, m->d_blk_seg, m->d_blk_rot, m->d_slot_bar, rot_off, bt.staging,
-                                                        m->d_blk_A, m->d_blk_B, m->d_blk_offAB, m->d_blk_offBA, m->d_rowptr,
-                                                        m->d_blk_pa, m->d_blk_pb, m->d_blk_len, bt.nz, bt.staging_stride, m->nnz);
-        };
-        const int64_t rot_off = 12 * m->n_blk_contrib;
-        if (kg && m->blk_even) launch(block_reduce_kernel<true, true>, rot_off);
-        else if (kg) launch(block_reduce_kernel<true, false>, rot_off);
-        else if (m->blk_even) launch(block_reduce_kernel<false, true>, 0);
-        else launch(block_reduce_kernel<false, false>, 0);
+        const int64_t rot_off = kg ? 12 * m->n_blk_contrib : 0;
+        if (m->blk_even) {
+            const dim3 grid1((unsigned)cdiv(cdiv(m->n_blk, 5), 4), nv);
+            if (kg)
+                block_reduce1_kernel<true><<<grid1, 128, 0, m->stream>>>(m->n_blk, m->d_blk_seg, m->d_blk_rot, m->d_slot_bar, rot_off,
+                                                                      bt.staging, m->d_blk_pa, m->d_blk_pb, m->d_blk_len, bt.nz,
+                                                                      bt.staging_stride, m->nnz);
+            else
+                block_reduce1_kernel<false><<<grid1, 128, 0, m->stream>>>(m->n_blk, m->d_blk_seg, m->d_blk_rot, m->d_slot_bar, 0,
+                                                                       bt.staging, m->d_blk_pa, m->d_blk_pb, m->d_blk_len, bt.nz,
+                                                                       bt.staging_stride, m->nnz);
+        } else if (kg) {
+            block_reduce_kernel<true><<<grid, 32 * kRedWarps, 0, m->stream>>>(
+                m->n_blk, m->d_blk_seg, m->d_blk_rot, m->d_slot_bar, rot_off, bt.staging, m->d_blk_A, m->d_blk_B,
+                m->d_blk_offAB, m->d_blk_offBA, m->d_rowptr, bt.nz, bt.staging_stride, m->nnz);
+        } else {
+            block_reduce_kernel<false><<<grid, 32 * kRedWarps, 0, m->stream>>>(
+                m->n_blk, m->d_blk_seg, m->d_blk_rot, m->d_slot_bar, 0, bt.staging, m->d_blk_A, m->d_blk_B,
+                m->d_blk_offAB, m->d_blk_offBA, m->d_rowptr, bt.nz, bt.staging_stride, m->nnz);
+        }
     }
     CK(cudaGetLastError());
     CK(mark(m, 5));

@@ -84,3 +84,16 @@ def warped(m):
     c[n] = c[n] + 0.5 * np.cross(c[m.q4_nodes[0, 1]] - c[m.q4_nodes[0, 0]], c[m.q4_nodes[0, 3]] - c[m.q4_nodes[0, 0]]) / 100.0
     del R
     return dataclasses.replace(m, coords=c)
+
+
+def plate_axis_rbe2(n=6, size=120.0, cm="123"):
+    """Flat plate with an RBE2 whose slave lies on its master's grid row: the
+    offset is along x, so the image of the slave's translations has no theta_x
+    term and the master's theta_x row holds fewer columns than its other rows."""
+    p = D.plate_c1(n=n, size=size)
+    nn = n + 1
+    idx = lambda i, j: j * nn + i
+    j = n // 2
+    return dataclasses.replace(p, rbe2_master=np.array([idx(2, j)], np.int32), rbe2_cm=np.array([D.cm_mask(cm)], np.int32),
+                               rbe2_slave_ptr=np.array([0, 1], np.int64), rbe2_slaves=np.array([idx(n - 1, j)], np.int32),
+                               name="plate_axis_rbe2")

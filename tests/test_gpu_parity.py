@@ -19,8 +19,11 @@ GOLD = os.path.join(os.path.dirname(__file__), "golden", "oracle_fixtures.npz")
 
 
 def _decks():
-    from decks_extra import skewed_plane, with_unused_nodes
+    from decks_extra import plate_axis_rbe2, skewed_plane, with_unused_nodes
     return {
+        # partial-CM RBE2 with an axis offset: the master's rows hold different
+        # columns, which the block path avoids by treating masters as special
+        "plate_axis_rbe2": plate_axis_rbe2(),
         "plate_40x40": decks.plate_c1(),
         "panel_no_offset": decks.stiffened_panel_c2(seed=1, lx=300.0, ly=200.0, stringer_every=4, stringer_offset=0.0),
         "barrel_small": decks.barrel_small(seed=2, n_circ=72, n_axial=24),
