@@ -10,11 +10,15 @@ longerons every 5 degrees and an RBE2 tying the loaded end to a centre node
 (about 1.17M elements, 6.0M dof).  Synthetic, seeded inputs.
 
 value: elements/s with all inputs resident in HBM (device-pointer C ABI).
-e2e:   the same metric through the host-buffer C ABI calls (pinned host
-       u in, K and KG values out, copies inside the timed region).
+e2e:   the same metric through the host-buffer C ABI calls (u in, K and KG
+       values out, copies inside the timed region), with ordinary pageable
+       host arrays as the Julia binding passes them; the pinned-memory figure
+       is reported beside it.
 
 --impl reference times the CPU restatement of the reference algorithm (the
-reference itself is Julia and cannot run on this image) on a bounded sample.
+reference itself is Julia and cannot run on this image) on the same barrel:
+each step assembles K and KG of one axial band (1/24) of it, on its full node
+set, and consecutive steps walk the bands.
 
 Multi-GPU (torchrun): every rank assembles its own barrel replica (design
 variants are independent units, no data-path collective); value is the sum
@@ -83,31 +87,95 @@ def workload_config(m, workload: str, world: int):
             "replicas": world, "l2": "inputs and outputs larger than L2 (staging and CSR values are GBs)"}
 
 
+CPU_BANDS = 24   # the barrel's 696 cell rows = 24 bands of 29 rows (~49k elements each)
+
+
+def barrel_band(m, band: int, n_bands: int = CPU_BANDS):
+    """Elements of one axial band of a barrel deck, in their deck order, on the
+    full node set (so K and KG keep the whole barrel's dof numbering, pattern
+    size and RBE2).  An element belongs to the band of its lowest cell row."""
+    import dataclasses
+    n_ring = m.n_nodes - (1 if m.rbe2_master.shape[0] else 0)
+    z = m.coords[:, 2]
+    rows_z = np.unique(np.round(z[:n_ring], 6))
+    n_rows = rows_z.shape[0] - 1
+    row_of = np.searchsorted(rows_z, np.round(z, 6))
+    lo, hi = band * n_rows // n_bands, (band + 1) * n_rows // n_bands
+
+    def pick(nodes):
+        r = row_of[nodes].min(axis=1)
+        return (r >= lo) & (r < hi)
+    q, t, b = pick(m.q4_nodes), pick(m.t3_nodes), pick(m.bar_nodes)
+    return dataclasses.replace(m, q4_nodes=m.q4_nodes[q], q4_prop=m.q4_prop[q], t3_nodes=m.t3_nodes[t],
+                               t3_prop=m.t3_prop[t], bar_nodes=m.bar_nodes[b], bar_prop=m.bar_prop[b],
+                               bar_pin=m.bar_pin[b], name=f"{m.name} band {band}/{n_bands}")
+
+
+class CpuBands:
+    """The CPU restatement of the reference assembly over bands of the bench barrel.
+
+    Each call of step() assembles K (with max_elem_stiff and orig_diag) and KG
+    of the next band, so consecutive steps walk the whole barrel; it returns
+    the band's element count and records the time spent in the element loops
+    and in the constraint redistribution + sparse() of each matrix."""
+
+    def __init__(self, full, n_bands: int = CPU_BANDS):
+        from jf_2026_05_19_b200 import decks
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O  # CPU restatement: the reported baseline and the reference arm
+        self.O = O
+        self.n_bands = n_bands
+        # models other than the barrel are small enough to assemble whole per step
+        self.bands = [barrel_band(full, b, n_bands) for b in range(n_bands)] if n_bands > 1 else [full]
+        self.u = decks.smooth_displacement(full, seed=1)
+        self.next = 0
+        self.t_elem = self.t_sparse = 0.0
+
+    def step(self) -> int:
+        m = self.bands[self.next % self.n_bands]
+        self.next += 1
+        dk = self.O.assemble_k(m, detail=True)[5]
+        dg = self.O.assemble_kg(m, self.u, detail=True)[3]
+        self.t_elem += dk["t_elements"] + dg["t_elements"]
+        self.t_sparse += dk["t_sparse"] + dg["t_sparse"]
+        return m.n_elements
+
+    def reset_phases(self):
+        self.t_elem = self.t_sparse = 0.0
+
+    def phases(self, steps: int) -> dict:
+        return {"element_loops_s_per_step": self.t_elem / steps,
+                "redistribution_and_sparse_s_per_step": self.t_sparse / steps,
+                "note": "sparse() is serial in the reference (SparseArrays); element loops use every thread"}
+
+    def sample_text(self, steps: int, n_el: int, seconds: float) -> str:
+        if self.n_bands == 1:
+            return f"{steps} steps, each K+KG of the whole model ({self.bands[0].name}); {n_el} elements in {seconds:.1f} s"
+        return (f"{steps} steps, each K+KG of one axial band (1/{self.n_bands}, 29 of 696 cell rows, "
+                f"~{n_el // max(steps, 1)} elements) of this barrel on its full 6.02M-dof node set, consecutive "
+                f"bands per step; {n_el} elements in {seconds:.1f} s")
+
+
+def time_cpu_oracle(full, seconds: float, steps_max: int = 24):
+    """Reported CPU baseline: bands of the bench barrel for about `seconds`."""
+    cpu = CpuBands(full)
+    cpu.step()  # page in
+    cpu.reset_phases()
+    n_el, steps = 0, 0
+    t0 = time.perf_counter()
+    while True:
+        n_el += cpu.step()
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or steps >= steps_max:
+            break
+    return n_el / el, cpu.O.num_threads(), cpu.sample_text(steps, n_el, el), cpu.phases(steps)
+
+
 def cpu_sample_model(seed: int = 0):
-    """Bounded sample with the barrel's element mix (~50k elements)."""
+    """A 480 x 96 barrel with the bench barrel's element mix (recovery baseline)."""
     from jf_2026_05_19_b200 import decks
     return decks.barrel_c4(seed=seed, n_circ=480, n_axial=96, ring_every=8, longeron_every=7, name="barrel_480x96")
-
-
-def time_cpu_oracle(seconds: float, reps_max: int = 50):
-    """Oracle K+KG on the bounded sample; returns (elements/s, threads, sample text)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O  # CPU restatement: reported baseline only
-    from jf_2026_05_19_b200 import decks
-    m = cpu_sample_model()
-    u = decks.smooth_displacement(m, seed=1)
-    threads = O.num_threads()
-    O.assemble_k(m)  # warm caches / page in
-    t0 = time.perf_counter()
-    reps = 0
-    while True:
-        O.assemble_k(m)
-        O.assemble_kg(m, u)
-        reps += 1
-        el = time.perf_counter() - t0
-        if el >= seconds or reps >= reps_max:
-            break
-    return m.n_elements * reps / el, threads, f"{m.name}: {m.n_elements} elements, {reps} K+KG passes, {el:.1f} s"
 
 
 def time_cpu_recovery(reps: int = 3):
@@ -271,32 +339,37 @@ def max_over_ranks(seconds: float, dist, device) -> float:
 
 
 def run_reference(args):
+    """The reference algorithm on the host cores (C++ restatement, OpenMP over
+    elements, serial sparse like the reference), on the GPU arm's workload:
+    each step is K+KG of one axial band of the same barrel."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from jf_2026_05_19_b200 import decks
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-    m = cpu_sample_model()
-    u = decks.smooth_displacement(m, seed=1)
-    threads = O.num_threads()
+    if args.workload == "variants":
+        from jf_2026_05_19_b200 import decks
+        full = decks.panel_variant_c3(0, seed=0, no_offset=True)
+    else:
+        full = make_model(args.workload, seed=0)
+    cpu = CpuBands(full, CPU_BANDS if args.workload == "barrel" else 1)
     for _ in range(max(args.warmup, 1)):
-        O.assemble_k(m); O.assemble_kg(m, u)
+        cpu.step()
+    cpu.reset_phases()
+    n_el = 0
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        O.assemble_k(m); O.assemble_kg(m, u)
+        n_el += cpu.step()
     el = time.perf_counter() - t0
-    v = m.n_elements * args.steps / el
-    sample = f"{m.name}: {m.n_elements} elements per step, barrel element mix"
-    # the config is the GPU arm's workload; each timed step is the bounded sample above
-    full = make_model(args.workload, seed=0)
-    config = dict(workload_config(full, args.workload, args.gpus), parallelism=f"replicas x{args.gpus}",
-                  timed_sample=m.name)
+    v = n_el / el
+    threads = cpu.O.num_threads()
+    config = dict(workload_config(full, args.workload, args.gpus), parallelism=f"replicas x{args.gpus}")
+    if args.workload == "variants":
+        config = {"workload": "stiffened-panel design variants, one variant's K+KG per step"}
     line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded barrel deck)",
             "config": config,
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": cpu.sample_text(args.steps, n_el, el), "phases": cpu.phases(args.steps),
                              "note": "reference is Julia 1.12 (absent here); C++ restatement of its algorithm"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -591,7 +664,7 @@ def run_reference_serving(args):
     """Oracle port, one request at a time: elements/s on the bounded barrel sample,
     converted with the stream's mean request size."""
     from jf_2026_05_19_b200 import decks
-    v_el, threads, sample = time_cpu_oracle(args.cpu_seconds)
+    v_el, threads, sample, _ = time_cpu_oracle(make_model("barrel", seed=0), args.cpu_seconds)
     fams = decks.serving_families()
     mean_el = float(np.mean([m.n_elements for m in fams]))
     v = v_el / mean_el
@@ -678,26 +751,29 @@ def main():
     kt, kn = g.timing_accumulated("k", reset=True)
     gt, gn = g.timing_accumulated("kg", reset=True)
 
-    # end-to-end through the host-buffer C ABI (pinned host memory)
+    # end-to-end through the host-buffer C ABI: ordinary pageable host arrays,
+    # as the Julia binding passes Vector{Float64}; pinned arrays beside it
     e2e_steps = max(1, min(args.e2e_steps, args.steps))
-    u_pin = torch.from_numpy(u_host).pin_memory()
-    nzk_pin = torch.empty(g.nnz, dtype=torch.float64).pin_memory()
-    nzg_pin = torch.empty(g.nnz, dtype=torch.float64).pin_memory()
-    dg_pin = torch.empty(g.ndof, dtype=torch.float64).pin_memory()
-    un, nkn, ngn, dgn = u_pin.numpy(), nzk_pin.numpy(), nzg_pin.numpy(), dg_pin.numpy()
-    g.assemble_k(nkn, want_diag=True, diag_out=dgn); g.assemble_kg(un, ngn)  # warm
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    s2 = torch.cuda.Event(enable_timing=True); e2 = torch.cuda.Event(enable_timing=True)
-    s2.record(stream)
-    for _ in range(e2e_steps):
-        nz, mxv, dgv = g.assemble_k(nkn, want_diag=True, diag_out=dgn)
-        g.assemble_kg(un, ngn)
-    e2.record(stream)
-    e2.synchronize()
-    e2e_el = s2.elapsed_time(e2) / 1e3
-    e2e_el = max_over_ranks(e2e_el, dist, dev)
+
+    def e2e_time(u_h, nzk_h, nzg_h, dg_h):
+        g.assemble_k(nzk_h, want_diag=True, diag_out=dg_h); g.assemble_kg(u_h, nzg_h)  # warm, pages in
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        s2 = torch.cuda.Event(enable_timing=True); e2 = torch.cuda.Event(enable_timing=True)
+        s2.record(stream)
+        for _ in range(e2e_steps):
+            g.assemble_k(nzk_h, want_diag=True, diag_out=dg_h)
+            g.assemble_kg(u_h, nzg_h)
+        e2.record(stream)
+        e2.synchronize()
+        return max_over_ranks(s2.elapsed_time(e2) / 1e3, dist, dev)
+
+    e2e_el = e2e_time(u_host.copy(), np.empty(g.nnz), np.empty(g.nnz), np.empty(g.ndof))
+    pin = [torch.from_numpy(u_host).pin_memory()] + [torch.empty(n, dtype=torch.float64).pin_memory()
+                                                     for n in (g.nnz, g.nnz, g.ndof)]
+    e2e_pinned_el = e2e_time(*[t.numpy() for t in pin])
+    del pin
 
     # SOL 101 output recovery of the same model and displacement, timed on its
     # own after the step (it follows the static solve, not the assembly)
@@ -722,6 +798,7 @@ def main():
     n_el = m.n_elements
     value = world * n_el * args.steps / elapsed
     e2e_value = world * n_el * e2e_steps / e2e_el
+    e2e_pinned_value = world * n_el * e2e_steps / e2e_pinned_el
     # dominant kernel over the timed region
     per_kernel = {}
     for tag, tt, nn in (("k", kt, kn), ("kg", gt, gn)):
@@ -759,16 +836,18 @@ def main():
             "data": "synthetic (seeded deck generator; smooth seeded displacement for KG)",
             "config": dict(workload_config(m, args.workload, world), parallelism=f"replicas x{world}", nnz=g.nnz),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "steps": e2e_steps},
+                    "steps": e2e_steps, "host_memory": "pageable (numpy arrays, as a Julia Vector{Float64})",
+                    "pinned_value": e2e_pinned_value},
             "roofline": roof, "gpu_launches": launches_per_step * args.steps, "clocks": clk,
             "kernel_ms": per_kernel, "fp64_dgemm_tflops": fp64_peak, "model_stats": st,
             "whole_step_roofline": {"flops": roofline.flops_per_step(counts), "bytes": roofline.bytes_per_step(counts, g.nnz)},
             "recovery": {"ms": rec_ms, "elements_per_s": n_el / rec_ms * 1e3, "timed_calls": 5,
                          "output_bytes": 8 * (rec_sh.numel() + (rec_bar.numel() if counts["bar"] else 0)),
                          "note": "jfg_recover_stresses_device on the same model and u, outside the timed step"}}
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, thr, sample = time_cpu_oracle(args.cpu_seconds)
-        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "barrel":
+        v, thr, sample, phases = time_cpu_oracle(m, args.cpu_seconds)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample,
+                                "phases": phases}
         line["recovery"]["cpu_port_elements_per_s"] = time_cpu_recovery()
     if rank == 0:
         print(json.dumps(line), flush=True)

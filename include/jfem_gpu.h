@@ -373,9 +373,10 @@ void jfg_server_destroy(jfg_server *s);
 
 /* ---- Allocation-free CQUAD4 stiffness assembly ---------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
- * memory where they need a stiffness matrix (inside a CUDA graph capture, or
- * under a host framework that owns all device memory, or in a loop that
- * forbids allocator calls): assembles K of a small patch of CQUAD4 elements
+ * memory where they need a stiffness matrix: a host framework that has
+ * reserved all device memory up front and hands out only its own buffers,
+ * or a real-time loop that forbids allocator calls because they may block or
+ * synchronise the device.  Assembles K of a small patch of CQUAD4 elements
  * into a caller-provided CSR value array without allocating anything.
  *
  * All pointers are device memory: coords (n_nodes*3), node_R (n_nodes*9 or
@@ -384,19 +385,27 @@ void jfg_server_destroy(jfg_server *s);
  * holds every element entry -- the arrays jfg_pattern_fill returns, minus 1,
  * for a CQUAD4-only model.  nzval receives one value per stored entry in the
  * same order (entries no element touches are written as 0).  stream is a
- * cudaStream_t (NULL: the legacy default stream); the call waits for it.
+ * cudaStream_t (NULL: the legacy default stream).  The call is synchronous:
+ * it waits for the stream after its input checks and again before it
+ * returns, to read the status back.
+ *
+ * Input checks are those of jfg_model_create for CQUAD4: a node index outside
+ * [0, n_nodes), a repeated node, or thickness or E not positive give
+ * JFG_ERR_INVALID; a non-flat quad (outside the flat default branch) gives
+ * JFG_ERR_UNSUPPORTED.  These run on the device before the element kernel,
+ * and nothing else is launched when one fails.
  *
  * Intermediate data lives in one fixed array in the library's device image
  * (about 6.3 MB, held by every GPU that loads the library until the process
  * exits).  Limits: n_quad4 <= JFG_NOALLOC_MAX_QUAD4, n_nodes <=
- * JFG_NOALLOC_MAX_NODES, at most JFG_NOALLOC_MAX_VALENCE elements per node;
- * larger inputs are rejected with JFG_ERR_UNSUPPORTED (size checks before
- * any launch, the valence check on the device); a node index outside
- * [0, n_nodes) returns JFG_ERR_INVALID before the element kernel runs.  The first call on each
- * device looks up the array's device address (cudaGetSymbolAddress); make
- * that first call before any stream capture.  Every call reuses the same
- * array, so calls that overlap on the GPU (concurrent streams or threads)
- * race and must be serialised by the caller. */
+ * JFG_NOALLOC_MAX_NODES (both checked before any launch), at most
+ * JFG_NOALLOC_MAX_VALENCE elements per node (checked on the device); larger
+ * inputs give JFG_ERR_UNSUPPORTED.  Whenever the status is not JFG_OK the
+ * contents of nzval are unspecified.  The first call on each device looks up
+ * the array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  Every call reuses the same array, so calls that
+ * overlap on the GPU (concurrent streams or threads) race and must be
+ * serialised by the caller. */
 #define JFG_NOALLOC_MAX_QUAD4 2048
 #define JFG_NOALLOC_MAX_NODES 8192
 #define JFG_NOALLOC_MAX_VALENCE 8

@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import hashlib
 import os
+import re
 import shutil
 import subprocess
 
@@ -16,7 +17,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libjfemgpu.so")
 SOURCES = ["jfg_api.cu", "jfg_server.cu"]
-HEADERS = ["jfg_common.cuh", "elem_q4.cuh", "elem_t3.cuh", "elem_bar.cuh"]  # plus the SOURCES
+_INCLUDE = re.compile(r'^\s*#\s*include\s*"([^"]+)"', re.M)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -32,7 +33,22 @@ def host_compiler() -> list:
 
 
 def deps() -> list:
-    return [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "jfem_gpu.h")]
+    """Every file the library is compiled from: the SOURCES and, transitively,
+    every quoted #include they reach (resolved against the including file's
+    folder, as the preprocessor does).  Sorted, so the hash is stable."""
+    seen, todo = set(), [os.path.join(CSRC, f) for f in SOURCES]
+    while todo:
+        p = os.path.normpath(todo.pop())
+        if p in seen:
+            continue
+        seen.add(p)
+        with open(p) as f:
+            for inc in _INCLUDE.findall(f.read()):
+                q = os.path.join(os.path.dirname(p), inc)
+                if not os.path.exists(q):
+                    raise FileNotFoundError(f"{p} includes {inc}, which does not exist")
+                todo.append(q)
+    return sorted(seen)
 
 
 def source_hash() -> str:
@@ -43,7 +59,7 @@ def source_hash() -> str:
     signatures -- is never loaded by mistake, whatever the file times are."""
     h = hashlib.sha256()
     for p in deps():
-        h.update(os.path.basename(p).encode())
+        h.update(os.path.relpath(p, ROOT).encode())
         with open(p, "rb") as f:
             h.update(f.read())
     return h.hexdigest()[:16]

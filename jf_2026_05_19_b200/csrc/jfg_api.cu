@@ -164,24 +164,7 @@ inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 // ---------------------------------------------------------------------------
 
 bool host_q4_flat(const double *p1, const double *p2, const double *p3, const double *p4) {
-    double d13[3], d24[3], n[3], c[3];
-    sub3(p3, p1, d13);
-    sub3(p4, p2, d24);
-    cross3(d13, d24, n);
-    double len = std::sqrt(dot3(n, n));
-    for (int i = 0; i < 3; ++i) c[i] = (p1[i] + p2[i] + p3[i] + p4[i]) / 4.0;
-    double maxdev = 0.0;
-    if (len > 1e-12) {
-        double g[3] = {n[0] / len, n[1] / len, n[2] / len};
-        const double *ps[4] = {p1, p2, p3, p4};
-        for (int k = 0; k < 4; ++k) {
-            double d[3];
-            sub3(ps[k], c, d);
-            maxdev = std::max(maxdev, std::fabs(dot3(d, g)));
-        }
-    }
-    double L = std::max(std::sqrt(dot3(d13, d13)), std::sqrt(dot3(d24, d24)));
-    return maxdev < 1e-6 * std::max(L, 1e-12);
+    return jfg::q4_is_flat(p1, p2, p3, p4);
 }
 
 // RBE2 dependent -> independent map (constraints.jl:7-74), 0-based dofs.
@@ -2020,14 +2003,16 @@ jfg_status jfg_last_timing(jfg_model *m, double *element_ms, double *reduce_ms, 
 // Allocation-free CQUAD4 stiffness assembly for small patches.
 //
 // Some callers cannot allocate GPU memory at the point where they need a
-// stiffness matrix: code that runs inside a CUDA graph capture, a host
-// framework that has reserved all device memory up front and hands out only
-// its own buffers, or a real-time loop that forbids allocator calls.  This
+// stiffness matrix: a host framework that has reserved all device memory up
+// front and hands out only its own buffers (an allocation would fail or
+// fragment its pool), or a real-time loop that forbids allocator calls
+// because cudaMalloc/cudaFree may block or synchronise the device.  This
 // entry point serves them: the caller passes every input and the output as
 // device pointers, and all intermediate data (element blocks, node incidence,
 // an error word) lives in the fixed array below, which every GPU that loads
 // this library keeps until the process exits.  No cudaMalloc, cudaFree or
-// allocating library call happens on this path.
+// allocating library call happens on this path.  The call is synchronous: it
+// waits for its stream twice to read the error word back to the host.
 // ===========================================================================
 
 namespace {
@@ -2078,15 +2063,39 @@ jfg_status jfg_na_scratch(double **out) {
     return JFG_OK;
 }
 
-// Checks the node indices (error word 2 when one is out of range) and writes
-// the identity block-slot map (no transposition: block (e, p) holds rows of
-// local node a, columns of local node b, a <= b).  The error word itself is
-// cleared beforehand: it is the only scratch that must start at zero.
-__global__ void na_prepare_kernel(int64_t nq, int64_t n_nodes, const int32_t *__restrict__ nodes, double *base) {
+// Error-word bits.  Any INVALID bit maps to JFG_ERR_INVALID, otherwise any
+// other bit to JFG_ERR_UNSUPPORTED, the statuses jfg_model_create gives for
+// the same input.
+constexpr int32_t kNaInvalid = 1;      // node index out of range, repeated node, h <= 0 or E <= 0
+constexpr int32_t kNaNotFlat = 2;      // warp >= 1e-6 of the diagonal (outside the flat default branch)
+constexpr int32_t kNaValence = 4;      // a node with more than JFG_NOALLOC_MAX_VALENCE elements
+
+// One thread per element: the per-element checks of the regular model build
+// (node range, repeated node, positive thickness and E, flatness), then the
+// element's identity block-slot map (no transposition: block (e, p) holds rows
+// of local node a, columns of local node b, a <= b).  The error word itself
+// is cleared beforehand: it is the only scratch that must start at zero.
+__global__ void na_prepare_kernel(int64_t nq, int64_t n_nodes, const int32_t *__restrict__ nodes,
+                                  const double *__restrict__ prop, const double *__restrict__ coords, double *base) {
     NaView v = na_view(base);
-    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < nq * 4 && (nodes[t] < 0 || nodes[t] >= n_nodes)) atomicExch(v.err, 2);
-    if (t < nq * 10) v.slot[t] = (int32_t)t;
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nq) return;
+    int32_t bad = 0;
+    int32_t n[4];
+    for (int k = 0; k < 4; ++k) {
+        n[k] = nodes[4 * e + k];
+        if (n[k] < 0 || n[k] >= n_nodes) bad |= kNaInvalid;
+    }
+    for (int a = 0; a < 4; ++a)
+        for (int b = a + 1; b < 4; ++b)
+            if (n[a] == n[b]) bad |= kNaInvalid;
+    const double *pr = prop + JFG_SHELL_PROP * e;
+    if (!(pr[0] > 0.0) || !(pr[1] > 0.0)) bad |= kNaInvalid;
+    if (!(bad & kNaInvalid) &&
+        !q4_is_flat(coords + 3 * n[0], coords + 3 * n[1], coords + 3 * n[2], coords + 3 * n[3]))
+        bad |= kNaNotFlat;
+    if (bad) atomicOr(v.err, bad);
+    for (int q = 0; q < 10; ++q) v.slot[10 * e + q] = (int32_t)(10 * e + q);
 }
 
 // Node -> incident elements, in ascending element order (deterministic).
@@ -2099,7 +2108,7 @@ __global__ void na_incidence_kernel(int64_t n_nodes, int64_t nq, const int32_t *
         for (int k = 0; k < 4; ++k)
             if (nodes[4 * e + k] == A) {
                 if (cnt < JFG_NOALLOC_MAX_VALENCE) v.inc[A * JFG_NOALLOC_MAX_VALENCE + cnt] = (int32_t)e;
-                else atomicExch(v.err, 1);
+                else atomicOr(v.err, kNaValence);
                 ++cnt;
             }
     v.inc_cnt[A] = cnt < JFG_NOALLOC_MAX_VALENCE ? cnt : JFG_NOALLOC_MAX_VALENCE;
@@ -2156,11 +2165,14 @@ extern "C" jfg_status jfg_assemble_k_quad4_noalloc(int64_t n_nodes, const double
     NaView v = na_view(base);
     int32_t err = 0;
     if (cudaMemsetAsync(v.err, 0, sizeof(int32_t), s) != cudaSuccess) return JFG_ERR_CUDA;
-    na_prepare_kernel<<<(unsigned)cdiv(n_quad4 * 10, 256), 256, 0, s>>>(n_quad4, n_nodes, quad4_nodes_dev, base);
+    na_prepare_kernel<<<(unsigned)cdiv(n_quad4, 128), 128, 0, s>>>(n_quad4, n_nodes, quad4_nodes_dev, quad4_prop_dev,
+                                                                    coords_dev, base);
     if (cudaGetLastError() != cudaSuccess) return JFG_ERR_CUDA;
     if (cudaMemcpyAsync(&err, v.err, sizeof(int32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess) return JFG_ERR_CUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess) return JFG_ERR_CUDA;
-    if (err) return JFG_ERR_INVALID;  // a node index outside [0, n_nodes): nothing else was launched
+    // rejected input: nothing past the checks was launched
+    if (err & kNaInvalid) return JFG_ERR_INVALID;
+    if (err) return JFG_ERR_UNSUPPORTED;
     ElemOut o;
     o.staging = v.blocks;
     o.exc_raw = nullptr;       // every slot is a regular block
@@ -2176,7 +2188,7 @@ extern "C" jfg_status jfg_assemble_k_quad4_noalloc(int64_t n_nodes, const double
     if (cudaGetLastError() != cudaSuccess) return JFG_ERR_CUDA;
     if (cudaMemcpyAsync(&err, v.err, sizeof(int32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess) return JFG_ERR_CUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess) return JFG_ERR_CUDA;
-    return err ? JFG_ERR_UNSUPPORTED : JFG_OK;
+    return err ? JFG_ERR_UNSUPPORTED : JFG_OK;  // only the valence bit can be set here
 }
 
 // ---------------------------------------------------------------------------

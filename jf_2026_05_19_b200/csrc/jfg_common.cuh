@@ -30,6 +30,30 @@ JFG_HD void normalize3(const double *a, double *o) {
     o[0] = a[0] * r; o[1] = a[1] * r; o[2] = a[2] * r;
 }
 
+// Flatness predicate of the default CQUAD4 branch (assembly.jl:2824-2840):
+// the largest distance of a corner from the mean plane through the centroid
+// (normal d13 x d24) is below 1e-6 of the longer diagonal.  Host code
+// (model build) and device code (the allocation-free entry point) share it.
+JFG_HD bool q4_is_flat(const double *p1, const double *p2, const double *p3, const double *p4) {
+    double d13[3], d24[3], n[3];
+    sub3(p3, p1, d13);
+    sub3(p4, p2, d24);
+    cross3(d13, d24, n);
+    const double len = sqrt(dot3(n, n));
+    double maxdev = 0.0;
+    if (len > 1e-12) {
+        const double g[3] = {n[0] / len, n[1] / len, n[2] / len};
+        const double *ps[4] = {p1, p2, p3, p4};
+        for (int k = 0; k < 4; ++k) {
+            double d[3];
+            for (int i = 0; i < 3; ++i) d[i] = ps[k][i] - (p1[i] + p2[i] + p3[i] + p4[i]) / 4.0;
+            maxdev = fmax(maxdev, fabs(dot3(d, g)));
+        }
+    }
+    const double L = fmax(sqrt(dot3(d13, d13)), sqrt(dot3(d24, d24)));
+    return maxdev < 1e-6 * fmax(L, 1e-12);
+}
+
 // CQUAD4 element frame in the reference's default ":diag" mode
 // (shell_element_frame_quad4 / _with_normal, helpers.jl:1134-1193).
 JFG_HD void q4_frame(const double *p1, const double *p2, const double *p3, const double *p4,

@@ -846,43 +846,98 @@ std::map<int64_t, std::vector<std::pair<int64_t, double>>> rbe2_map(const jfg_mo
     return mp;
 }
 
-// triplet redistribution (constraints.jl:329-361) + sparse() to 1-based CSC
+// Triplet redistribution (constraints.jl:329-361) followed by
+// SparseArrays.sparse(I, J, V, n, n) to 1-based CSC.
+//
+// sparse() is restated from SparseArrays' published algorithm (sparse! in
+// SparseArrays 1.12): (1) a counting sort of the triplets into rows, keeping
+// input order inside each row; (2) per row, every repeated column is merged
+// into its first occurrence, summing left to right in input order (the
+// combine = + fold, explicit zeros kept); (3) the row-compressed result is
+// transposed into CSC, which leaves each column's rows ascending.  It is
+// O(triplets + n) and serial, like the reference's.  The redistribution is
+// applied on the fly in both counting passes, in the reference's emission
+// order (images of a dependent dof in the order of its constraint row), so
+// the redistributed triplet list is never materialised.
+//
+// abs_sums (optional) receives, per stored entry, the same fold over |v|:
+// the magnitude of the terms the entry sums, i.e. the scale of its
+// summation-order rounding.  Only the tests use it.
 void constrain_and_csc(const jfg_model_desc *d, Triplets &t, std::vector<int64_t> &colptr, std::vector<int64_t> &rowval,
-                       std::vector<double> &nzval) {
+                       std::vector<double> &nzval, std::vector<double> *abs_sums = nullptr) {
     auto mp = rbe2_map(d);
-    int64_t ndof = 6 * d->n_nodes;
+    const int64_t ndof = 6 * d->n_nodes;
     std::vector<const std::vector<std::pair<int64_t, double>> *> dep(ndof, nullptr);
     for (auto &kv : mp) dep[kv.first] = &kv.second;
-    std::vector<std::pair<uint64_t, double>> kv;
-    kv.reserve(t.V.size() + t.V.size() / 10);
-    auto key = [&](int64_t i, int64_t j) { return (uint64_t)j * (uint64_t)ndof + (uint64_t)i; };
-    for (size_t k = 0; k < t.V.size(); ++k) {
-        int64_t i = t.I[k], j = t.J[k];
-        double v = t.V[k];
+    const size_t n_in = t.V.size();
+    // f(i, j, v) for every triplet that input k becomes, in emission order
+    auto emit = [&](size_t k, auto &&f) {
+        const int64_t i = t.I[k], j = t.J[k];
+        const double v = t.V[k];
         const auto *di = dep[i], *dj = dep[j];
-        if (!di && !dj) kv.push_back({key(i, j), v});
-        else if (di && !dj) { for (auto &p : *di) kv.push_back({key(p.first, j), v * p.second}); }
-        else if (!di && dj) { for (auto &p : *dj) kv.push_back({key(i, p.first), v * p.second}); }
+        if (!di && !dj) f(i, j, v);
+        else if (di && !dj) { for (auto &p : *di) f(p.first, j, v * p.second); }
+        else if (!di && dj) { for (auto &p : *dj) f(i, p.first, v * p.second); }
         else {
             for (auto &a : *di)
-                for (auto &b : *dj) kv.push_back({key(a.first, b.first), v * a.second * b.second});
+                for (auto &b : *dj) f(a.first, b.first, v * a.second * b.second);
+        }
+    };
+    // (1) counting sort into rows
+    std::vector<int64_t> row_at(ndof + 1, 0);
+    for (size_t k = 0; k < n_in; ++k) emit(k, [&](int64_t i, int64_t, double) { ++row_at[i + 1]; });
+    for (int64_t i = 0; i < ndof; ++i) row_at[i + 1] += row_at[i];
+    const int64_t n_trip = row_at[ndof];
+    std::vector<int32_t> ccol(n_trip);
+    std::vector<double> cval(n_trip), cabs(abs_sums ? n_trip : 0);
+    {
+        std::vector<int64_t> fill(row_at.begin(), row_at.end() - 1);
+        for (size_t k = 0; k < n_in; ++k)
+            emit(k, [&](int64_t i, int64_t j, double v) {
+                const int64_t q = fill[i]++;
+                ccol[q] = (int32_t)j;
+                cval[q] = v;
+                if (abs_sums) cabs[q] = std::fabs(v);
+            });
+    }
+    // (2) merge repeated columns per row into their first occurrence, in order
+    std::vector<int64_t> last(ndof, -1), crow(ndof + 1, 0);
+    int64_t w = 0;
+    for (int64_t i = 0; i < ndof; ++i) {
+        crow[i] = w;
+        for (int64_t q = row_at[i]; q < row_at[i + 1]; ++q) {
+            const int32_t j = ccol[q];
+            if (last[j] < crow[i]) {
+                last[j] = w;
+                ccol[w] = j;
+                cval[w] = cval[q];
+                if (abs_sums) cabs[w] = cabs[q];
+                ++w;
+            } else {
+                cval[last[j]] += cval[q];
+                if (abs_sums) cabs[last[j]] += cabs[q];
+            }
         }
     }
-    std::stable_sort(kv.begin(), kv.end(), [](const std::pair<uint64_t, double> &a, const std::pair<uint64_t, double> &b) { return a.first < b.first; });
+    crow[ndof] = w;
+    // (3) transpose to CSC (rows ascending within each column), 1-based
     colptr.assign(ndof + 1, 0);
-    rowval.clear(); nzval.clear();
-    size_t k = 0;
-    while (k < kv.size()) {
-        uint64_t kk = kv[k].first;
-        double s = 0.0;
-        while (k < kv.size() && kv[k].first == kk) { s += kv[k].second; ++k; }
-        int64_t col = (int64_t)(kk / ndof), row = (int64_t)(kk % ndof);
-        rowval.push_back(row + 1);
-        nzval.push_back(s);
-        colptr[col + 1] += 1;
-    }
-    colptr[0] = 1;
+    for (int64_t q = 0; q < w; ++q) ++colptr[ccol[q] + 1];
     for (int64_t c = 0; c < ndof; ++c) colptr[c + 1] += colptr[c];
+    rowval.assign(w, 0);
+    nzval.assign(w, 0.0);
+    if (abs_sums) abs_sums->assign(w, 0.0);
+    {
+        std::vector<int64_t> next(colptr.begin(), colptr.end() - 1);
+        for (int64_t i = 0; i < ndof; ++i)
+            for (int64_t q = crow[i]; q < crow[i + 1]; ++q) {
+                const int64_t r = next[ccol[q]]++;
+                rowval[r] = i + 1;
+                nzval[r] = cval[q];
+                if (abs_sums) (*abs_sums)[r] = cabs[q];
+            }
+    }
+    for (auto &c : colptr) c += 1;
 }
 
 }  // namespace
@@ -1525,10 +1580,21 @@ void bar_recover(const jfg_model_desc *d, int64_t e, const double *u, const doub
 
 struct OracleCSC {
     std::vector<int64_t> colptr, rowval;
-    std::vector<double> nzval, orig_diag;
+    std::vector<double> nzval, orig_diag, abs_sums;
     double max_elem_stiff = 0.0;
+    double t_elements = 0.0, t_sparse = 0.0;  // seconds: element loops; redistribution + sparse()
     std::string err;
 };
+
+bool g_abs_sums = false;  // also compute per-entry sums of |term| (tests only)
+
+double now_s() {
+#ifdef _OPENMP
+    return omp_get_wtime();
+#else
+    return 0.0;
+#endif
+}
 
 // Element triplets of KG before constraints (assembly.jl:4382-6634), element
 // order quads (576 each), trias (324 each), bars (144 each, zero-length bars
@@ -1872,6 +1938,7 @@ int oracle_assemble_k(const jfg_model_desc *d, void **handle) {
     *handle = out;
     int st = check_predicates(d, out->err);
     if (st) return st;
+    const double t0 = now_s();
     int64_t nq = d->n_quad4, nt = d->n_tria3, nb = d->n_bar;
     Triplets t;
     size_t total = (size_t)nq * 576 + (size_t)nt * 324 + (size_t)nb * 144;
@@ -1998,7 +2065,10 @@ int oracle_assemble_k(const jfg_model_desc *d, void **handle) {
     out->orig_diag.assign(6 * d->n_nodes, 0.0);
     for (size_t k = 0; k < t.V.size(); ++k)
         if (t.I[k] == t.J[k]) out->orig_diag[t.I[k]] += t.V[k];
-    constrain_and_csc(d, t, out->colptr, out->rowval, out->nzval);
+    const double t1 = now_s();
+    constrain_and_csc(d, t, out->colptr, out->rowval, out->nzval, g_abs_sums ? &out->abs_sums : nullptr);
+    out->t_elements = t1 - t0;
+    out->t_sparse = now_s() - t1;
     return 0;
 }
 
@@ -2007,9 +2077,13 @@ int oracle_assemble_kg(const jfg_model_desc *d, const double *u, void **handle) 
     auto *out = new OracleCSC();
     *handle = out;
     Triplets t;
+    const double t0 = now_s();
     int st = kg_element_triplets(d, u, t, out->err);
     if (st) return st;
-    constrain_and_csc(d, t, out->colptr, out->rowval, out->nzval);
+    const double t1 = now_s();
+    constrain_and_csc(d, t, out->colptr, out->rowval, out->nzval, g_abs_sums ? &out->abs_sums : nullptr);
+    out->t_elements = t1 - t0;
+    out->t_sparse = now_s() - t1;
     return 0;
 }
 
@@ -2050,6 +2124,19 @@ void oracle_fetch(void *h, int64_t *colptr, int64_t *rowval, double *nzval, doub
     if (orig_diag && !o->orig_diag.empty()) std::memcpy(orig_diag, o->orig_diag.data(), sizeof(double) * o->orig_diag.size());
 }
 void oracle_free(void *h) { delete (OracleCSC *)h; }
+// Per-entry sums of |term| of the next assemblies (tests only; 0 = off).
+void oracle_set_abs_sums(int on) { g_abs_sums = on != 0; }
+int oracle_fetch_abs_sums(void *h, double *out) {
+    auto *o = (OracleCSC *)h;
+    if (o->abs_sums.size() != o->nzval.size()) return 1;
+    std::memcpy(out, o->abs_sums.data(), sizeof(double) * o->abs_sums.size());
+    return 0;
+}
+// Seconds spent in the element loops and in redistribution + sparse().
+void oracle_phase_seconds(void *h, double *out2) {
+    out2[0] = ((OracleCSC *)h)->t_elements;
+    out2[1] = ((OracleCSC *)h)->t_sparse;
+}
 
 // rbe3_map as returned by assemble_stiffness (constraints.jl:319-322), 1-based
 int64_t oracle_constraint_map(const jfg_model_desc *d, int64_t *dep, int64_t *ptr, int64_t *ind, double *coef) {

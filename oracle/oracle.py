@@ -57,6 +57,10 @@ def lib():
         L.oracle_recover.argtypes = [C.POINTER(JfgModelDesc), pd, pd, C.c_int32, pd, pd]
         L.oracle_kg_contract.argtypes = [C.POINTER(JfgModelDesc), pd, pd, pd, pd, pd]
         L.oracle_kg_contract.restype = C.c_int
+        L.oracle_set_abs_sums.argtypes = [C.c_int]
+        L.oracle_fetch_abs_sums.argtypes = [C.c_void_p, pd]
+        L.oracle_fetch_abs_sums.restype = C.c_int
+        L.oracle_phase_seconds.argtypes = [C.c_void_p, pd]
         _lib = L
     return _lib
 
@@ -78,33 +82,62 @@ def _fetch(h, with_diag):
     return colptr, rowval, nzval, diag
 
 
-def assemble_k(m: ModelArrays):
-    """Returns (colptr, rowval, nzval, max_elem_stiff, orig_diag), 1-based CSC."""
+def _detail(h, nnz, abs_sums):
+    """Phase seconds and, when asked for, the per-entry sums of |term|."""
+    L = lib()
+    t = np.zeros(2)
+    L.oracle_phase_seconds(h, t.ctypes.data_as(C.POINTER(C.c_double)))
+    out = {"t_elements": float(t[0]), "t_sparse": float(t[1])}
+    if abs_sums:
+        a = np.empty(nnz)
+        if L.oracle_fetch_abs_sums(h, a.ctypes.data_as(C.POINTER(C.c_double))):
+            raise RuntimeError("oracle abs sums were not computed")
+        out["abs_sums"] = a
+    return out
+
+
+def assemble_k(m: ModelArrays, detail: bool = False, abs_sums: bool = False):
+    """Returns (colptr, rowval, nzval, max_elem_stiff, orig_diag), 1-based CSC.
+
+    With detail=True a sixth item is a dict with the phase times (element
+    loops, redistribution + sparse) and, with abs_sums=True, the per-entry
+    sums of |term| (the scale of each entry's summation rounding)."""
     L = lib()
     d, keep = make_desc(m)
     h = C.c_void_p()
-    st = L.oracle_assemble_k(C.byref(d), C.byref(h))
+    L.oracle_set_abs_sums(int(abs_sums))
+    try:
+        st = L.oracle_assemble_k(C.byref(d), C.byref(h))
+    finally:
+        L.oracle_set_abs_sums(0)
     try:
         if st != 0:
             raise OracleError(st, L.oracle_error(h).decode())
         colptr, rowval, nzval, diag = _fetch(h, True)
-        return colptr, rowval, nzval, L.oracle_max_elem_stiff(h), diag
+        res = (colptr, rowval, nzval, L.oracle_max_elem_stiff(h), diag)
+        return res + (_detail(h, len(nzval), abs_sums),) if detail else res
     finally:
         L.oracle_free(h)
         del keep
 
 
-def assemble_kg(m: ModelArrays, u: np.ndarray):
+def assemble_kg(m: ModelArrays, u: np.ndarray, detail: bool = False, abs_sums: bool = False):
+    """Returns (colptr, rowval, nzval); a fourth item as in assemble_k with detail=True."""
     L = lib()
     d, keep = make_desc(m)
     u = np.ascontiguousarray(u, np.float64)
     h = C.c_void_p()
-    st = L.oracle_assemble_kg(C.byref(d), u.ctypes.data_as(C.POINTER(C.c_double)), C.byref(h))
+    L.oracle_set_abs_sums(int(abs_sums))
+    try:
+        st = L.oracle_assemble_kg(C.byref(d), u.ctypes.data_as(C.POINTER(C.c_double)), C.byref(h))
+    finally:
+        L.oracle_set_abs_sums(0)
     try:
         if st != 0:
             raise OracleError(st, L.oracle_error(h).decode())
         colptr, rowval, nzval, _ = _fetch(h, False)
-        return colptr, rowval, nzval
+        res = (colptr, rowval, nzval)
+        return res + (_detail(h, len(nzval), abs_sums),) if detail else res
     finally:
         L.oracle_free(h)
         del keep

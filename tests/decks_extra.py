@@ -97,3 +97,26 @@ def plate_axis_rbe2(n=6, size=120.0, cm="123"):
     return dataclasses.replace(p, rbe2_master=np.array([idx(2, j)], np.int32), rbe2_cm=np.array([D.cm_mask(cm)], np.int32),
                                rbe2_slave_ptr=np.array([0, 1], np.int64), rbe2_slaves=np.array([idx(n - 1, j)], np.int32),
                                name="plate_axis_rbe2")
+
+
+def without_shells(m):
+    """The deck's line elements and constraints only (shells removed)."""
+    return dataclasses.replace(m, q4_nodes=np.zeros((0, 4), np.int32), q4_prop=np.zeros((0, D.N_SHELL_PROP)),
+                               t3_nodes=np.zeros((0, 3), np.int32), t3_prop=np.zeros((0, D.N_SHELL_PROP)),
+                               name=m.name + "_bars_only")
+
+
+def bars_only_barrel():
+    """The 72 x 24 barrel with its shells removed: CBEAM rings, CBAR longerons
+    and the RBE2 end ring, whose centre node's rows sum terms up to ~3e4 times
+    their row max."""
+    return without_shells(D.barrel_small(seed=2, n_circ=72, n_axial=24))
+
+
+def single_quad4():
+    return D.plate_c1(n=1)
+
+
+def single_cell_tria3():
+    """One quad cell split into two CTRIA3 (plus the plane's bars and RBE2)."""
+    return skewed_plane(seed=8, nx=1, ny=1, tri_frac=1.0)

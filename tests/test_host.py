@@ -39,3 +39,15 @@ def test_barrel_generator_counts():
     c = m.counts()
     assert c["quad4"] + c["tria3"] // 2 == 72 * 24
     assert c["rbe2_slaves"] == 72
+
+
+def test_build_hash_covers_every_included_file():
+    """The stale-library guard hashes every file the library is compiled from:
+    each csrc header and the public header are reached through #include."""
+    import glob
+    import os
+    from jf_2026_05_19_b200 import build
+    d = set(build.deps())
+    for p in glob.glob(os.path.join(build.CSRC, "*.cuh")) + glob.glob(os.path.join(build.CSRC, "*.cu")):
+        assert os.path.normpath(p) in d, p
+    assert os.path.join(build.ROOT, "include", "jfem_gpu.h") in d

@@ -122,3 +122,52 @@ def test_unsupported_branches_are_refused():
         O.assemble_k(dataclasses.replace(m, bar_pin=pin))
     with pytest.raises(O.OracleError):
         O.assemble_k(dataclasses.replace(m, param_snorm=20.0))
+
+
+def _bars_only_barrel():
+    import dataclasses
+    m = decks.barrel_small(seed=2, n_circ=72, n_axial=24)
+    return dataclasses.replace(m, q4_nodes=np.zeros((0, 4), np.int32), q4_prop=np.zeros((0, decks.N_SHELL_PROP)),
+                               t3_nodes=np.zeros((0, 3), np.int32), t3_prop=np.zeros((0, decks.N_SHELL_PROP)))
+
+
+def _reordered(m, seed):
+    import dataclasses
+    r = np.random.default_rng(seed)
+    pq, pt, pb = (r.permutation(a.shape[0]) for a in (m.q4_nodes, m.t3_nodes, m.bar_nodes))
+    return dataclasses.replace(m, q4_nodes=m.q4_nodes[pq], q4_prop=m.q4_prop[pq], t3_nodes=m.t3_nodes[pt],
+                               t3_prop=m.t3_prop[pt], bar_nodes=m.bar_nodes[pb], bar_prop=m.bar_prop[pb],
+                               bar_pin=m.bar_pin[pb])
+
+
+def test_element_order_rounding_sets_the_parity_bound():
+    """The reference sums each matrix entry in its element Dict order, which is
+    arbitrary.  On the bars-only barrel the RBE2 centre node's rows sum terms up
+    to ~3e4 times their row max, so reordering the elements moves the oracle's
+    own K past 1e-12 of the row max -- the bound cannot hold there for any
+    implementation -- while every entry stays within SUM_TOL * eps * sum|terms|."""
+    from helpers import EPS, SUM_TOL, parity_ratio
+    m = _bars_only_barrel()
+    cp, rv, nz, _, _, det = O.assemble_k(m, detail=True, abs_sums=True)
+    u = decks.smooth_displacement(m, seed=7)
+    _, _, kg, detg = O.assemble_kg(m, u, detail=True, abs_sums=True)
+    worst_row = 0.0
+    for seed in range(3):
+        mp = _reordered(m, seed)
+        cp2, rv2, nz2, _, _ = O.assemble_k(mp)
+        _, _, kg2 = O.assemble_kg(mp, u)
+        assert np.array_equal(cp, cp2) and np.array_equal(rv, rv2)
+        worst_row = max(worst_row, rowmax_rel_err(cp, nz, nz2))
+        assert np.abs(nz2 - nz).max() > 0.0
+        assert parity_ratio(cp, nz, nz2, det["abs_sums"]) <= 1.0
+        assert parity_ratio(cp, kg, kg2, detg["abs_sums"]) <= 1.0
+        assert np.all(np.abs(nz2 - nz) <= SUM_TOL * EPS * det["abs_sums"])
+    assert worst_row > ROW_TOL
+
+
+def test_abs_sums_bound_the_values():
+    m = decks.barrel_small(seed=2, n_circ=24, n_axial=12)
+    cp, rv, nz, _, _, det = O.assemble_k(m, detail=True, abs_sums=True)
+    a = det["abs_sums"]
+    assert a.shape == nz.shape and np.all(a >= np.abs(nz) * (1 - 1e-15))
+    assert det["t_elements"] >= 0.0 and det["t_sparse"] >= 0.0
