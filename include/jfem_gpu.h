@@ -371,6 +371,26 @@ jfg_status jfg_server_hold(jfg_server *s, int32_t hold);
 const char *jfg_server_last_error(jfg_server *s);
 void jfg_server_destroy(jfg_server *s);
 
+/* ---- Group handles: several models in one launch ------------------------
+ * The reference assembles one model per call; its batch drivers loop over
+ * models and design variants (tools/manifest_batch_core.jl:283-409,
+ * src/solver/optimize_thickness.jl:209-240).  A group handle holds several
+ * decks side by side as disjoint components: every element-kernel and
+ * reduction launch takes bins from all members, of uneven sizes and mixed
+ * element types, and jfg_assemble_batch_device runs design variants of every
+ * member in the same launches (one CUDA graph when captured).  The handle is a
+ * jfg_model: every entry point above works on it and jfg_model_destroy frees
+ * it.  Members must share PARAM K6ROT; each is validated against its own
+ * index ranges.  A member's dofs are [6 node_off, 6 (node_off + n_nodes)),
+ * its CSC columns the same range and its nonzeros [nnz_off, nnz_off + nnz);
+ * rows there are the member's own rows offset by 6 node_off.  Its values are
+ * bit for bit those of the member on its own handle.  max_elem_stiff is the
+ * group's (the max over members). */
+jfg_status jfg_group_create(int32_t n, const jfg_model_desc *const *descs, jfg_model **out);
+/* out8: n_nodes, node_off, nnz, nnz_off, CQUAD4 offset, CTRIA3 offset, bar
+ * offset, element count of member i. */
+jfg_status jfg_group_member(jfg_model *m, int32_t i, int64_t *out8);
+
 /* ---- Allocation-free CQUAD4 stiffness assembly ---------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory where they need a stiffness matrix: a host framework that has

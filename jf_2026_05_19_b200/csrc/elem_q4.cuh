@@ -129,14 +129,19 @@ struct Q4Pts {
 // condensations K_ab K_bb^-1 K_ab' are then c A B^-1 A' with the one 4x4
 // symmetric positive definite B.
 struct __align__(16) Q4KShared {
-    Q4Pts g;
-    double Dd[4][4];            // MacNeal sampling rows: dN_k/dx (rows 0, 1), dN_k/dy (rows 2, 3)
-    double ivd[4];              // 1 / (sqrt(2 Jp)^2 cs) per sampling point
-    double W[6];                // Zx^-1 (w00, w01, w11), Zy^-1 (w22, w23, w33)
-    double Am[8][4], Ab[8][4];  // rows: (node, component) of the membrane / bending B
-    double B[10];               // packed upper triangle
-    double Xm[4][8], Xb[4][8];  // B^-1 Am', B^-1 Ab'
-    int32_t slot[10];           // node-pair slots, for the warp's copy of the staged blocks
+    union {
+        struct {
+            Q4Pts g;
+            double Dd[4][4];            // MacNeal sampling rows: dN_k/dx (rows 0, 1), dN_k/dy (rows 2, 3)
+            double ivd[4];              // 1 / (sqrt(2 Jp)^2 cs) per sampling point
+            double W[6];                // Zx^-1 (w00, w01, w11), Zy^-1 (w22, w23, w33)
+            double Am[8][4], Ab[8][4];  // rows: (node, component) of the membrane / bending B
+            double B[10];               // packed upper triangle
+            double Xm[4][8], Xb[4][8];  // B^-1 Am', B^-1 Ab'
+        };
+        double blk[10][36];             // write phase: the element's rotated pair blocks, stored orientation
+    };
+    int32_t slot[10];                   // node-pair slots, for the warp's copy of the staged blocks
 };
 
 // KG kernel state of one element (membrane incompatible modes only; the
@@ -397,17 +402,21 @@ __device__ __forceinline__ void bend_pair(const double (*dNx)[4], const double (
     P[2][2] += cb * (Pxx + gam * T11);
 }
 
-__global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const int32_t *__restrict__ nodes,
+// W warps per CTA (3 W elements): 4 or 8.  The element records are dynamic
+// shared memory, Q4_TEAMS_PER_WARP * W * sizeof(Q4KShared) bytes.
+template <int W>
+__global__ void __launch_bounds__(32 * W, 16 / W) q4_k_kernel(int64_t nq, const int32_t *__restrict__ nodes,
                                                          const double *__restrict__ prop,
                                                          const double *__restrict__ coords,
                                                          const double *__restrict__ nodeR, double k6rot, ElemOut o) {
-    __shared__ Q4KShared sh[Q4_ELEMS_PER_BLOCK];
+    extern __shared__ __align__(16) unsigned char q4_smem[];
+    Q4KShared *sh = reinterpret_cast<Q4KShared *>(q4_smem);
     o = o.at(blockIdx.y);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int team = lane / Q4_TEAM, tl = lane - team * Q4_TEAM;
     const bool in_team = team < Q4_TEAMS_PER_WARP;
     const int slot_id = warp * Q4_TEAMS_PER_WARP + (in_team ? team : 0);
-    const int64_t e = (int64_t)blockIdx.x * Q4_ELEMS_PER_BLOCK + slot_id;
+    const int64_t e = (int64_t)blockIdx.x * Q4_TEAMS_PER_WARP * W + slot_id;
     const bool valid = in_team && e < nq;
     Q4KShared &S = sh[slot_id];
 
@@ -605,21 +614,18 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
             for (int i = 0; i < 9; ++i) { Qa[i] = V[i]; Qb[i] = V[i]; }
         }
         sl = __ldg(o.blk_slot + e * 10 + tl);
-        S.slot[tl] = sl;
     }
     // Phase 5: T'KT and the writes.  The block of a pair is stored with
     // rows of the lower-numbered global node (transposed when the slot says
-    // so).  Each half (stored rows 0-2, then 3-5) is rotated by sub-blocks,
-    // staged in the element's shared record -- no lane reads it any more --
-    // and copied out by the whole warp as 16-byte stores, 9 per half-slot,
-    // so a slot is written as whole contiguous lines instead of 36 scattered
+    // so).  Each half (stored rows 0-2, then 3-5) is rotated by sub-blocks
+    // and staged in the element's shared record -- no lane reads the phase
+    // data any more -- which then holds the element's ten 6x6 blocks.  The
+    // warp copies the staged slots out as 16-byte stores, 18 per slot, so a
+    // slot is written as whole contiguous lines instead of 36 scattered
     // 8-byte stores.  Pairs on the RBE2 path are written directly.
     __syncwarp();
     const bool t = valid && sl >= 0 && (sl & kBlkTranspose);
-    double *buf = reinterpret_cast<double *>(&S) + 18 * tl;
-    const int64_t e_warp = (int64_t)blockIdx.x * Q4_ELEMS_PER_BLOCK + warp * Q4_TEAMS_PER_WARP;
-    const int64_t n_left = nq - e_warp;
-    const int nv = n_left <= 0 ? 0 : (n_left >= Q4_TEAMS_PER_WARP ? Q4_TEAMS_PER_WARP : (int)n_left);
+    double *buf = S.blk[valid ? tl : 0];
 #pragma unroll
     for (int half = 0; half < 2; ++half) {
         if (valid) {
@@ -643,14 +649,15 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
                 write_sub_block(o, e, sl, a, b, half, 0, Of, lmax, 24);
                 write_sub_block(o, e, sl, a, b, half, 1, Os, lmax, 24);
             } else {
+                double *hb = buf + 18 * half;
 #pragma unroll
                 for (int r = 0; r < 3; ++r)
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
                         const double vf = t ? Of[c][r] : Of[r][c], vs = t ? Os[c][r] : Os[r][c];
                         lmax = fmax(lmax, fmax(fabs(vf), fabs(vs)));
-                        buf[6 * r + c] = vf;
-                        buf[6 * r + 3 + c] = vs;
+                        hb[6 * r + c] = vf;
+                        hb[6 * r + 3 + c] = vs;
                     }
                 if (o.diag_staging && a == b) {
                     // diagonal pair (never transposed): TT in the first, RR in the second column band
@@ -660,22 +667,27 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
                 }
             }
         }
-        __syncwarp();
-        // chunk ch = 90 team + 9 pair + part; lanes step by 32 = 3 pairs + 5 parts.
-        // The warp's valid teams are a prefix (elements are consecutive).
-        for (int tm = 0, pl = lane / 9, part = lane % 9; tm < nv;) {
+    }
+    if (valid) S.slot[tl] = sl;  // the copy below skips negative (RBE2 path) slots
+    __syncwarp();
+    // chunk ch = 180 team + 18 pair + part; lanes step by 32 = 1 pair + 14 parts.
+    // The warp's valid teams are a prefix (elements are consecutive).
+    {
+        const int64_t p_warp = (int64_t)blockIdx.x * Q4_TEAMS_PER_WARP * W + warp * Q4_TEAMS_PER_WARP;
+        const int64_t n_left = nq - p_warp;
+        const int nv = n_left <= 0 ? 0 : (n_left >= Q4_TEAMS_PER_WARP ? Q4_TEAMS_PER_WARP : (int)n_left);
+        for (int tm = 0, pl = lane / 18, part = lane % 18; tm < nv;) {
             const Q4KShared &R = sh[warp * Q4_TEAMS_PER_WARP + tm];
             const int32_t st = R.slot[pl];
             if (st >= 0) {
-                const double2 v2 = reinterpret_cast<const double2 *>(reinterpret_cast<const double *>(&R) + 18 * pl)[part];
-                reinterpret_cast<double2 *>(o.staging + 36 * (int64_t)(st & kBlkIndexMask) + 18 * half)[part] = v2;
+                const double2 v2 = reinterpret_cast<const double2 *>(R.blk[pl])[part];
+                reinterpret_cast<double2 *>(o.staging + 36 * (int64_t)(st & kBlkIndexMask))[part] = v2;
             }
-            part += 5;
-            pl += 3;
-            if (part >= 9) { part -= 9; ++pl; }
+            part += 14;
+            pl += 1;
+            if (part >= 18) { part -= 18; ++pl; }
             if (pl >= 10) { pl -= 10; ++tm; }
         }
-        __syncwarp();
     }
     if (o.maxabs) {
         for (int off = 16; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
@@ -683,19 +695,22 @@ __global__ void __launch_bounds__(Q4_THREADS, 4) q4_k_kernel(int64_t nq, const i
     }
 }
 
-__global__ void __launch_bounds__(Q4_THREADS) q4_kg_kernel(int64_t nq, const int32_t *__restrict__ nodes,
+// W warps per CTA (3 W elements): 4 or 8; dynamic shared memory as q4_k_kernel's.
+template <int W>
+__global__ void __launch_bounds__(32 * W) q4_kg_kernel(int64_t nq, const int32_t *__restrict__ nodes,
                                                           const double *__restrict__ prop,
                                                           const double *__restrict__ coords,
                                                           const double *__restrict__ nodeR,
                                                           const double *__restrict__ u, ElemOut o) {
-    __shared__ Q4GShared sh[Q4_ELEMS_PER_BLOCK];
+    extern __shared__ __align__(16) unsigned char q4_smem[];
+    Q4GShared *sh = reinterpret_cast<Q4GShared *>(q4_smem);
     o = o.at(blockIdx.y);
     u += (int64_t)blockIdx.y * o.u_stride;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int team = lane / Q4_TEAM, tl = lane - team * Q4_TEAM;
     const bool in_team = team < Q4_TEAMS_PER_WARP;
     const int slot_id = warp * Q4_TEAMS_PER_WARP + (in_team ? team : 0);
-    const int64_t e = (int64_t)blockIdx.x * Q4_ELEMS_PER_BLOCK + slot_id;
+    const int64_t e = (int64_t)blockIdx.x * Q4_TEAMS_PER_WARP * W + slot_id;
     const bool valid = in_team && e < nq;
     Q4GShared &S = sh[slot_id];
 
@@ -942,8 +957,8 @@ __global__ void __launch_bounds__(Q4_THREADS) q4_kg_kernel(int64_t nq, const int
     }
     __syncwarp();
     // chunk ch = 60 team + 6 pair + part; lanes step by 32 = 5 pairs + 2 parts
-    const int64_t e_warp = (int64_t)blockIdx.x * Q4_ELEMS_PER_BLOCK + warp * Q4_TEAMS_PER_WARP;
-    const int64_t n_left = nq - e_warp;
+    const int64_t p_warp = (int64_t)blockIdx.x * Q4_TEAMS_PER_WARP * W + warp * Q4_TEAMS_PER_WARP;
+    const int64_t n_left = nq - p_warp;
     const int nv = n_left <= 0 ? 0 : (n_left >= Q4_TEAMS_PER_WARP ? Q4_TEAMS_PER_WARP : (int)n_left);
     for (int tm = 0, pl = lane / 6, part = lane % 6; tm < nv;) {
         const Q4GShared &R = sh[warp * Q4_TEAMS_PER_WARP + tm];

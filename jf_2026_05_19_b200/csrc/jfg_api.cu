@@ -20,12 +20,17 @@
 // their weighted independent images with |coeff| > 1e-15
 // (constraints.jl:25-34), and zero-length bars contribute nothing.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
+#include <condition_variable>
+#include <cstdlib>
+#include <memory>
 #include <cstring>
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cub/cub.cuh>
@@ -50,6 +55,68 @@ struct DevBuf {
 };
 
 }  // namespace
+
+// Host threads that split a memcpy between them and the calling thread.  One
+// job at a time; the caller waits until every part is done.
+class CopyPool {
+  public:
+    explicit CopyPool(int workers) {
+        for (int i = 0; i < workers; ++i) th_.emplace_back([this, i] { run(i); });
+    }
+    ~CopyPool() {
+        {
+            std::lock_guard<std::mutex> l(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto &t : th_) t.join();
+    }
+    void copy(void *dst, const void *src, size_t len) {
+        {
+            std::lock_guard<std::mutex> l(mu_);
+            dst_ = static_cast<char *>(dst);
+            src_ = static_cast<const char *>(src);
+            len_ = len;
+            pending_ = (int)th_.size();
+            ++gen_;
+        }
+        cv_.notify_all();
+        part((int)th_.size());  // the caller takes the last part
+        std::unique_lock<std::mutex> l(mu_);
+        done_.wait(l, [this] { return pending_ == 0; });
+    }
+
+  private:
+    void part(int i) {
+        const size_t n = th_.size() + 1;
+        const size_t step = (len_ / n + 63) / 64 * 64;
+        const size_t a = std::min(len_, step * i), b = i + 1 == (int)n ? len_ : std::min(len_, step * (i + 1));
+        if (b > a) std::memcpy(dst_ + a, src_ + a, b - a);
+    }
+    void run(int i) {
+        uint64_t seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> l(mu_);
+                cv_.wait(l, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+            }
+            part(i);
+            std::lock_guard<std::mutex> l(mu_);
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+    std::vector<std::thread> th_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_;
+    char *dst_ = nullptr;
+    const char *src_ = nullptr;
+    size_t len_ = 0;
+    int pending_ = 0;
+    uint64_t gen_ = 0;
+    bool stop_ = false;
+};
 
 struct jfg_model {
     std::string err;
@@ -78,6 +145,7 @@ struct jfg_model {
     int64_t *d_blk_pa = nullptr, *d_blk_pb = nullptr;
     int2 *d_blk_len = nullptr;
     bool blk_even = false;
+    int q4_warps = 4;                    // warps per CQUAD4 CTA (3 elements each): 4 or 8
     int64_t staging_len = 0;            // staging doubles per assembly: max(K 36 per slot, KG 12 per slot + 27 per bar pair)
     double *d_staging = nullptr;        // 36 doubles per regular element pair
     int64_t *d_rowptr = nullptr, *d_colind = nullptr;   // 0-based symmetric CSR == CSC
@@ -132,6 +200,15 @@ struct jfg_model {
     double acc_ms[3][6] = {{0, 0, 0, 0, 0, 0}, {0, 0, 0, 0, 0, 0}, {0, 0, 0, 0, 0, 0}};  // K, KG, KG contractions
     int64_t acc_calls[3] = {0, 0, 0};
     std::vector<void *> allocs;
+    // group handles (jfg_group_create): per member n_nodes, node offset, nnz,
+    // nnz offset, CQUAD4 / CTRIA3 / bar offsets, element count
+    std::vector<std::array<int64_t, 8>> members;
+    // device -> pageable host copies: a ring of pinned chunks and host copy threads (made at first use)
+    static constexpr int kPinChunks = 4;
+    static constexpr size_t kPinChunkBytes = size_t(32) << 20;
+    char *pin = nullptr;
+    cudaEvent_t pin_ev[kPinChunks] = {nullptr, nullptr, nullptr, nullptr};
+    std::unique_ptr<CopyPool> copy_pool;
 };
 
 namespace {
@@ -757,6 +834,20 @@ cudaError_t exclusive_sum(jfg_model *m, T *in, U *out, int64_t n) {
     return e;
 }
 
+// The CQUAD4 kernels keep their element records in dynamic shared memory;
+// the 8-warp forms need more than the default 48 KB.
+cudaError_t set_q4_smem_limits() {
+    cudaError_t e = cudaFuncSetAttribute(q4_k_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(Q4_TEAMS_PER_WARP * 8 * sizeof(Q4KShared)));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(q4_kg_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(Q4_TEAMS_PER_WARP * 8 * sizeof(Q4GShared)));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(q4_kg_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(Q4_TEAMS_PER_WARP * 4 * sizeof(Q4GShared)));
+    return e;
+}
+
 jfg_status validate(jfg_model *m, const jfg_model_desc *d) {
     if (!d) return fail(m, JFG_ERR_INVALID, "null descriptor");
     if (d->n_nodes <= 0 || !d->coords) return fail(m, JFG_ERR_INVALID, "model has no nodes (is this a standalone deck?)");
@@ -832,7 +923,10 @@ void jfg_model_destroy(jfg_model *m) {
         cudaStreamSynchronize(m->own);
         cudaStreamDestroy(m->own);
     }
-    delete m;
+    if (m->pin) cudaFreeHost(m->pin);
+    for (auto &e : m->pin_ev)
+        if (e) cudaEventDestroy(e);
+    delete m;  // joins the copy threads
 }
 
 jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
@@ -843,6 +937,7 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
     jfg_status st = validate(m, d);
     if (st) return st;
     CK(cudaGetDevice(&m->device));
+    CK(set_q4_smem_limits());
     CK(cudaStreamCreateWithFlags(&m->own, cudaStreamNonBlocking));
     m->stream = m->own;
     m->own_stream = true;
@@ -1325,6 +1420,108 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
     return JFG_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Group handles: several decks as one handle, their meshes side by side as
+// disjoint components (node, element and RBE2 indices offset member by
+// member).  Every element-kernel and reduction launch then takes bins from
+// every member, whatever their sizes and element mixes, and the batched
+// variant call (jfg_assemble_batch_device) runs variants of all members in
+// the same launches.  A member's dofs, CSC columns and nonzeros are one
+// contiguous range of the group's; its element pairs keep their relative
+// order inside every block, so its values are bit for bit those of the member
+// assembled on its own handle.
+// ---------------------------------------------------------------------------
+
+jfg_status jfg_group_create(int32_t n, const jfg_model_desc *const *descs, jfg_model **out) {
+    if (!out) return JFG_ERR_INVALID;
+    *out = nullptr;
+    if (n <= 0 || !descs) {
+        *out = new jfg_model();
+        return fail(*out, JFG_ERR_INVALID, "a group needs at least one member");
+    }
+    // each member is checked against its own index ranges before merging
+    {
+        jfg_model probe;
+        for (int32_t i = 0; i < n; ++i) {
+            jfg_status st = validate(&probe, descs[i]);
+            if (st || descs[i]->k6rot != descs[0]->k6rot) {
+                *out = new jfg_model();
+                if (!st) return fail(*out, JFG_ERR_INVALID, "group members must share PARAM K6ROT");
+                return fail(*out, st, "group member " + std::to_string(i) + ": " + probe.err);
+            }
+        }
+    }
+    bool any_R = false, any_pin = false;
+    int64_t nn = 0, nq = 0, nt = 0, nb = 0, nr = 0, ns = 0;
+    for (int32_t i = 0; i < n; ++i) {
+        const jfg_model_desc *d = descs[i];
+        any_R |= d->node_R != nullptr;
+        any_pin |= d->bar_pin != nullptr;
+        nn += d->n_nodes; nq += d->n_quad4; nt += d->n_tria3; nb += d->n_bar; nr += d->n_rbe2;
+        ns += d->n_rbe2 ? d->rbe2_slave_ptr[d->n_rbe2] : 0;
+    }
+    std::vector<double> X(3 * nn), R(any_R ? 9 * nn : 0), qp(JFG_SHELL_PROP * nq), tp(JFG_SHELL_PROP * nt),
+        bp(JFG_BAR_PROP * nb);
+    std::vector<int32_t> qn(4 * nq), tn(3 * nt), bn(2 * nb), pin(any_pin ? 2 * nb : 0), rm(nr), rc(nr), rs(ns);
+    std::vector<int64_t> rptr(nr + 1, 0);
+    std::vector<std::array<int64_t, 8>> mem(n);
+    int64_t on = 0, oq = 0, ot = 0, ob = 0, orr = 0, os = 0;
+    double snorm = descs[0]->param_snorm;
+    for (int32_t i = 0; i < n; ++i) {
+        const jfg_model_desc *d = descs[i];
+        const int32_t off = (int32_t)on;
+        std::copy(d->coords, d->coords + 3 * d->n_nodes, X.begin() + 3 * on);
+        if (any_R)
+            for (int64_t k = 0; k < d->n_nodes; ++k)
+                for (int c = 0; c < 9; ++c) R[9 * (on + k) + c] = d->node_R ? d->node_R[9 * k + c] : (c % 4 == 0 ? 1.0 : 0.0);
+        for (int64_t k = 0; k < 4 * d->n_quad4; ++k) qn[4 * oq + k] = d->quad4_nodes[k] + off;
+        std::copy(d->quad4_prop, d->quad4_prop + JFG_SHELL_PROP * d->n_quad4, qp.begin() + JFG_SHELL_PROP * oq);
+        for (int64_t k = 0; k < 3 * d->n_tria3; ++k) tn[3 * ot + k] = d->tria3_nodes[k] + off;
+        std::copy(d->tria3_prop, d->tria3_prop + JFG_SHELL_PROP * d->n_tria3, tp.begin() + JFG_SHELL_PROP * ot);
+        for (int64_t k = 0; k < 2 * d->n_bar; ++k) bn[2 * ob + k] = d->bar_nodes[k] + off;
+        std::copy(d->bar_prop, d->bar_prop + JFG_BAR_PROP * d->n_bar, bp.begin() + JFG_BAR_PROP * ob);
+        if (any_pin)
+            for (int64_t k = 0; k < 2 * d->n_bar; ++k) pin[2 * ob + k] = d->bar_pin ? d->bar_pin[k] : 0;
+        for (int64_t r = 0; r < d->n_rbe2; ++r) {
+            rm[orr + r] = d->rbe2_master[r] + off;
+            rc[orr + r] = d->rbe2_cm[r];
+            for (int64_t q = d->rbe2_slave_ptr[r]; q < d->rbe2_slave_ptr[r + 1]; ++q) rs[os++] = d->rbe2_slaves[q] + off;
+            rptr[orr + r + 1] = os;
+        }
+        snorm = std::max(snorm, d->param_snorm);
+        mem[i] = {d->n_nodes, on, 0, 0, oq, ot, ob, d->n_quad4 + d->n_tria3 + d->n_bar};
+        on += d->n_nodes; oq += d->n_quad4; ot += d->n_tria3; ob += d->n_bar; orr += d->n_rbe2;
+    }
+    jfg_model_desc g{};
+    g.n_nodes = nn; g.coords = X.data(); g.node_R = any_R ? R.data() : nullptr;
+    g.n_quad4 = nq; g.quad4_nodes = qn.data(); g.quad4_prop = qp.data();
+    g.n_tria3 = nt; g.tria3_nodes = tn.data(); g.tria3_prop = tp.data();
+    g.n_bar = nb; g.bar_nodes = bn.data(); g.bar_prop = bp.data(); g.bar_pin = any_pin ? pin.data() : nullptr;
+    g.n_rbe2 = nr; g.rbe2_master = rm.data(); g.rbe2_cm = rc.data(); g.rbe2_slave_ptr = rptr.data(); g.rbe2_slaves = rs.data();
+    g.k6rot = descs[0]->k6rot; g.param_snorm = snorm;
+    jfg_status st = jfg_model_create(&g, out);
+    if (st) return st;
+    jfg_model *m = *out;
+    // nonzero ranges: a member's columns are [6 node_off, 6 (node_off + n_nodes))
+    for (int32_t i = 0; i < n; ++i) {
+        int64_t a = 0, b = 0;
+        CK(cudaMemcpyAsync(&a, m->d_rowptr + 6 * mem[i][1], sizeof(int64_t), cudaMemcpyDeviceToHost, m->stream));
+        CK(cudaMemcpyAsync(&b, m->d_rowptr + 6 * (mem[i][1] + mem[i][0]), sizeof(int64_t), cudaMemcpyDeviceToHost, m->stream));
+        CK(cudaStreamSynchronize(m->stream));
+        mem[i][2] = b - a;
+        mem[i][3] = a;
+    }
+    m->members = mem;
+    return JFG_OK;
+}
+
+jfg_status jfg_group_member(jfg_model *m, int32_t i, int64_t *out8) {
+    if (!m || !out8) return JFG_ERR_INVALID;
+    if (i < 0 || i >= (int32_t)m->members.size()) return fail(m, JFG_ERR_INVALID, "no such group member");
+    for (int k = 0; k < 8; ++k) out8[k] = m->members[i][k];
+    return JFG_OK;
+}
+
 jfg_status jfg_model_counts(jfg_model *m, int64_t *out4) {
     if (!m || !out4) return JFG_ERR_INVALID;
     out4[0] = m->n_nodes;
@@ -1429,11 +1626,17 @@ jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
         o.diag_slot = m->d_dslot + m->dslot_q4;
         o.h = bt.h;
         o.h_stride = m->nq + m->nt;
-        dim3 grid((unsigned)cdiv(m->nq, Q4_ELEMS_PER_BLOCK), nv);
-        if (kg)
-            q4_kg_kernel<<<grid, Q4_THREADS, 0, m->stream>>>(m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, du, o);
+        const int W = m->q4_warps;
+        const dim3 grid((unsigned)cdiv(m->nq, Q4_TEAMS_PER_WARP * W), nv);
+        const size_t smem = (size_t)Q4_TEAMS_PER_WARP * W * (kg ? sizeof(Q4GShared) : sizeof(Q4KShared));
+        if (kg && W == 8)
+            q4_kg_kernel<8><<<grid, 32 * W, smem, m->stream>>>(m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, du, o);
+        else if (kg)
+            q4_kg_kernel<4><<<grid, 32 * W, smem, m->stream>>>(m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, du, o);
+        else if (W == 8)
+            q4_k_kernel<8><<<grid, 32 * W, smem, m->stream>>>(m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, m->k6rot, o);
         else
-            q4_k_kernel<<<grid, Q4_THREADS, 0, m->stream>>>(m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, m->k6rot, o);
+            q4_k_kernel<4><<<grid, 32 * W, smem, m->stream>>>(m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, m->k6rot, o);
         CK(cudaGetLastError());
     }
     CK(mark(m, 1));
@@ -1678,13 +1881,68 @@ jfg_status jfg_assemble_batch_device(jfg_model *m, int32_t n_var, const double *
     return st;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Device -> host copy into caller memory, on the handle's stream; the caller
+// synchronises.  A page-locked destination gets one cudaMemcpyAsync.  An
+// ordinary pageable one -- what a Julia Vector or a numpy array is -- would
+// go through the driver's single-threaded staging at a fraction of the link
+// rate, so large copies run through the handle's ring of pinned chunks
+// instead: while the GPU fills chunk i + 1 .. i + 3, host threads move chunk
+// i into the destination.  The ring and the threads are made at first use
+// (JFG_COPY_THREADS sets the thread count, default min(8, cores / 2)).
+jfg_status copy_to_host(jfg_model *m, void *dst, const void *src, size_t bytes) {
+    cudaPointerAttributes at{};
+    const bool pinned = cudaPointerGetAttributes(&at, dst) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    cudaGetLastError();  // an unknown pointer may leave an error set on older runtimes
+    if (pinned || bytes < (size_t(4) << 20)) {
+        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, m->stream));
+        return JFG_OK;
+    }
+    constexpr int R = jfg_model::kPinChunks;
+    constexpr size_t C = jfg_model::kPinChunkBytes;
+    if (!m->pin) {
+        CK(cudaHostAlloc((void **)&m->pin, R * C, cudaHostAllocDefault));
+        for (auto &e : m->pin_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        int n = (int)std::min<unsigned>(8, std::max<unsigned>(1, std::thread::hardware_concurrency() / 2));
+        if (const char *env = std::getenv("JFG_COPY_THREADS")) n = std::max(1, std::atoi(env));
+        m->copy_pool.reset(new CopyPool(n - 1));
+    }
+    const size_t n = (bytes + C - 1) / C;
+    auto issue = [&](size_t i) -> cudaError_t {
+        const size_t len = std::min(C, bytes - i * C);
+        cudaError_t e = cudaMemcpyAsync(m->pin + (i % R) * C, static_cast<const char *>(src) + i * C, len,
+                                        cudaMemcpyDeviceToHost, m->stream);
+        return e != cudaSuccess ? e : cudaEventRecord(m->pin_ev[i % R], m->stream);
+    };
+    for (size_t i = 0; i < std::min<size_t>(R, n); ++i) CK(issue(i));
+    for (size_t i = 0; i < n; ++i) {
+        CK(cudaEventSynchronize(m->pin_ev[i % R]));
+        m->copy_pool->copy(static_cast<char *>(dst) + i * C, m->pin + (i % R) * C, std::min(C, bytes - i * C));
+        if (i + R < n) CK(issue(i + R));
+    }
+    return JFG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 jfg_status jfg_assemble_k(jfg_model *m, double *nzval, double *max_elem_stiff, double *orig_diag) {
     if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
     jfg_status st = launch_k(m, m->d_nz, m->d_max, orig_diag ? m->d_diag : nullptr);
     if (st) return st;
-    if (nzval) CK(cudaMemcpyAsync(nzval, m->d_nz, sizeof(double) * m->nnz, cudaMemcpyDeviceToHost, m->stream));
+    if (nzval) {
+        st = copy_to_host(m, nzval, m->d_nz, sizeof(double) * m->nnz);
+        if (st) return st;
+    }
     if (max_elem_stiff) CK(cudaMemcpyAsync(max_elem_stiff, m->d_max, sizeof(double), cudaMemcpyDeviceToHost, m->stream));
-    if (orig_diag) CK(cudaMemcpyAsync(orig_diag, m->d_diag, sizeof(double) * m->ndof, cudaMemcpyDeviceToHost, m->stream));
+    if (orig_diag) {
+        st = copy_to_host(m, orig_diag, m->d_diag, sizeof(double) * m->ndof);
+        if (st) return st;
+    }
     CK(cudaStreamSynchronize(m->stream));
     return finish_timing(m);
 }
@@ -1698,7 +1956,10 @@ jfg_status jfg_assemble_kg(jfg_model *m, const double *u_global, double *nzval) 
     CK(cudaMemcpyAsync(m->d_u, u_global, sizeof(double) * m->ndof, cudaMemcpyHostToDevice, m->stream));
     jfg_status st = launch_kg(m, m->d_u, m->d_nz);
     if (st) return st;
-    if (nzval) CK(cudaMemcpyAsync(nzval, m->d_nz, sizeof(double) * m->nnz, cudaMemcpyDeviceToHost, m->stream));
+    if (nzval) {
+        st = copy_to_host(m, nzval, m->d_nz, sizeof(double) * m->nnz);
+        if (st) return st;
+    }
     CK(cudaStreamSynchronize(m->stream));
     return finish_timing(m);
 }
@@ -2180,7 +2441,8 @@ extern "C" jfg_status jfg_assemble_k_quad4_noalloc(int64_t n_nodes, const double
     o.diag_staging = nullptr;
     o.diag_slot = nullptr;
     o.maxabs = nullptr;
-    q4_k_kernel<<<(unsigned)cdiv(n_quad4, Q4_ELEMS_PER_BLOCK), Q4_THREADS, 0, s>>>(n_quad4, quad4_nodes_dev, quad4_prop_dev,
+    q4_k_kernel<4><<<(unsigned)cdiv(n_quad4, Q4_ELEMS_PER_BLOCK), Q4_THREADS, Q4_ELEMS_PER_BLOCK * sizeof(Q4KShared), s>>>(
+        n_quad4, quad4_nodes_dev, quad4_prop_dev,
                                                                                  coords_dev, node_R_dev, k6rot, o);
     na_incidence_kernel<<<(unsigned)cdiv(n_nodes, 128), 128, 0, s>>>(n_nodes, n_quad4, quad4_nodes_dev, base);
     na_reduce_kernel<<<(unsigned)cdiv(6 * n_nodes, 128), 128, 0, s>>>(n_nodes, quad4_nodes_dev, rowptr_dev, colind_dev, base,

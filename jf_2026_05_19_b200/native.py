@@ -27,7 +27,8 @@ EXPORTS = ("jfg_model_create", "jfg_pattern", "jfg_pattern_fill", "jfg_assemble_
            "jfg_dkdh_contract_device", "jfg_dkdh_load_device", "jfg_recover_stresses",
            "jfg_recover_stresses_device", "jfg_kg_contract", "jfg_kg_contract_device", "jfg_server_create", "jfg_server_submit", "jfg_server_wait",
            "jfg_server_result", "jfg_server_release", "jfg_server_stats", "jfg_server_family_batch",
-           "jfg_server_hold", "jfg_server_last_error", "jfg_server_destroy", "jfg_assemble_k_quad4_noalloc", "jfg_model_destroy", "jfg_last_error",
+           "jfg_server_hold", "jfg_server_last_error", "jfg_server_destroy", "jfg_group_create", "jfg_group_member",
+           "jfg_assemble_k_quad4_noalloc", "jfg_model_destroy", "jfg_last_error",
            "jfg_version")
 
 _lib = None
@@ -63,6 +64,10 @@ def load(path: str = LIB_PATH):
         raise RuntimeError(f"{path} was built from other sources ({ver}); rebuild it (jf_2026_05_19_b200/build.py --force)")
     L.jfg_model_create.argtypes = [C.POINTER(JfgModelDesc), C.POINTER(C.c_void_p)]
     L.jfg_model_create.restype = C.c_int32
+    L.jfg_group_create.argtypes = [C.c_int32, C.POINTER(C.POINTER(JfgModelDesc)), C.POINTER(C.c_void_p)]
+    L.jfg_group_create.restype = C.c_int32
+    L.jfg_group_member.argtypes = [C.c_void_p, C.c_int32, _pi64]
+    L.jfg_group_member.restype = C.c_int32
     L.jfg_pattern.argtypes = [C.c_void_p, _pi64, _pi64]
     L.jfg_pattern_fill.argtypes = [C.c_void_p, _pi64, _pi64]
     L.jfg_assemble_k.argtypes = [C.c_void_p, _pd, _pd, _pd]
@@ -140,12 +145,15 @@ class GpuModel:
         self.h = C.c_void_p()
         d, keep = make_desc(m)
         st = self.L.jfg_model_create(C.byref(d), C.byref(self.h))
+        del keep
+        self._finish_create(st)
+
+    def _finish_create(self, st: int):
         if st != 0:
             msg = self.L.jfg_last_error(self.h).decode()
             self.L.jfg_model_destroy(self.h)
             self.h = C.c_void_p()
             raise JfgError(st, msg)
-        del keep
         nd = C.c_int64(); nnz = C.c_int64()
         self._check(self.L.jfg_pattern(self.h, C.byref(nd), C.byref(nnz)))
         self.ndof = int(nd.value)
@@ -359,6 +367,48 @@ def version() -> str:
 
 SERVE_BATCHED, SERVE_SERIAL = 0, 1
 
+
+
+class GpuGroup(GpuModel):
+    """A group handle (jfg_group_create): several models side by side in one
+    handle, so each launch takes bins from all of them.  Every GpuModel call
+    works on the group; member(i) gives a member's offsets and member_values /
+    member_pattern its slice of the group's arrays."""
+
+    def __init__(self, models):
+        self.L = load()
+        self.models = list(models)
+        self.model = None
+        self.h = C.c_void_p()
+        pairs = [make_desc(m) for m in self.models]
+        arr = (C.POINTER(JfgModelDesc) * len(pairs))(*[C.pointer(d) for d, _ in pairs])
+        st = self.L.jfg_group_create(len(pairs), arr, C.byref(self.h))
+        del pairs, arr
+        self._finish_create(st)
+
+    def member(self, i: int) -> dict:
+        o = np.zeros(8, np.int64)
+        self._check(self.L.jfg_group_member(self.h, int(i), _ptr(o, _pi64)))
+        keys = ("n_nodes", "node_off", "nnz", "nnz_off", "quad4_off", "tria3_off", "bar_off", "elements")
+        return dict(zip(keys, (int(x) for x in o)))
+
+    def member_values(self, nz: np.ndarray, i: int) -> np.ndarray:
+        """Member i's nonzeros (CSC order) out of a group-wide value array."""
+        d = self.member(i)
+        return nz[d["nnz_off"]:d["nnz_off"] + d["nnz"]]
+
+    def member_dofs(self, v: np.ndarray, i: int) -> np.ndarray:
+        d = self.member(i)
+        return v[6 * d["node_off"]:6 * (d["node_off"] + d["n_nodes"])]
+
+    def member_pattern(self, i: int):
+        """Member i's (colptr, rowval), 1-based, as its own handle would give them."""
+        cp, rv = self.pattern()
+        d = self.member(i)
+        a, n = 6 * d["node_off"], 6 * d["n_nodes"]
+        colptr = cp[a:a + n + 1] - d["nnz_off"]
+        rowval = rv[d["nnz_off"]:d["nnz_off"] + d["nnz"]] - a
+        return colptr, rowval
 
 class Server:
     """Device-resident request loop over model families (jfg_server_* in the C ABI).

@@ -24,6 +24,17 @@ FLOPS = {
     "bar_kg": 2 * 1_550,
 }
 
+# FP64 flops the closed-form kernels actually execute per element (2 DFMA +
+# DADD + DMUL thread instructions, from ncu counters of two launches of each
+# kernel on a 240 x 96 barrel; the capture is summarised under profiles/).
+# They divide the same launch time as FLOPS to give the hardware fraction of
+# the FP64 peak beside the canonical-work rate.
+EXECUTED_FLOPS = {
+    "quad4_k": 13_503,
+    "quad4_kg": 10_134,
+    "tria3_k": 27_734,
+}
+
 NODES = {"quad4": 4, "tria3": 3, "bar": 2}
 NDOF = {"quad4": 24, "tria3": 18, "bar": 12}
 
@@ -44,3 +55,9 @@ def bytes_per_step(counts: dict, nnz: int) -> float:
 def kernel_flops(kernel: str, count: int) -> float:
     """Algorithmic flops of one launch of an element kernel over `count` elements."""
     return FLOPS[kernel] * count
+
+
+def kernel_executed_flops(kernel: str, count: int):
+    """Executed FP64 flops of one launch, or None where no counter capture exists."""
+    f = EXECUTED_FLOPS.get(kernel)
+    return None if f is None else f * count

@@ -41,6 +41,40 @@ namespace {
 
 typedef double V3[3];
 
+// Forward-mode dual number v + d eps (eps^2 = 0): the oracle's restatement of
+// ForwardDiff's Dual with one partial, which the reference uses to
+// differentiate the shell elements in their thickness (dKdx.jl:219-228).
+// Comparisons and branches look at the value only, as ForwardDiff's do.
+struct Dual {
+    double v = 0.0, d = 0.0;
+    Dual() = default;
+    Dual(double x) : v(x), d(0.0) {}  // NOLINT: constants promote implicitly
+    Dual(double x, double dx) : v(x), d(dx) {}
+    Dual &operator+=(const Dual &o) { v += o.v; d += o.d; return *this; }
+    Dual &operator-=(const Dual &o) { v -= o.v; d -= o.d; return *this; }
+    Dual &operator*=(const Dual &o) { d = d * o.v + v * o.d; v *= o.v; return *this; }
+    Dual &operator/=(const Dual &o) { *this = Dual(v / o.v, (d * o.v - v * o.d) / (o.v * o.v)); return *this; }
+};
+inline Dual operator+(Dual a, const Dual &b) { return a += b; }
+inline Dual operator-(Dual a, const Dual &b) { return a -= b; }
+inline Dual operator*(Dual a, const Dual &b) { return a *= b; }
+inline Dual operator/(Dual a, const Dual &b) { return a /= b; }
+inline Dual operator-(const Dual &a) { return Dual(-a.v, -a.d); }
+inline bool operator<(const Dual &a, const Dual &b) { return a.v < b.v; }
+inline bool operator>(const Dual &a, const Dual &b) { return a.v > b.v; }
+inline bool operator==(const Dual &a, const Dual &b) { return a.v == b.v; }
+inline Dual fabs(const Dual &a) { return a.v < 0.0 ? -a : a; }
+inline Dual sqrt(const Dual &a) { const double r = std::sqrt(a.v); return Dual(r, a.d / (2.0 * r)); }
+inline double value(double x) { return x; }
+inline double value(const Dual &x) { return x.v; }
+// max(|x|, floor) with the derivative of the branch taken
+template <typename T> inline T abs_floor(const T &x, double floor) {
+    using std::fabs;
+    const T a = fabs(x);
+    return value(a) < floor ? T(floor) : a;
+}
+
+
 inline void sub3(const double *a, const double *b, double *o) { o[0] = a[0] - b[0]; o[1] = a[1] - b[1]; o[2] = a[2] - b[2]; }
 inline double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 inline void cross3(const double *a, const double *b, double *o) {
@@ -53,22 +87,23 @@ inline void normalize3(const double *a, double *o) { double n = norm3(a); o[0] =
 
 // Dense LU with partial pivoting: solve A X = B in place (A n x n, B n x m),
 // row-major.  Returns false on an exactly singular pivot.
-bool lu_solve(int n, int m, double *A, double *B) {
-    std::vector<int> piv(n);
+template <typename T>
+bool lu_solve(int n, int m, T *A, T *B) {
+    using std::fabs;
     for (int k = 0; k < n; ++k) {
         int p = k;
-        double best = std::fabs(A[k * n + k]);
+        T best = fabs(A[k * n + k]);
         for (int i = k + 1; i < n; ++i) {
-            double v = std::fabs(A[i * n + k]);
+            T v = fabs(A[i * n + k]);
             if (v > best) { best = v; p = i; }
         }
-        if (best == 0.0) return false;
+        if (value(best) == 0.0) return false;
         if (p != k) {
             for (int j = 0; j < n; ++j) std::swap(A[k * n + j], A[p * n + j]);
             for (int j = 0; j < m; ++j) std::swap(B[k * m + j], B[p * m + j]);
         }
         for (int i = k + 1; i < n; ++i) {
-            double f = A[i * n + k] / A[k * n + k];
+            T f = A[i * n + k] / A[k * n + k];
             A[i * n + k] = f;
             for (int j = k + 1; j < n; ++j) A[i * n + j] -= f * A[k * n + j];
             for (int j = 0; j < m; ++j) B[i * m + j] -= f * B[k * m + j];
@@ -76,7 +111,7 @@ bool lu_solve(int n, int m, double *A, double *B) {
     }
     for (int k = n - 1; k >= 0; --k) {
         for (int j = 0; j < m; ++j) {
-            double s = B[k * m + j];
+            T s = B[k * m + j];
             for (int i = k + 1; i < n; ++i) s -= A[k * n + i] * B[i * m + j];
             B[k * m + j] = s / A[k * n + k];
         }
@@ -85,8 +120,9 @@ bool lu_solve(int n, int m, double *A, double *B) {
 }
 
 // inv(SMatrix{4,4}) restated as Gauss-Jordan (identity right-hand side).
-void inv4(const double A[4][4], double Ai[4][4]) {
-    double a[16], b[16];
+template <typename T>
+void inv4(const T A[4][4], T Ai[4][4]) {
+    T a[16], b[16];
     for (int i = 0; i < 4; ++i)
         for (int j = 0; j < 4; ++j) { a[i * 4 + j] = A[i][j]; b[i * 4 + j] = (i == j) ? 1.0 : 0.0; }
     lu_solve(4, 4, a, b);
@@ -116,19 +152,21 @@ inline Jac jacobian(const double lc[4][2], const double dNr[4], const double dNs
 }
 
 // C += alpha * A' * B  with A (k x m), B (k x n), C (m x n), all row-major.
-void mul_At_add(double *C, const double *A, const double *B, int k, int m, int n, double alpha) {
+template <typename TC, typename TA, typename TB, typename TS>
+void mul_At_add(TC *C, const TA *A, const TB *B, int k, int m, int n, TS alpha) {
     for (int j = 0; j < n; ++j)
         for (int l = 0; l < k; ++l) {
-            double v = alpha * B[l * n + j];
+            TC v = alpha * B[l * n + j];
             for (int i = 0; i < m; ++i) C[i * n + j] += A[l * m + i] * v;
         }
 }
 // C = A * B  (A m x k, B k x n)
-void mul(double *C, const double *A, const double *B, int m, int k, int n) {
+template <typename TC, typename TA, typename TB>
+void mul(TC *C, const TA *A, const TB *B, int m, int k, int n) {
     for (int i = 0; i < m * n; ++i) C[i] = 0.0;
     for (int j = 0; j < n; ++j)
         for (int l = 0; l < k; ++l) {
-            double v = B[l * n + j];
+            TC v = B[l * n + j];
             for (int i = 0; i < m; ++i) C[i * n + j] += A[i * k + l] * v;
         }
 }
@@ -136,9 +174,12 @@ void mul(double *C, const double *A, const double *B, int m, int k, int n) {
 // add_quad4_macneal_shear_rbf! default branch (FEMKernels.jl:4715-4978):
 // epsilon 0.04, "diag" flexibility, paper length mode, zb_scale 0.65,
 // zb_u = zb_d, no per-GP delta, rigid_shear = false.
-void macneal_shear(double Ke[24][24], const double lc[4][2], const double Cb[3][3], const double Cs[2][2], double h) {
-    double csmax = std::max(std::max(std::fabs(Cs[0][0]), std::fabs(Cs[0][1])), std::max(std::fabs(Cs[1][0]), std::fabs(Cs[1][1])));
-    if (h < 1e-30 || csmax < 1e-30) return;
+template <typename T>
+void macneal_shear(T Ke[24][24], const double lc[4][2], const T Cb[3][3], const T Cs[2][2], T h) {
+    using std::fabs;
+    const double csmax = std::max(std::max(std::fabs(value(Cs[0][0])), std::fabs(value(Cs[0][1]))),
+                                  std::max(std::fabs(value(Cs[1][0])), std::fabs(value(Cs[1][1]))));
+    if (value(h) < 1e-30 || csmax < 1e-30) return;
     const double pt = 1.0 / std::sqrt(3.0);
     const double sp[4][3] = {{0.0, -pt, 1}, {0.0, pt, 1}, {-pt, 0.0, 2}, {pt, 0.0, 2}};
     double D[4][12] = {};
@@ -178,47 +219,47 @@ void macneal_shear(double Ke[24][24], const double lc[4][2], const double Cb[3][
     double eps = std::min(std::max(0.04, 1e-12), 1.0);
     double a_param = eps / (eps + (1.0 - eps) * Dx2 / std::max(Dy2, 1e-30));
     double b_param = eps / (eps + (1.0 - eps) * Dy2 / std::max(Dx2, 1e-30));
-    double flex_x = 1.0 / std::max(std::fabs(Cb[0][0]), 1e-30);
-    double flex_y = 1.0 / std::max(std::fabs(Cb[1][1]), 1e-30);
+    T flex_x = 1.0 / abs_floor(Cb[0][0], 1e-30);
+    T flex_y = 1.0 / abs_floor(Cb[1][1], 1e-30);
     double inv12A = 1.0 / (12.0 * A_elem);
     const double zb = 0.65;
-    double zbx_u = zb * inv12A * Dx2 * flex_x;
-    double zbx_d = zb * inv12A * a_param * Dx2 * flex_x;
-    double zby_u = zb * inv12A * Dy2 * flex_y;
-    double zby_d = zb * inv12A * b_param * Dy2 * flex_y;
-    double Zb[4][4] = {};
+    T zbx_u = zb * inv12A * Dx2 * flex_x;
+    T zbx_d = zb * inv12A * a_param * Dx2 * flex_x;
+    T zby_u = zb * inv12A * Dy2 * flex_y;
+    T zby_d = zb * inv12A * b_param * Dy2 * flex_y;
+    T Zb[4][4] = {};
     Zb[0][0] = zbx_u + zbx_d; Zb[0][1] = zbx_u - zbx_d; Zb[1][0] = Zb[0][1]; Zb[1][1] = Zb[0][0];
     Zb[2][2] = zby_u + zby_d; Zb[2][3] = zby_u - zby_d; Zb[3][2] = Zb[2][3]; Zb[3][3] = Zb[2][2];
     // physical shear compliance (eq 23-25)
     const int comps[4] = {1, 1, 2, 2};
-    double VGV[4][4];
+    T VGV[4][4];
     for (int i = 0; i < 4; ++i)
         for (int j = 0; j < 4; ++j) {
             double Jfac = std::sqrt(2.0 * Jp[i]) * std::sqrt(2.0 * Jp[j]);
-            if (comps[i] == comps[j]) VGV[i][j] = (i == j) ? Jfac * (comps[i] == 1 ? Cs[0][0] : Cs[1][1]) : 0.0;
+            if (comps[i] == comps[j]) VGV[i][j] = (i == j) ? Jfac * (comps[i] == 1 ? Cs[0][0] : Cs[1][1]) : T(0.0);
             else VGV[i][j] = 0.5 * Jfac * Cs[0][1];
         }
     for (int i = 0; i < 4; ++i)
-        if (VGV[i][i] < 1e-30) VGV[i][i] = 1e-30;
-    double VS[4][4], Zs[4][4], Zi[4][4];
+        if (value(VGV[i][i]) < 1e-30) VGV[i][i] = 1e-30;
+    T VS[4][4], Zs[4][4], Zi[4][4];
     for (int i = 0; i < 4; ++i)
         for (int j = 0; j < 4; ++j) VS[i][j] = 0.5 * (VGV[i][j] + VGV[j][i]);
     inv4(VS, Zi);
     for (int i = 0; i < 4; ++i)
         for (int j = 0; j < 4; ++j) Zs[i][j] = 0.5 * (Zi[i][j] + Zi[j][i]);
-    double Zt[4][4], Z[16];
+    T Zt[4][4], Z[16];
     for (int i = 0; i < 4; ++i)
         for (int j = 0; j < 4; ++j) Zt[i][j] = Zs[i][j] + Zb[i][j];
     for (int i = 0; i < 4; ++i)
         for (int j = 0; j < 4; ++j) Z[i * 4 + j] = 0.5 * (Zt[i][j] + Zt[j][i]);
-    double X[4 * 12];
+    T X[4 * 12];
     for (int i = 0; i < 4; ++i)
         for (int j = 0; j < 12; ++j) X[i * 12 + j] = D[i][j];
     lu_solve(4, 12, Z, X);
-    double Kp[12][12];
+    T Kp[12][12];
     for (int i = 0; i < 12; ++i)
         for (int j = 0; j < 12; ++j) {
-            double s = 0.0;
+            T s = 0.0;
             for (int l = 0; l < 4; ++l) s += D[l][i] * X[l * 12 + j];
             Kp[i][j] = s;
         }
@@ -232,11 +273,13 @@ void macneal_shear(double Ke[24][24], const double lc[4][2], const double Cb[3][
 // (:3466-3492), MITC4 shear skipped (:3762), Hughes-Brezzi drill
 // (:3556-3559), Wilson incompatible modes and 4x4 condensations
 // (:3790-3801, :3964-4011).  No Bmb, no curvature terms.
-void q4_stiffness(const double lc[4][2], const double Cm[3][3], const double Cb[3][3], const double Cs[2][2],
-                  double h, double E_ref, double k6rot, double drill_scale, bool bending_incomp,
-                  bool membrane_incomp, double Ke[24][24]) {
-    std::memset(Ke, 0, sizeof(double) * 576);
-    double K_ab[24][4] = {}, K_bb[4][4] = {}, K_abb[24][4] = {}, K_bbb[4][4] = {};
+template <typename T>
+void q4_stiffness(const double lc[4][2], const T Cm[3][3], const T Cb[3][3], const T Cs[2][2],
+                  T h, T E_ref, double k6rot, double drill_scale, bool bending_incomp,
+                  bool membrane_incomp, T Ke[24][24]) {
+    for (int i = 0; i < 24; ++i)
+        for (int j = 0; j < 24; ++j) Ke[i][j] = 0.0;
+    T K_ab[24][4] = {}, K_bb[4][4] = {}, K_abb[24][4] = {}, K_bbb[4][4] = {};
     const double dNr_c[4] = {-0.25, 0.25, 0.25, -0.25}, dNs_c[4] = {-0.25, -0.25, 0.25, 0.25};
     Jac jc = jacobian(lc, dNr_c, dNs_c);
     double dNdx_c[4], dNdy_c[4];
@@ -246,9 +289,9 @@ void q4_stiffness(const double lc[4][2], const double Cm[3][3], const double Cb[
     }
     const double pt = 1.0 / std::sqrt(3.0);
     const double gp[4][2] = {{-pt, -pt}, {pt, -pt}, {pt, pt}, {-pt, pt}};
-    double G_drill = Cm[2][2] / h;
-    if (G_drill < 1e-6) G_drill = E_ref / (2 * 3.0);
-    double alpha_drill = drill_scale * (k6rot / 1e5) * G_drill * h;
+    T G_drill = Cm[2][2] / h;
+    if (value(G_drill) < 1e-6) G_drill = E_ref / (2 * 3.0);
+    T alpha_drill = drill_scale * (k6rot / 1e5) * G_drill * h;
 
     for (int g = 0; g < 4; ++g) {
         double r = gp[g][0], s = gp[g][1];
@@ -280,7 +323,7 @@ void q4_stiffness(const double lc[4][2], const double Cm[3][3], const double Cb[
         Bib[0][2] = dphi1_dx; Bib[0][3] = dphi2_dx;
         Bib[2][0] = -dphi1_dx; Bib[2][1] = -dphi2_dx;
         Bib[2][2] = dphi1_dy; Bib[2][3] = dphi2_dy;
-        double t3x24[3 * 24], t3x4[3 * 4];
+        T t3x24[3 * 24], t3x4[3 * 4];
         mul(t3x24, &Cm[0][0], &Bm[0][0], 3, 3, 24);
         mul_At_add(&Ke[0][0], &Bm[0][0], t3x24, 3, 24, 24, absdet);
         mul(t3x24, &Cb[0][0], &Bb[0][0], 3, 3, 24);
@@ -299,15 +342,15 @@ void q4_stiffness(const double lc[4][2], const double Cm[3][3], const double Cb[
 
     double kbbmax = 0.0;
     for (int i = 0; i < 4; ++i)
-        for (int jj = 0; jj < 4; ++jj) kbbmax = std::max(kbbmax, std::fabs(K_bbb[i][jj]));
-    auto condense = [&](double Kab[24][4], double Kbb[4][4]) {
-        double Ii[4][4];
+        for (int jj = 0; jj < 4; ++jj) kbbmax = std::max(kbbmax, std::fabs(value(K_bbb[i][jj])));
+    auto condense = [&](T Kab[24][4], T Kbb[4][4]) {
+        T Ii[4][4];
         inv4(Kbb, Ii);
         for (int jj = 0; jj < 24; ++jj)
             for (int i = 0; i < 24; ++i) {
-                double sm = 0.0;
+                T sm = 0.0;
                 for (int l = 0; l < 4; ++l) {
-                    double t = 0.0;
+                    T t = 0.0;
                     for (int q = 0; q < 4; ++q) t += Ii[l][q] * Kab[jj][q];
                     sm += Kab[i][l] * t;
                 }
@@ -325,9 +368,11 @@ void q4_stiffness(const double lc[4][2], const double Cm[3][3], const double Cb[
 // stiffness_tria3_matrices_generic (FEMKernels.jl:7315-7385) with
 // tria3_plate_macro_data (:7157-7209): CST membrane, plate block from three
 // default-kwarg virtual quads condensed to the corners, Hughes-Brezzi drill.
-void t3_stiffness(const double lc[3][2], const double Dm[3][3], const double Db[3][3], const double Ds[2][2],
-                  double h, double G_ref, double br, double k6rot, double Ke[18][18]) {
-    std::memset(Ke, 0, sizeof(double) * 324);
+template <typename T>
+void t3_stiffness(const double lc[3][2], const T Dm[3][3], const T Db[3][3], const T Ds[2][2],
+                  T h, T G_ref, double br, double k6rot, T Ke[18][18]) {
+    for (int i = 0; i < 18; ++i)
+        for (int j = 0; j < 18; ++j) Ke[i][j] = 0.0;
     double x[3] = {lc[0][0], lc[1][0], lc[2][0]}, y[3] = {lc[0][1], lc[1][1], lc[2][1]};
     double A2 = x[0] * (y[1] - y[2]) + x[1] * (y[2] - y[0]) + x[2] * (y[0] - y[1]);
     double A = 0.5 * std::fabs(A2);
@@ -338,7 +383,7 @@ void t3_stiffness(const double lc[3][2], const double Dm[3][3], const double Db[
     for (int i = 0; i < 3; ++i) {
         Bm[0][2 * i] = bv[i]; Bm[1][2 * i + 1] = cv[i]; Bm[2][2 * i] = cv[i]; Bm[2][2 * i + 1] = bv[i];
     }
-    double DB[3 * 6], Km[6 * 6] = {};
+    T DB[3 * 6], Km[6 * 6] = {};
     mul(DB, &Dm[0][0], &Bm[0][0], 3, 3, 6);
     mul_At_add(Km, &Bm[0][0], DB, 3, 6, 6, A);
     const int m_idx[6] = {0, 1, 6, 7, 12, 13};
@@ -354,12 +399,13 @@ void t3_stiffness(const double lc[3][2], const double Dm[3][3], const double Db[
         pts[6][0] = (x[0] + x[1] + x[2]) / 3; pts[6][1] = (y[0] + y[1] + y[2]) / 3;
         const int quads[3][4] = {{0, 3, 6, 5}, {1, 4, 6, 3}, {2, 5, 6, 4}};
         const int pd[12] = {2, 3, 4, 8, 9, 10, 14, 15, 16, 20, 21, 22};
-        static thread_local double K21[21][21];
-        std::memset(K21, 0, sizeof(K21));
+        static thread_local T K21[21][21];
+        for (int i = 0; i < 21; ++i)
+            for (int j = 0; j < 21; ++j) K21[i][j] = 0.0;
         for (int q = 0; q < 3; ++q) {
             double qc[4][2];
             for (int k = 0; k < 4; ++k) { qc[k][0] = pts[quads[q][k]][0]; qc[k][1] = pts[quads[q][k]][1]; }
-            double Kq[24][24];
+            T Kq[24][24];
             q4_stiffness(qc, Dm, Db, Ds, h, G_ref, k6rot, 1.0, /*bending_incomp=*/false, /*membrane_incomp=*/true, Kq);
             int ed[12];
             for (int k = 0; k < 4; ++k)
@@ -367,7 +413,7 @@ void t3_stiffness(const double lc[3][2], const double Dm[3][3], const double Db[
             for (int i = 0; i < 12; ++i)
                 for (int j = 0; j < 12; ++j) K21[ed[i]][ed[j]] += Kq[pd[i]][pd[j]];
         }
-        double Kii[12 * 12], Aint[12 * 9];
+        T Kii[12 * 12], Aint[12 * 9];
         for (int i = 0; i < 12; ++i) {
             for (int j = 0; j < 12; ++j) Kii[i * 12 + j] = K21[9 + i][9 + j];
             for (int j = 0; j < 9; ++j) Aint[i * 9 + j] = K21[9 + i][j];
@@ -377,12 +423,12 @@ void t3_stiffness(const double lc[3][2], const double Dm[3][3], const double Db[
         const int b_idx[9] = {2, 3, 4, 8, 9, 10, 14, 15, 16};
         for (int i = 0; i < 9; ++i)
             for (int j = 0; j < 9; ++j) {
-                double s = K21[i][j];
+                T s = K21[i][j];
                 for (int l = 0; l < 12; ++l) s += K21[i][9 + l] * Aint[l * 9 + j];
                 Ke[b_idx[i]][b_idx[j]] += s;
             }
     }
-    double alpha_drill = (k6rot / 1e5) * G_ref * h;
+    T alpha_drill = (k6rot / 1e5) * G_ref * h;
     double Bd[18] = {};
     for (int i = 0; i < 3; ++i) {
         Bd[6 * i + 0] = 0.5 * cv[i]; Bd[6 * i + 1] = -0.5 * bv[i]; Bd[6 * i + 5] = 1.0 / 3.0;
@@ -599,6 +645,11 @@ void frame3d_geometric(double L, double P, double kg[12][12]) {
 struct Triplets {
     std::vector<int64_t> I, J;  // 0-based
     std::vector<double> V;
+    // Rounding scale of each value (tests only; empty: |V|).  It differs from
+    // |V| where the value is a product of a cancelling sum, e.g. a bar KG term
+    // proportional to an axial force P that is a small difference of large
+    // end displacements.
+    std::vector<double> M;
 };
 
 const double *node_R_of(const jfg_model_desc *d, int64_t n, double tmp[9]) {
@@ -693,6 +744,124 @@ void transform_sym(int nn, const double *Q /* nn*9 */, const double *K, double *
             for (int l = 0; l < n; ++l) s += T[l * n + i] * tmp[l * n + j];
             out[i * n + j] = s;
         }
+}
+
+// ---------------------------------------------------------------------------
+// Rounding scales of KG element values (tests only).  A KG term is a product
+// of a membrane stress or a bar axial force, which the element forms from
+// differences of nodal displacements.  Where that stress or force is small
+// next to the displacement terms it is formed from, any two implementations
+// (the reference's own included) round it differently by eps times those
+// terms.  These functions carry the magnitudes of the terms, instead of the
+// values, through the same products, giving each KG value's rounding scale.
+// ---------------------------------------------------------------------------
+
+// |Q|' K |Q| for the block-diagonal node rotations (K >= 0 entrywise).
+void transform_sym_abs(int nn, const double *Q, const double *K, double *out) {
+    int n = 6 * nn;
+    std::vector<double> T(n * n, 0.0), tmp(n * n, 0.0);
+    for (int k = 0; k < nn; ++k)
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) {
+                T[(6 * k + r) * n + 6 * k + c] = std::fabs(Q[9 * k + 3 * r + c]);
+                T[(6 * k + 3 + r) * n + 6 * k + 3 + c] = std::fabs(Q[9 * k + 3 * r + c]);
+            }
+    mul(tmp.data(), K, T.data(), n, n, n);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            double s = 0.0;
+            for (int l = 0; l < n; ++l) s += T[l * n + i] * tmp[l * n + j];
+            out[i * n + j] = s;
+        }
+}
+
+// Scale of the local displacements u_loc = Q u_global: sum |Q_rl u_l|.
+void local_u_scale(int nn, const int32_t *nd, const double *Q, const double *u, double *us) {
+    for (int k = 0; k < nn; ++k) {
+        const double *ug = u + 6 * (int64_t)nd[k];
+        for (int dd = 0; dd < 3; ++dd) {
+            double a = 0.0, b = 0.0;
+            for (int l = 0; l < 3; ++l) {
+                a += std::fabs(Q[9 * k + 3 * dd + l] * ug[l]);
+                b += std::fabs(Q[9 * k + 3 * dd + l] * ug[3 + l]);
+            }
+            us[6 * k + dd] = a;
+            us[6 * k + 3 + dd] = b;
+        }
+    }
+}
+
+// CQUAD4 KG (principal-transverse, incompatible membrane modes): the stress
+// of every Gauss point over the magnitudes of its strain terms (B u and the
+// incompatible modes B_i alpha, alpha = -K_bb^-1 K_ab' u), then both
+// principal directions with |lambda| <= |sxx| + |syy| + 2 |sxy| and
+// |cos|, |sin| <= 1 over the gradient vectors' magnitudes.
+void q4_kg_scale(const double lc[4][2], const double us[24], const double Cm[3][3], double h, double M[24][24]) {
+    std::memset(M, 0, sizeof(double) * 576);
+    if (h < 1e-30) return;
+    const double pt = 1.0 / std::sqrt(3.0);
+    const double gp[4][2] = {{-pt, -pt}, {pt, -pt}, {pt, pt}, {-pt, pt}};
+    double K_ab[24][4] = {}, K_bb[4][4] = {}, Bm[4][3][24] = {}, Bi[4][3][4] = {}, det[4];
+    Jac js[4];
+    for (int g = 0; g < 4; ++g) {
+        double dNr[4], dNs[4];
+        shape_derivs_quad(gp[g][0], gp[g][1], dNr, dNs);
+        js[g] = jacobian(lc, dNr, dNs);
+        det[g] = std::max(std::fabs(js[g].det), 1e-12);
+        for (int k = 0; k < 4; ++k) {
+            const double dx = js[g].iJ11 * dNr[k] + js[g].iJ12 * dNs[k], dy = js[g].iJ21 * dNr[k] + js[g].iJ22 * dNs[k];
+            Bm[g][0][6 * k] = dx; Bm[g][1][6 * k + 1] = dy; Bm[g][2][6 * k] = dy; Bm[g][2][6 * k + 1] = dx;
+        }
+        const double r = gp[g][0], s = gp[g][1];
+        const double d1x = js[g].iJ11 * (-2.0 * r), d1y = js[g].iJ21 * (-2.0 * r), d2x = js[g].iJ12 * (-2.0 * s),
+                     d2y = js[g].iJ22 * (-2.0 * s);
+        Bi[g][0][0] = d1x; Bi[g][2][0] = d1y; Bi[g][1][1] = d1y; Bi[g][2][1] = d1x;
+        Bi[g][0][2] = d2x; Bi[g][2][2] = d2y; Bi[g][1][3] = d2y; Bi[g][2][3] = d2x;
+        double CBi[12];
+        mul(CBi, &Cm[0][0], &Bi[g][0][0], 3, 3, 4);
+        mul_At_add(&K_ab[0][0], &Bm[g][0][0], CBi, 3, 24, 4, det[g]);
+        mul_At_add(&K_bb[0][0], &Bi[g][0][0], CBi, 3, 4, 4, det[g]);
+    }
+    double Kbi[4][4], am[4], Amap[4][24];
+    inv4(K_bb, Kbi);
+    q4_incomp_map(lc, Cm, Amap);
+    for (int l = 0; l < 4; ++l) {
+        double r = 0.0;
+        for (int m = 0; m < 4; ++m) {
+            double t = 0.0;
+            for (int i = 0; i < 24; ++i) t += std::fabs(K_ab[i][m]) * us[i];
+            r += std::fabs(Kbi[l][m]) * t;
+        }
+        am[l] = r;
+    }
+    for (int g = 0; g < 4; ++g) {
+        double em[3], sm[3];
+        for (int c = 0; c < 3; ++c) {
+            double t = 0.0;
+            for (int i = 0; i < 24; ++i) t += std::fabs(Bm[g][c][i]) * us[i];
+            for (int l = 0; l < 4; ++l) t += std::fabs(Bi[g][c][l]) * am[l];
+            em[c] = t;
+        }
+        for (int c = 0; c < 3; ++c) sm[c] = (std::fabs(Cm[c][0]) * em[0] + std::fabs(Cm[c][1]) * em[1] + std::fabs(Cm[c][2]) * em[2]) / h;
+        const double lam = sm[0] + sm[1] + 2.0 * sm[2];
+        const double r = gp[g][0], s = gp[g][1];
+        const double d1x = js[g].iJ11 * (-2.0 * r), d1y = js[g].iJ21 * (-2.0 * r), d2x = js[g].iJ12 * (-2.0 * s),
+                     d2y = js[g].iJ22 * (-2.0 * s);
+        double Gxy[24] = {}, Gz[24] = {};
+        double dNr[4], dNs[4];
+        shape_derivs_quad(r, s, dNr, dNs);
+        for (int k = 0; k < 4; ++k) {
+            const double dx = std::fabs(js[g].iJ11 * dNr[k] + js[g].iJ12 * dNs[k]),
+                         dy = std::fabs(js[g].iJ21 * dNr[k] + js[g].iJ22 * dNs[k]);
+            Gxy[6 * k] += dx + dy; Gxy[6 * k + 1] += dx + dy; Gz[6 * k + 2] = dx + dy;
+        }
+        for (int a = 0; a < 24; ++a)
+            Gxy[a] += (std::fabs(d1x) + std::fabs(d1y)) * (std::fabs(Amap[0][a]) + std::fabs(Amap[1][a])) +
+                      (std::fabs(d2x) + std::fabs(d2y)) * (std::fabs(Amap[2][a]) + std::fabs(Amap[3][a]));
+        const double f = 2.0 * h * det[g] * lam;
+        for (int i = 0; i < 24; ++i)
+            for (int j = 0; j < 24; ++j) M[i][j] += f * (Gxy[i] * Gxy[j] + Gz[i] * Gz[j]);
+    }
 }
 
 struct Err { int code = 0; std::string msg; };
@@ -860,9 +1029,9 @@ std::map<int64_t, std::vector<std::pair<int64_t, double>>> rbe2_map(const jfg_mo
 // order (images of a dependent dof in the order of its constraint row), so
 // the redistributed triplet list is never materialised.
 //
-// abs_sums (optional) receives, per stored entry, the same fold over |v|:
-// the magnitude of the terms the entry sums, i.e. the scale of its
-// summation-order rounding.  Only the tests use it.
+// abs_sums (optional) receives, per stored entry, the same fold over the
+// terms' rounding scales (|v|, or t.M): the scale of the entry's rounding
+// in any summation order.  Only the tests use it.
 void constrain_and_csc(const jfg_model_desc *d, Triplets &t, std::vector<int64_t> &colptr, std::vector<int64_t> &rowval,
                        std::vector<double> &nzval, std::vector<double> *abs_sums = nullptr) {
     auto mp = rbe2_map(d);
@@ -870,22 +1039,24 @@ void constrain_and_csc(const jfg_model_desc *d, Triplets &t, std::vector<int64_t
     std::vector<const std::vector<std::pair<int64_t, double>> *> dep(ndof, nullptr);
     for (auto &kv : mp) dep[kv.first] = &kv.second;
     const size_t n_in = t.V.size();
-    // f(i, j, v) for every triplet that input k becomes, in emission order
+    // f(i, j, v, mag) for every triplet that input k becomes, in emission
+    // order; mag is the rounding scale of v (|v| unless t.M says otherwise)
+    const bool has_m = !t.M.empty();
     auto emit = [&](size_t k, auto &&f) {
         const int64_t i = t.I[k], j = t.J[k];
-        const double v = t.V[k];
+        const double v = t.V[k], mg = has_m ? t.M[k] : std::fabs(v);
         const auto *di = dep[i], *dj = dep[j];
-        if (!di && !dj) f(i, j, v);
-        else if (di && !dj) { for (auto &p : *di) f(p.first, j, v * p.second); }
-        else if (!di && dj) { for (auto &p : *dj) f(i, p.first, v * p.second); }
+        if (!di && !dj) f(i, j, v, mg);
+        else if (di && !dj) { for (auto &p : *di) f(p.first, j, v * p.second, mg * std::fabs(p.second)); }
+        else if (!di && dj) { for (auto &p : *dj) f(i, p.first, v * p.second, mg * std::fabs(p.second)); }
         else {
             for (auto &a : *di)
-                for (auto &b : *dj) f(a.first, b.first, v * a.second * b.second);
+                for (auto &b : *dj) f(a.first, b.first, v * a.second * b.second, mg * std::fabs(a.second * b.second));
         }
     };
     // (1) counting sort into rows
     std::vector<int64_t> row_at(ndof + 1, 0);
-    for (size_t k = 0; k < n_in; ++k) emit(k, [&](int64_t i, int64_t, double) { ++row_at[i + 1]; });
+    for (size_t k = 0; k < n_in; ++k) emit(k, [&](int64_t i, int64_t, double, double) { ++row_at[i + 1]; });
     for (int64_t i = 0; i < ndof; ++i) row_at[i + 1] += row_at[i];
     const int64_t n_trip = row_at[ndof];
     std::vector<int32_t> ccol(n_trip);
@@ -893,11 +1064,11 @@ void constrain_and_csc(const jfg_model_desc *d, Triplets &t, std::vector<int64_t
     {
         std::vector<int64_t> fill(row_at.begin(), row_at.end() - 1);
         for (size_t k = 0; k < n_in; ++k)
-            emit(k, [&](int64_t i, int64_t j, double v) {
+            emit(k, [&](int64_t i, int64_t j, double v, double mg) {
                 const int64_t q = fill[i]++;
                 ccol[q] = (int32_t)j;
                 cval[q] = v;
-                if (abs_sums) cabs[q] = std::fabs(v);
+                if (abs_sums) cabs[q] = mg;
             });
     }
     // (2) merge repeated columns per row into their first occurrence, in order
@@ -1086,19 +1257,24 @@ void t3_generic(const double lc[3][2], double E, double nu, double h, double Ke[
     t3_stiffness(lc, Dm, Db, Ds, h, G, 1.0, 100.0, Ke);
 }
 
-// dK/dh of the CTRIA3 by central differences with one Richardson step
-// (step h / 256, error O(step^4)); the reference differentiates the same
-// function by forward-mode AD, which this matches to about 1e-10 relative.
+// dK/dh of the CTRIA3 by forward-mode differentiation, as the reference's
+// _shell_thickness_dKe_forward_ad does (dKdx.jl:219-228): the same element
+// evaluated on a dual thickness h + eps.  Exact up to rounding, pivots and
+// branches chosen on the values like ForwardDiff's.
 void t3_generic_dkdh(const double lc[3][2], double E, double nu, double h, double dKe[18][18]) {
-    double Kp[18][18], Km[18][18], Kp2[18][18], Km2[18][18];
-    const double d = h / 256.0;
-    t3_generic(lc, E, nu, h + d, Kp); t3_generic(lc, E, nu, h - d, Km);
-    t3_generic(lc, E, nu, h + 0.5 * d, Kp2); t3_generic(lc, E, nu, h - 0.5 * d, Km2);
+    const double G = E / (2 * (1 + nu));
+    const double base[3][3] = {{1.0, nu, 0.0}, {nu, 1.0, 0.0}, {0.0, 0.0, (1 - nu) / 2}};
+    const Dual hd(h, 1.0);
+    Dual Dm[3][3], Db[3][3], Ds[2][2];
+    const Dual cm = E * hd / (1 - nu * nu), cb = 1.0 * (E * hd * hd * hd / (12 * (1 - nu * nu)));
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) { Dm[i][j] = cm * base[i][j]; Db[i][j] = cb * base[i][j]; }
+    Ds[0][0] = Ds[1][1] = (5.0 / 6.0) * G * hd;
+    Ds[0][1] = Ds[1][0] = 0.0;
+    static thread_local Dual K[18][18];
+    t3_stiffness(lc, Dm, Db, Ds, hd, Dual(G), 1.0, 100.0, K);
     for (int i = 0; i < 18; ++i)
-        for (int c = 0; c < 18; ++c) {
-            const double D1 = (Kp[i][c] - Km[i][c]) / (2 * d), D2 = (Kp2[i][c] - Km2[i][c]) / d;
-            dKe[i][c] = (4.0 * D2 - D1) / 3.0;
-        }
+        for (int c = 0; c < 18; ++c) dKe[i][c] = K[i][c].d;
 }
 
 // Shell element setup of _shell_elem_local_data (dKdx.jl:128-176): frame
@@ -1616,6 +1792,7 @@ int kg_element_triplets(const jfg_model_desc *d, const double *u, Triplets &t, s
     }
     size_t total = (size_t)nq * 576 + (size_t)nt * 324 + (size_t)nb * 144;
     t.I.resize(total); t.J.resize(total); t.V.resize(total);
+    if (g_abs_sums) t.M.assign(total, 0.0);
 #pragma omp parallel for schedule(static)
     for (int64_t e = 0; e < nq; ++e) {
         const int32_t *nd = d->quad4_nodes + 4 * e;
@@ -1658,6 +1835,15 @@ int kg_element_triplets(const jfg_model_desc *d, const double *u, Triplets &t, s
             for (int r = 0; r < 24; ++r) { G[r * 24 + dd] = 0.0; G[dd * 24 + r] = 0.0; }
         }
         size_t base = (size_t)e * 576;
+        if (g_abs_sums) {
+            double us[24], Ml[24][24], Mg[576];
+            local_u_scale(4, nd, Q, u, us);
+            q4_kg_scale(lc, us, Cm, h, Ml);
+            transform_sym_abs(4, Q, &Ml[0][0], Mg);
+            int q = 0;
+            for (int cc = 0; cc < 24; ++cc)
+                for (int rr = 0; rr < 24; ++rr, ++q) t.M[base + q] = (rr % 6 == 5 || cc % 6 == 5) ? 0.0 : Mg[rr * 24 + cc];
+        }
         int cnt = 0;
         for (int cc = 0; cc < 24; ++cc)
             for (int rr = 0; rr < 24; ++rr) {
@@ -1719,6 +1905,29 @@ int kg_element_triplets(const jfg_model_desc *d, const double *u, Triplets &t, s
                     double val = h * A * (sxx * b[i] * b[j] + syy * cv[i] * cv[j] + sxy * (b[i] * cv[j] + cv[i] * b[j]));
                     for (int dd = 0; dd < 3; ++dd) Kl[6 * i + dd][6 * j + dd] += val;
                 }
+            if (g_abs_sums) {
+                // rounding scale: the CST stress over the magnitudes of its strain terms
+                double us[18], em[3] = {0, 0, 0}, Ml[18][18] = {}, Mg[324];
+                local_u_scale(3, nd, Q, u, us);
+                for (int i = 0; i < 3; ++i) {
+                    em[0] += std::fabs(b[i]) * us[6 * i];
+                    em[1] += std::fabs(cv[i]) * us[6 * i + 1];
+                    em[2] += std::fabs(cv[i]) * us[6 * i] + std::fabs(b[i]) * us[6 * i + 1];
+                }
+                double sm[3];
+                for (int r = 0; r < 3; ++r) sm[r] = std::fabs(D[r][0]) * em[0] + std::fabs(D[r][1]) * em[1] + std::fabs(D[r][2]) * em[2];
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) {
+                        const double mv = h * A * (sm[0] * std::fabs(b[i] * b[j]) + sm[1] * std::fabs(cv[i] * cv[j]) +
+                                                   sm[2] * (std::fabs(b[i] * cv[j]) + std::fabs(cv[i] * b[j])));
+                        for (int dd = 0; dd < 3; ++dd) Ml[6 * i + dd][6 * j + dd] = mv;
+                    }
+                transform_sym_abs(3, Q, &Ml[0][0], Mg);
+                const size_t mb = (size_t)nq * 576 + (size_t)e * 324;
+                int q = 0;
+                for (int cc = 0; cc < 18; ++cc)
+                    for (int rr = 0; rr < 18; ++rr, ++q) t.M[mb + q] = (rr % 6 == 5 || cc % 6 == 5) ? 0.0 : Mg[rr * 18 + cc];
+            }
         }
         double G[324];
         transform_sym(3, Q, &Kl[0][0], G);
@@ -1755,6 +1964,30 @@ int kg_element_triplets(const jfg_model_desc *d, const double *u, Triplets &t, s
         frame3d_stiffness(L, A, Iy, Iz, J, E, G, Asy, Asz, I12, k);
         double P = 0.0;
         for (int q = 0; q < 12; ++q) P += k[6][q] * ub[q];
+        if (g_abs_sums) {
+            // rounding scale of P: the sum k[6][q] ub[q] over the magnitudes
+            // of its terms, each ub[q] itself a sum T u
+            double Pm = 0.0;
+            for (int q = 0; q < 12; ++q) {
+                double um = 0.0;
+                const int kq = q / 6;
+                for (int l = 0; l < 6; ++l) um += std::fabs(T12[q][6 * kq + l] * u[6 * (int64_t)nd[kq] + l]);
+                Pm += std::fabs(k[6][q]) * um;
+            }
+            double kg1[12][12], Mb[144];
+            frame3d_geometric(L, 1.0, kg1);
+            for (int i = 0; i < 12; ++i)
+                for (int j = 0; j < 12; ++j) {
+                    double s = 0.0;
+                    for (int l = 0; l < 12; ++l)
+                        for (int q = 0; q < 12; ++q) s += std::fabs(T12[l][i] * kg1[l][q] * T12[q][j]);
+                    Mb[i * 12 + j] = Pm * s;
+                }
+            size_t base = (size_t)nq * 576 + (size_t)nt * 324 + (size_t)e * 144;
+            int cnt = 0;
+            for (int cc = 0; cc < 12; ++cc)
+                for (int rr = 0; rr < 12; ++rr) t.M[base + cnt++] = Mb[rr * 12 + cc];
+        }
         double kg[12][12], tmp[144], Kb[144];
         frame3d_geometric(L, P, kg);
         mul(tmp, &kg[0][0], &T12[0][0], 12, 12, 12);
@@ -1776,14 +2009,21 @@ int kg_element_triplets(const jfg_model_desc *d, const double *u, Triplets &t, s
     }
     {
         size_t nbase = (size_t)nq * 576 + (size_t)nt * 324;
+        if (g_abs_sums)  // a shell value with no stress term (A or h below the cutoffs) is 0; keep |V| there
+            for (size_t q = 0; q < nbase; ++q) t.M[q] = std::max(t.M[q], std::fabs(t.V[q]));
         bool any = false;
         for (int64_t e = 0; e < nb; ++e) any |= !bar_ok[e];
         if (any) {
             Triplets u2;
             u2.I.assign(t.I.begin(), t.I.begin() + nbase); u2.J.assign(t.J.begin(), t.J.begin() + nbase); u2.V.assign(t.V.begin(), t.V.begin() + nbase);
+            if (g_abs_sums) u2.M.assign(t.M.begin(), t.M.begin() + nbase);
             for (int64_t e = 0; e < nb; ++e)
                 if (bar_ok[e])
-                    for (int q = 0; q < 144; ++q) { size_t s = nbase + e * 144 + q; u2.I.push_back(t.I[s]); u2.J.push_back(t.J[s]); u2.V.push_back(t.V[s]); }
+                    for (int q = 0; q < 144; ++q) {
+                        size_t s = nbase + e * 144 + q;
+                        u2.I.push_back(t.I[s]); u2.J.push_back(t.J[s]); u2.V.push_back(t.V[s]);
+                        if (g_abs_sums) u2.M.push_back(t.M[s]);
+                    }
             t = std::move(u2);
         }
     }

@@ -118,5 +118,13 @@ def single_quad4():
 
 
 def single_cell_tria3():
-    """One quad cell split into two CTRIA3 (plus the plane's bars and RBE2)."""
-    return skewed_plane(seed=8, nx=1, ny=1, tri_frac=1.0)
+    """One skewed, arbitrarily oriented quad cell split into two CTRIA3, nothing else."""
+    rng = np.random.default_rng(8)
+    P = np.array([[0.0, 0.0, 0.0], [23.0, 1.5, 0.0], [25.0, 19.0, 0.0], [-2.0, 17.0, 0.0]])
+    coords = P @ rotation(rng).T + rng.uniform(-50, 50, 3)
+    tris = np.array([[0, 1, 2], [0, 2, 3]], np.int32)
+    prop = np.array([D.shell_prop_row(1.7, 70000.0, 0.33), D.shell_prop_row(2.3, 70000.0, 0.33)])
+    p = D.plate_c1(n=1)
+    return dataclasses.replace(p, coords=coords, q4_nodes=np.zeros((0, 4), np.int32), q4_prop=np.zeros((0, D.N_SHELL_PROP)),
+                               t3_nodes=tris, t3_prop=prop, node_ids=np.arange(1, 5), spc_dofs=None,
+                               force=np.zeros(24), name="single_cell_tria3")
