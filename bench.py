@@ -51,8 +51,10 @@ def parse_args():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["barrel", "barrel_medium", "barrel_small", "panel", "plate", "serving", "variants"],
-                   default="barrel")
+    p.add_argument("--workload", choices=["barrel", "barrel_medium", "barrel_small", "panel", "plate", "serving", "variants",
+                                          "group"], default="barrel")
+    p.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
+    p.add_argument("--group-variants", type=int, default=4, help="group: design variants of every member per launch")
     p.add_argument("--rates", type=str, default="100,1000,5000", help="serving: Poisson arrival rates, req/s")
     p.add_argument("--requests", type=int, default=256, help="serving: requests per rate (server arms)")
     p.add_argument("--plain-requests", type=int, default=48, help="serving: requests per rate (plain arm)")
@@ -477,12 +479,27 @@ def run_serving(args):
     models = [native.GpuModel(m) for m in fams]
     launches_per_batch = [2 * (sum(1 for c in ("quad4", "tria3", "bar") if m.counts()[c]) + 1 +
                                (2 if m.rbe2_master.shape[0] else 0)) for m in fams]
+    # families under 64k elements share one group handle, so their requests
+    # share launches; the large families keep their own handles
+    small = [i for i, n in enumerate(sizes) if n < 64_000]
+    large = [i for i in range(len(fams)) if i not in small]
+    group = native.GpuGroup([fams[i] for i in small])
+    g_units = [group] + [models[i] for i in large]
+    g_u = [np.concatenate([us[i] for i in small])] + [us[i] for i in large]
+    g_map = [None] * len(fams)
+    for k, i in enumerate(small):
+        g_map[i] = (0, k)
+    for k, i in enumerate(large):
+        g_map[i] = (1 + k, -1)
     arms = {}
     clocks = ClockSampler(uuid=device_uuid(torch, torch.device("cuda", 0)), index=0)
     clocks.start()
-    for name, policy in (("batched", native.SERVE_BATCHED), ("serial_resident", native.SERVE_SERIAL)):
-        with native.Server(models, us, hbm_budget_bytes=int(args.hbm_budget_gb * 1e9), max_batch=args.max_batch,
-                           policy=policy) as srv:
+    for name, policy, units, uu, fmap in (
+            ("batched", native.SERVE_BATCHED, g_units, g_u, g_map),
+            ("batched_per_family", native.SERVE_BATCHED, models, us, None),
+            ("serial_resident", native.SERVE_SERIAL, models, us, None)):
+        with native.Server(units, uu, hbm_budget_bytes=int(args.hbm_budget_gb * 1e9), max_batch=args.max_batch,
+                           policy=policy, family_map=fmap) as srv:
             warm = [srv.submit(f, pools[f][0], keep=False) for f in range(len(fams))]
             for t in warm:
                 srv.wait(t, -1.0); srv.release(t)
@@ -493,11 +510,12 @@ def run_serving(args):
             st = srv.stats()
             res["batches"] = st["batches"] - b0
             res["largest_batch"] = st["max_batch"]
-            res["reserved_gb"] = st["reserved_bytes"] / 1e9
+            res["pool_peak_gb"] = st["pool_peak_bytes"] / 1e9
             res["batch_limits"] = [srv.batch_limit(f) for f in range(len(fams))]
             arms[name] = res
     for g in models:
         g.close()
+    group.close()
     torch.cuda.synchronize()
     us_dev = [torch.from_numpy(u).cuda() for u in us]
     nz_bufs = []
@@ -520,11 +538,14 @@ def run_serving(args):
             "data": "synthetic: seeded plate/panel/barrel families, Poisson arrivals, lognormal(0.1) thickness vectors",
             "config": {"workload": "serving: 8 device-resident families, K+KG per request, uniform family choice",
                        "family_elements": sizes, "rates_req_s": rates, "hbm_budget_gb": args.hbm_budget_gb,
-                       "max_batch": args.max_batch, "value_at_rate": float(top)},
+                       "max_batch": args.max_batch, "value_at_rate": float(top),
+                       "grouped_families": small,
+                       "admission": "one device pool of the budget; batches take workspace and results as they form"},
             "serving": arms,
             "speedup_at_top_rate": {
                 "vs_plain_one_deck_per_launch": v / arms["plain_one_deck_per_launch"][top]["throughput_req_s"],
-                "vs_serial_resident": v / arms["serial_resident"][top]["throughput_req_s"]},
+                "vs_serial_resident": v / arms["serial_resident"][top]["throughput_req_s"],
+                "vs_batched_per_family": v / arms["batched_per_family"][top]["throughput_req_s"]},
             "e2e": {"value": v, "unit": "req/s", "h2d_bytes_per_step": 8 * mean_shell, "d2h_bytes_per_step": 0,
                     "note": "submit-to-done wall clock through the server's C ABI; thickness vectors copied in, "
                             "K and KG stay on the device"},
@@ -660,6 +681,103 @@ def run_variants(args):
     return 0
 
 
+def run_group(args):
+    """Mixed-model batch: the eight serving-stream families (plate, stiffened panel and
+    barrel meshes of 1.6k to 596k elements, CQUAD4/CTRIA3/CBAR/CBEAM, RBE2) in one group
+    handle, each with --group-variants thickness variants, K and KG of every member and
+    variant in one CUDA-graph replay; against one launch sequence per member and variant
+    on the members' own handles."""
+    import torch
+    from jf_2026_05_19_b200 import decks, native
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    fams = decks.serving_families(seed=0)
+    nv = max(1, args.group_variants)
+    rng = np.random.default_rng(3)
+    hv = [[np.concatenate([m.q4_prop[:, 0], m.t3_prop[:, 0]]) * np.exp(0.1 * rng.standard_normal(m.q4_nodes.shape[0] + m.t3_nodes.shape[0]))
+           for m in fams] for _ in range(nv)]
+    nq = [m.q4_nodes.shape[0] for m in fams]
+    H = np.stack([np.concatenate([np.concatenate([hv[v][i][:nq[i]] for i in range(len(fams))]),
+                                  np.concatenate([hv[v][i][nq[i]:] for i in range(len(fams))])]) for v in range(nv)])
+    us = [decks.smooth_displacement(m, seed=20 + i) for i, m in enumerate(fams)]
+    g = native.GpuGroup(fams)
+    tuned = g.launch_config() if args.no_autotune else g.autotune()
+    g.batch_reserve(nv)
+    s = torch.cuda.Stream()
+    g.set_stream(s.cuda_stream)
+    Hd = torch.from_numpy(H).to(dev)
+    ud = torch.from_numpy(np.concatenate(us)).to(dev)
+    nzk = torch.empty(nv, g.nnz, dtype=torch.float64, device=dev)
+    nzg = torch.empty_like(nzk)
+
+    def call():
+        g.assemble_batch_device(nv, Hd.data_ptr(), 0, ud.data_ptr(), 0, nzk.data_ptr(), 0, 0, nzg.data_ptr())
+
+    torch.cuda.synchronize()
+    call(); call()
+    s.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=s):
+        call()
+    for _ in range(max(args.warmup, 3)):
+        graph.replay()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(uuid=device_uuid(torch, dev), index=0)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    with torch.cuda.stream(s):
+        for _ in range(args.steps):
+            graph.replay()
+    e1.record(s)
+    e1.synchronize()
+    clk = clocks.stop()
+    el = e0.elapsed_time(e1) / 1e3 / args.steps
+    # the same work as one launch sequence per member and variant, on the members' own handles
+    own = [native.GpuModel(m) for m in fams]
+    bufs = []
+    for i, gm in enumerate(own):
+        gm.set_stream(s.cuda_stream)
+        gm.batch_reserve(1)
+        h1 = torch.from_numpy(np.stack([hv[v][i] for v in range(nv)])).to(dev)
+        u1 = torch.from_numpy(us[i]).to(dev)
+        bufs.append((h1, u1, torch.empty(gm.nnz, dtype=torch.float64, device=dev), torch.empty(gm.nnz, dtype=torch.float64, device=dev)))
+
+    def per_model():
+        for gm, (h1, u1, k1, kg1) in zip(own, bufs):
+            for v in range(nv):
+                gm.assemble_batch_device(1, h1[v].data_ptr(), 0, u1.data_ptr(), 0, k1.data_ptr(), 0, 0, kg1.data_ptr())
+
+    per_model()
+    s.synchronize()
+    p0 = torch.cuda.Event(enable_timing=True); p1 = torch.cuda.Event(enable_timing=True)
+    p0.record(s)
+    for _ in range(args.steps):
+        per_model()
+    p1.record(s)
+    p1.synchronize()
+    sep = p0.elapsed_time(p1) / 1e3 / args.steps
+    for gm in own:
+        gm.close()
+    n_el = nv * sum(m.n_elements for m in fams)
+    line = {"metric": METRIC, "value": n_el / el, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": el * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: the eight seeded serving families, lognormal(0.1) thickness variants",
+            "config": {"workload": f"mixed-model group: {len(fams)} meshes x {nv} variants, K+KG of all in one CUDA-graph replay",
+                       "members_elements": [int(m.n_elements) for m in fams], "variants": nv,
+                       "elements_per_step": int(n_el), "nnz_group": int(g.nnz), "l2": "outputs larger than L2",
+                       "parallelism": "one GPU; members side by side in each launch, variants on blockIdx.y"},
+            "group": {"graph_replay_ms": el * 1e3, "launch_sequence_per_member_and_variant_ms": sep * 1e3,
+                      "speedup_vs_per_member_launches": sep / el, "launch_config": tuned},
+            "gpu_launches": args.steps * 2 * (3 + 2 + 1),  # element kernels, RBE2 path, block reduction
+            "clocks": clk}
+    g.close()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference_serving(args):
     """Oracle port, one request at a time: elements/s on the bounded barrel sample,
     converted with the stream's mean request size."""
@@ -687,6 +805,10 @@ def main():
         if args.impl == "reference":
             return run_reference(args)
         return run_variants(args)
+    if args.workload == "group":
+        if int(os.environ.get("RANK", "0")) != 0 or args.impl == "reference":
+            return 0
+        return run_group(args)
     if args.workload == "serving":
         if int(os.environ.get("RANK", "0")) != 0:
             return 0  # one GPU serves; other ranks have nothing to do
@@ -711,6 +833,9 @@ def main():
     fp64_peak = measure_fp64_peak(torch, dev)
     m = make_model(args.workload, seed=rank)
     g = native.GpuModel(m)
+    t_tune = time.perf_counter()
+    launch_cfg = g.launch_config() if args.no_autotune else g.autotune()
+    t_tune = time.perf_counter() - t_tune
     # a dedicated (non-default) stream shared by the library and the timing events
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
@@ -849,6 +974,7 @@ def main():
                     "pinned_value": e2e_pinned_value},
             "roofline": roof, "gpu_launches": launches_per_step * args.steps, "clocks": clk,
             "kernel_ms": per_kernel, "fp64_dgemm_tflops": fp64_peak, "model_stats": st,
+            "launch_config": dict(launch_cfg, autotuned=not args.no_autotune, tune_s=round(t_tune, 3)),
             "whole_step_roofline": {"flops": roofline.flops_per_step(counts), "bytes": roofline.bytes_per_step(counts, g.nnz)},
             "recovery": {"ms": rec_ms, "elements_per_s": n_el / rec_ms * 1e3, "timed_calls": 5,
                          "output_bytes": 8 * (rec_sh.numel() + (rec_bar.numel() if counts["bar"] else 0)),

@@ -200,6 +200,15 @@ jfg_status jfg_batch_reserve(jfg_model *m, int32_t n_var);
 jfg_status jfg_assemble_batch_device(jfg_model *m, int32_t n_var, const double *h_dev, const double *bar_prop_dev,
                                      const double *u_dev, int64_t u_stride, double *nzk_dev, double *max_dev,
                                      double *diag_dev, double *nzkg_dev);
+/* The same with caller-provided batch workspace instead of the handle's
+ * reserved one: workspace_dev, 256-byte aligned, at least
+ * jfg_batch_workspace_bytes(m, n_var) bytes, used until the stream reaches
+ * the end of the call's kernels.  Lets a server carve batches of any size out
+ * of one device pool (no allocation inside the call). */
+jfg_status jfg_assemble_batch_device_ws(jfg_model *m, int32_t n_var, void *workspace_dev, int64_t workspace_bytes,
+                                        const double *h_dev, const double *bar_prop_dev, const double *u_dev,
+                                        int64_t u_stride, double *nzk_dev, double *max_dev, double *diag_dev,
+                                        double *nzkg_dev);
 
 /* ---- Free-dof submatrices for the solver --------------------------------
  * The step right after assembly in the SOL 105 consumer: A_ff = A[free,
@@ -337,10 +346,13 @@ jfg_status jfg_recover_stresses_device(jfg_model *m, const double *u_dev, const 
  *                      families run on their own streams and overlap.
  *   JFG_SERVE_SERIAL   one request per launch, in arrival order, each
  *                      finished before the next starts (the plain path).
- * Admission: every family gets batch workspace and two result slots sized to
- * an equal share of hbm_budget_bytes (batch limit <= max_batch); requests
- * wait in their family's queue until a slot is free.  Results of a batched
- * request equal, bit for bit, the same request served alone. */
+ * Admission by HBM budget: one device pool of hbm_budget_bytes holds every
+ * batch's workspace and results.  A batch takes both when it is formed (as
+ * many queued requests as fit, at most max_batch); its workspace returns when
+ * its kernels finish, its results when its last request is released.  A
+ * request waits only while its launch unit has two batches in flight or the
+ * pool lacks room.  Results of a batched request equal, bit for bit, the same
+ * request served alone. */
 #define JFG_SERVE_BATCHED 0
 #define JFG_SERVE_SERIAL 1
 typedef struct jfg_server jfg_server;
@@ -349,6 +361,20 @@ typedef struct jfg_server jfg_server;
  * each) for KG, or NULL entries / NULL array for K only. */
 jfg_status jfg_server_create(jfg_model *const *families, const double *const *u_host, int32_t n_families,
                              int64_t hbm_budget_bytes, int32_t max_batch, int32_t policy, jfg_server **out);
+/* Launch units: units[n_units] are handles, plain or group handles
+ * (jfg_group_create), with u_host[n_units] displacement fields (ndof of the
+ * unit, the group's concatenation for a group) or NULL entries.  Family f is
+ * served by unit family_unit[f]: the whole handle when family_member[f] < 0
+ * (one family per such unit), else member family_member[f] of the group.
+ * Requests of a group's families share batches: variant v of a group batch
+ * carries the v-th queued request of every member that has one, the members
+ * without one are computed at the handle's current thickness and discarded.
+ * A grouped family's max_elem_stiff result is the group's (max over its
+ * members).  Group units need JFG_SERVE_BATCHED.  jfg_server_create is the
+ * case of one plain unit per family. */
+jfg_status jfg_server_create_units(jfg_model *const *units, const double *const *u_host, int32_t n_units,
+                                   const int32_t *family_unit, const int32_t *family_member, int32_t n_families,
+                                   int64_t hbm_budget_bytes, int32_t max_batch, int32_t policy, jfg_server **out);
 /* Queue a request (the thickness vector is copied).  keep = 0 returns the
  * result slot as soon as the request is computed (timing only: its record
  * and times stay readable until jfg_server_release, its result pointers are
@@ -361,8 +387,10 @@ jfg_status jfg_server_wait(jfg_server *s, int64_t ticket, double timeout_s, int3
  * times3 = {submitted, launched, finished} in seconds since creation. */
 jfg_status jfg_server_result(jfg_server *s, int64_t ticket, double **nzk_dev, double **nzkg_dev, double **max_dev,
                              double *times3);
+/* A batch's results (all its variants) return to the pool when the last of
+ * its requests is released: release results as they complete. */
 jfg_status jfg_server_release(jfg_server *s, int64_t ticket);
-/* out6 = {submitted, completed, batches launched, largest batch, reserved device bytes, queued}. */
+/* out6 = {submitted, completed, batches launched, largest batch, most pool bytes in use at once, queued}. */
 jfg_status jfg_server_stats(jfg_server *s, int64_t *out6);
 jfg_status jfg_server_family_batch(jfg_server *s, int32_t family, int32_t *batch_limit);
 /* hold != 0: queue new requests without launching them; hold = 0 admits the
@@ -370,6 +398,32 @@ jfg_status jfg_server_family_batch(jfg_server *s, int32_t family, int32_t *batch
 jfg_status jfg_server_hold(jfg_server *s, int32_t hold);
 const char *jfg_server_last_error(jfg_server *s);
 void jfg_server_destroy(jfg_server *s);
+
+/* Current shell thicknesses of the handle (PSHELL T after any update):
+ * n_quad4 + n_tria3 doubles, CQUAD4s then CTRIA3s, the jfg_update_properties
+ * layout. */
+jfg_status jfg_shell_thickness(jfg_model *m, double *h_host);
+
+/* ---- Launch-shape autotuner ------------------------------------------------
+ * No counterpart in the reference, whose assembly loops are CPU threads.
+ * jfg_autotune times the candidate CTA shapes of every element kernel on this
+ * handle's model (K and, unless KG raises for the deck, KG assemblies, device
+ * times from the handle's timing events) and keeps the fastest of each:
+ *   cfg[0] warps per CQUAD4 CTA, 4 or 8 (12 or 24 elements per CTA)
+ *   cfg[1] warps per CTRIA3-stiffness CTA, 2 or 4 (4 or 8 elements)
+ *   cfg[2..4] elements per CTA of the CTRIA3 KG, bar K and bar KG kernels
+ *          (one thread per element node pair): 32, 64 or 128
+ * The choice is stored per kernel and model-size class (floor(log2) of the
+ * element count of the kernel's type) in a text file: JFG_TUNE_FILE, else
+ * $HOME/.cache/jfem_b200/launch_tune.txt.  flags: JFG_TUNE_READ takes a stored
+ * choice when every kernel's size class has one (no timing); JFG_TUNE_WRITE
+ * stores the choice made.  The tuner overwrites the handle's work buffers
+ * (its last K / KG values).  cfg_out (5 int32) may be NULL.
+ * jfg_launch_config sets (cfg_in) and/or reads (cfg_out) the shapes. */
+#define JFG_TUNE_READ 1
+#define JFG_TUNE_WRITE 2
+jfg_status jfg_autotune(jfg_model *m, int32_t flags, int32_t *cfg_out);
+jfg_status jfg_launch_config(jfg_model *m, const int32_t *cfg_in, int32_t *cfg_out);
 
 /* ---- Group handles: several models in one launch ------------------------
  * The reference assembles one model per call; its batch drivers loop over

@@ -200,16 +200,18 @@ __device__ __forceinline__ void stage_sub_block(double *buf, bool t, int bi, int
         }
 }
 
-__global__ void __launch_bounds__(T3_THREADS, 5) t3_k_kernel(int64_t nt, const int32_t *__restrict__ nodes,
+// W warps per CTA (2 W elements): 2 or 4, both at 20 warps per SM.
+template <int W>
+__global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t nt, const int32_t *__restrict__ nodes,
                                                          const double *__restrict__ prop,
                                                          const double *__restrict__ coords,
                                                          const double *__restrict__ nodeR, double k6rot, ElemOut o) {
-    __shared__ T3KShared sh[T3_ELEMS_PER_BLOCK];
+    __shared__ T3KShared sh[T3_TEAMS_PER_WARP * W];
     o = o.at(blockIdx.y);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int team = lane >> 4, tl = lane & 15;
     const unsigned tm = 0xFFFFu << (16 * team);
-    const int64_t e = (int64_t)blockIdx.x * T3_ELEMS_PER_BLOCK + warp * T3_TEAMS_PER_WARP + team;
+    const int64_t e = (int64_t)blockIdx.x * (T3_TEAMS_PER_WARP * W) + warp * T3_TEAMS_PER_WARP + team;
     if (e >= nt) return;  // the whole team leaves; syncs below are team-local
     T3KShared &S = sh[warp * T3_TEAMS_PER_WARP + team];
 

@@ -35,6 +35,7 @@
 
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
+#include <sys/stat.h>
 
 #include "../../include/jfem_gpu.h"
 #include "elem_bar.cuh"
@@ -145,7 +146,12 @@ struct jfg_model {
     int64_t *d_blk_pa = nullptr, *d_blk_pb = nullptr;
     int2 *d_blk_len = nullptr;
     bool blk_even = false;
-    int q4_warps = 4;                    // warps per CQUAD4 CTA (3 elements each): 4 or 8
+    // launch shapes (jfg_autotune): warps per CQUAD4 CTA (3 elements each,
+    // 4 or 8), warps per CTRIA3-stiffness CTA (2 elements each, 2 or 4), and
+    // threads (elements of one node pair) per CTA of the CTRIA3 KG, bar K and
+    // bar KG kernels (32, 64 or 128)
+    int q4_warps = 4, t3_warps = 4;
+    int t3kg_threads = 128, bark_threads = 128, barkg_threads = 128;
     int64_t staging_len = 0;            // staging doubles per assembly: max(K 36 per slot, KG 12 per slot + 27 per bar pair)
     double *d_staging = nullptr;        // 36 doubles per regular element pair
     int64_t *d_rowptr = nullptr, *d_colind = nullptr;   // 0-based symmetric CSR == CSC
@@ -1645,11 +1651,15 @@ jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
         o.diag_slot = m->d_dslot + m->dslot_t3;
         o.h = bt.h ? bt.h + m->nq : nullptr;
         o.h_stride = m->nq + m->nt;
+        const int tt = m->t3kg_threads, W3 = m->t3_warps;
         if (kg)
-            t3_kg_kernel<<<dim3((unsigned)cdiv(6 * m->nt, 128), nv), 128, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords,
-                                                                                     m->d_nodeR, du, o);
+            t3_kg_kernel<<<dim3((unsigned)cdiv(6 * m->nt, tt), nv), tt, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords,
+                                                                                   m->d_nodeR, du, o);
+        else if (W3 == 2)
+            t3_k_kernel<2><<<dim3((unsigned)cdiv(m->nt, T3_TEAMS_PER_WARP * 2), nv), 64, 0, m->stream>>>(
+                m->nt, m->d_t3n, m->d_t3p, m->d_coords, m->d_nodeR, m->k6rot, o);
         else
-            t3_k_kernel<<<dim3((unsigned)cdiv(m->nt, T3_ELEMS_PER_BLOCK), nv), T3_THREADS, 0, m->stream>>>(
+            t3_k_kernel<4><<<dim3((unsigned)cdiv(m->nt, T3_TEAMS_PER_WARP * 4), nv), 128, 0, m->stream>>>(
                 m->nt, m->d_t3n, m->d_t3p, m->d_coords, m->d_nodeR, m->k6rot, o);
         CK(cudaGetLastError());
     }
@@ -1660,11 +1670,12 @@ jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
         o.h = nullptr;
         o.bprop = bt.bprop;
         o.bprop_stride = JFG_BAR_PROP * m->nb;
-        dim3 grid((unsigned)cdiv(3 * m->nb, 128), nv);
+        const int bt_ = kg ? m->barkg_threads : m->bark_threads;
+        dim3 grid((unsigned)cdiv(3 * m->nb, bt_), nv);
         if (kg)
-            bar_kg_kernel<<<grid, 128, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, du, o);
+            bar_kg_kernel<<<grid, bt_, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, du, o);
         else
-            bar_k_kernel<<<grid, 128, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, o);
+            bar_k_kernel<<<grid, bt_, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, o);
         CK(cudaGetLastError());
     }
     CK(mark(m, 3));
@@ -1842,19 +1853,54 @@ jfg_status jfg_batch_reserve(jfg_model *m, int32_t n_var) {
     return JFG_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+jfg_status batch_with_workspace(jfg_model *m, int32_t n_var, double *ws, const double *h_dev, const double *bar_prop_dev,
+                                const double *u_dev, int64_t u_stride, double *nzk_dev, double *max_dev, double *diag_dev,
+                                double *nzkg_dev);
+
+}  // namespace
+
+extern "C" {
+
 jfg_status jfg_assemble_batch_device(jfg_model *m, int32_t n_var, const double *h_dev, const double *bar_prop_dev,
                                      const double *u_dev, int64_t u_stride, double *nzk_dev, double *max_dev, double *diag_dev,
                                      double *nzkg_dev) {
     if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
     if (n_var < 1 || n_var > m->b_cap)
         return fail(m, JFG_ERR_INVALID, "n_var must be in [1, reserved variants]; call jfg_batch_reserve first");
+    return batch_with_workspace(m, n_var, m->d_bw, h_dev, bar_prop_dev, u_dev, u_stride, nzk_dev, max_dev, diag_dev, nzkg_dev);
+}
+
+jfg_status jfg_assemble_batch_device_ws(jfg_model *m, int32_t n_var, void *workspace_dev, int64_t workspace_bytes,
+                                        const double *h_dev, const double *bar_prop_dev, const double *u_dev,
+                                        int64_t u_stride, double *nzk_dev, double *max_dev, double *diag_dev,
+                                        double *nzkg_dev) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    if (n_var < 1 || n_var > 65535) return fail(m, JFG_ERR_INVALID, "n_var must be in [1, 65535]");
+    if (!workspace_dev || (reinterpret_cast<uintptr_t>(workspace_dev) & 255) ||
+        workspace_bytes < 8 * batch_sizes(m).total * (int64_t)n_var)
+        return fail(m, JFG_ERR_INVALID, "workspace must be 256-byte aligned and hold jfg_batch_workspace_bytes(n_var)");
+    return batch_with_workspace(m, n_var, static_cast<double *>(workspace_dev), h_dev, bar_prop_dev, u_dev, u_stride,
+                                nzk_dev, max_dev, diag_dev, nzkg_dev);
+}
+
+}  // extern "C"
+
+namespace {
+
+jfg_status batch_with_workspace(jfg_model *m, int32_t n_var, double *ws, const double *h_dev, const double *bar_prop_dev,
+                                const double *u_dev, int64_t u_stride, double *nzk_dev, double *max_dev, double *diag_dev,
+                                double *nzkg_dev) {
     if (nzkg_dev && !u_dev) return fail(m, JFG_ERR_INVALID, "KG needs u");
     if (u_stride != 0 && u_stride != m->ndof) return fail(m, JFG_ERR_INVALID, "u_stride must be 0 (shared u) or ndof");
     if (!nzk_dev && (max_dev || diag_dev)) return fail(m, JFG_ERR_INVALID, "max/diag outputs belong to K");
     const BatchSizes z = batch_sizes(m);
     Batch b;
     b.n_var = n_var;
-    b.staging = m->d_bw;
+    b.staging = ws;
     b.exc_raw = b.staging + z.staging * n_var;
     b.x_part = b.exc_raw + z.exc * n_var;
     b.dstaging = b.x_part + z.part * n_var;
@@ -1880,6 +1926,10 @@ jfg_status jfg_assemble_batch_device(jfg_model *m, int32_t n_var, const double *
     }
     return st;
 }
+
+}  // namespace
+
+extern "C" {
 
 }  // extern "C"
 
@@ -2221,6 +2271,154 @@ jfg_status jfg_timing_accumulated(jfg_model *m, int kind, double *ms6_sum, int64
     if (reset) {
         for (int k = 0; k < 6; ++k) m->acc_ms[kind][k] = 0.0;
         m->acc_calls[kind] = 0;
+    }
+    return JFG_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+__global__ void tune_u_kernel(int64_t n, double *u) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) u[i] = 1e-3 * sin(0.37 * (double)i) * ((i % 6) < 3 ? 1.0 : 1e-2);
+}
+
+// The launch-shape store: lines "<kernel> <size class> <value>".
+std::mutex g_tune_mutex;
+
+std::string tune_path() {
+    if (const char *p = std::getenv("JFG_TUNE_FILE")) return p;
+    const char *home = std::getenv("HOME");
+    return std::string(home ? home : ".") + "/.cache/jfem_b200/launch_tune.txt";
+}
+
+std::map<std::string, int> tune_read() {
+    std::map<std::string, int> out;
+    FILE *f = std::fopen(tune_path().c_str(), "r");
+    if (!f) return out;
+    char name[64];
+    int cls = 0, val = 0;
+    while (std::fscanf(f, "%63s %d %d", name, &cls, &val) == 3) out[std::string(name) + " " + std::to_string(cls)] = val;
+    std::fclose(f);
+    return out;
+}
+
+bool tune_write(const std::map<std::string, int> &kv) {
+    const std::string p = tune_path();
+    const size_t slash = p.rfind('/');
+    if (slash != std::string::npos) {
+        std::string dir = p.substr(0, slash), acc;
+        for (size_t i = 0; i <= dir.size(); ++i)  // mkdir -p
+            if (i == dir.size() || (dir[i] == '/' && i > 0)) { acc = dir.substr(0, i); mkdir(acc.c_str(), 0755); }
+    }
+    FILE *f = std::fopen(p.c_str(), "w");
+    if (!f) return false;
+    for (auto &e : kv) std::fprintf(f, "%s %d\n", e.first.c_str(), e.second);
+    std::fclose(f);
+    return true;
+}
+
+int size_class(int64_t n) {
+    int c = 0;
+    while (n > 1) { n >>= 1; ++c; }
+    return c;
+}
+
+}  // namespace
+
+extern "C" {
+
+jfg_status jfg_shell_thickness(jfg_model *m, double *h_host) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    if (!h_host) return fail(m, JFG_ERR_INVALID, "null output");
+    const size_t pitch = sizeof(double) * JFG_SHELL_PROP;
+    if (m->nq)
+        CK(cudaMemcpy2DAsync(h_host, sizeof(double), m->d_q4p, pitch, sizeof(double), m->nq, cudaMemcpyDeviceToHost, m->stream));
+    if (m->nt)
+        CK(cudaMemcpy2DAsync(h_host + m->nq, sizeof(double), m->d_t3p, pitch, sizeof(double), m->nt, cudaMemcpyDeviceToHost,
+                             m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    return JFG_OK;
+}
+
+jfg_status jfg_launch_config(jfg_model *m, const int32_t *cfg_in, int32_t *cfg_out) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    if (cfg_in) {
+        auto one_of = [](int v, std::initializer_list<int> ok) { for (int o : ok) if (v == o) return true; return false; };
+        if (!one_of(cfg_in[0], {4, 8}) || !one_of(cfg_in[1], {2, 4}) || !one_of(cfg_in[2], {32, 64, 128}) ||
+            !one_of(cfg_in[3], {32, 64, 128}) || !one_of(cfg_in[4], {32, 64, 128}))
+            return fail(m, JFG_ERR_INVALID, "launch config: CQUAD4 warps 4|8, CTRIA3 warps 2|4, threads 32|64|128");
+        m->q4_warps = cfg_in[0]; m->t3_warps = cfg_in[1];
+        m->t3kg_threads = cfg_in[2]; m->bark_threads = cfg_in[3]; m->barkg_threads = cfg_in[4];
+    }
+    if (cfg_out) {
+        cfg_out[0] = m->q4_warps; cfg_out[1] = m->t3_warps;
+        cfg_out[2] = m->t3kg_threads; cfg_out[3] = m->bark_threads; cfg_out[4] = m->barkg_threads;
+    }
+    return JFG_OK;
+}
+
+jfg_status jfg_autotune(jfg_model *m, int32_t flags, int32_t *cfg_out) {
+    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
+    const int cq = size_class(m->nq), ct = size_class(m->nt), cb = size_class(m->nb);
+    const std::string keys[5] = {"q4 " + std::to_string(cq), "t3k " + std::to_string(ct), "t3kg " + std::to_string(ct),
+                                 "bark " + std::to_string(cb), "barkg " + std::to_string(cb)};
+    int32_t cfg[5];
+    jfg_launch_config(m, nullptr, cfg);
+    if (flags & JFG_TUNE_READ) {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        const auto kv = tune_read();
+        bool all = true;
+        int32_t c2[5];
+        for (int i = 0; i < 5; ++i) {
+            auto it = kv.find(keys[i]);
+            if (it == kv.end()) { all = false; break; }
+            c2[i] = it->second;
+        }
+        if (all && jfg_launch_config(m, c2, cfg_out) == JFG_OK) return JFG_OK;
+    }
+    // Time three passes; pass p runs candidate p of every knob (a knob with
+    // two candidates repeats its second).  Per-kernel device times come from
+    // the handle's timing events over REPS K (+ KG) assemblies per pass.
+    static const int q4c[3] = {4, 8, 8}, t3c[3] = {2, 4, 4}, thr[3] = {32, 64, 128};
+    constexpr int REPS = 3;
+    const bool kg = !m->bar_offsets;
+    if (kg) {
+        tune_u_kernel<<<(unsigned)cdiv(m->ndof, 256), 256, 0, m->stream>>>(m->ndof, m->d_u);
+        CK(cudaGetLastError());
+    }
+    double best[5] = {1e300, 1e300, 1e300, 1e300, 1e300};
+    int choice[5] = {cfg[0], cfg[1], cfg[2], cfg[3], cfg[4]};
+    for (int pass = 0; pass < 3; ++pass) {
+        const int32_t c[5] = {q4c[pass], t3c[pass], thr[pass], thr[pass], thr[pass]};
+        jfg_status st = jfg_launch_config(m, c, nullptr);
+        if (st) return st;
+        for (int warm = 0; warm < 2; ++warm) {  // pass 0 warms up, then REPS timed
+            for (int k = 0; k < 2; ++k) jfg_timing_accumulated(m, k, nullptr, nullptr, 1);
+            for (int r = 0; r < (warm ? REPS : 1); ++r) {
+                st = launch_k(m, m->d_nz, m->d_max, m->d_diag);
+                if (st) return st;
+                if (kg) {
+                    st = launch_kg(m, m->d_u, m->d_nz);
+                    if (st) return st;
+                }
+            }
+        }
+        double tk[6] = {0}, tg[6] = {0};
+        jfg_timing_accumulated(m, 0, tk, nullptr, 1);
+        if (kg) jfg_timing_accumulated(m, 1, tg, nullptr, 1);
+        const double t[5] = {tk[0] + tg[0], tk[1], tg[1], tk[2], tg[2]};  // quad4 K+KG, tria3 K, tria3 KG, bar K, bar KG
+        for (int i = 0; i < 5; ++i)
+            if (t[i] < best[i]) { best[i] = t[i]; choice[i] = c[i]; }
+    }
+    jfg_status st = jfg_launch_config(m, choice, cfg_out);
+    if (st) return st;
+    if (flags & JFG_TUNE_WRITE) {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto kv = tune_read();
+        for (int i = 0; i < 5; ++i) kv[keys[i]] = choice[i];
+        if (!tune_write(kv)) return fail(m, JFG_ERR_INVALID, "cannot write the launch-shape store " + tune_path());
     }
     return JFG_OK;
 }

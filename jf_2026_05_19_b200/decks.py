@@ -385,10 +385,10 @@ def barrel_small(seed: int = 0, n_circ: int = 72, n_axial: int = 24, **kw) -> Mo
 
 
 def serving_families(seed: int = 0, scale: float = 1.0):
-    """Eight model families spanning ~2k to ~500k elements (plate, panel, barrel)."""
+    """Eight model families spanning 2k to 500k elements (plate, panel, barrel)."""
     fams = []
-    specs = [("plate", 40), ("plate", 100), ("panel", 0.5), ("panel", 1.0),
-             ("barrel", (240, 96)), ("barrel", (480, 160)), ("barrel", (720, 348)), ("barrel", (960, 522))]
+    specs = [("plate", 45), ("plate", 100), ("panel", 0.5), ("panel", 1.0),
+             ("barrel", (240, 96)), ("barrel", (480, 160)), ("barrel", (720, 348)), ("barrel", (960, 432))]
     for k, (kind, arg) in enumerate(specs):
         if kind == "plate":
             n = max(2, int(round(arg * math.sqrt(scale))))

@@ -27,7 +27,8 @@ EXPORTS = ("jfg_model_create", "jfg_pattern", "jfg_pattern_fill", "jfg_assemble_
            "jfg_dkdh_contract_device", "jfg_dkdh_load_device", "jfg_recover_stresses",
            "jfg_recover_stresses_device", "jfg_kg_contract", "jfg_kg_contract_device", "jfg_server_create", "jfg_server_submit", "jfg_server_wait",
            "jfg_server_result", "jfg_server_release", "jfg_server_stats", "jfg_server_family_batch",
-           "jfg_server_hold", "jfg_server_last_error", "jfg_server_destroy", "jfg_group_create", "jfg_group_member",
+           "jfg_server_hold", "jfg_server_last_error", "jfg_server_destroy", "jfg_group_create", "jfg_group_member", "jfg_autotune", "jfg_launch_config", "jfg_assemble_batch_device_ws",
+           "jfg_shell_thickness", "jfg_server_create_units",
            "jfg_assemble_k_quad4_noalloc", "jfg_model_destroy", "jfg_last_error",
            "jfg_version")
 
@@ -68,6 +69,19 @@ def load(path: str = LIB_PATH):
     L.jfg_group_create.restype = C.c_int32
     L.jfg_group_member.argtypes = [C.c_void_p, C.c_int32, _pi64]
     L.jfg_group_member.restype = C.c_int32
+    _pi32 = C.POINTER(C.c_int32)
+    L.jfg_autotune.argtypes = [C.c_void_p, C.c_int32, _pi32]
+    L.jfg_autotune.restype = C.c_int32
+    L.jfg_launch_config.argtypes = [C.c_void_p, _pi32, _pi32]
+    L.jfg_launch_config.restype = C.c_int32
+    L.jfg_assemble_batch_device_ws.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int64] + [C.c_void_p] * 3 + \
+        [C.c_int64] + [C.c_void_p] * 4
+    L.jfg_assemble_batch_device_ws.restype = C.c_int32
+    L.jfg_shell_thickness.argtypes = [C.c_void_p, _pd]
+    L.jfg_shell_thickness.restype = C.c_int32
+    L.jfg_server_create_units.argtypes = [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int32, _pi32, _pi32, C.c_int32,
+                                          C.c_int64, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
+    L.jfg_server_create_units.restype = C.c_int32
     L.jfg_pattern.argtypes = [C.c_void_p, _pi64, _pi64]
     L.jfg_pattern_fill.argtypes = [C.c_void_p, _pi64, _pi64]
     L.jfg_assemble_k.argtypes = [C.c_void_p, _pd, _pd, _pd]
@@ -187,6 +201,24 @@ class GpuModel:
 
     def __exit__(self, *exc):
         self.close()
+
+    # -- launch shapes -----------------------------------------------------
+    CONFIG_KEYS = ("quad4_warps", "tria3_k_warps", "tria3_kg_threads", "bar_k_threads", "bar_kg_threads")
+
+    def autotune(self, read: bool = True, write: bool = True) -> dict:
+        """Time the candidate CTA shapes on this model and keep the fastest (jfg_autotune)."""
+        c = np.zeros(5, np.int32)
+        flags = (1 if read else 0) | (2 if write else 0)
+        self._check(self.L.jfg_autotune(self.h, flags, c.ctypes.data_as(C.POINTER(C.c_int32))))
+        return dict(zip(self.CONFIG_KEYS, (int(x) for x in c)))
+
+    def launch_config(self, cfg: Optional[dict] = None) -> dict:
+        pi32 = C.POINTER(C.c_int32)
+        cin = None if cfg is None else np.array([cfg[k] for k in self.CONFIG_KEYS], np.int32)
+        c = np.zeros(5, np.int32)
+        self._check(self.L.jfg_launch_config(self.h, None if cin is None else cin.ctypes.data_as(pi32),
+                                             c.ctypes.data_as(pi32)))
+        return dict(zip(self.CONFIG_KEYS, (int(x) for x in c)))
 
     # -- pattern -----------------------------------------------------------
     def pattern(self):
@@ -420,19 +452,35 @@ class Server:
     """
 
     def __init__(self, models, u=None, hbm_budget_bytes: int = 150 * 10**9, max_batch: int = 32,
-                 policy: int = SERVE_BATCHED):
+                 policy: int = SERVE_BATCHED, family_map=None):
+        """models: the launch units (GpuModel or GpuGroup handles), u: one
+        displacement field per unit (the group's concatenation for a group) or
+        None.  family_map: per family (unit, member), member -1 for a plain
+        handle; by default one plain unit per family (jfg_server_create_units)."""
         self.L = load()
         self.models = list(models)
         n = len(self.models)
+        fmap = family_map if family_map is not None else [(i, -1) for i in range(n)]
         hs = (C.c_void_p * n)(*[m.h.value for m in self.models])
         self._u = [None if (u is None or u[i] is None) else np.ascontiguousarray(u[i], np.float64) for i in range(n)]
         us = (C.c_void_p * n)(*[None if a is None else a.ctypes.data for a in self._u])
+        fu = np.array([f[0] for f in fmap], np.int32)
+        fm = np.array([f[1] for f in fmap], np.int32)
         out = C.c_void_p()
-        st = self.L.jfg_server_create(hs, us, n, int(hbm_budget_bytes), int(max_batch), int(policy), C.byref(out))
+        pi32 = C.POINTER(C.c_int32)
+        st = self.L.jfg_server_create_units(hs, us, n, fu.ctypes.data_as(pi32), fm.ctypes.data_as(pi32), len(fmap),
+                                            int(hbm_budget_bytes), int(max_batch), int(policy), C.byref(out))
         if st != 0:
-            raise JfgError(st, "jfg_server_create failed (status %d)" % st)
+            raise JfgError(st, "jfg_server_create_units failed (status %d)" % st)
         self.s = out.value
-        self.n_shell = [int(m.counts[1] + m.counts[2]) for m in self.models]
+        self.n_shell = []
+        for uidx, mem in fmap:
+            g = self.models[uidx]
+            if mem < 0:
+                self.n_shell.append(int(g.counts[1] + g.counts[2]))
+            else:
+                mm = g.models[mem]
+                self.n_shell.append(int(mm.q4_nodes.shape[0] + mm.t3_nodes.shape[0]))
 
     def _check(self, st: int):
         if st != 0:
@@ -464,7 +512,7 @@ class Server:
     def stats(self) -> dict:
         o = np.zeros(6, np.int64)
         self._check(self.L.jfg_server_stats(self.s, _ptr(o, _pi64)))
-        return dict(zip(("submitted", "completed", "batches", "max_batch", "reserved_bytes", "queued"), o.tolist()))
+        return dict(zip(("submitted", "completed", "batches", "max_batch", "pool_peak_bytes", "queued"), o.tolist()))
 
     def hold(self, on: bool = True):
         """Queue requests without launching them while on; off admits the queue."""

@@ -7,6 +7,7 @@ equal, bit for bit, the same request assembled alone on a fresh handle with
 that thickness vector.  The serial policy must give the same bits.
 """
 import ctypes as C
+import time
 
 import numpy as np
 import pytest
@@ -111,3 +112,75 @@ def test_server_rejects_bad_requests(cuda_device):
     finally:
         for g in models:
             g.close()
+
+
+def test_grouped_families_share_batches(cuda_device):
+    """Three small families as members of one group handle: a burst runs as
+    batches that mix families, and every request still equals itself alone."""
+    fams = _families()
+    us = [decks.smooth_displacement(m, seed=10 + i) for i, m in enumerate(fams)]
+    reqs = _requests(fams, 15, seed=6)
+    g = native.GpuGroup(fams)
+    try:
+        with native.Server([g], [np.concatenate(us)], hbm_budget_bytes=8 * 10**9, max_batch=8,
+                           family_map=[(0, i) for i in range(len(fams))]) as srv:
+            srv.hold(True)
+            tickets = [srv.submit(f, np.concatenate([hq, ht])) for f, hq, ht in reqs]
+            srv.hold(False)
+            got = []
+            for t, (f, _, _) in zip(tickets, reqs):
+                assert srv.wait(t, timeout=120.0)
+                pk, pkg, _, _ = srv.result(t)
+                nnz = g.member(f)["nnz"]
+                got.append((_d2h(pk, nnz), _d2h(pkg, nnz)))
+                srv.release(t)
+            st = srv.stats()
+    finally:
+        g.close()
+    counts = np.bincount([f for f, _, _ in reqs], minlength=len(fams))
+    assert st["completed"] == len(reqs) and st["batches"] <= int(np.ceil(counts.max() / 8)) + 1
+    for (f, hq, ht), (k, kg) in zip(reqs, got):
+        k1, kg1 = _alone(fams[f], hq, ht, us[f])
+        assert np.array_equal(k, k1) and np.array_equal(kg, kg1)
+
+
+def test_pool_admits_requests_as_memory_frees(cuda_device):
+    """A budget that holds about two variants of the largest family: a burst
+    is served in small batches as batches finish and results are released,
+    the pool never exceeds the budget, and the results stay exact."""
+    fams = _families()
+    us = [decks.smooth_displacement(m, seed=10 + i) for i, m in enumerate(fams)]
+    models = [native.GpuModel(m) for m in fams]
+    big = max(range(len(fams)), key=lambda i: models[i].nnz)
+    per = models[big].batch_workspace_bytes(1) + 8 * (2 * models[big].nnz + 1 + models[big].counts[1] + models[big].counts[2])
+    budget = int(2.5 * per)
+    reqs = [r for r in _requests(fams, 12, seed=8)]
+    try:
+        with native.Server(models, us, hbm_budget_bytes=budget, max_batch=8) as srv:
+            assert srv.batch_limit(big) == 2
+            srv.hold(True)
+            tickets = [srv.submit(f, np.concatenate([hq, ht])) for f, hq, ht in reqs]
+            srv.hold(False)
+            # results in completion order: a batch's result memory returns to
+            # the pool once all of its requests are released
+            got, todo = {}, dict(enumerate(tickets))
+            deadline = time.monotonic() + 300.0
+            while todo and time.monotonic() < deadline:
+                for i, t in list(todo.items()):
+                    if srv.wait(t, timeout=0.0):
+                        f = reqs[i][0]
+                        pk, pkg, _, _ = srv.result(t)
+                        got[i] = (_d2h(pk, models[f].nnz), _d2h(pkg, models[f].nnz))
+                        srv.release(t)
+                        del todo[i]
+                time.sleep(0.001)
+            assert not todo
+            got = [got[i] for i in range(len(reqs))]
+            st = srv.stats()
+    finally:
+        for m in models:
+            m.close()
+    assert st["completed"] == len(reqs) and st["pool_peak_bytes"] <= budget and st["max_batch"] <= 2
+    for (f, hq, ht), (k, kg) in zip(reqs, got):
+        k1, kg1 = _alone(fams[f], hq, ht, us[f])
+        assert np.array_equal(k, k1) and np.array_equal(kg, kg1)
