@@ -54,6 +54,8 @@ def parse_args():
     p.add_argument("--workload", choices=["barrel", "barrel_medium", "barrel_small", "panel", "plate", "serving", "variants",
                                           "group"], default="barrel")
     p.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
+    p.add_argument("--split", choices=["replicas", "rows"], default="replicas",
+                   help="N>1: one model replica per GPU (weak scaling) or one model's row blocks over the GPUs (strong)")
     p.add_argument("--group-variants", type=int, default=4, help="group: design variants of every member per launch")
     p.add_argument("--rates", type=str, default="100,1000,5000", help="serving: Poisson arrival rates, req/s")
     p.add_argument("--requests", type=int, default=256, help="serving: requests per rate (server arms)")
@@ -832,6 +834,13 @@ def main():
 
     fp64_peak = measure_fp64_peak(torch, dev)
     m = make_model(args.workload, seed=rank)
+    part = full = None
+    if args.split == "rows" and world > 1:
+        # one model over the GPUs: this rank assembles the elements of its row block
+        from jf_2026_05_19_b200 import partition
+        full = make_model(args.workload, seed=0)
+        part = partition.part_of(full, rank, world)
+        m = part.model
     g = native.GpuModel(m)
     t_tune = time.perf_counter()
     launch_cfg = g.launch_config() if args.no_autotune else g.autotune()
@@ -921,8 +930,31 @@ def main():
     rec_ms = s3.elapsed_time(e3) / 5
 
     n_el = m.n_elements
-    value = world * n_el * args.steps / elapsed
-    e2e_value = world * n_el * e2e_steps / e2e_el
+    value = (full.n_elements if part else world * n_el) * args.steps / elapsed
+    gather_ms = None
+    if part is not None:
+        # the one exchange of the split: every rank's owned K columns to every rank
+        cp, _ = g.pattern()
+        a, b = int(cp[part.dof_lo] - 1), int(cp[part.dof_hi] - 1)
+        n_own = torch.tensor([b - a], device=dev)
+        n_all = [torch.zeros_like(n_own) for _ in range(world)]
+        dist.all_gather(n_all, n_own)
+        width = int(max(int(x.item()) for x in n_all))
+        send = torch.zeros(width, dtype=torch.float64, device=dev)
+        send[:b - a] = nz_k[a:b]
+        recv = torch.empty(world * width, dtype=torch.float64, device=dev)
+        dist.all_gather_into_tensor(recv, send)
+        torch.cuda.synchronize()
+        dist.barrier()
+        ga = torch.cuda.Event(enable_timing=True); gb = torch.cuda.Event(enable_timing=True)
+        ga.record(stream)
+        with torch.cuda.stream(stream):
+            dist.all_gather_into_tensor(recv, send)
+        gb.record(stream)
+        gb.synchronize()
+        gather_ms = max_over_ranks(ga.elapsed_time(gb) / 1e3, dist, dev) * 1e3
+        del send, recv
+    e2e_value = (full.n_elements if part else world * n_el) * e2e_steps / e2e_el
     e2e_pinned_value = world * n_el * e2e_steps / e2e_pinned_el
     # dominant kernel over the timed region
     per_kernel = {}
@@ -966,15 +998,24 @@ def main():
     launches_per_step = (sum(1 for t in ("quad4", "tria3", "bar") if counts[t] > 0) * 2
                          + 2 * (1 if st["dof_contribs"] else 0) + 2 + 1)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong" if part else "weak",
+            "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded deck generator; smooth seeded displacement for KG)",
-            "config": dict(workload_config(m, args.workload, world), parallelism=f"replicas x{world}", nnz=g.nnz),
+            "config": (dict(workload_config(m, args.workload, world), parallelism=f"replicas x{world}", nnz=g.nnz)
+                       if part is None else
+                       dict(workload_config(full, args.workload, 1), parallelism=f"row blocks x{world}",
+                            part_elements_rank0=int(n_el), halo_elements=int(sum(
+                                partition.part_of(full, r, world).model.n_elements for r in range(world))
+                                - full.n_elements))),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": e2e_steps, "host_memory": "pageable (numpy arrays, as a Julia Vector{Float64})",
                     "pinned_value": e2e_pinned_value},
             "roofline": roof, "gpu_launches": launches_per_step * args.steps, "clocks": clk,
             "kernel_ms": per_kernel, "fp64_dgemm_tflops": fp64_peak, "model_stats": st,
             "launch_config": dict(launch_cfg, autotuned=not args.no_autotune, tune_s=round(t_tune, 3)),
+            **({"row_split": {"gather_owned_k_ms": gather_ms, "note": "NCCL all-gather of every rank's owned K "
+                              "columns, timed once after the step; the assembly itself has no collective"}}
+               if part is not None else {}),
             "whole_step_roofline": {"flops": roofline.flops_per_step(counts), "bytes": roofline.bytes_per_step(counts, g.nnz)},
             "recovery": {"ms": rec_ms, "elements_per_s": n_el / rec_ms * 1e3, "timed_calls": 5,
                          "output_bytes": 8 * (rec_sh.numel() + (rec_bar.numel() if counts["bar"] else 0)),
