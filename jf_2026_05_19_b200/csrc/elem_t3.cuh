@@ -52,8 +52,9 @@ struct __align__(16) T3KShared {
             double Dd[3][4][4], ivd[3][4], zs[3][4], W[3][6];
         } q;
         struct {  // condensation (phases 4-6)
-            double X[12][9];
+            double X[12][9];   // Kii^-1 Kie; the stiffness kernel keeps z = L^-1 Kie here
             double Kc[9][9];
+            double dk[12];     // pivots of the stiffness kernel's elimination
         } c;
     } u;
     // quad q, local node pair (a <= b): 3x3 over (w, theta_x, theta_y);
@@ -186,6 +187,73 @@ __device__ __forceinline__ void t3_condense(T3KShared &S, int tl, unsigned tm) {
     __syncwarp(tm);
 }
 
+// Condensed plate stiffness Kc = Kee - Kei Kii^-1 Kie into S.u.c.Kc, for the
+// stiffness kernel.  Kii is symmetric positive definite and Kei = Kie' (both
+// read from the same stored quad blocks), so only a forward elimination is
+// needed: with Kii = L D L', Kei Kii^-1 Kie = sum_k z_k z_k' / d_k, z = L^-1
+// Kie.  Lane r < 12 holds row r of [Kii | Kie] and eliminates below the
+// diagonal pivots; the row it holds when it is the pivot row is (u_k, z_k)
+// and its pivot d_k.  Kc is formed symmetric: 45 entries, the diagonal
+// blocks' lower triangles mirrored.
+__device__ __forceinline__ void t3_schur(T3KShared &S, int tl, unsigned tm) {
+    const bool act = tl < 12;
+    const int nA = 3 + tl / 3, ci = tl - 3 * (tl / 3);
+    double row[21];
+#pragma unroll
+    for (int c = 0; c < 21; ++c) row[c] = 0.0;
+    if (act) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            int la = -1;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (t3_quad_node(q, k) == nA) la = k;
+            if (la >= 0) {
+#pragma unroll
+                for (int kb = 0; kb < 4; ++kb) {
+                    const int nB = t3_quad_node(q, kb);
+                    const int cb0 = nB >= 3 ? 3 * (nB - 3) : 12 + 3 * nB;
+                    const bool tr = la > kb;
+                    const int pid = tr ? packed_index(kb, la, 4) : packed_index(la, kb, 4);
+#pragma unroll
+                    for (int cj = 0; cj < 3; ++cj) row[cb0 + cj] += S.Pb[q][pid][tr ? 3 * cj + ci : 3 * ci + cj];
+                }
+            }
+        }
+    }
+    double diag = 1.0;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+        const double akk = __shfl_sync(tm, row[k], k, 16);
+        if (tl == k) diag = akk;
+        const double f = (act && tl > k) ? row[k] / akk : 0.0;
+#pragma unroll
+        for (int j = k + 1; j < 21; ++j) {
+            const double pj = __shfl_sync(tm, row[j], k, 16);
+            row[j] -= f * pj;
+        }
+    }
+    __syncwarp(tm);  // every lane is past its last read of the quad data
+    if (act) {
+#pragma unroll
+        for (int c = 0; c < 9; ++c) S.u.c.X[tl][c] = row[12 + c];
+        S.u.c.dk[tl] = 1.0 / diag;
+    }
+    __syncwarp(tm);
+    // item it < 45: upper-triangle entry (r, c) of the 9x9, row-major
+    for (int it = tl; it < 45; it += T3_TEAM) {
+        int r = 0, rem = it;
+        while (rem >= 9 - r) { rem -= 9 - r; ++r; }
+        const int c = r + rem;
+        const int cr = r / 3, cc = c / 3;
+        double s = (cr == cc) ? S.Pb[cr][0][3 * (r - 3 * cr) + (c - 3 * cc)] : 0.0;
+#pragma unroll
+        for (int k = 0; k < 12; ++k) s -= S.u.c.X[k][r] * (S.u.c.X[k][c] * S.u.c.dk[k]);
+        S.u.c.Kc[r][c] = s;
+        S.u.c.Kc[c][r] = s;
+    }
+}
+
 // Sub-block (bi, bj) of a node-pair 6x6 block into a staged slot buffer of
 // 36 values in stored orientation (transposed when the slot says so).
 __device__ __forceinline__ void stage_sub_block(double *buf, bool t, int bi, int bj, const double O[3][3], double &lmax) {
@@ -265,21 +333,9 @@ __global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t n
     if (plate) {
         t3_plate_points(S, tl, tm, x, y, cs, cb, macneal);
         t3_plate_blocks(S, tl, tm, cb, nu, gam, macneal);
-        t3_condense(S, tl, tm);
-
-        // Phase 4: Kcond = Kee - Kei X (Kee, Kei from the corner's own quad).
-        for (int it = tl; it < 81; it += T3_TEAM) {
-            const int r = it / 9, col = it - 9 * r;
-            const int c = r / 3, i = r - 3 * c, c2 = col / 3, j = col - 3 * c2;
-            double kee = (c == c2) ? S.Pb[c][0][3 * i + j] : 0.0;
-            double s = 0.0;
-            for (int kl = 1; kl < 4; ++kl) {
-                const int l0 = 3 * (c_t3_quads[c][kl] - 3);
-#pragma unroll
-                for (int lj = 0; lj < 3; ++lj) s += S.Pb[c][kl][3 * i + lj] * S.u.c.X[l0 + lj][col];
-            }
-            S.u.c.Kc[r][col] = kee - s;
-        }
+        // Phases 3-4: Kcond = Kee - Kei Kii^-1 Kie by symmetric elimination
+        // (Kee and Kei from the corner's own quad)
+        t3_schur(S, tl, tm);
     }
     __syncwarp(tm);
 
