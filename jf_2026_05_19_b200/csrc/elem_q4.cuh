@@ -71,16 +71,6 @@ struct ElemOut {
     int64_t u_stride = 0;                // per-variant displacement stride (ndof)
     bool kg_layout = false;              // KG staging layout (see blk_entry), else K's
     double *kg_rot = nullptr;            // KG: rotation sub-blocks of bar pairs (27 doubles per bar pair)
-    // Direct blocks (CQUAD4 kernels): a global block whose only contribution
-    // is one CQUAD4 pair needs no reduction; the pair's lane writes it into
-    // the CSC values itself and the block reduction skips it.  pair_block
-    // (per CQUAD4 element pair) holds that block's index or -1; null stages
-    // every pair.
-    const int32_t *pair_block = nullptr;
-    const int64_t *blk_pa = nullptr, *blk_pb = nullptr;  // CSC positions of (6A, 6B) and (6B, 6A), -1 when A == B
-    const int2 *blk_len = nullptr;       // row lengths of A's and B's rows
-    double *nz = nullptr;                // CSC values (per variant: + v * nz_stride)
-    int64_t nz_stride = 0;
 
     __device__ __forceinline__ ElemOut at(int v) const {
         ElemOut r = *this;
@@ -91,7 +81,6 @@ struct ElemOut {
         if (h) r.h += v * h_stride;
         if (bprop) r.bprop += v * bprop_stride;
         if (kg_rot) r.kg_rot += v * staging_stride;
-        if (nz) r.nz += v * nz_stride;
         return r;
     }
     // Shell thickness of element e: the variant's own, else the property record's.
@@ -413,25 +402,6 @@ __device__ __forceinline__ void bend_pair(const double (*dNx)[4], const double (
     P[2][2] += cb * (Pxx + gam * T11);
 }
 
-// A direct block (see ElemOut::pair_block) from the lane's staged record,
-// VALS values in stored orientation (rows of the lower-numbered node): 36
-// for K (6x6 row-major), 12 for KG (translation 3x3 row-major; a shell's
-// KG rotation rows and columns are zero).  Entry (6A + r, 6B + c) sits at
-// pa + r la + c and its mirror (6B + c, 6A + r) at pb + c lb + r.
-template <int VALS>
-__device__ __forceinline__ void write_direct_block(const ElemOut &o, int32_t k, const double *blk) {
-    const int64_t pa = __ldg(o.blk_pa + k), pb = __ldg(o.blk_pb + k);
-    const int2 l = __ldg(o.blk_len + k);
-#pragma unroll
-    for (int r = 0; r < 6; ++r)
-#pragma unroll
-        for (int c = 0; c < 6; ++c) {
-            const double v = VALS == 36 ? blk[6 * r + c] : ((r < 3 && c < 3) ? blk[3 * r + c] : 0.0);
-            o.nz[pa + (int64_t)r * l.x + c] = v;
-            if (pb >= 0) o.nz[pb + (int64_t)c * l.y + r] = v;
-        }
-}
-
 // W warps per CTA (3 W elements): 4 or 8.  The element records are dynamic
 // shared memory, Q4_TEAMS_PER_WARP * W * sizeof(Q4KShared) bytes.
 template <int W>
@@ -698,8 +668,7 @@ __global__ void __launch_bounds__(32 * W, 16 / W) q4_k_kernel(int64_t nq, const 
             }
         }
     }
-    const int32_t direct = (valid && sl >= 0 && o.pair_block) ? __ldg(o.pair_block + e * 10 + tl) : -1;
-    if (valid) S.slot[tl] = direct >= 0 ? -1 : sl;  // the copy below skips negative slots
+    if (valid) S.slot[tl] = sl;  // the copy below skips negative (RBE2 path) slots
     __syncwarp();
     // chunk ch = 180 team + 18 pair + part; lanes step by 32 = 1 pair + 14 parts.
     // The warp's valid teams are a prefix (elements are consecutive).
@@ -720,7 +689,6 @@ __global__ void __launch_bounds__(32 * W, 16 / W) q4_k_kernel(int64_t nq, const 
             if (pl >= 10) { pl -= 10; ++tm; }
         }
     }
-    if (direct >= 0) write_direct_block<36>(o, direct, buf);
     if (o.maxabs) {
         for (int off = 16; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
         if (lane == 0 && lmax > 0.0) atomic_max_nonneg(o.maxabs, lmax);
@@ -965,7 +933,6 @@ __global__ void __launch_bounds__(32 * W) q4_kg_kernel(int64_t nq, const int32_t
         rot_sparse<0b100011011>(Qa, M, Qb, O);
         sl = __ldg(o.blk_slot + e * 10 + tl);
     }
-    const int32_t direct = (valid && sl >= 0 && o.pair_block) ? __ldg(o.pair_block + e * 10 + tl) : -1;
     __syncwarp();  // every lane is past its last read of the element's record
     if (valid) {
         double lmax = 0.0;
@@ -986,7 +953,7 @@ __global__ void __launch_bounds__(32 * W) q4_kg_kernel(int64_t nq, const int32_t
                 for (int c = 0; c < 3; ++c) buf[3 * r + c] = t ? O[c][r] : O[r][c];
             buf[9] = 0.0; buf[10] = 0.0; buf[11] = 0.0;
         }
-        S.slot[tl] = direct >= 0 ? -1 : sl;  // the copy below skips negative slots
+        S.slot[tl] = sl;
     }
     __syncwarp();
     // chunk ch = 60 team + 6 pair + part; lanes step by 32 = 5 pairs + 2 parts
@@ -1005,7 +972,6 @@ __global__ void __launch_bounds__(32 * W) q4_kg_kernel(int64_t nq, const int32_t
         if (part >= 6) { part -= 6; ++pl; }
         if (pl >= 10) { pl -= 10; ++tm; }
     }
-    if (direct >= 0) write_direct_block<12>(o, direct, reinterpret_cast<const double *>(&S) + 12 * tl);
 }
 
 }  // namespace jfg

@@ -152,16 +152,6 @@ struct jfg_model {
     // bar KG kernels (32, 64 or 128)
     int q4_warps = 4, t3_warps = 4;
     int t3kg_threads = 128, bark_threads = 128, barkg_threads = 128;
-    // direct blocks (jfg::ElemOut::pair_block): per CQUAD4 element pair the
-    // index of its block when that pair is the block's only contribution,
-    // else -1; and the block reduction's list of the other blocks (segment
-    // bounds, CSC positions, row lengths, first bar slot), gathered
-    bool direct = false;
-    int32_t *d_pair_block = nullptr;
-    int64_t n_red = 0, n_direct = 0;
-    int2 *d_red_ab = nullptr, *d_red_len = nullptr;
-    int64_t *d_red_pa = nullptr, *d_red_pb = nullptr;
-    int32_t *d_red_rot = nullptr;
     int64_t staging_len = 0;            // staging doubles per assembly: max(K 36 per slot, KG 12 per slot + 27 per bar pair)
     double *d_staging = nullptr;        // 36 doubles per regular element pair
     int64_t *d_rowptr = nullptr, *d_colind = nullptr;   // 0-based symmetric CSR == CSC
@@ -555,34 +545,6 @@ __global__ void key_pos_kernel(int64_t n, const uint64_t *__restrict__ keys, int
     pos[t] = p;
 }
 
-// Direct blocks: a block whose segment is one CQUAD4 pair.  Marks the pair
-// with the block index and the block as outside the reduction list.
-__global__ void direct_block_kernel(int64_t n_blk, const int32_t *__restrict__ seg, const int32_t *__restrict__ pair_of,
-                                    int64_t pair_t3, int32_t *pair_block, int32_t *in_list) {
-    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n_blk) return;
-    const int32_t a = seg[k], b = seg[k + 1];
-    const bool direct = b - a == 1 && pair_of[a] < pair_t3;
-    if (direct) pair_block[pair_of[a]] = (int32_t)k;
-    in_list[k] = direct ? 0 : 1;
-}
-
-// The block reduction's list: every block still in it, in block order.
-__global__ void red_gather_kernel(int64_t n_blk, const int32_t *__restrict__ flag, const int32_t *__restrict__ at,
-                                  const int32_t *__restrict__ seg, const int32_t *__restrict__ rot,
-                                  const int64_t *__restrict__ pa, const int64_t *__restrict__ pb,
-                                  const int2 *__restrict__ len, int2 *r_ab, int64_t *r_pa, int64_t *r_pb, int2 *r_len,
-                                  int32_t *r_rot) {
-    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n_blk || !flag[k]) return;
-    const int32_t i = at[k];
-    r_ab[i] = make_int2(seg[k], seg[k + 1]);
-    r_pa[i] = pa[k];
-    r_pb[i] = pb[k];
-    r_len[i] = len[k];
-    r_rot[i] = rot[k];
-}
-
 // ---------------------------------------------------------------------------
 // assembly kernels
 // ---------------------------------------------------------------------------
@@ -691,12 +653,10 @@ __device__ __forceinline__ void block_write(int64_t k, int i, const double sr[6]
 // (blk_pos_kernel): (6A + r, 6B + i) sits at pa + r * L_A + i, so the
 // block's CSC positions are loaded together with its segment bounds and the
 // path to the stores is two dependent memory round trips (positions and
-// bounds, then the staged rows).  Block k of the launch is entry k of the
-// reduction list: the blocks that are not written directly by their one
-// CQUAD4 contribution.  Thread (g, i) of a warp sums row i of block
+// bounds, then the staged rows).  Thread (g, i) of a warp sums row i of block
 // 5w + g; the rows meet in shared memory for the column writes.
 template <bool KG>
-__global__ void __launch_bounds__(128, 8) block_reduce1_kernel(int64_t n_blk, const int2 *__restrict__ ab,
+__global__ void __launch_bounds__(128, 8) block_reduce1_kernel(int64_t n_blk, const int32_t *__restrict__ seg,
                                                                const int32_t *__restrict__ rot,
                                                                const int32_t *__restrict__ slot_bar, int64_t kg_rot_off,
                                                                const double *__restrict__ staging,
@@ -717,8 +677,7 @@ __global__ void __launch_bounds__(128, 8) block_reduce1_kernel(int64_t n_blk, co
         p_a = __ldg(pa + k);
         p_b = __ldg(pb + k);
         l = __ldg(len + k);
-        const int2 s0 = __ldg(ab + k);
-        const int32_t a0 = s0.x, b0 = s0.y;
+        const int32_t a0 = __ldg(seg + k), b0 = __ldg(seg + k + 1);
         if (KG) {
             const int32_t aa[1] = {a0}, bb[1] = {b0}, rr[1] = {__ldg(rot + k)};
             double *const tt[1] = {tile};
@@ -893,50 +852,6 @@ cudaError_t set_q4_smem_limits() {
         e = cudaFuncSetAttribute(q4_kg_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(Q4_TEAMS_PER_WARP * 4 * sizeof(Q4GShared)));
     return e;
-}
-
-// Direct blocks (patterns with evenly spaced rows; JFG_DIRECT_BLOCKS=0 in
-// the environment turns them off) and the block reduction's list.  pair_of
-// holds the element pair of every sorted slot.
-jfg_status build_reduction_list(jfg_model *m, const int32_t *pair_of) {
-    const int64_t nb = m->n_blk;
-    if (!nb || !m->blk_even) return JFG_OK;
-    const char *env = std::getenv("JFG_DIRECT_BLOCKS");
-    m->direct = !(env && env[0] == '0') && m->nq > 0;
-    int32_t *d_flag = nullptr, *d_at = nullptr;
-    CK(cudaMallocAsync(&d_flag, sizeof(int32_t) * nb, m->stream));
-    CK(cudaMallocAsync(&d_at, sizeof(int32_t) * nb, m->stream));
-    CK(dalloc(m, &m->d_pair_block, std::max<int64_t>(10 * m->nq, 1)));
-    CK(cudaMemsetAsync(m->d_pair_block, 0xff, sizeof(int32_t) * std::max<int64_t>(10 * m->nq, 1), m->stream));  // -1
-    if (m->direct) {
-        direct_block_kernel<<<(unsigned)cdiv(nb, 256), 256, 0, m->stream>>>(nb, m->d_blk_seg, pair_of, m->pair_t3,
-                                                                            m->d_pair_block, d_flag);
-    } else {
-        std::vector<int32_t> ones(nb, 1);
-        CK(cudaMemcpyAsync(d_flag, ones.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice, m->stream));
-    }
-    CK(cudaGetLastError());
-    CK(exclusive_sum(m, d_flag, d_at, nb));
-    int32_t lf = 0, la = 0;
-    CK(cudaMemcpyAsync(&lf, d_flag + nb - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, m->stream));
-    CK(cudaMemcpyAsync(&la, d_at + nb - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, m->stream));
-    CK(cudaStreamSynchronize(m->stream));
-    m->n_red = (int64_t)la + lf;
-    m->n_direct = nb - m->n_red;
-    const int64_t nr = std::max<int64_t>(m->n_red, 1);
-    CK(dalloc(m, &m->d_red_ab, nr));
-    CK(dalloc(m, &m->d_red_len, nr));
-    CK(dalloc(m, &m->d_red_pa, nr));
-    CK(dalloc(m, &m->d_red_pb, nr));
-    CK(dalloc(m, &m->d_red_rot, nr));
-    red_gather_kernel<<<(unsigned)cdiv(nb, 256), 256, 0, m->stream>>>(nb, d_flag, d_at, m->d_blk_seg, m->d_blk_rot, m->d_blk_pa,
-                                                                      m->d_blk_pb, m->d_blk_len, m->d_red_ab, m->d_red_pa,
-                                                                      m->d_red_pb, m->d_red_len, m->d_red_rot);
-    CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(m->stream));
-    cudaFreeAsync(d_flag, m->stream);
-    cudaFreeAsync(d_at, m->stream);
-    return JFG_OK;
 }
 
 jfg_status validate(jfg_model *m, const jfg_model_desc *d) {
@@ -1365,8 +1280,6 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
         CK(cudaGetLastError());
         slot_bar_kernel<<<(unsigned)cdiv(nbc, 256), 256, 0, m->stream>>>(nbc, d_bv2, m->pair_bar, m->d_slot_bar);
         CK(cudaGetLastError());
-        jfg_status rs = build_reduction_list(m, d_bv2);
-        if (rs) return rs;
     }
     // exception pairs: raw blocks, then dof-level weighted contributions
     m->n_xpair = (int64_t)xpairs.size();
@@ -1672,7 +1585,6 @@ struct Batch {
     double *nz = nullptr;           // [n_var][nnz]
     double *dmax = nullptr;         // [n_var] (K, or null)
     double *ddiag = nullptr;        // [n_var][ndof] (K, or null)
-    bool stage_all = false;         // stage every CQUAD4 pair (callers that read the staged blocks)
 };
 
 Batch single_batch(jfg_model *m) {
@@ -1720,14 +1632,6 @@ jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
         o.diag_slot = m->d_dslot + m->dslot_q4;
         o.h = bt.h;
         o.h_stride = m->nq + m->nt;
-        if (m->direct && !bt.stage_all) {
-            o.pair_block = m->d_pair_block;
-            o.blk_pa = m->d_blk_pa;
-            o.blk_pb = m->d_blk_pb;
-            o.blk_len = m->d_blk_len;
-            o.nz = bt.nz;
-            o.nz_stride = m->nnz;
-        }
         const int W = m->q4_warps;
         const dim3 grid((unsigned)cdiv(m->nq, Q4_TEAMS_PER_WARP * W), nv);
         const size_t smem = (size_t)Q4_TEAMS_PER_WARP * W * (kg ? sizeof(Q4GShared) : sizeof(Q4KShared));
@@ -1742,7 +1646,6 @@ jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
         CK(cudaGetLastError());
     }
     CK(mark(m, 1));
-    o.pair_block = nullptr;
     if (m->nt) {
         o.blk_slot = m->d_blk_slot + m->pair_t3;
         o.diag_slot = m->d_dslot + m->dslot_t3;
@@ -1794,16 +1697,15 @@ jfg_status launch_reduce(jfg_model *m, const Batch &bt, bool kg) {
         const dim3 grid((unsigned)cdiv(cdiv((m->n_blk + 1) / 2, 5), kRedWarps), nv);
         const int64_t rot_off = kg ? 12 * m->n_blk_contrib : 0;
         if (m->blk_even) {
-            // the reduction list: every block not written directly by its one CQUAD4 pair
-            const dim3 grid1((unsigned)cdiv(cdiv(std::max<int64_t>(m->n_red, 1), 5), 4), nv);
-            if (m->n_red && kg)
-                block_reduce1_kernel<true><<<grid1, 128, 0, m->stream>>>(m->n_red, m->d_red_ab, m->d_red_rot, m->d_slot_bar, rot_off,
-                                                                      bt.staging, m->d_red_pa, m->d_red_pb, m->d_red_len, bt.nz,
+            const dim3 grid1((unsigned)cdiv(cdiv(m->n_blk, 5), 4), nv);
+            if (kg)
+                block_reduce1_kernel<true><<<grid1, 128, 0, m->stream>>>(m->n_blk, m->d_blk_seg, m->d_blk_rot, m->d_slot_bar, rot_off,
+                                                                      bt.staging, m->d_blk_pa, m->d_blk_pb, m->d_blk_len, bt.nz,
                                                                       bt.staging_stride, m->nnz);
-            else if (m->n_red)
-                block_reduce1_kernel<false><<<grid1, 128, 0, m->stream>>>(m->n_red, m->d_red_ab, m->d_red_rot, m->d_slot_bar, 0,
-                                                                       bt.staging, m->d_red_pa, m->d_red_pb, m->d_red_len,
-                                                                       bt.nz, bt.staging_stride, m->nnz);
+            else
+                block_reduce1_kernel<false><<<grid1, 128, 0, m->stream>>>(m->n_blk, m->d_blk_seg, m->d_blk_rot, m->d_slot_bar, 0,
+                                                                       bt.staging, m->d_blk_pa, m->d_blk_pb, m->d_blk_len, bt.nz,
+                                                                       bt.staging_stride, m->nnz);
         } else if (kg) {
             block_reduce_kernel<true><<<grid, 32 * kRedWarps, 0, m->stream>>>(
                 m->n_blk, m->d_blk_seg, m->d_blk_rot, m->d_slot_bar, rot_off, bt.staging, m->d_blk_A, m->d_blk_B,
@@ -2208,7 +2110,6 @@ jfg_status jfg_kg_contract_device(jfg_model *m, const double *u_dev, const doubl
     if (st) return st;
     Batch bt = single_batch(m);
     bt.u = u_dev;
-    bt.stage_all = true;  // the contractions read every staged block
     st = launch_elements(m, true, bt);
     if (st) return st;
     if (m->nq && c_q4_dev) {
