@@ -1942,7 +1942,7 @@ namespace {
 // rate, so large copies run through the handle's ring of pinned chunks
 // instead: while the GPU fills chunk i + 1 .. i + 3, host threads move chunk
 // i into the destination.  The ring and the threads are made at first use
-// (JFG_COPY_THREADS sets the thread count, default min(8, cores / 2)).
+// (JFG_COPY_THREADS sets the thread count, default min(16, cores)).
 jfg_status copy_to_host(jfg_model *m, void *dst, const void *src, size_t bytes) {
     cudaPointerAttributes at{};
     const bool pinned = cudaPointerGetAttributes(&at, dst) == cudaSuccess && at.type == cudaMemoryTypeHost;
@@ -1956,7 +1956,7 @@ jfg_status copy_to_host(jfg_model *m, void *dst, const void *src, size_t bytes) 
     if (!m->pin) {
         CK(cudaHostAlloc((void **)&m->pin, R * C, cudaHostAllocDefault));
         for (auto &e : m->pin_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        int n = (int)std::min<unsigned>(8, std::max<unsigned>(1, std::thread::hardware_concurrency() / 2));
+        int n = (int)std::min<unsigned>(16, std::max<unsigned>(1, std::thread::hardware_concurrency()));
         if (const char *env = std::getenv("JFG_COPY_THREADS")) n = std::max(1, std::atoi(env));
         m->copy_pool.reset(new CopyPool(n - 1));
     }
