@@ -374,6 +374,7 @@ def run_reference(args):
             "config": config,
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": cpu.sample_text(args.steps, n_el, el), "phases": cpu.phases(args.steps),
+                             "same_config": True,
                              "note": "reference is Julia 1.12 (absent here); C++ restatement of its algorithm"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -1023,7 +1024,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "barrel":
         v, thr, sample, phases = time_cpu_oracle(m, args.cpu_seconds)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample,
-                                "phases": phases}
+                                "phases": phases, "same_config": True}
         line["recovery"]["cpu_port_elements_per_s"] = time_cpu_recovery()
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -25,14 +25,14 @@ FLOPS = {
 }
 
 # FP64 flops the closed-form kernels actually execute per element (2 DFMA +
-# DADD + DMUL thread instructions, from ncu counters of two launches of each
+# DADD + DMUL thread instructions, from ncu counters of one launch of each
 # kernel on a 240 x 96 barrel; the capture is summarised under profiles/).
 # They divide the same launch time as FLOPS to give the hardware fraction of
 # the FP64 peak beside the canonical-work rate.
 EXECUTED_FLOPS = {
     "quad4_k": 13_503,
     "quad4_kg": 10_134,
-    "tria3_k": 27_734,
+    "tria3_k": 26_007,
 }
 
 NODES = {"quad4": 4, "tria3": 3, "bar": 2}
