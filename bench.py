@@ -54,10 +54,6 @@ def parse_args():
     p.add_argument("--workload", choices=["barrel", "barrel_medium", "barrel_small", "panel", "plate", "serving", "variants",
                                           "group"], default="barrel")
     p.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
-    p.add_argument("--persistent", choices=["auto", "on", "off"], default="auto",
-                   help="persistent CQUAD4 + block-reduction kernel: the autotuner's choice (auto, or off with "
-                        "--no-autotune), or forced")
-    p.add_argument("--chunk-quad4", type=int, default=0, help="persistent kernel: CQUAD4s per chunk (0 = default)")
     p.add_argument("--split", choices=["replicas", "rows"], default="replicas",
                    help="N>1: one model replica per GPU (weak scaling) or one model's row blocks over the GPUs (strong)")
     p.add_argument("--group-variants", type=int, default=4, help="group: design variants of every member per launch")
@@ -850,7 +846,6 @@ def main():
     t_tune = time.perf_counter()
     launch_cfg = g.launch_config() if args.no_autotune else g.autotune()
     t_tune = time.perf_counter() - t_tune
-    launch_cfg.update(g.persistent(None if args.persistent == "auto" else args.persistent == "on", args.chunk_quad4))
     # a dedicated (non-default) stream shared by the library and the timing events
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
@@ -1001,10 +996,8 @@ def main():
     ms_step = elapsed / args.steps * 1e3
     h2d = 8 * m.ndof
     d2h = 8 * g.nnz * 2 + 8 * m.ndof + 8
-    # the persistent kernel replaces the CQUAD4 and block-reduction launches of a call
-    fused = bool(launch_cfg.get("persistent")) and counts["quad4"] > 0
     launches_per_step = (sum(1 for t in ("quad4", "tria3", "bar") if counts[t] > 0) * 2
-                         + 2 * (1 if st["dof_contribs"] else 0) + (0 if fused else 2) + 1)
+                         + 2 * (1 if st["dof_contribs"] else 0) + 2 + 1)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong" if part else "weak",
             "vs_baseline": None, "dtype": "f64",

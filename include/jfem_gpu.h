@@ -417,31 +417,13 @@ jfg_status jfg_shell_thickness(jfg_model *m, double *h_host);
  * element count of the kernel's type) in a text file: JFG_TUNE_FILE, else
  * $HOME/.cache/jfem_b200/launch_tune.txt.  flags: JFG_TUNE_READ takes a stored
  * choice when every kernel's size class has one (no timing); JFG_TUNE_WRITE
- * stores the choice made.  With the chosen shapes it then times a whole K
- * (+ KG) call through the separate kernels against the persistent kernel
- * below, where the model allows it, and keeps the faster (stored under the
- * CQUAD4 size class).  The tuner overwrites the handle's work buffers (its
- * last K / KG values).  cfg_out (5 int32) may be NULL.
+ * stores the choice made.  The tuner overwrites the handle's work buffers
+ * (its last K / KG values).  cfg_out (5 int32) may be NULL.
  * jfg_launch_config sets (cfg_in) and/or reads (cfg_out) the shapes. */
 #define JFG_TUNE_READ 1
 #define JFG_TUNE_WRITE 2
 jfg_status jfg_autotune(jfg_model *m, int32_t flags, int32_t *cfg_out);
 jfg_status jfg_launch_config(jfg_model *m, const int32_t *cfg_in, int32_t *cfg_out);
-
-/* Persistent CQUAD4 + block-reduction kernel.  The separate path writes every
- * staged CQUAD4 block to device memory and sums it in a second kernel; the
- * persistent kernel runs CQUAD4 tiles and block sums as tasks of one launch,
- * chunk by chunk (chunk_quad4 consecutive CQUAD4s), so a block is summed while
- * its staged values are still in L2.  Values are bitwise those of the separate
- * path (same slot order, same arithmetic).  It serves single K / KG calls
- * (host-buffer and device forms) on models whose CSC rows of every node are
- * evenly spaced and that have CQUAD4s; batched calls keep the separate path.
- * The first call after a change of mode, chunk size or CQUAD4 width builds its
- * task list (a synchronous step, so make that call outside a stream capture).
- * mode: -1 keeps, 0 turns off (default), 1 turns on; chunk_quad4 <= 0 keeps
- * the current size (default 9600), else a multiple of 24.  mode_out and
- * chunk_out (may be NULL) receive the settings. */
-jfg_status jfg_persistent_config(jfg_model *m, int32_t mode, int64_t chunk_quad4, int32_t *mode_out, int64_t *chunk_out);
 
 /* ---- Group handles: several models in one launch ------------------------
  * The reference assembles one model per call; its batch drivers loop over

@@ -402,18 +402,21 @@ __device__ __forceinline__ void bend_pair(const double (*dNx)[4], const double (
     P[2][2] += cb * (Pxx + gam * T11);
 }
 
-// One tile of 3 W consecutive CQUAD4s (W warps): the body of q4_k_kernel and
-// of the persistent assembly kernel.  sh = the tile's element records
-// (Q4_TEAMS_PER_WARP * W of them); o is the variant's output.
+// W warps per CTA (3 W elements): 4 or 8.  The element records are dynamic
+// shared memory, Q4_TEAMS_PER_WARP * W * sizeof(Q4KShared) bytes.
 template <int W>
-__device__ __forceinline__ void q4_k_tile(int64_t tile, Q4KShared *sh, int64_t nq, const int32_t *__restrict__ nodes,
-                                          const double *__restrict__ prop, const double *__restrict__ coords,
-                                          const double *__restrict__ nodeR, double k6rot, const ElemOut &o) {
+__global__ void __launch_bounds__(32 * W, 16 / W) q4_k_kernel(int64_t nq, const int32_t *__restrict__ nodes,
+                                                         const double *__restrict__ prop,
+                                                         const double *__restrict__ coords,
+                                                         const double *__restrict__ nodeR, double k6rot, ElemOut o) {
+    extern __shared__ __align__(16) unsigned char q4_smem[];
+    Q4KShared *sh = reinterpret_cast<Q4KShared *>(q4_smem);
+    o = o.at(blockIdx.y);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int team = lane / Q4_TEAM, tl = lane - team * Q4_TEAM;
     const bool in_team = team < Q4_TEAMS_PER_WARP;
     const int slot_id = warp * Q4_TEAMS_PER_WARP + (in_team ? team : 0);
-    const int64_t e = tile * Q4_TEAMS_PER_WARP * W + slot_id;
+    const int64_t e = (int64_t)blockIdx.x * Q4_TEAMS_PER_WARP * W + slot_id;
     const bool valid = in_team && e < nq;
     Q4KShared &S = sh[slot_id];
 
@@ -670,7 +673,7 @@ __device__ __forceinline__ void q4_k_tile(int64_t tile, Q4KShared *sh, int64_t n
     // chunk ch = 180 team + 18 pair + part; lanes step by 32 = 1 pair + 14 parts.
     // The warp's valid teams are a prefix (elements are consecutive).
     {
-        const int64_t p_warp = tile * Q4_TEAMS_PER_WARP * W + warp * Q4_TEAMS_PER_WARP;
+        const int64_t p_warp = (int64_t)blockIdx.x * Q4_TEAMS_PER_WARP * W + warp * Q4_TEAMS_PER_WARP;
         const int64_t n_left = nq - p_warp;
         const int nv = n_left <= 0 ? 0 : (n_left >= Q4_TEAMS_PER_WARP ? Q4_TEAMS_PER_WARP : (int)n_left);
         for (int tm = 0, pl = lane / 18, part = lane % 18; tm < nv;) {
@@ -692,30 +695,22 @@ __device__ __forceinline__ void q4_k_tile(int64_t tile, Q4KShared *sh, int64_t n
     }
 }
 
-// W warps per CTA (3 W elements): 4 or 8.  The element records are dynamic
-// shared memory, Q4_TEAMS_PER_WARP * W * sizeof(Q4KShared) bytes.
+// W warps per CTA (3 W elements): 4 or 8; dynamic shared memory as q4_k_kernel's.
 template <int W>
-__global__ void __launch_bounds__(32 * W, 16 / W) q4_k_kernel(int64_t nq, const int32_t *__restrict__ nodes,
-                                                         const double *__restrict__ prop,
-                                                         const double *__restrict__ coords,
-                                                         const double *__restrict__ nodeR, double k6rot, ElemOut o) {
+__global__ void __launch_bounds__(32 * W) q4_kg_kernel(int64_t nq, const int32_t *__restrict__ nodes,
+                                                          const double *__restrict__ prop,
+                                                          const double *__restrict__ coords,
+                                                          const double *__restrict__ nodeR,
+                                                          const double *__restrict__ u, ElemOut o) {
     extern __shared__ __align__(16) unsigned char q4_smem[];
-    q4_k_tile<W>(blockIdx.x, reinterpret_cast<Q4KShared *>(q4_smem), nq, nodes, prop, coords, nodeR, k6rot,
-                 o.at(blockIdx.y));
-}
-
-// One tile of 3 W consecutive CQUAD4s: the body of q4_kg_kernel and of the
-// persistent assembly kernel (u = the variant's displacement).
-template <int W>
-__device__ __forceinline__ void q4_kg_tile(int64_t tile, Q4GShared *sh, int64_t nq, const int32_t *__restrict__ nodes,
-                                           const double *__restrict__ prop, const double *__restrict__ coords,
-                                           const double *__restrict__ nodeR, const double *__restrict__ u,
-                                           const ElemOut &o) {
+    Q4GShared *sh = reinterpret_cast<Q4GShared *>(q4_smem);
+    o = o.at(blockIdx.y);
+    u += (int64_t)blockIdx.y * o.u_stride;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int team = lane / Q4_TEAM, tl = lane - team * Q4_TEAM;
     const bool in_team = team < Q4_TEAMS_PER_WARP;
     const int slot_id = warp * Q4_TEAMS_PER_WARP + (in_team ? team : 0);
-    const int64_t e = tile * Q4_TEAMS_PER_WARP * W + slot_id;
+    const int64_t e = (int64_t)blockIdx.x * Q4_TEAMS_PER_WARP * W + slot_id;
     const bool valid = in_team && e < nq;
     Q4GShared &S = sh[slot_id];
 
@@ -962,7 +957,7 @@ __device__ __forceinline__ void q4_kg_tile(int64_t tile, Q4GShared *sh, int64_t 
     }
     __syncwarp();
     // chunk ch = 60 team + 6 pair + part; lanes step by 32 = 5 pairs + 2 parts
-    const int64_t p_warp = tile * Q4_TEAMS_PER_WARP * W + warp * Q4_TEAMS_PER_WARP;
+    const int64_t p_warp = (int64_t)blockIdx.x * Q4_TEAMS_PER_WARP * W + warp * Q4_TEAMS_PER_WARP;
     const int64_t n_left = nq - p_warp;
     const int nv = n_left <= 0 ? 0 : (n_left >= Q4_TEAMS_PER_WARP ? Q4_TEAMS_PER_WARP : (int)n_left);
     for (int tm = 0, pl = lane / 6, part = lane % 6; tm < nv;) {
@@ -977,18 +972,6 @@ __device__ __forceinline__ void q4_kg_tile(int64_t tile, Q4GShared *sh, int64_t 
         if (part >= 6) { part -= 6; ++pl; }
         if (pl >= 10) { pl -= 10; ++tm; }
     }
-}
-
-// W warps per CTA (3 W elements): 4 or 8; dynamic shared memory as q4_k_kernel's.
-template <int W>
-__global__ void __launch_bounds__(32 * W) q4_kg_kernel(int64_t nq, const int32_t *__restrict__ nodes,
-                                                          const double *__restrict__ prop,
-                                                          const double *__restrict__ coords,
-                                                          const double *__restrict__ nodeR,
-                                                          const double *__restrict__ u, ElemOut o) {
-    extern __shared__ __align__(16) unsigned char q4_smem[];
-    q4_kg_tile<W>(blockIdx.x, reinterpret_cast<Q4GShared *>(q4_smem), nq, nodes, prop, coords, nodeR,
-                  u + (int64_t)blockIdx.y * o.u_stride, o.at(blockIdx.y));
 }
 
 }  // namespace jfg

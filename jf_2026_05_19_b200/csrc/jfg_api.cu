@@ -152,17 +152,6 @@ struct jfg_model {
     // bar KG kernels (32, 64 or 128)
     int q4_warps = 4, t3_warps = 4;
     int t3kg_threads = 128, bark_threads = 128, barkg_threads = 128;
-    // persistent CQUAD4 + block-reduction kernel (assemble_fused.cuh): on or
-    // off, CQUAD4s per chunk, and the task list built for (q4_warps, chunk)
-    int fz_mode = 0;
-    int64_t fz_chunk = 9600;
-    int fz_built_w = 0;
-    int64_t fz_built_chunk = 0;
-    int4 *d_fz_task = nullptr;
-    int32_t *d_fz_order = nullptr, *d_fz_need = nullptr;
-    int *d_fz_ctr = nullptr;            // error word, claim counter, done E tasks per chunk
-    int64_t fz_n_task = 0, fz_n_chunk = 0;
-    int fz_grid[2][2] = {{0, 0}, {0, 0}};  // persistent CTAs: [K, KG][4 warps, 8 warps]
     int64_t staging_len = 0;            // staging doubles per assembly: max(K 36 per slot, KG 12 per slot + 27 per bar pair)
     double *d_staging = nullptr;        // 36 doubles per regular element pair
     int64_t *d_rowptr = nullptr, *d_colind = nullptr;   // 0-based symmetric CSR == CSC
@@ -206,7 +195,7 @@ struct jfg_model {
     std::vector<double> dep_coef;
     // ring of event sets, one per assembly call, so that per-kernel device
     // times can be accumulated over many back-to-back calls without a sync
-    struct EvSet { cudaEvent_t e[7]; int kind; bool pending; bool fused; };
+    struct EvSet { cudaEvent_t e[7]; int kind; bool pending; };
     static constexpr int kRing = 64;
     EvSet ring[kRing];
     int ring_head = 0, last_set = -1;
@@ -566,26 +555,19 @@ __global__ void key_pos_kernel(int64_t n, const uint64_t *__restrict__ keys, int
 // thread takes two blocks, k and k + half, whose loads are issued together to
 // keep more of them in flight.  The summed rows are then transposed through
 // shared memory and written with block_write.
-// Staged values: through the read-only path when an earlier kernel wrote them
-// (CG = false), through L2 (ld.global.cg) when the persistent kernel's own
-// element tiles did.
-template <bool CG>
-__device__ __forceinline__ double2 ld_stage(const double2 *p) { return CG ? __ldcg(p) : __ldg(p); }
-
-template <bool CG = false>
 __device__ __forceinline__ void block_row_sum(const double *__restrict__ staging, int32_t a, int32_t b, int i, double s[6]) {
     int32_t q = a;
     for (; q + 1 < b; q += 2) {
         const double2 *p0 = reinterpret_cast<const double2 *>(staging + 36 * (int64_t)q + 6 * i);
         const double2 *p1 = reinterpret_cast<const double2 *>(staging + 36 * (int64_t)(q + 1) + 6 * i);
-        const double2 x0 = ld_stage<CG>(p0), x1 = ld_stage<CG>(p0 + 1), x2 = ld_stage<CG>(p0 + 2);
-        const double2 y0 = ld_stage<CG>(p1), y1 = ld_stage<CG>(p1 + 1), y2 = ld_stage<CG>(p1 + 2);
+        const double2 x0 = __ldg(p0), x1 = __ldg(p0 + 1), x2 = __ldg(p0 + 2);
+        const double2 y0 = __ldg(p1), y1 = __ldg(p1 + 1), y2 = __ldg(p1 + 2);
         s[0] += x0.x; s[1] += x0.y; s[2] += x1.x; s[3] += x1.y; s[4] += x2.x; s[5] += x2.y;
         s[0] += y0.x; s[1] += y0.y; s[2] += y1.x; s[3] += y1.y; s[4] += y2.x; s[5] += y2.y;
     }
     if (q < b) {
         const double2 *p0 = reinterpret_cast<const double2 *>(staging + 36 * (int64_t)q + 6 * i);
-        const double2 x0 = ld_stage<CG>(p0), x1 = ld_stage<CG>(p0 + 1), x2 = ld_stage<CG>(p0 + 2);
+        const double2 x0 = __ldg(p0), x1 = __ldg(p0 + 1), x2 = __ldg(p0 + 2);
         s[0] += x0.x; s[1] += x0.y; s[2] += x1.x; s[3] += x1.y; s[4] += x2.x; s[5] += x2.y;
     }
 }
@@ -599,7 +581,7 @@ __device__ __forceinline__ void block_row_sum(const double *__restrict__ staging
 // order.  Bar contributions [rb, b) also carry three rotation sub-blocks:
 // row i < 3 adds them to columns 3-5, row i >= 3 to all six columns.  Shell-only
 // blocks leave zeros there.
-template <int NB, bool CG = false>
+template <int NB>
 __device__ __forceinline__ void block_kg_sums(const double *__restrict__ staging, const double *__restrict__ kg_rot,
                                               const int32_t *__restrict__ slot_bar, const int32_t a[NB], const int32_t rb[NB],
                                               const int32_t b[NB], int i, double *const tt_out[NB]) {
@@ -617,7 +599,7 @@ __device__ __forceinline__ void block_kg_sums(const double *__restrict__ staging
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int32_t q = a[m] + t + u;
-                    x[m][u] = q < b[m] ? ld_stage<CG>(reinterpret_cast<const double2 *>(staging + 12 * (int64_t)q) + i)
+                    x[m][u] = q < b[m] ? __ldg(reinterpret_cast<const double2 *>(staging + 12 * (int64_t)q) + i)
                                        : make_double2(0.0, 0.0);
                 }
 #pragma unroll
@@ -860,8 +842,6 @@ cudaError_t exclusive_sum(jfg_model *m, T *in, U *out, int64_t n) {
 
 // The CQUAD4 kernels keep their element records in dynamic shared memory;
 // the 8-warp forms need more than the default 48 KB.
-#include "assemble_fused.cuh"
-
 cudaError_t set_q4_smem_limits() {
     cudaError_t e = cudaFuncSetAttribute(q4_k_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(Q4_TEAMS_PER_WARP * 8 * sizeof(Q4KShared)));
@@ -871,107 +851,7 @@ cudaError_t set_q4_smem_limits() {
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(q4_kg_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(Q4_TEAMS_PER_WARP * 4 * sizeof(Q4GShared)));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(fused_k_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fz_smem_bytes<8>(false));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(fused_k_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fz_smem_bytes<4>(false));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(fused_kg_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fz_smem_bytes<8>(true));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(fused_kg_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fz_smem_bytes<4>(true));
     return e;
-}
-
-void fz_free(jfg_model *m) {
-    for (void *p : {(void *)m->d_fz_task, (void *)m->d_fz_order, (void *)m->d_fz_need, (void *)m->d_fz_ctr})
-        if (p) cudaFree(p);
-    m->d_fz_task = nullptr;
-    m->d_fz_order = m->d_fz_need = nullptr;
-    m->d_fz_ctr = nullptr;
-    m->fz_n_task = m->fz_n_chunk = 0;
-    m->fz_built_w = 0;
-    m->fz_built_chunk = 0;
-}
-
-// The persistent kernel's sticky error word (a chunk wait that ran out),
-// read after the caller's stream has finished the call.
-jfg_status fz_check(jfg_model *m) {
-    if (!m->d_fz_ctr) return JFG_OK;
-    int err = 0;
-    CK(cudaMemcpy(&err, m->d_fz_ctr, sizeof(int), cudaMemcpyDeviceToHost));
-    if (!err) return JFG_OK;
-    CK(cudaMemset(m->d_fz_ctr, 0, sizeof(int)));
-    return fail(m, JFG_ERR_CUDA, "persistent assembly kernel: a wait for the CQUAD4 tiles of a chunk ran out");
-}
-
-// Task list of the persistent kernel for the handle's CQUAD4 width and chunk
-// size (rebuilt when either changes).  Synchronous; not run under capture.
-jfg_status fz_build(jfg_model *m) {
-    const int W = m->q4_warps;
-    const int64_t chunk = m->fz_chunk, nq = m->nq, n_blk = m->n_blk;
-    if (m->d_fz_task && m->fz_built_w == W && m->fz_built_chunk == chunk) return JFG_OK;
-    if (chunk <= 0 || chunk % 24) return fail(m, JFG_ERR_INVALID, "CQUAD4 chunk size must be a positive multiple of 24");
-    fz_free(m);
-    const int64_t n_chunk = cdiv(nq, chunk);
-    if (n_chunk >= ((int64_t)1 << 29) || n_blk >= ((int64_t)1 << 31) - 1)
-        return fail(m, JFG_ERR_UNSUPPORTED, "model too large for the persistent kernel's task list");
-    int *cmin = nullptr, *cmax = nullptr, *cnt = nullptr, *span = nullptr;
-    int32_t *key = nullptr, *key2 = nullptr, *idx = nullptr;
-    CK(cudaMallocAsync(&cmin, sizeof(int) * n_blk, m->stream));
-    CK(cudaMallocAsync(&cmax, sizeof(int) * n_blk, m->stream));
-    CK(cudaMallocAsync(&cnt, sizeof(int) * (n_chunk + 2), m->stream));
-    CK(cudaMallocAsync(&key, sizeof(int32_t) * n_blk, m->stream));
-    CK(cudaMallocAsync(&key2, sizeof(int32_t) * n_blk, m->stream));
-    CK(cudaMallocAsync(&idx, sizeof(int32_t) * n_blk, m->stream));
-    CK(cudaMalloc(&m->d_fz_order, sizeof(int32_t) * n_blk));
-    span = cnt + n_chunk + 1;
-    CK(cudaMemsetAsync(cmin, 0x7f, sizeof(int) * n_blk, m->stream));
-    CK(cudaMemsetAsync(cmax, 0xff, sizeof(int) * n_blk, m->stream));
-    CK(cudaMemsetAsync(cnt, 0, sizeof(int) * (n_chunk + 2), m->stream));
-    fz_chunk_kernel<<<(unsigned)cdiv(10 * nq, 256), 256, 0, m->stream>>>(nq, chunk, m->d_blk_slot + m->pair_q4, m->d_blk_seg,
-                                                                          n_blk, cmin, cmax);
-    CK(cudaGetLastError());
-    fz_key_kernel<<<(unsigned)cdiv(n_blk, 256), 256, 0, m->stream>>>(n_blk, cmin, cmax, key, idx, cnt, span);
-    CK(cudaGetLastError());
-    int end_bit = 1;
-    while (((int64_t)1 << end_bit) <= n_chunk + 1) ++end_bit;
-    CK(radix_sort(m, key, key2, idx, m->d_fz_order, n_blk, end_bit));
-    std::vector<int> h_cnt(n_chunk + 2);
-    CK(cudaMemcpyAsync(h_cnt.data(), cnt, sizeof(int) * (n_chunk + 2), cudaMemcpyDeviceToHost, m->stream));
-    CK(cudaStreamSynchronize(m->stream));
-    for (void *p : {(void *)cmin, (void *)cmax, (void *)cnt, (void *)key, (void *)key2, (void *)idx}) cudaFreeAsync(p, m->stream);
-    const int S = h_cnt[n_chunk + 1];
-    // offsets of each completion key (chunk + 1) in the sorted order
-    std::vector<int64_t> off(n_chunk + 2, 0);
-    for (int64_t c = 0; c <= n_chunk; ++c) off[c + 1] = off[c] + h_cnt[c];
-    const int64_t rt = (int64_t)kFzRounds * W * 5, tile = 3 * W, per_chunk = chunk / tile, n_tiles = cdiv(nq, tile);
-    std::vector<int4> task;
-    std::vector<int32_t> need(n_chunk, 0);
-    auto push_r = [&](int64_t k) {  // blocks completing at chunk k - 1
-        const int lo = k >= 1 ? (int)std::max<int64_t>(0, k - 1 - S) : 0;
-        for (int64_t j = off[k]; j < off[k + 1]; j += rt)
-            task.push_back(make_int4((int)(k << 1) | 1, (int)j, (int)std::min(j + rt, off[k + 1]), lo));
-    };
-    push_r(0);
-    for (int64_t c = 0; c < n_chunk; ++c) {
-        for (int64_t t = c * per_chunk; t < std::min((c + 1) * per_chunk, n_tiles); ++t) {
-            task.push_back(make_int4((int)(c << 1), (int)t, (int)t + 1, 0));
-            ++need[c];
-        }
-        if (c >= 1) push_r(c);
-    }
-    push_r(n_chunk);
-    CK(cudaMalloc(&m->d_fz_task, sizeof(int4) * task.size()));
-    CK(cudaMalloc(&m->d_fz_need, sizeof(int32_t) * std::max<int64_t>(n_chunk, 1)));
-    CK(cudaMalloc(&m->d_fz_ctr, sizeof(int) * (2 + n_chunk)));
-    CK(cudaMemcpy(m->d_fz_task, task.data(), sizeof(int4) * task.size(), cudaMemcpyHostToDevice));
-    if (n_chunk) CK(cudaMemcpy(m->d_fz_need, need.data(), sizeof(int32_t) * n_chunk, cudaMemcpyHostToDevice));
-    CK(cudaMemset(m->d_fz_ctr, 0, sizeof(int) * (2 + n_chunk)));
-    m->fz_n_task = (int64_t)task.size();
-    m->fz_n_chunk = n_chunk;
-    m->fz_built_w = W;
-    m->fz_built_chunk = chunk;
-    return JFG_OK;
 }
 
 jfg_status validate(jfg_model *m, const jfg_model_desc *d) {
@@ -1042,7 +922,6 @@ void jfg_model_destroy(jfg_model *m) {
     if (m->stream) cudaStreamSynchronize(m->stream);
     for (void *p : m->allocs) cudaFree(p);
     if (m->d_bw) cudaFree(m->d_bw);
-    fz_free(m);
     for (auto &set : m->ring)
         for (auto &e : set.e)
             if (e) cudaEventDestroy(e);
@@ -1071,7 +950,6 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
     for (auto &set : m->ring) {
         for (auto &e : set.e) CK(cudaEventCreate(&e));
         set.pending = false;
-        set.fused = false;
         set.kind = 0;
     }
     m->n_nodes = d->n_nodes;
@@ -1734,7 +1612,8 @@ BatchSizes batch_sizes(const jfg_model *m) {
 // Timing event i of the current set (skipped while the stream is captured).
 cudaError_t mark(jfg_model *m, int i) { return m->capturing ? cudaSuccess : cudaEventRecord(m->ev[i], m->stream); }
 
-ElemOut elem_out(jfg_model *m, bool kg, const Batch &bt) {
+jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
+    const unsigned nv = (unsigned)bt.n_var;
     ElemOut o;
     o.staging = bt.staging;
     o.exc_raw = bt.exc_raw;
@@ -1746,100 +1625,72 @@ ElemOut elem_out(jfg_model *m, bool kg, const Batch &bt) {
     o.u_stride = bt.u_stride < 0 ? m->ndof : bt.u_stride;
     o.kg_layout = kg;
     o.kg_rot = kg ? bt.staging + 12 * m->n_blk_contrib : nullptr;
-    return o;
-}
-
-ElemOut q4_out(jfg_model *m, ElemOut o, const Batch &bt) {
-    o.blk_slot = m->d_blk_slot + m->pair_q4;
-    o.diag_slot = m->d_dslot + m->dslot_q4;
-    o.h = bt.h;
-    o.h_stride = m->nq + m->nt;
-    return o;
-}
-
-void launch_t3(jfg_model *m, bool kg, const Batch &bt, ElemOut o) {
-    const unsigned nv = (unsigned)bt.n_var;
-    o.blk_slot = m->d_blk_slot + m->pair_t3;
-    o.diag_slot = m->d_dslot + m->dslot_t3;
-    o.h = bt.h ? bt.h + m->nq : nullptr;
-    o.h_stride = m->nq + m->nt;
-    const int tt = m->t3kg_threads, W3 = m->t3_warps;
-    if (kg)
-        t3_kg_kernel<<<dim3((unsigned)cdiv(6 * m->nt, tt), nv), tt, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords,
-                                                                               m->d_nodeR, bt.u, o);
-    else if (W3 == 2)
-        t3_k_kernel<2><<<dim3((unsigned)cdiv(m->nt, T3_TEAMS_PER_WARP * 2), nv), 64, 0, m->stream>>>(
-            m->nt, m->d_t3n, m->d_t3p, m->d_coords, m->d_nodeR, m->k6rot, o);
-    else
-        t3_k_kernel<4><<<dim3((unsigned)cdiv(m->nt, T3_TEAMS_PER_WARP * 4), nv), 128, 0, m->stream>>>(
-            m->nt, m->d_t3n, m->d_t3p, m->d_coords, m->d_nodeR, m->k6rot, o);
-}
-
-void launch_bar(jfg_model *m, bool kg, const Batch &bt, ElemOut o) {
-    const unsigned nv = (unsigned)bt.n_var;
-    o.blk_slot = m->d_blk_slot + m->pair_bar;
-    o.diag_slot = m->d_dslot + m->dslot_bar;
-    o.h = nullptr;
-    o.bprop = bt.bprop;
-    o.bprop_stride = JFG_BAR_PROP * m->nb;
-    const int bt_ = kg ? m->barkg_threads : m->bark_threads;
-    dim3 grid((unsigned)cdiv(3 * m->nb, bt_), nv);
-    if (kg)
-        bar_kg_kernel<<<grid, bt_, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, bt.u, o);
-    else
-        bar_k_kernel<<<grid, bt_, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, o);
-}
-
-jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
-    const unsigned nv = (unsigned)bt.n_var;
-    const ElemOut o = elem_out(m, kg, bt);
     const double *du = bt.u;
     CK(mark(m, 0));
     if (m->nq) {
-        const ElemOut oq = q4_out(m, o, bt);
+        o.blk_slot = m->d_blk_slot + m->pair_q4;
+        o.diag_slot = m->d_dslot + m->dslot_q4;
+        o.h = bt.h;
+        o.h_stride = m->nq + m->nt;
         const int W = m->q4_warps;
         const dim3 grid((unsigned)cdiv(m->nq, Q4_TEAMS_PER_WARP * W), nv);
         const size_t smem = (size_t)Q4_TEAMS_PER_WARP * W * (kg ? sizeof(Q4GShared) : sizeof(Q4KShared));
         if (kg && W == 8)
-            q4_kg_kernel<8><<<grid, 32 * W, smem, m->stream>>>(m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, du, oq);
+            q4_kg_kernel<8><<<grid, 32 * W, smem, m->stream>>>(m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, du, o);
         else if (kg)
-            q4_kg_kernel<4><<<grid, 32 * W, smem, m->stream>>>(m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, du, oq);
+            q4_kg_kernel<4><<<grid, 32 * W, smem, m->stream>>>(m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, du, o);
         else if (W == 8)
-            q4_k_kernel<8><<<grid, 32 * W, smem, m->stream>>>(m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, m->k6rot, oq);
+            q4_k_kernel<8><<<grid, 32 * W, smem, m->stream>>>(m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, m->k6rot, o);
         else
-            q4_k_kernel<4><<<grid, 32 * W, smem, m->stream>>>(m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, m->k6rot, oq);
+            q4_k_kernel<4><<<grid, 32 * W, smem, m->stream>>>(m->nq, m->d_q4n, m->d_q4p, m->d_coords, m->d_nodeR, m->k6rot, o);
         CK(cudaGetLastError());
     }
     CK(mark(m, 1));
     if (m->nt) {
-        launch_t3(m, kg, bt, o);
+        o.blk_slot = m->d_blk_slot + m->pair_t3;
+        o.diag_slot = m->d_dslot + m->dslot_t3;
+        o.h = bt.h ? bt.h + m->nq : nullptr;
+        o.h_stride = m->nq + m->nt;
+        const int tt = m->t3kg_threads, W3 = m->t3_warps;
+        if (kg)
+            t3_kg_kernel<<<dim3((unsigned)cdiv(6 * m->nt, tt), nv), tt, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords,
+                                                                                   m->d_nodeR, du, o);
+        else if (W3 == 2)
+            t3_k_kernel<2><<<dim3((unsigned)cdiv(m->nt, T3_TEAMS_PER_WARP * 2), nv), 64, 0, m->stream>>>(
+                m->nt, m->d_t3n, m->d_t3p, m->d_coords, m->d_nodeR, m->k6rot, o);
+        else
+            t3_k_kernel<4><<<dim3((unsigned)cdiv(m->nt, T3_TEAMS_PER_WARP * 4), nv), 128, 0, m->stream>>>(
+                m->nt, m->d_t3n, m->d_t3p, m->d_coords, m->d_nodeR, m->k6rot, o);
         CK(cudaGetLastError());
     }
     CK(mark(m, 2));
     if (m->nb) {
-        launch_bar(m, kg, bt, o);
+        o.blk_slot = m->d_blk_slot + m->pair_bar;
+        o.diag_slot = m->d_dslot + m->dslot_bar;
+        o.h = nullptr;
+        o.bprop = bt.bprop;
+        o.bprop_stride = JFG_BAR_PROP * m->nb;
+        const int bt_ = kg ? m->barkg_threads : m->bark_threads;
+        dim3 grid((unsigned)cdiv(3 * m->nb, bt_), nv);
+        if (kg)
+            bar_kg_kernel<<<grid, bt_, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, du, o);
+        else
+            bar_k_kernel<<<grid, bt_, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, o);
         CK(cudaGetLastError());
     }
     CK(mark(m, 3));
     return JFG_OK;
 }
 
-void launch_exc(jfg_model *m, const Batch &bt) {
-    const unsigned nv = (unsigned)bt.n_var;
-    exc_chunk_kernel<<<dim3((unsigned)cdiv(m->n_xchunk * 32, 256), nv), 256, 0, m->stream>>>(
-        m->n_xchunk, m->d_x_cseg, m->d_x_src, m->d_x_w, bt.exc_raw, bt.x_part, bt.exc_stride, bt.part_stride);
-    exc_key_kernel<<<dim3((unsigned)cdiv(m->n_xkey * 32, 256), nv), 256, 0, m->stream>>>(
-        m->n_xkey, m->d_x_kchunk, bt.x_part, m->d_x_pos, bt.nz, bt.part_stride, m->nnz);
-}
-
-void launch_diag(jfg_model *m, const Batch &bt) {
-    diag_reduce_kernel<<<dim3((unsigned)cdiv(m->ndof, 256), (unsigned)bt.n_var), 256, 0, m->stream>>>(
-        m->ndof, m->d_dseg, bt.dstaging, bt.ddiag, bt.dstage_stride);
-}
-
 jfg_status launch_reduce(jfg_model *m, const Batch &bt, bool kg) {
     const unsigned nv = (unsigned)bt.n_var;
-    if (m->n_xkey) launch_exc(m, bt);
+    if (m->n_xkey) {
+        exc_chunk_kernel<<<dim3((unsigned)cdiv(m->n_xchunk * 32, 256), nv), 256, 0, m->stream>>>(
+            m->n_xchunk, m->d_x_cseg, m->d_x_src, m->d_x_w, bt.exc_raw, bt.x_part, bt.exc_stride, bt.part_stride);
+        CK(cudaGetLastError());
+        exc_key_kernel<<<dim3((unsigned)cdiv(m->n_xkey * 32, 256), nv), 256, 0, m->stream>>>(
+            m->n_xkey, m->d_x_kchunk, bt.x_part, m->d_x_pos, bt.nz, bt.part_stride, m->nnz);
+    }
     CK(cudaGetLastError());
     CK(mark(m, 4));
     if (m->n_blk) {
@@ -1867,89 +1718,9 @@ jfg_status launch_reduce(jfg_model *m, const Batch &bt, bool kg) {
     }
     CK(cudaGetLastError());
     CK(mark(m, 5));
-    if (bt.ddiag) launch_diag(m, bt);
-    CK(cudaGetLastError());
-    CK(mark(m, 6));
-    return JFG_OK;
-}
-
-// The persistent kernel serves single (not batched) calls on patterns with
-// evenly spaced rows; a handle whose task list is not built yet keeps the
-// separate kernels while its stream is being captured.
-bool use_fused(const jfg_model *m, const Batch &bt) {
-    return m->fz_mode && bt.n_var == 1 && m->blk_even && m->nq > 0 && m->n_blk > 0 &&
-           !(m->capturing && !(m->d_fz_task && m->fz_built_w == m->q4_warps && m->fz_built_chunk == m->fz_chunk));
-}
-
-// CTRIA3 and bar tiles, then the persistent CQUAD4 + block kernel, then the
-// RBE2 path and the diagonal (timing slots as finish_set maps them).
-jfg_status launch_fused(jfg_model *m, bool kg, const Batch &bt) {
-    jfg_status st = fz_build(m);
-    if (st) return st;
-    if (!m->capturing && m->last_set >= 0) m->ring[m->last_set].fused = true;
-    const ElemOut o = elem_out(m, kg, bt);
-    CK(mark(m, 0));
-    if (m->nt) {
-        launch_t3(m, kg, bt, o);
-        CK(cudaGetLastError());
-    }
-    CK(mark(m, 1));
-    if (m->nb) {
-        launch_bar(m, kg, bt, o);
-        CK(cudaGetLastError());
-    }
-    CK(mark(m, 2));
-    FzArgs a;
-    a.task = m->d_fz_task;
-    a.n_task = m->fz_n_task;
-    a.order = m->d_fz_order;
-    a.need = m->d_fz_need;
-    a.ctr = m->d_fz_ctr;
-    a.nq = m->nq;
-    a.nodes = m->d_q4n;
-    a.prop = m->d_q4p;
-    a.coords = m->d_coords;
-    a.nodeR = m->d_nodeR;
-    a.u = bt.u;
-    a.k6rot = m->k6rot;
-    a.o = q4_out(m, o, bt);
-    a.seg = m->d_blk_seg;
-    a.rot = m->d_blk_rot;
-    a.slot_bar = m->d_slot_bar;
-    a.kg_rot_off = kg ? 12 * m->n_blk_contrib : 0;
-    a.pa = m->d_blk_pa;
-    a.pb = m->d_blk_pb;
-    a.len = m->d_blk_len;
-    a.nz = bt.nz;
-    const int W = m->q4_warps;
-    int &grid = m->fz_grid[kg][W == 8];
-    if (!grid) {
-        int per_sm = 0, sms = 0;
-        const size_t smem = W == 8 ? fz_smem_bytes<8>(kg) : fz_smem_bytes<4>(kg);
-        if (kg)
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, W == 8 ? fused_kg_kernel<8> : fused_kg_kernel<4>, 32 * W, smem));
-        else
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, W == 8 ? fused_k_kernel<8> : fused_k_kernel<4>, 32 * W, smem));
-        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device));
-        grid = std::max(1, per_sm) * sms;
-    }
-    const unsigned g = (unsigned)std::min<int64_t>(grid, m->fz_n_task);
-    CK(cudaMemsetAsync(m->d_fz_ctr + 1, 0, sizeof(int) * (1 + m->fz_n_chunk), m->stream));
-    if (kg && W == 8)
-        fused_kg_kernel<8><<<g, 32 * W, fz_smem_bytes<8>(true), m->stream>>>(a);
-    else if (kg)
-        fused_kg_kernel<4><<<g, 32 * W, fz_smem_bytes<4>(true), m->stream>>>(a);
-    else if (W == 8)
-        fused_k_kernel<8><<<g, 32 * W, fz_smem_bytes<8>(false), m->stream>>>(a);
-    else
-        fused_k_kernel<4><<<g, 32 * W, fz_smem_bytes<4>(false), m->stream>>>(a);
-    CK(cudaGetLastError());
-    CK(mark(m, 3));
-    if (m->n_xkey) launch_exc(m, bt);
-    CK(cudaGetLastError());
-    CK(mark(m, 4));
-    CK(mark(m, 5));
-    if (bt.ddiag) launch_diag(m, bt);
+    if (bt.ddiag)
+        diag_reduce_kernel<<<dim3((unsigned)cdiv(m->ndof, 256), nv), 256, 0, m->stream>>>(m->ndof, m->d_dseg, bt.dstaging, bt.ddiag,
+                                                                                     bt.dstage_stride);
     CK(cudaGetLastError());
     CK(mark(m, 6));
     return JFG_OK;
@@ -1961,7 +1732,6 @@ jfg_status launch_k(jfg_model *m, const Batch &bt) {
     jfg_status st = begin_set(m, 0);
     if (st) return st;
     if (bt.dmax) CK(cudaMemsetAsync(bt.dmax, 0, sizeof(double) * bt.n_var, m->stream));
-    if (use_fused(m, bt)) return launch_fused(m, false, bt);
     st = launch_elements(m, false, bt);
     if (st) return st;
     return launch_reduce(m, bt, false);
@@ -1976,7 +1746,6 @@ jfg_status launch_kg(jfg_model *m, const Batch &bt) {
     Batch b = bt;
     b.dmax = nullptr;
     b.ddiag = nullptr;
-    if (use_fused(m, b)) return launch_fused(m, true, b);
     st = launch_elements(m, true, b);
     if (st) return st;
     return launch_reduce(m, b, true);
@@ -2002,25 +1771,10 @@ jfg_status finish_set(jfg_model *m, int idx) {
     auto &set = m->ring[idx];
     if (!set.pending) return JFG_OK;
     CK(cudaEventSynchronize(set.e[6]));
-    // A persistent-kernel call records CTRIA3, bars, CQUAD4 + blocks, RBE2
-    // path, (nothing), diagonal; its intervals go to the usual slots
-    // (quad4 = the persistent kernel, reduce = 0).
-    static const int seq[6] = {0, 1, 2, 3, 4, 5}, fz[6] = {1, 2, 0, 3, 4, 5};
-    const int *slot = set.fused ? fz : seq;
     float k[6];
     for (int i = 0; i < 6; ++i) {
-        float d = 0.f;
-        CK(cudaEventElapsedTime(&d, set.e[i], set.e[i + 1]));
-        k[slot[i]] = d;
-    }
-    for (int i = 0; i < 6; ++i) m->acc_ms[set.kind][i] += k[i];
-    if (set.fused) {
-        set.fused = false;
-        jfg_status fst = fz_check(m);
-        if (fst) {
-            set.pending = false;
-            return fst;
-        }
+        CK(cudaEventElapsedTime(&k[i], set.e[i], set.e[i + 1]));
+        m->acc_ms[set.kind][i] += k[i];
     }
     m->acc_calls[set.kind] += 1;
     if (idx == m->last_set) {
@@ -2055,7 +1809,6 @@ jfg_status begin_set(jfg_model *m, int kind) {
     m->ring_head = (idx + 1) % jfg_model::kRing;
     m->ring[idx].kind = kind;
     m->ring[idx].pending = true;
-    m->ring[idx].fused = false;
     m->last_set = idx;
     m->ev = m->ring[idx].e;
     return JFG_OK;
@@ -2606,42 +2359,25 @@ jfg_status jfg_launch_config(jfg_model *m, const int32_t *cfg_in, int32_t *cfg_o
     return JFG_OK;
 }
 
-jfg_status jfg_persistent_config(jfg_model *m, int32_t mode, int64_t chunk_quad4, int32_t *mode_out, int64_t *chunk_out) {
-    if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
-    if (mode < -1 || mode > 1) return fail(m, JFG_ERR_INVALID, "persistent kernel mode: -1 (keep), 0 (off) or 1 (on)");
-    if (chunk_quad4 > 0 && chunk_quad4 % 24)
-        return fail(m, JFG_ERR_INVALID, "CQUAD4 chunk size must be a positive multiple of 24");
-    if (mode >= 0) m->fz_mode = mode;
-    if (chunk_quad4 > 0) m->fz_chunk = chunk_quad4;
-    if (mode_out) *mode_out = m->fz_mode;
-    if (chunk_out) *chunk_out = m->fz_chunk;
-    return JFG_OK;
-}
-
 jfg_status jfg_autotune(jfg_model *m, int32_t flags, int32_t *cfg_out) {
     if (!m || !m->d_rowptr) return fail(m, JFG_ERR_STATE, "handle not initialised");
     const int cq = size_class(m->nq), ct = size_class(m->nt), cb = size_class(m->nb);
-    const std::string keys[6] = {"q4 " + std::to_string(cq), "t3k " + std::to_string(ct), "t3kg " + std::to_string(ct),
-                                 "bark " + std::to_string(cb), "barkg " + std::to_string(cb), "persistent " + std::to_string(cq)};
-    const bool fz_ok = m->blk_even && m->nq > 0 && m->n_blk > 0;
+    const std::string keys[5] = {"q4 " + std::to_string(cq), "t3k " + std::to_string(ct), "t3kg " + std::to_string(ct),
+                                 "bark " + std::to_string(cb), "barkg " + std::to_string(cb)};
     int32_t cfg[5];
     jfg_launch_config(m, nullptr, cfg);
     if (flags & JFG_TUNE_READ) {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         const auto kv = tune_read();
         bool all = true;
-        int32_t c2[6];
-        for (int i = 0; i < 6; ++i) {
+        int32_t c2[5];
+        for (int i = 0; i < 5; ++i) {
             auto it = kv.find(keys[i]);
             if (it == kv.end()) { all = false; break; }
             c2[i] = it->second;
         }
-        if (all && (c2[5] == 0 || c2[5] == 1) && jfg_launch_config(m, c2, cfg_out) == JFG_OK) {
-            m->fz_mode = fz_ok ? c2[5] : 0;
-            return JFG_OK;
-        }
+        if (all && jfg_launch_config(m, c2, cfg_out) == JFG_OK) return JFG_OK;
     }
-    m->fz_mode = 0;  // the shape passes time the separate kernels
     // Time three passes; pass p runs candidate p of every knob (a knob with
     // two candidates repeats its second).  Per-kernel device times come from
     // the handle's timing events over REPS K (+ KG) assemblies per pass.
@@ -2678,41 +2414,10 @@ jfg_status jfg_autotune(jfg_model *m, int32_t flags, int32_t *cfg_out) {
     }
     jfg_status st = jfg_launch_config(m, choice, cfg_out);
     if (st) return st;
-    // With the chosen shapes: the separate kernels against the persistent
-    // CQUAD4 + block kernel, by the whole call's device time.
-    int persistent = 0;
-    if (fz_ok) {
-        double total[2] = {0.0, 0.0};
-        for (int mode = 0; mode < 2; ++mode) {
-            m->fz_mode = mode;
-            for (int warm = 0; warm < 2; ++warm) {
-                for (int k = 0; k < 2; ++k) jfg_timing_accumulated(m, k, nullptr, nullptr, 1);
-                for (int r = 0; r < (warm ? REPS : 1); ++r) {
-                    st = launch_k(m, m->d_nz, m->d_max, m->d_diag);
-                    if (st) return st;
-                    if (kg) {
-                        st = launch_kg(m, m->d_u, m->d_nz);
-                        if (st) return st;
-                    }
-                }
-            }
-            double tk[6] = {0}, tg[6] = {0};
-            st = jfg_timing_accumulated(m, 0, tk, nullptr, 1);
-            if (st) return st;
-            if (kg) {
-                st = jfg_timing_accumulated(m, 1, tg, nullptr, 1);
-                if (st) return st;
-            }
-            for (int i = 0; i < 6; ++i) total[mode] += tk[i] + tg[i];
-        }
-        persistent = total[1] < total[0] ? 1 : 0;
-    }
-    m->fz_mode = persistent;
     if (flags & JFG_TUNE_WRITE) {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         auto kv = tune_read();
         for (int i = 0; i < 5; ++i) kv[keys[i]] = choice[i];
-        kv[keys[5]] = persistent;
         if (!tune_write(kv)) return fail(m, JFG_ERR_INVALID, "cannot write the launch-shape store " + tune_path());
     }
     return JFG_OK;

@@ -27,7 +27,7 @@ EXPORTS = ("jfg_model_create", "jfg_pattern", "jfg_pattern_fill", "jfg_assemble_
            "jfg_dkdh_contract_device", "jfg_dkdh_load_device", "jfg_recover_stresses",
            "jfg_recover_stresses_device", "jfg_kg_contract", "jfg_kg_contract_device", "jfg_server_create", "jfg_server_submit", "jfg_server_wait",
            "jfg_server_result", "jfg_server_release", "jfg_server_stats", "jfg_server_family_batch",
-           "jfg_server_hold", "jfg_server_last_error", "jfg_server_destroy", "jfg_group_create", "jfg_group_member", "jfg_autotune", "jfg_launch_config", "jfg_persistent_config", "jfg_assemble_batch_device_ws",
+           "jfg_server_hold", "jfg_server_last_error", "jfg_server_destroy", "jfg_group_create", "jfg_group_member", "jfg_autotune", "jfg_launch_config", "jfg_assemble_batch_device_ws",
            "jfg_shell_thickness", "jfg_server_create_units",
            "jfg_assemble_k_quad4_noalloc", "jfg_model_destroy", "jfg_last_error",
            "jfg_version")
@@ -74,8 +74,6 @@ def load(path: str = LIB_PATH):
     L.jfg_autotune.restype = C.c_int32
     L.jfg_launch_config.argtypes = [C.c_void_p, _pi32, _pi32]
     L.jfg_launch_config.restype = C.c_int32
-    L.jfg_persistent_config.argtypes = [C.c_void_p, C.c_int32, C.c_int64, _pi32, _pi64]
-    L.jfg_persistent_config.restype = C.c_int32
     L.jfg_assemble_batch_device_ws.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int64] + [C.c_void_p] * 3 + \
         [C.c_int64] + [C.c_void_p] * 4
     L.jfg_assemble_batch_device_ws.restype = C.c_int32
@@ -221,16 +219,6 @@ class GpuModel:
         self._check(self.L.jfg_launch_config(self.h, None if cin is None else cin.ctypes.data_as(pi32),
                                              c.ctypes.data_as(pi32)))
         return dict(zip(self.CONFIG_KEYS, (int(x) for x in c)))
-
-    def persistent(self, on: Optional[bool] = None, chunk_quad4: int = 0) -> dict:
-        """Turn the persistent CQUAD4 + block-reduction kernel on or off
-        (None keeps the mode) and/or set its chunk size; returns the settings
-        (jfg_persistent_config)."""
-        mode = C.c_int32(0)
-        chunk = C.c_int64(0)
-        self._check(self.L.jfg_persistent_config(self.h, -1 if on is None else int(bool(on)), int(chunk_quad4),
-                                                 C.byref(mode), C.byref(chunk)))
-        return {"persistent": int(mode.value), "chunk_quad4": int(chunk.value)}
 
     # -- pattern -----------------------------------------------------------
     def pattern(self):
