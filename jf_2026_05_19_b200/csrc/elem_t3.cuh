@@ -11,13 +11,13 @@
 //
 // Macro nodes: corners 0-2, edge midpoints 3 (0-1), 4 (1-2), 5 (2-0),
 // centroid 6.  No virtual quad holds two corners, so Kee is block diagonal
-// and every Kei entry comes from the one quad that holds the corner.  The
-// internal solve lu(Kii) \ Kie runs as Gauss-Jordan elimination with one row
-// of [Kii | Kie] per lane in registers, pivoting on the diagonal: Kii, the
-// plate stiffness of the midside and centroid dofs with the corners held, is
-// symmetric positive definite, so the reference's row exchanges change only
-// the rounding.  Eliminating above the pivot as well replaces the back
-// substitution.
+// and every Kei entry comes from the one quad that holds the corner.  Kii,
+// the plate stiffness of the midside and centroid dofs with the corners held,
+// is symmetric positive definite, so elimination on the diagonal pivots
+// changes only the rounding of the reference's pivoted lu(Kii) \ Kie.  The
+// stiffness kernel condenses by 3x3-block elimination (t3_schur); the
+// recovery and sensitivity kernels, which need X = Kii^-1 Kie itself, run
+// Gauss-Jordan elimination with one row of [Kii | Kie] per lane (t3_condense).
 //
 // KG: one thread per (element, node pair).  CST membrane resultant of stress_strain_tria3
 // (FEMKernels.jl:7391-7404) and geometric_stiffness_tria3's non-curvature
@@ -51,11 +51,13 @@ struct __align__(16) T3KShared {
             double dNx[3][5][4], dNy[3][5][4], wdet[3][4];
             double Dd[3][4][4], ivd[3][4], zs[3][4], W[3][6];
         } q;
-        struct {  // condensation (phases 4-6)
-            double X[12][9];   // Kii^-1 Kie; the stiffness kernel keeps z = L^-1 Kie here
+        struct {  // condensation of the recovery and sensitivity kernels
+            double X[12][9];   // Kii^-1 Kie
             double Kc[9][9];
-            double dk[12];     // pivots of the stiffness kernel's elimination
         } c;
+        struct {  // the stiffness kernel's macro system, 28 upper 3x3 blocks (t3_pblk)
+            double A[28][9];
+        } b;
     } u;
     // quad q, local node pair (a <= b): 3x3 over (w, theta_x, theta_y);
     // the K kernel's write phase reuses it for the six staged 6x6 blocks
@@ -187,70 +189,82 @@ __device__ __forceinline__ void t3_condense(T3KShared &S, int tl, unsigned tm) {
     __syncwarp(tm);
 }
 
-// Condensed plate stiffness Kc = Kee - Kei Kii^-1 Kie into S.u.c.Kc, for the
-// stiffness kernel.  Kii is symmetric positive definite and Kei = Kie' (both
-// read from the same stored quad blocks), so only a forward elimination is
-// needed: with Kii = L D L', Kei Kii^-1 Kie = sum_k z_k z_k' / d_k, z = L^-1
-// Kie.  Lane r < 12 holds row r of [Kii | Kie] and eliminates below the
-// diagonal pivots; the row it holds when it is the pivot row is (u_k, z_k)
-// and its pivot d_k.  Kc is formed symmetric: 45 entries, the diagonal
-// blocks' lower triangles mirrored.
+// Blocks of the 7-node macro system: nodes ordered midpoints 3, 4, 5,
+// centroid 6, corners 0, 1, 2; block (I, J), I <= J, packed upper-triangular.
+__host__ __device__ constexpr int t3_pblk(int I, int J) { return I * 7 - I * (I - 1) / 2 + (J - I); }
+__host__ __device__ constexpr int t3_mnode(int I) { return I < 4 ? I + 3 : I - 4; }
+
+// Condensed plate stiffness Kc = Kee - Kei Kii^-1 Kie, for the stiffness
+// kernel, by 3x3-block elimination of the four internal nodes.  The 28 upper
+// blocks of the macro system are summed from the quads' plate blocks (quad
+// order), then for each internal node K: its pivot block D = L diag(d) L' in
+// closed form (the three reciprocals 1/D00, D00/m2, m2/det are independent),
+// Z_J = L^-1 A_KJ and Zs_J = diag(d)^-1 Z_J for every later node J, and every
+// later block A_IJ -= Z_I' Zs_J.  Kii is symmetric positive definite, so this
+// unpivoted elimination matches the reference's pivoted LU up to rounding.
+// On return the corner blocks (4 + a, 4 + b) of S.u.b.A hold Kc.
 __device__ __forceinline__ void t3_schur(T3KShared &S, int tl, unsigned tm) {
-    const bool act = tl < 12;
-    const int nA = 3 + tl / 3, ci = tl - 3 * (tl / 3);
-    double row[21];
-#pragma unroll
-    for (int c = 0; c < 21; ++c) row[c] = 0.0;
-    if (act) {
+    double(*A)[9] = S.u.b.A;
+    for (int b = tl; b < 28; b += T3_TEAM) {
+        int I = 0, rem = b;
+        while (rem >= 7 - I) { rem -= 7 - I; ++I; }
+        const int J = I + rem, nI = t3_mnode(I), nJ = t3_mnode(J);
+        double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
-            int la = -1;
+            int la = -1, lb = -1;
 #pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if (t3_quad_node(q, k) == nA) la = k;
-            if (la >= 0) {
+            for (int k = 0; k < 4; ++k) {
+                if (t3_quad_node(q, k) == nI) la = k;
+                if (t3_quad_node(q, k) == nJ) lb = k;
+            }
+            if (la >= 0 && lb >= 0) {
+                const bool tr = la > lb;
+                const double *P = S.Pb[q][tr ? packed_index(lb, la, 4) : packed_index(la, lb, 4)];
 #pragma unroll
-                for (int kb = 0; kb < 4; ++kb) {
-                    const int nB = t3_quad_node(q, kb);
-                    const int cb0 = nB >= 3 ? 3 * (nB - 3) : 12 + 3 * nB;
-                    const bool tr = la > kb;
-                    const int pid = tr ? packed_index(kb, la, 4) : packed_index(la, kb, 4);
+                for (int r = 0; r < 3; ++r)
 #pragma unroll
-                    for (int cj = 0; cj < 3; ++cj) row[cb0 + cj] += S.Pb[q][pid][tr ? 3 * cj + ci : 3 * ci + cj];
-                }
+                    for (int c = 0; c < 3; ++c) v[3 * r + c] += P[tr ? 3 * c + r : 3 * r + c];
             }
         }
+#pragma unroll
+        for (int e = 0; e < 9; ++e) A[b][e] = v[e];
     }
-    double diag = 1.0;
+    __syncwarp(tm);  // plate blocks read; S.Pb holds Z below
+    double *Zb = &S.Pb[0][0][0];  // step K, later node J = K + 1 + j: Z at 18 j, Zs at 18 j + 9
 #pragma unroll
-    for (int k = 0; k < 12; ++k) {
-        const double akk = __shfl_sync(tm, row[k], k, 16);
-        if (tl == k) diag = akk;
-        const double f = (act && tl > k) ? row[k] / akk : 0.0;
+    for (int K = 0; K < 4; ++K) {
+        const int n = 6 - K;
+        const double *D = A[t3_pblk(K, K)];
+        const double D00 = D[0], D01 = D[1], D02 = D[2], D11 = D[4], D12 = D[5], D22 = D[8];
+        const double m2 = D00 * D11 - D01 * D01;
+        const double det = D00 * (D11 * D22 - D12 * D12) - D01 * (D01 * D22 - D12 * D02) + D02 * (D01 * D12 - D11 * D02);
+        const double i0 = 1.0 / D00, i1 = D00 / m2, i2 = m2 / det;
+        const double l10 = D01 * i0, l20 = D02 * i0, l21 = (D12 - l20 * D01) * i1;
+        if (tl < n) {
+            const double *B = A[t3_pblk(K, K + 1 + tl)];
+            double *Z = Zb + 18 * tl;
 #pragma unroll
-        for (int j = k + 1; j < 21; ++j) {
-            const double pj = __shfl_sync(tm, row[j], k, 16);
-            row[j] -= f * pj;
+            for (int c = 0; c < 3; ++c) {
+                const double z0 = B[c], z1 = B[3 + c] - l10 * z0, z2 = B[6 + c] - l20 * z0 - l21 * z1;
+                Z[c] = z0; Z[3 + c] = z1; Z[6 + c] = z2;
+                Z[9 + c] = z0 * i0; Z[12 + c] = z1 * i1; Z[15 + c] = z2 * i2;
+            }
         }
-    }
-    __syncwarp(tm);  // every lane is past its last read of the quad data
-    if (act) {
+        __syncwarp(tm);
+        for (int t = tl; t < n * (n + 1) / 2; t += T3_TEAM) {
+            int ip = 0, rem = t;
+            while (rem >= n - ip) { rem -= n - ip; ++ip; }
+            const int jp = ip + rem;
+            const double *Zi = Zb + 18 * ip, *Zs = Zb + 18 * jp + 9;
+            double *C = A[t3_pblk(K + 1 + ip, K + 1 + jp)];
 #pragma unroll
-        for (int c = 0; c < 9; ++c) S.u.c.X[tl][c] = row[12 + c];
-        S.u.c.dk[tl] = 1.0 / diag;
-    }
-    __syncwarp(tm);
-    // item it < 45: upper-triangle entry (r, c) of the 9x9, row-major
-    for (int it = tl; it < 45; it += T3_TEAM) {
-        int r = 0, rem = it;
-        while (rem >= 9 - r) { rem -= 9 - r; ++r; }
-        const int c = r + rem;
-        const int cr = r / 3, cc = c / 3;
-        double s = (cr == cc) ? S.Pb[cr][0][3 * (r - 3 * cr) + (c - 3 * cc)] : 0.0;
+            for (int r = 0; r < 3; ++r)
 #pragma unroll
-        for (int k = 0; k < 12; ++k) s -= S.u.c.X[k][r] * (S.u.c.X[k][c] * S.u.c.dk[k]);
-        S.u.c.Kc[r][c] = s;
-        S.u.c.Kc[c][r] = s;
+                for (int c = 0; c < 3; ++c)
+                    C[3 * r + c] -= Zi[r] * Zs[c] + Zi[3 + r] * Zs[3 + c] + Zi[6 + r] * Zs[6 + c];
+        }
+        __syncwarp(tm);
     }
 }
 
@@ -333,7 +347,7 @@ __global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t n
     if (plate) {
         t3_plate_points(S, tl, tm, x, y, cs, cb, macneal);
         t3_plate_blocks(S, tl, tm, cb, nu, gam, macneal);
-        // Phases 3-4: Kcond = Kee - Kei Kii^-1 Kie by symmetric elimination
+        // Phases 3-4: Kcond = Kee - Kei Kii^-1 Kie by 3x3-block elimination
         // (Kee and Kei from the corner's own quad)
         t3_schur(S, tl, tm);
     }
@@ -364,7 +378,7 @@ __global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t n
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
 #pragma unroll
-                    for (int j = 0; j < 3; ++j) Lp[i][j] = S.u.c.Kc[3 * a + i][3 * b + j];
+                    for (int j = 0; j < 3; ++j) Lp[i][j] = S.u.b.A[t3_pblk(4 + a, 4 + b)][3 * i + j];
         }
         double Qa[9], Qb[9];
         if (nodeR) {
