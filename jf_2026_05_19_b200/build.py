@@ -16,7 +16,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libjfemgpu.so")
-SOURCES = ["jfg_api.cu", "jfg_server.cu"]
+SOURCES = ["jfg_api.cu", "jfg_server.cu", "jfg_host.cpp"]
 _INCLUDE = re.compile(r'^\s*#\s*include\s*"([^"]+)"', re.M)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -33,11 +33,13 @@
 #include <thread>
 #include <vector>
 
+#include <functional>
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
 #include <sys/stat.h>
 
 #include "../../include/jfem_gpu.h"
+#include "jfg_host.h"
 #include "elem_bar.cuh"
 #include "elem_q4.cuh"
 #include "elem_t3.cuh"
@@ -72,28 +74,31 @@ class CopyPool {
         cv_.notify_all();
         for (auto &t : th_) t.join();
     }
-    void copy(void *dst, const void *src, size_t len) {
+    // f(i, n) for every part i of n = workers + 1; the caller takes the last.
+    void parallel(const std::function<void(int, int)> &f) {
         {
             std::lock_guard<std::mutex> l(mu_);
-            dst_ = static_cast<char *>(dst);
-            src_ = static_cast<const char *>(src);
-            len_ = len;
+            fn_ = &f;
             pending_ = (int)th_.size();
             ++gen_;
         }
         cv_.notify_all();
-        part((int)th_.size());  // the caller takes the last part
+        f((int)th_.size(), (int)th_.size() + 1);
         std::unique_lock<std::mutex> l(mu_);
         done_.wait(l, [this] { return pending_ == 0; });
     }
+    void copy(void *dst, const void *src, size_t len) {
+        char *d = static_cast<char *>(dst);
+        const char *s = static_cast<const char *>(src);
+        parallel([&](int i, int n) {
+            const size_t step = (len / n + 63) / 64 * 64;
+            const size_t a = std::min(len, step * i), b = i + 1 == n ? len : std::min(len, step * (i + 1));
+            if (b > a) jfg_host::copy_stream(d + a, s + a, b - a);
+        });
+    }
 
   private:
-    void part(int i) {
-        const size_t n = th_.size() + 1;
-        const size_t step = (len_ / n + 63) / 64 * 64;
-        const size_t a = std::min(len_, step * i), b = i + 1 == (int)n ? len_ : std::min(len_, step * (i + 1));
-        if (b > a) std::memcpy(dst_ + a, src_ + a, b - a);
-    }
+    void part(int i) { (*fn_)(i, (int)th_.size() + 1); }
     void run(int i) {
         uint64_t seen = 0;
         for (;;) {
@@ -111,9 +116,7 @@ class CopyPool {
     std::vector<std::thread> th_;
     std::mutex mu_;
     std::condition_variable cv_, done_;
-    char *dst_ = nullptr;
-    const char *src_ = nullptr;
-    size_t len_ = 0;
+    const std::function<void(int, int)> *fn_ = nullptr;
     int pending_ = 0;
     uint64_t gen_ = 0;
     bool stop_ = false;
@@ -152,6 +155,15 @@ struct jfg_model {
     // bar KG kernels (32, 64 or 128)
     int q4_warps = 4, t3_warps = 4;
     int t3kg_threads = 128, bark_threads = 128, barkg_threads = 128;
+    // KG to pageable host memory: a bit per CSC entry that KG can make nonzero
+    // (the translation 3x3 of shell-only blocks; all of a block with bar
+    // pairs; RBE2-path entries), the live count before each 32-entry word,
+    // the compacted values and host copies (built at the first such call)
+    uint32_t *d_kg_live = nullptr, *d_kg_pre = nullptr;
+    double *d_kg_cmp = nullptr;
+    int64_t kg_n_live = -1;
+    std::vector<uint32_t> h_kg_live, h_kg_pre;
+    std::vector<int64_t> kg_chunk_w;    // word bounds of the pinned-ring chunks
     int64_t staging_len = 0;            // staging doubles per assembly: max(K 36 per slot, KG 12 per slot + 27 per bar pair)
     double *d_staging = nullptr;        // 36 doubles per regular element pair
     int64_t *d_rowptr = nullptr, *d_colind = nullptr;   // 0-based symmetric CSR == CSC
@@ -211,7 +223,7 @@ struct jfg_model {
     std::vector<std::array<int64_t, 8>> members;
     // device -> pageable host copies: a ring of pinned chunks and host copy threads (made at first use)
     static constexpr int kPinChunks = 4;
-    static constexpr size_t kPinChunkBytes = size_t(32) << 20;
+    size_t pin_chunk = size_t(32) << 20;   // bytes per ring chunk (JFG_PIN_CHUNK_MB at first use)
     char *pin = nullptr;
     cudaEvent_t pin_ev[kPinChunks] = {nullptr, nullptr, nullptr, nullptr};
     std::unique_ptr<CopyPool> copy_pool;
@@ -809,6 +821,49 @@ __global__ void diag_reduce_kernel(int64_t ndof, const int32_t *__restrict__ seg
     out[d] = s;
 }
 
+// Entries KG can make nonzero, per regular block (the positions of
+// block_reduce1_kernel's two writes): all 36 when the block has bar pairs,
+// else the translation 3x3 (shell KG stages translations only).
+__global__ void kg_live_blocks_kernel(int64_t n_blk, const int32_t *__restrict__ seg, const int32_t *__restrict__ rot,
+                                      const int64_t *__restrict__ pa, const int64_t *__restrict__ pb,
+                                      const int2 *__restrict__ len, uint32_t *live) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n_blk) return;
+    const bool bars = rot[k] < seg[k + 1];
+    const int64_t p_a = pa[k], p_b = pb[k];
+    const int2 l = len[k];
+    const int nr = bars ? 6 : 3;
+    for (int r = 0; r < nr; ++r)
+        for (int c = 0; c < nr; ++c) {
+            const int64_t x = p_a + c + (int64_t)r * l.x;
+            atomicOr(live + (x >> 5), 1u << (x & 31));
+            if (p_b >= 0) {
+                const int64_t y = p_b + r + (int64_t)c * l.y;
+                atomicOr(live + (y >> 5), 1u << (y & 31));
+            }
+        }
+}
+
+__global__ void kg_live_positions_kernel(int64_t n, const int64_t *__restrict__ pos, uint32_t *live) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) atomicOr(live + (pos[i] >> 5), 1u << (pos[i] & 31));
+}
+
+__global__ void popc_kernel(int64_t nw, const uint32_t *__restrict__ live, uint32_t *cnt) {
+    const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w < nw) cnt[w] = __popc(live[w]);
+}
+
+// The live entries of nz, in order, into out (pre = live count before each word).
+__global__ void kg_compact_kernel(int64_t nnz, const double *__restrict__ nz, const uint32_t *__restrict__ live,
+                                  const uint32_t *__restrict__ pre, double *out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nnz) return;
+    const uint32_t m = __ldg(live + (i >> 5));
+    const int l = (int)(i & 31);
+    if ((m >> l) & 1u) out[__ldg(pre + (i >> 5)) + __popc(m & ((1u << l) - 1u))] = nz[i];
+}
+
 __global__ void set_h_kernel(int64_t n, const double *__restrict__ h, double *prop) {
     int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e < n) prop[7 * e] = h[e];
@@ -922,6 +977,8 @@ void jfg_model_destroy(jfg_model *m) {
     if (m->stream) cudaStreamSynchronize(m->stream);
     for (void *p : m->allocs) cudaFree(p);
     if (m->d_bw) cudaFree(m->d_bw);
+    for (void *p : {(void *)m->d_kg_live, (void *)m->d_kg_pre, (void *)m->d_kg_cmp})
+        if (p) cudaFree(p);
     for (auto &set : m->ring)
         for (auto &e : set.e)
             if (e) cudaEventDestroy(e);
@@ -1943,23 +2000,37 @@ namespace {
 // instead: while the GPU fills chunk i + 1 .. i + 3, host threads move chunk
 // i into the destination.  The ring and the threads are made at first use
 // (JFG_COPY_THREADS sets the thread count, default min(16, cores)).
-jfg_status copy_to_host(jfg_model *m, void *dst, const void *src, size_t bytes) {
+bool is_pinned(const void *p) {
     cudaPointerAttributes at{};
-    const bool pinned = cudaPointerGetAttributes(&at, dst) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    const bool pinned = cudaPointerGetAttributes(&at, p) == cudaSuccess && at.type == cudaMemoryTypeHost;
     cudaGetLastError();  // an unknown pointer may leave an error set on older runtimes
-    if (pinned || bytes < (size_t(4) << 20)) {
+    return pinned;
+}
+
+// The ring of pinned chunks and the host copy threads, made at first use.
+jfg_status ensure_ring(jfg_model *m) {
+    if (m->pin) return JFG_OK;
+    if (const char *env = std::getenv("JFG_PIN_CHUNK_MB")) {
+        const long mb = std::atol(env);
+        if (mb >= 1 && mb <= 256) m->pin_chunk = size_t(mb) << 20;
+    }
+    CK(cudaHostAlloc((void **)&m->pin, jfg_model::kPinChunks * m->pin_chunk, cudaHostAllocDefault));
+    for (auto &e : m->pin_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    int n = (int)std::min<unsigned>(16, std::max<unsigned>(1, std::thread::hardware_concurrency()));
+    if (const char *env = std::getenv("JFG_COPY_THREADS")) n = std::max(1, std::atoi(env));
+    m->copy_pool.reset(new CopyPool(n - 1));
+    return JFG_OK;
+}
+
+jfg_status copy_to_host(jfg_model *m, void *dst, const void *src, size_t bytes) {
+    if (is_pinned(dst) || bytes < (size_t(4) << 20)) {
         CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, m->stream));
         return JFG_OK;
     }
     constexpr int R = jfg_model::kPinChunks;
-    constexpr size_t C = jfg_model::kPinChunkBytes;
-    if (!m->pin) {
-        CK(cudaHostAlloc((void **)&m->pin, R * C, cudaHostAllocDefault));
-        for (auto &e : m->pin_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        int n = (int)std::min<unsigned>(16, std::max<unsigned>(1, std::thread::hardware_concurrency()));
-        if (const char *env = std::getenv("JFG_COPY_THREADS")) n = std::max(1, std::atoi(env));
-        m->copy_pool.reset(new CopyPool(n - 1));
-    }
+    jfg_status st = ensure_ring(m);
+    if (st) return st;
+    const size_t C = m->pin_chunk;
     const size_t n = (bytes + C - 1) / C;
     auto issue = [&](size_t i) -> cudaError_t {
         const size_t len = std::min(C, bytes - i * C);
@@ -1971,6 +2042,90 @@ jfg_status copy_to_host(jfg_model *m, void *dst, const void *src, size_t bytes) 
     for (size_t i = 0; i < n; ++i) {
         CK(cudaEventSynchronize(m->pin_ev[i % R]));
         m->copy_pool->copy(static_cast<char *>(dst) + i * C, m->pin + (i % R) * C, std::min(C, bytes - i * C));
+        if (i + R < n) CK(issue(i + R));
+    }
+    return JFG_OK;
+}
+
+// KG into pageable host memory moves only the entries KG can make nonzero
+// (about a quarter of a shell model's pattern): the live mask is built once
+// from the block structure (evenly spaced patterns) and the RBE2 positions;
+// each call compacts the live values on the device, and host threads expand
+// every pinned chunk into the caller's array (+0.0 elsewhere) while the GPU
+// fills the next.  JFG_KG_COMPACT=0 turns it off.
+bool kg_compact_eligible(const jfg_model *m, const void *dst) {
+    if (!m->blk_even || m->nnz * 8 < (int64_t(4) << 20) || m->nnz >= (int64_t(1) << 32)) return false;
+    if (const char *env = std::getenv("JFG_KG_COMPACT"))
+        if (env[0] == '0') return false;
+    return !is_pinned(dst);
+}
+
+jfg_status kg_live_build(jfg_model *m) {
+    if (m->kg_n_live >= 0) return JFG_OK;
+    const int64_t nnz = m->nnz, nw = cdiv(nnz, 32);
+    CK(cudaMalloc(&m->d_kg_live, sizeof(uint32_t) * nw));
+    CK(cudaMalloc(&m->d_kg_pre, sizeof(uint32_t) * (nw + 1)));
+    uint32_t *cnt = nullptr;
+    CK(cudaMallocAsync(&cnt, sizeof(uint32_t) * (nw + 1), m->stream));
+    CK(cudaMemsetAsync(m->d_kg_live, 0, sizeof(uint32_t) * nw, m->stream));
+    CK(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * (nw + 1), m->stream));
+    if (m->n_blk)
+        kg_live_blocks_kernel<<<(unsigned)cdiv(m->n_blk, 256), 256, 0, m->stream>>>(m->n_blk, m->d_blk_seg, m->d_blk_rot,
+                                                                                 m->d_blk_pa, m->d_blk_pb, m->d_blk_len,
+                                                                                 m->d_kg_live);
+    if (m->n_xkey)
+        kg_live_positions_kernel<<<(unsigned)cdiv(m->n_xkey, 256), 256, 0, m->stream>>>(m->n_xkey, m->d_x_pos, m->d_kg_live);
+    popc_kernel<<<(unsigned)cdiv(nw, 256), 256, 0, m->stream>>>(nw, m->d_kg_live, cnt);
+    CK(cudaGetLastError());
+    CK(exclusive_sum(m, cnt, m->d_kg_pre, nw + 1));
+    m->h_kg_live.resize(nw);
+    m->h_kg_pre.resize(nw + 1);
+    CK(cudaMemcpyAsync(m->h_kg_live.data(), m->d_kg_live, sizeof(uint32_t) * nw, cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaMemcpyAsync(m->h_kg_pre.data(), m->d_kg_pre, sizeof(uint32_t) * (nw + 1), cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaFreeAsync(cnt, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    const int64_t n_live = m->h_kg_pre[nw];
+    CK(cudaMalloc(&m->d_kg_cmp, sizeof(double) * std::max<int64_t>(n_live, 1)));
+    // chunk bounds in words: at most one pinned chunk of live values each
+    const int64_t cap = (int64_t)(m->pin_chunk / sizeof(double));
+    m->kg_chunk_w.assign(1, 0);
+    for (int64_t w = 0; w < nw; ++w)
+        if ((int64_t)m->h_kg_pre[w + 1] - (int64_t)m->h_kg_pre[m->kg_chunk_w.back()] > cap) m->kg_chunk_w.push_back(w);
+    m->kg_chunk_w.push_back(nw);
+    m->kg_n_live = n_live;
+    return JFG_OK;
+}
+
+jfg_status copy_kg_compact(jfg_model *m, double *dst) {
+    jfg_status st = ensure_ring(m);  // first: the chunk bounds follow the ring's chunk size
+    if (st) return st;
+    st = kg_live_build(m);
+    if (st) return st;
+    const int64_t nnz = m->nnz;
+    kg_compact_kernel<<<(unsigned)cdiv(nnz, 256), 256, 0, m->stream>>>(nnz, m->d_nz, m->d_kg_live, m->d_kg_pre, m->d_kg_cmp);
+    CK(cudaGetLastError());
+    constexpr int R = jfg_model::kPinChunks;
+    const size_t C = m->pin_chunk;
+    const std::vector<int64_t> &wb = m->kg_chunk_w;
+    const uint32_t *pre = m->h_kg_pre.data();
+    const size_t n = wb.size() - 1;
+    auto issue = [&](size_t i) -> cudaError_t {
+        const size_t len = sizeof(double) * (pre[wb[i + 1]] - pre[wb[i]]);
+        cudaError_t e = len ? cudaMemcpyAsync(m->pin + (i % R) * C, m->d_kg_cmp + pre[wb[i]], len, cudaMemcpyDeviceToHost,
+                                              m->stream)
+                            : cudaSuccess;
+        return e != cudaSuccess ? e : cudaEventRecord(m->pin_ev[i % R], m->stream);
+    };
+    for (size_t i = 0; i < std::min<size_t>(R, n); ++i) CK(issue(i));
+    for (size_t i = 0; i < n; ++i) {
+        CK(cudaEventSynchronize(m->pin_ev[i % R]));
+        const double *chunk = reinterpret_cast<const double *>(m->pin + (i % R) * C);
+        const int64_t w0 = wb[i], w1 = wb[i + 1];
+        m->copy_pool->parallel([&](int t, int nt) {
+            const int64_t a = w0 + (w1 - w0) * t / nt, b = w0 + (w1 - w0) * (t + 1) / nt;
+            const int64_t e0 = 32 * a, e1 = std::min(32 * b, nnz);
+            if (e1 > e0) jfg_host::expand_stream(dst + e0, chunk + (pre[a] - pre[w0]), m->h_kg_live.data() + a, e1 - e0);
+        });
         if (i + R < n) CK(issue(i + R));
     }
     return JFG_OK;
@@ -2007,7 +2162,7 @@ jfg_status jfg_assemble_kg(jfg_model *m, const double *u_global, double *nzval) 
     jfg_status st = launch_kg(m, m->d_u, m->d_nz);
     if (st) return st;
     if (nzval) {
-        st = copy_to_host(m, nzval, m->d_nz, sizeof(double) * m->nnz);
+        st = kg_compact_eligible(m, nzval) ? copy_kg_compact(m, nzval) : copy_to_host(m, nzval, m->d_nz, sizeof(double) * m->nnz);
         if (st) return st;
     }
     CK(cudaStreamSynchronize(m->stream));

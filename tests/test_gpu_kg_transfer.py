@@ -1,0 +1,48 @@
+"""KG into pageable host memory through the compacted transfer.
+
+Only the entries KG can make nonzero cross the bus; host threads expand them
+with +0.0 elsewhere.  The host result must equal, bit for bit, the device
+result of the same call (and the uncompacted transfer, JFG_KG_COMPACT=0, and
+a pinned destination, which takes the direct copy).
+"""
+import numpy as np
+import pytest
+
+from jf_2026_05_19_b200 import decks, native
+
+pytestmark = pytest.mark.gpu
+
+
+def _device_kg(g, u):
+    import torch
+    du = torch.from_numpy(u).cuda()
+    nz = torch.full((g.nnz,), float("nan"), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    g.assemble_kg_device(du.data_ptr(), nz.data_ptr())
+    torch.cuda.synchronize()
+    return nz.cpu().numpy()
+
+
+@pytest.mark.parametrize("make", [
+    lambda: decks.barrel_small(seed=3, n_circ=96, n_axial=32),     # shells, bars, RBE2
+    lambda: decks.plate_c1(n=150),                                  # shells only
+])
+def test_compacted_kg_equals_device_values(cuda_device, monkeypatch, make):
+    import torch
+    m = make()
+    u = decks.smooth_displacement(m, seed=5)
+    with native.GpuModel(m) as g:
+        assert g.nnz * 8 >= 4 << 20                               # large enough for the compacted path
+        ref = _device_kg(g, u)
+        got = g.assemble_kg(u)                                    # pageable numpy destination
+        assert np.array_equal(got, ref)
+        dead = got == 0.0
+        assert dead.mean() > 0.5 and not np.signbit(got[dead]).any()
+        again = np.full(g.nnz, np.nan)
+        g.assemble_kg(u, again)                                   # a second call reuses the mask
+        assert np.array_equal(again, ref)
+        pinned = torch.empty(g.nnz, dtype=torch.float64).pin_memory()
+        g.assemble_kg(u, pinned.numpy())
+        assert np.array_equal(pinned.numpy(), ref)
+        monkeypatch.setenv("JFG_KG_COMPACT", "0")
+        assert np.array_equal(g.assemble_kg(u), ref)
