@@ -995,7 +995,8 @@ def main():
                             "DFMA/DADD/DMUL the closed-form kernel issues (ncu counters, roofline.EXECUTED_FLOPS)")
     ms_step = elapsed / args.steps * 1e3
     h2d = 8 * m.ndof
-    d2h = 8 * g.nnz * 2 + 8 * m.ndof + 8
+    kg_live = g.kg_transfer_entries()       # KG entries moved by the pageable call (-1: the whole pattern)
+    d2h = 8 * g.nnz + 8 * (kg_live if kg_live >= 0 else g.nnz) + 8 * m.ndof + 8
     launches_per_step = (sum(1 for t in ("quad4", "tria3", "bar") if counts[t] > 0) * 2
                          + 2 * (1 if st["dof_contribs"] else 0) + 2 + 1)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -1010,6 +1011,9 @@ def main():
                                 - full.n_elements))),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": e2e_steps, "host_memory": "pageable (numpy arrays, as a Julia Vector{Float64})",
+                    "kg_live_entries": kg_live, "note": "pageable copies run through a pinned ring with host threads "
+                    "writing non-temporal stores; KG sends only its live entries (d2h_bytes_per_step counts them) "
+                    "and the host threads expand them; pinned_value: caller-pinned arrays, one DMA each",
                     "pinned_value": e2e_pinned_value},
             "roofline": roof, "gpu_launches": launches_per_step * args.steps, "clocks": clk,
             "kernel_ms": per_kernel, "fp64_dgemm_tflops": fp64_peak, "model_stats": st,

@@ -161,6 +161,12 @@ jfg_status jfg_timing_accumulated(jfg_model *m, int kind, double *ms6_sum, int64
  * orig_diag entries, device bytes in use}. */
 jfg_status jfg_model_stats(jfg_model *m, int64_t *out8);
 
+/* KG entries moved to pageable host memory per jfg_assemble_kg: only the
+ * entries KG can make nonzero cross the bus (the rest are +0.0 and written by
+ * host threads).  *n_live = that count once the first such call has built the
+ * live mask, -1 before (or when the model uses the plain copy). */
+jfg_status jfg_kg_transfer_entries(jfg_model *m, int64_t *n_live);
+
 /* Element and node counts of a handle: out4 = {n_nodes, n_quad4, n_tria3, n_bar}. */
 jfg_status jfg_model_counts(jfg_model *m, int64_t *out4);
 

@@ -2586,6 +2586,12 @@ jfg_status jfg_kernel_timing(jfg_model *m, double *ms6) {
     return JFG_OK;
 }
 
+jfg_status jfg_kg_transfer_entries(jfg_model *m, int64_t *n_live) {
+    if (!m || !n_live) return JFG_ERR_INVALID;
+    *n_live = m->kg_n_live;
+    return JFG_OK;
+}
+
 jfg_status jfg_model_stats(jfg_model *m, int64_t *out8) {
     if (!m || !out8) return JFG_ERR_INVALID;
     out8[0] = 36 * m->n_blk_contrib;      // staging values per assembly

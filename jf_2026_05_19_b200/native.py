@@ -28,7 +28,7 @@ EXPORTS = ("jfg_model_create", "jfg_pattern", "jfg_pattern_fill", "jfg_assemble_
            "jfg_recover_stresses_device", "jfg_kg_contract", "jfg_kg_contract_device", "jfg_server_create", "jfg_server_submit", "jfg_server_wait",
            "jfg_server_result", "jfg_server_release", "jfg_server_stats", "jfg_server_family_batch",
            "jfg_server_hold", "jfg_server_last_error", "jfg_server_destroy", "jfg_group_create", "jfg_group_member", "jfg_autotune", "jfg_launch_config", "jfg_assemble_batch_device_ws",
-           "jfg_shell_thickness", "jfg_server_create_units",
+           "jfg_shell_thickness", "jfg_server_create_units", "jfg_kg_transfer_entries",
            "jfg_assemble_k_quad4_noalloc", "jfg_model_destroy", "jfg_last_error",
            "jfg_version")
 
@@ -77,6 +77,8 @@ def load(path: str = LIB_PATH):
     L.jfg_assemble_batch_device_ws.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int64] + [C.c_void_p] * 3 + \
         [C.c_int64] + [C.c_void_p] * 4
     L.jfg_assemble_batch_device_ws.restype = C.c_int32
+    L.jfg_kg_transfer_entries.argtypes = [C.c_void_p, _pi64]
+    L.jfg_kg_transfer_entries.restype = C.c_int32
     L.jfg_shell_thickness.argtypes = [C.c_void_p, _pd]
     L.jfg_shell_thickness.restype = C.c_int32
     L.jfg_server_create_units.argtypes = [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int32, _pi32, _pi32, C.c_int32,
@@ -375,6 +377,12 @@ class GpuModel:
         ms = np.zeros(6); n = C.c_int64()
         self._check(self.L.jfg_timing_accumulated(self.h, 0 if kind == "k" else 1, _ptr(ms, _pd), C.byref(n), int(reset)))
         return dict(zip(("quad4", "tria3", "bar", "dof_reduce", "block_reduce", "diag"), ms.tolist())), int(n.value)
+
+    def kg_transfer_entries(self) -> int:
+        """KG values a pageable host-buffer call moves over the bus (-1 before the first such call)."""
+        n = C.c_int64()
+        self._check(self.L.jfg_kg_transfer_entries(self.h, C.byref(n)))
+        return int(n.value)
 
     def stats(self) -> dict:
         out = np.zeros(8, np.int64)

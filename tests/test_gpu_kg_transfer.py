@@ -38,6 +38,8 @@ def test_compacted_kg_equals_device_values(cuda_device, monkeypatch, make):
         assert np.array_equal(got, ref)
         dead = got == 0.0
         assert dead.mean() > 0.5 and not np.signbit(got[dead]).any()
+        n_live = g.kg_transfer_entries()                          # entries that crossed the bus
+        assert np.count_nonzero(got) <= n_live < g.nnz
         again = np.full(g.nnz, np.nan)
         g.assemble_kg(u, again)                                   # a second call reuses the mask
         assert np.array_equal(again, ref)
