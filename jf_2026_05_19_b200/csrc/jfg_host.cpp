@@ -7,8 +7,12 @@
 namespace jfg_host {
 
 bool have_avx512() {
+#ifdef JFG_HOST_SCALAR  // test builds of the portable path
+    return false;
+#else
     static const bool v = __builtin_cpu_supports("avx512f");
     return v;
+#endif
 }
 
 namespace {

@@ -26,13 +26,16 @@ int t_avx512() { return jfg_host::have_avx512() ? 1 : 0; }
 '''
 
 
-@pytest.fixture(scope="module")
-def lib(tmp_path_factory):
-    d = tmp_path_factory.mktemp("hostcopy")
+@pytest.fixture(scope="module", params=["vector", "scalar"])
+def lib(tmp_path_factory, request):
+    """The routines as the library builds them (AVX-512 where the CPU has it) and
+    with the portable path forced."""
+    d = tmp_path_factory.mktemp("hostcopy_" + request.param)
     w = d / "wrap.cpp"
     w.write_text(WRAP)
     so = d / "libt.so"
-    subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-I", CSRC, str(w),
+    flags = ["-DJFG_HOST_SCALAR"] if request.param == "scalar" else []
+    subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", *flags, "-I", CSRC, str(w),
                     os.path.join(CSRC, "jfg_host.cpp"), "-o", str(so)], check=True)
     L = C.CDLL(str(so))
     L.t_copy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
