@@ -418,7 +418,7 @@ jfg_status jfg_shell_thickness(jfg_model *m, double *h_host);
  *   cfg[0] warps per CQUAD4 CTA, 4 or 8 (12 or 24 elements per CTA)
  *   cfg[1] warps per CTRIA3-stiffness CTA, 2 or 4 (4 or 8 elements)
  *   cfg[2..4] elements per CTA of the CTRIA3 KG, bar K and bar KG kernels
- *          (one thread per element node pair): 32, 64 or 128
+ *          (one thread per CTRIA3, per bar node pair): 32, 64 or 128
  * The choice is stored per kernel and model-size class (floor(log2) of the
  * element count of the kernel's type) in a text file: JFG_TUNE_FILE, else
  * $HOME/.cache/jfem_b200/launch_tune.txt.  flags: JFG_TUNE_READ takes a stored

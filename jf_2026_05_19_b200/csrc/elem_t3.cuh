@@ -440,23 +440,32 @@ __global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t n
     }
 }
 
-// One (element, node pair) per thread, laid out pair-major so that a warp
-// runs one compile-time pair; each thread recomputes the element's frame and
-// membrane stress (cheap) and writes its own pair block.
-template <int PA, int PB>
-__device__ __forceinline__ void t3_kg_pair(int64_t e, const int32_t *__restrict__ nodes, const double *__restrict__ prop,
-                                           const double *__restrict__ coords, const double *__restrict__ nodeR,
-                                           const double *__restrict__ u, const ElemOut &o) {
+// One CTRIA3 per thread: frame, node blocks and the CST membrane stress
+// once, then the six node-pair blocks s_ab * Q_a' Q_b (shell KG acts on
+// translations only).
+__global__ void __launch_bounds__(128) t3_kg_kernel(int64_t nt, const int32_t *__restrict__ nodes,
+                                                   const double *__restrict__ prop,
+                                                   const double *__restrict__ coords,
+                                                   const double *__restrict__ nodeR,
+                                                   const double *__restrict__ u, ElemOut o) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nt) return;
+    o = o.at(blockIdx.y);
+    u += (int64_t)blockIdx.y * o.u_stride;
     int32_t nd[3];
     double p[3][3];
+#pragma unroll
     for (int k = 0; k < 3; ++k) {
         nd[k] = __ldg(nodes + 3 * e + k);
+#pragma unroll
         for (int i = 0; i < 3; ++i) p[k][i] = __ldg(coords + 3 * (int64_t)nd[k] + i);
     }
     double v1[3], v2[3], v3[3];
     t3_frame(p[0], p[1], p[2], v1, v2, v3);
     double c[3], lc[3][2];
+#pragma unroll
     for (int i = 0; i < 3; ++i) c[i] = (p[0][i] + p[1][i] + p[2][i]) / 3.0;
+#pragma unroll
     for (int k = 0; k < 3; ++k) {
         double d[3];
         sub3(p[k], c, d);
@@ -464,72 +473,60 @@ __device__ __forceinline__ void t3_kg_pair(int64_t e, const int32_t *__restrict_
         lc[k][1] = dot3(d, v2);
     }
     double Q[3][9];
+#pragma unroll
     for (int k = 0; k < 3; ++k) {
         double Rl[9];
         if (nodeR)
+#pragma unroll
             for (int i = 0; i < 9; ++i) Rl[i] = __ldg(nodeR + 9 * (int64_t)nd[k] + i);
         node_block(v1, v2, v3, nodeR ? Rl : nullptr, Q[k]);
     }
     const double *pr = prop + 7 * e;
     const double h = o.thickness(e, pr), E = __ldg(pr + 1), nu = __ldg(pr + 2);
-    double x[3] = {lc[0][0], lc[1][0], lc[2][0]}, y[3] = {lc[0][1], lc[1][1], lc[2][1]};
-    double A = 0.5 * fabs(x[0] * (y[1] - y[2]) + x[1] * (y[2] - y[0]) + x[2] * (y[0] - y[1]));
+    const double x[3] = {lc[0][0], lc[1][0], lc[2][0]}, y[3] = {lc[0][1], lc[1][1], lc[2][1]};
+    const double A = 0.5 * fabs(x[0] * (y[1] - y[2]) + x[1] * (y[2] - y[0]) + x[2] * (y[0] - y[1]));
     double val[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
     if (A >= 1e-12 && h >= 1e-30) {
-        double b[3] = {(y[1] - y[2]) / (2 * A), (y[2] - y[0]) / (2 * A), (y[0] - y[1]) / (2 * A)};
-        double cv[3] = {(x[2] - x[1]) / (2 * A), (x[0] - x[2]) / (2 * A), (x[1] - x[0]) / (2 * A)};
+        const double b[3] = {(y[1] - y[2]) / (2 * A), (y[2] - y[0]) / (2 * A), (y[0] - y[1]) / (2 * A)};
+        const double cv[3] = {(x[2] - x[1]) / (2 * A), (x[0] - x[2]) / (2 * A), (x[1] - x[0]) / (2 * A)};
         double eps0 = 0.0, eps1 = 0.0, eps2 = 0.0;
+#pragma unroll
         for (int k = 0; k < 3; ++k) {
             const double *ug = u + 6 * (int64_t)nd[k];
-            double u0 = __ldg(ug), u1 = __ldg(ug + 1), u2 = __ldg(ug + 2);
-            double ul = Q[k][0] * u0 + Q[k][1] * u1 + Q[k][2] * u2;
-            double vl = Q[k][3] * u0 + Q[k][4] * u1 + Q[k][5] * u2;
+            const double u0 = __ldg(ug), u1 = __ldg(ug + 1), u2 = __ldg(ug + 2);
+            const double ul = Q[k][0] * u0 + Q[k][1] * u1 + Q[k][2] * u2;
+            const double vl = Q[k][3] * u0 + Q[k][4] * u1 + Q[k][5] * u2;
             eps0 += b[k] * ul;
             eps1 += cv[k] * vl;
             eps2 += cv[k] * ul + b[k] * vl;
         }
-        double cm = E / (1 - nu * nu);
-        double Nx = (cm * eps0 + cm * nu * eps1) * h;
-        double Ny = (cm * nu * eps0 + cm * eps1) * h;
-        double Nxy = (cm * (1 - nu) / 2 * eps2) * h;
-        double sxx = Nx / h, syy = Ny / h, sxy = Nxy / h;
+        const double cm = E / (1 - nu * nu);
+        const double Nx = (cm * eps0 + cm * nu * eps1) * h;
+        const double Ny = (cm * nu * eps0 + cm * eps1) * h;
+        const double Nxy = (cm * (1 - nu) / 2 * eps2) * h;
+        const double sxx = Nx / h, syy = Ny / h, sxy = Nxy / h;
+#pragma unroll
         for (int i = 0; i < 3; ++i)
+#pragma unroll
             for (int j = 0; j < 3; ++j)
                 val[i][j] = h * A * (sxx * b[i] * b[j] + syy * cv[i] * cv[j] + sxy * (b[i] * cv[j] + cv[i] * b[j]));
     }
-    double L[3][3] = {{val[PA][PB], 0, 0}, {0, val[PA][PB], 0}, {0, 0, val[PA][PB]}};
-    double O[3][3];
-    rot_block(Q[PA], L, Q[PB], O);
-    const int32_t s = __ldg(o.blk_slot + e * 6 + packed_index(PA, PB, 3));
-    // staged blocks of KG shells are read as their translation 3x3 only; the
-    // dof-level RBE2 path (s < 0) reads whole raw blocks
 #pragma unroll
-    for (int i = 0; i < 6; ++i)
+    for (int pp = 0; pp < 6; ++pp) {
+        const int pa = (pp >= 3) + (pp >= 5), pb = pa + pp - (pa == 0 ? 0 : (pa == 1 ? 3 : 5));
+        const double L[3][3] = {{val[pa][pb], 0, 0}, {0, val[pa][pb], 0}, {0, 0, val[pa][pb]}};
+        double O[3][3];
+        rot_block(Q[pa], L, Q[pb], O);
+        const int32_t sl = __ldg(o.blk_slot + e * 6 + pp);
+        // staged blocks of KG shells are read as their translation 3x3 only; the
+        // dof-level RBE2 path (sl < 0) reads whole raw blocks
 #pragma unroll
-        for (int j = 0; j < 6; ++j)
-            if (i < 3 && j < 3) *blk_entry(o, s, i, j) = O[i][j];
-            else if (s < 0) *blk_entry(o, s, i, j) = 0.0;
-    kg_shell_pad(o, s);
-}
-
-__global__ void __launch_bounds__(128) t3_kg_kernel(int64_t nt, const int32_t *__restrict__ nodes,
-                                                   const double *__restrict__ prop,
-                                                   const double *__restrict__ coords,
-                                                   const double *__restrict__ nodeR,
-                                                   const double *__restrict__ u, ElemOut o) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int pair = (int)(t / nt);
-    const int64_t e = t - (int64_t)pair * nt;
-    o = o.at(blockIdx.y);
-    u += (int64_t)blockIdx.y * o.u_stride;
-    switch (pair) {
-        case 0: t3_kg_pair<0, 0>(e, nodes, prop, coords, nodeR, u, o); break;
-        case 1: t3_kg_pair<0, 1>(e, nodes, prop, coords, nodeR, u, o); break;
-        case 2: t3_kg_pair<0, 2>(e, nodes, prop, coords, nodeR, u, o); break;
-        case 3: t3_kg_pair<1, 1>(e, nodes, prop, coords, nodeR, u, o); break;
-        case 4: t3_kg_pair<1, 2>(e, nodes, prop, coords, nodeR, u, o); break;
-        case 5: t3_kg_pair<2, 2>(e, nodes, prop, coords, nodeR, u, o); break;
-        default: break;
+        for (int i = 0; i < 6; ++i)
+#pragma unroll
+            for (int j = 0; j < 6; ++j)
+                if (i < 3 && j < 3) *blk_entry(o, sl, i, j) = O[i][j];
+                else if (sl < 0) *blk_entry(o, sl, i, j) = 0.0;
+        kg_shell_pad(o, sl);
     }
 }
 

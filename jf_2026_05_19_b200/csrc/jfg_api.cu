@@ -151,7 +151,7 @@ struct jfg_model {
     bool blk_even = false;
     // launch shapes (jfg_autotune): warps per CQUAD4 CTA (3 elements each,
     // 4 or 8), warps per CTRIA3-stiffness CTA (2 elements each, 2 or 4), and
-    // threads (elements of one node pair) per CTA of the CTRIA3 KG, bar K and
+    // threads per CTA of the CTRIA3 KG (one element each), bar K and
     // bar KG kernels (32, 64 or 128)
     int q4_warps = 4, t3_warps = 4;
     int t3kg_threads = 128, bark_threads = 128, barkg_threads = 128;
@@ -1710,7 +1710,7 @@ jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
         o.h_stride = m->nq + m->nt;
         const int tt = m->t3kg_threads, W3 = m->t3_warps;
         if (kg)
-            t3_kg_kernel<<<dim3((unsigned)cdiv(6 * m->nt, tt), nv), tt, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords,
+            t3_kg_kernel<<<dim3((unsigned)cdiv(m->nt, tt), nv), tt, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords,
                                                                                    m->d_nodeR, du, o);
         else if (W3 == 2)
             t3_k_kernel<2><<<dim3((unsigned)cdiv(m->nt, T3_TEAMS_PER_WARP * 2), nv), 64, 0, m->stream>>>(
