@@ -198,7 +198,7 @@ __host__ __device__ constexpr int t3_mnode(int I) { return I < 4 ? I + 3 : I - 4
 // kernel, by 3x3-block elimination of the four internal nodes.  The 28 upper
 // blocks of the macro system are summed from the quads' plate blocks (quad
 // order), then for each internal node K: its pivot block D = L diag(d) L' in
-// closed form (the three reciprocals 1/D00, D00/m2, m2/det are independent),
+// closed form (1/D00, D00/m2 and m2/det from one reciprocal of D00 m2 det),
 // Z_J = L^-1 A_KJ and Zs_J = diag(d)^-1 Z_J for every later node J, and every
 // later block A_IJ -= Z_I' Zs_J.  Kii is symmetric positive definite, so this
 // unpivoted elimination matches the reference's pivoted LU up to rounding.
@@ -239,7 +239,9 @@ __device__ __forceinline__ void t3_schur(T3KShared &S, int tl, unsigned tm) {
         const double D00 = D[0], D01 = D[1], D02 = D[2], D11 = D[4], D12 = D[5], D22 = D[8];
         const double m2 = D00 * D11 - D01 * D01;
         const double det = D00 * (D11 * D22 - D12 * D12) - D01 * (D01 * D22 - D12 * D02) + D02 * (D01 * D12 - D11 * D02);
-        const double i0 = 1.0 / D00, i1 = D00 / m2, i2 = m2 / det;
+        // 1/D00, D00/m2 and m2/det from one reciprocal of D00 m2 det
+        const double r = 1.0 / (D00 * m2 * det);
+        const double i0 = (m2 * det) * r, i1 = D00 * ((D00 * det) * r), i2 = m2 * ((D00 * m2) * r);
         const double l10 = D01 * i0, l20 = D02 * i0, l21 = (D12 - l20 * D01) * i1;
         if (tl < n) {
             const double *B = A[t3_pblk(K, K + 1 + tl)];

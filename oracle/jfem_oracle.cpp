@@ -795,8 +795,15 @@ void local_u_scale(int nn, const int32_t *nd, const double *Q, const double *u, 
 // of every Gauss point over the magnitudes of its strain terms (B u and the
 // incompatible modes B_i alpha, alpha = -K_bb^-1 K_ab' u), then both
 // principal directions with |lambda| <= |sxx| + |syy| + 2 |sxy| and
-// |cos|, |sin| <= 1 over the gradient vectors' magnitudes.
-void q4_kg_scale(const double lc[4][2], const double us[24], const double Cm[3][3], double h, double M[24][24]) {
+// |cos|, |sin| <= 1 over the gradient vectors' magnitudes.  The direction
+// itself, theta = atan2(2 sxy, sxx - syy) / 2, moves by the stress rounding
+// over twice the deviatoric radius rad = |lambda_1 - lambda_2| / 2, and the
+// transverse terms move with it (d/dtheta of a unit direction is bounded by
+// the same gradient magnitudes): near an equibiaxial stress the reference's
+// own KG is that ill-conditioned, so the scale grows as 1 / rad there.
+// sig holds the Gauss-point stresses the element computed.
+void q4_kg_scale(const double lc[4][2], const double us[24], const double Cm[3][3], double h, const double sig[4][3],
+                 double M[24][24]) {
     std::memset(M, 0, sizeof(double) * 576);
     if (h < 1e-30) return;
     const double pt = 1.0 / std::sqrt(3.0);
@@ -859,8 +866,11 @@ void q4_kg_scale(const double lc[4][2], const double us[24], const double Cm[3][
             Gxy[a] += (std::fabs(d1x) + std::fabs(d1y)) * (std::fabs(Amap[0][a]) + std::fabs(Amap[1][a])) +
                       (std::fabs(d2x) + std::fabs(d2y)) * (std::fabs(Amap[2][a]) + std::fabs(Amap[3][a]));
         const double f = 2.0 * h * det[g] * lam;
+        const double hd = 0.5 * (sig[g][0] - sig[g][1]), rad = std::sqrt(hd * hd + sig[g][2] * sig[g][2]);
+        const double dth = lam / (2.0 * std::max(rad, 1e-30));  // rounding of theta, in units of eps
         for (int i = 0; i < 24; ++i)
-            for (int j = 0; j < 24; ++j) M[i][j] += f * (Gxy[i] * Gxy[j] + Gz[i] * Gz[j]);
+            for (int j = 0; j < 24; ++j)
+                M[i][j] += f * (Gxy[i] * Gxy[j] + Gz[i] * Gz[j]) + f * dth * (4.0 * Gxy[i] * Gxy[j] + 2.0 * Gz[i] * Gz[j]);
     }
 }
 
@@ -1838,7 +1848,7 @@ int kg_element_triplets(const jfg_model_desc *d, const double *u, Triplets &t, s
         if (g_abs_sums) {
             double us[24], Ml[24][24], Mg[576];
             local_u_scale(4, nd, Q, u, us);
-            q4_kg_scale(lc, us, Cm, h, Ml);
+            q4_kg_scale(lc, us, Cm, h, sig, Ml);
             transform_sym_abs(4, Q, &Ml[0][0], Mg);
             int q = 0;
             for (int cc = 0; cc < 24; ++cc)
