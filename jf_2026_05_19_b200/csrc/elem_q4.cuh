@@ -325,12 +325,14 @@ __device__ __forceinline__ void macneal_zs(const double lc[4][2], double cb, dou
     const double J22c = 0.25 * (-lc[0][1] - lc[1][1] + lc[2][1] + lc[3][1]);
     const double A_elem = 4.0 * fabs(J11c * J22c - J12c * J21c);
     const double eps = 0.04;
-    const double ap = eps / (eps + (1.0 - eps) * Dx2 / fmax(Dy2, 1e-30));
-    const double bp = eps / (eps + (1.0 - eps) * Dy2 / fmax(Dx2, 1e-30));
-    const double flex = 1.0 / fmax(fabs(cb), 1e-30);
-    const double c12 = 0.65 * (1.0 / (12.0 * A_elem));
-    const double zxu = c12 * Dx2 * flex, zxd = c12 * ap * Dx2 * flex;
-    const double zyu = c12 * Dy2 * flex, zyd = c12 * bp * Dy2 * flex;
+    // ap = eps / (eps + (1 - eps) Dx2 / Dy2) and bp likewise, each as one
+    // quotient; c12 * flex = 0.65 / (12 A_elem) / |cb| as one quotient
+    const double dy2 = fmax(Dy2, 1e-30), dx2 = fmax(Dx2, 1e-30);
+    const double ap = (eps * dy2) / (eps * dy2 + (1.0 - eps) * Dx2);
+    const double bp = (eps * dx2) / (eps * dx2 + (1.0 - eps) * Dy2);
+    const double cf = 0.65 / (12.0 * A_elem * fmax(fabs(cb), 1e-30));
+    const double zxu = cf * Dx2, zxd = cf * ap * Dx2;
+    const double zyu = cf * Dy2, zyd = cf * bp * Dy2;
     zs[0] = zxu + zxd; zs[1] = zxu - zxd; zs[2] = zyu + zyd; zs[3] = zyu - zyd;
 }
 
@@ -348,7 +350,8 @@ __device__ __forceinline__ double macneal_ivd(double det, double cs) {
 __device__ __forceinline__ void macneal_w(const double ivd[4], const double zs[4], double W[6]) {
     const double zx00 = ivd[0] + zs[0], zx11 = ivd[1] + zs[0], zx01 = zs[1];
     const double zy00 = ivd[2] + zs[2], zy11 = ivd[3] + zs[2], zy01 = zs[3];
-    const double ix = 1.0 / (zx00 * zx11 - zx01 * zx01), iy = 1.0 / (zy00 * zy11 - zy01 * zy01);
+    const double dx = zx00 * zx11 - zx01 * zx01, dy = zy00 * zy11 - zy01 * zy01;
+    const double r = 1.0 / (dx * dy), ix = dy * r, iy = dx * r;  // both inverses from one reciprocal
     W[0] = zx11 * ix; W[1] = -zx01 * ix; W[2] = zx00 * ix;
     W[3] = zy11 * iy; W[4] = -zy01 * iy; W[5] = zy00 * iy;
 }

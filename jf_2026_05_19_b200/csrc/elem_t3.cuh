@@ -44,6 +44,7 @@ __constant__ int c_t3_quads[3][4] = {{0, 3, 6, 5}, {1, 4, 6, 3}, {2, 5, 6, 4}};
 
 struct __align__(16) T3KShared {
     double V[9];
+    double R[3][9];  // stiffness kernel: the corners' CD frames, loaded in the set-up phase
     double bv[3], cv[3], A, cm, ad;
     int nd[3];
     union {
@@ -315,6 +316,13 @@ __global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t n
 #pragma unroll
             for (int i = 0; i < 3; ++i) p[k][i] = __ldg(coords + 3 * (int64_t)nd[k] + i);
         }
+        // the corners' CD frames into shared memory now, off the output phase's path
+        if (nodeR)
+            for (int i = tl; i < 27; i += T3_TEAM) {
+                const int k = i < 9 ? 0 : (i < 18 ? 1 : 2);
+                const int64_t n = k == 0 ? nd[0] : (k == 1 ? nd[1] : nd[2]);
+                S.R[k][i - 9 * k] = __ldg(nodeR + 9 * n + (i - 9 * k));
+            }
         double v1[3], v2[3], v3[3];
         t3_frame(p[0], p[1], p[2], v1, v2, v3);
         double c[3];
@@ -384,14 +392,8 @@ __global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t n
         }
         double Qa[9], Qb[9];
         if (nodeR) {
-            double Ra[9], Rb[9];
-#pragma unroll
-            for (int i = 0; i < 9; ++i) {
-                Ra[i] = __ldg(nodeR + 9 * (int64_t)S.nd[a] + i);
-                Rb[i] = __ldg(nodeR + 9 * (int64_t)S.nd[b] + i);
-            }
-            node_block(S.V, S.V + 3, S.V + 6, Ra, Qa);
-            node_block(S.V, S.V + 3, S.V + 6, Rb, Qb);
+            node_block(S.V, S.V + 3, S.V + 6, S.R[a], Qa);
+            node_block(S.V, S.V + 3, S.V + 6, S.R[b], Qb);
         } else {
 #pragma unroll
             for (int i = 0; i < 9; ++i) { Qa[i] = S.V[i]; Qb[i] = S.V[i]; }
