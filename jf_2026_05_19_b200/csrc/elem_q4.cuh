@@ -444,11 +444,12 @@ __global__ void __launch_bounds__(32 * W, 16 / W) q4_k_kernel(int64_t nq, const 
         q4_local(p, V, lc);
     }
     const double gam = (1 - nu) / 2;
-    const double cm = E * h / (1 - nu * nu);
-    const double cb = br * (E * h * h * h) / (12 * (1 - nu * nu));
+    const double inu = 1.0 / (1 - nu * nu);  // one reciprocal for cm, cb and G_drill
+    const double cm = E * h * inu;
+    const double cb = br * (E * h * h * h) * (inu * (1.0 / 12.0));
     const bool membrane_only = br <= 1e-12;
     const double cs = membrane_only ? 0.0 : tst * h * Gs;
-    double G_drill = (cm * gam) / h;
+    double G_drill = E * inu * gam;  // Cm33 / h
     if (G_drill < 1e-6) G_drill = E / (2 * 3.0);
     const double ad = membrane_only ? 0.0 : (k6rot / 1e5) * G_drill * h;
     const bool skip_mac = h < 1e-30 || fabs(cs) < 1e-30;
@@ -869,14 +870,17 @@ __global__ void __launch_bounds__(32 * W) q4_kg_kernel(int64_t nq, const int32_t
             // (cos theta, sin theta) follow from cos 2theta = hd / rad and
             // sin 2theta = sxy / rad by the half-angle identities, taking the
             // square root on the side without cancellation.
+            // With t = 1 / sqrt(2 rad (rad + |hd|)): for hd >= 0,
+            // cos = (rad + hd) t and sin = sxy t; otherwise sin =
+            // sign(sxy) (rad - hd) t and cos = |sxy| t.
             double c1, s1;
-            const double i2r = 1.0 / (2.0 * rad);
+            const double ah = fabs(hd), t = rsqrt(2.0 * rad * (rad + ah));
             if (hd >= 0.0) {
-                c1 = sqrt((rad + hd) * i2r);
-                s1 = (sxy * i2r) / c1;
+                c1 = (rad + ah) * t;
+                s1 = sxy * t;
             } else {
-                s1 = copysign(sqrt((rad - hd) * i2r), sxy);
-                c1 = (sxy * i2r) / s1;
+                s1 = copysign((rad + ah) * t, sxy);
+                c1 = fabs(sxy) * t;
             }
             if (dir == 0) { lam = mean + rad; c = c1; sn = s1; }
             else { lam = mean - rad; c = -s1; sn = c1; }

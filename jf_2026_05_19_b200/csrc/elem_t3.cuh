@@ -336,8 +336,9 @@ __global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t n
         }
         A = 0.5 * fabs(x[0] * (y[1] - y[2]) + x[1] * (y[2] - y[0]) + x[2] * (y[0] - y[1]));
         gam = (1 - nu) / 2;
-        const double cm = E * h / (1 - nu * nu);
-        cb = br * (E * h * h * h) / (12 * (1 - nu * nu));
+        const double inu = 1.0 / (1 - nu * nu);  // one reciprocal for cm and cb
+        const double cm = E * h * inu;
+        cb = br * (E * h * h * h) * (inu * (1.0 / 12.0));
         const bool membrane_only = br <= 1e-12;
         cs = membrane_only ? 0.0 : tst * h * Gs;
         plate = !membrane_only && A >= 1e-12;
