@@ -288,15 +288,21 @@ __device__ __forceinline__ void rot_sparse(const double *Qa, const double M[3][3
 // Solve B x = rhs with the LDL' factors of the packed SPD 4x4 B.
 struct Ldl4 {
     double l10, l20, l30, l21, l31, l32, r0, r1, r2, r3;
+    // The first three pivots are ratios of leading principal minors,
+    // d0 = m1, d1 = m2 / m1, d2 = m3 / m2, so their reciprocals come from one
+    // division, 1 / (m1 m2 m3), instead of a chain of three.
     __device__ __forceinline__ explicit Ldl4(const double *B) {
         const double b00 = B[0], b01 = B[1], b02 = B[2], b03 = B[3], b11 = B[4], b12 = B[5], b13 = B[6];
         const double b22 = B[7], b23 = B[8], b33 = B[9];
-        r0 = 1.0 / b00;
+        const double m1 = b00, m2 = b00 * b11 - b01 * b01;
+        const double m3 = b00 * (b11 * b22 - b12 * b12) - b01 * (b01 * b22 - b12 * b02) + b02 * (b01 * b12 - b11 * b02);
+        const double R = 1.0 / (m1 * m2 * m3);
+        r0 = (m2 * m3) * R;
+        r1 = m1 * ((m1 * m3) * R);
+        r2 = m2 * ((m1 * m2) * R);
         l10 = b01 * r0; l20 = b02 * r0; l30 = b03 * r0;
-        r1 = 1.0 / (b11 - l10 * b01);
         const double u12 = b12 - l10 * b02, u13 = b13 - l10 * b03;
         l21 = u12 * r1; l31 = u13 * r1;
-        r2 = 1.0 / (b22 - l20 * b02 - l21 * u12);
         const double u23 = b23 - l20 * b03 - l21 * u13;
         l32 = u23 * r2;
         r3 = 1.0 / (b33 - l30 * b03 - l31 * u13 - l32 * u23);
