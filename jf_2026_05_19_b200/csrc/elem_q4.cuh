@@ -743,7 +743,9 @@ __global__ void __launch_bounds__(32 * W) q4_kg_kernel(int64_t nq, const int32_t
         q4_local(p, V, lc);
     }
     const double gam = (1 - nu) / 2;
-    const double cmh = (E / (1 - nu * nu)) * h;  // Cm = cmh P(nu)
+    const double rdh = 1.0 / ((1 - nu * nu) * h);  // one reciprocal for cmh and 1/h
+    const double cmh = E * h * h * rdh;             // Cm = cmh P(nu)
+    const double ih = (1 - nu * nu) * rdh;
 
     // Phase 1: Gauss-point derivatives (lanes 0-3); local membrane
     // displacements u_elem = T u_global (lanes 4-7, assembly.jl:5176-5185).
@@ -859,7 +861,6 @@ __global__ void __launch_bounds__(32 * W) q4_kg_kernel(int64_t nq, const int32_t
         exx += d1x * alpha[0] + d2x * alpha[2];
         eyy += d1y * alpha[1] + d2y * alpha[3];
         gxy += d1y * alpha[0] + d1x * alpha[1] + d2y * alpha[2] + d2x * alpha[3];
-        const double ih = 1.0 / h;
         const double sxx = (cmh * (exx + nu * eyy)) * ih;
         const double syy = (cmh * (nu * exx + eyy)) * ih;
         const double sxy = (cmh * (gam * gxy)) * ih;
