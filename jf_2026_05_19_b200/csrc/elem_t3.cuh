@@ -68,7 +68,8 @@ struct __align__(16) T3KShared {
 
 // Corner coordinates of virtual quad q (corner q, midpoint to the next
 // corner, centroid, midpoint from the previous corner), as the macro points
-// (x_i + x_j) / 2 and (x_0 + x_1 + x_2) / 3 of tria3_plate_macro_data.
+// (x_i + x_j) / 2 and (x_0 + x_1 + x_2) / 3 of tria3_plate_macro_data (the
+// thirds as a product with 1/3, no division on the points' path).
 __device__ __forceinline__ void t3_quad_coords(int q, const double x[3], const double y[3], double lq[4][2]) {
     const int n = q == 2 ? 0 : q + 1, pv = q == 0 ? 2 : q - 1;
     const double xc = q == 0 ? x[0] : (q == 1 ? x[1] : x[2]), yc = q == 0 ? y[0] : (q == 1 ? y[1] : y[2]);
@@ -76,7 +77,7 @@ __device__ __forceinline__ void t3_quad_coords(int q, const double x[3], const d
     const double xp = pv == 0 ? x[0] : (pv == 1 ? x[1] : x[2]), yp = pv == 0 ? y[0] : (pv == 1 ? y[1] : y[2]);
     lq[0][0] = xc; lq[0][1] = yc;
     lq[1][0] = (xc + xn) / 2; lq[1][1] = (yc + yn) / 2;
-    lq[2][0] = (x[0] + x[1] + x[2]) / 3; lq[2][1] = (y[0] + y[1] + y[2]) / 3;
+    lq[2][0] = (x[0] + x[1] + x[2]) * (1.0 / 3.0); lq[2][1] = (y[0] + y[1] + y[2]) * (1.0 / 3.0);
     lq[3][0] = (xp + xc) / 2; lq[3][1] = (yp + yc) / 2;
 }
 
@@ -326,7 +327,7 @@ __global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t n
         double v1[3], v2[3], v3[3];
         t3_frame(p[0], p[1], p[2], v1, v2, v3);
         double c[3];
-        for (int i = 0; i < 3; ++i) c[i] = (p[0][i] + p[1][i] + p[2][i]) / 3.0;
+        for (int i = 0; i < 3; ++i) c[i] = (p[0][i] + p[1][i] + p[2][i]) * (1.0 / 3.0);
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             double d[3];
@@ -469,7 +470,7 @@ __global__ void __launch_bounds__(128) t3_kg_kernel(int64_t nt, const int32_t *_
     t3_frame(p[0], p[1], p[2], v1, v2, v3);
     double c[3], lc[3][2];
 #pragma unroll
-    for (int i = 0; i < 3; ++i) c[i] = (p[0][i] + p[1][i] + p[2][i]) / 3.0;
+    for (int i = 0; i < 3; ++i) c[i] = (p[0][i] + p[1][i] + p[2][i]) * (1.0 / 3.0);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         double d[3];
