@@ -506,6 +506,9 @@ def run_serving(args):
             warm = [srv.submit(f, pools[f][0], keep=False) for f in range(len(fams))]
             for t in warm:
                 srv.wait(t, -1.0); srv.release(t)
+            # warm-up stream at the top rate (another seed), so batches of every size the
+            # measured streams form have run once before the timing
+            run_server_stream(native, srv, serving_stream(max(rates), 64, len(fams), 1), pools)
             res = {}
             b0 = srv.stats()["batches"]
             for r in rates:
