@@ -126,6 +126,9 @@ struct jfg_model {
     std::string err;
     cudaStream_t stream = nullptr;
     cudaStream_t own = nullptr;
+    // the RBE2-path sums and orig_diag run here, beside the block reductions
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     bool own_stream = false;
     int device = 0;
     int64_t n_nodes = 0, ndof = 0, nq = 0, nt = 0, nb = 0;
@@ -207,7 +210,8 @@ struct jfg_model {
     std::vector<double> dep_coef;
     // ring of event sets, one per assembly call, so that per-kernel device
     // times can be accumulated over many back-to-back calls without a sync
-    struct EvSet { cudaEvent_t e[7]; int kind; bool pending; };
+    // e[7], e[8]: ends of the RBE2-path sums and of orig_diag on the side stream
+    struct EvSet { cudaEvent_t e[9]; int kind; bool pending; bool side; };
     static constexpr int kRing = 64;
     EvSet ring[kRing];
     int ring_head = 0, last_set = -1;
@@ -986,6 +990,12 @@ void jfg_model_destroy(jfg_model *m) {
         cudaStreamSynchronize(m->own);
         cudaStreamDestroy(m->own);
     }
+    if (m->side) {
+        cudaStreamSynchronize(m->side);
+        cudaStreamDestroy(m->side);
+    }
+    for (cudaEvent_t e : {m->fork_ev, m->join_ev})
+        if (e) cudaEventDestroy(e);
     if (m->pin) cudaFreeHost(m->pin);
     for (auto &e : m->pin_ev)
         if (e) cudaEventDestroy(e);
@@ -1002,11 +1012,20 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
     CK(cudaGetDevice(&m->device));
     CK(set_q4_smem_limits());
     CK(cudaStreamCreateWithFlags(&m->own, cudaStreamNonBlocking));
+    {
+        // highest priority: its few CTAs go ahead of the queued block-reduction CTAs
+        int least = 0, greatest = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CK(cudaStreamCreateWithPriority(&m->side, cudaStreamNonBlocking, greatest));
+    }
+    CK(cudaEventCreateWithFlags(&m->fork_ev, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&m->join_ev, cudaEventDisableTiming));
     m->stream = m->own;
     m->own_stream = true;
     for (auto &set : m->ring) {
         for (auto &e : set.e) CK(cudaEventCreate(&e));
         set.pending = false;
+        set.side = false;
         set.kind = 0;
     }
     m->n_nodes = d->n_nodes;
@@ -1739,16 +1758,34 @@ jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
     return JFG_OK;
 }
 
+// The RBE2-path sums and orig_diag read only what the element kernels wrote
+// and write positions the block reduction never does (RBE2 entries, the
+// diagonal array), so they run on the handle's side stream under the
+// HBM-bound block reduction: fork after the element kernels, join before
+// the call ends (also inside a stream capture, as graph dependencies).
 jfg_status launch_reduce(jfg_model *m, const Batch &bt, bool kg) {
     const unsigned nv = (unsigned)bt.n_var;
-    if (m->n_xkey) {
-        exc_chunk_kernel<<<dim3((unsigned)cdiv(m->n_xchunk * 32, 256), nv), 256, 0, m->stream>>>(
-            m->n_xchunk, m->d_x_cseg, m->d_x_src, m->d_x_w, bt.exc_raw, bt.x_part, bt.exc_stride, bt.part_stride);
+    const bool side = m->n_xkey || bt.ddiag;
+    if (side) {
+        if (!m->capturing) m->ring[m->last_set].side = true;
+        CK(cudaEventRecord(m->fork_ev, m->stream));
+        CK(cudaStreamWaitEvent(m->side, m->fork_ev, 0));
+        if (m->n_xkey) {
+            exc_chunk_kernel<<<dim3((unsigned)cdiv(m->n_xchunk * 32, 256), nv), 256, 0, m->side>>>(
+                m->n_xchunk, m->d_x_cseg, m->d_x_src, m->d_x_w, bt.exc_raw, bt.x_part, bt.exc_stride, bt.part_stride);
+            CK(cudaGetLastError());
+            exc_key_kernel<<<dim3((unsigned)cdiv(m->n_xkey * 32, 256), nv), 256, 0, m->side>>>(
+                m->n_xkey, m->d_x_kchunk, bt.x_part, m->d_x_pos, bt.nz, bt.part_stride, m->nnz);
+            CK(cudaGetLastError());
+        }
+        if (!m->capturing) CK(cudaEventRecord(m->ev[7], m->side));
+        if (bt.ddiag)
+            diag_reduce_kernel<<<dim3((unsigned)cdiv(m->ndof, 256), nv), 256, 0, m->side>>>(m->ndof, m->d_dseg, bt.dstaging,
+                                                                                      bt.ddiag, bt.dstage_stride);
         CK(cudaGetLastError());
-        exc_key_kernel<<<dim3((unsigned)cdiv(m->n_xkey * 32, 256), nv), 256, 0, m->stream>>>(
-            m->n_xkey, m->d_x_kchunk, bt.x_part, m->d_x_pos, bt.nz, bt.part_stride, m->nnz);
+        if (!m->capturing) CK(cudaEventRecord(m->ev[8], m->side));
+        CK(cudaEventRecord(m->join_ev, m->side));
     }
-    CK(cudaGetLastError());
     CK(mark(m, 4));
     if (m->n_blk) {
         const dim3 grid((unsigned)cdiv(cdiv((m->n_blk + 1) / 2, 5), kRedWarps), nv);
@@ -1775,10 +1812,7 @@ jfg_status launch_reduce(jfg_model *m, const Batch &bt, bool kg) {
     }
     CK(cudaGetLastError());
     CK(mark(m, 5));
-    if (bt.ddiag)
-        diag_reduce_kernel<<<dim3((unsigned)cdiv(m->ndof, 256), nv), 256, 0, m->stream>>>(m->ndof, m->d_dseg, bt.dstaging, bt.ddiag,
-                                                                                     bt.dstage_stride);
-    CK(cudaGetLastError());
+    if (side) CK(cudaStreamWaitEvent(m->stream, m->join_ev, 0));
     CK(mark(m, 6));
     return JFG_OK;
 }
@@ -1828,9 +1862,15 @@ jfg_status finish_set(jfg_model *m, int idx) {
     auto &set = m->ring[idx];
     if (!set.pending) return JFG_OK;
     CK(cudaEventSynchronize(set.e[6]));
+    // Sequential calls record e[0..6] in order.  With the side stream, the
+    // RBE2-path sums run e[3] -> e[7] and orig_diag e[7] -> e[8] there, while
+    // the block reduction runs e[4] -> e[5] on the handle's stream.
+    static const int seq[6][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 4}, {4, 5}, {5, 6}};
+    static const int sid[6][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 7}, {4, 5}, {7, 8}};
+    const int(*iv)[2] = set.side ? sid : seq;
     float k[6];
     for (int i = 0; i < 6; ++i) {
-        CK(cudaEventElapsedTime(&k[i], set.e[i], set.e[i + 1]));
+        CK(cudaEventElapsedTime(&k[i], set.e[iv[i][0]], set.e[iv[i][1]]));
         m->acc_ms[set.kind][i] += k[i];
     }
     m->acc_calls[set.kind] += 1;
@@ -1866,6 +1906,7 @@ jfg_status begin_set(jfg_model *m, int kind) {
     m->ring_head = (idx + 1) % jfg_model::kRing;
     m->ring[idx].kind = kind;
     m->ring[idx].pending = true;
+    m->ring[idx].side = false;
     m->last_set = idx;
     m->ev = m->ring[idx].e;
     return JFG_OK;
