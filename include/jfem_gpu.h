@@ -138,7 +138,11 @@ jfg_status jfg_constraint_map(jfg_model *m, int64_t *n_dep, int64_t *n_terms,
                               int64_t *dep_dof, int64_t *term_ptr, int64_t *ind_dof, double *coeff);
 
 /* Set the CUDA stream (a cudaStream_t passed as void*) used by the handle;
- * NULL selects the handle's own stream. */
+ * NULL selects the handle's own stream.  A K / KG call also runs its RBE2-path
+ * sums and orig_diag on an internal high-priority stream that forks from this
+ * stream after the element kernels and joins it before the call's last
+ * operation, so work queued after the call on this stream sees every output
+ * (in a stream capture the fork and join become graph dependencies). */
 jfg_status jfg_set_stream(jfg_model *m, void *stream);
 
 /* Timing of the last assembly on the device (CUDA events around the element
