@@ -9,8 +9,8 @@
 // predicates the library accepts (flat isotropic PSHELL/MAT1 CQUAD4/CTRIA3,
 // CBAR/CBEAM without pin flags, RBE2, PARAM SNORM <= 0, no JFEM_* overrides).
 //
-// PARITY UNPINNED: the reference is Julia 1.12 and cannot run in this build
-// environment (no julia, no network), and it ships no golden vectors or
+// PARITY UNPINNED: the reference is Julia 1.12 and cannot run where this
+// library is built and tested (no julia, no network), and it ships no golden vectors or
 // known-answer tests for this path.  The restatement follows the cited lines;
 // agreement with it is checked by tests, and physics known-answers (symmetry,
 // rigid-body null space, plate buckling coefficient) add sanity checks that
