@@ -171,3 +171,32 @@ def test_abs_sums_bound_the_values():
     a = det["abs_sums"]
     assert a.shape == nz.shape and np.all(a >= np.abs(nz) * (1 - 1e-15))
     assert det["t_elements"] >= 0.0 and det["t_sparse"] >= 0.0
+
+
+def test_kg_rounding_scale_covers_the_equibiaxial_conditioning():
+    """At an equibiaxial membrane stress the principal-transverse KG depends on a
+    principal angle set by rounding noise: one-ulp perturbations of u move the
+    oracle's own KG by a large fraction of the row max.  The rounding scale the
+    parity bound uses must cover that (and stay tight in a generic state)."""
+    from helpers import parity_ratio, rowmax_rel_err
+    m = decks.plate_c1(n=6)
+    x, y = m.coords[:, 0], m.coords[:, 1]
+    rng = np.random.default_rng(0)
+    for d, sensitive in ((0.0, True), (1e-9, True), (None, False)):
+        u = np.zeros(6 * m.n_nodes)
+        if d is None:                                   # uniaxial: a well-defined direction
+            u[0::6] = 1e-3 * x
+        else:
+            u[0::6], u[1::6] = 1e-3 * x, 1e-3 * (1.0 + d) * y
+        cp, rv, nz, det = O.assemble_kg(m, u, detail=True, abs_sums=True)
+        worst_err = worst_ratio = 0.0
+        for _ in range(3):
+            up = u * (1.0 + 2.2e-16 * rng.standard_normal(u.size))
+            nz2 = O.assemble_kg(m, up)[2]
+            worst_err = max(worst_err, rowmax_rel_err(cp, nz, nz2))
+            worst_ratio = max(worst_ratio, parity_ratio(cp, nz, nz2, det["abs_sums"]))
+        if sensitive:
+            assert worst_err > 1e-10, (d, worst_err)    # the reference formula is ill-conditioned here
+        else:
+            assert worst_err < 1e-12, worst_err
+        assert worst_ratio <= 1.0, (d, worst_ratio)
