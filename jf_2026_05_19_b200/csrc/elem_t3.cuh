@@ -56,8 +56,9 @@ struct __align__(16) T3KShared {
             double X[12][9];   // Kii^-1 Kie
             double Kc[9][9];
         } c;
-        struct {  // the stiffness kernel's macro system, 28 upper 3x3 blocks (t3_pblk)
-            double A[28][9];
+        struct {  // the stiffness kernel's macro system, 28 upper 3x3 blocks (t3_pblk),
+                  // each padded to 10 doubles so that it starts on 16 bytes
+            alignas(16) double A[28][10];
         } b;
     } u;
     // quad q, local node pair (a <= b): 3x3 over (w, theta_x, theta_y);
@@ -204,9 +205,22 @@ __host__ __device__ constexpr int t3_mnode(int I) { return I < 4 ? I + 3 : I - 4
 // Z_J = L^-1 A_KJ and Zs_J = diag(d)^-1 Z_J for every later node J, and every
 // later block A_IJ -= Z_I' Zs_J.  Kii is symmetric positive definite, so this
 // unpivoted elimination matches the reference's pivoted LU up to rounding.
-// On return the corner blocks (4 + a, 4 + b) of S.u.b.A hold Kc.
+// On return the corner blocks (4 + a, 4 + b) of S.u.b.A hold Kc.  Blocks and
+// Z columns start on 16 bytes and move as 128-bit shared-memory accesses.
+__device__ __forceinline__ void ld9(const double *p, double v[9]) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    const double2 a = q[0], b = q[1], c = q[2], d = q[3];
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y; v[4] = c.x; v[5] = c.y; v[6] = d.x; v[7] = d.y; v[8] = p[8];
+}
+__device__ __forceinline__ void st9(double *p, const double v[9]) {
+    double2 *q = reinterpret_cast<double2 *>(p);
+    q[0] = make_double2(v[0], v[1]); q[1] = make_double2(v[2], v[3]);
+    q[2] = make_double2(v[4], v[5]); q[3] = make_double2(v[6], v[7]);
+    p[8] = v[8];
+}
+
 __device__ __forceinline__ void t3_schur(T3KShared &S, int tl, unsigned tm) {
-    double(*A)[9] = S.u.b.A;
+    double(*A)[10] = S.u.b.A;
     for (int b = tl; b < 28; b += T3_TEAM) {
         int I = 0, rem = b;
         while (rem >= 7 - I) { rem -= 7 - I; ++I; }
@@ -229,15 +243,15 @@ __device__ __forceinline__ void t3_schur(T3KShared &S, int tl, unsigned tm) {
                     for (int c = 0; c < 3; ++c) v[3 * r + c] += P[tr ? 3 * c + r : 3 * r + c];
             }
         }
-#pragma unroll
-        for (int e = 0; e < 9; ++e) A[b][e] = v[e];
+        st9(A[b], v);
     }
     __syncwarp(tm);  // plate blocks read; S.Pb holds Z below
-    double *Zb = &S.Pb[0][0][0];  // step K, later node J = K + 1 + j: Z at 18 j, Zs at 18 j + 9
+    double *Zb = &S.Pb[0][0][0];  // step K, later node J = K + 1 + j: Z at 20 j, Zs at 20 j + 10
 #pragma unroll
     for (int K = 0; K < 4; ++K) {
         const int n = 6 - K;
-        const double *D = A[t3_pblk(K, K)];
+        double D[9];
+        ld9(A[t3_pblk(K, K)], D);
         const double D00 = D[0], D01 = D[1], D02 = D[2], D11 = D[4], D12 = D[5], D22 = D[8];
         const double m2 = D00 * D11 - D01 * D01;
         const double det = D00 * (D11 * D22 - D12 * D12) - D01 * (D01 * D22 - D12 * D02) + D02 * (D01 * D12 - D11 * D02);
@@ -246,27 +260,33 @@ __device__ __forceinline__ void t3_schur(T3KShared &S, int tl, unsigned tm) {
         const double i0 = (m2 * det) * r, i1 = D00 * ((D00 * det) * r), i2 = m2 * ((D00 * m2) * r);
         const double l10 = D01 * i0, l20 = D02 * i0, l21 = (D12 - l20 * D01) * i1;
         if (tl < n) {
-            const double *B = A[t3_pblk(K, K + 1 + tl)];
-            double *Z = Zb + 18 * tl;
+            double B[9], z[9], zs[9];
+            ld9(A[t3_pblk(K, K + 1 + tl)], B);
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 const double z0 = B[c], z1 = B[3 + c] - l10 * z0, z2 = B[6 + c] - l20 * z0 - l21 * z1;
-                Z[c] = z0; Z[3 + c] = z1; Z[6 + c] = z2;
-                Z[9 + c] = z0 * i0; Z[12 + c] = z1 * i1; Z[15 + c] = z2 * i2;
+                z[c] = z0; z[3 + c] = z1; z[6 + c] = z2;
+                zs[c] = z0 * i0; zs[3 + c] = z1 * i1; zs[6 + c] = z2 * i2;
             }
+            st9(Zb + 20 * tl, z);
+            st9(Zb + 20 * tl + 10, zs);
         }
         __syncwarp(tm);
         for (int t = tl; t < n * (n + 1) / 2; t += T3_TEAM) {
             int ip = 0, rem = t;
             while (rem >= n - ip) { rem -= n - ip; ++ip; }
             const int jp = ip + rem;
-            const double *Zi = Zb + 18 * ip, *Zs = Zb + 18 * jp + 9;
-            double *C = A[t3_pblk(K + 1 + ip, K + 1 + jp)];
+            double Zi[9], Zs[9], C[9];
+            ld9(Zb + 20 * ip, Zi);
+            ld9(Zb + 20 * jp + 10, Zs);
+            double *Cp = A[t3_pblk(K + 1 + ip, K + 1 + jp)];
+            ld9(Cp, C);
 #pragma unroll
             for (int r = 0; r < 3; ++r)
 #pragma unroll
                 for (int c = 0; c < 3; ++c)
                     C[3 * r + c] -= Zi[r] * Zs[c] + Zi[3 + r] * Zs[3 + c] + Zi[6 + r] * Zs[6 + c];
+            st9(Cp, C);
         }
         __syncwarp(tm);
     }
