@@ -61,11 +61,26 @@ struct __align__(16) T3KShared {
             alignas(16) double A[28][10];
         } b;
     } u;
-    // quad q, local node pair (a <= b): 3x3 over (w, theta_x, theta_y);
-    // the K kernel's write phase reuses it for the six staged 6x6 blocks
-    alignas(16) double Pb[3][10][9];
+    // quad q, local node pair (a <= b): 3x3 over (w, theta_x, theta_y), padded
+    // to 10 doubles; the K kernel's write phase reuses it for the six staged
+    // 6x6 blocks
+    alignas(16) double Pb[3][10][10];
     int32_t slot[6];
 };
+
+// A 3x3 block (9 doubles) at a 16-byte boundary as 128-bit shared-memory
+// accesses: the stiffness kernel's blocks are padded to 10 doubles for this.
+__device__ __forceinline__ void ld9(const double *p, double v[9]) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    const double2 a = q[0], b = q[1], c = q[2], d = q[3];
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y; v[4] = c.x; v[5] = c.y; v[6] = d.x; v[7] = d.y; v[8] = p[8];
+}
+__device__ __forceinline__ void st9(double *p, const double v[9]) {
+    double2 *q = reinterpret_cast<double2 *>(p);
+    q[0] = make_double2(v[0], v[1]); q[1] = make_double2(v[2], v[3]);
+    q[2] = make_double2(v[4], v[5]); q[3] = make_double2(v[6], v[7]);
+    p[8] = v[8];
+}
 
 // Corner coordinates of virtual quad q (corner q, midpoint to the next
 // corner, centroid, midpoint from the previous corner), as the macro points
@@ -135,10 +150,8 @@ __device__ __forceinline__ void t3_plate_blocks(T3KShared &S, int tl, unsigned t
         double v[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
         bend_pair(S.u.q.dNx[q], S.u.q.dNy[q], S.u.q.wdet[q], ka, kb, cb, nu, gam, v);
         if (macneal) macneal_pair(S.u.q.Dd[q], S.u.q.W[q], ka, kb, v);
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) S.Pb[q][pp][3 * i + j] = v[i][j];
+        const double vf[9] = {v[0][0], v[0][1], v[0][2], v[1][0], v[1][1], v[1][2], v[2][0], v[2][1], v[2][2]};
+        st9(S.Pb[q][pp], vf);
     }
     __syncwarp(tm);
 }
@@ -205,19 +218,7 @@ __host__ __device__ constexpr int t3_mnode(int I) { return I < 4 ? I + 3 : I - 4
 // Z_J = L^-1 A_KJ and Zs_J = diag(d)^-1 Z_J for every later node J, and every
 // later block A_IJ -= Z_I' Zs_J.  Kii is symmetric positive definite, so this
 // unpivoted elimination matches the reference's pivoted LU up to rounding.
-// On return the corner blocks (4 + a, 4 + b) of S.u.b.A hold Kc.  Blocks and
-// Z columns start on 16 bytes and move as 128-bit shared-memory accesses.
-__device__ __forceinline__ void ld9(const double *p, double v[9]) {
-    const double2 *q = reinterpret_cast<const double2 *>(p);
-    const double2 a = q[0], b = q[1], c = q[2], d = q[3];
-    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y; v[4] = c.x; v[5] = c.y; v[6] = d.x; v[7] = d.y; v[8] = p[8];
-}
-__device__ __forceinline__ void st9(double *p, const double v[9]) {
-    double2 *q = reinterpret_cast<double2 *>(p);
-    q[0] = make_double2(v[0], v[1]); q[1] = make_double2(v[2], v[3]);
-    q[2] = make_double2(v[4], v[5]); q[3] = make_double2(v[6], v[7]);
-    p[8] = v[8];
-}
+// On return the corner blocks (4 + a, 4 + b) of S.u.b.A hold Kc.
 
 __device__ __forceinline__ void t3_schur(T3KShared &S, int tl, unsigned tm) {
     double(*A)[10] = S.u.b.A;
@@ -236,7 +237,8 @@ __device__ __forceinline__ void t3_schur(T3KShared &S, int tl, unsigned tm) {
             }
             if (la >= 0 && lb >= 0) {
                 const bool tr = la > lb;
-                const double *P = S.Pb[q][tr ? packed_index(lb, la, 4) : packed_index(la, lb, 4)];
+                double P[9];
+                ld9(S.Pb[q][tr ? packed_index(lb, la, 4) : packed_index(la, lb, 4)], P);
 #pragma unroll
                 for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -406,11 +408,14 @@ __global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t n
             Lm[0][1] += (cm * (nu * (ba * cb_) + gam * (ca * bb))) * A;
             Lm[1][0] += (cm * (nu * (ca * bb) + gam * (ba * cb_))) * A;
             Lm[1][1] += (cm * (ca * cb_ + gam * (ba * bb))) * A;
-            if (plate)
+            if (plate) {
+                double kc[9];
+                ld9(S.u.b.A[t3_pblk(4 + a, 4 + b)], kc);
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
 #pragma unroll
-                    for (int j = 0; j < 3; ++j) Lp[i][j] = S.u.b.A[t3_pblk(4 + a, 4 + b)][3 * i + j];
+                    for (int j = 0; j < 3; ++j) Lp[i][j] = kc[3 * i + j];
+            }
         }
         double Qa[9], Qb[9];
         if (nodeR) {
