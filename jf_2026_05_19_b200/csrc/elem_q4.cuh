@@ -152,7 +152,8 @@ struct __align__(16) Q4GShared {
     double Am[8][4];
     double B[10];
     double map[4][8];     // -B^-1 Am'
-    double t[8][8], gz[8][4], f[8];
+    alignas(16) double t[8][8];  // (node, component) pairs adjacent: read as 16-byte pairs
+    double gz[8][4], f[8];
     int32_t slot[10];     // node-pair slots, for the warp's copy of the staged blocks
 };
 
@@ -924,7 +925,8 @@ __global__ void __launch_bounds__(32 * W) q4_kg_kernel(int64_t nq, const int32_t
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             const double f = S.f[q];
-            const double ta0 = S.t[q][2 * a], ta1 = S.t[q][2 * a + 1], tb0 = S.t[q][2 * b], tb1 = S.t[q][2 * b + 1];
+            const double2 ta = reinterpret_cast<const double2 *>(S.t[q])[a], tb = reinterpret_cast<const double2 *>(S.t[q])[b];
+            const double ta0 = ta.x, ta1 = ta.y, tb0 = tb.x, tb1 = tb.y;
             const double fa0 = f * ta0, fa1 = f * ta1;
             M[0][0] += fa0 * tb0; M[0][1] += fa0 * tb1;
             M[1][0] += fa1 * tb0; M[1][1] += fa1 * tb1;
