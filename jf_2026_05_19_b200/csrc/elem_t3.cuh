@@ -56,14 +56,17 @@ struct __align__(16) T3KShared {
             double X[12][9];   // Kii^-1 Kie
             double Kc[9][9];
         } c;
-        struct {  // the stiffness kernel's macro system, 28 upper 3x3 blocks (t3_pblk),
-                  // each padded to 10 doubles so that it starts on 16 bytes
-            alignas(16) double A[28][10];
-        } b;
+        struct {  // stiffness kernel, block elimination: Z and diag(d)^-1 Z of each later node
+            alignas(16) double Z[6][20];
+        } z;
+        struct {  // stiffness kernel, write phase: the six 6x6 node-pair blocks as staged
+            alignas(16) double O[6][36];
+        } o;
     } u;
-    // quad q, local node pair (a <= b): 3x3 over (w, theta_x, theta_y), padded
-    // to 10 doubles; the K kernel's write phase reuses it for the six staged
-    // 6x6 blocks
+    // recovery and sensitivity kernels: quad q, local node pair (a <= b), 3x3
+    // over (w, theta_x, theta_y), padded to 10 doubles.  The stiffness kernel
+    // keeps its 28 macro blocks here instead (t3_macro_blocks), padded alike,
+    // with one spare block.
     alignas(16) double Pb[3][10][10];
     int32_t slot[6];
 };
@@ -210,48 +213,76 @@ __device__ __forceinline__ void t3_condense(T3KShared &S, int tl, unsigned tm) {
 __host__ __device__ constexpr int t3_pblk(int I, int J) { return I * 7 - I * (I - 1) / 2 + (J - I); }
 __host__ __device__ constexpr int t3_mnode(int I) { return I < 4 ? I + 3 : I - 4; }
 
-// Condensed plate stiffness Kc = Kee - Kei Kii^-1 Kie, for the stiffness
-// kernel, by 3x3-block elimination of the four internal nodes.  The 28 upper
-// blocks of the macro system are summed from the quads' plate blocks (quad
-// order), then for each internal node K: its pivot block D = L diag(d) L' in
-// closed form (1/D00, D00/m2 and m2/det from one reciprocal of D00 m2 det),
-// Z_J = L^-1 A_KJ and Zs_J = diag(d)^-1 Z_J for every later node J, and every
-// later block A_IJ -= Z_I' Zs_J.  Kii is symmetric positive definite, so this
-// unpivoted elimination matches the reference's pivoted LU up to rounding.
-// On return the corner blocks (4 + a, 4 + b) of S.u.b.A hold Kc.
+// Macro blocks of the stiffness kernel, summed where they are computed.
+// Each of the 30 (virtual quad, node pair) plate blocks belongs to one upper
+// block (I, J) of the macro system (transposed when the quad's pair runs
+// against the node order), and every block's contributions sit on one lane
+// in quad order, so block I J is ((P_q0 + P_q1) + P_q2) as a sum over the
+// quads would give.  Entry [round][lane]: quad (bits 0-1), local pair (2-5),
+// block (6-10), transpose (11), mode (12-13): store, add to the block, store
+// to the spare block (the centroid's third quad, added by t3_schur), none.
+// Lanes 0-5 take the six blocks with two quads, lanes 6-7 the centroid's
+// three, lanes 7-14 the fifteen blocks with one; lane 15 zeroes the blocks
+// no quad touches that the elimination reads (its first step skips corner 2,
+// which shares no quad with midpoint 3).
+__device__ const uint16_t c_t3_macro_items[2][16] = {
+    {0x0010, 0x00d4, 0x01d1, 0x0255, 0x0364, 0x0ba0, 0x049c, 0x249e, 0x0098, 0x094d, 0x0ac5, 0x0bcc, 0x0cc8, 0x0d4a, 0x0641, 0x3000},
+    {0x1025, 0x18e1, 0x11e6, 0x1a62, 0x1352, 0x1396, 0x149d, 0x0859, 0x0904, 0x0a1a, 0x0b0e, 0x0c46, 0x0d09, 0x0580, 0x06c2, 0x3000},
+};
+constexpr int T3_SPARE_BLOCK = 28;  // the centroid block's third contribution
 
-__device__ __forceinline__ void t3_schur(T3KShared &S, int tl, unsigned tm) {
-    double(*A)[10] = S.u.b.A;
-    for (int b = tl; b < 28; b += T3_TEAM) {
-        int I = 0, rem = b;
-        while (rem >= 7 - I) { rem -= 7 - I; ++I; }
-        const int J = I + rem, nI = t3_mnode(I), nJ = t3_mnode(J);
-        double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+__device__ __forceinline__ void t3_macro_blocks(T3KShared &S, double (*A)[10], int tl, unsigned tm, double cb, double nu,
+                                                double gam, bool macneal) {
+    const int code[2] = {__ldg(&c_t3_macro_items[0][tl]), __ldg(&c_t3_macro_items[1][tl])};
 #pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            int la = -1, lb = -1;
+    for (int r = 0; r < 2; ++r) {
+        const int c = code[r], mode = c >> 12;
+        if (mode == 3) continue;
+        const int q = c & 3, pp = (c >> 2) & 15, b = (c >> 6) & 31;
+        const bool tr = (c >> 11) & 1;
+        int ka, kb;
+        q4_pair(pp, ka, kb);
+        double v[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        bend_pair(S.u.q.dNx[q], S.u.q.dNy[q], S.u.q.wdet[q], ka, kb, cb, nu, gam, v);
+        if (macneal) macneal_pair(S.u.q.Dd[q], S.u.q.W[q], ka, kb, v);
+        double f[9];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                if (t3_quad_node(q, k) == nI) la = k;
-                if (t3_quad_node(q, k) == nJ) lb = k;
-            }
-            if (la >= 0 && lb >= 0) {
-                const bool tr = la > lb;
-                double P[9];
-                ld9(S.Pb[q][tr ? packed_index(lb, la, 4) : packed_index(la, lb, 4)], P);
+        for (int i = 0; i < 3; ++i)
 #pragma unroll
-                for (int r = 0; r < 3; ++r)
+            for (int j = 0; j < 3; ++j) f[3 * i + j] = tr ? v[j][i] : v[i][j];
+        double *dst = A[mode == 2 ? T3_SPARE_BLOCK : b];
+        if (mode == 1) {
+            double o[9];
+            ld9(dst, o);
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) v[3 * r + c] += P[tr ? 3 * c + r : 3 * r + c];
-            }
+            for (int i = 0; i < 9; ++i) f[i] = o[i] + f[i];
         }
-        st9(A[b], v);
+        st9(dst, f);
     }
-    __syncwarp(tm);  // plate blocks read; S.Pb holds Z below
-    double *Zb = &S.Pb[0][0][0];  // step K, later node J = K + 1 + j: Z at 20 j, Zs at 20 j + 10
+    if (tl == 15) {
+        const double z[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        st9(A[t3_pblk(1, 4)], z); st9(A[t3_pblk(2, 5)], z);
+        st9(A[t3_pblk(4, 5)], z); st9(A[t3_pblk(4, 6)], z); st9(A[t3_pblk(5, 6)], z);
+    }
+    __syncwarp(tm);
+}
+
+// Condensed plate stiffness Kc = Kee - Kei Kii^-1 Kie, for the stiffness
+// kernel, by 3x3-block elimination of the four internal nodes from the macro
+// blocks of t3_macro_blocks.  For each internal node K: its pivot block
+// D = L diag(d) L' in closed form (1/D00, D00/m2 and m2/det from one
+// reciprocal of D00 m2 det), Z_J = L^-1 A_KJ and Zs_J = diag(d)^-1 Z_J for
+// every later node J, and every later block A_IJ -= Z_I' Zs_J.  Kii is
+// symmetric positive definite, so this unpivoted elimination matches the
+// reference's pivoted LU up to rounding.  On return the corner blocks
+// (4 + a, 4 + b) of A hold Kc.
+__device__ __forceinline__ void t3_schur(T3KShared &S, double (*A)[10], int tl, unsigned tm) {
+    double *Zb = &S.u.z.Z[0][0];  // step K, later node J = K + 1 + j: Z at 20 j, Zs at 20 j + 10
 #pragma unroll
     for (int K = 0; K < 4; ++K) {
-        const int n = 6 - K;
+        // the first step's last node, corner 2, has a zero block with midpoint 3 (no shared quad):
+        // its Z and every update through it are zero and skipped
+        const int n = K == 0 ? 5 : 6 - K;
         double D[9];
         ld9(A[t3_pblk(K, K)], D);
         const double D00 = D[0], D01 = D[1], D02 = D[2], D11 = D[4], D12 = D[5], D22 = D[8];
@@ -272,6 +303,14 @@ __device__ __forceinline__ void t3_schur(T3KShared &S, int tl, unsigned tm) {
             }
             st9(Zb + 20 * tl, z);
             st9(Zb + 20 * tl + 10, zs);
+        } else if (K == 0 && tl == 15) {
+            // the centroid block's third quad, before the first update reads the block
+            double c3[9], s3[9];
+            ld9(A[t3_pblk(3, 3)], c3);
+            ld9(A[T3_SPARE_BLOCK], s3);
+#pragma unroll
+            for (int i = 0; i < 9; ++i) c3[i] = c3[i] + s3[i];
+            st9(A[t3_pblk(3, 3)], c3);
         }
         __syncwarp(tm);
         for (int t = tl; t < n * (n + 1) / 2; t += T3_TEAM) {
@@ -378,12 +417,13 @@ __global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t n
         }
     }
 
+    double(*Am)[10] = reinterpret_cast<double(*)[10]>(&S.Pb[0][0][0]);  // the macro blocks
     if (plate) {
         t3_plate_points(S, tl, tm, x, y, cs, cb, macneal);
-        t3_plate_blocks(S, tl, tm, cb, nu, gam, macneal);
-        // Phases 3-4: Kcond = Kee - Kei Kii^-1 Kie by 3x3-block elimination
-        // (Kee and Kei from the corner's own quad)
-        t3_schur(S, tl, tm);
+        // Phases 2-4: macro blocks, then Kcond = Kee - Kei Kii^-1 Kie by
+        // 3x3-block elimination (Kee and Kei from the corner's own quad)
+        t3_macro_blocks(S, Am, tl, tm, cb, nu, gam, macneal);
+        t3_schur(S, Am, tl, tm);
     }
     __syncwarp(tm);
 
@@ -410,7 +450,7 @@ __global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t n
             Lm[1][1] += (cm * (ca * cb_ + gam * (ba * bb))) * A;
             if (plate) {
                 double kc[9];
-                ld9(S.u.b.A[t3_pblk(4 + a, 4 + b)], kc);
+                ld9(Am[t3_pblk(4 + a, 4 + b)], kc);
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -426,10 +466,10 @@ __global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t n
             for (int i = 0; i < 9; ++i) { Qa[i] = S.V[i]; Qb[i] = S.V[i]; }
         }
         const int32_t sl = __ldg(o.blk_slot + e * 6 + pair);
-        // Regular slots are staged in S.Pb (free after phase 4) in their
+        // Regular slots are staged in S.u.o (free after phase 4) in their
         // stored orientation and copied out by the team below; pairs on the
         // RBE2 path are written directly.
-        double *buf = &S.Pb[0][0][0] + 36 * pair;
+        double *buf = S.u.o.O[pair];
         const bool t = sl >= 0 && (sl & kBlkTranspose);
         double M[3][3], O[3][3];
         // diagonal sub-block: (u, v, w) x (u, v, w) or (rx, ry, rz) x (rx, ry, rz)
@@ -459,7 +499,7 @@ __global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t n
     for (int pair = 0, part = tl; pair < 6;) {
         const int32_t st = S.slot[pair];
         if (st >= 0) {
-            const double2 v2 = reinterpret_cast<const double2 *>(&S.Pb[0][0][0] + 36 * pair)[part];
+            const double2 v2 = reinterpret_cast<const double2 *>(S.u.o.O[pair])[part];
             reinterpret_cast<double2 *>(o.staging + 36 * (int64_t)(st & kBlkIndexMask))[part] = v2;
         }
         part += T3_TEAM;
