@@ -141,7 +141,6 @@ struct __align__(16) Q4KShared {
         };
         double blk[10][36];             // write phase: the element's rotated pair blocks, stored orientation
     };
-    int32_t slot[10];                   // node-pair slots, for the warp's copy of the staged blocks
 };
 
 // KG kernel state of one element (membrane incompatible modes only; the
@@ -154,7 +153,6 @@ struct __align__(16) Q4GShared {
     double map[4][8];     // -B^-1 Am'
     alignas(16) double t[8][8];  // (node, component) pairs adjacent: read as 16-byte pairs
     double gz[8][4], f[8];
-    int32_t slot[10];     // node-pair slots, for the warp's copy of the staged blocks
 };
 
 __device__ __forceinline__ void q4_shape_gp(int g, double &r, double &s) {
@@ -630,10 +628,10 @@ __global__ void __launch_bounds__(32 * W, 16 / W) q4_k_kernel(int64_t nq, const 
     // rows of the lower-numbered global node (transposed when the slot says
     // so).  Each half (stored rows 0-2, then 3-5) is rotated by sub-blocks
     // and staged in the element's shared record -- no lane reads the phase
-    // data any more -- which then holds the element's ten 6x6 blocks.  The
-    // warp copies the staged slots out as 16-byte stores, 18 per slot, so a
-    // slot is written as whole contiguous lines instead of 36 scattered
-    // 8-byte stores.  Pairs on the RBE2 path are written directly.
+    // data any more -- which then holds the element's ten 6x6 blocks.  Each
+    // lane then copies its own slot out as one 288-byte bulk copy, so a slot
+    // is written as whole contiguous lines instead of 36 scattered 8-byte
+    // stores.  Pairs on the RBE2 path are written directly.
     __syncwarp();
     const bool t = valid && sl >= 0 && (sl & kBlkTranspose);
     double *buf = S.blk[valid ? tl : 0];
@@ -679,31 +677,15 @@ __global__ void __launch_bounds__(32 * W, 16 / W) q4_k_kernel(int64_t nq, const 
             }
         }
     }
-    if (valid) S.slot[tl] = sl;  // the copy below skips negative (RBE2 path) slots
-    __syncwarp();
-    // chunk ch = 180 team + 18 pair + part; lanes step by 32 = 1 pair + 14 parts.
-    // The warp's valid teams are a prefix (elements are consecutive).
-    {
-        const int64_t p_warp = (int64_t)blockIdx.x * Q4_TEAMS_PER_WARP * W + warp * Q4_TEAMS_PER_WARP;
-        const int64_t n_left = nq - p_warp;
-        const int nv = n_left <= 0 ? 0 : (n_left >= Q4_TEAMS_PER_WARP ? Q4_TEAMS_PER_WARP : (int)n_left);
-        for (int tm = 0, pl = lane / 18, part = lane % 18; tm < nv;) {
-            const Q4KShared &R = sh[warp * Q4_TEAMS_PER_WARP + tm];
-            const int32_t st = R.slot[pl];
-            if (st >= 0) {
-                const double2 v2 = reinterpret_cast<const double2 *>(R.blk[pl])[part];
-                reinterpret_cast<double2 *>(o.staging + 36 * (int64_t)(st & kBlkIndexMask))[part] = v2;
-            }
-            part += 14;
-            pl += 1;
-            if (part >= 18) { part -= 18; ++pl; }
-            if (pl >= 10) { pl -= 10; ++tm; }
-        }
+    if (valid && sl >= 0) {  // the lane's own staged slot (RBE2-path slots are negative)
+        slot_fence();
+        slot_copy(o.staging + 36 * (int64_t)(sl & kBlkIndexMask), buf, 288);
     }
     if (o.maxabs) {
         for (int off = 16; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
         if (lane == 0 && lmax > 0.0) atomic_max_nonneg(o.maxabs, lmax);
     }
+    slot_copies_read();
 }
 
 // W warps per CTA (3 W elements): 4 or 8; dynamic shared memory as q4_k_kernel's.
@@ -914,8 +896,8 @@ __global__ void __launch_bounds__(32 * W) q4_kg_kernel(int64_t nq, const int32_t
     // Phase 5: one node pair per lane; translations only (the rotation
     // sub-blocks of a flat shell's KG are zero).  A staged slot holds the
     // translation 3x3 and three zeros of padding: each lane stages its slot in
-    // the element's shared record, then the warp copies the slots out as
-    // 16-byte stores, 6 per slot.  Pairs on the RBE2 path are written directly.
+    // the element's shared record and copies it out as one 96-byte bulk copy.
+    // Pairs on the RBE2 path are written directly.
     double O[3][3];
     int a = 0, b = 0;
     int32_t sl = -1;
@@ -968,26 +950,11 @@ __global__ void __launch_bounds__(32 * W) q4_kg_kernel(int64_t nq, const int32_t
 #pragma unroll
                 for (int c = 0; c < 3; ++c) buf[3 * r + c] = t ? O[c][r] : O[r][c];
             buf[9] = 0.0; buf[10] = 0.0; buf[11] = 0.0;
+            slot_fence();
+            slot_copy(o.staging + 12 * (int64_t)(sl & kBlkIndexMask), buf, 96);
         }
-        S.slot[tl] = sl;
     }
-    __syncwarp();
-    // chunk ch = 60 team + 6 pair + part; lanes step by 32 = 5 pairs + 2 parts
-    const int64_t p_warp = (int64_t)blockIdx.x * Q4_TEAMS_PER_WARP * W + warp * Q4_TEAMS_PER_WARP;
-    const int64_t n_left = nq - p_warp;
-    const int nv = n_left <= 0 ? 0 : (n_left >= Q4_TEAMS_PER_WARP ? Q4_TEAMS_PER_WARP : (int)n_left);
-    for (int tm = 0, pl = lane / 6, part = lane % 6; tm < nv;) {
-        const Q4GShared &R = sh[warp * Q4_TEAMS_PER_WARP + tm];
-        const int32_t st = R.slot[pl];
-        if (st >= 0) {
-            const double2 v2 = reinterpret_cast<const double2 *>(reinterpret_cast<const double *>(&R) + 12 * pl)[part];
-            reinterpret_cast<double2 *>(o.staging + 12 * (int64_t)(st & kBlkIndexMask))[part] = v2;
-        }
-        part += 2;
-        pl += 5;
-        if (part >= 6) { part -= 6; ++pl; }
-        if (pl >= 10) { pl -= 10; ++tm; }
-    }
+    slot_copies_read();
 }
 
 }  // namespace jfg

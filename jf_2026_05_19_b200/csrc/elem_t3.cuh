@@ -68,6 +68,7 @@ struct __align__(16) T3KShared {
     // keeps its 28 macro blocks here instead (t3_macro_blocks), padded alike,
     // with one spare block.
     alignas(16) double Pb[3][10][10];
+    alignas(16) double Qn[3][10];  // stiffness kernel: each corner's node block T R_k (t3_schur)
     int32_t slot[6];
 };
 
@@ -275,8 +276,9 @@ __device__ __forceinline__ void t3_macro_blocks(T3KShared &S, double (*A)[10], i
 // every later node J, and every later block A_IJ -= Z_I' Zs_J.  Kii is
 // symmetric positive definite, so this unpivoted elimination matches the
 // reference's pivoted LU up to rounding.  On return the corner blocks
-// (4 + a, 4 + b) of A hold Kc.
-__device__ __forceinline__ void t3_schur(T3KShared &S, double (*A)[10], int tl, unsigned tm) {
+// (4 + a, 4 + b) of A hold Kc.  Lanes 12-14, idle in the first step, form the
+// corners' node blocks S.Qn for the write phase (T R_k with CD frames, else T).
+__device__ __forceinline__ void t3_schur(T3KShared &S, double (*A)[10], int tl, unsigned tm, bool frames) {
     double *Zb = &S.u.z.Z[0][0];  // step K, later node J = K + 1 + j: Z at 20 j, Zs at 20 j + 10
 #pragma unroll
     for (int K = 0; K < 4; ++K) {
@@ -311,6 +313,16 @@ __device__ __forceinline__ void t3_schur(T3KShared &S, double (*A)[10], int tl, 
 #pragma unroll
             for (int i = 0; i < 9; ++i) c3[i] = c3[i] + s3[i];
             st9(A[t3_pblk(3, 3)], c3);
+        } else if (K == 0 && tl >= 12) {
+            const int k = tl - 12;
+            double Q[9];
+            if (frames) {
+                node_block(S.V, S.V + 3, S.V + 6, S.R[k], Q);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 9; ++i) Q[i] = S.V[i];
+            }
+            st9(S.Qn[k], Q);
         }
         __syncwarp(tm);
         for (int t = tl; t < n * (n + 1) / 2; t += T3_TEAM) {
@@ -423,7 +435,7 @@ __global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t n
         // Phases 2-4: macro blocks, then Kcond = Kee - Kei Kii^-1 Kie by
         // 3x3-block elimination (Kee and Kei from the corner's own quad)
         t3_macro_blocks(S, Am, tl, tm, cb, nu, gam, macneal);
-        t3_schur(S, Am, tl, tm);
+        t3_schur(S, Am, tl, tm, nodeR != nullptr);
     }
     __syncwarp(tm);
 
@@ -458,7 +470,10 @@ __global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t n
             }
         }
         double Qa[9], Qb[9];
-        if (nodeR) {
+        if (plate) {  // formed during the block elimination
+            ld9(S.Qn[a], Qa);
+            ld9(S.Qn[b], Qb);
+        } else if (nodeR) {
             node_block(S.V, S.V + 3, S.V + 6, S.R[a], Qa);
             node_block(S.V, S.V + 3, S.V + 6, S.R[b], Qb);
         } else {
@@ -467,7 +482,7 @@ __global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t n
         }
         const int32_t sl = __ldg(o.blk_slot + e * 6 + pair);
         // Regular slots are staged in S.u.o (free after phase 4) in their
-        // stored orientation and copied out by the team below; pairs on the
+        // stored orientation and copied out below as bulk copies; pairs on the
         // RBE2 path are written directly.
         double *buf = S.u.o.O[pair];
         const bool t = sl >= 0 && (sl & kBlkTranspose);
@@ -493,22 +508,18 @@ __global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t n
         else stage_sub_block(buf, t, bi, 1 - bi, O, lmax);
         if (bi == 0) S.slot[pair] = sl;
     }
+    slot_fence();  // the staged values, written by two lanes per slot, before the bulk copies
     __syncwarp(tm);
-    // the team copies the staged slots as 16-byte stores, 18 per slot
-    // (chunk 18 pair + part; lanes step by 16 parts)
-    for (int pair = 0, part = tl; pair < 6;) {
-        const int32_t st = S.slot[pair];
-        if (st >= 0) {
-            const double2 v2 = reinterpret_cast<const double2 *>(S.u.o.O[pair])[part];
-            reinterpret_cast<double2 *>(o.staging + 36 * (int64_t)(st & kBlkIndexMask))[part] = v2;
-        }
-        part += T3_TEAM;
-        if (part >= 18) { part -= 18; ++pair; }
+    // lane p < 6 copies staged slot p out as one 288-byte bulk copy
+    if (tl < 6) {
+        const int32_t st = S.slot[tl];
+        if (st >= 0) slot_copy(o.staging + 36 * (int64_t)(st & kBlkIndexMask), S.u.o.O[tl], 288);
     }
     if (o.maxabs) {
         for (int off = 8; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_xor_sync(tm, lmax, off, 16));
         if (tl == 0 && lmax > 0.0) atomic_max_nonneg(o.maxabs, lmax);
     }
+    slot_copies_read();
 }
 
 // One CTRIA3 per thread: frame, node blocks and the CST membrane stress

@@ -221,4 +221,18 @@ JFG_D void atomic_max_nonneg(double *addr, double v) {
     atomicMax(reinterpret_cast<unsigned long long *>(addr), (unsigned long long)__double_as_longlong(v));
 }
 
+// Staged slots leave shared memory as bulk asynchronous copies (the copy
+// engine moves a whole slot per instruction).  Both addresses are 16-byte
+// aligned and the size a multiple of 16 bytes.  Each thread that wrote a
+// slot's values runs slot_fence() before the copying thread, after a warp
+// sync where those differ, issues slot_copy(); every copying thread runs
+// slot_copies_read() before its shared memory is reused or released.
+JFG_D void slot_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+JFG_D void slot_copy(double *dst, const double *src, uint32_t bytes) {
+    const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(src));
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n\tcp.async.bulk.commit_group;"
+                 :: "l"(dst), "r"(s), "r"(bytes) : "memory");
+}
+JFG_D void slot_copies_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+
 }  // namespace jfg
