@@ -139,7 +139,10 @@ struct __align__(16) Q4KShared {
             double B[10];               // packed upper triangle
             double Xm[4][8], Xb[4][8];  // B^-1 Am', B^-1 Ab'
         };
-        double blk[10][36];             // write phase: the element's rotated pair blocks, stored orientation
+        // write phase: the element's rotated pair blocks, stored orientation, each
+        // padded to 38 doubles: the 16-byte staging stores of a warp's 30 lanes
+        // then spread over all eight 16-byte bank groups (36 would use four)
+        double blk[10][38];
     };
 };
 
@@ -154,6 +157,7 @@ struct __align__(16) Q4GShared {
     alignas(16) double t[8][8];  // (node, component) pairs adjacent: read as 16-byte pairs
     double gz[8][4], f[8];
 };
+static_assert(sizeof(Q4GShared) >= 10 * 14 * sizeof(double), "the KG write phase stages ten 14-double slots in the record");
 
 __device__ __forceinline__ void q4_shape_gp(int g, double &r, double &s) {
     const double pt = 0.57735026918962576451;  // 1/sqrt(3)
@@ -658,16 +662,21 @@ __global__ void __launch_bounds__(32 * W, 16 / W) q4_k_kernel(int64_t nq, const 
                 write_sub_block(o, e, sl, a, b, half, 0, Of, lmax, 24);
                 write_sub_block(o, e, sl, a, b, half, 1, Os, lmax, 24);
             } else {
-                double *hb = buf + 18 * half;
+                double2 *hb = reinterpret_cast<double2 *>(buf + 18 * half);  // stored row r: 3 pairs
 #pragma unroll
-                for (int r = 0; r < 3; ++r)
+                for (int r = 0; r < 3; ++r) {
+                    double v[6];
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
-                        const double vf = t ? Of[c][r] : Of[r][c], vs = t ? Os[c][r] : Os[r][c];
-                        lmax = fmax(lmax, fmax(fabs(vf), fabs(vs)));
-                        hb[6 * r + c] = vf;
-                        hb[6 * r + 3 + c] = vs;
+                        v[c] = t ? Of[c][r] : Of[r][c];
+                        v[3 + c] = t ? Os[c][r] : Os[r][c];
                     }
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) lmax = fmax(lmax, fabs(v[c]));
+                    hb[3 * r] = make_double2(v[0], v[1]);
+                    hb[3 * r + 1] = make_double2(v[2], v[3]);
+                    hb[3 * r + 2] = make_double2(v[4], v[5]);
+                }
                 if (o.diag_staging && a == b) {
                     // diagonal pair (never transposed): TT in the first, RR in the second column band
 #pragma unroll
@@ -944,12 +953,18 @@ __global__ void __launch_bounds__(32 * W) q4_kg_kernel(int64_t nq, const int32_t
             write_sub_block(o, e, sl, a, b, 1, 1, Z, lmax, 24);
         } else {
             const bool t = sl & kBlkTranspose;
-            double *buf = reinterpret_cast<double *>(&S) + 12 * tl;
+            // 14-double stride: the 16-byte stores of a warp's 30 lanes spread
+            // over all eight 16-byte bank groups
+            double *buf = reinterpret_cast<double *>(&S) + 14 * tl;
+            double v[9];
 #pragma unroll
             for (int r = 0; r < 3; ++r)
 #pragma unroll
-                for (int c = 0; c < 3; ++c) buf[3 * r + c] = t ? O[c][r] : O[r][c];
-            buf[9] = 0.0; buf[10] = 0.0; buf[11] = 0.0;
+                for (int c = 0; c < 3; ++c) v[3 * r + c] = t ? O[c][r] : O[r][c];
+            double2 *b2 = reinterpret_cast<double2 *>(buf);
+            b2[0] = make_double2(v[0], v[1]); b2[1] = make_double2(v[2], v[3]);
+            b2[2] = make_double2(v[4], v[5]); b2[3] = make_double2(v[6], v[7]);
+            b2[4] = make_double2(v[8], 0.0); b2[5] = make_double2(0.0, 0.0);
             slot_fence();
             slot_copy(o.staging + 12 * (int64_t)(sl & kBlkIndexMask), buf, 96);
         }

@@ -59,8 +59,9 @@ struct __align__(16) T3KShared {
         struct {  // stiffness kernel, block elimination: Z and diag(d)^-1 Z of each later node
             alignas(16) double Z[6][20];
         } z;
-        struct {  // stiffness kernel, write phase: the six 6x6 node-pair blocks as staged
-            alignas(16) double O[6][36];
+        struct {  // stiffness kernel, write phase: the six 6x6 node-pair blocks as staged,
+                  // padded to 38 doubles against shared-memory bank conflicts
+            alignas(16) double O[6][38];
         } o;
     } u;
     // recovery and sensitivity kernels: quad q, local node pair (a <= b), 3x3
