@@ -374,6 +374,8 @@ __global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t n
     const int64_t e = (int64_t)blockIdx.x * (T3_TEAMS_PER_WARP * W) + warp * T3_TEAMS_PER_WARP + team;
     if (e >= nt) return;  // the whole team leaves; syncs below are team-local
     T3KShared &S = sh[warp * T3_TEAMS_PER_WARP + team];
+    // lane tl < 12's node-pair slot (pair tl / 2), loaded now so that its latency hides behind the element's work
+    const int32_t sl_early = tl < 12 ? __ldg(o.blk_slot + e * 6 + (tl >> 1)) : -1;
 
     // Phase 0, every lane in registers: nodes, corners, properties, frame,
     // local coordinates, CST derivatives, constitutive scalars.
@@ -481,7 +483,7 @@ __global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t n
 #pragma unroll
             for (int i = 0; i < 9; ++i) { Qa[i] = S.V[i]; Qb[i] = S.V[i]; }
         }
-        const int32_t sl = __ldg(o.blk_slot + e * 6 + pair);
+        const int32_t sl = sl_early;
         // Regular slots are staged in S.u.o (free after phase 4) in their
         // stored orientation and copied out below as bulk copies; pairs on the
         // RBE2 path are written directly.
