@@ -180,14 +180,19 @@ __device__ __forceinline__ void tmul(const double *P, const double W[3][3], doub
         }
 }
 
+// sb: the thread's staged slot in shared memory (stored orientation), or null
+// to write through blk_entry.
 __device__ __forceinline__ void bar_store(const ElemOut &o, int64_t e, int32_t sl, int bi, int bj, const double G[3][3],
-                                          bool diag, int node, double &lmax, int64_t pair_id) {
+                                          bool diag, int node, double &lmax, int64_t pair_id, double *sb) {
+    const bool t = sl & kBlkTranspose;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
             lmax = fmax(lmax, fabs(G[i][j]));
-            *blk_entry(o, sl, 3 * bi + i, 3 * bj + j, pair_id) = G[i][j];
+            const int r = 3 * bi + i, c = 3 * bj + j;
+            if (sb) sb[t ? 6 * c + r : 6 * r + c] = G[i][j];
+            else *blk_entry(o, sl, r, c, pair_id) = G[i][j];
         }
     if (diag && o.diag_staging && bi == bj)
 #pragma unroll
@@ -199,22 +204,25 @@ __device__ __forceinline__ void bar_store(const ElemOut &o, int64_t e, int32_t s
 //   G_tt = R_A' k_tt R_B               G_tr = R_A' (k_tt O_B + k_tr R_B)
 //   G_rt = O_A' k_tt R_B + R_A' k_rt R_B
 //   G_rr = O_A' (k_tt O_B + k_tr R_B) + R_A' (k_rt O_B + k_rr R_B)
+// With a shared buffer sbuf (stiffness kernel), a regular slot is staged there
+// and sent out as one 288-byte bulk copy; RBE2-path slots are written directly.
 template <int A, int B>
 __device__ __forceinline__ void bar_pair(const ElemOut &o, int64_t e, int p, const BarFrame &F, const FrameK &c,
-                                         double &lmax) {
+                                         double &lmax, double *sbuf = nullptr) {
     const int32_t sl = __ldg(o.blk_slot + e * 3 + p);
+    double *sb = sl >= 0 ? sbuf : nullptr;
     const bool off = F.off;
     const double *RA = F.TR[A], *RB = F.TR[B], *OA = F.Toff[A], *OB = F.Toff[B];
     double W[3][3], W2[3][3], G[3][3];
     // tt
     kmul<A, B, 0, 0>(c, RB, W);
     tmul(RA, W, G, false);
-    bar_store(o, e, sl, 0, 0, G, A == B, A, lmax, 3 * e + p);
+    bar_store(o, e, sl, 0, 0, G, A == B, A, lmax, 3 * e + p, sb);
     // rt (W = k_tt R_B)
     kmul<A, B, 1, 0>(c, RB, W2);
     tmul(RA, W2, G, false);
     if (off) tmul(OA, W, G, true);
-    bar_store(o, e, sl, 1, 0, G, false, A, lmax, 3 * e + p);
+    bar_store(o, e, sl, 1, 0, G, false, A, lmax, 3 * e + p, sb);
     // tr: W = k_tt O_B + k_tr R_B
     kmul<A, B, 0, 1>(c, RB, W);
     if (off) {
@@ -225,7 +233,7 @@ __device__ __forceinline__ void bar_pair(const ElemOut &o, int64_t e, int p, con
             for (int j = 0; j < 3; ++j) W[i][j] = W2[i][j] + W[i][j];
     }
     tmul(RA, W, G, false);
-    bar_store(o, e, sl, 0, 1, G, false, A, lmax, 3 * e + p);
+    bar_store(o, e, sl, 0, 1, G, false, A, lmax, 3 * e + p, sb);
     // rr: R_A' (k_rt O_B + k_rr R_B) + O_A' W
     kmul<A, B, 1, 1>(c, RB, W2);
     if (off) {
@@ -238,14 +246,22 @@ __device__ __forceinline__ void bar_pair(const ElemOut &o, int64_t e, int p, con
     }
     tmul(RA, W2, G, false);
     if (off) tmul(OA, W, G, true);
-    bar_store(o, e, sl, 1, 1, G, A == B, A, lmax, 3 * e + p);
+    bar_store(o, e, sl, 1, 1, G, A == B, A, lmax, 3 * e + p, sb);
+    if (sb) {
+        slot_fence();
+        slot_copy(o.staging + 36 * (int64_t)(sl & kBlkIndexMask), sb, 288);
+    }
 }
 
 // One (bar, node pair) per thread, pair-major so that a warp runs one
 // compile-time pair; each of the three threads recomputes the bar frame.
+// Dynamic shared memory: kBarSlotStride doubles per thread, the staged slot.
+constexpr int kBarSlotStride = 38;  // 16-byte aligned, and off the 36-double bank period
 __global__ void __launch_bounds__(128, 3) bar_k_kernel(int64_t nb, const int32_t *__restrict__ nodes,
                                                       const double *__restrict__ prop, const double *__restrict__ coords,
                                                       const double *__restrict__ nodeR, ElemOut o) {
+    extern __shared__ __align__(16) double bar_smem[];
+    double *sbuf = bar_smem + kBarSlotStride * threadIdx.x;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int pair = (int)(t / nb);
     const int64_t e = t - (int64_t)pair * nb;
@@ -257,15 +273,16 @@ __global__ void __launch_bounds__(128, 3) bar_k_kernel(int64_t nb, const int32_t
         int32_t nd[2];
         if (bar_frame(e, nodes, prop, coords, nodeR, F, nd)) {
             const FrameK c = frame3d_k(prop + 18 * e, F.L);
-            if (pair == 0) bar_pair<0, 0>(o, e, 0, F, c, lmax);
-            else if (pair == 1) bar_pair<0, 1>(o, e, 1, F, c, lmax);
-            else bar_pair<1, 1>(o, e, 2, F, c, lmax);
+            if (pair == 0) bar_pair<0, 0>(o, e, 0, F, c, lmax, sbuf);
+            else if (pair == 1) bar_pair<0, 1>(o, e, 1, F, c, lmax, sbuf);
+            else bar_pair<1, 1>(o, e, 2, F, c, lmax, sbuf);
         }
     }
     if (o.maxabs) {
         for (int off = 16; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
         if ((threadIdx.x & 31) == 0 && lmax > 0.0) atomic_max_nonneg(o.maxabs, lmax);
     }
+    slot_copies_read();
 }
 
 __global__ void __launch_bounds__(128, 3) bar_kg_kernel(int64_t nb, const int32_t *__restrict__ nodes,

@@ -1751,7 +1751,8 @@ jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
         if (kg)
             bar_kg_kernel<<<grid, bt_, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, du, o);
         else
-            bar_k_kernel<<<grid, bt_, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, o);
+            bar_k_kernel<<<grid, bt_, (size_t)bt_ * kBarSlotStride * sizeof(double), m->stream>>>(
+                m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, o);
         CK(cudaGetLastError());
     }
     CK(mark(m, 3));
