@@ -180,8 +180,10 @@ __device__ __forceinline__ void tmul(const double *P, const double W[3][3], doub
         }
 }
 
-// sb: the thread's staged slot in shared memory (stored orientation), or null
-// to write through blk_entry.
+// sb: the thread's staged slot in shared memory in stored orientation, or
+// null to write through blk_entry.  K: the 36 values row-major.  KG: the
+// translation 3x3 and its padding (12), then the rotation sub-blocks as
+// blk_entry places them in kg_rot (kKgRotStride).
 __device__ __forceinline__ void bar_store(const ElemOut &o, int64_t e, int32_t sl, int bi, int bj, const double G[3][3],
                                           bool diag, int node, double &lmax, int64_t pair_id, double *sb) {
     const bool t = sl & kBlkTranspose;
@@ -190,9 +192,15 @@ __device__ __forceinline__ void bar_store(const ElemOut &o, int64_t e, int32_t s
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
             lmax = fmax(lmax, fabs(G[i][j]));
-            const int r = 3 * bi + i, c = 3 * bj + j;
-            if (sb) sb[t ? 6 * c + r : 6 * r + c] = G[i][j];
-            else *blk_entry(o, sl, r, c, pair_id) = G[i][j];
+            const int r0 = 3 * bi + i, c0 = 3 * bj + j;
+            if (sb) {
+                const int r = t ? c0 : r0, c = t ? r0 : c0;
+                if (!o.kg_layout) sb[6 * r + c] = G[i][j];
+                else if (r < 3 && c < 3) sb[3 * r + c] = G[i][j];
+                else sb[12 + 9 * (2 * (r / 3) + c / 3 - 1) + 3 * (r % 3) + (c % 3)] = G[i][j];
+            } else {
+                *blk_entry(o, sl, r0, c0, pair_id) = G[i][j];
+            }
         }
     if (diag && o.diag_staging && bi == bj)
 #pragma unroll
@@ -204,8 +212,9 @@ __device__ __forceinline__ void bar_store(const ElemOut &o, int64_t e, int32_t s
 //   G_tt = R_A' k_tt R_B               G_tr = R_A' (k_tt O_B + k_tr R_B)
 //   G_rt = O_A' k_tt R_B + R_A' k_rt R_B
 //   G_rr = O_A' (k_tt O_B + k_tr R_B) + R_A' (k_rt O_B + k_rr R_B)
-// With a shared buffer sbuf (stiffness kernel), a regular slot is staged there
-// and sent out as one 288-byte bulk copy; RBE2-path slots are written directly.
+// With a shared buffer sbuf, a regular slot is staged there and sent out as
+// bulk copies (K: one of 288 bytes; KG: the translation slot, 96 bytes, and the
+// rotation record, 224); RBE2-path slots are written directly.
 template <int A, int B>
 __device__ __forceinline__ void bar_pair(const ElemOut &o, int64_t e, int p, const BarFrame &F, const FrameK &c,
                                          double &lmax, double *sbuf = nullptr) {
@@ -248,8 +257,16 @@ __device__ __forceinline__ void bar_pair(const ElemOut &o, int64_t e, int p, con
     if (off) tmul(OA, W, G, true);
     bar_store(o, e, sl, 1, 1, G, A == B, A, lmax, 3 * e + p, sb);
     if (sb) {
-        slot_fence();
-        slot_copy(o.staging + 36 * (int64_t)(sl & kBlkIndexMask), sb, 288);
+        const int64_t idx = sl & kBlkIndexMask;
+        if (!o.kg_layout) {
+            slot_fence();
+            slot_copy(o.staging + 36 * idx, sb, 288);
+        } else {
+            sb[9] = 0.0; sb[10] = 0.0; sb[11] = 0.0; sb[12 + 27] = 0.0;  // padding
+            slot_fence();
+            slot_copy(o.staging + 12 * idx, sb, 96);
+            slot_copy(o.kg_rot + kKgRotStride * (3 * e + p), sb + 12, 8 * kKgRotStride);
+        }
     }
 }
 
@@ -257,6 +274,7 @@ __device__ __forceinline__ void bar_pair(const ElemOut &o, int64_t e, int p, con
 // compile-time pair; each of the three threads recomputes the bar frame.
 // Dynamic shared memory: kBarSlotStride doubles per thread, the staged slot.
 constexpr int kBarSlotStride = 38;  // 16-byte aligned, and off the 36-double bank period
+constexpr int kBarKgSlotStride = 42;  // KG: 12 + kKgRotStride values, 16-byte aligned
 __global__ void __launch_bounds__(128, 3) bar_k_kernel(int64_t nb, const int32_t *__restrict__ nodes,
                                                       const double *__restrict__ prop, const double *__restrict__ coords,
                                                       const double *__restrict__ nodeR, ElemOut o) {
@@ -285,10 +303,13 @@ __global__ void __launch_bounds__(128, 3) bar_k_kernel(int64_t nb, const int32_t
     slot_copies_read();
 }
 
+// Dynamic shared memory: kBarKgSlotStride doubles per thread, the staged slot.
 __global__ void __launch_bounds__(128, 3) bar_kg_kernel(int64_t nb, const int32_t *__restrict__ nodes,
                                                        const double *__restrict__ prop, const double *__restrict__ coords,
                                                        const double *__restrict__ nodeR, const double *__restrict__ u,
                                                        ElemOut o) {
+    extern __shared__ __align__(16) double bar_kg_smem[];
+    double *sbuf = bar_kg_smem + kBarKgSlotStride * threadIdx.x;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int pair = (int)(t / nb);
     const int64_t e = t - (int64_t)pair * nb;
@@ -318,9 +339,10 @@ __global__ void __launch_bounds__(128, 3) bar_kg_kernel(int64_t nb, const int32_
     double P = -X * ux[0] + X * ux[1];
     const FrameK c = frame3d_kg(F.L, P);
     double lmax = 0.0;
-    if (pair == 0) bar_pair<0, 0>(o, e, 0, F, c, lmax);
-    else if (pair == 1) bar_pair<0, 1>(o, e, 1, F, c, lmax);
-    else bar_pair<1, 1>(o, e, 2, F, c, lmax);
+    if (pair == 0) bar_pair<0, 0>(o, e, 0, F, c, lmax, sbuf);
+    else if (pair == 1) bar_pair<0, 1>(o, e, 1, F, c, lmax, sbuf);
+    else bar_pair<1, 1>(o, e, 2, F, c, lmax, sbuf);
+    slot_copies_read();
 }
 
 }  // namespace jfg

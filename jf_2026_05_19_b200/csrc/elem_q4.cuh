@@ -70,7 +70,7 @@ struct ElemOut {
     int64_t bprop_stride = 0;
     int64_t u_stride = 0;                // per-variant displacement stride (ndof)
     bool kg_layout = false;              // KG staging layout (see blk_entry), else K's
-    double *kg_rot = nullptr;            // KG: rotation sub-blocks of bar pairs (27 doubles per bar pair)
+    double *kg_rot = nullptr;            // KG: rotation sub-blocks of bar pairs (kKgRotStride doubles per bar pair)
 
     __device__ __forceinline__ ElemOut at(int v) const {
         ElemOut r = *this;
@@ -86,6 +86,10 @@ struct ElemOut {
     // Shell thickness of element e: the variant's own, else the property record's.
     __device__ __forceinline__ double thickness(int64_t e, const double *pr) const { return h ? __ldg(h + e) : __ldg(pr); }
 };
+
+// KG rotation sub-blocks of a bar pair: 27 values padded to 28 doubles, so
+// that every pair's record starts on 16 bytes (one bulk copy per pair).
+constexpr int kKgRotStride = 28;
 
 constexpr int32_t kBlkTranspose = 1 << 30;
 constexpr int32_t kBlkIndexMask = kBlkTranspose - 1;
@@ -103,7 +107,7 @@ __device__ __forceinline__ double *blk_entry(const ElemOut &o, int32_t s, int i,
     const int r = (s & kBlkTranspose) ? j : i, c = (s & kBlkTranspose) ? i : j;
     if (!o.kg_layout) return o.staging + 36 * idx + 6 * r + c;
     if (r < 3 && c < 3) return o.staging + 12 * idx + 3 * r + c;
-    return o.kg_rot + 27 * bar_pair + 9 * (2 * (r / 3) + c / 3 - 1) + 3 * (r % 3) + (c % 3);
+    return o.kg_rot + kKgRotStride * bar_pair + 9 * (2 * (r / 3) + c / 3 - 1) + 3 * (r % 3) + (c % 3);
 }
 
 // The padding of a staged KG shell slot (see blk_entry).

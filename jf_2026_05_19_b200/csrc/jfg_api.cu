@@ -629,7 +629,7 @@ __device__ __forceinline__ void block_kg_sums(const double *__restrict__ staging
     for (int m = 0; m < NB; ++m) {
         double s[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         for (int32_t q = rb[m]; q < b[m]; ++q) {
-            const double *p = kg_rot + 27 * (int64_t)__ldg(slot_bar + q) + 3 * i3;
+            const double *p = kg_rot + kKgRotStride * (int64_t)__ldg(slot_bar + q) + 3 * i3;
             if (i >= 3) { s[0] += __ldg(p + 9); s[1] += __ldg(p + 10); s[2] += __ldg(p + 11); }
             const int o3 = i < 3 ? 0 : 18;  // translation-rotation / rotation-rotation rows
             s[3] += __ldg(p + o3); s[4] += __ldg(p + o3 + 1); s[5] += __ldg(p + o3 + 2);
@@ -1437,7 +1437,7 @@ jfg_status jfg_model_create(const jfg_model_desc *d, jfg_model **out) {
         cudaFreeAsync(d_uk, m->stream);
     }
     CK(dalloc(m, &m->d_exc_raw, 36 * m->n_xpair));
-    m->staging_len = std::max<int64_t>(36 * nbc, 12 * nbc + 27 * 3 * m->nb);
+    m->staging_len = std::max<int64_t>(36 * nbc, 12 * nbc + kKgRotStride * 3 * m->nb);
     CK(dalloc(m, &m->d_staging, m->staging_len));
     {
         int32_t herr = 0;
@@ -1749,7 +1749,8 @@ jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
         const int bt_ = kg ? m->barkg_threads : m->bark_threads;
         dim3 grid((unsigned)cdiv(3 * m->nb, bt_), nv);
         if (kg)
-            bar_kg_kernel<<<grid, bt_, 0, m->stream>>>(m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, du, o);
+            bar_kg_kernel<<<grid, bt_, (size_t)bt_ * kBarKgSlotStride * sizeof(double), m->stream>>>(
+                m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, du, o);
         else
             bar_k_kernel<<<grid, bt_, (size_t)bt_ * kBarSlotStride * sizeof(double), m->stream>>>(
                 m->nb, m->d_barn, m->d_barp, m->d_coords, m->d_nodeR, o);
