@@ -528,11 +528,18 @@ __global__ void __launch_bounds__(32 * W, W == 2 ? 10 : 5) t3_k_kernel(int64_t n
 // One CTRIA3 per thread: frame, node blocks and the CST membrane stress
 // once, then the six node-pair blocks s_ab * Q_a' Q_b (shell KG acts on
 // translations only).
+// Dynamic shared memory: T3KG_STAGE_STRIDE doubles per thread, two staged
+// slots of 12 that alternate as the slots leave by bulk copies (a buffer is
+// refilled once the copy issued before the latest one has read it).  The
+// 26-double stride puts a warp's 16-byte stores on all eight bank groups.
+constexpr int T3KG_STAGE_STRIDE = 26;
 __global__ void __launch_bounds__(128) t3_kg_kernel(int64_t nt, const int32_t *__restrict__ nodes,
                                                    const double *__restrict__ prop,
                                                    const double *__restrict__ coords,
                                                    const double *__restrict__ nodeR,
                                                    const double *__restrict__ u, ElemOut o) {
+    extern __shared__ __align__(16) double t3kg_smem[];
+    double *sbuf = t3kg_smem + T3KG_STAGE_STRIDE * threadIdx.x;
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= nt) return;
     o = o.at(blockIdx.y);
@@ -596,6 +603,7 @@ __global__ void __launch_bounds__(128) t3_kg_kernel(int64_t nt, const int32_t *_
             for (int j = 0; j < 3; ++j)
                 val[i][j] = h * A * (sxx * b[i] * b[j] + syy * cv[i] * cv[j] + sxy * (b[i] * cv[j] + cv[i] * b[j]));
     }
+    int ncopy = 0;
 #pragma unroll
     for (int pp = 0; pp < 6; ++pp) {
         const int pa = (pp >= 3) + (pp >= 5), pb = pa + pp - (pa == 0 ? 0 : (pa == 1 ? 3 : 5));
@@ -603,16 +611,30 @@ __global__ void __launch_bounds__(128) t3_kg_kernel(int64_t nt, const int32_t *_
         double O[3][3];
         rot_block(Q[pa], L, Q[pb], O);
         const int32_t sl = __ldg(o.blk_slot + e * 6 + pp);
-        // staged blocks of KG shells are read as their translation 3x3 only; the
-        // dof-level RBE2 path (sl < 0) reads whole raw blocks
+        if (sl >= 0) {
+            // staged blocks of KG shells are read as their translation 3x3 only:
+            // the 3x3 in stored orientation and three zeros, one 96-byte copy
+            const bool t = sl & kBlkTranspose;
+            double *sb = sbuf + 12 * (ncopy & 1);
+            if (ncopy >= 2) slot_copies_read_but_last();
+            double2 *s2 = reinterpret_cast<double2 *>(sb);
+            const double v0 = O[0][0], v1 = t ? O[1][0] : O[0][1], v2 = t ? O[2][0] : O[0][2];
+            const double v3 = t ? O[0][1] : O[1][0], v4 = O[1][1], v5 = t ? O[2][1] : O[1][2];
+            const double v6 = t ? O[0][2] : O[2][0], v7 = t ? O[1][2] : O[2][1], v8 = O[2][2];
+            s2[0] = make_double2(v0, v1); s2[1] = make_double2(v2, v3); s2[2] = make_double2(v4, v5);
+            s2[3] = make_double2(v6, v7); s2[4] = make_double2(v8, 0.0); s2[5] = make_double2(0.0, 0.0);
+            slot_fence();
+            slot_copy(o.staging + 12 * (int64_t)(sl & kBlkIndexMask), sb, 96);
+            ++ncopy;
+        } else {
+            // the dof-level RBE2 path reads whole raw blocks
 #pragma unroll
-        for (int i = 0; i < 6; ++i)
+            for (int i = 0; i < 6; ++i)
 #pragma unroll
-            for (int j = 0; j < 6; ++j)
-                if (i < 3 && j < 3) *blk_entry(o, sl, i, j) = O[i][j];
-                else if (sl < 0) *blk_entry(o, sl, i, j) = 0.0;
-        kg_shell_pad(o, sl);
+                for (int j = 0; j < 6; ++j) *blk_entry(o, sl, i, j) = (i < 3 && j < 3) ? O[i][j] : 0.0;
+        }
     }
+    slot_copies_read();
 }
 
 }  // namespace jfg

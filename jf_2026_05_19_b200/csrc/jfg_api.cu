@@ -1729,7 +1729,7 @@ jfg_status launch_elements(jfg_model *m, bool kg, const Batch &bt) {
         o.h_stride = m->nq + m->nt;
         const int tt = m->t3kg_threads, W3 = m->t3_warps;
         if (kg)
-            t3_kg_kernel<<<dim3((unsigned)cdiv(m->nt, tt), nv), tt, 0, m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords,
+            t3_kg_kernel<<<dim3((unsigned)cdiv(m->nt, tt), nv), tt, (size_t)tt * T3KG_STAGE_STRIDE * sizeof(double), m->stream>>>(m->nt, m->d_t3n, m->d_t3p, m->d_coords,
                                                                                    m->d_nodeR, du, o);
         else if (W3 == 2)
             t3_k_kernel<2><<<dim3((unsigned)cdiv(m->nt, T3_TEAMS_PER_WARP * 2), nv), 64, 0, m->stream>>>(

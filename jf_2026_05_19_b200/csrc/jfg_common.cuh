@@ -234,5 +234,7 @@ JFG_D void slot_copy(double *dst, const double *src, uint32_t bytes) {
                  :: "l"(dst), "r"(s), "r"(bytes) : "memory");
 }
 JFG_D void slot_copies_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// All but the most recent copy have read their shared memory (double-buffered staging).
+JFG_D void slot_copies_read_but_last() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
 
 }  // namespace jfg
